@@ -1,0 +1,94 @@
+// Device-side data layout and helpers shared by every kernel of the aerocfd
+// residual-and-update path.
+//
+// Layout in HBM: one arena per case.  Each block owns, for every field, a
+// structure-of-arrays set of component planes over its full index box
+// is..ie x js..je x ks..ke (overlap ghosts included), i fastest, then j, then k.
+// Component c (1-based, as in the reference) of node (i,j,k) of field f lives at
+//   f + (c-1)*plane + (i-is) + nx*((j-js) + ny*(k-ks)),
+// with `plane` the box size rounded up to 32 doubles so every plane starts on a
+// 256-byte boundary.  The reference's host arrays are (component, i, j, k)
+// column-major; the transfer kernels in aero_transfer.cu convert between the two.
+#pragma once
+#include <cstdint>
+
+namespace aero {
+
+// Field ids of the C-ABI (AERO_F_* in include/aerocfd_gpu.h).
+enum FieldId {
+  F_Q = 0, F_PRI, F_RHSI, F_RHSV, F_RHS, F_DT, F_DXIDX, F_INVJ, F_AMU, F_NUT, F_SARHS,
+  F_X, F_Y, F_Z, F_DIST, F_ALPHA, F_BETA, F_GAMMA, F_DUDX, F_TAO, F_VOR, F_LENGTH, F_SPACING,
+  // device-only scratch
+  F_RA, F_RB, F_RC, F_DIAG, F_DQS, F_DQ, F_FVH, F_DIASD,
+  F_NUM
+};
+__host__ __device__ constexpr int field_nc(int f) {
+  return f == F_Q ? 5 : f == F_PRI ? 7 : f == F_RHSI ? 5 : f == F_RHSV ? 5 : f == F_RHS ? 5
+       : f == F_DXIDX ? 9 : f == F_AMU ? 3 : f == F_ALPHA ? 3 : f == F_BETA ? 3 : f == F_GAMMA ? 3
+       : f == F_DUDX ? 9 : f == F_TAO ? 6 : f == F_DQS ? 5 : f == F_DQ ? 5 : f == F_FVH ? 15 : 1;
+}
+constexpr int kNumPublicFields = F_SPACING + 1;
+
+struct Box {
+  int is, ie, js, je, ks, ke;
+  __host__ __device__ int nx() const { return ie - is + 1; }
+  __host__ __device__ int ny() const { return je - js + 1; }
+  __host__ __device__ int nz() const { return ke - ks + 1; }
+  __host__ __device__ long size() const { return (long)nx() * ny() * nz(); }
+  __host__ __device__ bool contains(int i, int j, int k) const {
+    return i >= is && i <= ie && j >= js && j <= je && k >= ks && k <= ke;
+  }
+};
+
+// Everything a kernel needs to address one block's fields.
+struct BlockView {
+  Box b, b0, b1;
+  int nx, ny;
+  long plane;            // doubles between component planes
+  double* f[F_NUM];      // base of component 1 of each field (nullptr if absent)
+
+  __device__ __forceinline__ long at(int i, int j, int k) const {
+    return (long)(i - b.is) + (long)nx * ((long)(j - b.js) + (long)ny * (long)(k - b.ks));
+  }
+  __device__ __forceinline__ double& v(int fid, int c, long n) const { return f[fid][(long)(c - 1) * plane + n]; }
+  __device__ __forceinline__ double& s(int fid, long n) const { return f[fid][n]; }
+};
+
+// Per-case scalars (module ns_const / flag_var values the path reads).
+struct CaseConsts {
+  double gamma, cv, re, tinf, prl, prt, cfl;
+  double d_0, u_0, p_0, c_0, aoa, nutinf;
+  int dimension, solver, time, turbulence, des, bufferLength;
+};
+
+// ---------------------------------------------------------------- arithmetic
+// Integer powers follow gfortran's powi expansion; x**2 is x*x.
+__device__ __forceinline__ double p2(double x) { return x * x; }
+__device__ __forceinline__ double p3(double x) { double x2 = x * x; return x2 * x; }
+__device__ __forceinline__ double p5(double x) { double x2 = x * x; double x3 = x2 * x; return x3 * x2; }
+__device__ __forceinline__ double p6(double x) { double x2 = x * x; double x3 = x2 * x; return x3 * x3; }
+
+// Spalart-Allmaras constants (module_tursa.f90:4-10).
+constexpr double SA_DTA = 2.0 / 3.0, SA_KAR = 0.41;
+constexpr double SA_CB1 = 0.1355, SA_CB2 = 0.622;
+constexpr double SA_CW1 = SA_CB1 / SA_KAR / SA_KAR + (1.0 + SA_CB2) / SA_DTA;
+constexpr double SA_CW2 = 0.3, SA_CW3 = 2.0;
+constexpr double SA_CT3 = 1.2, SA_CT4 = 0.5;
+constexpr double SA_CV1 = 7.1;
+constexpr double SA_KAR2 = SA_KAR * SA_KAR;
+constexpr double SA_CV13 = SA_CV1 * SA_CV1 * SA_CV1;
+
+// Reference flag values (module_flags.f90:30-87).
+enum {
+  IFLAG_2D = 2, IFLAG_3D = 3, IFLAG_NSSOLVER = 0, IFLAG_EULERSOLVER = 1,
+  IFLAG_STEADY = 0, IFLAG_UNSTEADY = 1, IFLAG_LAMINAR = 0, IFLAG_SA = 2,
+  IFLAG_DES97 = 1, IFLAG_DDES = 2,
+  BC_INFLOW = -50, BC_OUTFLOW = -40, BC_SYMM = -30, BC_WALL = -20, BC_FARFIELD = -10,
+};
+
+// Device status word bits (aero_get_status).
+enum StatusBits : unsigned {
+  ST_NEG_DENSITY = 1u, ST_NONFINITE_RESIDUAL = 2u, ST_NEG_PRESSURE = 4u, ST_TIMEOUT = 8u,
+};
+
+}  // namespace aero

@@ -1,0 +1,415 @@
+// Residual kernels: primitive variables, inviscid flux (WENO3 + Roe), viscous
+// flux and the local time step.  Every kernel keeps the reference's operation
+// order (this file is compiled with -fmad=false in the parity build), so the FP64
+// path reproduces the CPU result to the last bit except in libm functions.
+#include <cmath>
+
+#include "aero_device.cuh"
+#include "aero_kernels.h"
+
+namespace aero {
+
+// ----------------------------------------------------------------- primitives
+// sub_getpri_v.f90:19-62, over the full box of every block.
+__global__ void k_getpri(const BlockView* __restrict__ blocks, CaseConsts cc, unsigned* status) {
+  const BlockView& B = blocks[blockIdx.y];
+  long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long N = B.b.size();
+  if (n >= N) return;
+  double d = B.v(F_Q, 1, n);
+  double u = B.v(F_Q, 2, n) / d;
+  double v = B.v(F_Q, 3, n) / d;
+  double w = B.v(F_Q, 4, n) / d;
+  double q2 = 0.5 * (u * u + v * v + w * w);
+  double e = B.v(F_Q, 5, n) / d;
+  double t = (e - q2) / cc.cv;
+  double p = (B.v(F_Q, 5, n) - q2 * d) * (cc.gamma - 1.0);
+  double c = sqrt(cc.gamma * p / d);
+  B.v(F_PRI, 1, n) = d;
+  B.v(F_PRI, 2, n) = u;
+  B.v(F_PRI, 3, n) = v;
+  B.v(F_PRI, 4, n) = w;
+  B.v(F_PRI, 5, n) = p;
+  B.v(F_PRI, 6, n) = t;
+  B.v(F_PRI, 7, n) = c;
+  if (d < 0.0 && status) atomicOr(status, (unsigned)ST_NEG_DENSITY);
+}
+
+// -------------------------------------------------------------- inviscid flux
+// WENO3 weights and state (sub_inviscid_upwind.f90:32-41 right, :57-66 left).
+__device__ __forceinline__ double weno_right(double u1, double u2, double u3) {
+  const double eps = 1.0e-6;
+  double s1 = p2(u2 - u3);
+  double s2 = p2(u1 - u2);
+  double a1 = 1.0 / (3.0 * p2(eps + s1));
+  double a2 = 2.0 / (3.0 * p2(eps + s2));
+  double w1 = a1 / (a1 + a2);
+  double w2 = a2 / (a1 + a2);
+  return w1 * (-u3 / 2.0 + 3.0 * u2 / 2.0) + w2 * (u2 / 2.0 + u1 / 2.0);
+}
+__device__ __forceinline__ double weno_left(double u1, double u2, double u3) {
+  const double eps = 1.0e-6;
+  double s1 = p2(u2 - u1);
+  double s2 = p2(u3 - u2);
+  double a1 = 1.0 / (3.0 * p2(eps + s1));
+  double a2 = 2.0 / (3.0 * p2(eps + s2));
+  double w1 = a1 / (a1 + a2);
+  double w2 = a2 / (a1 + a2);
+  return w1 * (-u1 / 2.0 + 3.0 * u2 / 2.0) + w2 * (u2 / 2.0 + u3 / 2.0);
+}
+
+// Roe flux at face (node n, node n+s) along `coord` from conservative left/right
+// states (sub_inviscid1.f90:58-74 then sub_inviscid_splitting.f90:65-162).
+__device__ __forceinline__ void roe_face(const BlockView& B, int coord, long n, long ns,
+                                         const double ulc[5], const double urc[5], double gamma,
+                                         double flux[5]) {
+  double dl = ulc[0], ul = ulc[1] / ulc[0], vl = ulc[2] / ulc[0], wl = ulc[3] / ulc[0];
+  double pl = (ulc[4] - 0.5 * (p2(ulc[1]) + p2(ulc[2]) + p2(ulc[3])) / ulc[0]) * (gamma - 1.0);
+  double dr = urc[0], ur = urc[1] / urc[0], vr = urc[2] / urc[0], wr = urc[3] / urc[0];
+  double pr = (urc[4] - 0.5 * (p2(urc[1]) + p2(urc[2]) + p2(urc[3])) / urc[0]) * (gamma - 1.0);
+
+  int c1 = coord * 3 - 2;
+  double ja = B.s(F_INVJ, n), jb = B.s(F_INVJ, ns);
+  double dxidx1 = 0.5 * (B.v(F_DXIDX, c1, n) * ja + B.v(F_DXIDX, c1, ns) * jb);
+  double dxidy1 = 0.5 * (B.v(F_DXIDX, c1 + 1, n) * ja + B.v(F_DXIDX, c1 + 1, ns) * jb);
+  double dxidz1 = 0.5 * (B.v(F_DXIDX, c1 + 2, n) * ja + B.v(F_DXIDX, c1 + 2, ns) * jb);
+  double temp = sqrt(p2(dxidx1) + p2(dxidy1) + p2(dxidz1));
+  double dxidx0 = dxidx1 / temp, dxidy0 = dxidy1 / temp, dxidz0 = dxidz1 / temp;
+
+  double hl = gamma * pl / ((gamma - 1.0) * dl) + 0.5 * (p2(ul) + p2(vl) + p2(wl));
+  double hr = gamma * pr / ((gamma - 1.0) * dr) + 0.5 * (p2(ur) + p2(vr) + p2(wr));
+  double uul = ul * dxidx1 + vl * dxidy1 + wl * dxidz1;
+  double uur = ur * dxidx1 + vr * dxidy1 + wr * dxidz1;
+  double ubarl = uul / temp, ubarr = uur / temp;
+
+  double fl0 = dl * uul, fl1 = dl * ul * uul + dxidx1 * pl, fl2 = dl * vl * uul + dxidy1 * pl;
+  double fl3 = dl * wl * uul + dxidz1 * pl, fl4 = dl * hl * uul;
+  double fr0 = dr * uur, fr1 = dr * ur * uur + dxidx1 * pr, fr2 = dr * vr * uur + dxidy1 * pr;
+  double fr3 = dr * wr * uur + dxidz1 * pr, fr4 = dr * hr * uur;
+
+  double tmpp = sqrt(dr / dl);
+  double avd = sqrt(dl * dr);
+  double avu = (ul + ur * tmpp) / (1.0 + tmpp);
+  double avv = (vl + vr * tmpp) / (1.0 + tmpp);
+  double avw = (wl + wr * tmpp) / (1.0 + tmpp);
+  double avh = (hl + hr * tmpp) / (1.0 + tmpp);
+  double ava = sqrt((gamma - 1.0) * (avh - 0.5 * (p2(avu) + p2(avv) + p2(avw))));
+  double avuu = avu * dxidx0 + avv * dxidy0 + avw * dxidz0;
+
+  const double delt = 0.06;
+  double lam[5] = {fabs(avuu - ava), fabs(avuu), fabs(avuu), fabs(avuu), fabs(avuu + ava)};
+#pragma unroll
+  for (int m = 0; m < 5; ++m) {  // Harten entropy fix (sub_inviscid_splitting.f90:122-130)
+    double tmp = copysign(1.0, delt - lam[m]);
+    double tmp1 = 0.5 * (1.0 - tmp);
+    double tmp2 = 0.5 * (1.0 + tmp);
+    double harten = (p2(lam[m]) + p2(delt)) / (2.0 * delt);
+    lam[m] = tmp1 * lam[m] + tmp2 * harten;
+  }
+  double deltad = dr - dl, deltap = pr - pl;
+  double deltau = ur - ul, deltav = vr - vl, deltaw = wr - wl;
+  double deltauu = ubarr - ubarl;
+  double alpha1 = lam[1] * (deltad - deltap / p2(ava));
+  double alpha2 = lam[4] * (deltap + avd * ava * deltauu) / (2.0 * p2(ava));
+  double alpha3 = lam[0] * (deltap - avd * ava * deltauu) / (2.0 * p2(ava));
+  double alpha4 = alpha1 + alpha2 + alpha3;
+  double alpha5 = ava * (alpha2 - alpha3);
+  double alpha6 = lam[1] * (avd * deltau - avd * deltauu * dxidx0);
+  double alpha7 = lam[1] * (avd * deltav - avd * deltauu * dxidy0);
+  double alpha8 = lam[1] * (avd * deltaw - avd * deltauu * dxidz0);
+  double f0 = alpha4;
+  double f1 = avu * alpha4 + alpha5 * dxidx0 + alpha6;
+  double f2 = avv * alpha4 + alpha5 * dxidy0 + alpha7;
+  double f3 = avw * alpha4 + alpha5 * dxidz0 + alpha8;
+  double f4 = avh * alpha4 + avuu * alpha5 + avu * alpha6 + avv * alpha7 + avw * alpha8 -
+              p2(ava) * alpha1 / (gamma - 1.0);
+  flux[0] = 0.5 * (fl0 + fr0 - temp * f0);
+  flux[1] = 0.5 * (fl1 + fr1 - temp * f1);
+  flux[2] = 0.5 * (fl2 + fr2 - temp * f2);
+  flux[3] = 0.5 * (fl3 + fr3 - temp * f3);
+  flux[4] = 0.5 * (fl4 + fr4 - temp * f4);
+}
+
+// Flux through face pos+1/2 along `coord` starting at node (i,j,k); pos is the
+// node's index along coord, lo/hi the full-box bounds along coord, st the
+// linear stride along coord.
+__device__ __forceinline__ void face_flux(const BlockView& B, int coord, long n, int pos, int lo,
+                                          int hi, long st, double gamma, double flux[5]) {
+  double ulc[5], urc[5];
+  bool rone = (pos == hi - 1);  // right state one-sided at ie-1 (:25-26)
+  bool lone = (pos == lo);      // left state one-sided at is (:50-51)
+#pragma unroll
+  for (int c = 1; c <= 5; ++c) {
+    double f0 = B.v(F_Q, c, n);
+    double fp = B.v(F_Q, c, n + st);
+    if (rone) {
+      urc[c - 1] = fp;
+    } else {
+      double fpp = B.v(F_Q, c, n + 2 * st);
+      urc[c - 1] = weno_right(f0, fp, fpp);
+    }
+    if (lone) {
+      ulc[c - 1] = f0;
+    } else {
+      double fm = B.v(F_Q, c, n - st);
+      ulc[c - 1] = weno_left(fm, f0, fp);
+    }
+  }
+  roe_face(B, coord, n, n + st, ulc, urc, gamma, flux);
+}
+
+// sub_inviscid1.f90:8-189: rhsi on the updated nodes, one thread per node.
+// Directions are accumulated in the reference's order: rhsi = -dF; rhsi -= dG;
+// rhsi -= dH.
+__global__ void k_inviscid(const BlockView* __restrict__ blocks, CaseConsts cc) {
+  const BlockView& B = blocks[blockIdx.y];
+  const Box& b1 = B.b1;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long N1 = b1.size();
+  if (t >= N1) return;
+  int i = b1.is + (int)(t % b1.nx());
+  long r = t / b1.nx();
+  int j = b1.js + (int)(r % b1.ny());
+  int k = b1.ks + (int)(r / b1.ny());
+  long n = B.at(i, j, k);
+  const long st[3] = {1, (long)B.nx, (long)B.nx * B.ny};
+  const int pos[3] = {i, j, k};
+  const int lo[3] = {B.b.is, B.b.js, B.b.ks};
+  const int hi[3] = {B.b.ie, B.b.je, B.b.ke};
+  double acc[5];
+  int ndir = cc.dimension == IFLAG_3D ? 3 : 2;
+  for (int d = 0; d < ndir; ++d) {
+    double fm[5], fp[5];
+    face_flux(B, d + 1, n - st[d], pos[d] - 1, lo[d], hi[d], st[d], cc.gamma, fm);
+    face_flux(B, d + 1, n, pos[d], lo[d], hi[d], st[d], cc.gamma, fp);
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      double dd = fp[c] - fm[c];
+      acc[c] = (d == 0) ? -dd : acc[c] - dd;
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 5; ++c) B.v(F_RHSI, c + 1, n) = acc[c];
+}
+
+// Zero-fills one field over the full box of every block (the reference's
+// `rhsi = 0.d0`, sub_inviscid1.f90:40, and similar whole-array assignments).
+__global__ void k_fill(const BlockView* __restrict__ blocks, int fid, int nc, double val) {
+  const BlockView& B = blocks[blockIdx.y];
+  long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long N = B.b.size();
+  if (n >= N || !B.f[fid]) return;
+  for (int c = 1; c <= nc; ++c) B.v(fid, c, n) = val;
+}
+
+// --------------------------------------------------------------- viscous flux
+// Central difference along one direction inside the physical range, one-sided
+// at its ends (sub_viscous.f90:106-178 and :296-340).
+__device__ __forceinline__ double cdiff(const double* f, long n, long st, int pos, int lo, int hi) {
+  if (pos == lo) return f[n + st] - f[n];
+  if (pos == hi) return f[n] - f[n - st];
+  return (f[n + st] - f[n - st]) / 2.0;
+}
+
+// sub_viscous.f90:187-293: gradients, Sutherland viscosity, stresses, heat flux,
+// vorticity and the contravariant viscous fluxes on the physical nodes.  The
+// fluxes fv,gv,hv (components 2..5 each) go to the FVH scratch field.
+__global__ void k_viscous_a(const BlockView* __restrict__ blocks, CaseConsts cc, int store_dudx_tao) {
+  const BlockView& B = blocks[blockIdx.y];
+  const Box& b0 = B.b0;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b0.size()) return;
+  int i = b0.is + (int)(t % b0.nx());
+  long r = t / b0.nx();
+  int j = b0.js + (int)(r % b0.ny());
+  int k = b0.ks + (int)(r / b0.ny());
+  long n = B.at(i, j, k);
+  const long st[3] = {1, (long)B.nx, (long)B.nx * B.ny};
+  const int pos[3] = {i, j, k};
+  const int lo[3] = {b0.is, b0.js, b0.ks};
+  const int hi[3] = {b0.ie, b0.je, b0.ke};
+  const double* pu = B.f[F_PRI] + 1 * B.plane;
+  const double* pv = B.f[F_PRI] + 2 * B.plane;
+  const double* pw = B.f[F_PRI] + 3 * B.plane;
+  const double* pt = B.f[F_PRI] + 5 * B.plane;
+  double gt[3] = {0, 0, 0}, gu[3] = {0, 0, 0}, gv[3] = {0, 0, 0}, gw[3] = {0, 0, 0};
+  int ndir = cc.dimension == IFLAG_3D ? 3 : 2;
+  for (int d = 0; d < ndir; ++d) {
+    gt[d] = cdiff(pt, n, st[d], pos[d], lo[d], hi[d]);
+    gu[d] = cdiff(pu, n, st[d], pos[d], lo[d], hi[d]);
+    gv[d] = cdiff(pv, n, st[d], pos[d], lo[d], hi[d]);
+    gw[d] = cdiff(pw, n, st[d], pos[d], lo[d], hi[d]);
+  }
+  double u0 = pu[n], v0 = pv[n], w0 = pw[n], t0 = pt[n];
+  double amu1 = (1.0 + 124.0 / cc.tinf) / (t0 + 124.0 / cc.tinf) * pow(t0, 1.5);
+  double amu2 = B.v(F_AMU, 2, n);
+  double amu3 = amu1 + amu2;
+  B.v(F_AMU, 1, n) = amu1;
+  B.v(F_AMU, 3, n) = amu3;
+  double ki = cc.gamma * cc.cv * (amu1 / cc.prl + amu2 / cc.prt);
+  double m[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) m[c] = B.v(F_DXIDX, c + 1, n);
+  double tx = gt[0] * m[0] + gt[1] * m[3] + gt[2] * m[6];
+  double ty = gt[0] * m[1] + gt[1] * m[4] + gt[2] * m[7];
+  double tz = gt[0] * m[2] + gt[1] * m[5] + gt[2] * m[8];
+  double du[9];
+  const double* g[3] = {gu, gv, gw};
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) du[3 * a + c] = g[a][0] * m[c] + g[a][1] * m[c + 3] + g[a][2] * m[c + 6];
+  double ta[6];
+  ta[0] = amu3 * (4.0 / 3.0 * du[0] - 2.0 / 3.0 * (du[4] + du[8]));
+  ta[1] = amu3 * (du[1] + du[3]);
+  ta[2] = amu3 * (du[6] + du[2]);
+  ta[3] = amu3 * (4.0 / 3.0 * du[4] - 2.0 / 3.0 * (du[0] + du[8]));
+  ta[4] = amu3 * (du[7] + du[5]);
+  ta[5] = amu3 * (4.0 / 3.0 * du[8] - 2.0 / 3.0 * (du[0] + du[4]));
+  double bx = u0 * ta[0] + v0 * ta[1] + w0 * ta[2] + ki * tx;
+  double by = u0 * ta[1] + v0 * ta[3] + w0 * ta[4] + ki * ty;
+  double bz = u0 * ta[2] + v0 * ta[4] + w0 * ta[5] + ki * tz;
+  B.s(F_VOR, n) = sqrt(p2(du[5] - du[7]) + p2(du[2] - du[6]) + p2(du[1] - du[3]));
+  if (store_dudx_tao) {
+#pragma unroll
+    for (int c = 0; c < 9; ++c) B.v(F_DUDX, c + 1, n) = du[c];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) B.v(F_TAO, c + 1, n) = ta[c];
+  }
+  double ij = B.s(F_INVJ, n);
+  double* fvh = B.f[F_FVH];
+  long P = B.plane;
+  // fv/gv/hv components 2..5 -> FVH planes 0..3 (fv), 4..7 (gv), 8..11 (hv)
+#pragma unroll
+  for (int dd = 0; dd < 3; ++dd) {
+    double x1 = m[3 * dd], x2 = m[3 * dd + 1], x3 = m[3 * dd + 2];
+    fvh[(4 * dd + 0) * P + n] = (x1 * ta[0] + x2 * ta[1] + x3 * ta[2]) * ij;
+    fvh[(4 * dd + 1) * P + n] = (x1 * ta[1] + x2 * ta[3] + x3 * ta[4]) * ij;
+    fvh[(4 * dd + 2) * P + n] = (x1 * ta[2] + x2 * ta[4] + x3 * ta[5]) * ij;
+    fvh[(4 * dd + 3) * P + n] = (x1 * bx + x2 * by + x3 * bz) * ij;
+  }
+}
+
+// sub_viscous.f90:296-365: rhsv = (d fv/dxi + d gv/deta + d hv/dzeta)/re.
+__global__ void k_viscous_b(const BlockView* __restrict__ blocks, CaseConsts cc) {
+  const BlockView& B = blocks[blockIdx.y];
+  const Box& b0 = B.b0;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b0.size()) return;
+  int i = b0.is + (int)(t % b0.nx());
+  long r = t / b0.nx();
+  int j = b0.js + (int)(r % b0.ny());
+  int k = b0.ks + (int)(r / b0.ny());
+  long n = B.at(i, j, k);
+  const long st[3] = {1, (long)B.nx, (long)B.nx * B.ny};
+  const int pos[3] = {i, j, k};
+  const int lo[3] = {b0.is, b0.js, b0.ks};
+  const int hi[3] = {b0.ie, b0.je, b0.ke};
+  const double* fvh = B.f[F_FVH];
+  long P = B.plane;
+  bool three = cc.dimension == IFLAG_3D;
+  B.v(F_RHSV, 1, n) = 0.0;  // fv(1)=gv(1)=hv(1)=0: ((0+0)+0)/re
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    double a = cdiff(fvh + (0 + c) * P, n, st[0], pos[0], lo[0], hi[0]);
+    double b = cdiff(fvh + (4 + c) * P, n, st[1], pos[1], lo[1], hi[1]);
+    double h = three ? cdiff(fvh + (8 + c) * P, n, st[2], pos[2], lo[2], hi[2]) : 0.0;
+    B.v(F_RHSV, c + 2, n) = (a + b + h) / cc.re;
+  }
+}
+
+// ------------------------------------------------------------------ time step
+// sub_timeadvancement_finddt.f90:52-88 (steady).  Besides dt, each CTA writes
+// the maximum of its dt values (NaN skipped) for the quirk-exact dtmax/dtmin
+// reduction in k_dt_minmax.
+__global__ void k_find_dt(const BlockView* __restrict__ blocks, CaseConsts cc, double* cta_max) {
+  const BlockView& B = blocks[blockIdx.y];
+  long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long N = B.b.size();
+  double dt = nan("");
+  if (n < N) {
+    double m[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) m[c] = B.v(F_DXIDX, c + 1, n);
+    double tempxi = sqrt(p2(m[0]) + p2(m[1]) + p2(m[2]));
+    double tempeta = sqrt(p2(m[3]) + p2(m[4]) + p2(m[5]));
+    double tempzeta = sqrt(p2(m[6]) + p2(m[7]) + p2(m[8]));
+    double d0 = B.v(F_PRI, 1, n), u0 = B.v(F_PRI, 2, n), v0 = B.v(F_PRI, 3, n);
+    double w0 = B.v(F_PRI, 4, n), c0 = B.v(F_PRI, 7, n);
+    double uu = (m[0] * u0 + m[1] * v0 + m[2] * w0) / tempxi;
+    double vv = (m[3] * u0 + m[4] * v0 + m[5] * w0) / tempeta;
+    double ww = (m[6] * u0 + m[7] * v0 + m[8] * w0) / tempzeta;
+    double m3 = B.v(F_AMU, 3, n);
+    double t1 = fabs(uu) + c0 + 2.0 * tempxi * m3 * 4.0 / 3.0 / cc.re / d0;
+    double t2 = fabs(vv) + c0 + 2.0 * tempeta * m3 * 4.0 / 3.0 / cc.re / d0;
+    double t3 = fabs(ww) + c0 + 2.0 * tempzeta * m3 * 4.0 / 3.0 / cc.re / d0;
+    dt = cc.cfl / (tempxi * t1 + tempeta * t2 + tempzeta * t3);
+    B.s(F_DT, n) = dt;
+  }
+  if (cta_max) {
+    // block-wide max ignoring NaN
+    __shared__ double sm[32];
+    double v = (dt == dt) ? dt : -INFINITY;
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      v = (threadIdx.x < (blockDim.x >> 5)) ? sm[threadIdx.x] : -INFINITY;
+      for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+      if (threadIdx.x == 0) cta_max[(long)blockIdx.y * gridDim.x + blockIdx.x] = v;
+    }
+  }
+}
+
+// Reproduces find_dt's running `if (dt >= dtmax) ... else if (dt <= dtmin)`
+// (sub_timeadvancement_finddt.f90:81-85) for block `m` with one CTA: dtmax is
+// the plain maximum; dtmin is the minimum over nodes that did not set a new
+// running maximum when visited in (k,j,i) order.  Each thread scans a
+// contiguous chunk seeded with the exclusive prefix maximum of the chunk
+// maxima, so the result equals the serial loop.
+__global__ void k_dt_minmax(const BlockView* __restrict__ blocks, int m, const double* cta_max,
+                            int ncta, int cta_size, double* out2) {
+  const BlockView& B = blocks[m];
+  long N = B.b.size();
+  __shared__ double pref[1024];
+  __shared__ double red[1024];
+  int T = blockDim.x;
+  long chunk = (N + T - 1) / T;
+  // chunk maxima
+  double cm = -INFINITY;
+  long lo = (long)threadIdx.x * chunk, hi = min(N, lo + chunk);
+  for (long n = lo; n < hi; ++n) {
+    double v = B.s(F_DT, n);
+    if (v == v) cm = fmax(cm, v);
+  }
+  (void)cta_max; (void)ncta; (void)cta_size;
+  pref[threadIdx.x] = cm;
+  __syncthreads();
+  // inclusive scan (max), Hillis-Steele
+  for (int o = 1; o < T; o <<= 1) {
+    double x = pref[threadIdx.x];
+    if (threadIdx.x >= o) x = fmax(x, pref[threadIdx.x - o]);
+    __syncthreads();
+    pref[threadIdx.x] = x;
+    __syncthreads();
+  }
+  double run = (threadIdx.x == 0) ? 0.0 : fmax(0.0, pref[threadIdx.x - 1]);  // dtmax starts at 0
+  double mn = INFINITY;
+  for (long n = lo; n < hi; ++n) {
+    double v = B.s(F_DT, n);
+    if (v >= run) run = v;           // NaN compares false on both branches
+    else if (v == v) mn = fmin(mn, v);
+  }
+  red[threadIdx.x] = mn;
+  __syncthreads();
+  for (int o = T / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] = fmin(red[threadIdx.x], red[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out2[0] = fmax(0.0, pref[T - 1]);
+    out2[1] = fmin(1.0e10, red[0]);  // dtmin starts at 1e10 and only moves down
+  }
+}
+
+}  // namespace aero

@@ -1,0 +1,65 @@
+// Kernel declarations and the device tables built by the host runtime.
+#pragma once
+#include "aero_device.cuh"
+
+namespace aero {
+
+// Physical boundary operation on one subface; types resolved on the host from
+// blk_t and the solver (sub_bc.f90:39-60).
+enum BcType { BCT_INFLOW = 0, BCT_OUTFLOW, BCT_MIRROR, BCT_NOSLIP, BCT_FARFIELD };
+struct BcOp {
+  int type;
+  int face;
+  Box sb;  // subface box exactly as the BC routine receives it
+};
+
+// One ghost node of the halo and the interior node it copies.
+struct HaloEntry {
+  int dst_blk, src_blk;
+  long dst_n, src_n;
+};
+enum HaloMode { HALO_Q = 0, HALO_Q_NUT = 1, HALO_COORD = 2 };
+
+// average1 source (the neighbour's interface node) and average2 destination
+// (own interface node with its contributions buf[first .. first+count)).
+struct AvgSrc {
+  int blk;
+  long n;
+};
+struct AvgDst {
+  int blk;
+  int first, count;
+  long n;
+};
+
+__global__ void k_getpri(const BlockView* __restrict__ blocks, CaseConsts cc, unsigned* status);
+__global__ void k_fill(const BlockView* __restrict__ blocks, int fid, int nc, double val);
+__global__ void k_inviscid(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_viscous_a(const BlockView* __restrict__ blocks, CaseConsts cc, int store_dudx_tao);
+__global__ void k_viscous_b(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_find_dt(const BlockView* __restrict__ blocks, CaseConsts cc, double* cta_max);
+__global__ void k_dt_minmax(const BlockView* __restrict__ blocks, int m, const double* cta_max,
+                            int ncta, int cta_size, double* out2);
+__global__ void k_lusgs_prep(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_lusgs_sweep(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_physical_bc(const BlockView* __restrict__ blocks, const BcOp* __restrict__ ops,
+                              const int* __restrict__ op_start, CaseConsts cc);
+__global__ void k_sa_clip(const BlockView* __restrict__ blocks);
+__global__ void k_halo(const BlockView* __restrict__ blocks, const HaloEntry* __restrict__ map,
+                       long nmap, int mode);
+__global__ void k_avg_gather(const BlockView* __restrict__ blocks, const AvgSrc* __restrict__ src,
+                             long nsrc, double* __restrict__ buf, int with_nut);
+__global__ void k_avg_apply(const BlockView* __restrict__ blocks, const AvgDst* __restrict__ dst,
+                            long ndst, const double* __restrict__ buf, int with_nut);
+__global__ void k_residual_partial(const BlockView* __restrict__ blocks, double* __restrict__ part,
+                                   int with_sa);
+__global__ void k_residual_final(const double* __restrict__ part, long npart, double totalnodes,
+                                 double* __restrict__ out7, unsigned* status);
+// Host (Fortran column-major, component fastest) <-> device (component planes).
+__global__ void k_aos_to_soa(const double* __restrict__ src, double* __restrict__ dst, long n,
+                             int nc, long plane);
+__global__ void k_soa_to_aos(const double* __restrict__ src, double* __restrict__ dst, long n,
+                             int nc, long plane);
+__global__ void k_fill_plane(double* __restrict__ p, long n, double val);
+
+}  // namespace aero

@@ -1,0 +1,799 @@
+// Host runtime and C-ABI of libaerocfd_gpu.so (declared in include/aerocfd_gpu.h).
+//
+// State mirrors the reference's module variables: the flag and constant values
+// of Control.in (flag_var, ns_const, sa_var), the per-block index boxes and
+// subfaces (blk_var, glbindex_var), and, once registered, the per-block arrays,
+// which live on the device in one arena and are copied to or from the caller's
+// host arrays only on request.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/aerocfd_gpu.h"
+#include "aero_device.cuh"
+#include "aero_kernels.h"
+#include "aero_topology.h"
+
+using namespace aero;
+
+namespace {
+
+struct HostBlock {
+  bool used = false;
+  Box b{}, b0{}, b1{};
+  std::vector<SubRow> subs;
+  double* host[kNumPublicFields] = {};
+  bool pinned[kNumPublicFields] = {};
+  long plane = 0;
+  size_t arena_off = 0;  // doubles
+};
+
+struct State {
+  bool inited = false;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool configured = false;
+  int iflags[8] = {};
+  double params[7] = {};
+  CaseConsts cc{};
+  std::vector<HostBlock> blocks;
+  bool setup = false;
+  // device
+  double* arena = nullptr;
+  size_t arena_doubles = 0;
+  BlockView* d_blocks = nullptr;
+  std::vector<BlockView> views;
+  BcOp* d_bc_ops = nullptr;
+  int* d_bc_start = nullptr;
+  HaloEntry* d_halo = nullptr;
+  long nhalo = 0;
+  AvgSrc* d_avg_src = nullptr;
+  AvgDst* d_avg_dst = nullptr;
+  long navg_src = 0, navg_dst = 0;
+  double* d_avg_buf = nullptr;
+  double* d_part = nullptr;
+  int resid_ctas = 0;
+  double* d_out = nullptr;   // residual (7) + dt min/max (2)
+  double* h_out = nullptr;   // pinned
+  unsigned* d_status = nullptr;
+  double* d_staging = nullptr;
+  size_t staging_doubles = 0;
+  double totalnodes = 0;
+  long max_box = 0, max_b0 = 0, max_b1 = 0, max_ext = 0;
+  std::map<const double*, std::pair<int, int>> registry;  // host array -> (block, field)
+  // transient mode pool
+  double* t_arena = nullptr;
+  size_t t_doubles = 0;
+  BlockView* d_tview = nullptr;
+  double* d_tmax = nullptr;
+  size_t t_tmax = 0;
+  std::string err;
+};
+
+State g;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g.err = buf;
+  return code;
+}
+
+#define CK(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return fail(e_ == cudaErrorMemoryAllocation ? AERO_ERR_NOMEM : AERO_ERR_CUDA,       \
+                  "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+#define CKL() CK(cudaGetLastError())
+
+long round32(long n) { return (n + 31) / 32 * 32; }
+unsigned cdiv(long a, long b) { return (unsigned)((a + b - 1) / b); }
+
+Box box_of(const int* is, const int* ie, const int* js, const int* je, const int* ks, const int* ke) {
+  return Box{*is, *ie, *js, *je, *ks, *ke};
+}
+bool same(const Box& a, const Box& b) {
+  return a.is == b.is && a.ie == b.ie && a.js == b.js && a.je == b.je && a.ks == b.ks && a.ke == b.ke;
+}
+
+int need_init() {
+  if (!g.inited) return fail(AERO_ERR_STATE, "aero_init has not been called");
+  return AERO_OK;
+}
+int need_setup() {
+  if (!g.inited || !g.setup) return fail(AERO_ERR_STATE, "case set-up is not finished (aero_finish_setup)");
+  return AERO_OK;
+}
+
+// Every field of a view gets `plane`-strided component planes.
+size_t view_doubles(long plane) {
+  size_t s = 0;
+  for (int f = 0; f < F_NUM; ++f) s += (size_t)field_nc(f) * plane;
+  return s;
+}
+void fill_view(BlockView& v, const Box& b, const Box& b0, const Box& b1, long plane, double* base) {
+  v.b = b; v.b0 = b0; v.b1 = b1;
+  v.nx = b.nx(); v.ny = b.ny();
+  v.plane = plane;
+  size_t off = 0;
+  for (int f = 0; f < F_NUM; ++f) {
+    v.f[f] = base + off;
+    off += (size_t)field_nc(f) * plane;
+  }
+}
+
+int ensure_staging(size_t doubles) {
+  if (doubles <= g.staging_doubles) return AERO_OK;
+  if (g.d_staging) CK(cudaFree(g.d_staging));
+  g.d_staging = nullptr;
+  CK(cudaMalloc(&g.d_staging, doubles * sizeof(double)));
+  g.staging_doubles = doubles;
+  return AERO_OK;
+}
+
+// host (c, i, j, k) column-major <-> one field of a view
+int upload(const double* host, double* dev_field, long n, int nc, long plane) {
+  int rc = ensure_staging((size_t)n * nc);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(g.d_staging, host, (size_t)n * nc * sizeof(double), cudaMemcpyHostToDevice, g.stream));
+  k_aos_to_soa<<<cdiv(n, 256), 256, 0, g.stream>>>(g.d_staging, dev_field, n, nc, plane);
+  CKL();
+  return AERO_OK;
+}
+int download(double* host, const double* dev_field, long n, int nc, long plane) {
+  int rc = ensure_staging((size_t)n * nc);
+  if (rc) return rc;
+  k_soa_to_aos<<<cdiv(n, 256), 256, 0, g.stream>>>(dev_field, g.d_staging, n, nc, plane);
+  CKL();
+  CK(cudaMemcpyAsync(host, g.d_staging, (size_t)n * nc * sizeof(double), cudaMemcpyDeviceToHost, g.stream));
+  return AERO_OK;
+}
+
+// ------------------------------------------------------------ block operations
+// A drop-in call names its arrays; it runs resident (registered arrays of one
+// block, device copies) or transient (unregistered arrays, copied in and out).
+struct Arg {
+  int fid;
+  const double* host;
+  bool out;
+};
+
+struct BlockTarget {
+  const BlockView* d_view;  // device pointer to one view
+  BlockView view;           // host copy
+  bool resident;
+  int m;
+};
+
+int resolve(const Box& b, const Box& b0, const Box& b1, const std::vector<Arg>& args, BlockTarget& t) {
+  int nreg = 0, m = -1;
+  for (const Arg& a : args) {
+    auto it = g.registry.find(a.host);
+    if (it != g.registry.end()) {
+      ++nreg;
+      if (it->second.second != a.fid)
+        return fail(AERO_ERR_ARG, "array for field %d is registered as field %d", a.fid, it->second.second);
+      if (m >= 0 && it->second.first != m)
+        return fail(AERO_ERR_ARG, "arrays of blocks %d and %d in one call", m + 1, it->second.first + 1);
+      m = it->second.first;
+    }
+  }
+  if (nreg != 0 && nreg != (int)args.size())
+    return fail(AERO_ERR_ARG, "call mixes registered and unregistered arrays");
+  if (nreg > 0) {
+    const HostBlock& H = g.blocks[m];
+    if (!same(H.b, b) || !same(H.b0, b0) || !same(H.b1, b1))
+      return fail(AERO_ERR_ARG, "index bounds differ from block %d's registered boxes", m + 1);
+    t.resident = true;
+    t.m = m;
+    t.view = g.views[m];
+    t.d_view = g.d_blocks + m;
+    return AERO_OK;
+  }
+  // transient
+  long plane = round32(b.size());
+  size_t need = view_doubles(plane);
+  if (need > g.t_doubles) {
+    if (g.t_arena) CK(cudaFree(g.t_arena));
+    g.t_arena = nullptr;
+    CK(cudaMalloc(&g.t_arena, need * sizeof(double)));
+    g.t_doubles = need;
+  }
+  if (!g.d_tview) CK(cudaMalloc(&g.d_tview, sizeof(BlockView)));
+  CK(cudaMemsetAsync(g.t_arena, 0, need * sizeof(double), g.stream));
+  fill_view(t.view, b, b0, b1, plane, g.t_arena);
+  CK(cudaMemcpyAsync(g.d_tview, &t.view, sizeof(BlockView), cudaMemcpyHostToDevice, g.stream));
+  t.d_view = g.d_tview;
+  t.resident = false;
+  t.m = -1;
+  for (const Arg& a : args) {
+    int rc = upload(a.host, t.view.f[a.fid], b.size(), field_nc(a.fid), plane);
+    if (rc) return rc;
+  }
+  return AERO_OK;
+}
+
+// Routines that take only the full box (get_primitivevariables, find_dt):
+// resident calls use the registered block's inner boxes.
+int resolve_full(const Box& b, const std::vector<Arg>& args, BlockTarget& t) {
+  auto it = g.registry.find(args[0].host);
+  if (it != g.registry.end()) {
+    const HostBlock& H = g.blocks[it->second.first];
+    if (!same(H.b, b)) return fail(AERO_ERR_ARG, "index bounds differ from block %d's box", it->second.first + 1);
+    return resolve(H.b, H.b0, H.b1, args, t);
+  }
+  return resolve(b, b, b, args, t);
+}
+
+int finish(const BlockTarget& t, const std::vector<Arg>& args) {
+  if (!t.resident) {
+    for (const Arg& a : args)
+      if (a.out) {
+        int rc = download(const_cast<double*>(a.host), t.view.f[a.fid], t.view.b.size(),
+                          field_nc(a.fid), t.view.plane);
+        if (rc) return rc;
+      }
+    CK(cudaStreamSynchronize(g.stream));
+  }
+  CKL();
+  return AERO_OK;
+}
+
+CaseConsts consts_with(double gamma, double cv, double re) {
+  CaseConsts c = g.cc;
+  c.gamma = gamma;
+  c.cv = cv;
+  c.re = re;
+  return c;
+}
+
+// --------------------------------------------------------- launch helpers
+int launch_getpri(const BlockView* views, int nblk, long maxN, const CaseConsts& cc) {
+  dim3 grid(cdiv(maxN, 256), nblk);
+  k_getpri<<<grid, 256, 0, g.stream>>>(views, cc, g.d_status);
+  CKL();
+  return AERO_OK;
+}
+int launch_inviscid(const BlockView* views, int nblk, long maxN, long maxN1, const CaseConsts& cc) {
+  k_fill<<<dim3(cdiv(maxN, 256), nblk), 256, 0, g.stream>>>(views, F_RHSI, 5, 0.0);
+  CKL();
+  k_inviscid<<<dim3(cdiv(maxN1, 128), nblk), 128, 0, g.stream>>>(views, cc);
+  CKL();
+  return AERO_OK;
+}
+int launch_viscous(const BlockView* views, int nblk, long maxN0, const CaseConsts& cc, int store) {
+  k_viscous_a<<<dim3(cdiv(maxN0, 128), nblk), 128, 0, g.stream>>>(views, cc, store);
+  CKL();
+  k_viscous_b<<<dim3(cdiv(maxN0, 256), nblk), 256, 0, g.stream>>>(views, cc);
+  CKL();
+  return AERO_OK;
+}
+int launch_find_dt(const BlockView* views, int nblk, long maxN, const CaseConsts& cc) {
+  k_find_dt<<<dim3(cdiv(maxN, 256), nblk), 256, 0, g.stream>>>(views, cc, nullptr);
+  CKL();
+  return AERO_OK;
+}
+int launch_dt_minmax(const BlockView* views, int m, double* d_out2) {
+  k_dt_minmax<<<1, 1024, 0, g.stream>>>(views, m, nullptr, 0, 0, d_out2);
+  CKL();
+  return AERO_OK;
+}
+int launch_implicit(const BlockView* views, int nblk, long maxExt, const CaseConsts& cc) {
+  k_lusgs_prep<<<dim3(cdiv(maxExt, 256), nblk), 256, 0, g.stream>>>(views, cc);
+  CKL();
+  k_lusgs_sweep<<<nblk, 256, 0, g.stream>>>(views, cc);
+  CKL();
+  return AERO_OK;
+}
+
+bool viscous_on() { return g.cc.solver == IFLAG_NSSOLVER; }
+bool sa_on() { return g.cc.turbulence == IFLAG_SA && g.cc.solver == IFLAG_NSSOLVER; }
+
+int do_physical_bc() {
+  int nb = (int)g.blocks.size();
+  k_physical_bc<<<nb, 256, 0, g.stream>>>(g.d_blocks, g.d_bc_ops, g.d_bc_start, g.cc);
+  CKL();
+  if (sa_on()) {
+    k_sa_clip<<<dim3(cdiv(g.max_box, 256), nb), 256, 0, g.stream>>>(g.d_blocks);
+    CKL();
+  }
+  return AERO_OK;
+}
+int do_halo() {
+  if (g.nhalo == 0) return AERO_OK;
+  int mode = g.cc.turbulence == IFLAG_SA ? HALO_Q_NUT : HALO_Q;
+  k_halo<<<cdiv(g.nhalo, 256), 256, 0, g.stream>>>(g.d_blocks, g.d_halo, g.nhalo, mode);
+  CKL();
+  return AERO_OK;
+}
+int do_average1() {
+  if (g.navg_src == 0) return AERO_OK;
+  k_avg_gather<<<cdiv(g.navg_src, 256), 256, 0, g.stream>>>(g.d_blocks, g.d_avg_src, g.navg_src,
+                                                              g.d_avg_buf, g.cc.turbulence == IFLAG_SA);
+  CKL();
+  return AERO_OK;
+}
+int do_average2() {
+  if (g.navg_dst == 0) return AERO_OK;
+  k_avg_apply<<<cdiv(g.navg_dst, 256), 256, 0, g.stream>>>(g.d_blocks, g.d_avg_dst, g.navg_dst,
+                                                             g.d_avg_buf, g.cc.turbulence == IFLAG_SA);
+  CKL();
+  return AERO_OK;
+}
+int do_residual(double* d_out7) {
+  int nb = (int)g.blocks.size();
+  k_residual_partial<<<dim3(g.resid_ctas, nb), 256, 0, g.stream>>>(g.d_blocks, g.d_part, sa_on());
+  CKL();
+  k_residual_final<<<1, 256, 0, g.stream>>>(g.d_part, (long)g.resid_ctas * nb, g.totalnodes, d_out7,
+                                            g.d_status);
+  CKL();
+  return AERO_OK;
+}
+int do_getpri_all() {
+  return launch_getpri(g.d_blocks, (int)g.blocks.size(), g.max_box, g.cc);
+}
+
+// One iteration of main.f90:343-447 over every block.  main.f90:446 recomputes
+// the primitives at the end of an iteration from the same q that :357 uses at
+// the start of the next one, so the device computes them once, at the start;
+// aero_step recomputes them after its last iteration so the state it leaves
+// matches the reference's.
+int do_iteration(bool want_dt_minmax) {
+  int nb = (int)g.blocks.size();
+  int rc;
+  if ((rc = do_getpri_all())) return rc;
+  if ((rc = launch_inviscid(g.d_blocks, nb, g.max_box, g.max_b1, g.cc))) return rc;
+  if (viscous_on() && (rc = launch_viscous(g.d_blocks, nb, g.max_b0, g.cc, 0))) return rc;
+  if ((rc = launch_find_dt(g.d_blocks, nb, g.max_box, g.cc))) return rc;
+  if (want_dt_minmax && (rc = launch_dt_minmax(g.d_blocks, nb - 1, g.d_out + 7))) return rc;
+  if ((rc = launch_implicit(g.d_blocks, nb, g.max_ext, g.cc))) return rc;
+  if ((rc = do_physical_bc())) return rc;
+  if ((rc = do_halo())) return rc;
+  if ((rc = do_average1())) return rc;
+  if ((rc = do_average2())) return rc;
+  return AERO_OK;
+}
+
+}  // namespace
+
+// =================================================================== C ABI
+extern "C" {
+
+const char* aero_last_error(void) { return g.err.c_str(); }
+
+int aero_init(int device) {
+  if (g.inited) return AERO_OK;
+  CK(cudaSetDevice(device));
+  CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+  CK(cudaMalloc(&g.d_status, sizeof(unsigned)));
+  CK(cudaMemset(g.d_status, 0, sizeof(unsigned)));
+  CK(cudaMalloc(&g.d_out, 16 * sizeof(double)));
+  CK(cudaMallocHost(&g.h_out, 16 * sizeof(double)));
+  g.device = device;
+  g.inited = true;
+  return AERO_OK;
+}
+
+static void release_case() {
+  for (auto& H : g.blocks)
+    for (int f = 0; f < kNumPublicFields; ++f)
+      if (H.pinned[f]) cudaHostUnregister(H.host[f]);
+  g.blocks.clear();
+  g.registry.clear();
+  cudaFree(g.arena); g.arena = nullptr;
+  cudaFree(g.d_blocks); g.d_blocks = nullptr;
+  cudaFree(g.d_bc_ops); g.d_bc_ops = nullptr;
+  cudaFree(g.d_bc_start); g.d_bc_start = nullptr;
+  cudaFree(g.d_halo); g.d_halo = nullptr;
+  cudaFree(g.d_avg_src); g.d_avg_src = nullptr;
+  cudaFree(g.d_avg_dst); g.d_avg_dst = nullptr;
+  cudaFree(g.d_avg_buf); g.d_avg_buf = nullptr;
+  cudaFree(g.d_part); g.d_part = nullptr;
+  g.views.clear();
+  g.setup = false;
+}
+
+int aero_finalize(void) {
+  if (!g.inited) return AERO_OK;
+  cudaStreamSynchronize(g.stream);
+  release_case();
+  cudaFree(g.d_staging); g.d_staging = nullptr; g.staging_doubles = 0;
+  cudaFree(g.t_arena); g.t_arena = nullptr; g.t_doubles = 0;
+  cudaFree(g.d_tview); g.d_tview = nullptr;
+  cudaFree(g.d_status); g.d_status = nullptr;
+  cudaFree(g.d_out); g.d_out = nullptr;
+  cudaFreeHost(g.h_out); g.h_out = nullptr;
+  cudaStreamDestroy(g.stream); g.stream = nullptr;
+  g.inited = false;
+  g.configured = false;
+  return AERO_OK;
+}
+
+int aero_get_status(unsigned* status) {
+  int rc = need_init();
+  if (rc) return rc;
+  unsigned h = 0;
+  CK(cudaMemcpyAsync(&h, g.d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, g.stream));
+  CK(cudaMemsetAsync(g.d_status, 0, sizeof(unsigned), g.stream));
+  CK(cudaStreamSynchronize(g.stream));
+  *status = h;
+  return AERO_OK;
+}
+
+int aero_configure(const int* iflags, const double* params) {
+  int rc = need_init();
+  if (rc) return rc;
+  if (iflags[0] != IFLAG_3D) return fail(AERO_ERR_ARG, "iflag_dimension=%d: only 3-D is supported", iflags[0]);
+  if (iflags[1] != IFLAG_NSSOLVER && iflags[1] != IFLAG_EULERSOLVER)
+    return fail(AERO_ERR_ARG, "iflag_solver=%d is not 0 (NS) or 1 (Euler)", iflags[1]);
+  if (iflags[2] != IFLAG_STEADY) return fail(AERO_ERR_ARG, "iflag_time=%d: only steady is supported", iflags[2]);
+  if (iflags[3] != 2) return fail(AERO_ERR_ARG, "iflag_timeadvance=%d: only 1st-order implicit (2)", iflags[3]);
+  if (iflags[4] != IFLAG_LAMINAR && iflags[4] != IFLAG_SA)
+    return fail(AERO_ERR_ARG, "Wrong turbulence model type is input!!! (%d)", iflags[4]);
+  if (iflags[6] != 2 || iflags[7] != 4)
+    return fail(AERO_ERR_ARG, "bufferLength=%d/iflag_inviscid=%d: only the 3rd-order WENO (2 layers)", iflags[6], iflags[7]);
+  std::memcpy(g.iflags, iflags, sizeof g.iflags);
+  std::memcpy(g.params, params, sizeof g.params);
+  CaseConsts& c = g.cc;
+  const double pi = 3.1415926535897932;
+  c.gamma = 1.4; c.prl = 0.72; c.prt = 0.90;
+  double ma = params[0];
+  c.re = params[1]; c.tinf = params[2]; c.cfl = params[4]; c.nutinf = params[6];
+  // nondimensionalisation of sub_init_flowfield.f90:30-39
+  c.d_0 = 1.0; c.u_0 = 1.0;
+  double t_0 = 1.0;
+  c.p_0 = c.d_0 * t_0 / c.gamma / ma / ma;
+  c.c_0 = std::sqrt(t_0) / ma;
+  c.cv = 1.0 / c.gamma / (c.gamma - 1.0) / ma / ma;
+  c.aoa = params[3] * pi / 180.0;
+  c.dimension = iflags[0]; c.solver = iflags[1]; c.time = iflags[2];
+  c.turbulence = iflags[4]; c.des = iflags[5]; c.bufferLength = iflags[6];
+  g.configured = true;
+  return AERO_OK;
+}
+
+int aero_register_block(int m, const int* box18, int num_subface, const int* subfaces) {
+  int rc = need_init();
+  if (rc) return rc;
+  if (g.setup) release_case();
+  if (m < 1 || num_subface < 0) return fail(AERO_ERR_ARG, "bad block number %d", m);
+  if ((int)g.blocks.size() < m) g.blocks.resize(m);
+  HostBlock& H = g.blocks[m - 1];
+  H = HostBlock();
+  H.used = true;
+  H.b = Box{box18[0], box18[1], box18[2], box18[3], box18[4], box18[5]};
+  H.b0 = Box{box18[6], box18[7], box18[8], box18[9], box18[10], box18[11]};
+  H.b1 = Box{box18[12], box18[13], box18[14], box18[15], box18[16], box18[17]};
+  if (H.b.nx() < 1 || H.b.ny() < 1 || H.b.nz() < 1) return fail(AERO_ERR_ARG, "block %d: empty box", m);
+  for (int s = 0; s < num_subface; ++s) {
+    const int* r = subfaces + 11 * s;
+    H.subs.push_back(SubRow{r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7], r[8], r[9], r[10]});
+  }
+  return AERO_OK;
+}
+
+int aero_bind_field(int m, int field, double* host) {
+  int rc = need_init();
+  if (rc) return rc;
+  if (m < 1 || m > (int)g.blocks.size() || !g.blocks[m - 1].used) return fail(AERO_ERR_ARG, "block %d not registered", m);
+  if (field < 0 || field >= kNumPublicFields) return fail(AERO_ERR_ARG, "unknown field %d", field);
+  HostBlock& H = g.blocks[m - 1];
+  if (H.pinned[field]) cudaHostUnregister(H.host[field]);
+  H.host[field] = host;
+  H.pinned[field] = false;
+  size_t bytes = (size_t)H.b.size() * field_nc(field) * sizeof(double);
+  if (host && cudaHostRegister(host, bytes, cudaHostRegisterDefault) == cudaSuccess) H.pinned[field] = true;
+  cudaGetLastError();  // an unpinnable array is still usable (pageable copies)
+  if (host) g.registry[host] = std::make_pair(m - 1, field);
+  return AERO_OK;
+}
+
+int aero_finish_setup(void) {
+  int rc = need_init();
+  if (rc) return rc;
+  if (!g.configured) return fail(AERO_ERR_STATE, "aero_configure has not been called");
+  int nb = (int)g.blocks.size();
+  if (nb == 0) return fail(AERO_ERR_STATE, "no blocks registered");
+  for (int m = 0; m < nb; ++m)
+    if (!g.blocks[m].used) return fail(AERO_ERR_ARG, "block %d missing (blocks must be 1..n)", m + 1);
+  // topology tables
+  std::vector<TopoBlock> tb(nb);
+  for (int m = 0; m < nb; ++m) {
+    tb[m].b = g.blocks[m].b; tb[m].b0 = g.blocks[m].b0; tb[m].b1 = g.blocks[m].b1;
+    tb[m].subs = g.blocks[m].subs;
+  }
+  Topology topo;
+  std::string why = build_topology(tb, g.cc.bufferLength, g.cc.solver, topo);
+  if (!why.empty()) return fail(AERO_ERR_ARG, "%s", why.c_str());
+  // arena
+  size_t total = 0;
+  g.max_box = g.max_b0 = g.max_b1 = g.max_ext = 0;
+  g.totalnodes = 0;
+  long max_b1 = 0;
+  for (auto& H : g.blocks) {
+    H.plane = round32(H.b.size());
+    H.arena_off = total;
+    total += view_doubles(H.plane);
+    g.max_box = std::max(g.max_box, H.b.size());
+    g.max_b0 = std::max(g.max_b0, H.b0.size());
+    max_b1 = std::max(max_b1, H.b1.size());
+    Box e{H.b1.is - 1, H.b1.ie + 1, H.b1.js - 1, H.b1.je + 1, H.b1.ks - 1, H.b1.ke + 1};
+    g.max_ext = std::max(g.max_ext, e.size());
+    g.totalnodes += (double)H.b0.size();
+  }
+  g.max_b1 = max_b1;
+  CK(cudaMalloc(&g.arena, total * sizeof(double)));
+  CK(cudaMemsetAsync(g.arena, 0, total * sizeof(double), g.stream));
+  g.arena_doubles = total;
+  g.views.resize(nb);
+  for (int m = 0; m < nb; ++m) {
+    HostBlock& H = g.blocks[m];
+    fill_view(g.views[m], H.b, H.b0, H.b1, H.plane, g.arena + H.arena_off);
+  }
+  CK(cudaMalloc(&g.d_blocks, nb * sizeof(BlockView)));
+  CK(cudaMemcpyAsync(g.d_blocks, g.views.data(), nb * sizeof(BlockView), cudaMemcpyHostToDevice, g.stream));
+  // tables
+  CK(cudaMalloc(&g.d_bc_ops, std::max<size_t>(1, topo.bc_ops.size()) * sizeof(BcOp)));
+  CK(cudaMalloc(&g.d_bc_start, topo.bc_start.size() * sizeof(int)));
+  if (!topo.bc_ops.empty())
+    CK(cudaMemcpyAsync(g.d_bc_ops, topo.bc_ops.data(), topo.bc_ops.size() * sizeof(BcOp), cudaMemcpyHostToDevice, g.stream));
+  CK(cudaMemcpyAsync(g.d_bc_start, topo.bc_start.data(), topo.bc_start.size() * sizeof(int), cudaMemcpyHostToDevice, g.stream));
+  g.nhalo = (long)topo.halo.size();
+  g.navg_src = (long)topo.avg_src.size();
+  g.navg_dst = (long)topo.avg_dst.size();
+  CK(cudaMalloc(&g.d_halo, std::max<size_t>(1, topo.halo.size()) * sizeof(HaloEntry)));
+  CK(cudaMalloc(&g.d_avg_src, std::max<size_t>(1, topo.avg_src.size()) * sizeof(AvgSrc)));
+  CK(cudaMalloc(&g.d_avg_dst, std::max<size_t>(1, topo.avg_dst.size()) * sizeof(AvgDst)));
+  CK(cudaMalloc(&g.d_avg_buf, std::max<size_t>(1, topo.avg_src.size()) * 6 * sizeof(double)));
+  if (g.nhalo) CK(cudaMemcpyAsync(g.d_halo, topo.halo.data(), g.nhalo * sizeof(HaloEntry), cudaMemcpyHostToDevice, g.stream));
+  if (g.navg_src) CK(cudaMemcpyAsync(g.d_avg_src, topo.avg_src.data(), g.navg_src * sizeof(AvgSrc), cudaMemcpyHostToDevice, g.stream));
+  if (g.navg_dst) CK(cudaMemcpyAsync(g.d_avg_dst, topo.avg_dst.data(), g.navg_dst * sizeof(AvgDst), cudaMemcpyHostToDevice, g.stream));
+  g.resid_ctas = (int)cdiv(g.max_b1, 256);
+  CK(cudaMalloc(&g.d_part, (size_t)g.resid_ctas * nb * 6 * sizeof(double)));
+  CK(cudaStreamSynchronize(g.stream));
+  g.setup = true;
+  return AERO_OK;
+}
+
+static int sync_fields(unsigned long long mask, bool to_device) {
+  int rc = need_setup();
+  if (rc) return rc;
+  for (int m = 0; m < (int)g.blocks.size(); ++m) {
+    HostBlock& H = g.blocks[m];
+    for (int f = 0; f < kNumPublicFields; ++f) {
+      if (!(mask & (1ull << f)) || !H.host[f]) continue;
+      rc = to_device ? upload(H.host[f], g.views[m].f[f], H.b.size(), field_nc(f), H.plane)
+                     : download(H.host[f], g.views[m].f[f], H.b.size(), field_nc(f), H.plane);
+      if (rc) return rc;
+    }
+  }
+  CK(cudaStreamSynchronize(g.stream));
+  return AERO_OK;
+}
+int aero_sync_to_device(unsigned long long mask) { return sync_fields(mask, true); }
+int aero_sync_to_host(unsigned long long mask) { return sync_fields(mask, false); }
+
+// ------------------------------------------------------------ drop-in mirrors
+int aero_get_primitivevariables(const int* mm, double* pri_v, const double* q, const double* gamma,
+                                const double* cv, const int* is, const int* ie, const int* js,
+                                const int* je, const int* ks, const int* ke) {
+  (void)mm;
+  int rc = need_init();
+  if (rc) return rc;
+  Box b = box_of(is, ie, js, je, ks, ke);
+  std::vector<Arg> args = {{F_Q, q, false}, {F_PRI, pri_v, true}};
+  BlockTarget t;
+  if ((rc = resolve_full(b, args, t))) return rc;
+  CaseConsts cc = consts_with(*gamma, *cv, g.cc.re);
+  if ((rc = launch_getpri(t.d_view, 1, b.size(), cc))) return rc;
+  return finish(t, args);
+}
+
+int aero_inviscid_flux_1(double* rhsi, const double* q, const double* dxidx, const double* inv_j,
+                         const int* is, const int* ie, const int* js, const int* je, const int* ks,
+                         const int* ke, const int* is0, const int* ie0, const int* js0,
+                         const int* je0, const int* ks0, const int* ke0, const int* is1,
+                         const int* ie1, const int* js1, const int* je1, const int* ks1,
+                         const int* ke1, const double* gamma) {
+  int rc = need_init();
+  if (rc) return rc;
+  Box b = box_of(is, ie, js, je, ks, ke), b0 = box_of(is0, ie0, js0, je0, ks0, ke0),
+      b1 = box_of(is1, ie1, js1, je1, ks1, ke1);
+  std::vector<Arg> args = {{F_Q, q, false}, {F_DXIDX, dxidx, false}, {F_INVJ, inv_j, false}, {F_RHSI, rhsi, true}};
+  BlockTarget t;
+  if ((rc = resolve(b, b0, b1, args, t))) return rc;
+  CaseConsts cc = consts_with(*gamma, g.cc.cv, g.cc.re);
+  if ((rc = launch_inviscid(t.d_view, 1, b.size(), b1.size(), cc))) return rc;
+  return finish(t, args);
+}
+
+int aero_viscous_flux(double* rhsv, const double* pri_v, double* amu, double* vor, double* dudx,
+                      double* tao, const double* dxidx, const double* inv_j, const double* tinf,
+                      const double* prl, const double* prt, const double* gamma, const double* cv,
+                      const double* re, const int* is, const int* ie, const int* js,
+                      const int* je, const int* ks, const int* ke, const int* is0,
+                      const int* ie0, const int* js0, const int* je0, const int* ks0,
+                      const int* ke0, const int* is1, const int* ie1, const int* js1,
+                      const int* je1, const int* ks1, const int* ke1, const int* mm) {
+  (void)mm;
+  int rc = need_init();
+  if (rc) return rc;
+  Box b = box_of(is, ie, js, je, ks, ke), b0 = box_of(is0, ie0, js0, je0, ks0, ke0),
+      b1 = box_of(is1, ie1, js1, je1, ks1, ke1);
+  std::vector<Arg> args = {{F_PRI, pri_v, false}, {F_AMU, amu, true},  {F_VOR, vor, true},
+                           {F_DUDX, dudx, true},  {F_TAO, tao, true},  {F_DXIDX, dxidx, false},
+                           {F_INVJ, inv_j, false}, {F_RHSV, rhsv, true}};
+  BlockTarget t;
+  if ((rc = resolve(b, b0, b1, args, t))) return rc;
+  CaseConsts cc = consts_with(*gamma, *cv, *re);
+  cc.tinf = *tinf; cc.prl = *prl; cc.prt = *prt;
+  if ((rc = launch_viscous(t.d_view, 1, b0.size(), cc, 1))) return rc;
+  return finish(t, args);
+}
+
+int aero_find_dt(double* dt, double* dtmax, double* dtmin, double* cflmax, double* cflmin,
+                 const double* pri_v, const double* amu, const double* dxidx, const double* re,
+                 double* cfl, const int* is, const int* ie, const int* js, const int* je,
+                 const int* ks, const int* ke, const int* iflag_time, const int* iflag_steady,
+                 const int* iflag_unsteady) {
+  (void)iflag_steady; (void)iflag_unsteady;
+  int rc = need_init();
+  if (rc) return rc;
+  if (*iflag_time != IFLAG_STEADY) return fail(AERO_ERR_ARG, "find_dt: only the steady branch is supported");
+  Box b = box_of(is, ie, js, je, ks, ke);
+  std::vector<Arg> args = {{F_PRI, pri_v, false}, {F_AMU, amu, false}, {F_DXIDX, dxidx, false}, {F_DT, dt, true}};
+  BlockTarget t;
+  if ((rc = resolve_full(b, args, t))) return rc;
+  CaseConsts cc = consts_with(g.cc.gamma, g.cc.cv, *re);
+  cc.cfl = *cfl;
+  if ((rc = launch_find_dt(t.d_view, 1, b.size(), cc))) return rc;
+  if ((rc = launch_dt_minmax(t.d_view, 0, g.d_out + 7))) return rc;
+  CK(cudaMemcpyAsync(g.h_out + 7, g.d_out + 7, 2 * sizeof(double), cudaMemcpyDeviceToHost, g.stream));
+  if ((rc = finish(t, args))) return rc;
+  CK(cudaStreamSynchronize(g.stream));
+  *dtmax = g.h_out[7];
+  *dtmin = g.h_out[8];
+  *cflmax = 0.0;
+  *cflmin = 1.0e10;
+  return AERO_OK;
+}
+
+int aero_implicit1st(double* q, const double* dt, const double* pri_v, double* rhs,
+                     const double* rhsi, const double* rhsv, const double* dxidx,
+                     const double* inv_j, const int* is, const int* ie, const int* js,
+                     const int* je, const int* ks, const int* ke, const int* is0,
+                     const int* ie0, const int* js0, const int* je0, const int* ks0,
+                     const int* ke0, const int* is1, const int* ie1, const int* js1,
+                     const int* je1, const int* ks1, const int* ke1, const double* gamma,
+                     const double* cfl, const double* xx, const double* yy, const double* zz) {
+  (void)xx; (void)yy; (void)zz;
+  int rc = need_init();
+  if (rc) return rc;
+  Box b = box_of(is, ie, js, je, ks, ke), b0 = box_of(is0, ie0, js0, je0, ks0, ke0),
+      b1 = box_of(is1, ie1, js1, je1, ks1, ke1);
+  std::vector<Arg> args = {{F_Q, q, true},        {F_DT, dt, false},       {F_PRI, pri_v, false},
+                           {F_RHS, rhs, true},    {F_RHSI, rhsi, false},   {F_RHSV, rhsv, false},
+                           {F_DXIDX, dxidx, false}, {F_INVJ, inv_j, false}};
+  BlockTarget t;
+  if ((rc = resolve(b, b0, b1, args, t))) return rc;
+  CaseConsts cc = consts_with(*gamma, g.cc.cv, g.cc.re);
+  cc.cfl = *cfl;
+  Box e{b1.is - 1, b1.ie + 1, b1.js - 1, b1.je + 1, b1.ks - 1, b1.ke + 1};
+  if ((rc = launch_implicit(t.d_view, 1, e.size(), cc))) return rc;
+  return finish(t, args);
+}
+
+// ------------------------------------------------------ module-state routines
+int aero_physical_bc(void) {
+  int rc = need_setup();
+  return rc ? rc : do_physical_bc();
+}
+int aero_updatebuffer(void) {
+  int rc = need_setup();
+  return rc ? rc : do_halo();
+}
+int aero_average1(void) {
+  int rc = need_setup();
+  return rc ? rc : do_average1();
+}
+int aero_average2(void) {
+  int rc = need_setup();
+  return rc ? rc : do_average2();
+}
+int aero_updatebuffercoordinate(void) {
+  int rc = need_setup();
+  if (rc) return rc;
+  if (g.nhalo == 0) return AERO_OK;
+  k_halo<<<cdiv(g.nhalo, 256), 256, 0, g.stream>>>(g.d_blocks, g.d_halo, g.nhalo, HALO_COORD);
+  CKL();
+  return AERO_OK;
+}
+int aero_getpri_all(void) {
+  int rc = need_setup();
+  return rc ? rc : do_getpri_all();
+}
+
+int aero_residual(double* out7) {
+  int rc = need_setup();
+  if (rc) return rc;
+  if ((rc = do_residual(g.d_out))) return rc;
+  CK(cudaMemcpyAsync(g.h_out, g.d_out, 7 * sizeof(double), cudaMemcpyDeviceToHost, g.stream));
+  CK(cudaStreamSynchronize(g.stream));
+  std::memcpy(out7, g.h_out, 7 * sizeof(double));
+  return AERO_OK;
+}
+
+int aero_init_flowfield(void) {
+  int rc = need_setup();
+  if (rc) return rc;
+  // Fill on the host arrays' device copies: q, pri_v, dt, amu, nut, sa_rhs and
+  // the zeroed work arrays (sub_init_flowfield.f90:55-111).
+  int nb = (int)g.blocks.size();
+  const CaseConsts& c = g.cc;
+  double t_0 = 1.0;
+  double qv[5] = {c.d_0, c.d_0 * c.u_0 * std::cos(c.aoa), c.d_0 * c.u_0 * std::sin(c.aoa), 0.0,
+                  c.d_0 * t_0 * c.cv + 0.5 * c.d_0 * c.u_0 * c.u_0};
+  double pv[7] = {c.d_0, c.u_0 * std::cos(c.aoa), c.u_0 * std::sin(c.aoa), 0.0, c.p_0, t_0, c.c_0};
+  bool sa = c.turbulence == IFLAG_SA;
+  double amu2 = sa ? 0.009 : 0.0;
+  double av[3] = {1.0, amu2, 1.0 + amu2};
+  for (int m = 0; m < nb; ++m) {
+    const BlockView& v = g.views[m];
+    long N = g.blocks[m].b.size();
+    auto put = [&](double* dst, double val) -> int {
+      k_fill_plane<<<cdiv(N, 256), 256, 0, g.stream>>>(dst, N, val);
+      CKL();
+      return AERO_OK;
+    };
+    for (int x = 0; x < 5; ++x) if ((rc = put(v.f[F_Q] + x * v.plane, qv[x]))) return rc;
+    for (int x = 0; x < 7; ++x) if ((rc = put(v.f[F_PRI] + x * v.plane, pv[x]))) return rc;
+    for (int x = 0; x < 3; ++x) if ((rc = put(v.f[F_AMU] + x * v.plane, av[x]))) return rc;
+    if ((rc = put(v.f[F_DT], g.params[5]))) return rc;
+    if (sa) {
+      if ((rc = put(v.f[F_NUT], c.nutinf))) return rc;
+      if ((rc = put(v.f[F_SARHS], 0.0))) return rc;
+    }
+    for (int fid : {F_DUDX, F_VOR, F_TAO, F_RHSV, F_RHSI, F_RHS})
+      for (int x = 0; x < field_nc(fid); ++x)
+        if ((rc = put(v.f[fid] + x * v.plane, 0.0))) return rc;
+  }
+  CK(cudaStreamSynchronize(g.stream));
+  return AERO_OK;
+}
+
+int aero_step(int nsteps, double* resid_hist, double* dt_minmax) {
+  int rc = need_setup();
+  if (rc) return rc;
+  for (int s = 0; s < nsteps; ++s) {
+    bool last = (s == nsteps - 1);
+    if ((rc = do_iteration(last && dt_minmax != nullptr))) return rc;
+    if (resid_hist) {
+      if ((rc = do_residual(g.d_out))) return rc;
+      CK(cudaMemcpyAsync(g.h_out, g.d_out, 7 * sizeof(double), cudaMemcpyDeviceToHost, g.stream));
+      CK(cudaStreamSynchronize(g.stream));
+      std::memcpy(resid_hist + 7 * s, g.h_out, 7 * sizeof(double));
+    }
+  }
+  if (nsteps > 0 && (rc = do_getpri_all())) return rc;
+  if (dt_minmax) {
+    CK(cudaMemcpyAsync(g.h_out + 7, g.d_out + 7, 2 * sizeof(double), cudaMemcpyDeviceToHost, g.stream));
+    CK(cudaStreamSynchronize(g.stream));
+    dt_minmax[0] = g.h_out[7];
+    dt_minmax[1] = g.h_out[8];
+  }
+  CK(cudaStreamSynchronize(g.stream));
+  return AERO_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,171 @@
+"""Seeded, analytic generators of the synthetic cases the solver is measured on.
+
+The reference ships no grids, bcinfo or Control.in files, so every case is
+generated here with the shapes, sizes and boundary layouts of the workloads
+the path is quoted on:
+
+* ``bump_channel``  - single-block channel of length 3, height 1, with a
+  circular-arc bump of height h on x in [1, 2]; uniform in x, geometric in y;
+  inflow / outflow / wall / symmetry (k faces symmetry).
+* ``naca_ogrid``    - NACA 4-digit O-grid split into ``nblk`` blocks around the
+  airfoil, block interfaces on the i faces, wall at j=1, farfield at j=max.
+* ``bump_batch``    - many bump channels of uneven size (a Mach/geometry sweep).
+"""
+from __future__ import annotations
+
+import math
+from typing import List, Optional
+
+import numpy as np
+
+from .case import (BC_FARFIELD, BC_INFLOW, BC_OUTFLOW, BC_SYMM, BC_WALL, IFLAG_EULERSOLVER,
+                   IFLAG_NSSOLVER, Block, Case, Config, Subface)
+
+
+def _set_coords(blk: Block, X: np.ndarray, Y: np.ndarray, Z: np.ndarray) -> None:
+    """Stores physical-node coordinates (shape (nk, nj, ni)) into the block's
+    x, y, z arrays; ghost coordinates come from the coordinate halo."""
+    s = blk.sl(blk.box0)
+    blk.fields["x"][s] = X
+    blk.fields["y"][s] = Y
+    blk.fields["z"][s] = Z
+
+
+def bump_channel(ni: int = 97, nj: int = 49, nk: int = 5, h: float = 0.10, length: float = 3.0,
+                 ratio: float = 1.05, dz: float = 0.05, cfg: Optional[Config] = None,
+                 name: str = "bump") -> Case:
+    """Circular-arc bump channel, Euler.  The arc of chord 1 on x in [1,2] has
+    radius R = (1/4 + h^2)/(2h) and centre (1.5, h - R)."""
+    cfg = cfg or Config(solver=IFLAG_EULERSOLVER, ma=0.5, re=1.0e6, cfl=5.0)
+    subs = [
+        Subface(1, 1, 1, 1, 1, nj, 1, nk, BC_INFLOW),
+        Subface(2, 2, ni, ni, 1, nj, 1, nk, BC_OUTFLOW),
+        Subface(3, 3, 1, ni, 1, 1, 1, nk, BC_WALL),
+        Subface(4, 4, 1, ni, nj, nj, 1, nk, BC_SYMM),
+        Subface(5, 5, 1, ni, 1, nj, 1, 1, BC_SYMM),
+        Subface(6, 6, 1, ni, 1, nj, nk, nk, BC_SYMM),
+    ]
+    blk = Block(1, ni, nj, nk, subs, cfg.buffer_length, cfg.dimension)
+    x = np.linspace(0.0, length, ni)
+    R = (0.25 + h * h) / (2.0 * h)
+    ywall = np.where((x >= 1.0) & (x <= 2.0),
+                     np.sqrt(np.maximum(R * R - (x - 1.5) ** 2, 0.0)) - (R - h), 0.0)
+    n = nj - 1
+    eta = (ratio ** np.arange(nj) - 1.0) / (ratio ** n - 1.0)
+    Y2 = ywall[None, :] + (1.0 - ywall[None, :]) * eta[:, None]          # (nj, ni)
+    X2 = np.broadcast_to(x[None, :], (nj, ni))
+    zs = dz * np.arange(nk)
+    X = np.broadcast_to(X2[None], (nk, nj, ni)).copy()
+    Y = np.broadcast_to(Y2[None], (nk, nj, ni)).copy()
+    Z = np.broadcast_to(zs[:, None, None], (nk, nj, ni)).copy()
+    _set_coords(blk, X, Y, Z)
+    return Case(name, cfg, [blk])
+
+
+def naca4_surface(x: np.ndarray, t: float, m: float = 0.0, p: float = 0.4):
+    """Upper and lower surface of a NACA 4-digit section (closed trailing edge,
+    -0.1036 x^4 coefficient), chord 1."""
+    yt = 5.0 * t * (0.2969 * np.sqrt(x) - 0.1260 * x - 0.3516 * x ** 2 + 0.2843 * x ** 3 - 0.1036 * x ** 4)
+    if m > 0.0:
+        yc = np.where(x < p, m / p ** 2 * (2 * p * x - x ** 2), m / (1 - p) ** 2 * ((1 - 2 * p) + 2 * p * x - x ** 2))
+        dyc = np.where(x < p, 2 * m / p ** 2 * (p - x), 2 * m / (1 - p) ** 2 * (p - x))
+        th = np.arctan(dyc)
+        xu, yu = x - yt * np.sin(th), yc + yt * np.cos(th)
+        xl, yl = x + yt * np.sin(th), yc - yt * np.cos(th)
+    else:
+        xu, yu, xl, yl = x, yt, x, -yt
+    return xu, yu, xl, yl
+
+
+def radial_distribution(nj: int, first: float, ratio: float, outer: float = 1.0,
+                        n_inner: Optional[int] = None) -> np.ndarray:
+    """Wall-normal node positions 0..outer over nj nodes in two geometric
+    segments: ``n_inner`` intervals growing at ``ratio`` from spacing ``first``,
+    then a second ratio solved so the last node lands on ``outer`` (a single
+    ratio of 1.08 over 64 intervals would reach only ~0.17 chord)."""
+    n = nj - 1
+    n1 = n // 2 if n_inner is None else n_inner
+    inner = first * (ratio ** np.arange(n1 + 1) - 1.0) / (ratio - 1.0)
+    d = first * ratio ** (n1 - 1) if n1 > 0 else first
+    n2 = n - n1
+    left = outer - inner[-1]
+    lo, hi = 1.0 + 1e-12, 10.0
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        val = d * mid * (mid ** n2 - 1.0) / (mid - 1.0)
+        lo, hi = (mid, hi) if val < left else (lo, mid)
+    r2 = 0.5 * (lo + hi)
+    outer_part = inner[-1] + d * r2 * (r2 ** np.arange(1, n2 + 1) - 1.0) / (r2 - 1.0)
+    out = np.concatenate([inner, outer_part])
+    out[-1] = outer
+    return out
+
+
+def naca_ogrid(nblk: int = 4, ni: int = 129, nj: int = 65, nk: int = 3, t: float = 0.12,
+               m: float = 0.0, p: float = 0.4, first: float = 1.0e-4, ratio: float = 1.08,
+               outer: float = 20.0, dz: float = 0.1, cfg: Optional[Config] = None,
+               name: str = "naca_ogrid") -> Case:
+    """O-grid around a NACA 4-digit section.  i runs clockwise around the
+    airfoil starting at the trailing edge (lower surface first), j outward, k
+    spanwise.  Block b covers i-intervals [b*(ni-1), (b+1)*(ni-1)] of the loop;
+    neighbouring blocks share their i interface plane (overlap nodes) and are
+    connected face 2 -> face 1 with orientation code 2 (the reference's
+    transposed (l,m) convention between an i+ and an i- face)."""
+    cfg = cfg or Config(solver=IFLAG_NSSOLVER, ma=0.5, re=5000.0, aoa_deg=2.0, cfl=5.0)
+    ntot = nblk * (ni - 1)               # intervals around the loop
+    # loop parameter: 0 -> TE, along the lower surface to LE, back along upper
+    s = np.arange(ntot + 1) / ntot
+    theta = 2.0 * math.pi * s
+    # x from cosine clustering, lower half first
+    xs = 0.5 * (1.0 + np.cos(theta))     # 1 -> 0 -> 1
+    xu, yu, xl, yl = naca4_surface(np.clip(xs, 0.0, 1.0), t, m, p)
+    lower = theta <= math.pi
+    sx = np.where(lower, xl, xu)
+    sy = np.where(lower, yl, yu)
+    # outer circle, clockwise from angle 0
+    cx, cy = 0.5, 0.0
+    ox = cx + outer * np.cos(-theta)
+    oy = cy + outer * np.sin(-theta)
+    # wall-normal distribution reaching the outer circle; blend surface -> circle
+    dist = radial_distribution(nj, first / outer, ratio, 1.0)
+    blocks: List[Block] = []
+    zs = dz * np.arange(nk)
+    for b in range(nblk):
+        lo = b * (ni - 1)
+        idx = np.arange(lo, lo + ni) % ntot
+        bx = sx[idx]; by = sy[idx]; ex = ox[idx]; ey = oy[idx]
+        # initial direction: surface normal blended toward the straight line
+        X2 = bx[None, :] + (ex - bx)[None, :] * dist[:, None]
+        Y2 = by[None, :] + (ey - by)[None, :] * dist[:, None]
+        left = nblk if b == 0 else b          # neighbour on face 1 (i-)
+        right = 1 if b == nblk - 1 else b + 2  # neighbour on face 2 (i+)
+        subs = [
+            Subface(1, 1, 1, 1, 1, nj, 1, nk, left, 2, 2),
+            Subface(2, 2, ni, ni, 1, nj, 1, nk, right, 1, 2),
+            Subface(3, 3, 1, ni, 1, 1, 1, nk, BC_WALL),
+            Subface(4, 4, 1, ni, nj, nj, 1, nk, BC_FARFIELD),
+            Subface(5, 5, 1, ni, 1, nj, 1, 1, BC_SYMM),
+            Subface(6, 6, 1, ni, 1, nj, nk, nk, BC_SYMM),
+        ]
+        blk = Block(b + 1, ni, nj, nk, subs, cfg.buffer_length, cfg.dimension)
+        X = np.broadcast_to(X2[None], (nk, nj, ni)).copy()
+        Y = np.broadcast_to(Y2[None], (nk, nj, ni)).copy()
+        Z = np.broadcast_to(zs[:, None, None], (nk, nj, ni)).copy()
+        _set_coords(blk, X, Y, Z)
+        blocks.append(blk)
+    return Case(name, cfg, blocks)
+
+
+def bump_batch(ncase: int = 64, seed: int = 0, nk: int = 5):
+    """Uneven bump-channel sweep: ni ~ U{65..257}, nj ~ U{33..97}, nk = 5,
+    h ~ U[0.05, 0.12], M ~ U[0.3, 0.7]."""
+    rng = np.random.default_rng(seed)
+    cases = []
+    for c in range(ncase):
+        ni = int(rng.integers(65, 258))
+        nj = int(rng.integers(33, 98))
+        h = float(rng.uniform(0.05, 0.12))
+        ma = float(rng.uniform(0.3, 0.7))
+        cfg = Config(solver=IFLAG_EULERSOLVER, ma=ma, re=1.0e6, cfl=5.0)
+        cases.append(bump_channel(ni, nj, nk, h=h, cfg=cfg, name=f"bump{c:02d}"))
+    return cases

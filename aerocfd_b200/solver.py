@@ -1,0 +1,171 @@
+"""Host driver: replays the reference's main loop (main.f90:249-447) through the
+C-ABI, the way the Fortran program would once its call sites are routed to
+libaerocfd_gpu.so.
+
+``GpuCase`` registers a :class:`~aerocfd_b200.case.Case`'s host arrays with the
+library (resident mode).  Each drop-in method takes the same arguments the
+Fortran call site passes; ``step`` runs whole iterations on the device.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from .case import FIELD_ID, FIELDS, Case
+
+ALL = (1 << len(FIELDS)) - 1
+
+
+def mask(*names: str) -> int:
+    m = 0
+    for n in names:
+        m |= 1 << FIELD_ID[n]
+    return m
+
+
+def _i(v: int):
+    return ctypes.byref(ctypes.c_int(int(v)))
+
+
+def _d(v: float):
+    return ctypes.byref(ctypes.c_double(float(v)))
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def boxargs(box):
+    return [_i(v) for v in box]
+
+
+GAMMA, PRL, PRT = 1.4, 0.72, 0.90
+
+
+class GpuCase:
+    def __init__(self, case: Case, device: int = 0):
+        self.case = case
+        L = self.L = _lib.load()
+        _lib.check(L.aero_init(ctypes.c_int(device)), "aero_init")
+        iflags = case.cfg.iflags()
+        params = case.cfg.params()
+        _lib.check(L.aero_configure(_p_int(iflags), _p(params)), "aero_configure")
+        self._keep = [iflags, params]
+        for b in case.blocks:
+            box = b.box18()
+            sub = b.sub_table()
+            self._keep += [box, sub]
+            _lib.check(L.aero_register_block(ctypes.c_int(b.m), _p_int(box), ctypes.c_int(len(b.subfaces)),
+                                             _p_int(sub)), "aero_register_block")
+            for fid, (name, _) in enumerate(FIELDS):
+                _lib.check(L.aero_bind_field(ctypes.c_int(b.m), ctypes.c_int(fid),
+                                             ctypes.c_void_p(b.ptr(name))), "aero_bind_field")
+        _lib.check(L.aero_finish_setup(), "aero_finish_setup")
+        ma = case.cfg.ma
+        self.cv = 1.0 / GAMMA / (GAMMA - 1.0) / ma / ma
+
+    # ------------------------------------------------------------- transfers
+    def sync_to_device(self, m: int = ALL) -> None:
+        _lib.check(self.L.aero_sync_to_device(ctypes.c_ulonglong(m)), "aero_sync_to_device")
+
+    def sync_to_host(self, m: int = ALL) -> None:
+        _lib.check(self.L.aero_sync_to_host(ctypes.c_ulonglong(m)), "aero_sync_to_host")
+
+    # ------------------------------------------------- module-state routines
+    def init_flowfield(self) -> None:
+        _lib.check(self.L.aero_init_flowfield(), "aero_init_flowfield")
+
+    def physical_bc(self) -> None:
+        _lib.check(self.L.aero_physical_bc(), "aero_physical_bc")
+
+    def updatebuffer(self) -> None:
+        _lib.check(self.L.aero_updatebuffer(), "aero_updatebuffer")
+
+    def updatebuffercoordinate(self) -> None:
+        _lib.check(self.L.aero_updatebuffercoordinate(), "aero_updatebuffercoordinate")
+
+    def average1(self) -> None:
+        _lib.check(self.L.aero_average1(), "aero_average1")
+
+    def average2(self) -> None:
+        _lib.check(self.L.aero_average2(), "aero_average2")
+
+    def getpri_all(self) -> None:
+        _lib.check(self.L.aero_getpri_all(), "aero_getpri_all")
+
+    def residual(self) -> np.ndarray:
+        out = np.zeros(7)
+        _lib.check(self.L.aero_residual(_p(out)), "aero_residual")
+        return out
+
+    def status(self) -> int:
+        s = ctypes.c_uint(0)
+        _lib.check(self.L.aero_get_status(ctypes.byref(s)), "aero_get_status")
+        return s.value
+
+    def start(self) -> None:
+        """main.f90:249-318 on the device: BCs, primitives, BCs, halo, averaging."""
+        self.physical_bc()
+        self.getpri_all()
+        self.physical_bc()
+        self.updatebuffer()
+        self.average1()
+        self.average2()
+
+    def step(self, nsteps: int, history: bool = True, dt_minmax: bool = False):
+        hist = np.zeros((nsteps, 7)) if history else None
+        dtm = np.zeros(2) if dt_minmax else None
+        _lib.check(self.L.aero_step(ctypes.c_int(nsteps), _p(hist) if history else None,
+                                    _p(dtm) if dt_minmax else None), "aero_step")
+        return (hist, dtm) if dt_minmax else hist
+
+    # ------------------------------------------- drop-in calls (one block)
+    def get_primitivevariables(self, b) -> None:
+        f = b.fields
+        _lib.check(self.L.aero_get_primitivevariables(_i(b.m), _p(f["pri_v"]), _p(f["q"]), _d(GAMMA),
+                                                      _d(self.cv), *boxargs(b.box)), "get_primitivevariables")
+
+    def inviscid_flux_1(self, b) -> None:
+        f = b.fields
+        _lib.check(self.L.aero_inviscid_flux_1(_p(f["rhsi"]), _p(f["q"]), _p(f["dxidx"]), _p(f["inv_j"]),
+                                               *boxargs(b.box), *boxargs(b.box0), *boxargs(b.box1),
+                                               _d(GAMMA)), "inviscid_flux_1")
+
+    def viscous_flux(self, b) -> None:
+        f = b.fields
+        c = self.case.cfg
+        _lib.check(self.L.aero_viscous_flux(_p(f["rhsv"]), _p(f["pri_v"]), _p(f["amu"]), _p(f["vor"]),
+                                            _p(f["dudx"]), _p(f["tao"]), _p(f["dxidx"]), _p(f["inv_j"]),
+                                            _d(c.tinf), _d(PRL), _d(PRT), _d(GAMMA), _d(self.cv), _d(c.re),
+                                            *boxargs(b.box), *boxargs(b.box0), *boxargs(b.box1), _i(b.m)),
+                   "viscous_flux")
+
+    def find_dt(self, b):
+        f = b.fields
+        c = self.case.cfg
+        out = [ctypes.c_double(0) for _ in range(4)]
+        cfl = ctypes.c_double(c.cfl)
+        _lib.check(self.L.aero_find_dt(_p(f["dt"]), *[ctypes.byref(x) for x in out], _p(f["pri_v"]),
+                                       _p(f["amu"]), _p(f["dxidx"]), _d(c.re), ctypes.byref(cfl),
+                                       *boxargs(b.box), _i(c.time), _i(0), _i(1)), "find_dt")
+        return [x.value for x in out]
+
+    def implicit1st(self, b) -> None:
+        f = b.fields
+        c = self.case.cfg
+        _lib.check(self.L.aero_implicit1st(_p(f["q"]), _p(f["dt"]), _p(f["pri_v"]), _p(f["rhs"]),
+                                           _p(f["rhsi"]), _p(f["rhsv"]), _p(f["dxidx"]), _p(f["inv_j"]),
+                                           *boxargs(b.box), *boxargs(b.box0), *boxargs(b.box1), _d(GAMMA),
+                                           _d(c.cfl), _p(f["x"]), _p(f["y"]), _p(f["z"])), "implicit1st")
+
+    def close(self) -> None:
+        _lib.check(self.L.aero_finalize(), "aero_finalize")
+
+
+def _p_int(a: np.ndarray):
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return ctypes.c_void_p(a.ctypes.data)

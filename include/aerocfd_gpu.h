@@ -1,0 +1,164 @@
+/*
+ * aerocfd_gpu.h - C ABI of the B200 (sm_100a) residual-and-update path of the
+ * aerocfd multi-block structured compressible-flow solver.
+ *
+ * The reference's hot-path routines are external Fortran subroutines with
+ * implicit interfaces: every argument by reference, arrays explicit-shape and
+ * column-major with caller-supplied bounds, e.g. q(5,is:ie,js:je,ks:ke).  The
+ * drop-in entry points below take exactly those arguments, in the same order
+ * and with the same meaning, so a Fortran `interface ... bind(C)` block can
+ * route the existing call sites of main.f90:357-447 here unchanged
+ * (fortran/aerocfd_gpu.f90).  The Fortran routines return nothing and print or
+ * stop on errors; these return a status (0 = AERO_OK) that the Fortran shim
+ * turns into the reference's print + stop.
+ *
+ * Two modes:
+ *  - transient: called with arrays that were never registered, an entry point
+ *    copies its inputs to the GPU, runs, and copies its outputs back;
+ *  - resident: after aero_register_block/aero_bind_field/aero_finish_setup and
+ *    aero_sync_to_device, calls whose array arguments are registered host
+ *    arrays run purely on the device copies; host arrays are refreshed only by
+ *    aero_sync_to_host.  The no-argument routines (physical_bc, halo, average,
+ *    residual) work on the registered blocks, the way the reference works on
+ *    its module state.
+ *
+ * One host thread drives the library; calls run in order on the library's
+ * CUDA stream.  Only 3-D cases (iflag_dimension = 3) and the 1st-order
+ * implicit time advance are supported; other flags are rejected.
+ */
+#ifndef AEROCFD_GPU_H
+#define AEROCFD_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define AERO_OK 0
+#define AERO_ERR_ARG 1      /* bad argument: size, field id, unsupported flag   */
+#define AERO_ERR_STATE 2    /* call out of order (no aero_init / no setup)      */
+#define AERO_ERR_CUDA 3     /* CUDA runtime error (text in aero_last_error)     */
+#define AERO_ERR_NOMEM 4    /* device allocation failed                         */
+#define AERO_ERR_DEVICE 5   /* device status word set (see aero_get_status)     */
+
+/* device status word bits (aero_get_status) */
+#define AERO_ST_NEG_DENSITY 1u        /* sub_getpri_v.f90:54-56 would print  */
+#define AERO_ST_NONFINITE_RESIDUAL 2u /* NaN/Inf in the residual norm        */
+
+/* ---- field ids (module_block.f90:20-91 arrays) ------------------------- */
+enum {
+  AERO_F_Q = 0,     /* q(5,...)       conservative variables                */
+  AERO_F_PRI_V,     /* pri_v(7,...)   d,u,v,w,p,t,c                        */
+  AERO_F_RHSI,      /* rhsi(5,...)                                          */
+  AERO_F_RHSV,      /* rhsv(5,...)                                          */
+  AERO_F_RHS,       /* rhs(5,...)                                           */
+  AERO_F_DT,        /* dt(...)                                              */
+  AERO_F_DXIDX,     /* dxidx(9,...)   metric terms                          */
+  AERO_F_INV_J,     /* inv_j(...)     1/J                                   */
+  AERO_F_AMU,       /* amu(3,...)     laminar, eddy, total viscosity        */
+  AERO_F_NUT,       /* nut(...)       SA working variable                   */
+  AERO_F_SA_RHS,    /* sa_rhs(...)                                          */
+  AERO_F_X, AERO_F_Y, AERO_F_Z,
+  AERO_F_DIST,      /* dist(...)      wall distance                         */
+  AERO_F_ALPHA, AERO_F_BETA, AERO_F_GGAMMA, /* aalpha/bbeta/ggamma(3,...)   */
+  AERO_F_DUDX,      /* dudx(9,...)                                          */
+  AERO_F_TAO,       /* tao(6,...)                                           */
+  AERO_F_VOR,       /* vor(...)                                             */
+  AERO_F_LENGTH,    /* length(...)    SA length scale                       */
+  AERO_F_SPACING,   /* spacing(...)                                         */
+  AERO_NUM_FIELDS
+};
+#define AERO_MASK(f) (1ull << (f))
+#define AERO_MASK_ALL ((1ull << AERO_NUM_FIELDS) - 1ull)
+
+/* ---- runtime ----------------------------------------------------------- */
+int aero_init(int device);
+int aero_finalize(void);
+/* Text of the last error (valid until the next call). */
+const char* aero_last_error(void);
+/* OR of the device status bits raised since the last call; clears them. */
+int aero_get_status(unsigned* status);
+
+/* ---- case set-up (replaces init_readcontrolfile / init_readbcinfo /
+ *      init_allocatememory module state, main.f90:80-140) ---------------- */
+/* iflags[8]: iflag_dimension, iflag_solver, iflag_time, iflag_timeadvance,
+ *            iflag_turbulence, iflag_des, bufferLength, iflag_inviscid
+ *            (sub_init_readcontrolfile.f90:30-47, main.f90:636-653)
+ * params[7]: ma, re, tinf, aoa (degrees), cfl, dt, nutinf               */
+int aero_configure(const int* iflags, const double* params);
+/* box18: is,ie,js,je,ks,ke, is0..ke0, is1..ke1 of block m (1-based)
+ *        (sub_init_allocatememory.f90:73-144)
+ * subfaces: num_subface rows of f_no,face,is,ie,js,je,ks,ke,blk_t,
+ *           subface_t,ori (sub_init_readbcinfo.f90:96-98)               */
+int aero_register_block(int m, const int* box18, int num_subface, const int* subfaces);
+/* Associates host array `host` (the reference's blk(m)%<field>) with field
+ * `field` of block m.  The array is page-locked for fast transfers. */
+int aero_bind_field(int m, int field, double* host);
+/* Allocates the device arena, builds the halo/average/BC tables. */
+int aero_finish_setup(void);
+/* Copies the bound host arrays of the fields in `mask` to / from the GPU. */
+int aero_sync_to_device(unsigned long long mask);
+int aero_sync_to_host(unsigned long long mask);
+
+/* ---- drop-in mirrors of the hot-path routines ------------------------- */
+/* sub_getpri_v.f90:19 */
+int aero_get_primitivevariables(const int* mm, double* pri_v, const double* q, const double* gamma,
+                                const double* cv, const int* is, const int* ie, const int* js,
+                                const int* je, const int* ks, const int* ke);
+/* sub_inviscid1.f90:8-11 (Roe flux on WENO3 states, all directions) */
+int aero_inviscid_flux_1(double* rhsi, const double* q, const double* dxidx, const double* inv_j,
+                         const int* is, const int* ie, const int* js, const int* je,
+                         const int* ks, const int* ke, const int* is0, const int* ie0,
+                         const int* js0, const int* je0, const int* ks0, const int* ke0,
+                         const int* is1, const int* ie1, const int* js1, const int* je1,
+                         const int* ks1, const int* ke1, const double* gamma);
+/* sub_viscous.f90:9-12 */
+int aero_viscous_flux(double* rhsv, const double* pri_v, double* amu, double* vor, double* dudx,
+                      double* tao, const double* dxidx, const double* inv_j, const double* tinf,
+                      const double* prl, const double* prt, const double* gamma, const double* cv,
+                      const double* re, const int* is, const int* ie, const int* js,
+                      const int* je, const int* ks, const int* ke, const int* is0,
+                      const int* ie0, const int* js0, const int* je0, const int* ks0,
+                      const int* ke0, const int* is1, const int* ie1, const int* js1,
+                      const int* je1, const int* ks1, const int* ke1, const int* mm);
+/* sub_timeadvancement_finddt.f90:24-25 (steady branch) */
+int aero_find_dt(double* dt, double* dtmax, double* dtmin, double* cflmax, double* cflmin,
+                 const double* pri_v, const double* amu, const double* dxidx, const double* re,
+                 double* cfl, const int* is, const int* ie, const int* js, const int* je,
+                 const int* ks, const int* ke, const int* iflag_time, const int* iflag_steady,
+                 const int* iflag_unsteady);
+/* sub_timeadvancement_1stimplicit.f90:7-11 (xx,yy,zz are debug-only, unused) */
+int aero_implicit1st(double* q, const double* dt, const double* pri_v, double* rhs,
+                     const double* rhsi, const double* rhsv, const double* dxidx,
+                     const double* inv_j, const int* is, const int* ie, const int* js,
+                     const int* je, const int* ks, const int* ke, const int* is0,
+                     const int* ie0, const int* js0, const int* je0, const int* ks0,
+                     const int* ke0, const int* is1, const int* ie1, const int* js1,
+                     const int* je1, const int* ks1, const int* ke1, const double* gamma,
+                     const double* cfl, const double* xx, const double* yy, const double* zz);
+
+/* ---- module-state routines (no arguments in the reference) ------------ */
+int aero_physical_bc(void);          /* sub_bc.f90:9                        */
+int aero_updatebuffer(void);         /* sub_bc_updatebuffer.f90:10          */
+int aero_average1(void);             /* sub_bc_updatebufferaverage.f90:10   */
+int aero_average2(void);             /* sub_bc_updatebufferaverage.f90:442  */
+int aero_updatebuffercoordinate(void); /* sub_bc_updatebuffercoordinate.f90:10 */
+/* sub_output_residual.f90:8: out7 = rms of rho,rho*u,rho*v,rho*w,rho*E,
+ * nut, (unused) over the updated nodes / totalnodes; the reference prints
+ * these and appends them to resi_history.dat. */
+int aero_residual(double* out7);
+/* sub_init_flowfield.f90:29-111 (freestream start) on all registered blocks */
+int aero_init_flowfield(void);
+/* primitives of all registered blocks (main.f90:434-447) */
+int aero_getpri_all(void);
+
+/* ---- whole iterations (main.f90:343-447 for every block, plus the residual
+ *      of main.f90:603 each step); resid_hist receives nsteps x 7 values
+ *      when not NULL.  dt_minmax (may be NULL) receives dtmax, dtmin of the
+ *      last block's find_dt of the last step. ------------------------------ */
+int aero_step(int nsteps, double* resid_hist, double* dt_minmax);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AEROCFD_GPU_H */

@@ -1,0 +1,194 @@
+"""FP64 parity of the CUDA path (through the C-ABI) with the CPU oracle.
+
+Tolerance: 1e-12 relative to each field's max magnitude, per routine and per
+iteration.  The only operations whose results may differ in the last bit are
+libm functions (pow, exp, tanh, cos, sin); everything else uses the
+reference's operation order without fused multiply-add, so most fields match
+bit for bit.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from aerocfd_b200 import grids
+from aerocfd_b200.case import FIELDS, Config, IFLAG_NSSOLVER
+from conftest import perturb, relerr
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+def _p(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def _d(x):
+    return ctypes.byref(ctypes.c_double(x))
+
+
+def _i(x):
+    return ctypes.byref(ctypes.c_int(x))
+
+
+def prepared(make, oracle_mod, seed=0, amp=0.01):
+    """Two identical cases: geometry and a perturbed, BC-consistent start
+    state computed by the oracle, copied into the case the GPU will use."""
+    co, cg = make(), make()
+    oc = oracle_mod.OracleCase(co)
+    oc.geometry()
+    oc.init_flowfield()
+    perturb(co, seed=seed, amp=amp)
+    oc.start()
+    for bo, bg in zip(co.blocks, cg.blocks):
+        for name, _ in FIELDS:
+            bg.fields[name][...] = bo.fields[name]
+    return oc, co, cg
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    from aerocfd_b200 import build, solver
+    build.build()
+    return solver
+
+
+def bump_small():
+    return grids.bump_channel(ni=33, nj=17, nk=5)
+
+
+def bump_ns():
+    return grids.bump_channel(ni=33, nj=17, nk=5, cfg=Config(solver=IFLAG_NSSOLVER, ma=0.5, re=2000.0, cfl=3.0))
+
+
+def naca_small():
+    return grids.naca_ogrid(nblk=4, ni=33, nj=17, nk=3)
+
+
+# ------------------------------------------------------------ per routine
+def test_getpri_and_inviscid_transient(gpu, oracle_mod):
+    oc, co, cg = prepared(bump_small, oracle_mod)
+    gc = gpu.GpuCase(cg)      # registered, but the calls below use copies (transient mode)
+    b = co.blocks[0]
+    f = {k: v.copy() for k, v in b.fields.items()}
+    L = gc.L
+    # primitives
+    rc = L.aero_get_primitivevariables(_i(1), _p(f["pri_v"]), _p(f["q"]), _d(1.4), _d(gc.cv),
+                                       *[_i(v) for v in b.box])
+    assert rc == 0
+    oc.getpri_all()
+    assert relerr(f["pri_v"], b.fields["pri_v"]) == 0.0
+    # inviscid residual
+    rc = L.aero_inviscid_flux_1(_p(f["rhsi"]), _p(f["q"]), _p(f["dxidx"]), _p(f["inv_j"]),
+                                *[_i(v) for v in b.box + b.box0 + b.box1], _d(1.4))
+    assert rc == 0
+    oc.L.oracle_inviscid_flux_1(_p(b.fields["rhsi"]), _p(b.fields["q"]), _p(b.fields["dxidx"]),
+                                _p(b.fields["inv_j"]), *oracle_mod.box_args(b.box),
+                                *oracle_mod.box_args(b.box0), *oracle_mod.box_args(b.box1), _d(1.4))
+    assert relerr(f["rhsi"], b.fields["rhsi"]) <= TOL
+    gc.close()
+
+
+def test_viscous_dt_implicit_transient(gpu, oracle_mod):
+    oc, co, cg = prepared(bump_ns, oracle_mod, seed=3)
+    gc = gpu.GpuCase(cg)
+    b = co.blocks[0]
+    oc.getpri_all()
+    f = {k: v.copy() for k, v in b.fields.items()}
+    L = gc.L
+    c = co.cfg
+    consts = oc.consts()
+    ob = oracle_mod.box_args
+    # viscous
+    args_g = [_p(f[k]) for k in ("rhsv", "pri_v", "amu", "vor", "dudx", "tao", "dxidx", "inv_j")]
+    assert L.aero_viscous_flux(*args_g, _d(c.tinf), _d(0.72), _d(0.9), _d(1.4), _d(consts[5]), _d(c.re),
+                               *[_i(v) for v in b.box + b.box0 + b.box1], _i(1)) == 0
+    F = b.fields
+    oc.L.oracle_viscous_flux(*[_p(F[k]) for k in ("rhsv", "pri_v", "amu", "vor", "dudx", "tao", "dxidx", "inv_j")],
+                             _d(c.tinf), _d(0.72), _d(0.9), _d(1.4), _d(consts[5]), _d(c.re),
+                             *ob(b.box), *ob(b.box0), *ob(b.box1), _i(1))
+    for k in ("rhsv", "amu", "vor", "dudx", "tao"):
+        assert relerr(f[k], F[k]) <= TOL, k
+    # local time step and the (else-if) dtmax/dtmin
+    outs = [ctypes.c_double(0) for _ in range(4)]
+    cfl = ctypes.c_double(c.cfl)
+    assert L.aero_find_dt(_p(f["dt"]), *[ctypes.byref(x) for x in outs], _p(f["pri_v"]), _p(f["amu"]),
+                          _p(f["dxidx"]), _d(c.re), ctypes.byref(cfl), *[_i(v) for v in b.box],
+                          _i(0), _i(0), _i(1)) == 0
+    oo = [ctypes.c_double(0) for _ in range(4)]
+    cfl_o = ctypes.c_double(c.cfl)
+    oc.L.oracle_find_dt(_p(F["dt"]), *[ctypes.byref(x) for x in oo], _p(F["pri_v"]), _p(F["amu"]),
+                        _p(F["dxidx"]), _d(c.re), ctypes.byref(cfl_o), *ob(b.box), _i(0), _i(0), _i(1))
+    assert relerr(f["dt"], F["dt"]) <= TOL
+    assert abs(outs[0].value - oo[0].value) <= TOL * oo[0].value
+    assert abs(outs[1].value - oo[1].value) <= TOL * oo[1].value
+    # implicit update
+    args = ("q", "dt", "pri_v", "rhs", "rhsi", "rhsv", "dxidx", "inv_j")
+    f["rhsi"][...] = F["rhsi"]
+    assert L.aero_implicit1st(*[_p(f[k]) for k in args], *[_i(v) for v in b.box + b.box0 + b.box1],
+                              _d(1.4), _d(c.cfl), _p(f["x"]), _p(f["y"]), _p(f["z"])) == 0
+    oc.L.oracle_implicit1st(*[_p(F[k]) for k in args], *ob(b.box), *ob(b.box0), *ob(b.box1), _d(1.4),
+                            _d(c.cfl), _p(F["x"]), _p(F["y"]), _p(F["z"]))
+    assert relerr(f["q"], F["q"]) <= TOL
+    assert relerr(f["rhs"], F["rhs"]) <= TOL
+    gc.close()
+
+
+# ------------------------------------------------------- whole iterations
+def run_parity(make, oracle_mod, gpu, nsteps, seed=0, check_every=1):
+    oc, co, cg = prepared(make, oracle_mod, seed=seed)
+    gc = gpu.GpuCase(cg)
+    gc.sync_to_device()
+    worst = 0.0
+    for s in range(nsteps):
+        ho = oc.iterate(1)
+        hg = gc.step(1)
+        assert np.all(np.isfinite(hg))
+        r = float(np.max(np.abs(hg[0, :5] - ho[0, :5]) / np.maximum(np.abs(ho[0, :5]), 1e-300)))
+        assert r <= 1e-10, f"step {s}: residual history differs by {r}"
+        if (s + 1) % check_every == 0 or s == nsteps - 1:
+            gc.sync_to_host(gpu.mask("q", "pri_v", "dt", "rhs"))
+            for bo, bg in zip(co.blocks, cg.blocks):
+                for k in ("q", "pri_v", "dt", "rhs"):
+                    e = relerr(bg.fields[k], bo.fields[k])
+                    worst = max(worst, e)
+                    assert e <= TOL, f"step {s}, block {bo.m}, {k}: {e}"
+    assert gc.status() == 0
+    gc.close()
+    return worst
+
+
+def test_bump_euler_iterations(gpu, oracle_mod):
+    run_parity(bump_small, oracle_mod, gpu, nsteps=6)
+
+
+def test_bump_navier_stokes_iterations(gpu, oracle_mod):
+    run_parity(bump_ns, oracle_mod, gpu, nsteps=4)
+
+
+def test_naca_ogrid_four_blocks(gpu, oracle_mod):
+    """Laminar NS, 4 blocks: halo, interface averaging, no-slip wall, farfield."""
+    run_parity(naca_small, oracle_mod, gpu, nsteps=5)
+
+
+def test_full_size_bump_97x49x5(gpu, oracle_mod):
+    run_parity(lambda: grids.bump_channel(), oracle_mod, gpu, nsteps=3, check_every=3)
+
+
+def test_full_size_naca_4x129x65x3(gpu, oracle_mod):
+    run_parity(lambda: grids.naca_ogrid(), oracle_mod, gpu, nsteps=2, check_every=2)
+
+
+def test_wavefront_is_deterministic(gpu, oracle_mod):
+    """Two runs from the same state give bit-identical q (no race in the
+    hyperplane sweep or the reductions)."""
+    outs = []
+    for _ in range(2):
+        oc, co, cg = prepared(naca_small, oracle_mod, seed=7)
+        gc = gpu.GpuCase(cg)
+        gc.sync_to_device()
+        gc.step(3, history=False)
+        gc.sync_to_host(gpu.mask("q"))
+        outs.append(np.concatenate([b.fields["q"].ravel() for b in cg.blocks]))
+        gc.close()
+    assert np.array_equal(outs[0], outs[1])
