@@ -61,5 +61,13 @@ __global__ void k_aos_to_soa(const double* __restrict__ src, double* __restrict_
 __global__ void k_soa_to_aos(const double* __restrict__ src, double* __restrict__ dst, long n,
                              int nc, long plane);
 __global__ void k_fill_plane(double* __restrict__ p, long n, double val);
+// one-time geometry
+__global__ void k_metric_pass1(const BlockView* __restrict__ blocks);
+__global__ void k_metric_pass2(const BlockView* __restrict__ blocks);
+__global__ void k_spacing(const BlockView* __restrict__ blocks);
+__global__ void k_wall_points(const BlockView* __restrict__ blocks, const AvgSrc* __restrict__ wall,
+                              long nwall, double* __restrict__ xyz);
+__global__ void k_walldist(const BlockView* __restrict__ blocks, const double* __restrict__ xyz,
+                           long nwall);
 
 }  // namespace aero

@@ -78,6 +78,74 @@ struct State {
 
 State g;
 
+// ---------------------------------------------------------------- profiling
+// Per-kernel CUDA-event timing on the library's stream (aero_profile_*), and a
+// count of every kernel this library launches (aero_launch_count).
+enum ProfId {
+  P_GETPRI, P_FILL, P_INVISCID, P_VISC_A, P_VISC_B, P_FIND_DT, P_DT_MINMAX, P_LUSGS_PREP,
+  P_LUSGS_SWEEP, P_BC, P_SA_CLIP, P_HALO, P_AVG_GATHER, P_AVG_APPLY, P_RESID_PART, P_RESID_FINAL,
+  P_TRANSFER, P_GEOMETRY, P_NUM
+};
+const char* kProfName[P_NUM] = {
+    "k_getpri", "k_fill", "k_inviscid", "k_viscous_a", "k_viscous_b", "k_find_dt", "k_dt_minmax",
+    "k_lusgs_prep", "k_lusgs_sweep", "k_physical_bc", "k_sa_clip", "k_halo", "k_avg_gather",
+    "k_avg_apply", "k_residual_partial", "k_residual_final", "k_transfer", "k_geometry"};
+struct Prof {
+  bool on = false;
+  std::vector<cudaEvent_t> pool;
+  size_t used = 0;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
+  double ms[P_NUM] = {};
+  long count[P_NUM] = {};
+  unsigned long long launches = 0;
+} gp;
+
+cudaEvent_t prof_event() {
+  if (gp.used == gp.pool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    gp.pool.push_back(e);
+  }
+  return gp.pool[gp.used++];
+}
+struct ProfScope {
+  int id;
+  cudaEvent_t a{}, b{};
+  ProfScope(int id_, cudaStream_t s) : id(id_) {
+    ++gp.launches;
+    if (gp.on) {
+      a = prof_event();
+      cudaEventRecord(a, s);
+    }
+  }
+  void end(cudaStream_t s) {
+    if (gp.on) {
+      b = prof_event();
+      cudaEventRecord(b, s);
+      gp.marks.push_back({id, {a, b}});
+    }
+  }
+};
+#define PROF(id, launch)                 \
+  do {                                   \
+    ProfScope ps_(id, g.stream);         \
+    launch;                              \
+    ps_.end(g.stream);                   \
+  } while (0)
+
+void prof_collect() {
+  if (gp.marks.empty()) return;
+  cudaStreamSynchronize(g.stream);
+  for (auto& m : gp.marks) {
+    float t = 0.f;
+    cudaEventElapsedTime(&t, m.second.first, m.second.second);
+    gp.ms[m.first] += t;
+    gp.count[m.first] += 1;
+  }
+  gp.marks.clear();
+  gp.used = 0;
+}
+
 int fail(int code, const char* fmt, ...) {
   char buf[512];
   va_list ap;
@@ -147,14 +215,14 @@ int upload(const double* host, double* dev_field, long n, int nc, long plane) {
   int rc = ensure_staging((size_t)n * nc);
   if (rc) return rc;
   CK(cudaMemcpyAsync(g.d_staging, host, (size_t)n * nc * sizeof(double), cudaMemcpyHostToDevice, g.stream));
-  k_aos_to_soa<<<cdiv(n, 256), 256, 0, g.stream>>>(g.d_staging, dev_field, n, nc, plane);
+  PROF(P_TRANSFER, (k_aos_to_soa<<<cdiv(n, 256), 256, 0, g.stream>>>(g.d_staging, dev_field, n, nc, plane)));
   CKL();
   return AERO_OK;
 }
 int download(double* host, const double* dev_field, long n, int nc, long plane) {
   int rc = ensure_staging((size_t)n * nc);
   if (rc) return rc;
-  k_soa_to_aos<<<cdiv(n, 256), 256, 0, g.stream>>>(dev_field, g.d_staging, n, nc, plane);
+  PROF(P_TRANSFER, (k_soa_to_aos<<<cdiv(n, 256), 256, 0, g.stream>>>(dev_field, g.d_staging, n, nc, plane)));
   CKL();
   CK(cudaMemcpyAsync(host, g.d_staging, (size_t)n * nc * sizeof(double), cudaMemcpyDeviceToHost, g.stream));
   return AERO_OK;
@@ -261,38 +329,38 @@ CaseConsts consts_with(double gamma, double cv, double re) {
 // --------------------------------------------------------- launch helpers
 int launch_getpri(const BlockView* views, int nblk, long maxN, const CaseConsts& cc) {
   dim3 grid(cdiv(maxN, 256), nblk);
-  k_getpri<<<grid, 256, 0, g.stream>>>(views, cc, g.d_status);
+  PROF(P_GETPRI, (k_getpri<<<grid, 256, 0, g.stream>>>(views, cc, g.d_status)));
   CKL();
   return AERO_OK;
 }
 int launch_inviscid(const BlockView* views, int nblk, long maxN, long maxN1, const CaseConsts& cc) {
-  k_fill<<<dim3(cdiv(maxN, 256), nblk), 256, 0, g.stream>>>(views, F_RHSI, 5, 0.0);
+  PROF(P_FILL, (k_fill<<<dim3(cdiv(maxN, 256), nblk), 256, 0, g.stream>>>(views, F_RHSI, 5, 0.0)));
   CKL();
-  k_inviscid<<<dim3(cdiv(maxN1, 128), nblk), 128, 0, g.stream>>>(views, cc);
+  PROF(P_INVISCID, (k_inviscid<<<dim3(cdiv(maxN1, 128), nblk), 128, 0, g.stream>>>(views, cc)));
   CKL();
   return AERO_OK;
 }
 int launch_viscous(const BlockView* views, int nblk, long maxN0, const CaseConsts& cc, int store) {
-  k_viscous_a<<<dim3(cdiv(maxN0, 128), nblk), 128, 0, g.stream>>>(views, cc, store);
+  PROF(P_VISC_A, (k_viscous_a<<<dim3(cdiv(maxN0, 128), nblk), 128, 0, g.stream>>>(views, cc, store)));
   CKL();
-  k_viscous_b<<<dim3(cdiv(maxN0, 256), nblk), 256, 0, g.stream>>>(views, cc);
+  PROF(P_VISC_B, (k_viscous_b<<<dim3(cdiv(maxN0, 256), nblk), 256, 0, g.stream>>>(views, cc)));
   CKL();
   return AERO_OK;
 }
 int launch_find_dt(const BlockView* views, int nblk, long maxN, const CaseConsts& cc) {
-  k_find_dt<<<dim3(cdiv(maxN, 256), nblk), 256, 0, g.stream>>>(views, cc, nullptr);
+  PROF(P_FIND_DT, (k_find_dt<<<dim3(cdiv(maxN, 256), nblk), 256, 0, g.stream>>>(views, cc, nullptr)));
   CKL();
   return AERO_OK;
 }
 int launch_dt_minmax(const BlockView* views, int m, double* d_out2) {
-  k_dt_minmax<<<1, 1024, 0, g.stream>>>(views, m, nullptr, 0, 0, d_out2);
+  PROF(P_DT_MINMAX, (k_dt_minmax<<<1, 1024, 0, g.stream>>>(views, m, nullptr, 0, 0, d_out2)));
   CKL();
   return AERO_OK;
 }
 int launch_implicit(const BlockView* views, int nblk, long maxExt, const CaseConsts& cc) {
-  k_lusgs_prep<<<dim3(cdiv(maxExt, 256), nblk), 256, 0, g.stream>>>(views, cc);
+  PROF(P_LUSGS_PREP, (k_lusgs_prep<<<dim3(cdiv(maxExt, 256), nblk), 256, 0, g.stream>>>(views, cc)));
   CKL();
-  k_lusgs_sweep<<<nblk, 256, 0, g.stream>>>(views, cc);
+  PROF(P_LUSGS_SWEEP, (k_lusgs_sweep<<<nblk, 256, 0, g.stream>>>(views, cc)));
   CKL();
   return AERO_OK;
 }
@@ -302,10 +370,10 @@ bool sa_on() { return g.cc.turbulence == IFLAG_SA && g.cc.solver == IFLAG_NSSOLV
 
 int do_physical_bc() {
   int nb = (int)g.blocks.size();
-  k_physical_bc<<<nb, 256, 0, g.stream>>>(g.d_blocks, g.d_bc_ops, g.d_bc_start, g.cc);
+  PROF(P_BC, (k_physical_bc<<<nb, 256, 0, g.stream>>>(g.d_blocks, g.d_bc_ops, g.d_bc_start, g.cc)));
   CKL();
   if (sa_on()) {
-    k_sa_clip<<<dim3(cdiv(g.max_box, 256), nb), 256, 0, g.stream>>>(g.d_blocks);
+    PROF(P_SA_CLIP, (k_sa_clip<<<dim3(cdiv(g.max_box, 256), nb), 256, 0, g.stream>>>(g.d_blocks)));
     CKL();
   }
   return AERO_OK;
@@ -313,30 +381,30 @@ int do_physical_bc() {
 int do_halo() {
   if (g.nhalo == 0) return AERO_OK;
   int mode = g.cc.turbulence == IFLAG_SA ? HALO_Q_NUT : HALO_Q;
-  k_halo<<<cdiv(g.nhalo, 256), 256, 0, g.stream>>>(g.d_blocks, g.d_halo, g.nhalo, mode);
+  PROF(P_HALO, (k_halo<<<cdiv(g.nhalo, 256), 256, 0, g.stream>>>(g.d_blocks, g.d_halo, g.nhalo, mode)));
   CKL();
   return AERO_OK;
 }
 int do_average1() {
   if (g.navg_src == 0) return AERO_OK;
-  k_avg_gather<<<cdiv(g.navg_src, 256), 256, 0, g.stream>>>(g.d_blocks, g.d_avg_src, g.navg_src,
-                                                              g.d_avg_buf, g.cc.turbulence == IFLAG_SA);
+  PROF(P_AVG_GATHER, (k_avg_gather<<<cdiv(g.navg_src, 256), 256, 0, g.stream>>>(
+                         g.d_blocks, g.d_avg_src, g.navg_src, g.d_avg_buf, g.cc.turbulence == IFLAG_SA)));
   CKL();
   return AERO_OK;
 }
 int do_average2() {
   if (g.navg_dst == 0) return AERO_OK;
-  k_avg_apply<<<cdiv(g.navg_dst, 256), 256, 0, g.stream>>>(g.d_blocks, g.d_avg_dst, g.navg_dst,
-                                                             g.d_avg_buf, g.cc.turbulence == IFLAG_SA);
+  PROF(P_AVG_APPLY, (k_avg_apply<<<cdiv(g.navg_dst, 256), 256, 0, g.stream>>>(
+                        g.d_blocks, g.d_avg_dst, g.navg_dst, g.d_avg_buf, g.cc.turbulence == IFLAG_SA)));
   CKL();
   return AERO_OK;
 }
 int do_residual(double* d_out7) {
   int nb = (int)g.blocks.size();
-  k_residual_partial<<<dim3(g.resid_ctas, nb), 256, 0, g.stream>>>(g.d_blocks, g.d_part, sa_on());
+  PROF(P_RESID_PART, (k_residual_partial<<<dim3(g.resid_ctas, nb), 256, 0, g.stream>>>(g.d_blocks, g.d_part, sa_on())));
   CKL();
-  k_residual_final<<<1, 256, 0, g.stream>>>(g.d_part, (long)g.resid_ctas * nb, g.totalnodes, d_out7,
-                                            g.d_status);
+  PROF(P_RESID_FINAL, (k_residual_final<<<1, 256, 0, g.stream>>>(g.d_part, (long)g.resid_ctas * nb,
+                                                                  g.totalnodes, d_out7, g.d_status)));
   CKL();
   return AERO_OK;
 }
@@ -475,7 +543,16 @@ int aero_register_block(int m, const int* box18, int num_subface, const int* sub
   H.b = Box{box18[0], box18[1], box18[2], box18[3], box18[4], box18[5]};
   H.b0 = Box{box18[6], box18[7], box18[8], box18[9], box18[10], box18[11]};
   H.b1 = Box{box18[12], box18[13], box18[14], box18[15], box18[16], box18[17]};
-  if (H.b.nx() < 1 || H.b.ny() < 1 || H.b.nz() < 1) return fail(AERO_ERR_ARG, "block %d: empty box", m);
+  // Stencils reach two nodes along each direction and the updated box sits
+  // inside the physical one; require at least 3 nodes per direction and
+  // consistent nested boxes.
+  const Box &b = H.b, &b0 = H.b0, &b1 = H.b1;
+  if (b0.nx() < 3 || b0.ny() < 3 || b0.nz() < 3)
+    return fail(AERO_ERR_ARG, "block %d: need at least 3 nodes per direction in 3-D", m);
+  if (b.is > b0.is || b.ie < b0.ie || b.js > b0.js || b.je < b0.je || b.ks > b0.ks || b.ke < b0.ke ||
+      b1.is < b.is + 1 || b1.ie > b.ie - 1 || b1.js < b.js + 1 || b1.je > b.je - 1 ||
+      b1.ks < b.ks + 1 || b1.ke > b.ke - 1 || b1.is < b0.is - 0 || b1.ie > b0.ie)
+    return fail(AERO_ERR_ARG, "block %d: index boxes are not nested as is <= is0 <= is1", m);
   for (int s = 0; s < num_subface; ++s) {
     const int* r = subfaces + 11 * s;
     H.subs.push_back(SubRow{r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7], r[8], r[9], r[10]});
@@ -715,7 +792,7 @@ int aero_updatebuffercoordinate(void) {
   int rc = need_setup();
   if (rc) return rc;
   if (g.nhalo == 0) return AERO_OK;
-  k_halo<<<cdiv(g.nhalo, 256), 256, 0, g.stream>>>(g.d_blocks, g.d_halo, g.nhalo, HALO_COORD);
+  PROF(P_HALO, (k_halo<<<cdiv(g.nhalo, 256), 256, 0, g.stream>>>(g.d_blocks, g.d_halo, g.nhalo, HALO_COORD)));
   CKL();
   return AERO_OK;
 }
@@ -752,7 +829,7 @@ int aero_init_flowfield(void) {
     const BlockView& v = g.views[m];
     long N = g.blocks[m].b.size();
     auto put = [&](double* dst, double val) -> int {
-      k_fill_plane<<<cdiv(N, 256), 256, 0, g.stream>>>(dst, N, val);
+      PROF(P_FILL, (k_fill_plane<<<cdiv(N, 256), 256, 0, g.stream>>>(dst, N, val)));
       CKL();
       return AERO_OK;
     };
@@ -769,6 +846,153 @@ int aero_init_flowfield(void) {
         if ((rc = put(v.f[fid] + x * v.plane, 0.0))) return rc;
   }
   CK(cudaStreamSynchronize(g.stream));
+  return AERO_OK;
+}
+
+int aero_gridtransformation(double* dxidx, double* inv_j, double* alpha, double* beta, double* gamma,
+                            const double* x, const double* y, const double* z, const int* is,
+                            const int* ie, const int* js, const int* je, const int* ks,
+                            const int* ke, const int* is0, const int* ie0, const int* js0,
+                            const int* je0, const int* ks0, const int* ke0, const int* m0) {
+  (void)m0;
+  int rc = need_init();
+  if (rc) return rc;
+  Box b = box_of(is, ie, js, je, ks, ke), b0 = box_of(is0, ie0, js0, je0, ks0, ke0);
+  std::vector<Arg> args = {{F_X, x, false},        {F_Y, y, false},        {F_Z, z, false},
+                           {F_DXIDX, dxidx, true}, {F_INVJ, inv_j, true},  {F_ALPHA, alpha, true},
+                           {F_BETA, beta, true},   {F_GAMMA, gamma, true}};
+  BlockTarget t;
+  auto it = g.registry.find(x);
+  if (it != g.registry.end()) {
+    const HostBlock& H = g.blocks[it->second.first];
+    if (!same(H.b, b) || !same(H.b0, b0)) return fail(AERO_ERR_ARG, "gridtransformation: bounds differ from the registered block");
+    rc = resolve(H.b, H.b0, H.b1, args, t);
+  } else {
+    rc = resolve(b, b0, b0, args, t);
+  }
+  if (rc) return rc;
+  PROF(P_GEOMETRY, (k_metric_pass1<<<dim3(cdiv(b.size(), 256), 1), 256, 0, g.stream>>>(t.d_view)));
+  CKL();
+  PROF(P_GEOMETRY, (k_metric_pass2<<<dim3(cdiv(b.size(), 128), 1), 128, 0, g.stream>>>(t.d_view)));
+  CKL();
+  return finish(t, args);
+}
+
+int aero_init_walldist(void) {
+  int rc = need_setup();
+  if (rc) return rc;
+  // wall-subface nodes of every block (sub_init_readbcinfo.f90:286-388)
+  std::vector<AvgSrc> wall;
+  for (int m = 0; m < (int)g.blocks.size(); ++m) {
+    const HostBlock& H = g.blocks[m];
+    for (const SubRow& s : H.subs) {
+      if (s.blk_t != BC_WALL) continue;
+      for (int k = s.ks; k <= s.ke; ++k)
+        for (int j = s.js; j <= s.je; ++j)
+          for (int i = s.is; i <= s.ie; ++i) {
+            int ii = s.face == 1 ? H.b0.is : s.face == 2 ? H.b0.ie : i;
+            int jj = s.face == 3 ? H.b0.js : s.face == 4 ? H.b0.je : j;
+            int kk = s.face == 5 ? H.b0.ks : s.face == 6 ? H.b0.ke : k;
+            long n = (long)(ii - H.b.is) + (long)H.b.nx() * ((long)(jj - H.b.js) + (long)H.b.ny() * (long)(kk - H.b.ks));
+            wall.push_back(AvgSrc{m, n});
+          }
+    }
+  }
+  long nw = (long)wall.size();
+  AvgSrc* d_wall = nullptr;
+  double* d_xyz = nullptr;
+  if (nw > 0) {
+    CK(cudaMalloc(&d_wall, nw * sizeof(AvgSrc)));
+    CK(cudaMalloc(&d_xyz, nw * 3 * sizeof(double)));
+    CK(cudaMemcpyAsync(d_wall, wall.data(), nw * sizeof(AvgSrc), cudaMemcpyHostToDevice, g.stream));
+    PROF(P_GEOMETRY, (k_wall_points<<<cdiv(nw, 256), 256, 0, g.stream>>>(g.d_blocks, d_wall, nw, d_xyz)));
+    CKL();
+  }
+  PROF(P_GEOMETRY, (k_walldist<<<dim3(cdiv(g.max_b0, 256), (unsigned)g.blocks.size()), 256, 256 * 3 * sizeof(double), g.stream>>>( g.d_blocks, d_xyz, nw)));
+  CKL();
+  CK(cudaStreamSynchronize(g.stream));
+  if (d_wall) CK(cudaFree(d_wall));
+  if (d_xyz) CK(cudaFree(d_xyz));
+  return AERO_OK;
+}
+
+// Coordinate halo, metrics, spacing and (optionally) wall distance for every
+// registered block: main.f90:142-208 on the device.
+int aero_compute_geometry(int with_walldist) {
+  int rc = need_setup();
+  if (rc) return rc;
+  if ((rc = aero_updatebuffercoordinate())) return rc;
+  int nb = (int)g.blocks.size();
+  PROF(P_GEOMETRY, (k_metric_pass1<<<dim3(cdiv(g.max_box, 256), nb), 256, 0, g.stream>>>(g.d_blocks)));
+  CKL();
+  PROF(P_GEOMETRY, (k_metric_pass2<<<dim3(cdiv(g.max_box, 128), nb), 128, 0, g.stream>>>(g.d_blocks)));
+  CKL();
+  PROF(P_GEOMETRY, (k_spacing<<<dim3(cdiv(g.max_b0, 256), nb), 256, 0, g.stream>>>(g.d_blocks)));
+  CKL();
+  if (with_walldist && (rc = aero_init_walldist())) return rc;
+  CK(cudaStreamSynchronize(g.stream));
+  return AERO_OK;
+}
+
+// Device-timed iterations for benchmarking: each step is one iteration plus the
+// residual norm (the reference computes it every iteration, outinterval = 1).
+// With flush_l2 a 256 MiB buffer is overwritten (cudaMemsetAsync, outside the
+// timed interval) before every step so each step starts with a cold L2.
+int aero_step_timed(int nsteps, int flush_l2, double* device_ms) {
+  int rc = need_setup();
+  if (rc) return rc;
+  static void* flush = nullptr;
+  const size_t fbytes = 256ull << 20;
+  if (flush_l2 && !flush) CK(cudaMalloc(&flush, fbytes));
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  double total = 0.0;
+  for (int s = 0; s < nsteps; ++s) {
+    if (flush_l2) CK(cudaMemsetAsync(flush, s & 0xff, fbytes, g.stream));
+    CK(cudaEventRecord(a, g.stream));
+    if ((rc = do_iteration(false))) return rc;
+    if ((rc = do_residual(g.d_out))) return rc;
+    CK(cudaEventRecord(b, g.stream));
+    CK(cudaEventSynchronize(b));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, a, b));
+    total += ms;
+  }
+  if (nsteps > 0 && (rc = do_getpri_all())) return rc;
+  CK(cudaStreamSynchronize(g.stream));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *device_ms = total;
+  return AERO_OK;
+}
+
+int aero_profile(int enable) {
+  int rc = need_init();
+  if (rc) return rc;
+  prof_collect();
+  gp.on = enable != 0;
+  if (enable) {
+    for (int i = 0; i < P_NUM; ++i) { gp.ms[i] = 0.0; gp.count[i] = 0; }
+  }
+  return AERO_OK;
+}
+
+int aero_profile_read(double* ms, long long* counts, int n) {
+  int rc = need_init();
+  if (rc) return rc;
+  prof_collect();
+  for (int i = 0; i < n && i < P_NUM; ++i) {
+    ms[i] = gp.ms[i];
+    counts[i] = gp.count[i];
+  }
+  return P_NUM;
+}
+
+const char* aero_profile_name(int id) { return (id >= 0 && id < P_NUM) ? kProfName[id] : ""; }
+
+int aero_launch_count(unsigned long long* count) {
+  *count = gp.launches;
   return AERO_OK;
 }
 

@@ -95,6 +95,20 @@ std::string build_topology(const std::vector<TopoBlock>& blocks, int buffer_leng
         std::snprintf(msg, sizeof msg, "block %d subface %zu: bad face or non-planar range", m + 1, s + 1);
         return msg;
       }
+      const Box& b0 = blocks[m].b0;
+      if (!b0.contains(r.is, r.js, r.ks) || !b0.contains(r.ie, r.je, r.ke)) {
+        std::snprintf(msg, sizeof msg, "block %d subface %zu: range outside the block's nodes", m + 1, s + 1);
+        return msg;
+      }
+      // the no-slip wall reads three nodes inward, the other routines one
+      int dir = (r.face - 1) / 2;
+      int n0[3] = {b0.nx(), b0.ny(), b0.nz()};
+      int need = (r.blk_t == BC_WALL && solver == IFLAG_NSSOLVER) ? 4 : 2;
+      if (r.blk_t < 0 && n0[dir] < need) {
+        std::snprintf(msg, sizeof msg, "block %d: fewer than %d nodes normal to boundary face %d", m + 1,
+                      need, r.face);
+        return msg;
+      }
       if (r.blk_t > 0) {
         if (r.blk_t > nb || r.subface_t < 1 || r.subface_t > (int)blocks[r.blk_t - 1].subs.size() ||
             r.ori < 1 || r.ori > 4) {

@@ -1,0 +1,311 @@
+#!/usr/bin/env python
+"""Throughput of aerocfd's residual-and-update iteration on B200.
+
+Workload: the laminar Navier-Stokes 4-block O-grid around an analytic NACA0012
+(4 x 129x65x3 nodes, farfield radius 20 chords, wall spacing 1e-4 chord,
+M=0.5, Re=5000, AoA=2 deg), synthetic and generated in-process, started from
+freestream.  Scheme: the reference's Roe flux on WENO3 states with 2nd-order
+central viscous terms and the 1st-order implicit LU-SGS update, FP64.
+
+A step is one iteration of main.f90:343-447 for every block plus the residual
+norm of sub_output_residual.f90 (the reference computes it every iteration).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value: Mcell-iter/s (nodes x steps / device time), inputs resident on the GPU,
+L2 flushed before every timed step.  e2e: the same metric through the C-ABI
+with the solution held on the host: every step copies q host->device, runs
+the iteration and copies q and the residual back.  --impl reference times the
+CPU restatement of the reference's algorithm (the reference is Fortran + MPI
+and cannot be compiled in this image) on the host cores, one thread per block
+like one MPI rank per block.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "naca0012_ogrid_4x129x65x3_laminar_fp64"
+HBM_FALLBACK = 6650.0
+
+# Algorithmic bytes per processed node of each kernel class (FP64): every
+# array the kernel must read once plus every array it must write once.
+KERNEL_BYTES = {
+    "k_lusgs_sweep": 49 * 8,   # q,dxidx,inv_j,ra,rb,rc,diag,rhs read; dq*,dq w+r; q w
+    "k_inviscid": 20 * 8,      # q,dxidx,inv_j read; rhsi write
+    "k_viscous_a": 30 * 8,     # pri(u,v,w,t),amu2,dxidx,inv_j read; amu1,amu3,vor,fv/gv/hv write
+    "k_viscous_b": 17 * 8,     # fv/gv/hv read; rhsv write
+    "k_find_dt": 23 * 8,       # dxidx,pri(d,u,v,w,c),amu3 read; dt write
+    "k_lusgs_prep": 22 * 8,    # pri(u,v,w,c),dxidx,dt,rhsi,rhsv read; ra,rb,rc,diag,rhs write
+    "k_getpri": 12 * 8,        # q read; pri write
+}
+# The whole iteration's compulsory footprint for Euler/laminar FP64: read q,
+# dxidx, inv_j, write q, dq* write+read = 30 words per node.
+ITER_BYTES = 240
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-sample-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK, "fallback"
+
+
+def make_case():
+    from aerocfd_b200 import grids
+    return grids.naca_ogrid()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                p = [x.strip() for x in line.split(",")]
+                if len(p) >= 9:
+                    rows.append(p)
+        except Exception:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        for r in rows:
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"), r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def cpu_reference(seconds: float, steps: int = 0, warmup: int = 0):
+    """Times the CPU restatement (oracle/, -O3, one thread per block)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # CPU baseline only
+    case = make_case()
+    oc = oracle.OracleCase(case, fast=True)
+    oc.geometry()
+    oc.init_flowfield()
+    oc.start()
+    threads = min(len(case.blocks), os.cpu_count() or 1)
+    if warmup:
+        oc.iterate(warmup, threads)
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        oc.iterate(1, threads)
+        n += 1
+        el = time.perf_counter() - t0
+        if steps and n >= steps:
+            break
+        if not steps and (el >= seconds and n >= 2):
+            break
+    el = time.perf_counter() - t0
+    return case.nodes * n / el / 1e6, n, el, threads
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.warmup < 3:
+        args.warmup = 3
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        v, n, el, thr = cpu_reference(0.0, steps=args.steps, warmup=args.warmup)
+        line = {"metric": "Mcell-iter/s", "value": v, "unit": "Mcell-iter/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / n,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "impl": "reference",
+                "config": {"workload": WORKLOAD, "blocks": 4, "nodes": make_case().nodes},
+                "cpu_baseline": {"value": v, "unit": "Mcell-iter/s", "cores": thr, "kind": "port",
+                                 "sample": f"{n} full iterations of the workload on {thr} threads "
+                                           f"(one per block), C++ -O3 restatement"},
+                "e2e": {"value": v, "unit": "Mcell-iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        torch.cuda.set_device(local)
+
+    from aerocfd_b200 import _lib, solver
+    case = make_case()
+    gc = solver.GpuCase(case, device=local)
+    L = gc.L
+    _lib.check(L.aero_compute_geometry(ctypes.c_int(0)), "aero_compute_geometry")
+    gc.init_flowfield()
+    gc.start()
+    gc.step(args.warmup, history=False)
+
+    # ---- device-timed steps (resident inputs, L2 flushed before each step)
+    cnt0 = ctypes.c_ulonglong(0)
+    L.aero_launch_count(ctypes.byref(cnt0))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms = ctypes.c_double(0.0)
+    with ClockSampler(local) as clk:
+        _lib.check(L.aero_step_timed(ctypes.c_int(args.steps), ctypes.c_int(1), ctypes.byref(ms)), "aero_step_timed")
+    torch.cuda.synchronize()
+    cnt1 = ctypes.c_ulonglong(0)
+    L.aero_launch_count(ctypes.byref(cnt1))
+    dev_s = ms.value / 1e3
+    if dist:
+        t = torch.tensor([dev_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_s = float(t.item())
+    nodes = case.nodes
+    value = nodes * args.steps * world / dev_s / 1e6
+
+    # ---- per-kernel profile (separate pass) for the roofline
+    L.aero_profile(ctypes.c_int(1))
+    prof_steps = max(5, min(args.steps, 20))
+    _lib.check(L.aero_step_timed(ctypes.c_int(prof_steps), ctypes.c_int(1), ctypes.byref(ms)), "profile")
+    L.aero_profile(ctypes.c_int(0))
+    kms = (ctypes.c_double * 32)()
+    kct = (ctypes.c_longlong * 32)()
+    nk = L.aero_profile_read(kms, kct, ctypes.c_int(32))
+    L.aero_profile_name.restype = ctypes.c_char_p
+    kernels = {}
+    for i in range(nk):
+        if kct[i]:
+            kernels[L.aero_profile_name(ctypes.c_int(i)).decode()] = {"ms_total": kms[i], "launches": int(kct[i])}
+    dom = max(kernels, key=lambda k: kernels[k]["ms_total"])
+    hbm, hbm_kind = peaks()
+    per_launch_ms = kernels[dom]["ms_total"] / kernels[dom]["launches"]
+    def count(boxname):
+        tot = 0
+        for b in case.blocks:
+            bx = getattr(b, boxname)
+            tot += (bx[1] - bx[0] + 1) * (bx[3] - bx[2] + 1) * (bx[5] - bx[4] + 1)
+        return tot
+    box_of_kernel = {"k_lusgs_sweep": "box1", "k_inviscid": "box1", "k_viscous_a": "box0",
+                     "k_viscous_b": "box0", "k_residual_partial": "box1"}
+    n_units = count(box_of_kernel.get(dom, "box"))
+    alg_bytes = KERNEL_BYTES.get(dom, ITER_BYTES) * n_units
+    achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
+    step_ms_prof = ms.value / prof_steps
+    for k in kernels:
+        kernels[k]["share"] = kernels[k]["ms_total"] / max(1e-12, sum(x["ms_total"] for x in kernels.values()))
+
+    # ---- end-to-end through the C-ABI with host-held q
+    qbytes = sum(b.fields["q"].nbytes for b in case.blocks)
+    mq = solver.mask("q")
+    gc.sync_to_host(mq)
+    res = np.zeros(7)
+    for _ in range(2):
+        gc.sync_to_device(mq); gc.step(1); gc.sync_to_host(mq)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        gc.sync_to_device(mq)
+        _lib.check(L.aero_step(ctypes.c_int(1), res.ctypes.data_as(ctypes.c_void_p), None), "aero_step")
+        gc.sync_to_host(mq)
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = nodes * args.steps * world / e2e_s / 1e6
+
+    status = gc.status()
+    line = {
+        "metric": "Mcell-iter/s", "value": value, "unit": "Mcell-iter/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dev_s / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (analytic NACA0012 O-grid, freestream start)",
+        "config": {"workload": WORKLOAD, "blocks": len(case.blocks), "nodes": nodes,
+                   "ma": case.cfg.ma, "re": case.cfg.re, "aoa_deg": case.cfg.aoa_deg, "cfl": case.cfg.cfl,
+                   "scheme": "roe_weno3 + central viscous + lu-sgs (reference path)",
+                   "l2": "flushed (256 MiB write) before every timed step",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e, "unit": "Mcell-iter/s", "h2d_bytes_per_step": qbytes,
+                "d2h_bytes_per_step": qbytes + 56},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "peak_kind": hbm_kind, "traffic": None,
+                     "alg_bytes_per_launch": alg_bytes, "ms_per_launch": per_launch_ms},
+        "iteration_roofline": {"bytes_per_node_iter": ITER_BYTES,
+                               "achieved_gbs": ITER_BYTES * nodes / (dev_s / args.steps) / 1e9,
+                               "frac": ITER_BYTES * nodes / (dev_s / args.steps) / 1e9 / hbm},
+        "kernels": kernels,
+        "clocks": clk.summary(),
+        "gpu_launches": int(cnt1.value - cnt0.value),
+        "device_status": status,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, n, el, thr = cpu_reference(args.cpu_sample_seconds)
+        line["cpu_baseline"] = {"value": v, "unit": "Mcell-iter/s", "cores": thr, "kind": "port",
+                                "sample": f"{n} full iterations of the same workload, {el:.1f} s, "
+                                          f"{thr} threads (one per block), C++ -O3 restatement"}
+    if rank == 0:
+        print(json.dumps(line))
+    gc.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

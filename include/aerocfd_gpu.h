@@ -137,6 +137,15 @@ int aero_implicit1st(double* q, const double* dt, const double* pri_v, double* r
                      const int* je1, const int* ks1, const int* ke1, const double* gamma,
                      const double* cfl, const double* xx, const double* yy, const double* zz);
 
+/* sub_init_gridtransformation.f90:27-29 (3-D): metrics, 1/J, alpha/beta/gamma.
+ * Ghost-corner nodes (two or more indices in overlap layers) are left as the
+ * caller stored them, as in the reference. */
+int aero_gridtransformation(double* dxidx, double* inv_j, double* alpha, double* beta, double* gamma,
+                            const double* x, const double* y, const double* z, const int* is,
+                            const int* ie, const int* js, const int* je, const int* ks,
+                            const int* ke, const int* is0, const int* ie0, const int* js0,
+                            const int* je0, const int* ks0, const int* ke0, const int* m0);
+
 /* ---- module-state routines (no arguments in the reference) ------------ */
 int aero_physical_bc(void);          /* sub_bc.f90:9                        */
 int aero_updatebuffer(void);         /* sub_bc_updatebuffer.f90:10          */
@@ -149,6 +158,11 @@ int aero_updatebuffercoordinate(void); /* sub_bc_updatebuffercoordinate.f90:10 *
 int aero_residual(double* out7);
 /* sub_init_flowfield.f90:29-111 (freestream start) on all registered blocks */
 int aero_init_flowfield(void);
+/* sub_init_walldist.f90:9 (wall distance of every physical node) */
+int aero_init_walldist(void);
+/* main.f90:142-208 for every registered block on the device: coordinate halo,
+ * metrics, spacing (sub_init_spacing.f90) and, if with_walldist, wall distance */
+int aero_compute_geometry(int with_walldist);
 /* primitives of all registered blocks (main.f90:434-447) */
 int aero_getpri_all(void);
 
@@ -157,6 +171,24 @@ int aero_getpri_all(void);
  *      when not NULL.  dt_minmax (may be NULL) receives dtmax, dtmin of the
  *      last block's find_dt of the last step. ------------------------------ */
 int aero_step(int nsteps, double* resid_hist, double* dt_minmax);
+
+/* Benchmark form of aero_step: nsteps iterations, each with its residual
+ * norm, timed on the device with CUDA events (device_ms = total); with
+ * flush_l2 != 0 the L2 cache is overwritten before every step, outside the
+ * timed interval. */
+int aero_step_timed(int nsteps, int flush_l2, double* device_ms);
+
+/* ---- instrumentation ---------------------------------------------------
+ * aero_profile(1) starts timing every kernel launch with CUDA events on the
+ * library's stream (and zeroes the totals); aero_profile(0) stops.
+ * aero_profile_read fills ms[i] (total milliseconds) and counts[i] (launches)
+ * for kernel class i < n and returns the number of classes;
+ * aero_profile_name(i) names class i.  aero_launch_count returns how many
+ * kernels the library has launched since it was loaded. */
+int aero_profile(int enable);
+int aero_profile_read(double* ms, long long* counts, int n);
+const char* aero_profile_name(int id);
+int aero_launch_count(unsigned long long* count);
 
 #ifdef __cplusplus
 }

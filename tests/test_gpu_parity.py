@@ -192,3 +192,26 @@ def test_wavefront_is_deterministic(gpu, oracle_mod):
         outs.append(np.concatenate([b.fields["q"].ravel() for b in cg.blocks]))
         gc.close()
     assert np.array_equal(outs[0], outs[1])
+
+
+# ------------------------------------------------------------ geometry
+@pytest.mark.parametrize("make", [naca_small, lambda: grids.bump_channel(ni=33, nj=17, nk=5)])
+def test_geometry_matches_oracle(gpu, oracle_mod, make):
+    """Coordinate halo, metrics, 1/J, alpha/beta/gamma, spacing and wall
+    distance computed on the GPU (aero_compute_geometry) equal the oracle's."""
+    co, cg = make(), make()
+    oc = oracle_mod.OracleCase(co)
+    oc.geometry(walldist=True)
+    gc = gpu.GpuCase(cg)
+    gc.sync_to_device(gpu.mask("x", "y", "z"))
+    from aerocfd_b200 import _lib
+    _lib.check(gc.L.aero_compute_geometry(ctypes.c_int(1)), "aero_compute_geometry")
+    names = ("x", "y", "z", "dxidx", "inv_j", "alpha", "beta", "ggamma", "spacing", "dist")
+    gc.sync_to_host(gpu.mask(*names))
+    for bo, bg in zip(co.blocks, cg.blocks):
+        for k in names:
+            a, b = bg.fields[k], bo.fields[k]
+            if k in ("spacing", "dist"):  # the oracle writes physical nodes only
+                a, b = a[bg.sl(bg.box0)], b[bo.sl(bo.box0)]
+            assert relerr(a, b) <= TOL, (bo.m, k, relerr(a, b))
+    gc.close()
