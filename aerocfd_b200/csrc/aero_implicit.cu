@@ -49,25 +49,18 @@ __global__ void k_lusgs_prep(const BlockView* __restrict__ blocks, CaseConsts cc
   B.s(F_DIAG, n) = phi * 1.0 / B.s(F_DT, n) + rr[0] + rr[1] + rr[2];
 }
 
-// calc_jm (sub_timeadvancement_jac.f90:17-62) at node nb with the metric row
-// starting at component cbase, the spectral radius added (forward, sgn>0) or
-// subtracted (backward) on the diagonal, everything scaled by 0.5*inv_j(nb)
-// (sub_timeadvancement_1stimplicit.f90:283-301), then multiplied into dqn:
-// out[n] = sum_c M(n,c)*dqn[c], summed left to right (:346-350).
-__device__ __forceinline__ void lusgs_matvec(const BlockView& B, long nb, int cbase, int radf,
-                                             bool plus, double gamma, const double dqn[5],
-                                             double out[5]) {
-  double rho = B.v(F_Q, 1, nb), mu0 = B.v(F_Q, 2, nb), mv0 = B.v(F_Q, 3, nb);
-  double mw0 = B.v(F_Q, 4, nb), e0 = B.v(F_Q, 5, nb);
-  double dxidx = B.v(F_DXIDX, cbase, nb), dxidy = B.v(F_DXIDX, cbase + 1, nb);
-  double dxidz = B.v(F_DXIDX, cbase + 2, nb);
-  double rad = B.s(radf, nb);
-  double invj = B.s(F_INVJ, nb);
+// calc_jm (sub_timeadvancement_jac.f90:17-62) at node n with the metric row
+// starting at component cbase; A is row-major, A[r*5+c] = a(r+1,c+1).
+__device__ __forceinline__ void calc_jm(const BlockView& B, long n, int cbase, double gamma,
+                                        double A[25]) {
+  double rho = B.v(F_Q, 1, n), mu0 = B.v(F_Q, 2, n), mv0 = B.v(F_Q, 3, n);
+  double mw0 = B.v(F_Q, 4, n), e0 = B.v(F_Q, 5, n);
+  double dxidx = B.v(F_DXIDX, cbase, n), dxidy = B.v(F_DXIDX, cbase + 1, n);
+  double dxidz = B.v(F_DXIDX, cbase + 2, n);
   double a2 = gamma - 1.0, a3 = gamma - 2.0;
   double uu = (dxidx * mu0 + dxidy * mv0 + dxidz * mw0) / rho;
   double phi = 0.5 * a2 * (p2(mu0) + p2(mv0) + p2(mw0)) / p2(rho);
   double a1 = gamma * e0 / rho - phi;
-  double A[25];  // row-major A[r*5+c] = a(r+1,c+1)
   A[0] = 0.0; A[1] = dxidx; A[2] = dxidy; A[3] = dxidz; A[4] = 0.0;
   A[5] = phi * dxidx - uu * mu0 / rho;
   A[6] = uu - a3 * dxidx * mu0 / rho;
@@ -89,120 +82,179 @@ __device__ __forceinline__ void lusgs_matvec(const BlockView& B, long nb, int cb
   A[22] = a1 * dxidy - a2 * uu * mv0 / rho;
   A[23] = a1 * dxidz - a2 * uu * mw0 / rho;
   A[24] = gamma * uu;
-#pragma unroll
-  for (int d = 0; d < 5; ++d) A[d * 6] = plus ? A[d * 6] + rad : A[d * 6] - rad;
-#pragma unroll
-  for (int x = 0; x < 25; ++x) A[x] = 0.5 * A[x] * invj;
-#pragma unroll
-  for (int r = 0; r < 5; ++r) {
-    double s = A[r * 5 + 0] * dqn[0];
-    s = s + A[r * 5 + 1] * dqn[1];
-    s = s + A[r * 5 + 2] * dqn[2];
-    s = s + A[r * 5 + 3] * dqn[3];
-    s = s + A[r * 5 + 4] * dqn[4];
-    out[r] = s;
-  }
 }
 
-// Node `t` of hyperplane h (offsets a+b+c = h inside an nx1 x ny1 x nz1 box);
-// returns false when t is past the plane's node count.
-__device__ __forceinline__ bool plane_node(int h, long t, int nx1, int ny1, int nz1, int& a, int& b,
-                                           int& c) {
+// Position of updated-box offsets (a,b,c) in the hyperplane-major order:
+// planes h = a+b+c one after another; inside a plane, c ascending, then b.
+__device__ __forceinline__ long plane_pos(const BlockView& B, int a, int b, int c) {
+  int nx1 = B.b1.nx(), ny1 = B.b1.ny();
+  int h = a + b + c;
+  long pos = B.poff[h];
   int cmin = max(0, h - (nx1 - 1) - (ny1 - 1));
-  int cmax = min(nz1 - 1, h);
-  for (c = cmin; c <= cmax; ++c) {
-    int r = h - c;
-    int bmin = max(0, r - (nx1 - 1));
-    int bmax = min(ny1 - 1, r);
-    long cnt = bmax - bmin + 1;
-    if (cnt <= 0) continue;
-    if (t < cnt) {
-      b = bmin + (int)t;
-      a = r - b;
-      return true;
-    }
-    t -= cnt;
+  for (int cc = cmin; cc < c; ++cc) {
+    int r = h - cc;
+    int bmin = max(0, r - (nx1 - 1)), bmax = min(ny1 - 1, r);
+    if (bmax >= bmin) pos += bmax - bmin + 1;
   }
-  return false;
+  int bmin = max(0, (h - c) - (nx1 - 1));
+  return pos + (b - bmin);
 }
 
-// Forward and backward sweeps and the update q += dq for one block per CTA
-// (sub_timeadvancement_1stimplicit.f90:279-368, :455-545, :568-574).
+// The off-diagonal blocks of both sweeps, off the critical path.  For every
+// updated node (the provider) and direction d: A = calc_jm at the provider,
+// S+ = 0.5*(A + r*I)*inv_j goes to the forward record of the node one step up
+// in d, S- = 0.5*(A - r*I)*inv_j to the backward record of the node one step
+// down (sub_timeadvancement_1stimplicit.f90:283-301, :459-477, same
+// operations).  Each node also stores rhs, diag, inv_j and the positions of
+// its six neighbours in the hyperplane-major order.
+__global__ void k_lusgs_mats(const BlockView* __restrict__ blocks, CaseConsts cc) {
+  const BlockView& B = blocks[blockIdx.y];
+  const Box& b1 = B.b1;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long N1 = b1.size();
+  if (t >= 3 * N1) return;
+  int d = (int)(t % 3);
+  long u = t / 3;
+  int nx1 = b1.nx(), ny1 = b1.ny(), nz1 = b1.nz();
+  int a = (int)(u % nx1);
+  long r = u / nx1;
+  int b = (int)(r % ny1);
+  int c = (int)(r / ny1);
+  long n = B.at(b1.is + a, b1.js + b, b1.ks + c);
+  int off[3] = {a, b, c};
+  const int lim[3] = {nx1, ny1, nz1};
+  long pos = plane_pos(B, a, b, c);
+  if (d == 0) {
+    double* sc = B.sca + 8 * pos;
+#pragma unroll
+    for (int x = 0; x < 5; ++x) sc[x] = B.v(F_RHS, x + 1, n);
+    sc[5] = B.s(F_DIAG, n);
+    sc[6] = B.s(F_INVJ, n);
+    sc[7] = 0.0;
+    B.nat[pos] = n;
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+      int lo[3] = {a, b, c}, hi[3] = {a, b, c};
+      lo[e] -= 1;
+      hi[e] += 1;
+      B.nbr[6 * pos + e] = off[e] > 0 ? (int)plane_pos(B, lo[0], lo[1], lo[2]) : -1;
+      B.nbr[6 * pos + 3 + e] = off[e] < lim[e] - 1 ? (int)plane_pos(B, hi[0], hi[1], hi[2]) : -1;
+    }
+  }
+  bool up = off[d] < lim[d] - 1;    // a forward consumer exists
+  bool down = off[d] > 0;           // a backward consumer exists
+  if (!up && !down) return;
+  double A[25];
+  calc_jm(B, n, 3 * d + 1, cc.gamma, A);
+  const int radf[3] = {F_RA, F_RB, F_RC};
+  double rad = B.s(radf[d], n);
+  double invj = B.s(F_INVJ, n);
+  if (up) {
+    int q[3] = {a, b, c};
+    q[d] += 1;
+    double* dst = B.rec_f + 75 * plane_pos(B, q[0], q[1], q[2]) + 25 * d;
+#pragma unroll
+    for (int x = 0; x < 25; ++x) {
+      double v = (x % 6 == 0) ? A[x] + rad : A[x];
+      dst[x] = 0.5 * v * invj;
+    }
+  }
+  if (down) {
+    int q[3] = {a, b, c};
+    q[d] -= 1;
+    double* dst = B.rec_b + 75 * plane_pos(B, q[0], q[1], q[2]) + 25 * d;
+#pragma unroll
+    for (int x = 0; x < 25; ++x) {
+      double v = (x % 6 == 0) ? A[x] - rad : A[x];
+      dst[x] = 0.5 * v * invj;
+    }
+  }
+}
+
+// Forward and backward hyperplane sweeps for one block per CTA.  Thread t of a
+// plane handles equation row t%5 of node t/5 of that plane: the row of the
+// three neighbour blocks times the neighbours' dq, summed in the reference's
+// order (:346-364, :522-540).  The previous plane's results sit in shared
+// memory; q += dq is applied as soon as dq is known (the blocks were built
+// from the old q before the sweep, so nothing reads q afterwards).
 __global__ void k_lusgs_sweep(const BlockView* __restrict__ blocks, CaseConsts cc) {
   const BlockView& B = blocks[blockIdx.x];
-  const Box& b1 = B.b1;
-  int nx1 = b1.nx(), ny1 = b1.ny(), nz1 = b1.nz();
-  int H = nx1 + ny1 + nz1 - 2;
-  const long st[3] = {1, (long)B.nx, (long)B.nx * B.ny};
-  double gamma = cc.gamma;
+  extern __shared__ double sdq[];  // two planes of 5*pmax values
+  const int P = B.pmax;
+  const int H = B.nplanes;
   // forward
   for (int h = 0; h < H; ++h) {
-    for (long t = threadIdx.x;; t += blockDim.x) {
-      int a, b, c;
-      if (!plane_node(h, t, nx1, ny1, nz1, a, b, c)) break;
-      long n = B.at(b1.is + a, b1.js + b, b1.ks + c);
-      double acc[3][5];
-      const int off[3] = {a, b, c};
-      const int radf[3] = {F_RA, F_RB, F_RC};
+    long base = B.poff[h];
+    int cnt = (int)(B.poff[h + 1] - base);
+    long pbase = h > 0 ? B.poff[h - 1] : 0;
+    double* prev = sdq + 5 * P * ((h + 1) & 1);
+    double* cur = sdq + 5 * P * (h & 1);
+    for (int t = threadIdx.x; t < 5 * cnt; t += blockDim.x) {
+      int node = t / 5, row = t - 5 * (t / 5);
+      long pos = base + node;
+      const double* rec = B.rec_f + 75 * pos + 5 * row;
+      const int* nb = B.nbr + 6 * pos;
+      double acc[3];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        if (off[d] == 0) {
-#pragma unroll
-          for (int x = 0; x < 5; ++x) acc[d][x] = 0.0;
+        int p = nb[d];
+        if (p < 0) {
+          acc[d] = 0.0;
         } else {
-          long nb = n - st[d];
-          double dqn[5];
-#pragma unroll
-          for (int x = 0; x < 5; ++x) dqn[x] = B.v(F_DQS, x + 1, nb);
-          lusgs_matvec(B, nb, 3 * d + 1, radf[d], true, gamma, dqn, acc[d]);
+          const double* m = rec + 25 * d;
+          const double* x = prev + 5 * (p - pbase);
+          double s = m[0] * x[0];
+          s = s + m[1] * x[1];
+          s = s + m[2] * x[2];
+          s = s + m[3] * x[3];
+          s = s + m[4] * x[4];
+          acc[d] = s;
         }
       }
-      double diag = B.s(F_DIAG, n), invj = B.s(F_INVJ, n);
-#pragma unroll
-      for (int x = 0; x < 5; ++x)
-        B.v(F_DQS, x + 1, n) = (B.v(F_RHS, x + 1, n) + (acc[0][x] + acc[1][x] + acc[2][x])) / diag / invj;
+      const double* sc = B.sca + 8 * pos;
+      double v = (sc[row] + (acc[0] + acc[1] + acc[2])) / sc[5] / sc[6];
+      cur[t] = v;
+      B.dqs[5 * pos + row] = v;
     }
     __syncthreads();
   }
   // backward
   for (int h = H - 1; h >= 0; --h) {
-    for (long t = threadIdx.x;; t += blockDim.x) {
-      int a, b, c;
-      if (!plane_node(h, t, nx1, ny1, nz1, a, b, c)) break;
-      long n = B.at(b1.is + a, b1.js + b, b1.ks + c);
-      double acc[3][5];
-      const int off[3] = {nx1 - 1 - a, ny1 - 1 - b, nz1 - 1 - c};
-      const int radf[3] = {F_RA, F_RB, F_RC};
+    long base = B.poff[h];
+    int cnt = (int)(B.poff[h + 1] - base);
+    long pbase = h + 1 < H ? B.poff[h + 1] : 0;
+    double* prev = sdq + 5 * P * ((h + 1) & 1);
+    double* cur = sdq + 5 * P * (h & 1);
+    for (int t = threadIdx.x; t < 5 * cnt; t += blockDim.x) {
+      int node = t / 5, row = t - 5 * (t / 5);
+      long pos = base + node;
+      const double* rec = B.rec_b + 75 * pos + 5 * row;
+      const int* nb = B.nbr + 6 * pos + 3;
+      double acc[3];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        if (off[d] == 0) {
-#pragma unroll
-          for (int x = 0; x < 5; ++x) acc[d][x] = 0.0;
+        int p = nb[d];
+        if (p < 0) {
+          acc[d] = 0.0;
         } else {
-          long nb = n + st[d];
-          double dqn[5];
-#pragma unroll
-          for (int x = 0; x < 5; ++x) dqn[x] = B.v(F_DQ, x + 1, nb);
-          lusgs_matvec(B, nb, 3 * d + 1, radf[d], false, gamma, dqn, acc[d]);
+          const double* m = rec + 25 * d;
+          const double* x = prev + 5 * (p - pbase);
+          double s = m[0] * x[0];
+          s = s + m[1] * x[1];
+          s = s + m[2] * x[2];
+          s = s + m[3] * x[3];
+          s = s + m[4] * x[4];
+          acc[d] = s;
         }
       }
-      double diag = B.s(F_DIAG, n), invj = B.s(F_INVJ, n);
-#pragma unroll
-      for (int x = 0; x < 5; ++x)
-        B.v(F_DQ, x + 1, n) = B.v(F_DQS, x + 1, n) - (acc[0][x] + acc[1][x] + acc[2][x]) / invj / diag;
+      const double* sc = B.sca + 8 * pos;
+      double v = B.dqs[5 * pos + row] - (acc[0] + acc[1] + acc[2]) / sc[6] / sc[5];
+      cur[t] = v;
+      B.dq[5 * pos + row] = v;
+      long n = B.nat[pos];
+      B.v(F_Q, row + 1, n) = B.v(F_Q, row + 1, n) + v;
     }
     __syncthreads();
-  }
-  // q = q + dq on the updated box
-  long N1 = b1.size();
-  for (long t = threadIdx.x; t < N1; t += blockDim.x) {
-    int i = b1.is + (int)(t % nx1);
-    long r = t / nx1;
-    int j = b1.js + (int)(r % ny1);
-    int k = b1.ks + (int)(r / ny1);
-    long n = B.at(i, j, k);
-#pragma unroll
-    for (int x = 1; x <= 5; ++x) B.v(F_Q, x, n) = B.v(F_Q, x, n) + B.v(F_DQ, x, n);
   }
 }
 

@@ -41,6 +41,7 @@ __global__ void k_find_dt(const BlockView* __restrict__ blocks, CaseConsts cc, d
 __global__ void k_dt_minmax(const BlockView* __restrict__ blocks, int m, const double* cta_max,
                             int ncta, int cta_size, double* out2);
 __global__ void k_lusgs_prep(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_lusgs_mats(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_lusgs_sweep(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_physical_bc(const BlockView* __restrict__ blocks, const BcOp* __restrict__ ops,
                               const int* __restrict__ op_start, CaseConsts cc);

@@ -32,7 +32,28 @@ struct HostBlock {
   bool pinned[kNumPublicFields] = {};
   long plane = 0;
   size_t arena_off = 0;  // doubles
+  void* ws = nullptr;    // LU-SGS workspace (one allocation)
 };
+
+// Hyperplane offsets of an nx1 x ny1 x nz1 updated box (planes h = a+b+c).
+std::vector<long> plane_offsets(const Box& b1, int& pmax) {
+  int nx1 = b1.nx(), ny1 = b1.ny(), nz1 = b1.nz();
+  int H = nx1 + ny1 + nz1 - 2;
+  std::vector<long> off(H + 1, 0);
+  pmax = 0;
+  for (int h = 0; h < H; ++h) {
+    long n = 0;
+    for (int c = 0; c < nz1; ++c) {
+      int r = h - c;
+      if (r < 0) break;
+      int bmin = std::max(0, r - (nx1 - 1)), bmax = std::min(ny1 - 1, r);
+      if (bmax >= bmin) n += bmax - bmin + 1;
+    }
+    off[h + 1] = off[h] + n;
+    pmax = std::max<long>(pmax, n);
+  }
+  return off;
+}
 
 struct State {
   bool inited = false;
@@ -71,6 +92,9 @@ struct State {
   double* t_arena = nullptr;
   size_t t_doubles = 0;
   BlockView* d_tview = nullptr;
+  void* t_ws = nullptr;
+  size_t t_ws_bytes = 0;
+  int pmax_all = 0;
   double* d_tmax = nullptr;
   size_t t_tmax = 0;
   std::string err;
@@ -83,12 +107,12 @@ State g;
 // count of every kernel this library launches (aero_launch_count).
 enum ProfId {
   P_GETPRI, P_FILL, P_INVISCID, P_VISC_A, P_VISC_B, P_FIND_DT, P_DT_MINMAX, P_LUSGS_PREP,
-  P_LUSGS_SWEEP, P_BC, P_SA_CLIP, P_HALO, P_AVG_GATHER, P_AVG_APPLY, P_RESID_PART, P_RESID_FINAL,
+  P_LUSGS_MATS, P_LUSGS_SWEEP, P_BC, P_SA_CLIP, P_HALO, P_AVG_GATHER, P_AVG_APPLY, P_RESID_PART, P_RESID_FINAL,
   P_TRANSFER, P_GEOMETRY, P_NUM
 };
 const char* kProfName[P_NUM] = {
     "k_getpri", "k_fill", "k_inviscid", "k_viscous_a", "k_viscous_b", "k_find_dt", "k_dt_minmax",
-    "k_lusgs_prep", "k_lusgs_sweep", "k_physical_bc", "k_sa_clip", "k_halo", "k_avg_gather",
+    "k_lusgs_prep", "k_lusgs_mats", "k_lusgs_sweep", "k_physical_bc", "k_sa_clip", "k_halo", "k_avg_gather",
     "k_avg_apply", "k_residual_partial", "k_residual_final", "k_transfer", "k_geometry"};
 struct Prof {
   bool on = false;
@@ -201,6 +225,30 @@ void fill_view(BlockView& v, const Box& b, const Box& b0, const Box& b1, long pl
   }
 }
 
+// LU-SGS workspace of one view (see BlockView): one device allocation holding
+// poff, rec_f, rec_b, sca, dqs, dq, nat, nbr.
+size_t workspace_bytes(const Box& b1, int H) {
+  size_t N1 = (size_t)b1.size();
+  return (size_t)(H + 1) * sizeof(long) + N1 * (75 + 75 + 8 + 5 + 5) * sizeof(double) + N1 * sizeof(long) +
+         N1 * 6 * sizeof(int) + 256;
+}
+int attach_workspace(BlockView& v, void* ws, const std::vector<long>& poff, int pmax) {
+  size_t N1 = (size_t)v.b1.size();
+  char* p = (char*)ws;
+  v.nplanes = (int)poff.size() - 1;
+  v.pmax = pmax;
+  v.rec_f = (double*)p; p += N1 * 75 * sizeof(double);
+  v.rec_b = (double*)p; p += N1 * 75 * sizeof(double);
+  v.sca = (double*)p; p += N1 * 8 * sizeof(double);
+  v.dqs = (double*)p; p += N1 * 5 * sizeof(double);
+  v.dq = (double*)p; p += N1 * 5 * sizeof(double);
+  v.nat = (long*)p; p += N1 * sizeof(long);
+  v.poff = (long*)p; p += poff.size() * sizeof(long);
+  v.nbr = (int*)p;
+  CK(cudaMemcpyAsync(v.poff, poff.data(), poff.size() * sizeof(long), cudaMemcpyHostToDevice, g.stream));
+  return AERO_OK;
+}
+
 int ensure_staging(size_t doubles) {
   if (doubles <= g.staging_doubles) return AERO_OK;
   if (g.d_staging) CK(cudaFree(g.d_staging));
@@ -281,6 +329,19 @@ int resolve(const Box& b, const Box& b0, const Box& b1, const std::vector<Arg>& 
   if (!g.d_tview) CK(cudaMalloc(&g.d_tview, sizeof(BlockView)));
   CK(cudaMemsetAsync(g.t_arena, 0, need * sizeof(double), g.stream));
   fill_view(t.view, b, b0, b1, plane, g.t_arena);
+  if (b1.nx() > 0 && b1.ny() > 0 && b1.nz() > 0) {
+    int pmax = 0;
+    std::vector<long> poff = plane_offsets(b1, pmax);
+    size_t wsb = workspace_bytes(b1, (int)poff.size() - 1);
+    if (wsb > g.t_ws_bytes) {
+      if (g.t_ws) CK(cudaFree(g.t_ws));
+      g.t_ws = nullptr;
+      CK(cudaMalloc(&g.t_ws, wsb));
+      g.t_ws_bytes = wsb;
+    }
+    int rc2 = attach_workspace(t.view, g.t_ws, poff, pmax);
+    if (rc2) return rc2;
+  }
   CK(cudaMemcpyAsync(g.d_tview, &t.view, sizeof(BlockView), cudaMemcpyHostToDevice, g.stream));
   t.d_view = g.d_tview;
   t.resident = false;
@@ -357,10 +418,19 @@ int launch_dt_minmax(const BlockView* views, int m, double* d_out2) {
   CKL();
   return AERO_OK;
 }
-int launch_implicit(const BlockView* views, int nblk, long maxExt, const CaseConsts& cc) {
+int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, int pmax, const CaseConsts& cc) {
   PROF(P_LUSGS_PREP, (k_lusgs_prep<<<dim3(cdiv(maxExt, 256), nblk), 256, 0, g.stream>>>(views, cc)));
   CKL();
-  PROF(P_LUSGS_SWEEP, (k_lusgs_sweep<<<nblk, 256, 0, g.stream>>>(views, cc)));
+  PROF(P_LUSGS_MATS, (k_lusgs_mats<<<dim3(cdiv(3 * maxN1, 128), nblk), 128, 0, g.stream>>>(views, cc)));
+  CKL();
+  size_t smem = (size_t)2 * 5 * std::max(pmax, 1) * sizeof(double);
+  static size_t smem_set = 0;
+  if (smem > 48 * 1024 && smem > smem_set) {
+    CK(cudaFuncSetAttribute(k_lusgs_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    smem_set = smem;
+  }
+  int threads = (int)std::min<long>(1024, std::max<long>(64, (5L * pmax + 31) / 32 * 32));
+  PROF(P_LUSGS_SWEEP, (k_lusgs_sweep<<<nblk, threads, smem, g.stream>>>(views, cc)));
   CKL();
   return AERO_OK;
 }
@@ -425,7 +495,7 @@ int do_iteration(bool want_dt_minmax) {
   if (viscous_on() && (rc = launch_viscous(g.d_blocks, nb, g.max_b0, g.cc, 0))) return rc;
   if ((rc = launch_find_dt(g.d_blocks, nb, g.max_box, g.cc))) return rc;
   if (want_dt_minmax && (rc = launch_dt_minmax(g.d_blocks, nb - 1, g.d_out + 7))) return rc;
-  if ((rc = launch_implicit(g.d_blocks, nb, g.max_ext, g.cc))) return rc;
+  if ((rc = launch_implicit(g.d_blocks, nb, g.max_ext, g.max_b1, g.pmax_all, g.cc))) return rc;
   if ((rc = do_physical_bc())) return rc;
   if ((rc = do_halo())) return rc;
   if ((rc = do_average1())) return rc;
@@ -454,9 +524,12 @@ int aero_init(int device) {
 }
 
 static void release_case() {
-  for (auto& H : g.blocks)
+  for (auto& H : g.blocks) {
     for (int f = 0; f < kNumPublicFields; ++f)
       if (H.pinned[f]) cudaHostUnregister(H.host[f]);
+    if (H.ws) cudaFree(H.ws);
+    H.ws = nullptr;
+  }
   g.blocks.clear();
   g.registry.clear();
   cudaFree(g.arena); g.arena = nullptr;
@@ -479,6 +552,7 @@ int aero_finalize(void) {
   cudaFree(g.d_staging); g.d_staging = nullptr; g.staging_doubles = 0;
   cudaFree(g.t_arena); g.t_arena = nullptr; g.t_doubles = 0;
   cudaFree(g.d_tview); g.d_tview = nullptr;
+  cudaFree(g.t_ws); g.t_ws = nullptr; g.t_ws_bytes = 0;
   cudaFree(g.d_status); g.d_status = nullptr;
   cudaFree(g.d_out); g.d_out = nullptr;
   cudaFreeHost(g.h_out); g.h_out = nullptr;
@@ -614,9 +688,15 @@ int aero_finish_setup(void) {
   CK(cudaMemsetAsync(g.arena, 0, total * sizeof(double), g.stream));
   g.arena_doubles = total;
   g.views.resize(nb);
+  g.pmax_all = 0;
   for (int m = 0; m < nb; ++m) {
     HostBlock& H = g.blocks[m];
     fill_view(g.views[m], H.b, H.b0, H.b1, H.plane, g.arena + H.arena_off);
+    int pmax = 0;
+    std::vector<long> poff = plane_offsets(H.b1, pmax);
+    CK(cudaMalloc(&H.ws, workspace_bytes(H.b1, (int)poff.size() - 1)));
+    if ((rc = attach_workspace(g.views[m], H.ws, poff, pmax))) return rc;
+    g.pmax_all = std::max(g.pmax_all, pmax);
   }
   CK(cudaMalloc(&g.d_blocks, nb * sizeof(BlockView)));
   CK(cudaMemcpyAsync(g.d_blocks, g.views.data(), nb * sizeof(BlockView), cudaMemcpyHostToDevice, g.stream));
@@ -767,7 +847,7 @@ int aero_implicit1st(double* q, const double* dt, const double* pri_v, double* r
   CaseConsts cc = consts_with(*gamma, g.cc.cv, g.cc.re);
   cc.cfl = *cfl;
   Box e{b1.is - 1, b1.ie + 1, b1.js - 1, b1.je + 1, b1.ks - 1, b1.ke + 1};
-  if ((rc = launch_implicit(t.d_view, 1, e.size(), cc))) return rc;
+  if ((rc = launch_implicit(t.d_view, 1, e.size(), b1.size(), t.view.pmax, cc))) return rc;
   return finish(t, args);
 }
 

@@ -63,9 +63,9 @@ def bump_channel(ni: int = 97, nj: int = 49, nk: int = 5, h: float = 0.10, lengt
 
 
 def naca4_surface(x: np.ndarray, t: float, m: float = 0.0, p: float = 0.4):
-    """Upper and lower surface of a NACA 4-digit section (closed trailing edge,
-    -0.1036 x^4 coefficient), chord 1."""
-    yt = 5.0 * t * (0.2969 * np.sqrt(x) - 0.1260 * x - 0.3516 * x ** 2 + 0.2843 * x ** 3 - 0.1036 * x ** 4)
+    """Upper and lower surface of a NACA 4-digit section (standard thickness
+    law, open trailing edge of thickness 0.0021*t/0.01... at x = 1), chord 1."""
+    yt = 5.0 * t * (0.2969 * np.sqrt(x) - 0.1260 * x - 0.3516 * x ** 2 + 0.2843 * x ** 3 - 0.1015 * x ** 4)
     if m > 0.0:
         yc = np.where(x < p, m / p ** 2 * (2 * p * x - x ** 2), m / (1 - p) ** 2 * ((1 - 2 * p) + 2 * p * x - x ** 2))
         dyc = np.where(x < p, 2 * m / p ** 2 * (p - x), 2 * m / (1 - p) ** 2 * (p - x))
@@ -75,6 +75,32 @@ def naca4_surface(x: np.ndarray, t: float, m: float = 0.0, p: float = 0.4):
     else:
         xu, yu, xl, yl = x, yt, x, -yt
     return xu, yu, xl, yl
+
+
+def naca4_loop(n: int, t: float, m: float = 0.0, p: float = 0.4, n_cap: int = 8):
+    """Closed surface loop of n intervals, clockwise from the trailing-edge tip:
+    a semicircular cap of n_cap intervals closes the blunt trailing edge (its
+    lower half first), then the lower surface to the leading edge and the upper
+    surface back.  x is clustered toward the leading edge and mildly toward the
+    trailing edge."""
+    half = (n - n_cap) // 2
+    tt = np.linspace(0.0, 1.0, half + 1)
+    xs = 0.5 * (0.5 * (1.0 - np.cos(np.pi * tt))) + 0.5 * (1.0 - np.cos(0.5 * np.pi * tt))  # 0 -> 1
+    xu, yu, xl, yl = naca4_surface(xs, t, m, p)
+    # trailing-edge cap: centre midway between the TE corners, radius half the gap
+    cx, cy = 0.5 * (xu[-1] + xl[-1]), 0.5 * (yu[-1] + yl[-1])
+    r = 0.5 * np.hypot(xu[-1] - xl[-1], yu[-1] - yl[-1])
+    ang0 = np.arctan2(yl[-1] - cy, xl[-1] - cx)     # lower corner (about -pi/2)
+    k = n_cap // 2
+    a_low = np.linspace(0.0, ang0, k + 1)           # tip (0) -> lower corner
+    a_up = np.linspace(-ang0, 0.0, n_cap - k + 1)    # upper corner -> tip
+    cap_lo_x, cap_lo_y = cx + r * np.cos(a_low), cy + r * np.sin(a_low)
+    cap_up_x, cap_up_y = cx + r * np.cos(a_up), cy + r * np.sin(a_up)
+    lx, ly = xl[::-1], yl[::-1]                     # TE -> LE along the lower surface
+    X = np.concatenate([cap_lo_x, lx[1:], xu[1:], cap_up_x[1:]])
+    Y = np.concatenate([cap_lo_y, ly[1:], yu[1:], cap_up_y[1:]])
+    assert len(X) == n + 1, (len(X), n)
+    return X, Y
 
 
 def radial_distribution(nj: int, first: float, ratio: float, outer: float = 1.0,
@@ -105,24 +131,18 @@ def naca_ogrid(nblk: int = 4, ni: int = 129, nj: int = 65, nk: int = 3, t: float
                m: float = 0.0, p: float = 0.4, first: float = 1.0e-4, ratio: float = 1.08,
                outer: float = 20.0, dz: float = 0.1, cfg: Optional[Config] = None,
                name: str = "naca_ogrid") -> Case:
-    """O-grid around a NACA 4-digit section.  i runs clockwise around the
-    airfoil starting at the trailing edge (lower surface first), j outward, k
+    """O-grid around a NACA 4-digit section (blunt trailing edge closed by a
+    small semicircular cap).  i runs clockwise around the airfoil starting at
+    the trailing-edge tip (lower surface first), j outward, k
     spanwise.  Block b covers i-intervals [b*(ni-1), (b+1)*(ni-1)] of the loop;
     neighbouring blocks share their i interface plane (overlap nodes) and are
     connected face 2 -> face 1 with orientation code 2 (the reference's
     transposed (l,m) convention between an i+ and an i- face)."""
-    cfg = cfg or Config(solver=IFLAG_NSSOLVER, ma=0.5, re=5000.0, aoa_deg=2.0, cfl=5.0)
+    cfg = cfg or Config(solver=IFLAG_NSSOLVER, ma=0.5, re=5000.0, aoa_deg=2.0, cfl=2.0)
     ntot = nblk * (ni - 1)               # intervals around the loop
-    # loop parameter: 0 -> TE, along the lower surface to LE, back along upper
-    s = np.arange(ntot + 1) / ntot
-    theta = 2.0 * math.pi * s
-    # x from cosine clustering, lower half first
-    xs = 0.5 * (1.0 + np.cos(theta))     # 1 -> 0 -> 1
-    xu, yu, xl, yl = naca4_surface(np.clip(xs, 0.0, 1.0), t, m, p)
-    lower = theta <= math.pi
-    sx = np.where(lower, xl, xu)
-    sy = np.where(lower, yl, yu)
-    # outer circle, clockwise from angle 0
+    sx, sy = naca4_loop(ntot, t, m, p)
+    # outer circle, clockwise from angle 0, at the same loop fraction
+    theta = 2.0 * math.pi * np.arange(ntot + 1) / ntot
     cx, cy = 0.5, 0.0
     ox = cx + outer * np.cos(-theta)
     oy = cy + outer * np.sin(-theta)

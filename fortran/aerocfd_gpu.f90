@@ -1,0 +1,186 @@
+!! ISO_C_BINDING interface to libaerocfd_gpu.so (include/aerocfd_gpu.h).
+!!
+!! Every hot-path routine of aerocfd keeps its argument list; the interfaces
+!! below bind the same arguments (all by reference, explicit-shape arrays) to
+!! the C entry points.  A call site such as main.f90:359
+!!
+!!   call inviscid_flux_1(blk(m0)%rhsi, blk(m0)%q, blk(m0)%dxidx, blk(m0)%inv_j, &
+!!                        is,ie,js,je,ks,ke, is0,ie0,js0,je0,ks0,ke0, is1,ie1,js1,je1,ks1,ke1, gamma)
+!!
+!! becomes
+!!
+!!   ierr = aero_inviscid_flux_1(blk(m0)%rhsi, blk(m0)%q, blk(m0)%dxidx, blk(m0)%inv_j, &
+!!                        is,ie,js,je,ks,ke, is0,ie0,js0,je0,ks0,ke0, is1,ie1,js1,je1,ks1,ke1, gamma)
+!!   call aero_check(ierr)
+!!
+!! This file is source only: the image it was written in has no Fortran
+!! compiler.
+module aerocfd_gpu
+  use iso_c_binding
+  implicit none
+
+  integer(c_int), parameter :: AERO_OK = 0
+  integer(c_int), parameter :: AERO_F_Q = 0, AERO_F_PRI_V = 1, AERO_F_RHSI = 2, AERO_F_RHSV = 3, &
+                               AERO_F_RHS = 4, AERO_F_DT = 5, AERO_F_DXIDX = 6, AERO_F_INV_J = 7, &
+                               AERO_F_AMU = 8, AERO_F_NUT = 9, AERO_F_SA_RHS = 10, AERO_F_X = 11, &
+                               AERO_F_Y = 12, AERO_F_Z = 13, AERO_F_DIST = 14, AERO_F_ALPHA = 15, &
+                               AERO_F_BETA = 16, AERO_F_GGAMMA = 17, AERO_F_DUDX = 18, AERO_F_TAO = 19, &
+                               AERO_F_VOR = 20, AERO_F_LENGTH = 21, AERO_F_SPACING = 22
+
+  interface
+    integer(c_int) function aero_init(device) bind(C, name="aero_init")
+      import :: c_int
+      integer(c_int), value :: device
+    end function
+
+    integer(c_int) function aero_finalize() bind(C, name="aero_finalize")
+      import :: c_int
+    end function
+
+    integer(c_int) function aero_configure(iflags, params) bind(C, name="aero_configure")
+      import :: c_int, c_double
+      integer(c_int) :: iflags(8)
+      real(c_double) :: params(7)
+    end function
+
+    integer(c_int) function aero_register_block(m, box18, num_subface, subfaces) &
+        bind(C, name="aero_register_block")
+      import :: c_int
+      integer(c_int), value :: m, num_subface
+      integer(c_int) :: box18(18), subfaces(11, *)
+    end function
+
+    integer(c_int) function aero_bind_field(m, field, host) bind(C, name="aero_bind_field")
+      import :: c_int, c_ptr
+      integer(c_int), value :: m, field
+      type(c_ptr), value :: host
+    end function
+
+    integer(c_int) function aero_finish_setup() bind(C, name="aero_finish_setup")
+      import :: c_int
+    end function
+
+    integer(c_int) function aero_sync_to_device(mask) bind(C, name="aero_sync_to_device")
+      import :: c_long_long
+      integer(c_long_long), value :: mask
+    end function
+
+    integer(c_int) function aero_sync_to_host(mask) bind(C, name="aero_sync_to_host")
+      import :: c_long_long
+      integer(c_long_long), value :: mask
+    end function
+
+    ! sub_getpri_v.f90:19
+    integer(c_int) function aero_get_primitivevariables(mm, pri_v, q, gamma, cv, is, ie, js, je, ks, ke) &
+        bind(C, name="aero_get_primitivevariables")
+      import :: c_int, c_double
+      integer(c_int) :: mm, is, ie, js, je, ks, ke
+      real(c_double) :: pri_v(7, is:ie, js:je, ks:ke), q(5, is:ie, js:je, ks:ke), gamma, cv
+    end function
+
+    ! sub_inviscid1.f90:8
+    integer(c_int) function aero_inviscid_flux_1(rhsi, q, dxidx, inv_j, is, ie, js, je, ks, ke, &
+        is0, ie0, js0, je0, ks0, ke0, is1, ie1, js1, je1, ks1, ke1, gamma) bind(C, name="aero_inviscid_flux_1")
+      import :: c_int, c_double
+      integer(c_int) :: is, ie, js, je, ks, ke, is0, ie0, js0, je0, ks0, ke0, is1, ie1, js1, je1, ks1, ke1
+      real(c_double) :: rhsi(5, is:ie, js:je, ks:ke), q(5, is:ie, js:je, ks:ke)
+      real(c_double) :: dxidx(9, is:ie, js:je, ks:ke), inv_j(is:ie, js:je, ks:ke), gamma
+    end function
+
+    ! sub_viscous.f90:9
+    integer(c_int) function aero_viscous_flux(rhsv, pri_v, amu, vor, dudx, tao, dxidx, inv_j, tinf, prl, prt, &
+        gamma, cv, re, is, ie, js, je, ks, ke, is0, ie0, js0, je0, ks0, ke0, is1, ie1, js1, je1, ks1, ke1, mm) &
+        bind(C, name="aero_viscous_flux")
+      import :: c_int, c_double
+      integer(c_int) :: is, ie, js, je, ks, ke, is0, ie0, js0, je0, ks0, ke0, is1, ie1, js1, je1, ks1, ke1, mm
+      real(c_double) :: rhsv(5, is:ie, js:je, ks:ke), pri_v(7, is:ie, js:je, ks:ke), amu(3, is:ie, js:je, ks:ke)
+      real(c_double) :: vor(is:ie, js:je, ks:ke), dudx(9, is:ie, js:je, ks:ke), tao(6, is:ie, js:je, ks:ke)
+      real(c_double) :: dxidx(9, is:ie, js:je, ks:ke), inv_j(is:ie, js:je, ks:ke)
+      real(c_double) :: tinf, prl, prt, gamma, cv, re
+    end function
+
+    ! sub_timeadvancement_finddt.f90:24
+    integer(c_int) function aero_find_dt(dt, dtmax, dtmin, cflmax, cflmin, pri_v, amu, dxidx, re, cfl, &
+        is, ie, js, je, ks, ke, iflag_time, iflag_steady, iflag_unsteady) bind(C, name="aero_find_dt")
+      import :: c_int, c_double
+      integer(c_int) :: is, ie, js, je, ks, ke, iflag_time, iflag_steady, iflag_unsteady
+      real(c_double) :: dt(is:ie, js:je, ks:ke), dtmax, dtmin, cflmax, cflmin, re, cfl
+      real(c_double) :: pri_v(7, is:ie, js:je, ks:ke), amu(3, is:ie, js:je, ks:ke), dxidx(9, is:ie, js:je, ks:ke)
+    end function
+
+    ! sub_timeadvancement_1stimplicit.f90:7
+    integer(c_int) function aero_implicit1st(q, dt, pri_v, rhs, rhsi, rhsv, dxidx, inv_j, &
+        is, ie, js, je, ks, ke, is0, ie0, js0, je0, ks0, ke0, is1, ie1, js1, je1, ks1, ke1, &
+        gamma, cfl, xx, yy, zz) bind(C, name="aero_implicit1st")
+      import :: c_int, c_double
+      integer(c_int) :: is, ie, js, je, ks, ke, is0, ie0, js0, je0, ks0, ke0, is1, ie1, js1, je1, ks1, ke1
+      real(c_double) :: q(5, is:ie, js:je, ks:ke), dt(is:ie, js:je, ks:ke), pri_v(7, is:ie, js:je, ks:ke)
+      real(c_double) :: rhs(5, is:ie, js:je, ks:ke), rhsi(5, is:ie, js:je, ks:ke), rhsv(5, is:ie, js:je, ks:ke)
+      real(c_double) :: dxidx(9, is:ie, js:je, ks:ke), inv_j(is:ie, js:je, ks:ke), gamma, cfl
+      real(c_double) :: xx(is:ie, js:je, ks:ke), yy(is:ie, js:je, ks:ke), zz(is:ie, js:je, ks:ke)
+    end function
+
+    ! sub_init_gridtransformation.f90:27
+    integer(c_int) function aero_gridtransformation(dxidx, inv_j, alpha, beta, gamma, x, y, z, &
+        is, ie, js, je, ks, ke, is0, ie0, js0, je0, ks0, ke0, m0) bind(C, name="aero_gridtransformation")
+      import :: c_int, c_double
+      integer(c_int) :: is, ie, js, je, ks, ke, is0, ie0, js0, je0, ks0, ke0, m0
+      real(c_double) :: dxidx(9, is:ie, js:je, ks:ke), inv_j(is:ie, js:je, ks:ke)
+      real(c_double) :: alpha(3, is:ie, js:je, ks:ke), beta(3, is:ie, js:je, ks:ke), gamma(3, is:ie, js:je, ks:ke)
+      real(c_double) :: x(is:ie, js:je, ks:ke), y(is:ie, js:je, ks:ke), z(is:ie, js:je, ks:ke)
+    end function
+
+    ! module-state routines: no arguments, as in the reference
+    integer(c_int) function aero_physical_bc() bind(C, name="aero_physical_bc")
+      import :: c_int
+    end function
+    integer(c_int) function aero_updatebuffer() bind(C, name="aero_updatebuffer")
+      import :: c_int
+    end function
+    integer(c_int) function aero_average1() bind(C, name="aero_average1")
+      import :: c_int
+    end function
+    integer(c_int) function aero_average2() bind(C, name="aero_average2")
+      import :: c_int
+    end function
+    integer(c_int) function aero_updatebuffercoordinate() bind(C, name="aero_updatebuffercoordinate")
+      import :: c_int
+    end function
+    integer(c_int) function aero_init_walldist() bind(C, name="aero_init_walldist")
+      import :: c_int
+    end function
+    integer(c_int) function aero_residual(out7) bind(C, name="aero_residual")
+      import :: c_int, c_double
+      real(c_double) :: out7(7)
+    end function
+    integer(c_int) function aero_step(nsteps, resid_hist, dt_minmax) bind(C, name="aero_step")
+      import :: c_int, c_ptr
+      integer(c_int), value :: nsteps
+      type(c_ptr), value :: resid_hist, dt_minmax
+    end function
+
+    function aero_last_error() bind(C, name="aero_last_error")
+      import :: c_ptr
+      type(c_ptr) :: aero_last_error
+    end function
+  end interface
+
+contains
+
+  !! The reference prints and stops on errors (main.f90:87-90, :647-650);
+  !! a non-zero status from the library does the same.
+  subroutine aero_check(ierr)
+    integer(c_int), intent(in) :: ierr
+    character(kind=c_char), pointer :: msg(:)
+    integer :: n
+    if (ierr == AERO_OK) return
+    call c_f_pointer(aero_last_error(), msg, [512])
+    n = 0
+    do while (n < 512)
+      if (msg(n + 1) == c_null_char) exit
+      n = n + 1
+    end do
+    print *, "aerocfd_gpu error", ierr, ": ", msg(1:n)
+    stop
+  end subroutine
+end module aerocfd_gpu
