@@ -19,13 +19,13 @@ enum FieldId {
   F_Q = 0, F_PRI, F_RHSI, F_RHSV, F_RHS, F_DT, F_DXIDX, F_INVJ, F_AMU, F_NUT, F_SARHS,
   F_X, F_Y, F_Z, F_DIST, F_ALPHA, F_BETA, F_GAMMA, F_DUDX, F_TAO, F_VOR, F_LENGTH, F_SPACING,
   // device-only scratch
-  F_RA, F_RB, F_RC, F_DIAG, F_FVH, F_DIASD,
+  F_RA, F_RB, F_RC, F_DIAG, F_FVH, F_DIASD, F_SAS,
   F_NUM
 };
 __host__ __device__ constexpr int field_nc(int f) {
   return f == F_Q ? 5 : f == F_PRI ? 7 : f == F_RHSI ? 5 : f == F_RHSV ? 5 : f == F_RHS ? 5
        : f == F_DXIDX ? 9 : f == F_AMU ? 3 : f == F_ALPHA ? 3 : f == F_BETA ? 3 : f == F_GAMMA ? 3
-       : f == F_DUDX ? 9 : f == F_TAO ? 6 : f == F_FVH ? 15 : 1;
+       : f == F_DUDX ? 9 : f == F_TAO ? 6 : f == F_FVH ? 15 : f == F_SAS ? 7 : 1;
 }
 constexpr int kNumPublicFields = F_SPACING + 1;
 
@@ -50,12 +50,12 @@ struct BlockView {
   // node (nodes of plane h = (i-is1)+(j-js1)+(k-ks1) are contiguous):
   int nplanes, pmax;     // number of hyperplanes, largest plane
   long* poff;            // nplanes+1 plane offsets
-  double* rec_f;         // 75 per node: forward blocks from the i-1, j-1, k-1 neighbours
-  double* rec_b;         // 75 per node: backward blocks from the i+1, j+1, k+1 neighbours
+  double* rec_f;         // kRec per node: forward blocks from the i-1, j-1, k-1 neighbours
+  double* rec_b;         // kRec per node: backward blocks from the i+1, j+1, k+1 neighbours
   double* sca;           // 8 per node: rhs(5), diag, inv_j, unused
   int* nbr;              // 6 per node: hyperplane-major positions of those neighbours (-1: outside)
   long* nat;             // natural (box) index of the node
-  double* dqs;           // 5 per node: dq* (forward result)
+  double* dqs;           // 8 per node: dq* (forward result), padded to 64 bytes
   double* dq;            // 5 per node: dq (backward result)
 
   __device__ __forceinline__ long at(int i, int j, int k) const {
@@ -64,6 +64,10 @@ struct BlockView {
   __device__ __forceinline__ double& v(int fid, int c, long n) const { return f[fid][(long)(c - 1) * plane + n]; }
   __device__ __forceinline__ double& s(int fid, long n) const { return f[fid][n]; }
 };
+
+// LU-SGS record stride: three 5x5 blocks (75 doubles) padded to 608 bytes so
+// every record starts on a 16-byte boundary (bulk-copy alignment).
+constexpr int kRec = 76;
 
 // Per-case scalars (module ns_const / flag_var values the path reads).
 struct CaseConsts {

@@ -41,8 +41,16 @@ __global__ void k_find_dt(const BlockView* __restrict__ blocks, CaseConsts cc, d
 __global__ void k_dt_minmax(const BlockView* __restrict__ blocks, int m, const double* cta_max,
                             int ncta, int cta_size, double* out2);
 __global__ void k_lusgs_prep(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_plane_index(const BlockView* __restrict__ blocks);
 __global__ void k_lusgs_mats(const BlockView* __restrict__ blocks, CaseConsts cc);
-__global__ void k_lusgs_sweep(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_sa_length(const BlockView* __restrict__ blocks);
+__global__ void k_sa_a(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_sa_b(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_sa_recs(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_sa_sweep(const BlockView* __restrict__ blocks);
+__global__ void k_lusgs_sweep_staged(const BlockView* __restrict__ blocks, int nst, unsigned* status);
+__global__ void k_lusgs_sweep_global(const BlockView* __restrict__ blocks, int nst, unsigned* status);
+__global__ void k_lusgs_update(const BlockView* __restrict__ blocks);
 __global__ void k_physical_bc(const BlockView* __restrict__ blocks, const BcOp* __restrict__ ops,
                               const int* __restrict__ op_start, CaseConsts cc);
 __global__ void k_sa_clip(const BlockView* __restrict__ blocks);

@@ -107,12 +107,13 @@ State g;
 // count of every kernel this library launches (aero_launch_count).
 enum ProfId {
   P_GETPRI, P_FILL, P_INVISCID, P_VISC_A, P_VISC_B, P_FIND_DT, P_DT_MINMAX, P_LUSGS_PREP,
-  P_LUSGS_MATS, P_LUSGS_SWEEP, P_BC, P_SA_CLIP, P_HALO, P_AVG_GATHER, P_AVG_APPLY, P_RESID_PART, P_RESID_FINAL,
+  P_LUSGS_MATS, P_LUSGS_SWEEP, P_LUSGS_UPDATE, P_SA_A, P_SA_B, P_SA_RECS, P_SA_SWEEP, P_INDEX, P_BC, P_SA_CLIP, P_HALO, P_AVG_GATHER, P_AVG_APPLY, P_RESID_PART, P_RESID_FINAL,
   P_TRANSFER, P_GEOMETRY, P_NUM
 };
 const char* kProfName[P_NUM] = {
     "k_getpri", "k_fill", "k_inviscid", "k_viscous_a", "k_viscous_b", "k_find_dt", "k_dt_minmax",
-    "k_lusgs_prep", "k_lusgs_mats", "k_lusgs_sweep", "k_physical_bc", "k_sa_clip", "k_halo", "k_avg_gather",
+    "k_lusgs_prep", "k_lusgs_mats", "k_lusgs_sweep", "k_lusgs_update", "k_sa_a", "k_sa_b", "k_sa_recs", "k_sa_sweep",
+    "k_plane_index", "k_physical_bc", "k_sa_clip", "k_halo", "k_avg_gather",
     "k_avg_apply", "k_residual_partial", "k_residual_final", "k_transfer", "k_geometry"};
 struct Prof {
   bool on = false;
@@ -229,7 +230,7 @@ void fill_view(BlockView& v, const Box& b, const Box& b0, const Box& b1, long pl
 // poff, rec_f, rec_b, sca, dqs, dq, nat, nbr.
 size_t workspace_bytes(const Box& b1, int H) {
   size_t N1 = (size_t)b1.size();
-  return (size_t)(H + 1) * sizeof(long) + N1 * (75 + 75 + 8 + 5 + 5) * sizeof(double) + N1 * sizeof(long) +
+  return (size_t)(H + 1) * sizeof(long) + N1 * (2 * kRec + 8 + 8 + 5) * sizeof(double) + N1 * sizeof(long) +
          N1 * 6 * sizeof(int) + 256;
 }
 int attach_workspace(BlockView& v, void* ws, const std::vector<long>& poff, int pmax) {
@@ -237,10 +238,10 @@ int attach_workspace(BlockView& v, void* ws, const std::vector<long>& poff, int 
   char* p = (char*)ws;
   v.nplanes = (int)poff.size() - 1;
   v.pmax = pmax;
-  v.rec_f = (double*)p; p += N1 * 75 * sizeof(double);
-  v.rec_b = (double*)p; p += N1 * 75 * sizeof(double);
+  v.rec_f = (double*)p; p += N1 * kRec * sizeof(double);
+  v.rec_b = (double*)p; p += N1 * kRec * sizeof(double);
   v.sca = (double*)p; p += N1 * 8 * sizeof(double);
-  v.dqs = (double*)p; p += N1 * 5 * sizeof(double);
+  v.dqs = (double*)p; p += N1 * 8 * sizeof(double);
   v.dq = (double*)p; p += N1 * 5 * sizeof(double);
   v.nat = (long*)p; p += N1 * sizeof(long);
   v.poff = (long*)p; p += poff.size() * sizeof(long);
@@ -423,14 +424,56 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
   CKL();
   PROF(P_LUSGS_MATS, (k_lusgs_mats<<<dim3(cdiv(3 * maxN1, 128), nblk), 128, 0, g.stream>>>(views, cc)));
   CKL();
-  size_t smem = (size_t)2 * 5 * std::max(pmax, 1) * sizeof(double);
-  static size_t smem_set = 0;
-  if (smem > 48 * 1024 && smem > smem_set) {
-    CK(cudaFuncSetAttribute(k_lusgs_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    smem_set = smem;
-  }
+  // shared memory: ring of two planes + nst staged planes (records, scalars,
+  // dq*) + one mbarrier per stage; stage as many planes ahead as fit (2..3).
+  const size_t kSmemMax = 227 * 1024;
+  size_t ring = (size_t)2 * 5 * std::max(pmax, 1) * sizeof(double);
+  size_t stage = (size_t)std::max(pmax, 1) * (kRec + 16) * sizeof(double);
+  int nst = 3;
+  while (nst >= 2 && ring + nst * stage + nst * 8 > kSmemMax) --nst;
   int threads = (int)std::min<long>(1024, std::max<long>(64, (5L * pmax + 31) / 32 * 32));
-  PROF(P_LUSGS_SWEEP, (k_lusgs_sweep<<<nblk, threads, smem, g.stream>>>(views, cc)));
+  if (nst >= 2) {
+    size_t smem = ring + nst * stage + nst * 8;
+    static size_t set_staged = 0;
+    if (smem > 48 * 1024 && smem > set_staged) {
+      CK(cudaFuncSetAttribute(k_lusgs_sweep_staged, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      set_staged = smem;
+    }
+    PROF(P_LUSGS_SWEEP, (k_lusgs_sweep_staged<<<nblk, threads, smem, g.stream>>>(views, nst, g.d_status)));
+  } else {
+    size_t smem = ring;
+    static size_t set_global = 0;
+    if (smem > 48 * 1024 && smem > set_global) {
+      CK(cudaFuncSetAttribute(k_lusgs_sweep_global, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      set_global = smem;
+    }
+    PROF(P_LUSGS_SWEEP, (k_lusgs_sweep_global<<<nblk, threads, smem, g.stream>>>(views, 1, g.d_status)));
+  }
+  CKL();
+  PROF(P_LUSGS_UPDATE, (k_lusgs_update<<<dim3(cdiv(maxN1, 256), nblk), 256, 0, g.stream>>>(views)));
+  CKL();
+  return AERO_OK;
+}
+
+int launch_index(const BlockView* views, int nblk, long maxN1) {
+  PROF(P_INDEX, (k_plane_index<<<dim3(cdiv(maxN1, 256), nblk), 256, 0, g.stream>>>(views)));
+  CKL();
+  return AERO_OK;
+}
+
+// sa_model (sub_tur_sa.f90:7-122) on nblk views; needs the hyperplane index.
+int launch_sa(const BlockView* views, int nblk, long maxN, long maxN1, int pmax, const CaseConsts& cc) {
+  PROF(P_FILL, (k_sa_length<<<dim3(cdiv(maxN, 256), nblk), 256, 0, g.stream>>>(views)));
+  CKL();
+  PROF(P_SA_A, (k_sa_a<<<dim3(cdiv(maxN1, 256), nblk), 256, 0, g.stream>>>(views, cc)));
+  CKL();
+  PROF(P_SA_B, (k_sa_b<<<dim3(cdiv(maxN1, 128), nblk), 128, 0, g.stream>>>(views, cc)));
+  CKL();
+  PROF(P_SA_RECS, (k_sa_recs<<<dim3(cdiv(maxN1, 256), nblk), 256, 0, g.stream>>>(views, cc)));
+  CKL();
+  size_t smem = (size_t)2 * std::max(pmax, 1) * sizeof(double);
+  int threads = (int)std::min<long>(1024, std::max<long>(64, (pmax + 31) / 32 * 32));
+  PROF(P_SA_SWEEP, (k_sa_sweep<<<nblk, threads, smem, g.stream>>>(views)));
   CKL();
   return AERO_OK;
 }
@@ -496,6 +539,7 @@ int do_iteration(bool want_dt_minmax) {
   if ((rc = launch_find_dt(g.d_blocks, nb, g.max_box, g.cc))) return rc;
   if (want_dt_minmax && (rc = launch_dt_minmax(g.d_blocks, nb - 1, g.d_out + 7))) return rc;
   if ((rc = launch_implicit(g.d_blocks, nb, g.max_ext, g.max_b1, g.pmax_all, g.cc))) return rc;
+  if (sa_on() && (rc = launch_sa(g.d_blocks, nb, g.max_box, g.max_b1, g.pmax_all, g.cc))) return rc;
   if ((rc = do_physical_bc())) return rc;
   if ((rc = do_halo())) return rc;
   if ((rc = do_average1())) return rc;
@@ -585,6 +629,7 @@ int aero_configure(const int* iflags, const double* params) {
     return fail(AERO_ERR_ARG, "Wrong turbulence model type is input!!! (%d)", iflags[4]);
   if (iflags[6] != 2 || iflags[7] != 4)
     return fail(AERO_ERR_ARG, "bufferLength=%d/iflag_inviscid=%d: only the 3rd-order WENO (2 layers)", iflags[6], iflags[7]);
+  if (iflags[5] != 0) return fail(AERO_ERR_ARG, "iflag_des=%d: DES97/DDES are not supported on the GPU", iflags[5]);
   std::memcpy(g.iflags, iflags, sizeof g.iflags);
   std::memcpy(g.params, params, sizeof g.params);
   CaseConsts& c = g.cc;
@@ -716,6 +761,7 @@ int aero_finish_setup(void) {
   if (g.nhalo) CK(cudaMemcpyAsync(g.d_halo, topo.halo.data(), g.nhalo * sizeof(HaloEntry), cudaMemcpyHostToDevice, g.stream));
   if (g.navg_src) CK(cudaMemcpyAsync(g.d_avg_src, topo.avg_src.data(), g.navg_src * sizeof(AvgSrc), cudaMemcpyHostToDevice, g.stream));
   if (g.navg_dst) CK(cudaMemcpyAsync(g.d_avg_dst, topo.avg_dst.data(), g.navg_dst * sizeof(AvgDst), cudaMemcpyHostToDevice, g.stream));
+  if ((rc = launch_index(g.d_blocks, nb, g.max_b1))) return rc;
   g.resid_ctas = (int)cdiv(g.max_b1, 256);
   CK(cudaMalloc(&g.d_part, (size_t)g.resid_ctas * nb * 6 * sizeof(double)));
   CK(cudaStreamSynchronize(g.stream));
@@ -847,6 +893,7 @@ int aero_implicit1st(double* q, const double* dt, const double* pri_v, double* r
   CaseConsts cc = consts_with(*gamma, g.cc.cv, g.cc.re);
   cc.cfl = *cfl;
   Box e{b1.is - 1, b1.ie + 1, b1.js - 1, b1.je + 1, b1.ks - 1, b1.ke + 1};
+  if (!t.resident && (rc = launch_index(t.d_view, 1, b1.size()))) return rc;
   if ((rc = launch_implicit(t.d_view, 1, e.size(), b1.size(), t.view.pmax, cc))) return rc;
   return finish(t, args);
 }
@@ -927,6 +974,34 @@ int aero_init_flowfield(void) {
   }
   CK(cudaStreamSynchronize(g.stream));
   return AERO_OK;
+}
+
+int aero_sa_model(double* nut, double* sa_rhs, const double* dt, const double* pri_v, const double* amu,
+                  const double* dudx, const double* vor, const double* dxidx, const double* inv_j,
+                  const double* alpha, const double* beta, const double* gamma, double* length,
+                  const double* dist, const double* spac, const double* re, const double* cfl,
+                  const int* is, const int* ie, const int* js, const int* je, const int* ks,
+                  const int* ke, const int* is0, const int* ie0, const int* js0, const int* je0,
+                  const int* ks0, const int* ke0, const int* is1, const int* ie1, const int* js1,
+                  const int* je1, const int* ks1, const int* ke1) {
+  (void)dudx; (void)spac;
+  int rc = need_init();
+  if (rc) return rc;
+  if (g.cc.des != 0) return fail(AERO_ERR_ARG, "sa_model: DES97/DDES length scales are not supported");
+  Box b = box_of(is, ie, js, je, ks, ke), b0 = box_of(is0, ie0, js0, je0, ks0, ke0),
+      b1 = box_of(is1, ie1, js1, je1, ks1, ke1);
+  std::vector<Arg> args = {{F_NUT, nut, true},     {F_SARHS, sa_rhs, true}, {F_DT, dt, false},
+                           {F_PRI, pri_v, false},  {F_AMU, amu, false},     {F_VOR, vor, false},
+                           {F_DXIDX, dxidx, false}, {F_INVJ, inv_j, false}, {F_ALPHA, alpha, false},
+                           {F_BETA, beta, false},  {F_GAMMA, gamma, false}, {F_LENGTH, length, true},
+                           {F_DIST, dist, false}};
+  BlockTarget t;
+  if ((rc = resolve(b, b0, b1, args, t))) return rc;
+  CaseConsts cc = consts_with(g.cc.gamma, g.cc.cv, *re);
+  cc.cfl = *cfl;
+  if (!t.resident && (rc = launch_index(t.d_view, 1, b1.size()))) return rc;
+  if ((rc = launch_sa(t.d_view, 1, b.size(), b1.size(), t.view.pmax, cc))) return rc;
+  return finish(t, args);
 }
 
 int aero_gridtransformation(double* dxidx, double* inv_j, double* alpha, double* beta, double* gamma,

@@ -1,0 +1,253 @@
+// Spalart-Allmaras one-equation model (sub_tur_sa.f90): residual of the
+// advection, diffusion and source terms plus the scalar LU-SGS update, loosely
+// coupled after the mean-flow update as in main.f90:414-419.
+//
+// sa_rhs2 works on zero-filled temporaries written only on the updated box, so
+// a second difference next to a physical boundary reads a zero neighbour
+// (sub_tur_sa.f90:259-291, :359-403).  The SA scratch planes here are written
+// only on the updated box and are zero elsewhere, which reproduces that.
+#include <cmath>
+
+#include "aero_device.cuh"
+#include "aero_kernels.h"
+
+namespace aero {
+
+namespace {
+
+// One-sided at the physical ends is0/ie0, central elsewhere (sub_tur_sa.f90:297-303).
+__device__ __forceinline__ double d1(const double* f, long n, long st, int pos, int lo0, int hi0) {
+  if (pos == lo0) return f[n + st] - f[n];
+  if (pos == hi0) return f[n] - f[n - st];
+  return (f[n + st] - f[n - st]) / 2.0;
+}
+
+__device__ __forceinline__ void node_of(const Box& bx, long t, int& i, int& j, int& k) {
+  i = bx.is + (int)(t % bx.nx());
+  long r = t / bx.nx();
+  j = bx.js + (int)(r % bx.ny());
+  k = bx.ks + (int)(r / bx.ny());
+}
+
+}  // namespace
+
+// Pass A over the updated box: dnut/dxi, dnut/deta, dnut/dzeta, the alpha/beta/
+// gamma contractions and nu + (1+cb2)*nut (sub_tur_sa.f90:294-413) into SA
+// scratch planes 0..6.
+__global__ void k_sa_a(const BlockView* __restrict__ blocks, CaseConsts cc) {
+  const BlockView& B = blocks[blockIdx.y];
+  const Box& b1 = B.b1;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b1.size()) return;
+  int i, j, k;
+  node_of(b1, t, i, j, k);
+  long n = B.at(i, j, k);
+  const long st[3] = {1, (long)B.nx, (long)B.nx * B.ny};
+  const int pos[3] = {i, j, k};
+  const int lo0[3] = {B.b0.is, B.b0.js, B.b0.ks}, hi0[3] = {B.b0.ie, B.b0.je, B.b0.ke};
+  const double* nut = B.f[F_NUT];
+  double g[3] = {0.0, 0.0, 0.0};
+  int ndir = cc.dimension == IFLAG_3D ? 3 : 2;
+  for (int d = 0; d < ndir; ++d) g[d] = d1(nut, n, st[d], pos[d], lo0[d], hi0[d]);
+  double* S = B.f[F_SAS];
+  long P = B.plane;
+  S[0 * P + n] = g[0];
+  S[1 * P + n] = g[1];
+  S[2 * P + n] = g[2];
+  S[3 * P + n] = B.v(F_ALPHA, 1, n) * g[0] + B.v(F_ALPHA, 2, n) * g[1] + B.v(F_ALPHA, 3, n) * g[2];
+  S[4 * P + n] = B.v(F_BETA, 1, n) * g[0] + B.v(F_BETA, 2, n) * g[1] + B.v(F_BETA, 3, n) * g[2];
+  S[5 * P + n] = B.v(F_GAMMA, 1, n) * g[0] + B.v(F_GAMMA, 2, n) * g[1] + B.v(F_GAMMA, 3, n) * g[2];
+  double nu0 = B.v(F_AMU, 1, n) / B.v(F_PRI, 1, n);
+  S[6 * P + n] = nu0 + (1.0 + SA_CB2) * nut[n];
+}
+
+// Pass B over the updated box: sa_rhs = advection (sa_rhs1) + diffusion
+// (sa_rhs2) + production/destruction (sa_rhs3), in that order, and the source
+// linearisation diasd (sub_tur_sa.f90:152-208, :359-512, :561-625).
+__global__ void k_sa_b(const BlockView* __restrict__ blocks, CaseConsts cc) {
+  const BlockView& B = blocks[blockIdx.y];
+  const Box& b1 = B.b1;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b1.size()) return;
+  int i, j, k;
+  node_of(b1, t, i, j, k);
+  long n = B.at(i, j, k);
+  const long st[3] = {1, (long)B.nx, (long)B.nx * B.ny};
+  const int pos[3] = {i, j, k};
+  const int lo0[3] = {B.b0.is, B.b0.js, B.b0.ks}, hi0[3] = {B.b0.ie, B.b0.je, B.b0.ke};
+  const double* nut = B.f[F_NUT];
+  const double* S = B.f[F_SAS];
+  long P = B.plane;
+  bool three = cc.dimension == IFLAG_3D;
+  double re = cc.re;
+  double m[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) m[c] = B.v(F_DXIDX, c + 1, n);
+  double u = B.v(F_PRI, 2, n), v = B.v(F_PRI, 3, n), w = B.v(F_PRI, 4, n);
+  double nut0 = nut[n];
+  // sa_rhs1: first-order upwind advection on the contravariant velocities
+  double adv[3] = {0.0, 0.0, 0.0};
+  for (int d = 0; d < (three ? 3 : 2); ++d) {
+    double uu = m[3 * d] * u + m[3 * d + 1] * v + m[3 * d + 2] * w;
+    double nutp = nut[n + st[d]], nutm = nut[n - st[d]];
+    adv[d] = -(0.5 * (uu + fabs(uu)) * (nut0 - nutm) + 0.5 * (uu - fabs(uu)) * (nutp - nut0));
+  }
+  double rhs = adv[0] + adv[1] + adv[2];
+  // sa_rhs2: diffusion
+  double ta = d1(S + 3 * P, n, st[0], pos[0], lo0[0], hi0[0]);
+  double tb = d1(S + 4 * P, n, st[1], pos[1], lo0[1], hi0[1]);
+  double tc = three ? d1(S + 5 * P, n, st[2], pos[2], lo0[2], hi0[2]) : 0.0;
+  double txi = d1(S + 6 * P, n, st[0], pos[0], lo0[0], hi0[0]);
+  double teta = d1(S + 6 * P, n, st[1], pos[1], lo0[1], hi0[1]);
+  double tzeta = three ? d1(S + 6 * P, n, st[2], pos[2], lo0[2], hi0[2]) : 0.0;
+  double tx = txi * m[0] + teta * m[3] + tzeta * m[6];
+  double ty = txi * m[1] + teta * m[4] + tzeta * m[7];
+  double tz = txi * m[2] + teta * m[5] + tzeta * m[8];
+  double inv_j0 = B.s(F_INVJ, n);
+  double deltanut = (ta + tb + tc) / inv_j0;
+  double gx = S[0 * P + n], ge = S[1 * P + n], gz = S[2 * P + n];
+  double dnutdx = gx * m[0] + ge * m[3] + gz * m[6];
+  double dnutdy = gx * m[1] + ge * m[4] + gz * m[7];
+  double dnutdz = gx * m[2] + ge * m[5] + gz * m[8];
+  double temp = S[6 * P + n];
+  double diff = -(SA_CB2 / (re * SA_DTA)) * nut0 * deltanut +
+                (1.0 / (re * SA_DTA)) * (temp * deltanut + tx * dnutdx + ty * dnutdy + tz * dnutdz);
+  rhs = rhs + diff;
+  // sa_rhs3: production / destruction and the derivative of the source
+  double d = B.v(F_PRI, 1, n);
+  double nu0 = B.v(F_AMU, 1, n) / d;
+  double omega = fabs(B.s(F_VOR, n));
+  double dist0 = B.s(F_LENGTH, n);
+  double leix = fmax(nut0 / nu0, 0.001);
+  double fv1 = p3(leix) / (p3(leix) + SA_CV13);
+  double fv2 = 1.0 - leix / (1.0 + leix * fv1);
+  double s = omega + nut0 * fv2 / (re * SA_KAR2 * p2(dist0));
+  s = fmax(s, 0.3 * omega);
+  double dv = s * re * SA_KAR2 * p2(dist0);
+  dv = fmax(dv, 1.0e-6);
+  double r = nut0 * dv;  // the reference's r (sub_tur_sa.f90:579)
+  r = fmin(r, 10.0);
+  double g = r + SA_CW2 * (p6(r) - r);
+  double fw = g * pow((1.0 + 64.0) / (p6(g) + 64.0), 1.0 / 6.0);
+  double ft2 = SA_CT3 * exp(-SA_CT4 * p2(leix));
+  double aaa = SA_CB1 * ((1.0 - ft2) * fv2 + ft2) / SA_KAR2;
+  double bbb = SA_CW1 * fw;
+  double ccc = nut0 / p2(dist0);
+  double sd1 = (aaa - bbb) * ccc / re;
+  double sd = sd1 * nut0;
+  double sp = SA_CB1 * (1.0 - ft2) * omega * nut0;
+  rhs = rhs + sd + sp;
+  B.s(F_SARHS, n) = rhs;
+  double leixn = 1.0 / nu0;
+  double fv1n = (3.0 * p2(leix) * leixn * (p3(leix) + SA_CV13) - p3(leix) * (3.0 * p2(leix) * leixn)) /
+                p2(p3(leix) + SA_CV13);
+  double fv2n = (leixn * (1.0 + leix * fv1) - leix * (leixn * fv1 + leix * fv1n)) / p2(1.0 + leix * fv1);
+  double ft2n = -(2.0 * SA_CT4 * leix * leixn * ft2);
+  double sn = 1.0 / (re * SA_KAR2 * p2(dist0)) * (fv2 + fv2n * nut0);
+  dv = p2(s) * (re * SA_KAR2 * p2(dist0));
+  dv = fmax(dv, 1.0e-6);
+  double rn = (s - sn * nut0) / dv;
+  double gn = (1.0 + SA_CW2 * 6.0 * p5(r) - SA_CW2) * rn;
+  const double cw3m6 = 0.015625;  // cw3**(-6)
+  double fwn = -((1.0 / 6.0) * pow((pow(g, -6.0) + cw3m6) / (1.0 + cw3m6), -7.0 / 6.0));
+  fwn = fwn / (1.0 + cw3m6) * (-(6.0 * pow(g, -7.0))) * gn;
+  double spn = SA_CB1 * (1.0 - ft2) * omega + SA_CB1 * (-ft2n) * omega * nut0;
+  double sdn = (1.0 / re) * (SA_CB1 * (fv2 - ft2 * fv2 + ft2) / SA_KAR2 - SA_CW1 * fw) * 2.0 * nut0 / p2(dist0);
+  sdn = (1.0 / re) * (SA_CB1 * (fv2n - ft2n * fv2 - ft2 * fv2n + ft2n) / SA_KAR2 - SA_CW1 * fwn) *
+            (p2(nut0) / p2(dist0)) + sdn;
+  B.s(F_DIASD, n) = fmin(spn + sdn, 0.0);
+}
+
+// sa_lusgs diagonal and upwind coefficients of every updated node, stored in
+// the node's hyperplane-major record: rec_f[0..2] = 0.5*(U+|U|) per
+// direction, rec_f[3..5] = 0.5*(U-|U|), rec_f[6] = sa_rhs, rec_f[7] = diag
+// (sub_tur_sa.f90:676-750, :762-778).
+__global__ void k_sa_recs(const BlockView* __restrict__ blocks, CaseConsts cc) {
+  const BlockView& B = blocks[blockIdx.y];
+  const Box& b1 = B.b1;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b1.size()) return;
+  long pos = t;  // the record of the t-th node in hyperplane-major order
+  long n = B.nat[pos];
+  double phi = (cc.cfl >= 1.0e3 && cc.time == IFLAG_STEADY) ? 0.0 : 1.0;
+  double u = B.v(F_PRI, 2, n), v = B.v(F_PRI, 3, n), w = B.v(F_PRI, 4, n);
+  double x0 = B.v(F_DXIDX, 1, n), y0 = B.v(F_DXIDX, 2, n), z0 = B.v(F_DXIDX, 3, n);
+  double d2 = x0 * x0 + y0 * y0 + z0 * z0;
+  double cu = x0 * u + y0 * v + z0 * w;
+  x0 = B.v(F_DXIDX, 4, n); y0 = B.v(F_DXIDX, 5, n); z0 = B.v(F_DXIDX, 6, n);
+  d2 = d2 + x0 * x0 + y0 * y0 + z0 * z0;
+  double cv = x0 * u + y0 * v + z0 * w;
+  x0 = B.v(F_DXIDX, 7, n); y0 = B.v(F_DXIDX, 8, n); z0 = B.v(F_DXIDX, 9, n);
+  d2 = d2 + x0 * x0 + y0 * y0 + z0 * z0;
+  double cw = x0 * u + y0 * v + z0 * w;
+  double tm = 4.0 * d2 * B.s(F_NUT, n) / cc.re;
+  double diag = 1.0 / B.s(F_DT, n) * phi + fabs(cu) + fabs(cv) + fabs(cw) + tm - B.s(F_DIASD, n);
+  double* rec = B.rec_f + kRec * pos;
+  rec[0] = 0.5 * (cu + fabs(cu));
+  rec[1] = 0.5 * (cv + fabs(cv));
+  rec[2] = 0.5 * (cw + fabs(cw));
+  rec[3] = 0.5 * (cu - fabs(cu));
+  rec[4] = 0.5 * (cv - fabs(cv));
+  rec[5] = 0.5 * (cw - fabs(cw));
+  rec[6] = B.s(F_SARHS, n);
+  rec[7] = diag;
+}
+
+// Scalar LU-SGS sweeps of the SA equation and nut += dnut, one CTA per block,
+// one thread per node of a hyperplane (sub_tur_sa.f90:759-818).
+__global__ void k_sa_sweep(const BlockView* __restrict__ blocks) {
+  const BlockView& B = blocks[blockIdx.x];
+  extern __shared__ double sdn[];  // two planes of pmax values
+  const int P = B.pmax;
+  const int H = B.nplanes;
+  for (int h = 0; h < H; ++h) {
+    long base = B.poff[h];
+    int cnt = (int)(B.poff[h + 1] - base);
+    long pbase = h > 0 ? B.poff[h - 1] : 0;
+    double* prev = sdn + P * ((h + 1) & 1);
+    double* cur = sdn + P * (h & 1);
+    for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+      long pos = base + t;
+      const double* rec = B.rec_f + kRec * pos;
+      const int* nb = B.nbr + 6 * pos;
+      double tt[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) tt[d] = nb[d] < 0 ? 0.0 : rec[d] * prev[nb[d] - pbase];
+      double v = (rec[6] + (tt[0] + tt[1] + tt[2])) / rec[7];
+      cur[t] = v;
+      B.dqs[pos] = v;
+    }
+    __syncthreads();
+  }
+  for (int h = H - 1; h >= 0; --h) {
+    long base = B.poff[h];
+    int cnt = (int)(B.poff[h + 1] - base);
+    long pbase = h + 1 < H ? B.poff[h + 1] : 0;
+    double* prev = sdn + P * ((h + 1) & 1);
+    double* cur = sdn + P * (h & 1);
+    for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+      long pos = base + t;
+      const double* rec = B.rec_f + kRec * pos;
+      const int* nb = B.nbr + 6 * pos + 3;
+      double tt[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) tt[d] = nb[d] < 0 ? 0.0 : rec[3 + d] * prev[nb[d] - pbase];
+      double v = B.dqs[pos] - (tt[0] + tt[1] + tt[2]) / rec[7];
+      cur[t] = v;
+      long n = B.nat[pos];
+      B.s(F_NUT, n) = B.s(F_NUT, n) + v;
+    }
+    __syncthreads();
+  }
+}
+
+// length = dist over the full box (sub_tur_sa.f90:51-57; no DES).
+__global__ void k_sa_length(const BlockView* __restrict__ blocks) {
+  const BlockView& B = blocks[blockIdx.y];
+  long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= B.b.size()) return;
+  B.s(F_LENGTH, n) = B.s(F_DIST, n);
+  B.s(F_SARHS, n) = 0.0;
+}
+
+}  // namespace aero

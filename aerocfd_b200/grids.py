@@ -189,3 +189,81 @@ def bump_batch(ncase: int = 64, seed: int = 0, nk: int = 5):
         cfg = Config(solver=IFLAG_EULERSOLVER, ma=ma, re=1.0e6, cfl=5.0)
         cases.append(bump_channel(ni, nj, nk, h=h, cfg=cfg, name=f"bump{c:02d}"))
     return cases
+
+
+def geometric_nodes(n: int, first: float, length: float) -> np.ndarray:
+    """n intervals from 0 to `length` growing geometrically from `first`."""
+    if abs(first * n - length) < 1e-15 * length:
+        return np.linspace(0.0, length, n + 1)
+    lo, hi = (1.0 + 1e-12, 10.0) if first * n < length else (1e-6, 1.0 - 1e-12)
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        val = first * (mid ** n - 1.0) / (mid - 1.0)
+        lo, hi = (mid, hi) if val < length else (lo, mid)
+    r = 0.5 * (lo + hi)
+    s = first * (r ** np.arange(n + 1) - 1.0) / (r - 1.0)
+    s[-1] = length
+    return s
+
+
+def flat_plate(nbi: int = 2, nbj: int = 2, nbk: int = 2, ni: int = 193, nj: int = 129, nk: int = 33,
+               x_up: float = 0.5, dx_le: float = 2.0e-3, dy_wall: float = 5.0e-6, ratio_y: float = 1.1,
+               span: float = 0.32, cfg: Optional[Config] = None, name: str = "flat_plate") -> Case:
+    """Turbulent flat plate of length 1 split into nbi x nbj x nbk blocks that
+    share their interface planes (ni = nbi*(bi-1)+1 etc.).  The leading edge
+    sits on the first i-interface, so the j=1 faces of the upstream blocks are
+    symmetry planes and those of the downstream blocks no-slip walls.  x is
+    clustered geometrically at the leading edge from both sides, y grows from
+    the wall spacing dy_wall at ratio_y, z is uniform.  Inflow at i=1, outflow
+    at i=max, farfield at j=max, symmetry on both k faces."""
+    cfg = cfg or Config(solver=IFLAG_NSSOLVER, turbulence=2, ma=0.2, re=5.0e6, cfl=2.0, nutinf=3.0)
+    bi, bj, bk = (ni - 1) // nbi + 1, (nj - 1) // nbj + 1, (nk - 1) // nbk + 1
+    assert nbi * (bi - 1) + 1 == ni and nbj * (bj - 1) + 1 == nj and nbk * (bk - 1) + 1 == nk
+    i_le = bi  # global index of the leading edge
+    up = geometric_nodes(i_le - 1, dx_le, x_up)[::-1] * -1.0
+    down = geometric_nodes(ni - i_le, dx_le, 1.0)
+    X = np.concatenate([up, down[1:]])
+    Y = dy_wall * (ratio_y ** np.arange(nj) - 1.0) / (ratio_y - 1.0)
+    Z = np.linspace(0.0, span, nk)
+    blocks: List[Block] = []
+
+    def bid(a, b, c):
+        return 1 + a + nbi * (b + nbj * c)
+
+    for c in range(nbk):
+        for b in range(nbj):
+            for a in range(nbi):
+                m = bid(a, b, c)
+                subs = []
+                fno = 0
+
+                def add(face, box, kind, partner=0):
+                    nonlocal fno
+                    fno += 1
+                    subs.append(Subface(fno, face, *box, kind, partner, 2 if kind > 0 else 0))
+                full = {1: (1, 1, 1, bj, 1, bk), 2: (bi, bi, 1, bj, 1, bk), 3: (1, bi, 1, 1, 1, bk),
+                        4: (1, bi, bj, bj, 1, bk), 5: (1, bi, 1, bj, 1, 1), 6: (1, bi, 1, bj, bk, bk)}
+                # face 1, 2 (i)
+                add(1, full[1], bid(a - 1, b, c) if a > 0 else BC_INFLOW)
+                add(2, full[2], bid(a + 1, b, c) if a < nbi - 1 else BC_OUTFLOW)
+                # face 3, 4 (j)
+                wall = BC_WALL if a * (bi - 1) + 1 >= i_le else BC_SYMM
+                add(3, full[3], bid(a, b - 1, c) if b > 0 else wall)
+                add(4, full[4], bid(a, b + 1, c) if b < nbj - 1 else BC_FARFIELD)
+                # face 5, 6 (k)
+                add(5, full[5], bid(a, b, c - 1) if c > 0 else BC_SYMM)
+                add(6, full[6], bid(a, b, c + 1) if c < nbk - 1 else BC_SYMM)
+                blk = Block(m, bi, bj, bk, subs, cfg.buffer_length, cfg.dimension)
+                xs = X[a * (bi - 1):a * (bi - 1) + bi]
+                ys = Y[b * (bj - 1):b * (bj - 1) + bj]
+                zs = Z[c * (bk - 1):c * (bk - 1) + bk]
+                ZZ, YY, XX = np.meshgrid(zs, ys, xs, indexing="ij")
+                _set_coords(blk, XX, YY, ZZ)
+                blocks.append(blk)
+    # interface partners: face 1 <-> face 2 (subface 1 <-> 2), 3 <-> 4, 5 <-> 6
+    pair = {1: 2, 2: 1, 3: 4, 4: 3, 5: 6, 6: 5}
+    for blk in blocks:
+        for s in blk.subfaces:
+            if s.blk_t > 0:
+                s.subface_t = pair[s.face]
+    return Case(name, cfg, blocks)

@@ -76,6 +76,14 @@ class GpuCase:
         _lib.check(self.L.aero_sync_to_host(ctypes.c_ulonglong(m)), "aero_sync_to_host")
 
     # ------------------------------------------------- module-state routines
+    def compute_geometry(self, walldist: Optional[bool] = None) -> None:
+        """main.f90:142-208 on the device: uploads the grid coordinates, then the
+        coordinate halo, metrics, spacing and (SA cases) the wall distance."""
+        if walldist is None:
+            walldist = self.case.cfg.turbulence > 0
+        self.sync_to_device(mask("x", "y", "z"))
+        _lib.check(self.L.aero_compute_geometry(ctypes.c_int(1 if walldist else 0)), "aero_compute_geometry")
+
     def init_flowfield(self) -> None:
         _lib.check(self.L.aero_init_flowfield(), "aero_init_flowfield")
 

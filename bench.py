@@ -192,7 +192,7 @@ def main():
     case = make_case()
     gc = solver.GpuCase(case, device=local)
     L = gc.L
-    _lib.check(L.aero_compute_geometry(ctypes.c_int(0)), "aero_compute_geometry")
+    gc.compute_geometry()
     gc.init_flowfield()
     gc.start()
     gc.step(args.warmup, history=False)
@@ -271,6 +271,8 @@ def main():
     e2e = nodes * args.steps * world / e2e_s / 1e6
 
     status = gc.status()
+    if status:
+        print(f"warning: device status word {status} (non-finite residual or negative density)", file=sys.stderr)
     line = {
         "metric": "Mcell-iter/s", "value": value, "unit": "Mcell-iter/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dev_s / args.steps,

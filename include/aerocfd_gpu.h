@@ -137,6 +137,15 @@ int aero_implicit1st(double* q, const double* dt, const double* pri_v, double* r
                      const int* je1, const int* ks1, const int* ke1, const double* gamma,
                      const double* cfl, const double* xx, const double* yy, const double* zz);
 
+/* sub_tur_sa.f90:7-11 (no DES; dudx and spac are accepted and unused) */
+int aero_sa_model(double* nut, double* sa_rhs, const double* dt, const double* pri_v, const double* amu,
+                  const double* dudx, const double* vor, const double* dxidx, const double* inv_j,
+                  const double* alpha, const double* beta, const double* gamma, double* length,
+                  const double* dist, const double* spac, const double* re, const double* cfl,
+                  const int* is, const int* ie, const int* js, const int* je, const int* ks,
+                  const int* ke, const int* is0, const int* ie0, const int* js0, const int* je0,
+                  const int* ks0, const int* ke0, const int* is1, const int* ie1, const int* js1,
+                  const int* je1, const int* ks1, const int* ke1);
 /* sub_init_gridtransformation.f90:27-29 (3-D): metrics, 1/J, alpha/beta/gamma.
  * Ghost-corner nodes (two or more indices in overlap layers) are left as the
  * caller stored them, as in the reference. */

@@ -147,9 +147,10 @@ def run_parity(make, oracle_mod, gpu, nsteps, seed=0, check_every=1):
         r = float(np.max(np.abs(hg[0, :5] - ho[0, :5]) / np.maximum(np.abs(ho[0, :5]), 1e-300)))
         assert r <= 1e-10, f"step {s}: residual history differs by {r}"
         if (s + 1) % check_every == 0 or s == nsteps - 1:
-            gc.sync_to_host(gpu.mask("q", "pri_v", "dt", "rhs"))
+            names = ("q", "pri_v", "dt", "rhs") + (("nut", "sa_rhs", "amu") if co.cfg.turbulence else ())
+            gc.sync_to_host(gpu.mask(*names))
             for bo, bg in zip(co.blocks, cg.blocks):
-                for k in ("q", "pri_v", "dt", "rhs"):
+                for k in names:
                     e = relerr(bg.fields[k], bo.fields[k])
                     worst = max(worst, e)
                     assert e <= TOL, f"step {s}, block {bo.m}, {k}: {e}"
@@ -214,4 +215,62 @@ def test_geometry_matches_oracle(gpu, oracle_mod, make):
             if k in ("spacing", "dist"):  # the oracle writes physical nodes only
                 a, b = a[bg.sl(bg.box0)], b[bo.sl(bo.box0)]
             assert relerr(a, b) <= TOL, (bo.m, k, relerr(a, b))
+    gc.close()
+
+
+# ------------------------------------------------------------ Spalart-Allmaras
+def plate_small():
+    return grids.flat_plate(ni=33, nj=25, nk=9, dy_wall=1e-4, cfg=Config(
+        solver=IFLAG_NSSOLVER, turbulence=2, ma=0.2, re=1.0e5, cfl=2.0, nutinf=3.0))
+
+
+def test_sa_model_transient(gpu, oracle_mod):
+    """sa_model through the drop-in entry point on one block of the plate."""
+    oc, co, cg = prepared(plate_small, oracle_mod, seed=11)
+    oc.iterate(1)  # realistic vor, amu, dt from one iteration
+    gc = gpu.GpuCase(cg)
+    b = co.blocks[1]
+    F = b.fields
+    f = {k: v.copy() for k, v in F.items()}
+    c = co.cfg
+    ob = oracle_mod.box_args
+    names = ("nut", "sa_rhs", "dt", "pri_v", "amu", "dudx", "vor", "dxidx", "inv_j", "alpha", "beta",
+             "ggamma", "length", "dist", "spacing")
+    assert gc.L.aero_sa_model(*[_p(f[k]) for k in names], _d(c.re), _d(c.cfl),
+                              *[_i(v) for v in b.box + b.box0 + b.box1]) == 0
+    oc.L.oracle_sa_model(*[_p(F[k]) for k in names], _d(c.re), _d(c.cfl), *ob(b.box), *ob(b.box0), *ob(b.box1))
+    for k in ("sa_rhs", "nut"):
+        assert relerr(f[k], F[k]) <= TOL, (k, relerr(f[k], F[k]))
+    gc.close()
+
+
+def test_flat_plate_sa_iterations(gpu, oracle_mod):
+    """SA RANS, 2x2x2 blocks: edge/corner interfaces, wall + symmetry on one
+    face row, farfield, SA clip and eddy viscosity."""
+    run_parity(plate_small, oracle_mod, gpu, nsteps=4)
+
+
+@pytest.mark.parametrize("make,nsteps", [(lambda: grids.naca_ogrid(), 12), (plate_small, 6)])
+def test_device_setup_flow_matches_oracle(gpu, oracle_mod, make, nsteps):
+    """The flow bench.py uses end to end: geometry computed on the GPU,
+    freestream initialisation and start-up on the GPU, then iterations; the
+    residual history and final state match the oracle's own set-up."""
+    co, cg = make(), make()
+    oc = oracle_mod.OracleCase(co)
+    oc.geometry()
+    oc.init_flowfield()
+    oc.start()
+    ho = oc.iterate(nsteps)
+    gc = gpu.GpuCase(cg)
+    gc.compute_geometry()
+    gc.init_flowfield()
+    gc.start()
+    hg = gc.step(nsteps)
+    assert np.all(np.isfinite(ho)) and np.all(np.isfinite(hg))
+    r = np.max(np.abs(hg[:, :6] - ho[:, :6]) / np.maximum(np.abs(ho[:, :6]), 1e-300))
+    assert r <= 1e-10, r
+    gc.sync_to_host(gpu.mask("q"))
+    for bo, bg in zip(co.blocks, cg.blocks):
+        assert relerr(bg.fields["q"], bo.fields["q"]) <= TOL
+    assert gc.status() == 0
     gc.close()
