@@ -52,87 +52,86 @@ __device__ __forceinline__ void unit_normal(const BlockView& B, long n, int dir,
   }
 }
 
-// sub_bc.f90:26-62: one CTA per block walks its subfaces in bcinfo order (later
-// subfaces overwrite shared edge nodes and read what earlier ones wrote, as in
-// the serial reference); the nodes of one subface are independent.
+// sub_bc.f90:26-62 for the o-th subface of every block (launched once per
+// subface index o, in bcinfo order, so a later subface overwrites shared edge
+// nodes and reads what an earlier one wrote, as in the serial reference).
+// The nodes of one subface are independent and spread over the grid's x.
 __global__ void k_physical_bc(const BlockView* __restrict__ blocks, const BcOp* __restrict__ ops,
-                              const int* __restrict__ op_start, CaseConsts cc) {
-  const BlockView& B = blocks[blockIdx.x];
+                              const int* __restrict__ op_start, int o, CaseConsts cc) {
+  const BlockView& B = blocks[blockIdx.y];
+  int idx = op_start[blockIdx.y] + o;
+  if (idx >= op_start[blockIdx.y + 1]) return;
+  const BcOp op = ops[idx];
   bool tur = cc.turbulence >= 1;
   double gamma = cc.gamma;
-  for (int o = op_start[blockIdx.x]; o < op_start[blockIdx.x + 1]; ++o) {
-    BcOp op = ops[o];
-    for (long t = threadIdx.x;; t += blockDim.x) {
-      int i, j, k, di, dj, dk, s;
-      if (!bc_node(op, t, i, j, k, di, dj, dk, s)) break;
-      long n = B.at(i, j, k);
-      long st = di ? 1 : (dj ? (long)B.nx : (long)B.nx * B.ny);
-      long n1 = n + s * st;
-      int dir = di ? 0 : (dj ? 1 : 2);
-      if (op.type == BCT_INFLOW) {  // sub_bc_-50_inflow.f90:21-40
-        B.v(F_Q, 1, n) = cc.d_0;
-        B.v(F_Q, 2, n) = cc.d_0 * cc.u_0 * cos(cc.aoa);
-        B.v(F_Q, 3, n) = cc.d_0 * cc.u_0 * sin(cc.aoa);
-        B.v(F_Q, 4, n) = 0.0;
-        B.v(F_Q, 5, n) = cc.p_0 / (gamma - 1.0) + 0.5 * p2(cc.u_0);
-        if (tur) B.s(F_NUT, n) = cc.nutinf;
-      } else if (op.type == BCT_OUTFLOW) {  // sub_bc_-40_outflow.f90:21-35
-        for (int c = 1; c <= 5; ++c) B.v(F_Q, c, n) = B.v(F_Q, c, n1);
-        if (tur) B.s(F_NUT, n) = B.s(F_NUT, n1);
-      } else if (op.type == BCT_MIRROR) {  // symmetry plane or slip wall
-        double x0, y0, z0;
-        unit_normal(B, n, dir, s, x0, y0, z0);
-        double cu = B.v(F_Q, 2, n1) * x0 + B.v(F_Q, 3, n1) * y0 + B.v(F_Q, 4, n1) * z0;
-        B.v(F_Q, 1, n) = B.v(F_Q, 1, n1);
-        B.v(F_Q, 2, n) = B.v(F_Q, 2, n1) - cu * x0;
-        B.v(F_Q, 3, n) = B.v(F_Q, 3, n1) - cu * y0;
-        B.v(F_Q, 4, n) = B.v(F_Q, 4, n1) - cu * z0;
-        B.v(F_Q, 5, n) = B.v(F_Q, 5, n1);
-        if (tur) B.s(F_NUT, n) = B.s(F_NUT, n1);
-      } else if (op.type == BCT_NOSLIP) {  // no-slip (sub_bc_-20_solidwall.f90:225-240)
-        long n2 = n + 2 * s * st, n3 = n + 3 * s * st;
-        B.v(F_Q, 1, n) = (11.0 * B.v(F_Q, 1, n1) - 7.0 * B.v(F_Q, 1, n2) + 2.0 * B.v(F_Q, 1, n3)) / 6.0;
-        B.v(F_Q, 2, n) = 0.0;
-        B.v(F_Q, 3, n) = 0.0;
-        B.v(F_Q, 4, n) = 0.0;
-        B.v(F_Q, 5, n) = (11.0 * B.v(F_Q, 5, n1) - 7.0 * B.v(F_Q, 5, n2) + 2.0 * B.v(F_Q, 5, n3)) / 6.0;
-        if (tur) B.s(F_NUT, n) = 0.0;
-      } else if (op.type == BCT_FARFIELD) {  // sub_bc_-10_farfield.f90:30-106
-        double u_inf = cc.u_0 * cos(cc.aoa), v_inf = cc.u_0 * sin(cc.aoa), w_inf = 0.0;
-        double s_inf = cc.p_0 / pow(cc.d_0, gamma);
-        double c_inf = cc.c_0;
-        double x0, y0, z0;
-        unit_normal(B, n, dir, s, x0, y0, z0);
-        double d_p = B.v(F_Q, 1, n1);
-        double u_p = B.v(F_Q, 2, n1) / d_p;
-        double v_p = B.v(F_Q, 3, n1) / d_p;
-        double w_p = B.v(F_Q, 4, n1) / d_p;
-        double p_p = (B.v(F_Q, 5, n1) - 0.5 * d_p * (p2(u_p) + p2(v_p) + p2(w_p))) * (gamma - 1.0);
-        double c_p = sqrt(gamma * p_p / d_p);
-        double s_p = p_p / pow(d_p, gamma);
-        double vn_inf = u_inf * x0 + v_inf * y0 + w_inf * z0;
-        double vn_p = u_p * x0 + v_p * y0 + w_p * z0;
-        double rm = vn_inf - 2.0 * c_inf / (gamma - 1.0);
-        double rp = vn_p + 2.0 * c_p / (gamma - 1.0);
-        double vn_b = 0.5 * (rp + rm);
-        double s_b = 0, u_ref = 0, v_ref = 0, w_ref = 0, turVal = 0;
-        if (vn_b < 0.0) { s_b = s_inf; u_ref = u_inf; v_ref = v_inf; w_ref = w_inf; turVal = cc.nutinf; }
-        if (vn_b >= 0.0) { s_b = s_p; u_ref = u_p; v_ref = v_p; w_ref = w_p; turVal = tur ? B.s(F_NUT, n1) : 0.0; }
-        double u_ref_t = u_ref * x0 + v_ref * y0 + w_ref * z0;
-        double u_b = u_ref + (vn_b - u_ref_t) * x0;
-        double v_b = v_ref + (vn_b - u_ref_t) * y0;
-        double w_b = w_ref + (vn_b - u_ref_t) * z0;
-        double d_b = pow(c_p * c_p / (gamma * s_b), 1.0 / (gamma - 1.0));
-        double p_b = s_b * pow(d_b, gamma);
-        B.v(F_Q, 1, n) = d_b;
-        B.v(F_Q, 2, n) = d_b * u_b;
-        B.v(F_Q, 3, n) = d_b * v_b;
-        B.v(F_Q, 4, n) = d_b * w_b;
-        B.v(F_Q, 5, n) = p_b / (gamma - 1.0) + 0.5 * d_b * (p2(u_b) + p2(v_b) + p2(w_b));
-        if (tur) B.s(F_NUT, n) = turVal;
-      }
-    }
-    __syncthreads();
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, k, di, dj, dk, s;
+  if (!bc_node(op, t, i, j, k, di, dj, dk, s)) return;
+  long n = B.at(i, j, k);
+  long st = di ? 1 : (dj ? (long)B.nx : (long)B.nx * B.ny);
+  long n1 = n + s * st;
+  int dir = di ? 0 : (dj ? 1 : 2);
+  if (op.type == BCT_INFLOW) {  // sub_bc_-50_inflow.f90:21-40
+    B.v(F_Q, 1, n) = cc.d_0;
+    B.v(F_Q, 2, n) = cc.d_0 * cc.u_0 * cos(cc.aoa);
+    B.v(F_Q, 3, n) = cc.d_0 * cc.u_0 * sin(cc.aoa);
+    B.v(F_Q, 4, n) = 0.0;
+    B.v(F_Q, 5, n) = cc.p_0 / (gamma - 1.0) + 0.5 * p2(cc.u_0);
+    if (tur) B.s(F_NUT, n) = cc.nutinf;
+  } else if (op.type == BCT_OUTFLOW) {  // sub_bc_-40_outflow.f90:21-35
+    for (int c = 1; c <= 5; ++c) B.v(F_Q, c, n) = B.v(F_Q, c, n1);
+    if (tur) B.s(F_NUT, n) = B.s(F_NUT, n1);
+  } else if (op.type == BCT_MIRROR) {  // symmetry plane or slip wall
+    double x0, y0, z0;
+    unit_normal(B, n, dir, s, x0, y0, z0);
+    double cu = B.v(F_Q, 2, n1) * x0 + B.v(F_Q, 3, n1) * y0 + B.v(F_Q, 4, n1) * z0;
+    B.v(F_Q, 1, n) = B.v(F_Q, 1, n1);
+    B.v(F_Q, 2, n) = B.v(F_Q, 2, n1) - cu * x0;
+    B.v(F_Q, 3, n) = B.v(F_Q, 3, n1) - cu * y0;
+    B.v(F_Q, 4, n) = B.v(F_Q, 4, n1) - cu * z0;
+    B.v(F_Q, 5, n) = B.v(F_Q, 5, n1);
+    if (tur) B.s(F_NUT, n) = B.s(F_NUT, n1);
+  } else if (op.type == BCT_NOSLIP) {  // no-slip (sub_bc_-20_solidwall.f90:225-240)
+    long n2 = n + 2 * s * st, n3 = n + 3 * s * st;
+    B.v(F_Q, 1, n) = (11.0 * B.v(F_Q, 1, n1) - 7.0 * B.v(F_Q, 1, n2) + 2.0 * B.v(F_Q, 1, n3)) / 6.0;
+    B.v(F_Q, 2, n) = 0.0;
+    B.v(F_Q, 3, n) = 0.0;
+    B.v(F_Q, 4, n) = 0.0;
+    B.v(F_Q, 5, n) = (11.0 * B.v(F_Q, 5, n1) - 7.0 * B.v(F_Q, 5, n2) + 2.0 * B.v(F_Q, 5, n3)) / 6.0;
+    if (tur) B.s(F_NUT, n) = 0.0;
+  } else if (op.type == BCT_FARFIELD) {  // sub_bc_-10_farfield.f90:30-106
+    double u_inf = cc.u_0 * cos(cc.aoa), v_inf = cc.u_0 * sin(cc.aoa), w_inf = 0.0;
+    double s_inf = cc.p_0 / pow(cc.d_0, gamma);
+    double c_inf = cc.c_0;
+    double x0, y0, z0;
+    unit_normal(B, n, dir, s, x0, y0, z0);
+    double d_p = B.v(F_Q, 1, n1);
+    double u_p = B.v(F_Q, 2, n1) / d_p;
+    double v_p = B.v(F_Q, 3, n1) / d_p;
+    double w_p = B.v(F_Q, 4, n1) / d_p;
+    double p_p = (B.v(F_Q, 5, n1) - 0.5 * d_p * (p2(u_p) + p2(v_p) + p2(w_p))) * (gamma - 1.0);
+    double c_p = sqrt(gamma * p_p / d_p);
+    double s_p = p_p / pow(d_p, gamma);
+    double vn_inf = u_inf * x0 + v_inf * y0 + w_inf * z0;
+    double vn_p = u_p * x0 + v_p * y0 + w_p * z0;
+    double rm = vn_inf - 2.0 * c_inf / (gamma - 1.0);
+    double rp = vn_p + 2.0 * c_p / (gamma - 1.0);
+    double vn_b = 0.5 * (rp + rm);
+    double s_b = 0, u_ref = 0, v_ref = 0, w_ref = 0, turVal = 0;
+    if (vn_b < 0.0) { s_b = s_inf; u_ref = u_inf; v_ref = v_inf; w_ref = w_inf; turVal = cc.nutinf; }
+    if (vn_b >= 0.0) { s_b = s_p; u_ref = u_p; v_ref = v_p; w_ref = w_p; turVal = tur ? B.s(F_NUT, n1) : 0.0; }
+    double u_ref_t = u_ref * x0 + v_ref * y0 + w_ref * z0;
+    double u_b = u_ref + (vn_b - u_ref_t) * x0;
+    double v_b = v_ref + (vn_b - u_ref_t) * y0;
+    double w_b = w_ref + (vn_b - u_ref_t) * z0;
+    double d_b = pow(c_p * c_p / (gamma * s_b), 1.0 / (gamma - 1.0));
+    double p_b = s_b * pow(d_b, gamma);
+    B.v(F_Q, 1, n) = d_b;
+    B.v(F_Q, 2, n) = d_b * u_b;
+    B.v(F_Q, 3, n) = d_b * v_b;
+    B.v(F_Q, 4, n) = d_b * w_b;
+    B.v(F_Q, 5, n) = p_b / (gamma - 1.0) + 0.5 * d_b * (p2(u_b) + p2(v_b) + p2(w_b));
+    if (tur) B.s(F_NUT, n) = turVal;
   }
 }
 

@@ -158,38 +158,47 @@ __device__ __forceinline__ void face_flux(const BlockView& B, int coord, long n,
   roe_face(B, coord, n, n + st, ulc, urc, gamma, flux);
 }
 
-// sub_inviscid1.f90:8-189: rhsi on the updated nodes, one thread per node.
-// Directions are accumulated in the reference's order: rhsi = -dF; rhsi -= dG;
-// rhsi -= dH.
+// sub_inviscid1.f90:8-189: rhsi on the updated nodes.  A CTA covers kInvTile
+// nodes x 3 directions; thread (x, d) computes the flux difference of
+// direction d at its node (both faces), and the three differences are
+// combined in the reference's order: rhsi = -dF; rhsi -= dG; rhsi -= dH.
 __global__ void k_inviscid(const BlockView* __restrict__ blocks, CaseConsts cc) {
   const BlockView& B = blocks[blockIdx.y];
   const Box& b1 = B.b1;
-  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  __shared__ double dsm[3][5][kInvTile];
+  long t = (long)blockIdx.x * kInvTile + threadIdx.x;
   long N1 = b1.size();
-  if (t >= N1) return;
-  int i = b1.is + (int)(t % b1.nx());
-  long r = t / b1.nx();
-  int j = b1.js + (int)(r % b1.ny());
-  int k = b1.ks + (int)(r / b1.ny());
-  long n = B.at(i, j, k);
-  const long st[3] = {1, (long)B.nx, (long)B.nx * B.ny};
-  const int pos[3] = {i, j, k};
-  const int lo[3] = {B.b.is, B.b.js, B.b.ks};
-  const int hi[3] = {B.b.ie, B.b.je, B.b.ke};
-  double acc[5];
+  int d = threadIdx.y;
   int ndir = cc.dimension == IFLAG_3D ? 3 : 2;
-  for (int d = 0; d < ndir; ++d) {
-    double fm[5], fp[5];
-    face_flux(B, d + 1, n - st[d], pos[d] - 1, lo[d], hi[d], st[d], cc.gamma, fm);
-    face_flux(B, d + 1, n, pos[d], lo[d], hi[d], st[d], cc.gamma, fp);
+  long n = 0;
+  if (t < N1) {
+    int i = b1.is + (int)(t % b1.nx());
+    long r = t / b1.nx();
+    int j = b1.js + (int)(r % b1.ny());
+    int k = b1.ks + (int)(r / b1.ny());
+    n = B.at(i, j, k);
+    if (d < ndir) {
+      const long st = d == 0 ? 1 : (d == 1 ? (long)B.nx : (long)B.nx * B.ny);
+      const int pos = d == 0 ? i : (d == 1 ? j : k);
+      const int lo = d == 0 ? B.b.is : (d == 1 ? B.b.js : B.b.ks);
+      const int hi = d == 0 ? B.b.ie : (d == 1 ? B.b.je : B.b.ke);
+      double fm[5], fp[5];
+      face_flux(B, d + 1, n - st, pos - 1, lo, hi, st, cc.gamma, fm);
+      face_flux(B, d + 1, n, pos, lo, hi, st, cc.gamma, fp);
 #pragma unroll
-    for (int c = 0; c < 5; ++c) {
-      double dd = fp[c] - fm[c];
-      acc[c] = (d == 0) ? -dd : acc[c] - dd;
+      for (int c = 0; c < 5; ++c) dsm[d][c][threadIdx.x] = fp[c] - fm[c];
     }
   }
+  __syncthreads();
+  if (d == 0 && t < N1) {
 #pragma unroll
-  for (int c = 0; c < 5; ++c) B.v(F_RHSI, c + 1, n) = acc[c];
+    for (int c = 0; c < 5; ++c) {
+      double acc = -dsm[0][c][threadIdx.x];
+      acc = acc - dsm[1][c][threadIdx.x];
+      if (ndir == 3) acc = acc - dsm[2][c][threadIdx.x];
+      B.v(F_RHSI, c + 1, n) = acc;
+    }
+  }
 }
 
 // Zero-fills one field over the full box of every block (the reference's

@@ -313,9 +313,10 @@ __device__ __forceinline__ void lusgs_sweep(const BlockView* __restrict__ blocks
       if (!fwd) bulk_g2s(stg + P * (kRec + 8), B.dqs + 8 * base, cnt * 64u, bar);
     };
     if (STAGED && threadIdx.x == 0) {
-      // earlier generic writes (dq* of the forward pass, reads of the stages)
-      // are ordered before the async-proxy copies
-      asm volatile("fence.proxy.async;" ::: "memory");
+      // the generic reads of the stage buffers are ordered before the
+      // async-proxy writes into them (the dq* stores of the forward pass are
+      // fenced for the async proxy by every thread at the end of that pass)
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       for (int st = 0; st < nst && st < H; ++st) issue(st);
     }
     for (int st = 0; st < H; ++st) {
@@ -376,7 +377,7 @@ __device__ __forceinline__ void lusgs_sweep(const BlockView* __restrict__ blocks
         return;
       }
       if (STAGED && threadIdx.x == 0 && st + nst < H) {
-        asm volatile("fence.proxy.async;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         issue(st + nst);
       }
     }

@@ -34,6 +34,7 @@ struct AvgDst {
 
 __global__ void k_getpri(const BlockView* __restrict__ blocks, CaseConsts cc, unsigned* status);
 __global__ void k_fill(const BlockView* __restrict__ blocks, int fid, int nc, double val);
+constexpr int kInvTile = 64;  // nodes per CTA of k_inviscid (x 3 directions)
 __global__ void k_inviscid(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_viscous_a(const BlockView* __restrict__ blocks, CaseConsts cc, int store_dudx_tao);
 __global__ void k_viscous_b(const BlockView* __restrict__ blocks, CaseConsts cc);
@@ -52,7 +53,7 @@ __global__ void k_lusgs_sweep_staged(const BlockView* __restrict__ blocks, int n
 __global__ void k_lusgs_sweep_global(const BlockView* __restrict__ blocks, int nst, unsigned* status);
 __global__ void k_lusgs_update(const BlockView* __restrict__ blocks);
 __global__ void k_physical_bc(const BlockView* __restrict__ blocks, const BcOp* __restrict__ ops,
-                              const int* __restrict__ op_start, CaseConsts cc);
+                              const int* __restrict__ op_start, int o, CaseConsts cc);
 __global__ void k_sa_clip(const BlockView* __restrict__ blocks);
 __global__ void k_halo(const BlockView* __restrict__ blocks, const HaloEntry* __restrict__ map,
                        long nmap, int mode);

@@ -87,6 +87,8 @@ struct State {
   size_t staging_doubles = 0;
   double totalnodes = 0;
   long max_box = 0, max_b0 = 0, max_b1 = 0, max_ext = 0;
+  int max_ops = 0;       // most physical-BC subfaces in one block
+  long max_face = 0;     // most nodes in one physical-BC subface
   std::map<const double*, std::pair<int, int>> registry;  // host array -> (block, field)
   // transient mode pool
   double* t_arena = nullptr;
@@ -398,7 +400,7 @@ int launch_getpri(const BlockView* views, int nblk, long maxN, const CaseConsts&
 int launch_inviscid(const BlockView* views, int nblk, long maxN, long maxN1, const CaseConsts& cc) {
   PROF(P_FILL, (k_fill<<<dim3(cdiv(maxN, 256), nblk), 256, 0, g.stream>>>(views, F_RHSI, 5, 0.0)));
   CKL();
-  PROF(P_INVISCID, (k_inviscid<<<dim3(cdiv(maxN1, 128), nblk), 128, 0, g.stream>>>(views, cc)));
+  PROF(P_INVISCID, (k_inviscid<<<dim3(cdiv(maxN1, kInvTile), nblk), dim3(kInvTile, 3), 0, g.stream>>>(views, cc)));
   CKL();
   return AERO_OK;
 }
@@ -483,8 +485,11 @@ bool sa_on() { return g.cc.turbulence == IFLAG_SA && g.cc.solver == IFLAG_NSSOLV
 
 int do_physical_bc() {
   int nb = (int)g.blocks.size();
-  PROF(P_BC, (k_physical_bc<<<nb, 256, 0, g.stream>>>(g.d_blocks, g.d_bc_ops, g.d_bc_start, g.cc)));
-  CKL();
+  for (int o = 0; o < g.max_ops; ++o) {
+    PROF(P_BC, (k_physical_bc<<<dim3(cdiv(g.max_face, 128), nb), 128, 0, g.stream>>>(
+                    g.d_blocks, g.d_bc_ops, g.d_bc_start, o, g.cc)));
+    CKL();
+  }
   if (sa_on()) {
     PROF(P_SA_CLIP, (k_sa_clip<<<dim3(cdiv(g.max_box, 256), nb), 256, 0, g.stream>>>(g.d_blocks)));
     CKL();
@@ -746,6 +751,15 @@ int aero_finish_setup(void) {
   CK(cudaMalloc(&g.d_blocks, nb * sizeof(BlockView)));
   CK(cudaMemcpyAsync(g.d_blocks, g.views.data(), nb * sizeof(BlockView), cudaMemcpyHostToDevice, g.stream));
   // tables
+  g.max_ops = 0;
+  g.max_face = 1;
+  for (int m = 0; m < nb; ++m) g.max_ops = std::max(g.max_ops, topo.bc_start[m + 1] - topo.bc_start[m]);
+  for (const BcOp& op : topo.bc_ops) {
+    int dir = (op.face - 1) / 2;
+    long n = dir == 0 ? (long)op.sb.ny() * op.sb.nz() : dir == 1 ? (long)op.sb.nx() * op.sb.nz()
+                                                                  : (long)op.sb.nx() * op.sb.ny();
+    g.max_face = std::max(g.max_face, n);
+  }
   CK(cudaMalloc(&g.d_bc_ops, std::max<size_t>(1, topo.bc_ops.size()) * sizeof(BcOp)));
   CK(cudaMalloc(&g.d_bc_start, topo.bc_start.size() * sizeof(int)));
   if (!topo.bc_ops.empty())

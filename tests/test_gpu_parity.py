@@ -267,7 +267,13 @@ def test_device_setup_flow_matches_oracle(gpu, oracle_mod, make, nsteps):
     gc.start()
     hg = gc.step(nsteps)
     assert np.all(np.isfinite(ho)) and np.all(np.isfinite(hg))
-    r = np.max(np.abs(hg[:, :6] - ho[:, :6]) / np.maximum(np.abs(ho[:, :6]), 1e-300))
+    # The GPU computes the freestream with its own cos/sin, which may differ from
+    # the host libm by an ulp.  A component whose residual is round-off (rho*w on
+    # a quasi-2D grid, ~1e-18 against ~1e-2) then differs by O(1e-7) relative,
+    # as the oracle itself does under a 1-ulp change of the angle of attack, so
+    # each row is compared against its largest component with a 1e-10 bound.
+    scale = np.maximum(np.abs(ho[:, :6]), 1e-6 * np.max(np.abs(ho[:, :5]), axis=1, keepdims=True))
+    r = np.max(np.abs(hg[:, :6] - ho[:, :6]) / scale)
     assert r <= 1e-10, r
     gc.sync_to_host(gpu.mask("q"))
     for bo, bg in zip(co.blocks, cg.blocks):
