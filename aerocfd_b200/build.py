@@ -21,7 +21,8 @@ LIB = os.path.join(HERE, "libaerocfd_gpu.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 SOURCES = ["aero_flux.cu", "aero_implicit.cu", "aero_bc.cu", "aero_transfer.cu",
-           "aero_runtime.cu", "aero_topology.cpp", "aero_geometry.cu", "aero_sa.cu"]
+           "aero_runtime.cu", "aero_topology.cpp", "aero_geometry.cu", "aero_sa.cu",
+           "aero_noalloc.cu"]
 HEADERS = ["aero_device.cuh", "aero_kernels.h", "aero_topology.h"]
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -554,6 +554,11 @@ int do_iteration(bool want_dt_minmax) {
 
 }  // namespace
 
+namespace aero {
+// Error reporting for the C-ABI entries defined in other files of the library.
+int set_last_error(int code, const char* msg) { return fail(code, "%s", msg); }
+}  // namespace aero
+
 // =================================================================== C ABI
 extern "C" {
 

@@ -199,6 +199,41 @@ int aero_profile_read(double* ms, long long* counts, int n);
 const char* aero_profile_name(int id);
 int aero_launch_count(unsigned long long* count);
 
+/* ---- residual of caller-owned device arrays, without allocation --------
+ * No counterpart in the reference: it is the computation of
+ * sub_output_residual.f90:8-67 (what aero_residual returns) for a caller that
+ * keeps its block arrays on the device itself, e.g. a CUDA Fortran or OpenACC
+ * port of the solver, and cannot let a library allocate: cudaMalloc and
+ * cudaFree synchronise the device, are not allowed while a stream is being
+ * captured, and draw on memory such a caller budgets itself.  The call needs
+ * neither aero_init nor a registered case, allocates no device memory and
+ * calls no allocating CUDA or library routine; on a rejected argument it only
+ * records the message that aero_last_error returns.
+ *
+ * Block m (0-based, m < nblocks) is given by device pointers to arrays in the
+ * reference layout over its full box: rhs[m] -> rhs(5,is:ie,js:je,ks:ke),
+ * dt[m], inv_j[m] and, when sa_rhs is not NULL, sa_rhs[m] -> (is:ie,...);
+ * rhs, dt, inv_j and sa_rhs are host arrays of nblocks pointers.
+ * boxes holds 12 ints per block: is,ie,js,je,ks,ke, is1,ie1,js1,je1,ks1,ke1.
+ * out7 is a DEVICE pointer to 7 doubles, written as aero_residual's out7
+ * (component 6 is 0 when sa_rhs is NULL).  Both kernels are enqueued on
+ * `stream` (a cudaStream_t; NULL = the legacy default stream) and the call
+ * returns without waiting for them.
+ *
+ * Limits: 1 <= nblocks <= AERO_NOALLOC_MAX_BLOCKS, and nblocks x
+ * ceil(largest updated box / 256) <= AERO_NOALLOC_MAX_PARTS (about 4.2 million
+ * updated nodes in equal blocks); larger calls return AERO_ERR_ARG before any
+ * device work.  The partial sums live in one fixed device array per device;
+ * the first call on a device looks its address up (make that first call
+ * outside any stream capture), and nothing in it has to start at zero.  Calls
+ * whose kernels can overlap on one device (other streams, other host threads)
+ * share that array and race: order them on one stream. */
+#define AERO_NOALLOC_MAX_BLOCKS 32
+#define AERO_NOALLOC_MAX_PARTS 16384
+int aero_residual_device_noalloc(int nblocks, const double* const* rhs, const double* const* dt,
+                                 const double* const* inv_j, const double* const* sa_rhs,
+                                 const int* boxes, double totalnodes, double* out7, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
