@@ -65,9 +65,11 @@ struct BlockView {
   __device__ __forceinline__ double& s(int fid, long n) const { return f[fid][n]; }
 };
 
-// LU-SGS record stride: three 5x5 blocks (75 doubles) padded to 608 bytes so
-// every record starts on a 16-byte boundary (bulk-copy alignment).
+// LU-SGS record stride: three 5x5 blocks (75 doubles) plus the packed
+// neighbour positions, 608 bytes (bulk-copy alignment: multiples of 16).
 constexpr int kRec = 76;
+// LU-SGS per-node scalars: rhs(5), diag, inv_j, 1/diag, 1/inv_j, unused.
+constexpr int kSca = 10;
 
 // Per-case scalars (module ns_const / flag_var values the path reads).
 struct CaseConsts {
@@ -82,6 +84,27 @@ __device__ __forceinline__ double p2(double x) { return x * x; }
 __device__ __forceinline__ double p3(double x) { double x2 = x * x; return x2 * x; }
 __device__ __forceinline__ double p5(double x) { double x2 = x * x; double x3 = x2 * x; return x3 * x2; }
 __device__ __forceinline__ double p6(double x) { double x2 = x * x; double x3 = x2 * x; return x3 * x3; }
+
+// a / b rounded to nearest, given rb = 1/b rounded to nearest: Markstein's
+// correction (P. Markstein, IBM J. Res. Dev. 34(1), 1990, Theorem 1: with rb
+// correctly rounded and q within one ulp of a/b, q + (a - b*q)*rb rounded once
+// is the correctly rounded quotient).  The first correction makes a*rb
+// faithful, the second rounds it correctly; each remainder a - b*q is exact
+// in one fma.  The theorem needs normal operands and quotient with room for the
+// remainder, so values outside [2^-960, 2^960] (and a = 0, whose sign the
+// corrections would lose) take the IEEE division.  The result is bit-identical
+// to a / b.
+__device__ __forceinline__ double div_rn(double a, double b, double rb) {
+  double q = a * rb;
+  double r = fma(-q, b, a);
+  q = fma(r, rb, q);
+  r = fma(-q, b, a);
+  q = fma(r, rb, q);
+  double aa = fabs(a), ab = fabs(b), aq = fabs(q);
+  if (!(aa > 0x1p-960 && aa < 0x1p960 && ab > 0x1p-960 && ab < 0x1p960 && aq > 0x1p-960 && aq < 0x1p960))
+    q = a / b;
+  return q;
+}
 
 // Spalart-Allmaras constants (module_tursa.f90:4-10).
 constexpr double SA_DTA = 2.0 / 3.0, SA_KAR = 0.41;

@@ -158,11 +158,108 @@ __device__ __forceinline__ void face_flux(const BlockView& B, int coord, long n,
   roe_face(B, coord, n, n + st, ulc, urc, gamma, flux);
 }
 
-// sub_inviscid1.f90:8-189: rhsi on the updated nodes.  A CTA covers kInvTile
-// nodes x 3 directions; thread (x, d) computes the flux difference of
-// direction d at its node (both faces), and the three differences are
-// combined in the reference's order: rhsi = -dF; rhsi -= dG; rhsi -= dH.
-__global__ void k_inviscid(const BlockView* __restrict__ blocks, CaseConsts cc) {
+// ------------------------------------------------ inviscid flux, mixed precision
+// The same face flux with FP32 arithmetic where it only forms increments:
+// the WENO3 states are written as the centre value (FP64) plus a correction
+// w1*(u2-u1)/2 + w2*(u3-u2)/2 evaluated in FP32 from FP64 differences, and the
+// Roe flux as the FP64 central part 0.5*(F_L + F_R) minus the FP32 dissipation
+// 0.5*|grad xi/J|*|A|*dU, whose inputs are FP64 differences.  Near a
+// converged state every FP32 term is proportional to a jump, so its rounding
+// error shrinks with the residual instead of setting a floor.
+__device__ __forceinline__ double weno_corr(double um, double u0, double up) {
+  // the reference's left state weno_left(um, u0, up) =
+  //   w1*(-um/2 + 3u0/2) + w2*(u0/2 + up/2) = u0 + w1*(u0-um)/2 + w2*(up-u0)/2
+  const float eps = 1.0e-6f;
+  float d1 = (float)(u0 - um), d2 = (float)(up - u0);
+  float a1 = 1.0f / (3.0f * (eps + d1 * d1) * (eps + d1 * d1));
+  float a2 = 2.0f / (3.0f * (eps + d2 * d2) * (eps + d2 * d2));
+  float w1 = a1 / (a1 + a2), w2 = a2 / (a1 + a2);
+  return (double)(0.5f * (w1 * d1 + w2 * d2));
+}
+
+__device__ __forceinline__ void roe_face_mixed(const BlockView& B, int coord, long n, long ns,
+                                               const double ulc[5], const double urc[5], double gamma,
+                                               double flux[5]) {
+  double dl = ulc[0], ul = ulc[1] / ulc[0], vl = ulc[2] / ulc[0], wl = ulc[3] / ulc[0];
+  double pl = (ulc[4] - 0.5 * (p2(ulc[1]) + p2(ulc[2]) + p2(ulc[3])) / ulc[0]) * (gamma - 1.0);
+  double dr = urc[0], ur = urc[1] / urc[0], vr = urc[2] / urc[0], wr = urc[3] / urc[0];
+  double pr = (urc[4] - 0.5 * (p2(urc[1]) + p2(urc[2]) + p2(urc[3])) / urc[0]) * (gamma - 1.0);
+  int c1 = coord * 3 - 2;
+  double ja = B.s(F_INVJ, n), jb = B.s(F_INVJ, ns);
+  double dxidx1 = 0.5 * (B.v(F_DXIDX, c1, n) * ja + B.v(F_DXIDX, c1, ns) * jb);
+  double dxidy1 = 0.5 * (B.v(F_DXIDX, c1 + 1, n) * ja + B.v(F_DXIDX, c1 + 1, ns) * jb);
+  double dxidz1 = 0.5 * (B.v(F_DXIDX, c1 + 2, n) * ja + B.v(F_DXIDX, c1 + 2, ns) * jb);
+  double hl = gamma * pl / ((gamma - 1.0) * dl) + 0.5 * (p2(ul) + p2(vl) + p2(wl));
+  double hr = gamma * pr / ((gamma - 1.0) * dr) + 0.5 * (p2(ur) + p2(vr) + p2(wr));
+  double uul = ul * dxidx1 + vl * dxidy1 + wl * dxidz1;
+  double uur = ur * dxidx1 + vr * dxidy1 + wr * dxidz1;
+  // central part (FP64)
+  double fc[5];
+  fc[0] = dl * uul + dr * uur;
+  fc[1] = dl * ul * uul + dxidx1 * pl + (dr * ur * uur + dxidx1 * pr);
+  fc[2] = dl * vl * uul + dxidy1 * pl + (dr * vr * uur + dxidy1 * pr);
+  fc[3] = dl * wl * uul + dxidz1 * pl + (dr * wr * uur + dxidz1 * pr);
+  fc[4] = dl * hl * uul + dr * hr * uur;
+  // dissipation (FP32 on FP64 differences)
+  const float g = (float)gamma;
+  float mx = (float)dxidx1, my = (float)dxidy1, mz = (float)dxidz1;
+  float temp = sqrtf(mx * mx + my * my + mz * mz);
+  float nx = mx / temp, ny = my / temp, nz = mz / temp;
+  float fdl = (float)dl, fdr = (float)dr;
+  float tmpp = sqrtf(fdr / fdl);
+  float avd = sqrtf(fdl * fdr);
+  float inv1 = 1.0f / (1.0f + tmpp);
+  float avu = ((float)ul + (float)ur * tmpp) * inv1;
+  float avv = ((float)vl + (float)vr * tmpp) * inv1;
+  float avw = ((float)wl + (float)wr * tmpp) * inv1;
+  float avh = ((float)hl + (float)hr * tmpp) * inv1;
+  float ava2 = (g - 1.0f) * (avh - 0.5f * (avu * avu + avv * avv + avw * avw));
+  float ava = sqrtf(ava2);
+  float avuu = avu * nx + avv * ny + avw * nz;
+  const float delt = 0.06f;
+  float lam[5] = {fabsf(avuu - ava), fabsf(avuu), fabsf(avuu), fabsf(avuu), fabsf(avuu + ava)};
+#pragma unroll
+  for (int m = 0; m < 5; ++m)  // Harten entropy fix
+    if (lam[m] < delt) lam[m] = (lam[m] * lam[m] + delt * delt) / (2.0f * delt);
+  float deltad = (float)(dr - dl), deltap = (float)(pr - pl);
+  float deltau = (float)(ur - ul), deltav = (float)(vr - vl), deltaw = (float)(wr - wl);
+  float deltauu = (float)(uur - uul) / temp;
+  float alpha1 = lam[1] * (deltad - deltap / ava2);
+  float alpha2 = lam[4] * (deltap + avd * ava * deltauu) / (2.0f * ava2);
+  float alpha3 = lam[0] * (deltap - avd * ava * deltauu) / (2.0f * ava2);
+  float alpha4 = alpha1 + alpha2 + alpha3;
+  float alpha5 = ava * (alpha2 - alpha3);
+  float alpha6 = lam[1] * avd * (deltau - deltauu * nx);
+  float alpha7 = lam[1] * avd * (deltav - deltauu * ny);
+  float alpha8 = lam[1] * avd * (deltaw - deltauu * nz);
+  float fd[5];
+  fd[0] = alpha4;
+  fd[1] = avu * alpha4 + alpha5 * nx + alpha6;
+  fd[2] = avv * alpha4 + alpha5 * ny + alpha7;
+  fd[3] = avw * alpha4 + alpha5 * nz + alpha8;
+  fd[4] = avh * alpha4 + avuu * alpha5 + avu * alpha6 + avv * alpha7 + avw * alpha8 - ava2 * alpha1 / (g - 1.0f);
+#pragma unroll
+  for (int c = 0; c < 5; ++c) flux[c] = 0.5 * fc[c] - (double)(0.5f * temp * fd[c]);
+}
+
+__device__ __forceinline__ void face_flux_mixed(const BlockView& B, int coord, long n, int pos, int lo, int hi,
+                                                long st, double gamma, double flux[5]) {
+  double ulc[5], urc[5];
+  bool rone = (pos == hi - 1);
+  bool lone = (pos == lo);
+#pragma unroll
+  for (int c = 1; c <= 5; ++c) {
+    double f0 = B.v(F_Q, c, n);
+    double fp = B.v(F_Q, c, n + st);
+    // right state = weno_right(f0, fp, fpp) = weno_left(fpp, fp, f0) (mirror)
+    urc[c - 1] = rone ? fp : fp + weno_corr(B.v(F_Q, c, n + 2 * st), fp, f0);
+    ulc[c - 1] = lone ? f0 : f0 + weno_corr(B.v(F_Q, c, n - st), f0, fp);
+  }
+  roe_face_mixed(B, coord, n, n + st, ulc, urc, gamma, flux);
+}
+
+template <bool MIXED>
+__device__ __forceinline__ void inviscid_body(const BlockView* __restrict__ blocks, CaseConsts cc) {
   const BlockView& B = blocks[blockIdx.y];
   const Box& b1 = B.b1;
   __shared__ double dsm[3][5][kInvTile];
@@ -183,8 +280,13 @@ __global__ void k_inviscid(const BlockView* __restrict__ blocks, CaseConsts cc) 
       const int lo = d == 0 ? B.b.is : (d == 1 ? B.b.js : B.b.ks);
       const int hi = d == 0 ? B.b.ie : (d == 1 ? B.b.je : B.b.ke);
       double fm[5], fp[5];
-      face_flux(B, d + 1, n - st, pos - 1, lo, hi, st, cc.gamma, fm);
-      face_flux(B, d + 1, n, pos, lo, hi, st, cc.gamma, fp);
+      if (MIXED) {
+        face_flux_mixed(B, d + 1, n - st, pos - 1, lo, hi, st, cc.gamma, fm);
+        face_flux_mixed(B, d + 1, n, pos, lo, hi, st, cc.gamma, fp);
+      } else {
+        face_flux(B, d + 1, n - st, pos - 1, lo, hi, st, cc.gamma, fm);
+        face_flux(B, d + 1, n, pos, lo, hi, st, cc.gamma, fp);
+      }
 #pragma unroll
       for (int c = 0; c < 5; ++c) dsm[d][c][threadIdx.x] = fp[c] - fm[c];
     }
@@ -199,6 +301,18 @@ __global__ void k_inviscid(const BlockView* __restrict__ blocks, CaseConsts cc) 
       B.v(F_RHSI, c + 1, n) = acc;
     }
   }
+}
+
+// sub_inviscid1.f90:8-189: rhsi on the updated nodes.  A CTA covers kInvTile
+// nodes x 3 directions; thread (x, d) computes the flux difference of
+// direction d at its node (both faces), and the three differences are
+// combined in the reference's order: rhsi = -dF; rhsi -= dG; rhsi -= dH.
+__global__ void k_inviscid(const BlockView* __restrict__ blocks, CaseConsts cc) {
+  inviscid_body<false>(blocks, cc);
+}
+// The mixed-precision variant (face_flux_mixed).
+__global__ void k_inviscid_mixed(const BlockView* __restrict__ blocks, CaseConsts cc) {
+  inviscid_body<true>(blocks, cc);
 }
 
 // Zero-fills one field over the full box of every block (the reference's
@@ -296,6 +410,88 @@ __global__ void k_viscous_a(const BlockView* __restrict__ blocks, CaseConsts cc,
     fvh[(4 * dd + 1) * P + n] = (x1 * ta[1] + x2 * ta[3] + x3 * ta[4]) * ij;
     fvh[(4 * dd + 2) * P + n] = (x1 * ta[2] + x2 * ta[4] + x3 * ta[5]) * ij;
     fvh[(4 * dd + 3) * P + n] = (x1 * bx + x2 * by + x3 * bz) * ij;
+  }
+}
+
+// Mixed-precision variant of k_viscous_a: the gradients are FP64 central
+// differences, the viscosity (Sutherland) stays FP64 since the local time step
+// reads it; the velocity-gradient chain rule, stresses, heat flux, vorticity
+// and the contravariant fluxes are FP32.
+__global__ void k_viscous_a_mixed(const BlockView* __restrict__ blocks, CaseConsts cc, int store_dudx_tao) {
+  const BlockView& B = blocks[blockIdx.y];
+  const Box& b0 = B.b0;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b0.size()) return;
+  int i = b0.is + (int)(t % b0.nx());
+  long r = t / b0.nx();
+  int j = b0.js + (int)(r % b0.ny());
+  int k = b0.ks + (int)(r / b0.ny());
+  long n = B.at(i, j, k);
+  const long st[3] = {1, (long)B.nx, (long)B.nx * B.ny};
+  const int pos[3] = {i, j, k};
+  const int lo[3] = {b0.is, b0.js, b0.ks};
+  const int hi[3] = {b0.ie, b0.je, b0.ke};
+  const double* pu = B.f[F_PRI] + 1 * B.plane;
+  const double* pv = B.f[F_PRI] + 2 * B.plane;
+  const double* pw = B.f[F_PRI] + 3 * B.plane;
+  const double* pt = B.f[F_PRI] + 5 * B.plane;
+  float gt[3] = {0, 0, 0}, gu[3] = {0, 0, 0}, gv[3] = {0, 0, 0}, gw[3] = {0, 0, 0};
+  int ndir = cc.dimension == IFLAG_3D ? 3 : 2;
+  for (int d = 0; d < ndir; ++d) {
+    gt[d] = (float)cdiff(pt, n, st[d], pos[d], lo[d], hi[d]);
+    gu[d] = (float)cdiff(pu, n, st[d], pos[d], lo[d], hi[d]);
+    gv[d] = (float)cdiff(pv, n, st[d], pos[d], lo[d], hi[d]);
+    gw[d] = (float)cdiff(pw, n, st[d], pos[d], lo[d], hi[d]);
+  }
+  double t0 = pt[n];
+  double amu1 = (1.0 + 124.0 / cc.tinf) / (t0 + 124.0 / cc.tinf) * pow(t0, 1.5);
+  double amu2 = B.v(F_AMU, 2, n);
+  double amu3d = amu1 + amu2;
+  B.v(F_AMU, 1, n) = amu1;
+  B.v(F_AMU, 3, n) = amu3d;
+  float amu3 = (float)amu3d;
+  float ki = (float)(cc.gamma * cc.cv * (amu1 / cc.prl + amu2 / cc.prt));
+  float u0 = (float)pu[n], v0 = (float)pv[n], w0 = (float)pw[n];
+  float m[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) m[c] = (float)B.v(F_DXIDX, c + 1, n);
+  float tx = gt[0] * m[0] + gt[1] * m[3] + gt[2] * m[6];
+  float ty = gt[0] * m[1] + gt[1] * m[4] + gt[2] * m[7];
+  float tz = gt[0] * m[2] + gt[1] * m[5] + gt[2] * m[8];
+  float du[9];
+  const float* gg[3] = {gu, gv, gw};
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) du[3 * a + c] = gg[a][0] * m[c] + gg[a][1] * m[c + 3] + gg[a][2] * m[c + 6];
+  float ta[6];
+  ta[0] = amu3 * (4.0f / 3.0f * du[0] - 2.0f / 3.0f * (du[4] + du[8]));
+  ta[1] = amu3 * (du[1] + du[3]);
+  ta[2] = amu3 * (du[6] + du[2]);
+  ta[3] = amu3 * (4.0f / 3.0f * du[4] - 2.0f / 3.0f * (du[0] + du[8]));
+  ta[4] = amu3 * (du[7] + du[5]);
+  ta[5] = amu3 * (4.0f / 3.0f * du[8] - 2.0f / 3.0f * (du[0] + du[4]));
+  float bx = u0 * ta[0] + v0 * ta[1] + w0 * ta[2] + ki * tx;
+  float by = u0 * ta[1] + v0 * ta[3] + w0 * ta[4] + ki * ty;
+  float bz = u0 * ta[2] + v0 * ta[4] + w0 * ta[5] + ki * tz;
+  float a1 = du[5] - du[7], a2 = du[2] - du[6], a3 = du[1] - du[3];
+  B.s(F_VOR, n) = (double)sqrtf(a1 * a1 + a2 * a2 + a3 * a3);
+  if (store_dudx_tao) {
+#pragma unroll
+    for (int c = 0; c < 9; ++c) B.v(F_DUDX, c + 1, n) = (double)du[c];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) B.v(F_TAO, c + 1, n) = (double)ta[c];
+  }
+  float ij = (float)B.s(F_INVJ, n);
+  double* fvh = B.f[F_FVH];
+  long P = B.plane;
+#pragma unroll
+  for (int dd = 0; dd < 3; ++dd) {
+    float x1 = m[3 * dd], x2 = m[3 * dd + 1], x3 = m[3 * dd + 2];
+    fvh[(4 * dd + 0) * P + n] = (double)((x1 * ta[0] + x2 * ta[1] + x3 * ta[2]) * ij);
+    fvh[(4 * dd + 1) * P + n] = (double)((x1 * ta[1] + x2 * ta[3] + x3 * ta[4]) * ij);
+    fvh[(4 * dd + 2) * P + n] = (double)((x1 * ta[2] + x2 * ta[4] + x3 * ta[5]) * ij);
+    fvh[(4 * dd + 3) * P + n] = (double)((x1 * bx + x2 * by + x3 * bz) * ij);
   }
 }
 

@@ -127,12 +127,43 @@ __global__ void k_plane_index(const BlockView* __restrict__ blocks) {
   }
 }
 
+// Plane-local record layout of the sweeps.  The records of hyperplane h
+// (cnt = poff[h+1]-poff[h] nodes) form one contiguous chunk starting at
+// kRec*poff[h] (rec_f, rec_b) or 8*poff[h] (sca, dqs); element x of the node
+// with plane-local index t sits at x*cnt + t, so the threads of a warp, which
+// take consecutive t, read consecutive words.
+//   rec_f/rec_b x = 25*d + 5*row + col : block of neighbour direction d
+//               x = 75                 : neighbours' plane-local indices, packed
+//   sca         x = 0..4 rhs, 5 diag, 6 inv_j, 7 1/diag, 8 1/inv_j (kSca per node)
+//   dqs         x = 0..4 dq* (forward result)
+__device__ __forceinline__ long rec_at(const BlockView& B, long pos, int h, int stride, int x) {
+  long base = B.poff[h];
+  long cnt = B.poff[h + 1] - base;
+  return stride * base + x * cnt + (pos - base);
+}
+// Three plane-local indices (+1; 0 = no neighbour) in one 64-bit word.
+constexpr int kNbrBits = 21;
+__device__ __forceinline__ double pack_nbrs(const int* nb, long prev_base) {
+  unsigned long long u = 0;
+#pragma unroll
+  for (int e = 0; e < 3; ++e) {
+    unsigned long long f = nb[e] < 0 ? 0ull : (unsigned long long)(nb[e] - prev_base + 1);
+    u |= f << (kNbrBits * e);
+  }
+  return __longlong_as_double((long long)u);
+}
+__device__ __forceinline__ int nbr_local(double packed, int e) {
+  unsigned long long u = (unsigned long long)__double_as_longlong(packed);
+  return (int)((u >> (kNbrBits * e)) & ((1ull << kNbrBits) - 1)) - 1;
+}
+
 // The off-diagonal blocks of both sweeps, off the critical path.  For every
 // updated node (the provider) and direction d: A = calc_jm at the provider,
 // S+ = 0.5*(A + r*I)*inv_j goes to the forward record of the node one step up
 // in d, S- = 0.5*(A - r*I)*inv_j to the backward record of the node one step
 // down (sub_timeadvancement_1stimplicit.f90:283-301, :459-477, same
-// operations).  Each node also stores rhs, diag and inv_j in its record.
+// operations).  Each node also stores rhs, diag and inv_j, and the packed
+// positions of its forward and backward neighbours.
 __global__ void k_lusgs_mats(const BlockView* __restrict__ blocks, CaseConsts cc) {
   const BlockView& B = blocks[blockIdx.y];
   const Box& b1 = B.b1;
@@ -149,14 +180,21 @@ __global__ void k_lusgs_mats(const BlockView* __restrict__ blocks, CaseConsts cc
   long n = B.at(b1.is + a, b1.js + b, b1.ks + c);
   int off[3] = {a, b, c};
   const int lim[3] = {nx1, ny1, nz1};
+  const int h = a + b + c;
   long pos = plane_pos(B, a, b, c);
   if (d == 0) {
-    double* sc = B.sca + 8 * pos;
+    long base = B.poff[h], cnt = B.poff[h + 1] - base, lt = pos - base;
+    double* sc = B.sca + kSca * base + lt;
 #pragma unroll
-    for (int x = 0; x < 5; ++x) sc[x] = B.v(F_RHS, x + 1, n);
-    sc[5] = B.s(F_DIAG, n);
-    sc[6] = B.s(F_INVJ, n);
-    sc[7] = 0.0;
+    for (int x = 0; x < 5; ++x) sc[x * cnt] = B.v(F_RHS, x + 1, n);
+    double diag = B.s(F_DIAG, n), invj = B.s(F_INVJ, n);
+    sc[5 * cnt] = diag;
+    sc[6 * cnt] = invj;
+    sc[7 * cnt] = 1.0 / diag;
+    sc[8 * cnt] = 1.0 / invj;
+    const int* nb = B.nbr + 6 * pos;
+    B.rec_f[kRec * base + 75 * cnt + lt] = pack_nbrs(nb, h > 0 ? B.poff[h - 1] : 0);
+    B.rec_b[kRec * base + 75 * cnt + lt] = pack_nbrs(nb + 3, h + 1 < B.nplanes ? B.poff[h + 1] : 0);
   }
   bool up = off[d] < lim[d] - 1;    // a forward consumer exists
   bool down = off[d] > 0;           // a backward consumer exists
@@ -169,21 +207,25 @@ __global__ void k_lusgs_mats(const BlockView* __restrict__ blocks, CaseConsts cc
   if (up) {
     int q[3] = {a, b, c};
     q[d] += 1;
-    double* dst = B.rec_f + kRec * plane_pos(B, q[0], q[1], q[2]) + 25 * d;
+    long qp = plane_pos(B, q[0], q[1], q[2]);
+    long base = B.poff[h + 1], cnt = B.poff[h + 2] - base;
+    double* dst = B.rec_f + kRec * base + 25 * d * cnt + (qp - base);
 #pragma unroll
     for (int x = 0; x < 25; ++x) {
       double v = (x % 6 == 0) ? A[x] + rad : A[x];
-      dst[x] = 0.5 * v * invj;
+      dst[x * cnt] = 0.5 * v * invj;
     }
   }
   if (down) {
     int q[3] = {a, b, c};
     q[d] -= 1;
-    double* dst = B.rec_b + kRec * plane_pos(B, q[0], q[1], q[2]) + 25 * d;
+    long qp = plane_pos(B, q[0], q[1], q[2]);
+    long base = B.poff[h - 1], cnt = B.poff[h] - base;
+    double* dst = B.rec_b + kRec * base + 25 * d * cnt + (qp - base);
 #pragma unroll
     for (int x = 0; x < 25; ++x) {
       double v = (x % 6 == 0) ? A[x] - rad : A[x];
-      dst[x] = 0.5 * v * invj;
+      dst[x * cnt] = 0.5 * v * invj;
     }
   }
 }
@@ -200,6 +242,9 @@ __device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned coun
 __device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
   unsigned ok;
@@ -219,179 +264,310 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
 }
-
-// Offsets (a,b,c) of node t of hyperplane h, and the index of offsets (b,c)
-// of plane h inside that plane (c ascending, then b) - the order of plane_pos.
-__device__ __forceinline__ void plane_abc(int h, int t, int nx1, int ny1, int& a, int& b, int& c) {
-  c = max(0, h - (nx1 - 1) - (ny1 - 1));
-  for (;; ++c) {
-    int r = h - c;
-    int bmin = max(0, r - (nx1 - 1)), bmax = min(ny1 - 1, r);
-    int cnt = bmax - bmin + 1;
-    if (t < cnt) {
-      b = bmin + t;
-      a = r - b;
-      return;
-    }
-    t -= cnt;
-  }
-}
-__device__ __forceinline__ int within(int h, int b, int c, int nx1, int ny1) {
-  int w = 0;
-  for (int cc = max(0, h - (nx1 - 1) - (ny1 - 1)); cc < c; ++cc) {
-    int r = h - cc;
-    int bmin = max(0, r - (nx1 - 1)), bmax = min(ny1 - 1, r);
-    if (bmax >= bmin) w += bmax - bmin + 1;
-  }
-  return w + (b - max(0, (h - c) - (nx1 - 1)));
+// Barrier 1 over the first n threads (the consumer warps), returning the OR of
+// `pred` over them; orders memory like __syncthreads.
+__device__ __forceinline__ bool consumers_sync_or(bool pred, int n) {
+  unsigned r;
+  asm volatile(
+      "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, 1, %2, p;\n selp.u32 %0, 1, 0, q;\n}"
+      : "=r"(r)
+      : "r"((unsigned)pred), "r"(n)
+      : "memory");
+  return r != 0;
 }
 
-__device__ __forceinline__ double row_dot(const double* m, const double* x) {
+__device__ __forceinline__ double row_dot5(const double* m, int mst, const double* x, int xst) {
   double s = m[0] * x[0];
-  s = s + m[1] * x[1];
-  s = s + m[2] * x[2];
-  s = s + m[3] * x[3];
-  s = s + m[4] * x[4];
+  s = s + m[mst] * x[xst];
+  s = s + m[2 * mst] * x[2 * xst];
+  s = s + m[3 * mst] * x[3 * xst];
+  s = s + m[4 * mst] * x[4 * xst];
   return s;
 }
 
 constexpr long kSpinLimit = 1L << 20;  // bounded mbarrier wait (well under a second)
 
+// Rows r0 .. r0+nr-1 (nr <= 3) of plane-local node `t` of one plane of the
+// sweep: each row of the three neighbour blocks times the neighbours' dq,
+// summed in the reference's order (sub_timeadvancement_1stimplicit.f90:346-364,
+// :522-540); the two divisions are exact (div_rn with the stored
+// reciprocals).  rec/sca/dsv point at the plane's chunks (element stride
+// cnt); prev holds the previous plane's dq, component c of node w at
+// prev[c*pst + w*wst].
+template <bool FWD>
+__device__ __forceinline__ void lusgs_rows(const double* rec, const double* sca, const double* dsv, int cnt,
+                                           int t, int r0, int nr, const double* prev, long pst, int wst,
+                                           double out[3]) {
+  double packed = rec[75 * cnt + t];
+  double x[3][5];
+  bool has[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    int w = nbr_local(packed, d);
+    has[d] = w >= 0;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) x[d][c] = has[d] ? prev[c * pst + (long)w * wst] : 0.0;
+  }
+  const double diag = sca[5 * cnt + t], invj = sca[6 * cnt + t];
+  const double rdiag = sca[7 * cnt + t], rinvj = sca[8 * cnt + t];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    if (k < nr) {
+      int row = r0 + k;
+      double acc[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        acc[d] = has[d] ? row_dot5(rec + (25 * d + 5 * row) * cnt + t, cnt, x[d], 1) : 0.0;
+      if (FWD)
+        out[k] = div_rn(div_rn(sca[row * cnt + t] + (acc[0] + acc[1] + acc[2]), diag, rdiag), invj, rinvj);
+      else
+        out[k] = dsv[row * cnt + t] - div_rn(div_rn(acc[0] + acc[1] + acc[2], invj, rinvj), diag, rdiag);
+    }
+  }
+}
+
 }  // namespace
 
-// Forward and backward hyperplane sweeps for one block per CTA.  Thread t of a
-// plane handles equation row t%5 of node t/5: the row of the three neighbour
-// blocks times the neighbours' dq, summed in the reference's order
-// (sub_timeadvancement_1stimplicit.f90:346-364, :522-540).  The previous
-// plane's results sit in shared memory.
-//
-// With STAGED, the records of the next NST planes (contiguous in the
-// hyperplane-major layout) are brought into shared memory by bulk copies
-// issued by one thread and tracked by mbarriers, so a plane's loads are never
-// on the critical path.  Without it (planes too large for shared memory) the
-// records are read from global memory.  Waits are bounded: on a timeout the
-// kernel raises ST_TIMEOUT in `status` and stops.
-template <bool STAGED>
-__device__ __forceinline__ void lusgs_sweep(const BlockView* __restrict__ blocks, int nst, unsigned* status) {
+// Forward and backward hyperplane sweeps of one block per CTA with the plane
+// records staged in shared memory.  Warps 0..C/32-1 are consumers: thread
+// (row, t) computes equation `row` of node t of every plane; the previous
+// plane's dq sits in a two-plane ring in shared memory.  The last warp is the
+// producer: it brings the records of the next planes into nst stages with bulk
+// copies, each stage guarded by a `full` mbarrier (copies landed) and an
+// `empty` mbarrier (every consumer warp done with it).  The backward pass also
+// needs dq* of the forward pass, which the consumers publish with a proxy
+// fence and the `fwd_done` mbarrier.  Every wait is bounded: a consumer that
+// gives up makes all consumers stop at the next plane barrier and raise
+// ST_TIMEOUT; the producer then waits (bounded) for its copies in flight.
+__global__ void k_lusgs_sweep_staged(const BlockView* __restrict__ blocks, int nst, unsigned* status) {
   const BlockView& B = blocks[blockIdx.x];
   extern __shared__ __align__(16) unsigned char smem[];
   const int P = B.pmax;
   const int H = B.nplanes;
-  const int nx1 = B.b1.nx(), ny1 = B.b1.ny();
-  const long* poff = B.poff;
-  // shared layout: ring (2 planes x 5*P) | stages (nst x P*(kRec + 8 + 8)) | mbarriers
-  double* ring = (double*)smem;
+  const int C = blockDim.x - 32;  // consumer threads
+  // shared layout: plane offsets (H+1, padded to 16 B) | ring (2 planes x 5*P)
+  // | nst stages (P*(kRec+kSca+8)) | mbarriers
+  long* poff = (long*)smem;
+  double* ring = (double*)(poff + ((H + 2) & ~1));
   double* stage0 = ring + 10 * P;
-  const int sdoubles = P * (kRec + 16);
-  unsigned long long* bars = (unsigned long long*)(stage0 + (STAGED ? nst * sdoubles : 0));
-  __shared__ int abort_flag;
+  const int sdoubles = P * (kRec + kSca + 8);
+  unsigned long long* full = (unsigned long long*)(stage0 + nst * sdoubles);
+  unsigned long long* empty = full + nst;
+  unsigned long long* fwd_done = empty + nst;
+  __shared__ volatile int abort_flag;
+  for (int x = threadIdx.x; x <= H; x += blockDim.x) poff[x] = B.poff[x];
   if (threadIdx.x == 0) {
     abort_flag = 0;
-    if (STAGED) {
-      for (int x = 0; x < nst; ++x) mbar_init(&bars[x], 1);
-      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    for (int x = 0; x < nst; ++x) {
+      mbar_init(&full[x], 1);
+      mbar_init(&empty[x], C / 32);
     }
+    mbar_init(fwd_done, C / 32);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  // Steps gs = 0 .. 2H-1 run the forward planes then the backward planes; step
-  // gs uses stage gs % nst, whose mbarrier completes once per use, so the
-  // phase to wait for has parity (gs / nst) & 1.
-  for (int pass = 0; pass < 2; ++pass) {
-    const bool fwd = pass == 0;
-    const double* rec_g = fwd ? B.rec_f : B.rec_b;
-    auto plane_of = [&](int st) { return fwd ? st : H - 1 - st; };
-    auto issue = [&](int st) {  // copies of step st of this pass
-      int gs = pass * H + st;
-      int h = plane_of(st);
+
+  if (threadIdx.x >= C) {  // ------------------------------------ producer
+    if (threadIdx.x != C) return;
+    auto stage_of = [&](int gs) { return stage0 + (gs % nst) * sdoubles; };
+    auto wait_bar = [&](unsigned long long* bar, unsigned parity) {
+      long spins = 0;
+      while (!mbar_try_wait(bar, parity)) {
+        if (abort_flag || ++spins > kSpinLimit) return false;
+      }
+      return true;
+    };
+    bool ok = true;
+    int issued = 0;  // steps whose copies were issued
+    // issue the copies of global step gs (forward: gs < H); with_dqs = false
+    // leaves the backward dq* copy for later
+    auto issue = [&](int gs, bool with_dqs) {
+      bool fwd = gs < H;
+      int h = fwd ? gs : 2 * H - 1 - gs;
       long base = poff[h];
       unsigned cnt = (unsigned)(poff[h + 1] - base);
-      double* stg = stage0 + (gs % nst) * sdoubles;
-      unsigned long long* bar = &bars[gs % nst];
-      mbar_expect_tx(bar, cnt * (kRec + 8 + (fwd ? 0 : 8)) * 8u);
-      bulk_g2s(stg, rec_g + kRec * base, cnt * kRec * 8u, bar);
-      bulk_g2s(stg + P * kRec, B.sca + 8 * base, cnt * 64u, bar);
-      if (!fwd) bulk_g2s(stg + P * (kRec + 8), B.dqs + 8 * base, cnt * 64u, bar);
-    };
-    if (STAGED && threadIdx.x == 0) {
-      // the generic reads of the stage buffers are ordered before the
-      // async-proxy writes into them (the dq* stores of the forward pass are
-      // fenced for the async proxy by every thread at the end of that pass)
+      double* stg = stage_of(gs);
+      unsigned long long* bar = &full[gs % nst];
+      if (gs >= nst && !wait_bar(&empty[gs % nst], (unsigned)((gs / nst - 1) & 1))) return false;
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      for (int st = 0; st < nst && st < H; ++st) issue(st);
-    }
-    for (int st = 0; st < H; ++st) {
-      int gs = pass * H + st;
-      int h = plane_of(st);
+      mbar_expect_tx(bar, cnt * (kRec + kSca + (fwd ? 0 : 8)) * 8u);
+      bulk_g2s(stg, (fwd ? B.rec_f : B.rec_b) + kRec * base, cnt * kRec * 8u, bar);
+      bulk_g2s(stg + P * kRec, B.sca + kSca * base, cnt * kSca * 8u, bar);
+      if (!fwd && with_dqs) bulk_g2s(stg + P * (kRec + kSca), B.dqs + 8 * base, cnt * 64u, bar);
+      ++issued;
+      return true;
+    };
+    auto issue_dqs = [&](int gs) {
+      int h = 2 * H - 1 - gs;
       long base = poff[h];
-      int cnt = (int)(poff[h + 1] - base);
-      int hn = fwd ? h - 1 : h + 1;  // plane holding the neighbours
-      double* prev = ring + 5 * P * ((st + 1) & 1);
-      double* cur = ring + 5 * P * (st & 1);
-      const double* stg = stage0 + (gs % nst) * sdoubles;
-      if (STAGED) {
-        unsigned parity = (unsigned)((gs / nst) & 1);
+      unsigned cnt = (unsigned)(poff[h + 1] - base);
+      bulk_g2s(stage_of(gs) + P * (kRec + kSca), B.dqs + 8 * base, cnt * 64u, &full[gs % nst]);
+    };
+    for (int gs = 0; gs < H && ok; ++gs) ok = issue(gs, true);
+    int head = nst < H ? nst : H;
+    for (int x = 0; x < head && ok; ++x) ok = issue(H + x, false);
+    if (ok) ok = wait_bar(fwd_done, 0u);
+    if (ok) {
+      asm volatile("fence.proxy.async.global;" ::: "memory");
+      for (int x = 0; x < head; ++x) issue_dqs(H + x);
+    }
+    for (int gs = H + head; gs < 2 * H && ok; ++gs) ok = issue(gs, true);
+    if (!ok) {
+      // drain: wait (bounded) for the copies of the last issued stages
+      for (int gs = issued > nst ? issued - nst : 0; gs < issued; ++gs) {
         long spins = 0;
-        while (!mbar_try_wait(&bars[gs % nst], parity)) {
-          if (++spins > kSpinLimit) {
-            abort_flag = 1;
-            break;
-          }
+        while (!mbar_try_wait(&full[gs % nst], (unsigned)((gs / nst) & 1)) && ++spins < kSpinLimit) {
         }
-      }
-      for (int t = threadIdx.x; t < 5 * cnt && !abort_flag; t += blockDim.x) {
-        int node = t / 5, row = t - 5 * node;
-        int a, b, c;
-        plane_abc(h, node, nx1, ny1, a, b, c);
-        const double* rec = STAGED ? stg + kRec * node : rec_g + kRec * (base + node);
-        const double* sc = STAGED ? stg + P * kRec + 8 * node : B.sca + 8 * (base + node);
-        const int off[3] = {a, b, c};
-        const int lim[3] = {nx1, ny1, B.b1.nz()};
-        double acc[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          bool has = fwd ? off[d] > 0 : off[d] < lim[d] - 1;
-          if (!has) {
-            acc[d] = 0.0;
-          } else {
-            int sgn = fwd ? -1 : 1;
-            int nb = d == 1 ? b + sgn : b;
-            int nc = d == 2 ? c + sgn : c;
-            int w = within(hn, nb, nc, nx1, ny1);
-            acc[d] = row_dot(rec + 25 * d + 5 * row, prev + 5 * w);
-          }
-        }
-        double v;
-        if (fwd) {
-          v = (sc[row] + (acc[0] + acc[1] + acc[2])) / sc[5] / sc[6];
-          B.dqs[8 * (base + node) + row] = v;
-        } else {
-          double ds = STAGED ? stg[P * (kRec + 8) + 8 * node + row] : B.dqs[8 * (base + node) + row];
-          v = ds - (acc[0] + acc[1] + acc[2]) / sc[6] / sc[5];
-          B.dq[5 * (base + node) + row] = v;
-        }
-        cur[t] = v;
-      }
-      __syncthreads();
-      if (abort_flag) {
-        if (threadIdx.x == 0 && status) atomicOr(status, (unsigned)ST_TIMEOUT);
-        return;
-      }
-      if (STAGED && threadIdx.x == 0 && st + nst < H) {
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        issue(st + nst);
       }
     }
-    // every thread orders its dq* stores before the backward bulk copies read them
-    if (STAGED && fwd) asm volatile("fence.proxy.async.global;" ::: "memory");
-    __syncthreads();
+    return;
+  }
+
+  // ------------------------------------------------------------ consumers
+  // Thread t < 5*cnt of a plane computes row t / cnt of node t % cnt (a warp
+  // mostly covers consecutive nodes of one row, so its shared-memory reads
+  // are consecutive words); warps beyond 5*cnt only take the barrier.  The
+  // ring holds the previous plane's dq node-major (5 per node).
+  const int lane = threadIdx.x & 31;
+  double* const g_dqs = B.dqs;
+  double* const g_dq = B.dq;
+  const double* prev = ring + 5 * P;
+  double* cur = ring;
+  int ls = 0;  // stage of the current step and its phase parity
+  unsigned lph = 0;
+  for (int gs = 0; gs < 2 * H; ++gs) {
+    const bool fwd = gs < H;
+    const int h = fwd ? gs : 2 * H - 1 - gs;
+    const long base = poff[h];
+    const int cnt = (int)(poff[h + 1] - base);
+    const double* stg = stage0 + ls * sdoubles;
+    bool timeout = false;
+    {
+      long spins = 0;
+      while (!mbar_try_wait(&full[ls], lph)) {
+        if (++spins > kSpinLimit) {
+          timeout = true;
+          break;
+        }
+      }
+    }
+    const int t = threadIdx.x;
+    if (!timeout && t < 5 * cnt) {
+      // t / cnt through a float reciprocal: exact here since t < 5*cnt <= 5*P
+      int row = (int)(((float)t + 0.5f) * (1.0f / (float)cnt));
+      int node = t - row * cnt;
+      const double* rec = stg + node;
+      const double* sca = stg + P * kRec + node;
+      double packed = rec[75 * cnt];
+      double acc[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        int w = nbr_local(packed, d);
+        double sd = 0.0;
+        if (w >= 0) {
+          const double* mr = rec + (25 * d + 5 * row) * cnt;
+          const double* x = prev + 5 * w;
+          sd = mr[0] * x[0];
+          sd = sd + mr[cnt] * x[1];
+          sd = sd + mr[2 * cnt] * x[2];
+          sd = sd + mr[3 * cnt] * x[3];
+          sd = sd + mr[4 * cnt] * x[4];
+        }
+        acc[d] = sd;
+      }
+      double v;
+      if (fwd) {
+        v = div_rn(div_rn(sca[row * cnt] + (acc[0] + acc[1] + acc[2]), sca[5 * cnt], sca[7 * cnt]), sca[6 * cnt],
+                   sca[8 * cnt]);
+        g_dqs[8 * base + row * cnt + node] = v;
+      } else {
+        double ds = stg[P * (kRec + kSca) + row * cnt + node];
+        v = ds - div_rn(div_rn(acc[0] + acc[1] + acc[2], sca[6 * cnt], sca[8 * cnt]), sca[5 * cnt], sca[7 * cnt]);
+        g_dq[5 * (base + node) + row] = v;
+      }
+      cur[5 * node + row] = v;
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[ls]);
+    if (gs == H - 1) {
+      // every thread orders its dq* stores before the backward bulk copies
+      // read them; the producer waits for all consumer warps
+      asm volatile("fence.proxy.async.global;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(fwd_done);
+    }
+    if (consumers_sync_or(timeout, C)) {
+      abort_flag = 1;
+      if (threadIdx.x == 0 && status) atomicOr(status, (unsigned)ST_TIMEOUT);
+      return;
+    }
+    if (++ls == nst) {
+      ls = 0;
+      lph ^= 1u;
+    }
+    // the first plane of each pass has no neighbours in the previous one, so
+    // the ring needs no reset between passes
+    const double* tmp = prev;
+    prev = cur;
+    cur = (double*)tmp;
   }
 }
 
-__global__ void k_lusgs_sweep_staged(const BlockView* __restrict__ blocks, int nst, unsigned* status) {
-  lusgs_sweep<true>(blocks, nst, status);
-}
+// The same sweeps with the records read from global memory, for blocks whose
+// planes do not fit the shared-memory stages; the previous plane's dq is read
+// back from dqs / dq (written before the last __syncthreads).
 __global__ void k_lusgs_sweep_global(const BlockView* __restrict__ blocks, int nst, unsigned* status) {
-  lusgs_sweep<false>(blocks, 1, status);
+  const BlockView& B = blocks[blockIdx.x];
+  const int H = B.nplanes;
+  const long* poff = B.poff;
+  for (int pass = 0; pass < 2; ++pass) {
+    const bool fwd = pass == 0;
+    for (int st = 0; st < H; ++st) {
+      int h = fwd ? st : H - 1 - st;
+      long base = poff[h];
+      int cnt = (int)(poff[h + 1] - base);
+      const double* rec = (fwd ? B.rec_f : B.rec_b) + kRec * base;
+      const double* sca = B.sca + kSca * base;
+      const double* dsv = B.dqs + 8 * base;
+      // previous plane: forward dq* (plane-local chunk, component stride = its
+      // node count), backward dq (node-major, 5 per node)
+      const double* prev = sca;
+      long pst = 0;
+      int wst = 0;
+      if (fwd && h > 0) {
+        prev = B.dqs + 8 * poff[h - 1];
+        pst = poff[h] - poff[h - 1];
+        wst = 1;
+      } else if (!fwd && h + 1 < H) {
+        prev = B.dq + 5 * poff[h + 1];
+        pst = 1;
+        wst = 5;
+      }
+      for (int t = threadIdx.x; t < 2 * cnt; t += blockDim.x) {
+        int half = t >= cnt;
+        int node = t - half * cnt;
+        int r0 = half ? 3 : 0, nr = half ? 2 : 3;
+        double v[3];
+        if (fwd)
+          lusgs_rows<true>(rec, sca, dsv, cnt, node, r0, nr, prev, pst, wst, v);
+        else
+          lusgs_rows<false>(rec, sca, dsv, cnt, node, r0, nr, prev, pst, wst, v);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          if (k < nr) {
+            int row = r0 + k;
+            if (fwd)
+              B.dqs[8 * base + row * cnt + node] = v[k];
+            else
+              B.dq[5 * (base + node) + row] = v[k];
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  (void)nst;
+  (void)status;
 }
 
 // q = q + dq on every updated node (sub_timeadvancement_1stimplicit.f90:568-574).

@@ -36,7 +36,9 @@ __global__ void k_getpri(const BlockView* __restrict__ blocks, CaseConsts cc, un
 __global__ void k_fill(const BlockView* __restrict__ blocks, int fid, int nc, double val);
 constexpr int kInvTile = 64;  // nodes per CTA of k_inviscid (x 3 directions)
 __global__ void k_inviscid(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_inviscid_mixed(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_viscous_a(const BlockView* __restrict__ blocks, CaseConsts cc, int store_dudx_tao);
+__global__ void k_viscous_a_mixed(const BlockView* __restrict__ blocks, CaseConsts cc, int store_dudx_tao);
 __global__ void k_viscous_b(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_find_dt(const BlockView* __restrict__ blocks, CaseConsts cc, double* cta_max);
 __global__ void k_dt_minmax(const BlockView* __restrict__ blocks, int m, const double* cta_max,

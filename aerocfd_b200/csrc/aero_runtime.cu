@@ -97,6 +97,8 @@ struct State {
   void* t_ws = nullptr;
   size_t t_ws_bytes = 0;
   int pmax_all = 0;
+  int hmax_all = 0;
+  bool mixed = false;  // aero_set_precision(1): FP32 increments in the flux kernels
   double* d_tmax = nullptr;
   size_t t_tmax = 0;
   std::string err;
@@ -232,7 +234,7 @@ void fill_view(BlockView& v, const Box& b, const Box& b0, const Box& b1, long pl
 // poff, rec_f, rec_b, sca, dqs, dq, nat, nbr.
 size_t workspace_bytes(const Box& b1, int H) {
   size_t N1 = (size_t)b1.size();
-  return (size_t)(H + 1) * sizeof(long) + N1 * (2 * kRec + 8 + 8 + 5) * sizeof(double) + N1 * sizeof(long) +
+  return (size_t)(H + 1) * sizeof(long) + N1 * (2 * kRec + kSca + 8 + 5) * sizeof(double) + N1 * sizeof(long) +
          N1 * 6 * sizeof(int) + 256;
 }
 int attach_workspace(BlockView& v, void* ws, const std::vector<long>& poff, int pmax) {
@@ -242,7 +244,7 @@ int attach_workspace(BlockView& v, void* ws, const std::vector<long>& poff, int 
   v.pmax = pmax;
   v.rec_f = (double*)p; p += N1 * kRec * sizeof(double);
   v.rec_b = (double*)p; p += N1 * kRec * sizeof(double);
-  v.sca = (double*)p; p += N1 * 8 * sizeof(double);
+  v.sca = (double*)p; p += N1 * kSca * sizeof(double);
   v.dqs = (double*)p; p += N1 * 8 * sizeof(double);
   v.dq = (double*)p; p += N1 * 5 * sizeof(double);
   v.nat = (long*)p; p += N1 * sizeof(long);
@@ -400,12 +402,18 @@ int launch_getpri(const BlockView* views, int nblk, long maxN, const CaseConsts&
 int launch_inviscid(const BlockView* views, int nblk, long maxN, long maxN1, const CaseConsts& cc) {
   PROF(P_FILL, (k_fill<<<dim3(cdiv(maxN, 256), nblk), 256, 0, g.stream>>>(views, F_RHSI, 5, 0.0)));
   CKL();
-  PROF(P_INVISCID, (k_inviscid<<<dim3(cdiv(maxN1, kInvTile), nblk), dim3(kInvTile, 3), 0, g.stream>>>(views, cc)));
+  if (g.mixed)
+    PROF(P_INVISCID, (k_inviscid_mixed<<<dim3(cdiv(maxN1, kInvTile), nblk), dim3(kInvTile, 3), 0, g.stream>>>(views, cc)));
+  else
+    PROF(P_INVISCID, (k_inviscid<<<dim3(cdiv(maxN1, kInvTile), nblk), dim3(kInvTile, 3), 0, g.stream>>>(views, cc)));
   CKL();
   return AERO_OK;
 }
 int launch_viscous(const BlockView* views, int nblk, long maxN0, const CaseConsts& cc, int store) {
-  PROF(P_VISC_A, (k_viscous_a<<<dim3(cdiv(maxN0, 128), nblk), 128, 0, g.stream>>>(views, cc, store)));
+  if (g.mixed)
+    PROF(P_VISC_A, (k_viscous_a_mixed<<<dim3(cdiv(maxN0, 128), nblk), 128, 0, g.stream>>>(views, cc, store)));
+  else
+    PROF(P_VISC_A, (k_viscous_a<<<dim3(cdiv(maxN0, 128), nblk), 128, 0, g.stream>>>(views, cc, store)));
   CKL();
   PROF(P_VISC_B, (k_viscous_b<<<dim3(cdiv(maxN0, 256), nblk), 256, 0, g.stream>>>(views, cc)));
   CKL();
@@ -421,35 +429,44 @@ int launch_dt_minmax(const BlockView* views, int m, double* d_out2) {
   CKL();
   return AERO_OK;
 }
-int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, int pmax, const CaseConsts& cc) {
+int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, int pmax, int hmax,
+                    const CaseConsts& cc) {
   PROF(P_LUSGS_PREP, (k_lusgs_prep<<<dim3(cdiv(maxExt, 256), nblk), 256, 0, g.stream>>>(views, cc)));
   CKL();
   PROF(P_LUSGS_MATS, (k_lusgs_mats<<<dim3(cdiv(3 * maxN1, 128), nblk), 128, 0, g.stream>>>(views, cc)));
   CKL();
-  // shared memory: ring of two planes + nst staged planes (records, scalars,
-  // dq*) + one mbarrier per stage; stage as many planes ahead as fit (2..3).
+  // Staged sweep: plane offsets + ring of two planes + nst staged planes
+  // (records, scalars, dq*) + 2*nst+1 mbarriers, as many stages as fit
+  // (2..4); one consumer thread per row of every node of the largest plane
+  // plus one producer warp.
+  if (pmax >= (1 << 21) - 1) return fail(AERO_ERR_ARG, "hyperplane of %d nodes exceeds the LU-SGS index range", pmax);
   const size_t kSmemMax = 227 * 1024;
+  size_t offs = (size_t)((hmax + 2) & ~1) * sizeof(long);
   size_t ring = (size_t)2 * 5 * std::max(pmax, 1) * sizeof(double);
-  size_t stage = (size_t)std::max(pmax, 1) * (kRec + 16) * sizeof(double);
-  int nst = 3;
-  while (nst >= 2 && ring + nst * stage + nst * 8 > kSmemMax) --nst;
-  int threads = (int)std::min<long>(1024, std::max<long>(64, (5L * pmax + 31) / 32 * 32));
+  size_t stage = (size_t)std::max(pmax, 1) * (kRec + kSca + 8) * sizeof(double);
+  int nst = 4;
+  while (nst >= 2 && offs + ring + nst * stage + (2 * nst + 1) * 8 > kSmemMax) --nst;
+  static int staged_max_threads = 0;  // limited by the kernel's registers
+  if (!staged_max_threads) {
+    cudaFuncAttributes fa;
+    CK(cudaFuncGetAttributes(&fa, k_lusgs_sweep_staged));
+    staged_max_threads = fa.maxThreadsPerBlock;
+  }
+  // consumer threads: one per row of every node of the largest plane
+  auto consumers_for = [](int p) { return (5 * std::max(p, 1) + 31) / 32 * 32; };
+  if (nst >= 2 && consumers_for(pmax) + 32 > staged_max_threads) nst = 0;
   if (nst >= 2) {
-    size_t smem = ring + nst * stage + nst * 8;
+    int consumers = consumers_for(pmax);
+    size_t smem = offs + ring + nst * stage + (2 * nst + 1) * 8;
     static size_t set_staged = 0;
     if (smem > 48 * 1024 && smem > set_staged) {
       CK(cudaFuncSetAttribute(k_lusgs_sweep_staged, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       set_staged = smem;
     }
-    PROF(P_LUSGS_SWEEP, (k_lusgs_sweep_staged<<<nblk, threads, smem, g.stream>>>(views, nst, g.d_status)));
+    PROF(P_LUSGS_SWEEP, (k_lusgs_sweep_staged<<<nblk, consumers + 32, smem, g.stream>>>(views, nst, g.d_status)));
   } else {
-    size_t smem = ring;
-    static size_t set_global = 0;
-    if (smem > 48 * 1024 && smem > set_global) {
-      CK(cudaFuncSetAttribute(k_lusgs_sweep_global, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      set_global = smem;
-    }
-    PROF(P_LUSGS_SWEEP, (k_lusgs_sweep_global<<<nblk, threads, smem, g.stream>>>(views, 1, g.d_status)));
+    int threads = (int)std::min<long>(1024, std::max<long>(64, (2L * pmax + 31) / 32 * 32));
+    PROF(P_LUSGS_SWEEP, (k_lusgs_sweep_global<<<nblk, threads, 0, g.stream>>>(views, 1, g.d_status)));
   }
   CKL();
   PROF(P_LUSGS_UPDATE, (k_lusgs_update<<<dim3(cdiv(maxN1, 256), nblk), 256, 0, g.stream>>>(views)));
@@ -543,7 +560,7 @@ int do_iteration(bool want_dt_minmax) {
   if (viscous_on() && (rc = launch_viscous(g.d_blocks, nb, g.max_b0, g.cc, 0))) return rc;
   if ((rc = launch_find_dt(g.d_blocks, nb, g.max_box, g.cc))) return rc;
   if (want_dt_minmax && (rc = launch_dt_minmax(g.d_blocks, nb - 1, g.d_out + 7))) return rc;
-  if ((rc = launch_implicit(g.d_blocks, nb, g.max_ext, g.max_b1, g.pmax_all, g.cc))) return rc;
+  if ((rc = launch_implicit(g.d_blocks, nb, g.max_ext, g.max_b1, g.pmax_all, g.hmax_all, g.cc))) return rc;
   if (sa_on() && (rc = launch_sa(g.d_blocks, nb, g.max_box, g.max_b1, g.pmax_all, g.cc))) return rc;
   if ((rc = do_physical_bc())) return rc;
   if ((rc = do_halo())) return rc;
@@ -613,6 +630,12 @@ int aero_finalize(void) {
   cudaStreamDestroy(g.stream); g.stream = nullptr;
   g.inited = false;
   g.configured = false;
+  return AERO_OK;
+}
+
+int aero_set_precision(int mode) {
+  if (mode != 0 && mode != 1) return fail(AERO_ERR_ARG, "precision mode %d is not 0 (FP64) or 1 (mixed)", mode);
+  g.mixed = mode == 1;
   return AERO_OK;
 }
 
@@ -744,6 +767,7 @@ int aero_finish_setup(void) {
   g.arena_doubles = total;
   g.views.resize(nb);
   g.pmax_all = 0;
+  g.hmax_all = 0;
   for (int m = 0; m < nb; ++m) {
     HostBlock& H = g.blocks[m];
     fill_view(g.views[m], H.b, H.b0, H.b1, H.plane, g.arena + H.arena_off);
@@ -752,6 +776,7 @@ int aero_finish_setup(void) {
     CK(cudaMalloc(&H.ws, workspace_bytes(H.b1, (int)poff.size() - 1)));
     if ((rc = attach_workspace(g.views[m], H.ws, poff, pmax))) return rc;
     g.pmax_all = std::max(g.pmax_all, pmax);
+    g.hmax_all = std::max(g.hmax_all, (int)poff.size() - 1);
   }
   CK(cudaMalloc(&g.d_blocks, nb * sizeof(BlockView)));
   CK(cudaMemcpyAsync(g.d_blocks, g.views.data(), nb * sizeof(BlockView), cudaMemcpyHostToDevice, g.stream));
@@ -913,7 +938,7 @@ int aero_implicit1st(double* q, const double* dt, const double* pri_v, double* r
   cc.cfl = *cfl;
   Box e{b1.is - 1, b1.ie + 1, b1.js - 1, b1.je + 1, b1.ks - 1, b1.ke + 1};
   if (!t.resident && (rc = launch_index(t.d_view, 1, b1.size()))) return rc;
-  if ((rc = launch_implicit(t.d_view, 1, e.size(), b1.size(), t.view.pmax, cc))) return rc;
+  if ((rc = launch_implicit(t.d_view, 1, e.size(), b1.size(), t.view.pmax, t.view.nplanes, cc))) return rc;
   return finish(t, args);
 }
 

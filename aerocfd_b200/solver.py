@@ -110,6 +110,10 @@ class GpuCase:
         _lib.check(self.L.aero_residual(_p(out)), "aero_residual")
         return out
 
+    def set_precision(self, mixed: bool) -> None:
+        """aero_set_precision: 0 = FP64 reference arithmetic, 1 = mixed."""
+        _lib.check(self.L.aero_set_precision(ctypes.c_int(1 if mixed else 0)), "aero_set_precision")
+
     def status(self) -> int:
         s = ctypes.c_uint(0)
         _lib.check(self.L.aero_get_status(ctypes.byref(s)), "aero_get_status")

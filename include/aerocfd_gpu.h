@@ -86,6 +86,13 @@ int aero_get_status(unsigned* status);
  *            (sub_init_readcontrolfile.f90:30-47, main.f90:636-653)
  * params[7]: ma, re, tinf, aoa (degrees), cfl, dt, nutinf               */
 int aero_configure(const int* iflags, const double* params);
+/* Arithmetic of the flux kernels (no counterpart in the reference, which is
+ * FP64 throughout).  mode 0 (default): FP64 in the reference's operation order.
+ * mode 1 (mixed): the WENO3 corrections, the Roe dissipation and the viscous
+ * stresses and fluxes in FP32, each formed from FP64 differences around FP64
+ * base states; metrics, Jacobians, the implicit diagonal and sweeps, the time
+ * step, the viscosity and the residual stay FP64.  Applies to later calls. */
+int aero_set_precision(int mode);
 /* box18: is,ie,js,je,ks,ke, is0..ke0, is1..ke1 of block m (1-based)
  *        (sub_init_allocatememory.f90:73-144)
  * subfaces: num_subface rows of f_no,face,is,ie,js,je,ks,ke,blk_t,

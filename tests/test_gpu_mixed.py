@@ -1,0 +1,96 @@
+"""Mixed-precision path (aero_set_precision(1)) against the FP64 GPU path.
+
+The FP64 path is checked against the oracle elsewhere; here the mixed path is
+stated as its max and L2 error against FP64 GPU runs from the same state:
+per routine (rhsi, rhsv) and over whole iterations (q, residual history).
+Bounds: rhsi/rhsv max error 1e-5 of the field's max magnitude, q after 10
+iterations 1e-6, residual history 1e-3 relative.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from aerocfd_b200 import grids
+from aerocfd_b200.case import FIELDS
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    from aerocfd_b200 import build, solver
+    build.build()
+    return solver
+
+
+def errs(a, b):
+    """(max, L2) error of a against b, relative to b's max / L2 norm."""
+    d = (a - b).ravel()
+    return float(np.max(np.abs(d)) / np.max(np.abs(b))), float(np.linalg.norm(d) / np.linalg.norm(b))
+
+
+def started(gpu, make, steps=3):
+    case = make()
+    gc = gpu.GpuCase(case)
+    gc.compute_geometry()
+    gc.init_flowfield()
+    gc.start()
+    gc.step(steps, history=False)
+    return case, gc
+
+
+def snapshot(gc, case, gpu):
+    gc.sync_to_host(gpu.ALL)
+    return [{k: v.copy() for k, v in b.fields.items()} for b in case.blocks]
+
+
+def restore(gc, case, gpu, snap):
+    for b, s in zip(case.blocks, snap):
+        for k, v in s.items():
+            b.fields[k][...] = v
+    gc.sync_to_device(gpu.ALL)
+
+
+@pytest.mark.parametrize("make", [lambda: grids.naca_ogrid(nblk=4, ni=33, nj=17, nk=3),
+                                  lambda: grids.bump_channel(ni=33, nj=17, nk=5)])
+def test_mixed_iterations_close_to_fp64(gpu, make):
+    case, gc = started(gpu, make)
+    try:
+        snap = snapshot(gc, case, gpu)
+        h64 = gc.step(10)
+        gc.sync_to_host(gpu.mask("q", "rhsi", "rhsv"))
+        q64 = [b.fields["q"].copy() for b in case.blocks]
+        restore(gc, case, gpu, snap)
+        gc.set_precision(True)
+        hmx = gc.step(10)
+        gc.sync_to_host(gpu.mask("q"))
+        qmx = [b.fields["q"].copy() for b in case.blocks]
+        gc.set_precision(False)
+        em = errs(np.concatenate([q.ravel() for q in qmx]), np.concatenate([q.ravel() for q in q64]))
+        rh = np.max(np.abs(hmx[:, :5] - h64[:, :5]) / np.max(np.abs(h64[:, :5]), axis=1, keepdims=True))
+        print(f"mixed vs fp64 after 10 iterations: q max {em[0]:.2e} L2 {em[1]:.2e}; residual history {rh:.2e}")
+        assert em[0] <= 1e-6 and rh <= 1e-3
+        assert gc.status() == 0
+    finally:
+        gc.close()
+
+
+def test_mixed_fluxes_close_to_fp64(gpu):
+    case, gc = started(gpu, lambda: grids.naca_ogrid(nblk=4, ni=33, nj=17, nk=3))
+    try:
+        res = {}
+        for mixed in (False, True):
+            gc.set_precision(mixed)
+            for b in case.blocks:
+                gc.inviscid_flux_1(b)
+                gc.viscous_flux(b)
+            gc.sync_to_host(gpu.mask("rhsi", "rhsv"))
+            res[mixed] = {k: np.concatenate([b.fields[k].ravel() for b in case.blocks]) for k in ("rhsi", "rhsv")}
+        gc.set_precision(False)
+        for k in ("rhsi", "rhsv"):
+            e = errs(res[True][k], res[False][k])
+            print(f"{k}: mixed vs fp64 max {e[0]:.2e} L2 {e[1]:.2e}")
+            assert e[0] <= 1e-5, (k, e)
+    finally:
+        gc.close()
