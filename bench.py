@@ -19,6 +19,13 @@ the iteration and copies q and the residual back.  --impl reference times the
 CPU restatement of the reference's algorithm (the reference is Fortran + MPI
 and cannot be compiled in this image) on the host cores, one thread per block
 like one MPI rank per block.
+
+Extra objects on the line: `mixed` (the same device-timed metric with
+aero_set_precision(1), and the mixed solution's max / L2 error against FP64
+after 50 iterations from one state) and `convergence` (wall time to each drop
+milestone 1e-3 .. 1e-8 of the density residual on the 97x49x5 Euler bump
+channel, FP64 and mixed, with the CPU restatement's time estimated from its
+iteration rate; a milestone the scheme does not reach is null).
 """
 from __future__ import annotations
 
@@ -52,6 +59,9 @@ KERNEL_BYTES = {
     "k_lusgs_mats": 24 * 8,    # q,dxidx,inv_j,ra,rb,rc,rhs,diag read (the blocks it writes are workspace)
     "k_getpri": 12 * 8,        # q read; pri write
 }
+# DRAM bytes (read + write) per launch of the dominant kernel on this workload,
+# from one ncu capture (profiles/k_lusgs_sweep_staged_naca0012.md).
+KERNEL_TRAFFIC = {"k_lusgs_sweep": 42.97e6 + 0.09e6}
 # The whole iteration's compulsory footprint for Euler/laminar FP64: read q,
 # dxidx, inv_j, write q, dq* write+read = 30 words per node.
 ITER_BYTES = 240
@@ -65,6 +75,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-sample-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-converge", action="store_true", help="skip the time-to-1e-8 runs")
     return ap.parse_args()
 
 
@@ -79,6 +90,67 @@ def peaks():
 def make_case():
     from aerocfd_b200 import grids
     return grids.naca_ogrid()
+
+
+CONV_WORKLOAD = "bump_channel_97x49x5_euler_m0.5_cfl5"
+CONV_TARGET = 1e-8
+CONV_MILESTONES = (1e-3, 1e-4, 1e-5, 1e-6, 1e-8)
+
+
+def make_bump():
+    from aerocfd_b200 import grids
+    return grids.bump_channel()
+
+
+def converge_gpu(solver, mixed: bool, chunk: int = 500, its: int = 12000):
+    """Wall time to each drop milestone of the density residual (relative to
+    iteration 1) on the Euler bump channel, freestream start, over `its`
+    iterations; the time to a milestone is the run's time per iteration times
+    the iteration that first reached it."""
+    import torch
+    case = make_bump()
+    gc = solver.GpuCase(case)
+    try:
+        gc.compute_geometry()
+        gc.init_flowfield()
+        gc.start()
+        gc.set_precision(mixed)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        hs = [gc.step(chunk) for _ in range(its // chunk)]
+        el = time.perf_counter() - t0
+        status = gc.status()
+    finally:
+        gc.close()
+    d = np.concatenate(hs)[:, 0]
+    d = d / d[0]
+    first = {}
+    for m in CONV_MILESTONES:
+        hit = np.nonzero(d <= m)[0]
+        first[f"{m:.0e}"] = int(hit[0]) + 1 if len(hit) else None
+    per_it = el / len(d)
+    return {"iterations_run": len(d), "wall_s_run": el, "final_drop": float(d[-1]), "min_drop": float(d.min()),
+            "iterations_to": first,
+            "wall_s_to": {k: (v * per_it if v else None) for k, v in first.items()},
+            "device_status": status}
+
+
+def bump_cpu_rate(seconds: float = 4.0):
+    """Iterations per second of the CPU restatement on the bump case (1 block, 1 thread)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # CPU baseline only
+    case = make_bump()
+    oc = oracle.OracleCase(case, fast=True)
+    oc.geometry()
+    oc.init_flowfield()
+    oc.start()
+    oc.iterate(2, 1)
+    t0 = time.perf_counter()
+    n = 0
+    while time.perf_counter() - t0 < seconds or n < 2:
+        oc.iterate(5, 1)
+        n += 5
+    return n / (time.perf_counter() - t0)
 
 
 class ClockSampler:
@@ -248,6 +320,42 @@ def main():
     for k in kernels:
         kernels[k]["share"] = kernels[k]["ms_total"] / max(1e-12, sum(x["ms_total"] for x in kernels.values()))
 
+    # ---- mixed precision: device-timed throughput, and its error against
+    # FP64 after the same iterations from the same state
+    gc.set_precision(True)
+    gc.step(3, history=False)
+    torch.cuda.synchronize()
+    _lib.check(L.aero_step_timed(ctypes.c_int(args.steps), ctypes.c_int(1), ctypes.byref(ms)), "mixed timed")
+    mixed_s = ms.value / 1e3
+    if dist:
+        t = torch.tensor([mixed_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        mixed_s = float(t.item())
+    gc.set_precision(False)
+    gc.sync_to_host(solver.ALL)
+    snap = [{k: v.copy() for k, v in b.fields.items()} for b in case.blocks]
+    kerr = 50
+    h64 = gc.step(kerr)
+    gc.sync_to_host(solver.mask("q"))
+    q64 = np.concatenate([b.fields["q"].ravel().copy() for b in case.blocks])
+    for b, sn in zip(case.blocks, snap):
+        for k, v in sn.items():
+            b.fields[k][...] = v
+    gc.sync_to_device(solver.ALL)
+    gc.set_precision(True)
+    hmx = gc.step(kerr)
+    gc.set_precision(False)
+    gc.sync_to_host(solver.mask("q"))
+    qmx = np.concatenate([b.fields["q"].ravel() for b in case.blocks])
+    dq = qmx - q64
+    mixed = {"value": nodes * args.steps * world / mixed_s / 1e6, "unit": "Mcell-iter/s",
+             "ms_per_step": 1e3 * mixed_s / args.steps,
+             "dtype": "f32 WENO corrections / Roe dissipation / viscous stresses; f64 state, metrics, "
+                      "Jacobians, LU-SGS, dt, residual",
+             "error_vs_fp64": {"iterations": kerr, "q_max_rel": float(np.max(np.abs(dq)) / np.max(np.abs(q64))),
+                               "q_l2_rel": float(np.linalg.norm(dq) / np.linalg.norm(q64)),
+                               "resid_rho_rel": float(abs(hmx[-1, 0] - h64[-1, 0]) / abs(h64[-1, 0]))}}
+
     # ---- end-to-end through the C-ABI with host-held q
     qbytes = sum(b.fields["q"].nbytes for b in case.blocks)
     mq = solver.mask("q")
@@ -286,7 +394,7 @@ def main():
         "e2e": {"value": e2e, "unit": "Mcell-iter/s", "h2d_bytes_per_step": qbytes,
                 "d2h_bytes_per_step": qbytes + 56},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "peak_kind": hbm_kind, "traffic": None,
+                     "frac": achieved / hbm, "peak_kind": hbm_kind, "traffic": KERNEL_TRAFFIC.get(dom),
                      "alg_bytes_per_launch": alg_bytes, "ms_per_launch": per_launch_ms},
         "iteration_roofline": {"bytes_per_node_iter": ITER_BYTES,
                                "achieved_gbs": ITER_BYTES * nodes / (dev_s / args.steps) / 1e9,
@@ -296,14 +404,26 @@ def main():
         "gpu_launches": int(cnt1.value - cnt0.value),
         "device_status": status,
     }
+    line["mixed"] = mixed
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, n, el, thr = cpu_reference(args.cpu_sample_seconds)
         line["cpu_baseline"] = {"value": v, "unit": "Mcell-iter/s", "cores": thr, "kind": "port",
                                 "sample": f"{n} full iterations of the same workload, {el:.1f} s, "
                                           f"{thr} threads (one per block), C++ -O3 restatement"}
+    gc.close()
+    if world == 1 and not args.no_converge:
+        conv = {"workload": CONV_WORKLOAD, "target_drop": CONV_TARGET,
+                "fp64": converge_gpu(solver, False), "mixed": converge_gpu(solver, True)}
+        if not args.no_cpu_baseline:
+            rate = bump_cpu_rate()
+            conv["cpu_reference"] = {
+                "its_per_s": rate, "cores": 1, "kind": "port",
+                "wall_s_to_est": {k: (v / rate if v else None) for k, v in conv["fp64"]["iterations_to"].items()},
+                "note": "oracle iteration rate x the FP64 GPU iteration counts (the FP64 path reproduces the "
+                        "oracle's iterates); 1 thread = the reference's layout for a 1-block case"}
+        line["convergence"] = conv
     if rank == 0:
         print(json.dumps(line))
-    gc.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
