@@ -167,23 +167,23 @@ __device__ __forceinline__ int nbr_local(double packed, int e) {
 __global__ void k_lusgs_mats(const BlockView* __restrict__ blocks, CaseConsts cc) {
   const BlockView& B = blocks[blockIdx.y];
   const Box& b1 = B.b1;
+  // thread t: direction d = t / N1 and provider position p = t % N1 in the
+  // hyperplane-major order, so a warp's record stores go to consecutive
+  // plane-local slots of one consumer plane
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   long N1 = b1.size();
   if (t >= 3 * N1) return;
-  int d = (int)(t % 3);
-  long u = t / 3;
-  int nx1 = b1.nx(), ny1 = b1.ny(), nz1 = b1.nz();
-  int a = (int)(u % nx1);
-  long r = u / nx1;
-  int b = (int)(r % ny1);
-  int c = (int)(r / ny1);
-  long n = B.at(b1.is + a, b1.js + b, b1.ks + c);
-  int off[3] = {a, b, c};
-  const int lim[3] = {nx1, ny1, nz1};
-  const int h = a + b + c;
-  long pos = plane_pos(B, a, b, c);
+  int d = (int)(t / N1);
+  long p = t - d * N1;
+  long n = B.nat[p];
+  long r = n / B.nx;
+  int i = B.b.is + (int)(n - r * B.nx);
+  int j = B.b.js + (int)(r % B.ny);
+  int k = B.b.ks + (int)(r / B.ny);
+  const int h = (i - b1.is) + (j - b1.js) + (k - b1.ks);
+  const int* nb = B.nbr + 6 * p;
   if (d == 0) {
-    long base = B.poff[h], cnt = B.poff[h + 1] - base, lt = pos - base;
+    long base = B.poff[h], cnt = B.poff[h + 1] - base, lt = p - base;
     double* sc = B.sca + kSca * base + lt;
 #pragma unroll
     for (int x = 0; x < 5; ++x) sc[x * cnt] = B.v(F_RHS, x + 1, n);
@@ -192,36 +192,29 @@ __global__ void k_lusgs_mats(const BlockView* __restrict__ blocks, CaseConsts cc
     sc[6 * cnt] = invj;
     sc[7 * cnt] = 1.0 / diag;
     sc[8 * cnt] = 1.0 / invj;
-    const int* nb = B.nbr + 6 * pos;
     B.rec_f[kRec * base + 75 * cnt + lt] = pack_nbrs(nb, h > 0 ? B.poff[h - 1] : 0);
     B.rec_b[kRec * base + 75 * cnt + lt] = pack_nbrs(nb + 3, h + 1 < B.nplanes ? B.poff[h + 1] : 0);
   }
-  bool up = off[d] < lim[d] - 1;    // a forward consumer exists
-  bool down = off[d] > 0;           // a backward consumer exists
-  if (!up && !down) return;
+  const int up = nb[3 + d];    // forward consumer: the neighbour one step up in d
+  const int down = nb[d];      // backward consumer: one step down
+  if (up < 0 && down < 0) return;
   double A[25];
   calc_jm(B, n, 3 * d + 1, cc.gamma, A);
   const int radf[3] = {F_RA, F_RB, F_RC};
   double rad = B.s(radf[d], n);
   double invj = B.s(F_INVJ, n);
-  if (up) {
-    int q[3] = {a, b, c};
-    q[d] += 1;
-    long qp = plane_pos(B, q[0], q[1], q[2]);
+  if (up >= 0) {
     long base = B.poff[h + 1], cnt = B.poff[h + 2] - base;
-    double* dst = B.rec_f + kRec * base + 25 * d * cnt + (qp - base);
+    double* dst = B.rec_f + kRec * base + 25 * d * cnt + (up - base);
 #pragma unroll
     for (int x = 0; x < 25; ++x) {
       double v = (x % 6 == 0) ? A[x] + rad : A[x];
       dst[x * cnt] = 0.5 * v * invj;
     }
   }
-  if (down) {
-    int q[3] = {a, b, c};
-    q[d] -= 1;
-    long qp = plane_pos(B, q[0], q[1], q[2]);
+  if (down >= 0) {
     long base = B.poff[h - 1], cnt = B.poff[h] - base;
-    double* dst = B.rec_b + kRec * base + 25 * d * cnt + (qp - base);
+    double* dst = B.rec_b + kRec * base + 25 * d * cnt + (down - base);
 #pragma unroll
     for (int x = 0; x < 25; ++x) {
       double v = (x % 6 == 0) ? A[x] - rad : A[x];
