@@ -32,7 +32,20 @@ struct AvgDst {
   long n;
 };
 
+// One wall subface (blk_t = -20) of clcd_output: quads (t1, t2) with t1 in
+// [lo1, lo1+n1) along the inner tangential direction, t2 in [lo2, lo2+n2)
+// along the outer one; w0 the wall layer; qoff the first quad's global index.
+struct WallFace {
+  int block, face;
+  int lo1, n1, lo2, n2, w0;
+  long qoff;
+};
+
 __global__ void k_getpri(const BlockView* __restrict__ blocks, CaseConsts cc, unsigned* status);
+__global__ void k_forces(const BlockView* __restrict__ blocks, const WallFace* __restrict__ walls, int nwall,
+                         long nquad, CaseConsts cc, double* __restrict__ part);
+__global__ void k_forces_final(const double* __restrict__ part, int npart, CaseConsts cc, double sref,
+                               double* __restrict__ out8);
 __global__ void k_fill(const BlockView* __restrict__ blocks, int fid, int nc, double val);
 constexpr int kInvTile = 64;  // nodes per CTA of k_inviscid (x 3 directions)
 __global__ void k_inviscid(const BlockView* __restrict__ blocks, CaseConsts cc);

@@ -80,6 +80,10 @@ struct State {
   double* d_avg_buf = nullptr;
   double* d_part = nullptr;
   int resid_ctas = 0;
+  WallFace* d_walls = nullptr;  // clcd_output: wall subfaces and per-CTA force partials
+  int nwall = 0;
+  long nquad = 0;
+  double* d_fpart = nullptr;
   double* d_out = nullptr;   // residual (7) + dt min/max (2)
   double* h_out = nullptr;   // pinned
   unsigned* d_status = nullptr;
@@ -112,13 +116,13 @@ State g;
 enum ProfId {
   P_GETPRI, P_FILL, P_INVISCID, P_VISC_A, P_VISC_B, P_FIND_DT, P_DT_MINMAX, P_LUSGS_PREP,
   P_LUSGS_MATS, P_LUSGS_SWEEP, P_LUSGS_UPDATE, P_SA_A, P_SA_B, P_SA_RECS, P_SA_SWEEP, P_INDEX, P_BC, P_SA_CLIP, P_HALO, P_AVG_GATHER, P_AVG_APPLY, P_RESID_PART, P_RESID_FINAL,
-  P_TRANSFER, P_GEOMETRY, P_NUM
+  P_TRANSFER, P_GEOMETRY, P_FORCES, P_NUM
 };
 const char* kProfName[P_NUM] = {
     "k_getpri", "k_fill", "k_inviscid", "k_viscous_a", "k_viscous_b", "k_find_dt", "k_dt_minmax",
     "k_lusgs_prep", "k_lusgs_mats", "k_lusgs_sweep", "k_lusgs_update", "k_sa_a", "k_sa_b", "k_sa_recs", "k_sa_sweep",
     "k_plane_index", "k_physical_bc", "k_sa_clip", "k_halo", "k_avg_gather",
-    "k_avg_apply", "k_residual_partial", "k_residual_final", "k_transfer", "k_geometry"};
+    "k_avg_apply", "k_residual_partial", "k_residual_final", "k_transfer", "k_geometry", "k_forces"};
 struct Prof {
   bool on = false;
   std::vector<cudaEvent_t> pool;
@@ -612,6 +616,10 @@ static void release_case() {
   cudaFree(g.d_avg_dst); g.d_avg_dst = nullptr;
   cudaFree(g.d_avg_buf); g.d_avg_buf = nullptr;
   cudaFree(g.d_part); g.d_part = nullptr;
+  cudaFree(g.d_walls); g.d_walls = nullptr;
+  cudaFree(g.d_fpart); g.d_fpart = nullptr;
+  g.nwall = 0;
+  g.nquad = 0;
   g.views.clear();
   g.setup = false;
 }
@@ -808,6 +816,30 @@ int aero_finish_setup(void) {
   if ((rc = launch_index(g.d_blocks, nb, g.max_b1))) return rc;
   g.resid_ctas = (int)cdiv(g.max_b1, 256);
   CK(cudaMalloc(&g.d_part, (size_t)g.resid_ctas * nb * 6 * sizeof(double)));
+  // wall subfaces of clcd_output, in block and bcinfo order
+  {
+    std::vector<WallFace> walls;
+    long q = 0;
+    for (int m = 0; m < nb; ++m)
+      for (const SubRow& r : g.blocks[m].subs) {
+        if (r.blk_t != BC_WALL) continue;
+        int D = (r.face - 1) / 2;
+        int T1 = D == 0 ? 1 : 0, T2 = D == 2 ? 1 : 2;
+        const int lo[3] = {r.is, r.js, r.ks}, hi[3] = {r.ie, r.je, r.ke};
+        WallFace w{m, r.face, lo[T1], hi[T1] - lo[T1], lo[T2], hi[T2] - lo[T2], r.face % 2 ? lo[D] : hi[D], q};
+        if (w.n1 <= 0 || w.n2 <= 0) continue;  // a wall line has no quads
+        walls.push_back(w);
+        q += (long)w.n1 * w.n2;
+      }
+    g.nwall = (int)walls.size();
+    g.nquad = q;
+    if (g.nwall) {
+      CK(cudaMalloc(&g.d_walls, walls.size() * sizeof(WallFace)));
+      CK(cudaMemcpyAsync(g.d_walls, walls.data(), walls.size() * sizeof(WallFace), cudaMemcpyHostToDevice,
+                         g.stream));
+      CK(cudaMalloc(&g.d_fpart, (size_t)cdiv(q, 256) * 6 * sizeof(double)));
+    }
+  }
   CK(cudaStreamSynchronize(g.stream));
   g.setup = true;
   return AERO_OK;
@@ -979,6 +1011,25 @@ int aero_residual(double* out7) {
   CK(cudaMemcpyAsync(g.h_out, g.d_out, 7 * sizeof(double), cudaMemcpyDeviceToHost, g.stream));
   CK(cudaStreamSynchronize(g.stream));
   std::memcpy(out7, g.h_out, 7 * sizeof(double));
+  return AERO_OK;
+}
+
+int aero_clcd_output(double sref, double* out8) {
+  int rc = need_setup();
+  if (rc) return rc;
+  if (!(sref > 0.0)) return fail(AERO_ERR_ARG, "sref = %g is not positive", sref);
+  if (!g.nwall) {
+    for (int x = 0; x < 8; ++x) out8[x] = 0.0;
+    return AERO_OK;
+  }
+  unsigned ctas = cdiv(g.nquad, 256);
+  PROF(P_FORCES, (k_forces<<<ctas, 256, 0, g.stream>>>(g.d_blocks, g.d_walls, g.nwall, g.nquad, g.cc, g.d_fpart)));
+  CKL();
+  PROF(P_FORCES, (k_forces_final<<<1, 256, 0, g.stream>>>(g.d_fpart, (int)ctas, g.cc, sref, g.d_out)));
+  CKL();
+  CK(cudaMemcpyAsync(g.h_out, g.d_out, 8 * sizeof(double), cudaMemcpyDeviceToHost, g.stream));
+  CK(cudaStreamSynchronize(g.stream));
+  std::memcpy(out8, g.h_out, 8 * sizeof(double));
   return AERO_OK;
 }
 

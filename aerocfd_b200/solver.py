@@ -114,6 +114,12 @@ class GpuCase:
         """aero_set_precision: 0 = FP64 reference arithmetic, 1 = mixed."""
         _lib.check(self.L.aero_set_precision(ctypes.c_int(1 if mixed else 0)), "aero_set_precision")
 
+    def clcd_output(self, sref: float = 1.0) -> np.ndarray:
+        """clcd_output on the device: fpx, fpy, fpz, fvx, fvy, fvz, cl, cd."""
+        out = np.zeros(8)
+        _lib.check(self.L.aero_clcd_output(ctypes.c_double(sref), _p(out)), "aero_clcd_output")
+        return out
+
     def status(self) -> int:
         s = ctypes.c_uint(0)
         _lib.check(self.L.aero_get_status(ctypes.byref(s)), "aero_get_status")

@@ -56,6 +56,13 @@ module aerocfd_gpu
       type(c_ptr), value :: host
     end function
 
+    ! sub_output_forceintegration.f90:8 (clcd_output): out8 = fp(3), fv(3), cl, cd
+    integer(c_int) function aero_clcd_output(sref, out8) bind(C, name="aero_clcd_output")
+      import :: c_int, c_double
+      real(c_double), value :: sref
+      real(c_double) :: out8(8)
+    end function
+
     integer(c_int) function aero_finish_setup() bind(C, name="aero_finish_setup")
       import :: c_int
     end function

@@ -172,6 +172,14 @@ int aero_updatebuffercoordinate(void); /* sub_bc_updatebuffercoordinate.f90:10 *
  * nut, (unused) over the updated nodes / totalnodes; the reference prints
  * these and appends them to resi_history.dat. */
 int aero_residual(double* out7);
+/* sub_output_forceintegration.f90:8-479 (clcd_output, 3-D): pressure and
+ * viscous forces over every wall subface (blk_t = -20) of the registered
+ * blocks from their current pri_v, dxidx, amu and x, y, z, then the lift and
+ * drag coefficients.  out8 = fpx, fpy, fpz, fvx, fvy, fvz, cl, cd (what the
+ * reference prints and appends to clcd_history.dat); sref is Control.in's
+ * reference area.  The per-element arithmetic is the reference's; the sums
+ * over elements run in a fixed parallel order. */
+int aero_clcd_output(double sref, double* out8);
 /* sub_init_flowfield.f90:29-111 (freestream start) on all registered blocks */
 int aero_init_flowfield(void);
 /* sub_init_walldist.f90:9 (wall distance of every physical node) */

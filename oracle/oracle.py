@@ -137,6 +137,12 @@ class OracleCase:
         self.L.oracle_residual(_p(out))
         return out
 
+    def clcd_output(self, sref: float = 1.0) -> np.ndarray:
+        """fp(3), fv(3), cl, cd, then the sums of |f_prs| and |f_vis| per component."""
+        out = np.zeros(14)
+        self.L.oracle_clcd_output(ctypes.c_double(sref), _p(out))
+        return out
+
     def last_dt_minmax(self) -> np.ndarray:
         out = np.zeros(4)
         self.L.oracle_last_dt_minmax(_p(out))

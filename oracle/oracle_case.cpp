@@ -462,6 +462,93 @@ void residual(double out[7]) {
   out[6] = std::sqrt(tur[1] / (double)totalnodes);
 }
 
+// sub_output_forceintegration.f90:8-479, 3-D branch (:182-457) with
+// force_compute (:481-509): pressure and viscous forces summed over every
+// quad of every wall subface (blk_t = -20) in the reference's loop order, then
+// cl and cd.  out: fp(3), fv(3), cl, cd, and (test use) the sums of |f_prs|
+// and |f_vis| per component.  The wall-normal unit vector keeps the
+// reference's component mix (e.g. face 1: x from dxidx(1) at the first two
+// corners and dxidx(2) at the last two).
+void clcd_output(double sref, double out[14]) {
+  const Consts& c = g_consts;
+  double pinf = c.p_0;
+  double div = 1.0 / (0.5 * c.d_0 * c.u_0 * c.u_0 * sref);
+  double fp[3] = {0, 0, 0}, fv[3] = {0, 0, 0}, ap[3] = {0, 0, 0}, av[3] = {0, 0, 0};
+  for (auto& B : g_blk) {
+    if (!B.used) continue;
+    size_t N = (size_t)B.b.size();
+    std::vector<double> si(N), sj(N), sk(N), spc(N), vol(N);
+    init_spacing(V{si.data(), 1, B.b}, V{sj.data(), 1, B.b}, V{sk.data(), 1, B.b}, V{spc.data(), 1, B.b},
+                 V{vol.data(), 1, B.b}, B.v(F_X), B.v(F_Y), B.v(F_Z), B.b, B.b0);
+    V spcv[3] = {V{si.data(), 1, B.b}, V{sj.data(), 1, B.b}, V{sk.data(), 1, B.b}};
+    V pri = B.v(F_PRI), m = B.v(F_DXIDX), amu = B.v(F_AMU);
+    for (auto& s : B.bc) {
+      if (s.blk_t != BC_WALL) continue;
+      const int D = (s.face - 1) / 2;
+      const bool low = s.face % 2 == 1;
+      const int lo[3] = {s.is, s.js, s.ks}, hi[3] = {s.ie, s.je, s.ke};
+      const int T1 = D == 0 ? 1 : 0, T2 = D == 2 ? 1 : 2;  // inner, outer loop directions
+      const int w0 = low ? lo[D] : hi[D], w1 = low ? w0 + 1 : w0 - 1;
+      const int c1 = 3 * D + 1, c2 = 3 * D + 2, c3 = 3 * D + 3;
+      const double sgn = low ? -1.0 : 1.0;
+      for (int t2 = lo[T2]; t2 <= hi[T2] - 1; ++t2)
+        for (int t1 = lo[T1]; t1 <= hi[T1] - 1; ++t1) {
+          // node at (tangential a, tangential b, layer)
+          auto at = [&](int a, int b, int layer, int& i, int& j, int& k) {
+            int ijk[3];
+            ijk[D] = layer; ijk[T1] = a; ijk[T2] = b;
+            i = ijk[0]; j = ijk[1]; k = ijk[2];
+          };
+          int I[4], J[4], K[4], Iw[4], Jw[4], Kw[4];
+          const int da[4] = {0, 1, 0, 1}, db[4] = {0, 0, 1, 1};  // corners 00, 10, 01, 11
+          for (int q = 0; q < 4; ++q) {
+            at(t1 + da[q], t2 + db[q], w1, I[q], J[q], K[q]);
+            at(t1 + da[q], t2 + db[q], w0, Iw[q], Jw[q], Kw[q]);
+          }
+          auto avg = [&](V f, int comp, const int* Ii, const int* Jj, const int* Kk) {
+            return (f(comp, Ii[0], Jj[0], Kk[0]) + f(comp, Ii[1], Jj[1], Kk[1]) + f(comp, Ii[2], Jj[2], Kk[2]) +
+                    f(comp, Ii[3], Jj[3], Kk[3])) * 0.25;
+          };
+          double uc = avg(pri, 2, I, J, K), vc = avg(pri, 3, I, J, K), wc = avg(pri, 4, I, J, K);
+          double pc = avg(pri, 5, Iw, Jw, Kw);
+          double t[4];
+          for (int q = 0; q < 4; ++q)
+            t[q] = 1.0 / std::sqrt(p2(m(c1, I[q], J[q], K[q])) + p2(m(c2, I[q], J[q], K[q])) +
+                                   p2(m(c3, I[q], J[q], K[q])));
+          auto mix = [&](int ca, int cb) {
+            return (m(ca, I[0], J[0], K[0]) * t[0] + m(ca, I[1], J[1], K[1]) * t[1] +
+                    m(cb, I[2], J[2], K[2]) * t[2] + m(cb, I[3], J[3], K[3]) * t[3]) * 0.25;
+          };
+          double nx = sgn * mix(c1, c2), ny = sgn * mix(c3, c1), nz = sgn * mix(c2, c3);
+          double miuc = avg(amu, 3, Iw, Jw, Kw);
+          int i0, j0, k0;
+          at(t1, t2, w0, i0, j0, k0);
+          // element area: the two tangential spacings in i, j, k order
+          double area = spcv[T1](1, i0, j0, k0) * spcv[T2](1, i0, j0, k0);
+          double dn = spcv[D](1, i0, j0, k0);
+          double n3[3] = {nx, ny, nz}, u3[3] = {uc, vc, wc};
+          double un = uc * nx + vc * ny + wc * nz;
+          for (int x = 0; x < 3; ++x) {
+            double f_prs = (pc - pinf) * area * n3[x];
+            double f_vis = miuc * (u3[x] - un * n3[x]) / dn * area / c.re;
+            fp[x] = fp[x] + f_prs;
+            fv[x] = fv[x] + f_vis;
+            ap[x] += std::fabs(f_prs);
+            av[x] += std::fabs(f_vis);
+          }
+        }
+    }
+  }
+  for (int x = 0; x < 3; ++x) {
+    out[x] = fp[x];
+    out[3 + x] = fv[x];
+    out[8 + x] = ap[x];
+    out[11 + x] = av[x];
+  }
+  out[6] = ((fp[1] + fv[1]) * std::cos(c.aoa) - (fp[0] + fv[0]) * std::sin(c.aoa)) * div;
+  out[7] = ((fp[1] + fv[1]) * std::sin(c.aoa) + (fp[0] + fv[0]) * std::cos(c.aoa)) * div;
+}
+
 // sub_init_flowfield.f90:29-111 (freestream start, iflag_init = 0).  ma, aoa in
 // degrees and dt come from Control.in; the nondimensional constants are derived
 // here exactly as the reference does.
@@ -756,6 +843,7 @@ void oracle_updatebuffercoordinate() { updatebuffercoordinate(); }
 void oracle_average1() { average1(); }
 void oracle_average2() { average2(); }
 void oracle_residual(double* out7) { residual(out7); }
+void oracle_clcd_output(double sref, double* out14) { clcd_output(sref, out14); }
 void oracle_init_flowfield(const double* ma, const double* aoa_deg, const double* dt) {
   init_flowfield(*ma, *aoa_deg, *dt);
 }
