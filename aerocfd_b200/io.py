@@ -1,4 +1,5 @@
-"""Reference input formats: Control.in, the grid file and the bcinfo file.
+"""Reference file formats: Control.in, the grid and bcinfo files, and the
+flow-field output that also serves as the restart file.
 
 The reference reads all three with Fortran list-directed input on rank 0:
 
@@ -15,7 +16,9 @@ The reference reads all three with Fortran list-directed input on rank 0:
 separators, ``d`` exponents, quoted strings, ``r*value`` repeats); ``write_*``
 produce files the reference can read.  ``load_case`` builds a
 :class:`~aerocfd_b200.case.Case` from a Control.in and the grid and bcinfo it
-names; ``save_case`` writes the three files for a case.
+names; ``save_case`` writes the three files for a case.  ``write_flowfield``
+and ``read_restart`` follow sub_output_flowfield.f90 and the restart branch of
+sub_init_flowfield.f90.
 """
 from __future__ import annotations
 
@@ -291,3 +294,67 @@ def save_case(case: Case, directory: str, control: Control = None) -> str:
     path = os.path.join(directory, "Control.in")
     write_control(path, c)
     return path
+
+
+# ------------------------------------------------- flow field output / restart
+def write_flowfield(path: str, case: Case) -> None:
+    """flowfield_output (sub_output_flowfield.f90:15-90, 3-D): per block a
+    Tecplot point-format zone of x, y, z, d, u, v, w, p, nut over the physical
+    nodes, i fastest, from the case's host arrays (sync them from the device
+    first).  Values carry 17 significant digits, so the file restarts a run
+    exactly as the reference's list-directed output does."""
+    with open(path, "w") as f:
+        for b in case.blocks:
+            s = b.sl(b.box0)
+            pri = b.fields["pri_v"][s]
+            cols = [b.fields["x"][s], b.fields["y"][s], b.fields["z"][s]] + [pri[..., c] for c in range(5)] + \
+                   [b.fields["nut"][s]]
+            f.write(" variables = x,y,z,d,u,v,w,p,nut\n")
+            f.write(f" zone i= {b.ni} j= {b.nj} k= {b.nk} datapacking=point\n")
+            table = np.stack([c.ravel() for c in cols], axis=1)
+            for row in table:
+                f.write(" ".join(f"{v:.17e}" for v in row) + "\n")
+
+
+def read_restart(path: str, case: Case) -> None:
+    """The restart branch of sub_init_flowfield.f90:117-268 (iflag_init = 1,
+    3-D): reads a flowfield file written by flowfield_output and sets, on the
+    physical nodes of every block, q from (d, u, v, w, p), the primitive
+    variables the reference derives there, rhs = rhsi = rhsv = 0, dt = the
+    Control.in dt, amu(1) = 1 and, with SA, nut.  The derived primitives keep
+    the reference's expressions, including q2 = d**2 + u**2 + v**2 and
+    c = sqrt(p)/ma; the iteration's start-up recomputes them from q."""
+    cfg = case.cfg
+    gamma = 1.4
+    ma = cfg.ma
+    cv = 1.0 / gamma / (gamma - 1.0) / ma / ma
+    r = _Reader(path)
+    for b in case.blocks:
+        r.skip(2)
+        n = b.ni * b.nj * b.nk
+        vals = r.read_array(9 * n).reshape(n, 9)
+        col = lambda c: vals[:, c].reshape(b.nk, b.nj, b.ni)
+        d, u, v, w, p, tur = col(3), col(4), col(5), col(6), col(7), col(8)
+        s = b.sl(b.box0)
+        t = p / d * gamma * ma * ma
+        q = b.fields["q"][s]
+        q[..., 0] = d
+        q[..., 1] = d * u
+        q[..., 2] = d * v
+        q[..., 3] = d * w
+        q[..., 4] = d * t * cv + 0.5 * d * (u * u + v * v + w * w)
+        pri = b.fields["pri_v"][s]
+        pri[..., 0] = q[..., 0]
+        pri[..., 1] = q[..., 1] / pri[..., 0]
+        pri[..., 2] = q[..., 2] / pri[..., 0]
+        pri[..., 3] = q[..., 3] / pri[..., 0]
+        q2 = pri[..., 0] ** 2 + pri[..., 1] ** 2 + pri[..., 2] ** 2
+        pri[..., 5] = (q[..., 4] / pri[..., 0] - 0.5 * q2) / cv
+        pri[..., 4] = pri[..., 0] * pri[..., 5] / gamma / ma / ma
+        pri[..., 6] = np.sqrt(pri[..., 4]) / ma
+        for name in ("rhs", "rhsi", "rhsv"):
+            b.fields[name][s] = 0.0
+        b.fields["dt"][s] = cfg.dt
+        b.fields["amu"][s][..., 0] = 1.0
+        if cfg.turbulence == 2:
+            b.fields["nut"][s] = tur

@@ -76,3 +76,38 @@ def test_bcinfo_2d_rows(tmp_path):
     (subs,) = io.read_bcinfo(str(p), 1, dimension=2)
     assert [(s.face, s.is_, s.ie, s.js, s.je, s.ks, s.ke, s.blk_t, s.subface_t, s.ori) for s in subs] == [
         (1, 1, 1, 1, 9, 1, 1, -50, 0, 0), (3, 1, 5, 1, 1, 1, 1, 2, 3, 1)]
+
+
+def test_flowfield_restart_round_trip(tmp_path, oracle_mod):
+    """A flow field written by write_flowfield restarts the same state: q
+    within a few ulps (q is rebuilt from d, u, v, w, p), nut exactly, and the
+    primitive variables the reference's restart derives, with its quirks
+    (q2 = d**2 + u**2 + v**2 in t, hence p; c = sqrt(p)/ma); those feed the first physical_bc
+    of the start-up, so a restarted run does not continue the original one bit
+    for bit in the reference either."""
+    make = lambda: grids.flat_plate(ni=17, nj=13, nk=5)
+    ca = make()
+    oa = oracle_mod.OracleCase(ca)
+    oa.geometry()
+    oa.init_flowfield()
+    oa.start()
+    oa.iterate(5)
+    path = str(tmp_path / "flowfield.dat")
+    io.write_flowfield(path, ca)
+    cb = make()
+    io.read_restart(path, cb)
+    ma, gamma = cb.cfg.ma, 1.4
+    cv = 1.0 / gamma / (gamma - 1.0) / ma / ma
+    for a, b in zip(ca.blocks, cb.blocks):
+        s = a.sl(a.box0)
+        qa, qb = a.fields["q"][s], b.fields["q"][s]
+        assert np.max(np.abs(qa - qb) / np.maximum(np.abs(qa), 1e-300)) < 1e-14
+        assert np.array_equal(a.fields["nut"][s], b.fields["nut"][s])
+        pa, pb = a.fields["pri_v"][s], b.fields["pri_v"][s]
+        assert np.allclose(pb[..., :4], pa[..., :4], rtol=1e-14, atol=1e-15)
+        d, u, v = pb[..., 0], pb[..., 1], pb[..., 2]
+        assert np.array_equal(pb[..., 5], (qb[..., 4] / d - 0.5 * (d ** 2 + u ** 2 + v ** 2)) / cv)
+        assert np.array_equal(pb[..., 4], d * pb[..., 5] / gamma / ma / ma)
+        assert np.array_equal(pb[..., 6], np.sqrt(pb[..., 4]) / ma)
+        assert np.all(b.fields["dt"][s] == cb.cfg.dt) and np.all(b.fields["amu"][s][..., 0] == 1.0)
+        assert not b.fields["rhs"][s].any()
