@@ -18,7 +18,7 @@ import numpy as np
 IFLAG_2D, IFLAG_3D = 2, 3
 IFLAG_NSSOLVER, IFLAG_EULERSOLVER = 0, 1
 IFLAG_STEADY, IFLAG_UNSTEADY = 0, 1
-IFLAG_1STIMPLICIT = 2
+IFLAG_1STIMPLICIT, IFLAG_2NDCRANK = 2, 3
 IFLAG_LAMINAR, IFLAG_SA = 0, 2
 IFLAG_3RDWENO = 4
 BC_INFLOW, BC_OUTFLOW, BC_SYMM, BC_WALL, BC_FARFIELD = -50, -40, -30, -20, -10
@@ -29,7 +29,7 @@ FIELDS: List[Tuple[str, int]] = [
     ("dxidx", 9), ("inv_j", 1), ("amu", 3), ("nut", 1), ("sa_rhs", 1),
     ("x", 1), ("y", 1), ("z", 1), ("dist", 1), ("alpha", 3), ("beta", 3),
     ("ggamma", 3), ("dudx", 9), ("tao", 6), ("vor", 1), ("length", 1),
-    ("spacing", 1),
+    ("spacing", 1), ("q0", 10),
 ]
 FIELD_ID = {name: n for n, (name, _) in enumerate(FIELDS)}
 FIELD_NC = dict(FIELDS)

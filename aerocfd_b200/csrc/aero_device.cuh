@@ -17,7 +17,7 @@ namespace aero {
 // Field ids of the C-ABI (AERO_F_* in include/aerocfd_gpu.h).
 enum FieldId {
   F_Q = 0, F_PRI, F_RHSI, F_RHSV, F_RHS, F_DT, F_DXIDX, F_INVJ, F_AMU, F_NUT, F_SARHS,
-  F_X, F_Y, F_Z, F_DIST, F_ALPHA, F_BETA, F_GAMMA, F_DUDX, F_TAO, F_VOR, F_LENGTH, F_SPACING,
+  F_X, F_Y, F_Z, F_DIST, F_ALPHA, F_BETA, F_GAMMA, F_DUDX, F_TAO, F_VOR, F_LENGTH, F_SPACING, F_Q0,
   // device-only scratch
   F_RA, F_RB, F_RC, F_DIAG, F_FVH, F_DIASD, F_SAS,
   F_NUM
@@ -25,9 +25,9 @@ enum FieldId {
 __host__ __device__ constexpr int field_nc(int f) {
   return f == F_Q ? 5 : f == F_PRI ? 7 : f == F_RHSI ? 5 : f == F_RHSV ? 5 : f == F_RHS ? 5
        : f == F_DXIDX ? 9 : f == F_AMU ? 3 : f == F_ALPHA ? 3 : f == F_BETA ? 3 : f == F_GAMMA ? 3
-       : f == F_DUDX ? 9 : f == F_TAO ? 6 : f == F_FVH ? 15 : f == F_SAS ? 7 : 1;
+       : f == F_DUDX ? 9 : f == F_TAO ? 6 : f == F_FVH ? 15 : f == F_SAS ? 7 : f == F_Q0 ? 10 : 1;
 }
-constexpr int kNumPublicFields = F_SPACING + 1;
+constexpr int kNumPublicFields = F_Q0 + 1;
 
 struct Box {
   int is, ie, js, je, ks, ke;
@@ -120,6 +120,7 @@ constexpr double SA_CV13 = SA_CV1 * SA_CV1 * SA_CV1;
 enum {
   IFLAG_2D = 2, IFLAG_3D = 3, IFLAG_NSSOLVER = 0, IFLAG_EULERSOLVER = 1,
   IFLAG_STEADY = 0, IFLAG_UNSTEADY = 1, IFLAG_LAMINAR = 0, IFLAG_SA = 2,
+  IFLAG_1STIMPLICIT = 2, IFLAG_2NDCRANK = 3,
   IFLAG_DES97 = 1, IFLAG_DDES = 2,
   BC_INFLOW = -50, BC_OUTFLOW = -40, BC_SYMM = -30, BC_WALL = -20, BC_FARFIELD = -10,
 };

@@ -44,6 +44,10 @@ struct WallFace {
 __global__ void k_getpri(const BlockView* __restrict__ blocks, CaseConsts cc, unsigned* status);
 __global__ void k_forces(const BlockView* __restrict__ blocks, const WallFace* __restrict__ walls, int nwall,
                          long nquad, CaseConsts cc, double* __restrict__ part);
+__global__ void k_crank_rhs(const BlockView* __restrict__ blocks);
+__global__ void k_crank_sweep(const BlockView* __restrict__ blocks, int d, double gamma);
+__global__ void k_crank_update(const BlockView* __restrict__ blocks);
+__global__ void k_update_q0(const BlockView* __restrict__ blocks);
 __global__ void k_forces_final(const double* __restrict__ part, int npart, CaseConsts cc, double sref,
                                double* __restrict__ out8);
 __global__ void k_fill(const BlockView* __restrict__ blocks, int fid, int nc, double val);

@@ -91,6 +91,7 @@ struct State {
   size_t staging_doubles = 0;
   double totalnodes = 0;
   long max_box = 0, max_b0 = 0, max_b1 = 0, max_ext = 0;
+  Box max_b1_box{1, 0, 1, 0, 1, 0};  // largest updated extent per direction over the blocks
   int max_ops = 0;       // most physical-BC subfaces in one block
   long max_face = 0;     // most nodes in one physical-BC subface
   std::map<const double*, std::pair<int, int>> registry;  // host array -> (block, field)
@@ -116,13 +117,13 @@ State g;
 enum ProfId {
   P_GETPRI, P_FILL, P_INVISCID, P_VISC_A, P_VISC_B, P_FIND_DT, P_DT_MINMAX, P_LUSGS_PREP,
   P_LUSGS_MATS, P_LUSGS_SWEEP, P_LUSGS_UPDATE, P_SA_A, P_SA_B, P_SA_RECS, P_SA_SWEEP, P_INDEX, P_BC, P_SA_CLIP, P_HALO, P_AVG_GATHER, P_AVG_APPLY, P_RESID_PART, P_RESID_FINAL,
-  P_TRANSFER, P_GEOMETRY, P_FORCES, P_NUM
+  P_TRANSFER, P_GEOMETRY, P_FORCES, P_CRANK, P_NUM
 };
 const char* kProfName[P_NUM] = {
     "k_getpri", "k_fill", "k_inviscid", "k_viscous_a", "k_viscous_b", "k_find_dt", "k_dt_minmax",
     "k_lusgs_prep", "k_lusgs_mats", "k_lusgs_sweep", "k_lusgs_update", "k_sa_a", "k_sa_b", "k_sa_recs", "k_sa_sweep",
     "k_plane_index", "k_physical_bc", "k_sa_clip", "k_halo", "k_avg_gather",
-    "k_avg_apply", "k_residual_partial", "k_residual_final", "k_transfer", "k_geometry", "k_forces"};
+    "k_avg_apply", "k_residual_partial", "k_residual_final", "k_transfer", "k_geometry", "k_forces", "k_crank"};
 struct Prof {
   bool on = false;
   std::vector<cudaEvent_t> pool;
@@ -556,7 +557,54 @@ int do_getpri_all() {
 // the start of the next one, so the device computes them once, at the start;
 // aero_step recomputes them after its last iteration so the state it leaves
 // matches the reference's.
+// crank2nd on nblk views (sub_timeadvancement_2ndcrank.f90): dual-time rhs,
+// dq = 0, the i, j, k line recurrences, q += dq/inv_j.
+int launch_crank(const BlockView* views, int nblk, long maxN, long maxN1, const Box* lines, const CaseConsts& cc) {
+  PROF(P_CRANK, (k_crank_rhs<<<dim3(cdiv(maxN1, 256), nblk), 256, 0, g.stream>>>(views)));
+  CKL();
+  PROF(P_CRANK, (k_fill<<<dim3(cdiv(maxN, 256), nblk), 256, 0, g.stream>>>(views, F_FVH, 5, 0.0)));
+  CKL();
+  const long nl[3] = {(long)lines->ny() * lines->nz(), (long)lines->nx() * lines->nz(), (long)lines->nx() * lines->ny()};
+  for (int d = 0; d < 3; ++d) {
+    PROF(P_CRANK, (k_crank_sweep<<<dim3(cdiv(nl[d], 64), nblk), 64, 0, g.stream>>>(views, d, cc.gamma)));
+    CKL();
+  }
+  PROF(P_CRANK, (k_crank_update<<<dim3(cdiv(maxN1, 256), nblk), 256, 0, g.stream>>>(views)));
+  CKL();
+  return AERO_OK;
+}
+
+bool crank_on() { return g.cc.time == IFLAG_UNSTEADY; }
+
+// main.f90:450-573: three dual-time sub-iterations, then update_q0, SA and
+// the closing BCs / halo / averaging (the primitives are recomputed by the
+// caller, as after the implicit path).  find_dt's unsteady branch leaves dt
+// unchanged, so it launches nothing here.
+int do_iteration_crank() {
+  int nb = (int)g.blocks.size();
+  int rc;
+  for (int sub = 1; sub <= 3; ++sub) {
+    if ((rc = do_physical_bc())) return rc;
+    if ((rc = do_halo())) return rc;
+    if ((rc = do_average1())) return rc;
+    if ((rc = do_average2())) return rc;
+    if ((rc = do_getpri_all())) return rc;
+    if ((rc = launch_inviscid(g.d_blocks, nb, g.max_box, g.max_b1, g.cc))) return rc;
+    if (viscous_on() && (rc = launch_viscous(g.d_blocks, nb, g.max_b0, g.cc, 0))) return rc;
+    if ((rc = launch_crank(g.d_blocks, nb, g.max_box, g.max_b1, &g.max_b1_box, g.cc))) return rc;
+  }
+  PROF(P_CRANK, (k_update_q0<<<dim3(cdiv(g.max_b0, 256), nb), 256, 0, g.stream>>>(g.d_blocks)));
+  CKL();
+  if (sa_on() && (rc = launch_sa(g.d_blocks, nb, g.max_box, g.max_b1, g.pmax_all, g.cc))) return rc;
+  if ((rc = do_physical_bc())) return rc;
+  if ((rc = do_halo())) return rc;
+  if ((rc = do_average1())) return rc;
+  if ((rc = do_average2())) return rc;
+  return AERO_OK;
+}
+
 int do_iteration(bool want_dt_minmax) {
+  if (crank_on()) return do_iteration_crank();
   int nb = (int)g.blocks.size();
   int rc;
   if ((rc = do_getpri_all())) return rc;
@@ -664,8 +712,12 @@ int aero_configure(const int* iflags, const double* params) {
   if (iflags[0] != IFLAG_3D) return fail(AERO_ERR_ARG, "iflag_dimension=%d: only 3-D is supported", iflags[0]);
   if (iflags[1] != IFLAG_NSSOLVER && iflags[1] != IFLAG_EULERSOLVER)
     return fail(AERO_ERR_ARG, "iflag_solver=%d is not 0 (NS) or 1 (Euler)", iflags[1]);
-  if (iflags[2] != IFLAG_STEADY) return fail(AERO_ERR_ARG, "iflag_time=%d: only steady is supported", iflags[2]);
-  if (iflags[3] != 2) return fail(AERO_ERR_ARG, "iflag_timeadvance=%d: only 1st-order implicit (2)", iflags[3]);
+  bool steady_lusgs = iflags[2] == IFLAG_STEADY && iflags[3] == IFLAG_1STIMPLICIT;
+  bool unsteady_crank = iflags[2] == IFLAG_UNSTEADY && iflags[3] == IFLAG_2NDCRANK;
+  if (!steady_lusgs && !unsteady_crank)
+    return fail(AERO_ERR_ARG,
+                "iflag_time=%d/iflag_timeadvance=%d: supported are steady 1st-order implicit (0/2) and "
+                "unsteady 2nd-order Crank-Nicolson (1/3)", iflags[2], iflags[3]);
   if (iflags[4] != IFLAG_LAMINAR && iflags[4] != IFLAG_SA)
     return fail(AERO_ERR_ARG, "Wrong turbulence model type is input!!! (%d)", iflags[4]);
   if (iflags[6] != 2 || iflags[7] != 4)
@@ -756,6 +808,7 @@ int aero_finish_setup(void) {
   // arena
   size_t total = 0;
   g.max_box = g.max_b0 = g.max_b1 = g.max_ext = 0;
+  g.max_b1_box = Box{1, 0, 1, 0, 1, 0};
   g.totalnodes = 0;
   long max_b1 = 0;
   for (auto& H : g.blocks) {
@@ -768,6 +821,9 @@ int aero_finish_setup(void) {
     Box e{H.b1.is - 1, H.b1.ie + 1, H.b1.js - 1, H.b1.je + 1, H.b1.ks - 1, H.b1.ke + 1};
     g.max_ext = std::max(g.max_ext, e.size());
     g.totalnodes += (double)H.b0.size();
+    g.max_b1_box.ie = std::max(g.max_b1_box.ie, H.b1.nx());
+    g.max_b1_box.je = std::max(g.max_b1_box.je, H.b1.ny());
+    g.max_b1_box.ke = std::max(g.max_b1_box.ke, H.b1.nz());
   }
   g.max_b1 = max_b1;
   CK(cudaMalloc(&g.arena, total * sizeof(double)));
@@ -974,6 +1030,42 @@ int aero_implicit1st(double* q, const double* dt, const double* pri_v, double* r
   return finish(t, args);
 }
 
+int aero_crank2nd(double* q, const double* q0, const double* dt, const double* pri_v, double* rhs,
+                  const double* rhsi, const double* rhsv, const double* dxidx, const double* inv_j,
+                  const int* is, const int* ie, const int* js, const int* je, const int* ks, const int* ke,
+                  const int* is0, const int* ie0, const int* js0, const int* je0, const int* ks0,
+                  const int* ke0, const int* is1, const int* ie1, const int* js1, const int* je1,
+                  const int* ks1, const int* ke1, const double* gamma, const int* mm, const int* ssub) {
+  (void)mm; (void)ssub;
+  int rc = need_init();
+  if (rc) return rc;
+  Box b = box_of(is, ie, js, je, ks, ke), b0 = box_of(is0, ie0, js0, je0, ks0, ke0),
+      b1 = box_of(is1, ie1, js1, je1, ks1, ke1);
+  std::vector<Arg> args = {{F_Q, q, true},         {F_Q0, q0, false},     {F_DT, dt, false},
+                           {F_PRI, pri_v, false},  {F_RHS, rhs, true},    {F_RHSI, rhsi, false},
+                           {F_RHSV, rhsv, false},  {F_DXIDX, dxidx, false}, {F_INVJ, inv_j, false}};
+  BlockTarget t;
+  if ((rc = resolve(b, b0, b1, args, t))) return rc;
+  CaseConsts cc = consts_with(*gamma, g.cc.cv, g.cc.re);
+  Box lines{1, b1.nx(), 1, b1.ny(), 1, b1.nz()};
+  if ((rc = launch_crank(t.d_view, 1, b.size(), b1.size(), &lines, cc))) return rc;
+  return finish(t, args);
+}
+
+int aero_update_q0(double* q0, const double* q, const int* is, const int* ie, const int* js, const int* je,
+                   const int* ks, const int* ke, const int* is0, const int* ie0, const int* js0,
+                   const int* je0, const int* ks0, const int* ke0) {
+  int rc = need_init();
+  if (rc) return rc;
+  Box b = box_of(is, ie, js, je, ks, ke), b0 = box_of(is0, ie0, js0, je0, ks0, ke0);
+  std::vector<Arg> args = {{F_Q0, q0, true}, {F_Q, q, false}};
+  BlockTarget t;
+  if ((rc = resolve(b, b0, b0, args, t))) return rc;
+  PROF(P_CRANK, (k_update_q0<<<cdiv(b0.size(), 256), 256, 0, g.stream>>>(t.d_view)));
+  CKL();
+  return finish(t, args);
+}
+
 // ------------------------------------------------------ module-state routines
 int aero_physical_bc(void) {
   int rc = need_setup();
@@ -1059,6 +1151,8 @@ int aero_init_flowfield(void) {
     for (int x = 0; x < 7; ++x) if ((rc = put(v.f[F_PRI] + x * v.plane, pv[x]))) return rc;
     for (int x = 0; x < 3; ++x) if ((rc = put(v.f[F_AMU] + x * v.plane, av[x]))) return rc;
     if ((rc = put(v.f[F_DT], g.params[5]))) return rc;
+    for (int x = 0; x < 10; ++x)  // q0(l, c) = q(c) at both time levels (sub_init_flowfield.f90:78-82)
+      if ((rc = put(v.f[F_Q0] + x * v.plane, qv[x / 2]))) return rc;
     if (sa) {
       if ((rc = put(v.f[F_NUT], c.nutinf))) return rc;
       if ((rc = put(v.f[F_SARHS], 0.0))) return rc;
@@ -1202,6 +1296,7 @@ int aero_step_timed(int nsteps, int flush_l2, double* device_ms) {
     if (flush_l2) CK(cudaMemsetAsync(flush, s & 0xff, fbytes, g.stream));
     CK(cudaEventRecord(a, g.stream));
     if ((rc = do_iteration(false))) return rc;
+    if ((rc = do_getpri_all())) return rc;  // end of the time step (main.f90:434-447)
     if ((rc = do_residual(g.d_out))) return rc;
     CK(cudaEventRecord(b, g.stream));
     CK(cudaEventSynchronize(b));
@@ -1209,7 +1304,6 @@ int aero_step_timed(int nsteps, int flush_l2, double* device_ms) {
     CK(cudaEventElapsedTime(&ms, a, b));
     total += ms;
   }
-  if (nsteps > 0 && (rc = do_getpri_all())) return rc;
   CK(cudaStreamSynchronize(g.stream));
   cudaEventDestroy(a);
   cudaEventDestroy(b);
@@ -1252,6 +1346,7 @@ int aero_step(int nsteps, double* resid_hist, double* dt_minmax) {
   for (int s = 0; s < nsteps; ++s) {
     bool last = (s == nsteps - 1);
     if ((rc = do_iteration(last && dt_minmax != nullptr))) return rc;
+    if ((rc = do_getpri_all())) return rc;  // end of the time step (main.f90:434-447)
     if (resid_hist) {
       if ((rc = do_residual(g.d_out))) return rc;
       CK(cudaMemcpyAsync(g.h_out, g.d_out, 7 * sizeof(double), cudaMemcpyDeviceToHost, g.stream));
@@ -1259,7 +1354,6 @@ int aero_step(int nsteps, double* resid_hist, double* dt_minmax) {
       std::memcpy(resid_hist + 7 * s, g.h_out, 7 * sizeof(double));
     }
   }
-  if (nsteps > 0 && (rc = do_getpri_all())) return rc;
   if (dt_minmax) {
     CK(cudaMemcpyAsync(g.h_out + 7, g.d_out + 7, 2 * sizeof(double), cudaMemcpyDeviceToHost, g.stream));
     CK(cudaStreamSynchronize(g.stream));

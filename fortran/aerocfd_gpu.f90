@@ -25,7 +25,7 @@ module aerocfd_gpu
                                AERO_F_AMU = 8, AERO_F_NUT = 9, AERO_F_SA_RHS = 10, AERO_F_X = 11, &
                                AERO_F_Y = 12, AERO_F_Z = 13, AERO_F_DIST = 14, AERO_F_ALPHA = 15, &
                                AERO_F_BETA = 16, AERO_F_GGAMMA = 17, AERO_F_DUDX = 18, AERO_F_TAO = 19, &
-                               AERO_F_VOR = 20, AERO_F_LENGTH = 21, AERO_F_SPACING = 22
+                               AERO_F_VOR = 20, AERO_F_LENGTH = 21, AERO_F_SPACING = 22, AERO_F_Q0 = 23
 
   interface
     integer(c_int) function aero_init(device) bind(C, name="aero_init")
@@ -54,6 +54,27 @@ module aerocfd_gpu
       import :: c_int, c_ptr
       integer(c_int), value :: m, field
       type(c_ptr), value :: host
+    end function
+
+    ! sub_timeadvancement_2ndcrank.f90:1 (crank2nd)
+    integer(c_int) function aero_crank2nd(q, q0, dt, pri_v, rhs, rhsi, rhsv, dxidx, inv_j, &
+        is, ie, js, je, ks, ke, is0, ie0, js0, je0, ks0, ke0, is1, ie1, js1, je1, ks1, ke1, &
+        gamma, mm, ssub) bind(C, name="aero_crank2nd")
+      import :: c_int, c_double
+      integer(c_int) :: is, ie, js, je, ks, ke, is0, ie0, js0, je0, ks0, ke0
+      integer(c_int) :: is1, ie1, js1, je1, ks1, ke1, mm, ssub
+      real(c_double) :: q(5, is:ie, js:je, ks:ke), q0(-1:0, 5, is:ie, js:je, ks:ke), dt(is:ie, js:je, ks:ke)
+      real(c_double) :: pri_v(7, is:ie, js:je, ks:ke), rhs(5, is:ie, js:je, ks:ke)
+      real(c_double) :: rhsi(5, is:ie, js:je, ks:ke), rhsv(5, is:ie, js:je, ks:ke)
+      real(c_double) :: dxidx(9, is:ie, js:je, ks:ke), inv_j(is:ie, js:je, ks:ke), gamma
+    end function
+
+    ! main.f90:692 (update_q0)
+    integer(c_int) function aero_update_q0(q0, q, is, ie, js, je, ks, ke, is0, ie0, js0, je0, ks0, ke0) &
+        bind(C, name="aero_update_q0")
+      import :: c_int, c_double
+      integer(c_int) :: is, ie, js, je, ks, ke, is0, ie0, js0, je0, ks0, ke0
+      real(c_double) :: q0(-1:0, 5, is:ie, js:je, ks:ke), q(5, is:ie, js:je, ks:ke)
     end function
 
     ! sub_output_forceintegration.f90:8 (clcd_output): out8 = fp(3), fv(3), cl, cd

@@ -23,8 +23,9 @@
  *    its module state.
  *
  * One host thread drives the library; calls run in order on the library's
- * CUDA stream.  Only 3-D cases (iflag_dimension = 3) and the 1st-order
- * implicit time advance are supported; other flags are rejected.
+ * CUDA stream.  Only 3-D cases (iflag_dimension = 3) are supported, with the
+ * steady 1st-order implicit (LU-SGS) or the unsteady 2nd-order Crank-Nicolson
+ * time advance; other flags are rejected.
  */
 #ifndef AEROCFD_GPU_H
 #define AEROCFD_GPU_H
@@ -66,6 +67,7 @@ enum {
   AERO_F_VOR,       /* vor(...)                                             */
   AERO_F_LENGTH,    /* length(...)    SA length scale                       */
   AERO_F_SPACING,   /* spacing(...)                                         */
+  AERO_F_Q0,        /* q0(-1:0,5,...) the two earlier time levels (Crank-Nicolson) */
   AERO_NUM_FIELDS
 };
 #define AERO_MASK(f) (1ull << (f))
@@ -162,6 +164,21 @@ int aero_gridtransformation(double* dxidx, double* inv_j, double* alpha, double*
                             const int* ke, const int* is0, const int* ie0, const int* js0,
                             const int* je0, const int* ks0, const int* ke0, const int* m0);
 
+/* sub_timeadvancement_2ndcrank.f90:1-11 (crank2nd, 3-D): the dual-time
+ * Crank-Nicolson sub-iteration update of q (alph = 1/2) with the factorised
+ * point-implicit i, j, k line recurrences; q0 is q0(-1:0,5,is:ie,js:je,ks:ke).
+ * mm and ssub are accepted for the reference's argument list. */
+int aero_crank2nd(double* q, const double* q0, const double* dt, const double* pri_v, double* rhs,
+                  const double* rhsi, const double* rhsv, const double* dxidx, const double* inv_j,
+                  const int* is, const int* ie, const int* js, const int* je, const int* ks, const int* ke,
+                  const int* is0, const int* ie0, const int* js0, const int* je0, const int* ks0,
+                  const int* ke0, const int* is1, const int* ie1, const int* js1, const int* je1,
+                  const int* ks1, const int* ke1, const double* gamma, const int* mm, const int* ssub);
+/* main.f90:692-711 (update_q0): q0(-1) = q0(0), q0(0) = q on the physical nodes */
+int aero_update_q0(double* q0, const double* q, const int* is, const int* ie, const int* js, const int* je,
+                   const int* ks, const int* ke, const int* is0, const int* ie0, const int* js0,
+                   const int* je0, const int* ks0, const int* ke0);
+
 /* ---- module-state routines (no arguments in the reference) ------------ */
 int aero_physical_bc(void);          /* sub_bc.f90:9                        */
 int aero_updatebuffer(void);         /* sub_bc_updatebuffer.f90:10          */
@@ -190,10 +207,13 @@ int aero_compute_geometry(int with_walldist);
 /* primitives of all registered blocks (main.f90:434-447) */
 int aero_getpri_all(void);
 
-/* ---- whole iterations (main.f90:343-447 for every block, plus the residual
+/* ---- whole iterations (main.f90:343-447, or :450-573 for Crank-Nicolson,
+ *      for every block, plus the residual
  *      of main.f90:603 each step); resid_hist receives nsteps x 7 values
  *      when not NULL.  dt_minmax (may be NULL) receives dtmax, dtmin of the
- *      last block's find_dt of the last step. ------------------------------ */
+ *      last block's find_dt of the last step (steady runs; the unsteady
+ *      find_dt leaves dt unchanged and dt_minmax is not written).  Every step
+ *      ends with the primitives of all blocks, as main.f90:434-447. ------- */
 int aero_step(int nsteps, double* resid_hist, double* dt_minmax);
 
 /* Benchmark form of aero_step: nsteps iterations, each with its residual

@@ -742,3 +742,138 @@ void sa_model(V nut, V sa_rhs, V dt, V pri_v, V amu, V dudx, V vor, V dxidx, V i
 }
 
 }  // namespace oracle
+
+namespace oracle {
+
+// q0(l, c, i, j, k) with l = -1, 0 (sub_init_allocatememory.f90:285): the
+// time level is the fastest index, then the component.
+static inline double& Q0(V q0, int l, int c, int i, int j, int k) { return q0(1 + (l + 1) + 2 * (c - 1), i, j, k); }
+
+// One point of the factorised sweep (sub_timeadvancement_2ndcrank.f90:129-161
+// and its j, k twins): a = the flux-Jacobian product of neighbour node nb
+// with its dq, plus/minus the spectral radius (sgn = +1 forward, -1
+// backward); cb = first metric component of the direction.
+static inline void crank_a(V pri_v, V dxidx, double r, int cb, double hdv, double gamma, const double s[5],
+                           double sgn, int i, int j, int k, double a[5]) {
+  double u = pri_v(2, i, j, k), v = pri_v(3, i, j, k), w = pri_v(4, i, j, k), c = pri_v(7, i, j, k);
+  double dxidx0 = dxidx(cb, i, j, k), dxidy0 = dxidx(cb + 1, i, j, k), dxidz0 = dxidx(cb + 2, i, j, k);
+  double q2 = 0.5 * (p2(u) + p2(v) + p2(w));
+  double h = p2(c) / (gamma - 1.0) + q2;
+  double cu = dxidx0 * u + dxidy0 * v + dxidz0 * w;
+  double b1 = hdv * (-(cu * s[0]) + dxidx0 * s[1] + dxidy0 * s[2] + dxidz0 * s[3]);
+  double b2 = hdv * (q2 * s[0] - u * s[1] - v * s[2] - w * s[3] + s[4]) * (gamma - 1.0);
+  double b3 = sgn > 0 ? hdv * (cu + r) : hdv * (cu - r);
+  a[0] = b1 + b3 * s[0];
+  a[1] = b1 * u + b2 * dxidx0 + b3 * s[1];
+  a[2] = b1 * v + b2 * dxidy0 + b3 * s[2];
+  a[3] = b1 * w + b2 * dxidz0 + b3 * s[3];
+  a[4] = b1 * h + b2 * cu + b3 * s[4];
+}
+
+static inline double crank_rou(V pri_v, V dxidx, int cb, int i, int j, int k) {
+  double u = pri_v(2, i, j, k), v = pri_v(3, i, j, k), w = pri_v(4, i, j, k), c = pri_v(7, i, j, k);
+  double x0 = dxidx(cb, i, j, k), y0 = dxidx(cb + 1, i, j, k), z0 = dxidx(cb + 2, i, j, k);
+  double temp = p2(x0) + p2(y0) + p2(z0);
+  temp = std::sqrt(temp);
+  double cu = u * x0 + v * y0 + w * z0;
+  return std::fabs(cu) + std::fabs(c * temp);
+}
+
+// sub_timeadvancement_2ndcrank.f90:1-466 (crank2nd, 3-D): the dual-time
+// right-hand side with alph = 1/2, then the approximately factorised
+// point-implicit sweeps along i, j and k lines and q += dq/inv_j.  The forward
+// k recurrence starts at ks1+1, as in the reference (:352).
+void crank2nd(V q, V q0, V dt, V pri_v, V rhs, V rhsi, V rhsv, V dxidx, V inv_j, const Box& b, const Box& b0,
+              const Box& b1, double gamma) {
+  (void)b0;
+  for (int k = b1.ks; k <= b1.ke; ++k)
+    for (int j = b1.js; j <= b1.je; ++j)
+      for (int i = b1.is; i <= b1.ie; ++i)
+        for (int c = 1; c <= 5; ++c) rhs(c, i, j, k) = rhsi(c, i, j, k) + rhsv(c, i, j, k);
+  const double alph = 0.5;
+  const double alph_i = 1.0 / (1.0 + alph);
+  for (int k = b1.ks; k <= b1.ke; ++k)
+    for (int j = b1.js; j <= b1.je; ++j)
+      for (int i = b1.is; i <= b1.ie; ++i)
+        for (int c = 1; c <= 5; ++c)
+          rhs(c, i, j, k) = alph_i * (rhs(c, i, j, k) * dt(i, j, k) -
+                                      ((1.0 + alph) * q(c, i, j, k) - (1.0 + 2.0 * alph) * Q0(q0, 0, c, i, j, k) +
+                                       alph * Q0(q0, -1, c, i, j, k)) * inv_j(i, j, k));
+  std::vector<double> dtsub_s(b.size(), 0.0), rou_s(b.size(), 0.0), dq_s(5 * (size_t)b.size(), 0.0);
+  V dtsub{dtsub_s.data(), 1, b}, rou{rou_s.data(), 1, b}, dq{dq_s.data(), 5, b};
+  for (int k = b1.ks - 1; k <= b1.ke + 1; ++k)
+    for (int j = b1.js - 1; j <= b1.je + 1; ++j)
+      for (int i = b1.is - 1; i <= b1.ie + 1; ++i) dtsub(i, j, k) = dt(i, j, k) / (1.0 + alph);
+  double s[5], a[5];
+  auto load = [&](int i, int j, int k) {
+    for (int c = 0; c < 5; ++c) s[c] = dq(c + 1, i, j, k);
+  };
+  // i lines
+  for (int k = b1.ks; k <= b1.ke; ++k)
+    for (int j = b1.js; j <= b1.je; ++j) {
+      for (int i = b1.is - 1; i <= b1.ie + 1; ++i) rou(i, j, k) = crank_rou(pri_v, dxidx, 1, i, j, k);
+      for (int i = b1.is; i <= b1.ie; ++i) {
+        load(i - 1, j, k);
+        crank_a(pri_v, dxidx, rou(i - 1, j, k), 1, 0.5 * dtsub(i, j, k), gamma, s, 1.0, i - 1, j, k, a);
+        double div = 1.0 / (1.0 + dtsub(i, j, k) * rou(i, j, k));
+        for (int c = 0; c < 5; ++c) dq(c + 1, i, j, k) = div * (rhs(c + 1, i, j, k) + a[c]);
+      }
+      for (int i = b1.ie; i >= b1.is; --i) {
+        load(i + 1, j, k);
+        crank_a(pri_v, dxidx, rou(i + 1, j, k), 1, 0.5 * dtsub(i, j, k), gamma, s, -1.0, i + 1, j, k, a);
+        double div = 1.0 / (1.0 + dtsub(i, j, k) * rou(i, j, k));
+        for (int c = 0; c < 5; ++c) dq(c + 1, i, j, k) = dq(c + 1, i, j, k) - div * a[c];
+      }
+    }
+  // j lines
+  for (int k = b1.ks; k <= b1.ke; ++k)
+    for (int i = b1.is; i <= b1.ie; ++i) {
+      for (int j = b1.js - 1; j <= b1.je + 1; ++j) rou(i, j, k) = crank_rou(pri_v, dxidx, 4, i, j, k);
+      for (int j = b1.js; j <= b1.je; ++j) {
+        load(i, j - 1, k);
+        crank_a(pri_v, dxidx, rou(i, j - 1, k), 4, 0.5 * dtsub(i, j, k), gamma, s, 1.0, i, j - 1, k, a);
+        double div = 1.0 / (1.0 + dtsub(i, j, k) * rou(i, j, k));
+        for (int c = 0; c < 5; ++c) dq(c + 1, i, j, k) = div * (dq(c + 1, i, j, k) + a[c]);
+      }
+      for (int j = b1.je; j >= b1.js; --j) {
+        load(i, j + 1, k);
+        crank_a(pri_v, dxidx, rou(i, j + 1, k), 4, 0.5 * dtsub(i, j, k), gamma, s, -1.0, i, j + 1, k, a);
+        double div = 1.0 / (1.0 + dtsub(i, j, k) * rou(i, j, k));
+        for (int c = 0; c < 5; ++c) dq(c + 1, i, j, k) = dq(c + 1, i, j, k) - div * a[c];
+      }
+    }
+  // k lines
+  for (int j = b1.js; j <= b1.je; ++j)
+    for (int i = b1.is; i <= b1.ie; ++i) {
+      for (int k = b1.ks - 1; k <= b1.ke + 1; ++k) rou(i, j, k) = crank_rou(pri_v, dxidx, 7, i, j, k);
+      for (int k = b1.ks + 1; k <= b1.ke; ++k) {
+        load(i, j, k - 1);
+        crank_a(pri_v, dxidx, rou(i, j, k - 1), 7, 0.5 * dtsub(i, j, k), gamma, s, 1.0, i, j, k - 1, a);
+        double div = 1.0 / (1.0 + dtsub(i, j, k) * rou(i, j, k));
+        for (int c = 0; c < 5; ++c) dq(c + 1, i, j, k) = div * (dq(c + 1, i, j, k) + a[c]);
+      }
+      for (int k = b1.ke - 1; k >= b1.ks; --k) {
+        load(i, j, k + 1);
+        crank_a(pri_v, dxidx, rou(i, j, k + 1), 7, 0.5 * dtsub(i, j, k), gamma, s, -1.0, i, j, k + 1, a);
+        double div = 1.0 / (1.0 + dtsub(i, j, k) * rou(i, j, k));
+        for (int c = 0; c < 5; ++c) dq(c + 1, i, j, k) = dq(c + 1, i, j, k) - div * a[c];
+      }
+    }
+  for (int k = b1.ks; k <= b1.ke; ++k)
+    for (int j = b1.js; j <= b1.je; ++j)
+      for (int i = b1.is; i <= b1.ie; ++i)
+        for (int c = 1; c <= 5; ++c) q(c, i, j, k) = q(c, i, j, k) + dq(c, i, j, k) / inv_j(i, j, k);
+}
+
+// main.f90:692-711: q0(-1) = q0(0), q0(0) = q on the physical nodes.
+void update_q0(V q0, V q, const Box& b0) {
+  for (int k = b0.ks; k <= b0.ke; ++k)
+    for (int j = b0.js; j <= b0.je; ++j)
+      for (int i = b0.is; i <= b0.ie; ++i)
+        for (int c = 1; c <= 5; ++c) {
+          Q0(q0, -1, c, i, j, k) = Q0(q0, 0, c, i, j, k);
+          Q0(q0, 0, c, i, j, k) = q(c, i, j, k);
+        }
+}
+
+}  // namespace oracle

@@ -17,6 +17,9 @@ void find_dt(V dt, double* dtmax, double* dtmin, double* cflmax, double* cflmin,
              V dxidx, double re, double* cfl, const Box& b, int iflag_time);
 void calc_jm(double a[25], double q1, double q2, double q3, double q4, double q5, double dxidx,
              double dxidy, double dxidz, double gamma);
+void crank2nd(V q, V q0, V dt, V pri_v, V rhs, V rhsi, V rhsv, V dxidx, V inv_j, const Box& b, const Box& b0,
+              const Box& b1, double gamma);
+void update_q0(V q0, V q, const Box& b0);
 void implicit1st(V q, V dt, V pri_v, V rhs, V rhsi, V rhsv, V dxidx, V inv_j, const Box& b,
                  const Box& b0, const Box& b1, double gamma, double cfl);
 void sa_model(V nut, V sa_rhs, V dt, V pri_v, V amu, V dudx, V vor, V dxidx, V inv_j, V alpha,

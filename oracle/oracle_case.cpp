@@ -15,10 +15,10 @@ namespace oracle {
 
 enum Field {
   F_Q, F_PRI, F_RHSI, F_RHSV, F_RHS, F_DT, F_DXIDX, F_INVJ, F_AMU, F_NUT, F_SARHS,
-  F_X, F_Y, F_Z, F_DIST, F_ALPHA, F_BETA, F_GAMMA, F_DUDX, F_TAO, F_VOR, F_LENGTH, F_SPACING,
+  F_X, F_Y, F_Z, F_DIST, F_ALPHA, F_BETA, F_GAMMA, F_DUDX, F_TAO, F_VOR, F_LENGTH, F_SPACING, F_Q0,
   F_COUNT
 };
-static const int kNc[F_COUNT] = {5, 7, 5, 5, 5, 1, 9, 1, 3, 1, 1, 1, 1, 1, 1, 3, 3, 3, 9, 6, 1, 1, 1};
+static const int kNc[F_COUNT] = {5, 7, 5, 5, 5, 1, 9, 1, 3, 1, 1, 1, 1, 1, 1, 3, 3, 3, 9, 6, 1, 1, 1, 10};
 
 struct Sub {
   int f_no, face, is, ie, js, je, ks, ke, blk_t, subface_t, ori;
@@ -575,6 +575,8 @@ void init_flowfield(double ma, double aoa_deg, double dt) {
       q.p[5 * n + 2] = c.d_0 * c.u_0 * std::sin(c.aoa);
       q.p[5 * n + 3] = 0.0;
       q.p[5 * n + 4] = c.d_0 * c.t_0 * c.cv + 0.5 * c.d_0 * c.u_0 * c.u_0;
+      if (B.f[F_Q0])  // q0(:, c) = q(c) at both time levels (:78-82)
+        for (int x = 0; x < 10; ++x) B.f[F_Q0][10 * n + x] = q.p[5 * n + x / 2];
       pri.p[7 * n + 0] = c.d_0;
       pri.p[7 * n + 1] = c.u_0 * std::cos(c.aoa);
       pri.p[7 * n + 2] = c.u_0 * std::sin(c.aoa);
@@ -661,6 +663,52 @@ static void block_update(Block& B, int m, double* dtmax, double* dtmin, double* 
 // main.f90:342-448 and the residual of :603, for nsteps iterations.  The
 // per-block phase runs one host thread per block (at most nthreads at a
 // time), as the reference runs one MPI rank per block group.
+// main.f90:450-573 (iflag_timeadvance = 2nd Crank-Nicolson) and the
+// residual of :603 for nsteps physical time steps: three dual-time
+// sub-iterations of [physical_bc, halo, averaging, then per block getpri,
+// inviscid, viscous, find_dt, crank2nd], then update_q0 and SA per block, and
+// the closing BCs, halo, averaging and primitives.
+void iterate_crank(int nsteps, double* resid_hist) {
+  const Consts& c = g_consts;
+  for (int step = 0; step < nsteps; ++step) {
+    for (int sub = 1; sub <= 3; ++sub) {
+      physical_bc();
+      updatebuffer();
+      average1();
+      average2();
+      for (auto& B : g_blk) {
+        if (!B.used) continue;
+        const Box &b = B.b, &b0 = B.b0, &b1 = B.b1;
+        get_primitivevariables(0, B.v(F_PRI), B.v(F_Q), c.gamma, c.cv, b);
+        inviscid_flux_1(B.v(F_RHSI), B.v(F_Q), B.v(F_DXIDX), B.v(F_INVJ), b, b0, b1, c.gamma);
+        if (g_flags.solver == IFLAG_NSSOLVER)
+          viscous_flux(B.v(F_RHSV), B.v(F_PRI), B.v(F_AMU), B.v(F_VOR), B.v(F_DUDX), B.v(F_TAO), B.v(F_DXIDX),
+                       B.v(F_INVJ), c.tinf, c.prl, c.prt, c.gamma, c.cv, c.re, b, b0, b1);
+        double cfl = c.cfl;
+        find_dt(B.v(F_DT), &g_last_dtmax, &g_last_dtmin, &g_last_cflmax, &g_last_cflmin, B.v(F_PRI),
+                B.v(F_AMU), B.v(F_DXIDX), c.re, &cfl, b, g_flags.time);
+        crank2nd(B.v(F_Q), B.v(F_Q0), B.v(F_DT), B.v(F_PRI), B.v(F_RHS), B.v(F_RHSI), B.v(F_RHSV),
+                 B.v(F_DXIDX), B.v(F_INVJ), b, b0, b1, c.gamma);
+      }
+    }
+    for (auto& B : g_blk)
+      if (B.used) update_q0(B.v(F_Q0), B.v(F_Q), B.b0);
+    if (g_flags.turbulence == IFLAG_SA && g_flags.solver == IFLAG_NSSOLVER)
+      for (auto& B : g_blk)
+        if (B.used)
+          sa_model(B.v(F_NUT), B.v(F_SARHS), B.v(F_DT), B.v(F_PRI), B.v(F_AMU), B.v(F_DUDX), B.v(F_VOR),
+                   B.v(F_DXIDX), B.v(F_INVJ), B.v(F_ALPHA), B.v(F_BETA), B.v(F_GAMMA), B.v(F_LENGTH),
+                   B.v(F_DIST), B.v(F_SPACING), c.re, c.cfl, B.b, B.b0, B.b1);
+    physical_bc();
+    updatebuffer();
+    average1();
+    average2();
+    for (auto& B : g_blk)
+      if (B.used) get_primitivevariables(0, B.v(F_PRI), B.v(F_Q), c.gamma, c.cv, B.b);
+    if (resid_hist) residual(resid_hist + 7 * step);
+  }
+}
+
 void iterate(int nsteps, int nthreads, double* resid_hist) {
   int nb = (int)g_blk.size();
   std::vector<double> dmx(nb), dmn(nb), cmx(nb), cmn(nb);
@@ -848,7 +896,25 @@ void oracle_init_flowfield(const double* ma, const double* aoa_deg, const double
   init_flowfield(*ma, *aoa_deg, *dt);
 }
 void oracle_init_walldist() { init_walldist(); }
-void oracle_iterate(int nsteps, int nthreads, double* resid_hist) { iterate(nsteps, nthreads, resid_hist); }
+void oracle_iterate(int nsteps, int nthreads, double* resid_hist) {
+  if (g_flags.timeadvance == IFLAG_2NDCRANK)
+    iterate_crank(nsteps, resid_hist);
+  else
+    iterate(nsteps, nthreads, resid_hist);
+}
+void oracle_crank2nd(double* q, double* q0, double* dt, double* pri_v, double* rhs, double* rhsi, double* rhsv,
+                     double* dxidx, double* inv_j, const int* box18, double gamma) {
+  Box b{box18[0], box18[1], box18[2], box18[3], box18[4], box18[5]};
+  Box b0{box18[6], box18[7], box18[8], box18[9], box18[10], box18[11]};
+  Box b1{box18[12], box18[13], box18[14], box18[15], box18[16], box18[17]};
+  crank2nd(V{q, 5, b}, V{q0, 10, b}, V{dt, 1, b}, V{pri_v, 7, b}, V{rhs, 5, b}, V{rhsi, 5, b}, V{rhsv, 5, b},
+           V{dxidx, 9, b}, V{inv_j, 1, b}, b, b0, b1, gamma);
+}
+void oracle_update_q0(double* q0, double* q, const int* box18) {
+  Box b{box18[0], box18[1], box18[2], box18[3], box18[4], box18[5]};
+  Box b0{box18[6], box18[7], box18[8], box18[9], box18[10], box18[11]};
+  update_q0(V{q0, 10, b}, V{q, 5, b}, b0);
+}
 void oracle_last_dt_minmax(double* out4) {
   out4[0] = g_last_dtmax; out4[1] = g_last_dtmin; out4[2] = g_last_cflmax; out4[3] = g_last_cflmin;
 }
