@@ -57,8 +57,9 @@ __device__ __forceinline__ void unit_normal(const BlockView& B, long n, int dir,
 // nodes and reads what an earlier one wrote, as in the serial reference).
 // The nodes of one subface are independent and spread over the grid's x.
 __global__ void k_physical_bc(const BlockView* __restrict__ blocks, const BcOp* __restrict__ ops,
-                              const int* __restrict__ op_start, int o, CaseConsts cc) {
+                              const int* __restrict__ op_start, int o, CaseConsts cc_launch) {
   const BlockView& B = blocks[blockIdx.y];
+  const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
   int idx = op_start[blockIdx.y] + o;
   if (idx >= op_start[blockIdx.y + 1]) return;
   const BcOp op = ops[idx];
@@ -269,6 +270,38 @@ __global__ void k_residual_final(const double* __restrict__ part, long npart, do
       if (!isfinite(out7[c])) bad = true;
     }
     out7[6] = 0.0;
+    if (bad && status) atomicOr(status, (unsigned)ST_NONFINITE_RESIDUAL);
+  }
+}
+
+// The norms of each block on its own (the residual a one-block case prints):
+// CTA m adds block m's partials in a fixed order and divides by that block's
+// physical node count.  out7 holds 7 values per block.
+__global__ void k_residual_final_blocks(const BlockView* __restrict__ blocks, const double* __restrict__ part,
+                                        int ctas, double* __restrict__ out7, unsigned* status) {
+  __shared__ double sm[6][256];
+  const int m = blockIdx.x;
+  double v[6] = {0, 0, 0, 0, 0, 0};
+  for (int p = threadIdx.x; p < ctas; p += blockDim.x)
+#pragma unroll
+    for (int c = 0; c < 6; ++c) v[c] += part[6 * ((long)m * ctas + p) + c];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) sm[c][threadIdx.x] = v[c];
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+#pragma unroll
+      for (int c = 0; c < 6; ++c) sm[c][threadIdx.x] += sm[c][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    double nodes = (double)blocks[m].b0.size();
+    bool bad = false;
+    for (int c = 0; c < 6; ++c) {
+      out7[7 * m + c] = sqrt(sm[c][0] / nodes);
+      if (!isfinite(out7[7 * m + c])) bad = true;
+    }
+    out7[7 * m + 6] = 0.0;
     if (bad && status) atomicOr(status, (unsigned)ST_NONFINITE_RESIDUAL);
   }
 }

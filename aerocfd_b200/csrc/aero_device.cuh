@@ -40,6 +40,13 @@ struct Box {
   }
 };
 
+// Per-case scalars (module ns_const / flag_var values the path reads).
+struct CaseConsts {
+  double gamma, cv, re, tinf, prl, prt, cfl;
+  double d_0, u_0, p_0, c_0, aoa, nutinf;
+  int dimension, solver, time, turbulence, des, bufferLength;
+};
+
 // Everything a kernel needs to address one block's fields.
 struct BlockView {
   Box b, b0, b1;
@@ -57,6 +64,9 @@ struct BlockView {
   long* nat;             // natural (box) index of the node
   double* dqs;           // 8 per node: dq* (forward result), padded to 64 bytes
   double* dq;            // 5 per node: dq (backward result)
+  // Case constants of this block when blocks of different cases share one
+  // launch (a batch); nullptr: the launch's constants apply.
+  const CaseConsts* ccb;
 
   __device__ __forceinline__ long at(int i, int j, int k) const {
     return (long)(i - b.is) + (long)nx * ((long)(j - b.js) + (long)ny * (long)(k - b.ks));
@@ -71,12 +81,6 @@ constexpr int kRec = 76;
 // LU-SGS per-node scalars: rhs(5), diag, inv_j, 1/diag, 1/inv_j, unused.
 constexpr int kSca = 10;
 
-// Per-case scalars (module ns_const / flag_var values the path reads).
-struct CaseConsts {
-  double gamma, cv, re, tinf, prl, prt, cfl;
-  double d_0, u_0, p_0, c_0, aoa, nutinf;
-  int dimension, solver, time, turbulence, des, bufferLength;
-};
 
 // ---------------------------------------------------------------- arithmetic
 // Integer powers follow gfortran's powi expansion; x**2 is x*x.

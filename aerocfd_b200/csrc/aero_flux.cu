@@ -11,8 +11,9 @@ namespace aero {
 
 // ----------------------------------------------------------------- primitives
 // sub_getpri_v.f90:19-62, over the full box of every block.
-__global__ void k_getpri(const BlockView* __restrict__ blocks, CaseConsts cc, unsigned* status) {
+__global__ void k_getpri(const BlockView* __restrict__ blocks, CaseConsts cc_launch, unsigned* status) {
   const BlockView& B = blocks[blockIdx.y];
+  const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
   long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
   long N = B.b.size();
   if (n >= N) return;
@@ -258,12 +259,12 @@ __device__ __forceinline__ void face_flux_mixed(const BlockView& B, int coord, l
   roe_face_mixed(B, coord, n, n + st, ulc, urc, gamma, flux);
 }
 
-template <bool MIXED>
+template <bool MIXED, int TILE>
 __device__ __forceinline__ void inviscid_body(const BlockView* __restrict__ blocks, CaseConsts cc) {
   const BlockView& B = blocks[blockIdx.y];
   const Box& b1 = B.b1;
-  __shared__ double dsm[3][5][kInvTile];
-  long t = (long)blockIdx.x * kInvTile + threadIdx.x;
+  __shared__ double dsm[3][5][TILE];
+  long t = (long)blockIdx.x * TILE + threadIdx.x;
   long N1 = b1.size();
   int d = threadIdx.y;
   int ndir = cc.dimension == IFLAG_3D ? 3 : 2;
@@ -303,17 +304,17 @@ __device__ __forceinline__ void inviscid_body(const BlockView* __restrict__ bloc
   }
 }
 
-// sub_inviscid1.f90:8-189: rhsi on the updated nodes.  A CTA covers kInvTile
-// nodes x 3 directions; thread (x, d) computes the flux difference of
-// direction d at its node (both faces), and the three differences are
-// combined in the reference's order: rhsi = -dF; rhsi -= dG; rhsi -= dH.
-__global__ void k_inviscid(const BlockView* __restrict__ blocks, CaseConsts cc) {
-  inviscid_body<false>(blocks, cc);
-}
-// The mixed-precision variant (face_flux_mixed).
-__global__ void k_inviscid_mixed(const BlockView* __restrict__ blocks, CaseConsts cc) {
-  inviscid_body<true>(blocks, cc);
-}
+// sub_inviscid1.f90:8-189: rhsi on the updated nodes.  A CTA covers TILE
+// nodes x 3 directions (TILE = 32, 64 or 128, picked by the autotuner); thread
+// (x, d) computes the flux difference of direction d at its node (both
+// faces), and the three differences are combined in the reference's order:
+// rhsi = -dF; rhsi -= dG; rhsi -= dH.  The _mixed kernels use face_flux_mixed.
+__global__ void k_inviscid_32(const BlockView* __restrict__ blocks, CaseConsts cc) { inviscid_body<false, 32>(blocks, cc); }
+__global__ void k_inviscid_64(const BlockView* __restrict__ blocks, CaseConsts cc) { inviscid_body<false, 64>(blocks, cc); }
+__global__ void k_inviscid_128(const BlockView* __restrict__ blocks, CaseConsts cc) { inviscid_body<false, 128>(blocks, cc); }
+__global__ void k_inviscid_mixed_32(const BlockView* __restrict__ blocks, CaseConsts cc) { inviscid_body<true, 32>(blocks, cc); }
+__global__ void k_inviscid_mixed_64(const BlockView* __restrict__ blocks, CaseConsts cc) { inviscid_body<true, 64>(blocks, cc); }
+__global__ void k_inviscid_mixed_128(const BlockView* __restrict__ blocks, CaseConsts cc) { inviscid_body<true, 128>(blocks, cc); }
 
 // Zero-fills one field over the full box of every block (the reference's
 // `rhsi = 0.d0`, sub_inviscid1.f90:40, and similar whole-array assignments).
@@ -337,8 +338,9 @@ __device__ __forceinline__ double cdiff(const double* f, long n, long st, int po
 // sub_viscous.f90:187-293: gradients, Sutherland viscosity, stresses, heat flux,
 // vorticity and the contravariant viscous fluxes on the physical nodes.  The
 // fluxes fv,gv,hv (components 2..5 each) go to the FVH scratch field.
-__global__ void k_viscous_a(const BlockView* __restrict__ blocks, CaseConsts cc, int store_dudx_tao) {
+__global__ void k_viscous_a(const BlockView* __restrict__ blocks, CaseConsts cc_launch, int store_dudx_tao) {
   const BlockView& B = blocks[blockIdx.y];
+  const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
   const Box& b0 = B.b0;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= b0.size()) return;
@@ -417,8 +419,9 @@ __global__ void k_viscous_a(const BlockView* __restrict__ blocks, CaseConsts cc,
 // differences, the viscosity (Sutherland) stays FP64 since the local time step
 // reads it; the velocity-gradient chain rule, stresses, heat flux, vorticity
 // and the contravariant fluxes are FP32.
-__global__ void k_viscous_a_mixed(const BlockView* __restrict__ blocks, CaseConsts cc, int store_dudx_tao) {
+__global__ void k_viscous_a_mixed(const BlockView* __restrict__ blocks, CaseConsts cc_launch, int store_dudx_tao) {
   const BlockView& B = blocks[blockIdx.y];
+  const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
   const Box& b0 = B.b0;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= b0.size()) return;
@@ -496,8 +499,9 @@ __global__ void k_viscous_a_mixed(const BlockView* __restrict__ blocks, CaseCons
 }
 
 // sub_viscous.f90:296-365: rhsv = (d fv/dxi + d gv/deta + d hv/dzeta)/re.
-__global__ void k_viscous_b(const BlockView* __restrict__ blocks, CaseConsts cc) {
+__global__ void k_viscous_b(const BlockView* __restrict__ blocks, CaseConsts cc_launch) {
   const BlockView& B = blocks[blockIdx.y];
+  const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
   const Box& b0 = B.b0;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= b0.size()) return;
@@ -527,8 +531,9 @@ __global__ void k_viscous_b(const BlockView* __restrict__ blocks, CaseConsts cc)
 // sub_timeadvancement_finddt.f90:52-88 (steady).  Besides dt, each CTA writes
 // the maximum of its dt values (NaN skipped) for the quirk-exact dtmax/dtmin
 // reduction in k_dt_minmax.
-__global__ void k_find_dt(const BlockView* __restrict__ blocks, CaseConsts cc, double* cta_max) {
+__global__ void k_find_dt(const BlockView* __restrict__ blocks, CaseConsts cc_launch, double* cta_max) {
   const BlockView& B = blocks[blockIdx.y];
+  const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
   long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
   long N = B.b.size();
   double dt = nan("");

@@ -17,8 +17,9 @@ namespace aero {
 
 // sub_timeadvancement_1stimplicit.f90:72-156: rhs on the updated nodes and the
 // spectral radii ra, rb, rc and the diagonal on the updated box grown by one.
-__global__ void k_lusgs_prep(const BlockView* __restrict__ blocks, CaseConsts cc) {
+__global__ void k_lusgs_prep(const BlockView* __restrict__ blocks, CaseConsts cc_launch) {
   const BlockView& B = blocks[blockIdx.y];
+  const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
   const Box& b1 = B.b1;
   Box e{b1.is - 1, b1.ie + 1, b1.js - 1, b1.je + 1, b1.ks - 1, b1.ke + 1};
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;

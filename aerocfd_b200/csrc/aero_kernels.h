@@ -44,6 +44,8 @@ struct WallFace {
 __global__ void k_getpri(const BlockView* __restrict__ blocks, CaseConsts cc, unsigned* status);
 __global__ void k_forces(const BlockView* __restrict__ blocks, const WallFace* __restrict__ walls, int nwall,
                          long nquad, CaseConsts cc, double* __restrict__ part);
+__global__ void k_residual_final_blocks(const BlockView* __restrict__ blocks, const double* __restrict__ part,
+                                        int ctas, double* __restrict__ out7, unsigned* status);
 __global__ void k_crank_rhs(const BlockView* __restrict__ blocks);
 __global__ void k_crank_sweep(const BlockView* __restrict__ blocks, int d, double gamma);
 __global__ void k_crank_update(const BlockView* __restrict__ blocks);
@@ -51,9 +53,13 @@ __global__ void k_update_q0(const BlockView* __restrict__ blocks);
 __global__ void k_forces_final(const double* __restrict__ part, int npart, CaseConsts cc, double sref,
                                double* __restrict__ out8);
 __global__ void k_fill(const BlockView* __restrict__ blocks, int fid, int nc, double val);
-constexpr int kInvTile = 64;  // nodes per CTA of k_inviscid (x 3 directions)
-__global__ void k_inviscid(const BlockView* __restrict__ blocks, CaseConsts cc);
-__global__ void k_inviscid_mixed(const BlockView* __restrict__ blocks, CaseConsts cc);
+// inviscid flux, FP64 and mixed, for CTA tiles of 32, 64 and 128 nodes (x 3 directions)
+__global__ void k_inviscid_32(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_inviscid_64(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_inviscid_128(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_inviscid_mixed_32(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_inviscid_mixed_64(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_inviscid_mixed_128(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_viscous_a(const BlockView* __restrict__ blocks, CaseConsts cc, int store_dudx_tao);
 __global__ void k_viscous_a_mixed(const BlockView* __restrict__ blocks, CaseConsts cc, int store_dudx_tao);
 __global__ void k_viscous_b(const BlockView* __restrict__ blocks, CaseConsts cc);

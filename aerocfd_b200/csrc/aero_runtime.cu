@@ -33,6 +33,9 @@ struct HostBlock {
   long plane = 0;
   size_t arena_off = 0;  // doubles
   void* ws = nullptr;    // LU-SGS workspace (one allocation)
+  bool own_params = false;  // aero_set_block_params: this block's case constants
+  double params[7] = {};
+  CaseConsts cc{};
 };
 
 // Hyperplane offsets of an nx1 x ny1 x nz1 updated box (planes h = a+b+c).
@@ -84,6 +87,8 @@ struct State {
   int nwall = 0;
   long nquad = 0;
   double* d_fpart = nullptr;
+  CaseConsts* d_ccb = nullptr;   // per-block case constants (batches)
+  double* d_resid_blocks = nullptr;  // 7 per block (aero_residual_blocks)
   double* d_out = nullptr;   // residual (7) + dt min/max (2)
   double* h_out = nullptr;   // pinned
   unsigned* d_status = nullptr;
@@ -104,9 +109,22 @@ struct State {
   int pmax_all = 0;
   int hmax_all = 0;
   bool mixed = false;  // aero_set_precision(1): FP32 increments in the flux kernels
+  // launch shapes (aero_autotune); none of them changes the arithmetic
+  struct Tune {
+    int inv_tile = 64;  // nodes per CTA of the inviscid flux
+    int ew = 256;       // threads per CTA of the element-wise kernels
+    int visc = 128;     // threads per CTA of k_viscous_a
+    int mats = 128;     // threads per CTA of k_lusgs_mats
+    int nst_max = 4;    // most shared-memory stages of the staged sweep
+  } tune;
+  // CUDA graph of one time step (aero_use_graphs)
+  bool graph_want = false;
+  cudaGraphExec_t graph_exec = nullptr;
+  unsigned long long graph_kernels = 0;
   double* d_tmax = nullptr;
   size_t t_tmax = 0;
   std::string err;
+  std::string tuning = "inviscid_tile=64 elementwise_threads=256 viscous_threads=128 mats_threads=128 sweep_stages<=4";
 };
 
 State g;
@@ -226,6 +244,7 @@ size_t view_doubles(long plane) {
 }
 void fill_view(BlockView& v, const Box& b, const Box& b0, const Box& b1, long plane, double* base) {
   v.b = b; v.b0 = b0; v.b1 = b1;
+  v.ccb = nullptr;
   v.nx = b.nx(); v.ny = b.ny();
   v.plane = plane;
   size_t off = 0;
@@ -399,33 +418,34 @@ CaseConsts consts_with(double gamma, double cv, double re) {
 
 // --------------------------------------------------------- launch helpers
 int launch_getpri(const BlockView* views, int nblk, long maxN, const CaseConsts& cc) {
-  dim3 grid(cdiv(maxN, 256), nblk);
-  PROF(P_GETPRI, (k_getpri<<<grid, 256, 0, g.stream>>>(views, cc, g.d_status)));
+  const int ew = g.tune.ew;
+  PROF(P_GETPRI, (k_getpri<<<dim3(cdiv(maxN, ew), nblk), ew, 0, g.stream>>>(views, cc, g.d_status)));
   CKL();
   return AERO_OK;
 }
 int launch_inviscid(const BlockView* views, int nblk, long maxN, long maxN1, const CaseConsts& cc) {
-  PROF(P_FILL, (k_fill<<<dim3(cdiv(maxN, 256), nblk), 256, 0, g.stream>>>(views, F_RHSI, 5, 0.0)));
+  PROF(P_FILL, (k_fill<<<dim3(cdiv(maxN, g.tune.ew), nblk), g.tune.ew, 0, g.stream>>>(views, F_RHSI, 5, 0.0)));
   CKL();
-  if (g.mixed)
-    PROF(P_INVISCID, (k_inviscid_mixed<<<dim3(cdiv(maxN1, kInvTile), nblk), dim3(kInvTile, 3), 0, g.stream>>>(views, cc)));
-  else
-    PROF(P_INVISCID, (k_inviscid<<<dim3(cdiv(maxN1, kInvTile), nblk), dim3(kInvTile, 3), 0, g.stream>>>(views, cc)));
+  const int tile = g.tune.inv_tile;
+  auto kern = g.mixed ? (tile == 32 ? k_inviscid_mixed_32 : tile == 128 ? k_inviscid_mixed_128 : k_inviscid_mixed_64)
+                      : (tile == 32 ? k_inviscid_32 : tile == 128 ? k_inviscid_128 : k_inviscid_64);
+  PROF(P_INVISCID, (kern<<<dim3(cdiv(maxN1, tile), nblk), dim3(tile, 3), 0, g.stream>>>(views, cc)));
   CKL();
   return AERO_OK;
 }
 int launch_viscous(const BlockView* views, int nblk, long maxN0, const CaseConsts& cc, int store) {
+  const int vt = g.tune.visc, ew = g.tune.ew;
   if (g.mixed)
-    PROF(P_VISC_A, (k_viscous_a_mixed<<<dim3(cdiv(maxN0, 128), nblk), 128, 0, g.stream>>>(views, cc, store)));
+    PROF(P_VISC_A, (k_viscous_a_mixed<<<dim3(cdiv(maxN0, vt), nblk), vt, 0, g.stream>>>(views, cc, store)));
   else
-    PROF(P_VISC_A, (k_viscous_a<<<dim3(cdiv(maxN0, 128), nblk), 128, 0, g.stream>>>(views, cc, store)));
+    PROF(P_VISC_A, (k_viscous_a<<<dim3(cdiv(maxN0, vt), nblk), vt, 0, g.stream>>>(views, cc, store)));
   CKL();
-  PROF(P_VISC_B, (k_viscous_b<<<dim3(cdiv(maxN0, 256), nblk), 256, 0, g.stream>>>(views, cc)));
+  PROF(P_VISC_B, (k_viscous_b<<<dim3(cdiv(maxN0, ew), nblk), ew, 0, g.stream>>>(views, cc)));
   CKL();
   return AERO_OK;
 }
 int launch_find_dt(const BlockView* views, int nblk, long maxN, const CaseConsts& cc) {
-  PROF(P_FIND_DT, (k_find_dt<<<dim3(cdiv(maxN, 256), nblk), 256, 0, g.stream>>>(views, cc, nullptr)));
+  PROF(P_FIND_DT, (k_find_dt<<<dim3(cdiv(maxN, g.tune.ew), nblk), g.tune.ew, 0, g.stream>>>(views, cc, nullptr)));
   CKL();
   return AERO_OK;
 }
@@ -436,9 +456,9 @@ int launch_dt_minmax(const BlockView* views, int m, double* d_out2) {
 }
 int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, int pmax, int hmax,
                     const CaseConsts& cc) {
-  PROF(P_LUSGS_PREP, (k_lusgs_prep<<<dim3(cdiv(maxExt, 256), nblk), 256, 0, g.stream>>>(views, cc)));
+  PROF(P_LUSGS_PREP, (k_lusgs_prep<<<dim3(cdiv(maxExt, g.tune.ew), nblk), g.tune.ew, 0, g.stream>>>(views, cc)));
   CKL();
-  PROF(P_LUSGS_MATS, (k_lusgs_mats<<<dim3(cdiv(3 * maxN1, 128), nblk), 128, 0, g.stream>>>(views, cc)));
+  PROF(P_LUSGS_MATS, (k_lusgs_mats<<<dim3(cdiv(3 * maxN1, g.tune.mats), nblk), g.tune.mats, 0, g.stream>>>(views, cc)));
   CKL();
   // Staged sweep: plane offsets + ring of two planes + nst staged planes
   // (records, scalars, dq*) + 2*nst+1 mbarriers, as many stages as fit
@@ -449,7 +469,7 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
   size_t offs = (size_t)((hmax + 2) & ~1) * sizeof(long);
   size_t ring = (size_t)2 * 5 * std::max(pmax, 1) * sizeof(double);
   size_t stage = (size_t)std::max(pmax, 1) * (kRec + kSca + 8) * sizeof(double);
-  int nst = 4;
+  int nst = g.tune.nst_max;
   while (nst >= 2 && offs + ring + nst * stage + (2 * nst + 1) * 8 > kSmemMax) --nst;
   static int staged_max_threads = 0;  // limited by the kernel's registers
   if (!staged_max_threads) {
@@ -474,7 +494,7 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
     PROF(P_LUSGS_SWEEP, (k_lusgs_sweep_global<<<nblk, threads, 0, g.stream>>>(views, 1, g.d_status)));
   }
   CKL();
-  PROF(P_LUSGS_UPDATE, (k_lusgs_update<<<dim3(cdiv(maxN1, 256), nblk), 256, 0, g.stream>>>(views)));
+  PROF(P_LUSGS_UPDATE, (k_lusgs_update<<<dim3(cdiv(maxN1, g.tune.ew), nblk), g.tune.ew, 0, g.stream>>>(views)));
   CKL();
   return AERO_OK;
 }
@@ -621,6 +641,70 @@ int do_iteration(bool want_dt_minmax) {
   return AERO_OK;
 }
 
+// Case constants from Control.in's flags and values; the nondimensional
+// freestream of sub_init_flowfield.f90:30-39.
+CaseConsts consts_from(const int* iflags, const double* params) {
+  CaseConsts c{};
+  const double pi = 3.1415926535897932;
+  c.gamma = 1.4; c.prl = 0.72; c.prt = 0.90;
+  double ma = params[0];
+  c.re = params[1]; c.tinf = params[2]; c.cfl = params[4]; c.nutinf = params[6];
+  c.d_0 = 1.0; c.u_0 = 1.0;
+  double t_0 = 1.0;
+  c.p_0 = c.d_0 * t_0 / c.gamma / ma / ma;
+  c.c_0 = std::sqrt(t_0) / ma;
+  c.cv = 1.0 / c.gamma / (c.gamma - 1.0) / ma / ma;
+  c.aoa = params[3] * pi / 180.0;
+  c.dimension = iflags[0]; c.solver = iflags[1]; c.time = iflags[2];
+  c.turbulence = iflags[4]; c.des = iflags[5]; c.bufferLength = iflags[6];
+  return c;
+}
+
+// One time step as aero_step runs it: the iteration, the closing primitives
+// and the residual norm (into g.d_out).
+int step_once() {
+  int rc;
+  if ((rc = do_iteration(false))) return rc;
+  if ((rc = do_getpri_all())) return rc;
+  return do_residual(g.d_out);
+}
+
+void graph_release() {
+  if (g.graph_exec) cudaGraphExecDestroy(g.graph_exec);
+  g.graph_exec = nullptr;
+  g.graph_kernels = 0;
+}
+
+// step_once, replayed from a CUDA graph captured on first use when graphs are
+// on (and profiling is off); the graph is captured again after any change of
+// precision mode or launch shapes.
+int run_step() {
+  if (!g.graph_want || gp.on) return step_once();
+  if (!g.graph_exec) {
+    unsigned long long before = gp.launches;
+    CK(cudaStreamBeginCapture(g.stream, cudaStreamCaptureModeRelaxed));
+    int rc = step_once();
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(g.stream, &graph);
+    if (rc) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    if (e != cudaSuccess) return fail(AERO_ERR_CUDA, "stream capture failed: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&g.graph_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      g.graph_exec = nullptr;
+      return fail(AERO_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
+    }
+    g.graph_kernels = gp.launches - before;
+    gp.launches = before;
+  }
+  CK(cudaGraphLaunch(g.graph_exec, g.stream));
+  gp.launches += g.graph_kernels;
+  return AERO_OK;
+}
+
 }  // namespace
 
 namespace aero {
@@ -666,6 +750,9 @@ static void release_case() {
   cudaFree(g.d_part); g.d_part = nullptr;
   cudaFree(g.d_walls); g.d_walls = nullptr;
   cudaFree(g.d_fpart); g.d_fpart = nullptr;
+  cudaFree(g.d_ccb); g.d_ccb = nullptr;
+  graph_release();
+  cudaFree(g.d_resid_blocks); g.d_resid_blocks = nullptr;
   g.nwall = 0;
   g.nquad = 0;
   g.views.clear();
@@ -689,8 +776,125 @@ int aero_finalize(void) {
   return AERO_OK;
 }
 
+int aero_set_block_params(int m, const double* params) {
+  int rc = need_init();
+  if (rc) return rc;
+  if (!g.configured) return fail(AERO_ERR_STATE, "aero_configure has not been called");
+  if (g.setup) return fail(AERO_ERR_STATE, "block parameters must be set before aero_finish_setup");
+  if (m < 1 || m > (int)g.blocks.size() || !g.blocks[m - 1].used)
+    return fail(AERO_ERR_ARG, "block %d is not registered", m);
+  if (!(params[0] > 0.0) || !(params[1] > 0.0) || !(params[4] > 0.0))
+    return fail(AERO_ERR_ARG, "block %d: ma, re and cfl must be positive", m);
+  HostBlock& H = g.blocks[m - 1];
+  std::memcpy(H.params, params, sizeof H.params);
+  H.cc = consts_from(g.iflags, params);
+  H.own_params = true;
+  return AERO_OK;
+}
+
+int aero_residual_blocks(double* out7) {
+  int rc = need_setup();
+  if (rc) return rc;
+  int nb = (int)g.blocks.size();
+  PROF(P_RESID_PART, (k_residual_partial<<<dim3(g.resid_ctas, nb), 256, 0, g.stream>>>(g.d_blocks, g.d_part, sa_on())));
+  CKL();
+  PROF(P_RESID_FINAL, (k_residual_final_blocks<<<nb, 256, 0, g.stream>>>(g.d_blocks, g.d_part, g.resid_ctas,
+                                                                         g.d_resid_blocks, g.d_status)));
+  CKL();
+  CK(cudaMemcpyAsync(out7, g.d_resid_blocks, (size_t)7 * nb * sizeof(double), cudaMemcpyDeviceToHost, g.stream));
+  CK(cudaStreamSynchronize(g.stream));
+  return AERO_OK;
+}
+
+int aero_use_graphs(int on) {
+  int rc = need_init();
+  if (rc) return rc;
+  g.graph_want = on != 0;
+  if (!g.graph_want) graph_release();
+  return AERO_OK;
+}
+
+int aero_autotune(int iters) {
+  int rc = need_setup();
+  if (rc) return rc;
+  if (iters < 1) return fail(AERO_ERR_ARG, "iters = %d", iters);
+  // the solution state that carries over between steps
+  const int kState[] = {F_Q, F_NUT, F_Q0, F_DT, F_AMU};
+  size_t per_block = 0;
+  for (int f : kState) per_block += (size_t)field_nc(f);
+  int nb = (int)g.blocks.size();
+  size_t total = 0;
+  for (int m = 0; m < nb; ++m) total += per_block * g.views[m].plane;
+  double* snap = nullptr;
+  CK(cudaMalloc(&snap, total * sizeof(double)));
+  auto copy_state = [&](bool save) -> int {
+    size_t off = 0;
+    for (int m = 0; m < nb; ++m)
+      for (int f : kState) {
+        size_t n = (size_t)field_nc(f) * g.views[m].plane;
+        double* dev = g.views[m].f[f];
+        CK(cudaMemcpyAsync(save ? snap + off : dev, save ? dev : snap + off, n * sizeof(double),
+                           cudaMemcpyDeviceToDevice, g.stream));
+        off += n;
+      }
+    return AERO_OK;
+  };
+  if ((rc = copy_state(true))) { cudaFree(snap); return rc; }
+  bool graphs = g.graph_want;
+  g.graph_want = false;
+  graph_release();
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  auto time_steps = [&](double& ms) -> int {
+    int r;
+    if ((r = step_once())) return r;  // warm
+    CK(cudaEventRecord(a, g.stream));
+    for (int x = 0; x < iters; ++x)
+      if ((r = step_once())) return r;
+    CK(cudaEventRecord(b, g.stream));
+    CK(cudaEventSynchronize(b));
+    float f = 0.f;
+    CK(cudaEventElapsedTime(&f, a, b));
+    ms = f;
+    return AERO_OK;
+  };
+  struct Knob { int* v; std::vector<int> cand; };
+  std::vector<Knob> knobs = {{&g.tune.inv_tile, {32, 64, 128}}, {&g.tune.ew, {128, 256, 512}},
+                             {&g.tune.visc, {64, 128, 256}}, {&g.tune.mats, {64, 128, 256}},
+                             {&g.tune.nst_max, {2, 3, 4}}};
+  for (Knob& k : knobs) {
+    int best = *k.v;
+    double best_ms = 1e300;
+    for (int c : k.cand) {
+      *k.v = c;
+      double ms = 0;
+      if ((rc = time_steps(ms))) break;
+      if (ms < best_ms) { best_ms = ms; best = c; }
+    }
+    *k.v = best;
+    if (rc) break;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  int rc2 = copy_state(false);
+  CK(cudaStreamSynchronize(g.stream));
+  cudaFree(snap);
+  g.graph_want = graphs;
+  if (rc) return rc;
+  if (rc2) return rc2;
+  char buf[160];
+  std::snprintf(buf, sizeof buf, "inviscid_tile=%d elementwise_threads=%d viscous_threads=%d mats_threads=%d sweep_stages<=%d",
+                g.tune.inv_tile, g.tune.ew, g.tune.visc, g.tune.mats, g.tune.nst_max);
+  g.tuning = buf;
+  return AERO_OK;
+}
+
+const char* aero_tuning(void) { return g.tuning.c_str(); }
+
 int aero_set_precision(int mode) {
   if (mode != 0 && mode != 1) return fail(AERO_ERR_ARG, "precision mode %d is not 0 (FP64) or 1 (mixed)", mode);
+  if (g.mixed != (mode == 1)) graph_release();
   g.mixed = mode == 1;
   return AERO_OK;
 }
@@ -725,20 +929,7 @@ int aero_configure(const int* iflags, const double* params) {
   if (iflags[5] != 0) return fail(AERO_ERR_ARG, "iflag_des=%d: DES97/DDES are not supported on the GPU", iflags[5]);
   std::memcpy(g.iflags, iflags, sizeof g.iflags);
   std::memcpy(g.params, params, sizeof g.params);
-  CaseConsts& c = g.cc;
-  const double pi = 3.1415926535897932;
-  c.gamma = 1.4; c.prl = 0.72; c.prt = 0.90;
-  double ma = params[0];
-  c.re = params[1]; c.tinf = params[2]; c.cfl = params[4]; c.nutinf = params[6];
-  // nondimensionalisation of sub_init_flowfield.f90:30-39
-  c.d_0 = 1.0; c.u_0 = 1.0;
-  double t_0 = 1.0;
-  c.p_0 = c.d_0 * t_0 / c.gamma / ma / ma;
-  c.c_0 = std::sqrt(t_0) / ma;
-  c.cv = 1.0 / c.gamma / (c.gamma - 1.0) / ma / ma;
-  c.aoa = params[3] * pi / 180.0;
-  c.dimension = iflags[0]; c.solver = iflags[1]; c.time = iflags[2];
-  c.turbulence = iflags[4]; c.des = iflags[5]; c.bufferLength = iflags[6];
+  g.cc = consts_from(iflags, params);
   g.configured = true;
   return AERO_OK;
 }
@@ -842,6 +1033,17 @@ int aero_finish_setup(void) {
     g.pmax_all = std::max(g.pmax_all, pmax);
     g.hmax_all = std::max(g.hmax_all, (int)poff.size() - 1);
   }
+  // per-block case constants of a batch (aero_set_block_params)
+  bool any_own = false;
+  for (auto& H : g.blocks) any_own = any_own || H.own_params;
+  if (any_own) {
+    std::vector<CaseConsts> ccs(nb);
+    for (int m = 0; m < nb; ++m) ccs[m] = g.blocks[m].own_params ? g.blocks[m].cc : g.cc;
+    CK(cudaMalloc(&g.d_ccb, nb * sizeof(CaseConsts)));
+    CK(cudaMemcpyAsync(g.d_ccb, ccs.data(), nb * sizeof(CaseConsts), cudaMemcpyHostToDevice, g.stream));
+    for (int m = 0; m < nb; ++m)
+      if (g.blocks[m].own_params) g.views[m].ccb = g.d_ccb + m;
+  }
   CK(cudaMalloc(&g.d_blocks, nb * sizeof(BlockView)));
   CK(cudaMemcpyAsync(g.d_blocks, g.views.data(), nb * sizeof(BlockView), cudaMemcpyHostToDevice, g.stream));
   // tables
@@ -872,6 +1074,7 @@ int aero_finish_setup(void) {
   if ((rc = launch_index(g.d_blocks, nb, g.max_b1))) return rc;
   g.resid_ctas = (int)cdiv(g.max_b1, 256);
   CK(cudaMalloc(&g.d_part, (size_t)g.resid_ctas * nb * 6 * sizeof(double)));
+  CK(cudaMalloc(&g.d_resid_blocks, (size_t)nb * 7 * sizeof(double)));
   // wall subfaces of clcd_output, in block and bcinfo order
   {
     std::vector<WallFace> walls;
@@ -1131,15 +1334,16 @@ int aero_init_flowfield(void) {
   // Fill on the host arrays' device copies: q, pri_v, dt, amu, nut, sa_rhs and
   // the zeroed work arrays (sub_init_flowfield.f90:55-111).
   int nb = (int)g.blocks.size();
-  const CaseConsts& c = g.cc;
   double t_0 = 1.0;
-  double qv[5] = {c.d_0, c.d_0 * c.u_0 * std::cos(c.aoa), c.d_0 * c.u_0 * std::sin(c.aoa), 0.0,
-                  c.d_0 * t_0 * c.cv + 0.5 * c.d_0 * c.u_0 * c.u_0};
-  double pv[7] = {c.d_0, c.u_0 * std::cos(c.aoa), c.u_0 * std::sin(c.aoa), 0.0, c.p_0, t_0, c.c_0};
-  bool sa = c.turbulence == IFLAG_SA;
+  bool sa = g.cc.turbulence == IFLAG_SA;
   double amu2 = sa ? 0.009 : 0.0;
   double av[3] = {1.0, amu2, 1.0 + amu2};
   for (int m = 0; m < nb; ++m) {
+    const CaseConsts& c = g.blocks[m].own_params ? g.blocks[m].cc : g.cc;
+    const double dt0 = g.blocks[m].own_params ? g.blocks[m].params[5] : g.params[5];
+    double qv[5] = {c.d_0, c.d_0 * c.u_0 * std::cos(c.aoa), c.d_0 * c.u_0 * std::sin(c.aoa), 0.0,
+                    c.d_0 * t_0 * c.cv + 0.5 * c.d_0 * c.u_0 * c.u_0};
+    double pv[7] = {c.d_0, c.u_0 * std::cos(c.aoa), c.u_0 * std::sin(c.aoa), 0.0, c.p_0, t_0, c.c_0};
     const BlockView& v = g.views[m];
     long N = g.blocks[m].b.size();
     auto put = [&](double* dst, double val) -> int {
@@ -1150,7 +1354,7 @@ int aero_init_flowfield(void) {
     for (int x = 0; x < 5; ++x) if ((rc = put(v.f[F_Q] + x * v.plane, qv[x]))) return rc;
     for (int x = 0; x < 7; ++x) if ((rc = put(v.f[F_PRI] + x * v.plane, pv[x]))) return rc;
     for (int x = 0; x < 3; ++x) if ((rc = put(v.f[F_AMU] + x * v.plane, av[x]))) return rc;
-    if ((rc = put(v.f[F_DT], g.params[5]))) return rc;
+    if ((rc = put(v.f[F_DT], dt0))) return rc;
     for (int x = 0; x < 10; ++x)  // q0(l, c) = q(c) at both time levels (sub_init_flowfield.f90:78-82)
       if ((rc = put(v.f[F_Q0] + x * v.plane, qv[x / 2]))) return rc;
     if (sa) {
@@ -1295,9 +1499,7 @@ int aero_step_timed(int nsteps, int flush_l2, double* device_ms) {
   for (int s = 0; s < nsteps; ++s) {
     if (flush_l2) CK(cudaMemsetAsync(flush, s & 0xff, fbytes, g.stream));
     CK(cudaEventRecord(a, g.stream));
-    if ((rc = do_iteration(false))) return rc;
-    if ((rc = do_getpri_all())) return rc;  // end of the time step (main.f90:434-447)
-    if ((rc = do_residual(g.d_out))) return rc;
+    if ((rc = run_step())) return rc;  // iteration, closing primitives, residual
     CK(cudaEventRecord(b, g.stream));
     CK(cudaEventSynchronize(b));
     float ms = 0.f;
@@ -1345,10 +1547,14 @@ int aero_step(int nsteps, double* resid_hist, double* dt_minmax) {
   if (rc) return rc;
   for (int s = 0; s < nsteps; ++s) {
     bool last = (s == nsteps - 1);
-    if ((rc = do_iteration(last && dt_minmax != nullptr))) return rc;
-    if ((rc = do_getpri_all())) return rc;  // end of the time step (main.f90:434-447)
-    if (resid_hist) {
+    if (last && dt_minmax != nullptr) {
+      if ((rc = do_iteration(true))) return rc;
+      if ((rc = do_getpri_all())) return rc;  // end of the time step (main.f90:434-447)
       if ((rc = do_residual(g.d_out))) return rc;
+    } else if ((rc = run_step())) {
+      return rc;
+    }
+    if (resid_hist) {
       CK(cudaMemcpyAsync(g.h_out, g.d_out, 7 * sizeof(double), cudaMemcpyDeviceToHost, g.stream));
       CK(cudaStreamSynchronize(g.stream));
       std::memcpy(resid_hist + 7 * s, g.h_out, 7 * sizeof(double));

@@ -34,8 +34,9 @@ __device__ __forceinline__ void node_of(const Box& bx, long t, int& i, int& j, i
 // Pass A over the updated box: dnut/dxi, dnut/deta, dnut/dzeta, the alpha/beta/
 // gamma contractions and nu + (1+cb2)*nut (sub_tur_sa.f90:294-413) into SA
 // scratch planes 0..6.
-__global__ void k_sa_a(const BlockView* __restrict__ blocks, CaseConsts cc) {
+__global__ void k_sa_a(const BlockView* __restrict__ blocks, CaseConsts cc_launch) {
   const BlockView& B = blocks[blockIdx.y];
+  const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
   const Box& b1 = B.b1;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= b1.size()) return;
@@ -64,8 +65,9 @@ __global__ void k_sa_a(const BlockView* __restrict__ blocks, CaseConsts cc) {
 // Pass B over the updated box: sa_rhs = advection (sa_rhs1) + diffusion
 // (sa_rhs2) + production/destruction (sa_rhs3), in that order, and the source
 // linearisation diasd (sub_tur_sa.f90:152-208, :359-512, :561-625).
-__global__ void k_sa_b(const BlockView* __restrict__ blocks, CaseConsts cc) {
+__global__ void k_sa_b(const BlockView* __restrict__ blocks, CaseConsts cc_launch) {
   const BlockView& B = blocks[blockIdx.y];
+  const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
   const Box& b1 = B.b1;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= b1.size()) return;
@@ -162,8 +164,9 @@ __global__ void k_sa_b(const BlockView* __restrict__ blocks, CaseConsts cc) {
 // the node's hyperplane-major record: rec_f[0..2] = 0.5*(U+|U|) per
 // direction, rec_f[3..5] = 0.5*(U-|U|), rec_f[6] = sa_rhs, rec_f[7] = diag
 // (sub_tur_sa.f90:676-750, :762-778).
-__global__ void k_sa_recs(const BlockView* __restrict__ blocks, CaseConsts cc) {
+__global__ void k_sa_recs(const BlockView* __restrict__ blocks, CaseConsts cc_launch) {
   const BlockView& B = blocks[blockIdx.y];
+  const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
   const Box& b1 = B.b1;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= b1.size()) return;

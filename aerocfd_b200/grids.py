@@ -191,6 +191,26 @@ def bump_batch(ncase: int = 64, seed: int = 0, nk: int = 5):
     return cases
 
 
+def batch_case(cases, name: str = "batch"):
+    """Independent single-block cases as the blocks of one registered set (a
+    batch): returns the Case (blocks renumbered 1..n, each keeping its own
+    arrays) and {m: Config} with every block's own Control.in values, for
+    GpuCase(..., block_params=...).  The flags (solver, time advance, ...) of
+    the first case apply to all."""
+    from .case import Block as _Block
+    blocks, params = [], {}
+    for m, c in enumerate(cases, start=1):
+        if len(c.blocks) != 1:
+            raise ValueError(f"case {c.name} has {len(c.blocks)} blocks; a batch takes single-block cases")
+        b = c.blocks[0]
+        nb = _Block(m, b.ni, b.nj, b.nk, b.subfaces, c.cfg.buffer_length, c.cfg.dimension)
+        for k, v in b.fields.items():
+            nb.fields[k][...] = v
+        blocks.append(nb)
+        params[m] = c.cfg
+    return Case(name, cases[0].cfg, blocks), params
+
+
 def geometric_nodes(n: int, first: float, length: float) -> np.ndarray:
     """n intervals from 0 to `length` growing geometrically from `first`."""
     if abs(first * n - length) < 1e-15 * length:

@@ -47,7 +47,9 @@ GAMMA, PRL, PRT = 1.4, 0.72, 0.90
 
 
 class GpuCase:
-    def __init__(self, case: Case, device: int = 0):
+    def __init__(self, case: Case, device: int = 0, block_params=None):
+        """block_params: optional {m: Config} giving blocks their own Control.in
+        values (a batch of independent cases, aero_set_block_params)."""
         self.case = case
         L = self.L = _lib.load()
         _lib.check(L.aero_init(ctypes.c_int(device)), "aero_init")
@@ -64,6 +66,10 @@ class GpuCase:
             for fid, (name, _) in enumerate(FIELDS):
                 _lib.check(L.aero_bind_field(ctypes.c_int(b.m), ctypes.c_int(fid),
                                              ctypes.c_void_p(b.ptr(name))), "aero_bind_field")
+        for m, cfg in (block_params or {}).items():
+            prm = cfg.params()
+            self._keep.append(prm)
+            _lib.check(L.aero_set_block_params(ctypes.c_int(m), _p(prm)), "aero_set_block_params")
         _lib.check(L.aero_finish_setup(), "aero_finish_setup")
         ma = case.cfg.ma
         self.cv = 1.0 / GAMMA / (GAMMA - 1.0) / ma / ma
@@ -109,6 +115,20 @@ class GpuCase:
         out = np.zeros(7)
         _lib.check(self.L.aero_residual(_p(out)), "aero_residual")
         return out
+
+    def residual_blocks(self) -> np.ndarray:
+        """Each block's own residual norms (nblocks x 7)."""
+        out = np.zeros((len(self.case.blocks), 7))
+        _lib.check(self.L.aero_residual_blocks(_p(out)), "aero_residual_blocks")
+        return out
+
+    def use_graphs(self, on: bool = True) -> None:
+        _lib.check(self.L.aero_use_graphs(ctypes.c_int(1 if on else 0)), "aero_use_graphs")
+
+    def autotune(self, iters: int = 3) -> str:
+        _lib.check(self.L.aero_autotune(ctypes.c_int(iters)), "aero_autotune")
+        self.L.aero_tuning.restype = ctypes.c_char_p
+        return self.L.aero_tuning().decode()
 
     def set_precision(self, mixed: bool) -> None:
         """aero_set_precision: 0 = FP64 reference arithmetic, 1 = mixed."""

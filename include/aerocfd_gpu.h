@@ -95,6 +95,15 @@ int aero_configure(const int* iflags, const double* params);
  * base states; metrics, Jacobians, the implicit diagonal and sweeps, the time
  * step, the viscosity and the residual stay FP64.  Applies to later calls. */
 int aero_set_precision(int mode);
+/* Batches (no counterpart in the reference, which runs one case per job):
+ * gives block m its own Control.in values (params[7] as aero_configure) so
+ * that independent cases, e.g. a Mach sweep, run together as the blocks of one
+ * registered set; the flags of aero_configure apply to all.  Call after
+ * aero_register_block(m) and before aero_finish_setup.  aero_residual_blocks
+ * then returns each block's own residual norms (7 per block, normalised by its
+ * own node count). */
+int aero_set_block_params(int m, const double* params);
+int aero_residual_blocks(double* out7_per_block);
 /* box18: is,ie,js,je,ks,ke, is0..ke0, is1..ke1 of block m (1-based)
  *        (sub_init_allocatememory.f90:73-144)
  * subfaces: num_subface rows of f_no,face,is,ie,js,je,ks,ke,blk_t,
@@ -221,6 +230,19 @@ int aero_step(int nsteps, double* resid_hist, double* dt_minmax);
  * flush_l2 != 0 the L2 cache is overwritten before every step, outside the
  * timed interval. */
 int aero_step_timed(int nsteps, int flush_l2, double* device_ms);
+
+/* ---- execution options (no counterpart in the reference) ---------------
+ * aero_use_graphs(1): aero_step and aero_step_timed replay each time step
+ * (iteration, closing primitives, residual) from a CUDA graph captured on its
+ * first use; results are those of the launches it replays.
+ * aero_autotune(iters): times iters steps for each candidate launch shape
+ * (inviscid-flux CTA tile, element-wise / viscous / block-record thread
+ * counts, sweep stages), keeps the fastest of each in turn, and restores the
+ * solution state (q, nut, q0, dt, amu) it started from; the arithmetic is the
+ * same for every shape.  aero_tuning() describes the shapes in use. */
+int aero_use_graphs(int on);
+int aero_autotune(int iters);
+const char* aero_tuning(void);
 
 /* ---- instrumentation ---------------------------------------------------
  * aero_profile(1) starts timing every kernel launch with CUDA events on the

@@ -1,0 +1,93 @@
+"""Batches of independent cases (aero_set_block_params): each block of the
+batch follows the oracle's run of its case alone (Mach number, size and bump
+height differ per case), step by step; CUDA-graph replay gives bit-identical
+results; aero_autotune restores the state it started from and changes no
+result."""
+import numpy as np
+import pytest
+
+from aerocfd_b200 import grids
+from conftest import relerr
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    from aerocfd_b200 import build, solver
+    build.build()
+    return solver
+
+
+def small_batch():
+    rng = np.random.default_rng(7)
+    cases = []
+    for c in range(5):
+        cfg = grids.Config(solver=grids.IFLAG_EULERSOLVER, ma=float(rng.uniform(0.3, 0.7)), re=1.0e6, cfl=5.0)
+        cases.append(grids.bump_channel(int(rng.integers(17, 40)), int(rng.integers(9, 20)), 5,
+                                        h=float(rng.uniform(0.05, 0.12)), cfg=cfg, name=f"b{c}"))
+    return cases
+
+
+def run_oracle(oracle_mod, case, nsteps):
+    oc = oracle_mod.OracleCase(case)
+    oc.geometry()
+    oc.init_flowfield()
+    oc.start()
+    return oc.iterate(nsteps)
+
+
+def started_batch(gpu, cases):
+    batch, params = grids.batch_case(cases)
+    gc = gpu.GpuCase(batch, block_params=params)
+    gc.compute_geometry()
+    gc.init_flowfield()
+    gc.start()
+    return batch, gc
+
+
+def test_batch_blocks_follow_their_own_cases(gpu, oracle_mod):
+    cases = small_batch()
+    nsteps = 4
+    hist = [run_oracle(oracle_mod, c, nsteps) for c in cases]
+    batch, gc = started_batch(gpu, small_batch())
+    try:
+        for s in range(nsteps):
+            gc.step(1, history=False)
+            r = gc.residual_blocks()
+            for m, h in enumerate(hist):
+                scale = np.maximum(np.abs(h[s, :5]), 1e-6 * np.abs(h[s, :5]).max())
+                assert np.max(np.abs(r[m, :5] - h[s, :5]) / scale) <= 1e-10, (s, m)
+        gc.sync_to_host(gpu.mask("q"))
+        for m, c in enumerate(cases):
+            assert relerr(batch.blocks[m].fields["q"], c.blocks[0].fields["q"]) <= TOL
+    finally:
+        gc.close()
+
+
+def test_graphs_and_autotune_change_no_result(gpu):
+    qs = []
+    for mode in ("plain", "graphs", "autotuned"):
+        batch, gc = started_batch(gpu, small_batch())
+        try:
+            if mode == "autotuned":
+                gc.sync_to_host(gpu.mask("q"))
+                q_before = [b.fields["q"].copy() for b in batch.blocks]
+                desc = gc.autotune(2)
+                assert "inviscid_tile=" in desc
+                gc.sync_to_host(gpu.mask("q"))
+                for b, q in zip(batch.blocks, q_before):
+                    assert np.array_equal(b.fields["q"], q)   # state restored
+            if mode != "plain":
+                gc.use_graphs(True)
+            h = gc.step(6)
+            gc.sync_to_host(gpu.mask("q"))
+            qs.append((h, [b.fields["q"].copy() for b in batch.blocks]))
+            assert gc.status() == 0
+        finally:
+            gc.close()
+    for h, q in qs[1:]:
+        assert np.array_equal(h, qs[0][0])
+        for a, b in zip(q, qs[0][1]):
+            assert np.array_equal(a, b)
