@@ -490,7 +490,13 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
     }
     PROF(P_LUSGS_SWEEP, (k_lusgs_sweep_staged<<<nblk, consumers + 32, smem, g.stream>>>(views, nst, g.d_status)));
   } else {
-    int threads = (int)std::min<long>(1024, std::max<long>(64, (2L * pmax + 31) / 32 * 32));
+    static int global_max_threads = 0;  // limited by the kernel's registers
+    if (!global_max_threads) {
+      cudaFuncAttributes fa;
+      CK(cudaFuncGetAttributes(&fa, k_lusgs_sweep_global));
+      global_max_threads = fa.maxThreadsPerBlock / 32 * 32;
+    }
+    int threads = (int)std::min<long>(global_max_threads, std::max<long>(64, (2L * pmax + 31) / 32 * 32));
     PROF(P_LUSGS_SWEEP, (k_lusgs_sweep_global<<<nblk, threads, 0, g.stream>>>(views, 1, g.d_status)));
   }
   CKL();

@@ -25,7 +25,10 @@ aero_set_precision(1), and the mixed solution's max / L2 error against FP64
 after 50 iterations from one state) and `convergence` (wall time to each drop
 milestone 1e-3 .. 1e-8 of the density residual on the 97x49x5 Euler bump
 channel, FP64 and mixed, with the CPU restatement's time estimated from its
-iteration rate; a milestone the scheme does not reach is null).
+iteration rate; a milestone the scheme does not reach is null) and `batched`
+(64 bump channels of uneven size in one batch, mixed precision, CUDA-graph
+replay, autotuned launch shapes, against the same 64 cases run one after
+another).
 """
 from __future__ import annotations
 
@@ -76,6 +79,7 @@ def parse():
     ap.add_argument("--cpu-sample-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-converge", action="store_true", help="skip the time-to-1e-8 runs")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 64-case batch")
     return ap.parse_args()
 
 
@@ -133,6 +137,58 @@ def converge_gpu(solver, mixed: bool, chunk: int = 500, its: int = 12000):
             "iterations_to": first,
             "wall_s_to": {k: (v * per_it if v else None) for k, v in first.items()},
             "device_status": status}
+
+
+BATCH_WORKLOAD = "bump_batch_64_uneven_euler_mixed"
+
+
+def batched_gpu(solver, steps: int, warmup: int):
+    """64 bump channels of uneven size (seed 0: ni ~ U{65..257}, nj ~ U{33..97},
+    nk = 5, h ~ U[0.05,0.12], M ~ U[0.3,0.7]), mixed precision, as one batch
+    with CUDA-graph replay and autotuned launch shapes, against the same cases
+    run one after another with the same settings.  Device time, L2 flushed
+    before every timed step."""
+    import torch
+    from aerocfd_b200 import _lib, grids
+    cases = grids.bump_batch(64, seed=0)
+    nodes = sum(c.nodes for c in cases)
+    batch, params = grids.batch_case(cases)
+    gc = solver.GpuCase(batch, block_params=params)
+    ms = ctypes.c_double(0.0)
+    try:
+        gc.compute_geometry()
+        gc.init_flowfield()
+        gc.start()
+        gc.set_precision(True)
+        tuning = gc.autotune(3)
+        gc.use_graphs(True)
+        gc.step(warmup, history=False)
+        torch.cuda.synchronize()
+        _lib.check(gc.L.aero_step_timed(ctypes.c_int(steps), ctypes.c_int(1), ctypes.byref(ms)), "batch timed")
+        batch_s = ms.value / 1e3
+        status = gc.status()
+    finally:
+        gc.close()
+    seq_s = 0.0
+    for c in grids.bump_batch(64, seed=0):
+        g1 = solver.GpuCase(c)
+        try:
+            g1.compute_geometry()
+            g1.init_flowfield()
+            g1.start()
+            g1.set_precision(True)
+            g1.use_graphs(True)
+            g1.step(warmup, history=False)
+            _lib.check(g1.L.aero_step_timed(ctypes.c_int(steps), ctypes.c_int(1), ctypes.byref(ms)), "case timed")
+            seq_s += ms.value / 1e3
+        finally:
+            g1.close()
+    return {"workload": BATCH_WORKLOAD, "cases": 64, "nodes": nodes, "steps": steps,
+            "value": nodes * steps / batch_s / 1e6, "unit": "Mcell-iter/s", "ms_per_step": 1e3 * batch_s / steps,
+            "sequential_value": nodes * steps / seq_s / 1e6, "sequential_ms_per_step": 1e3 * seq_s / steps,
+            "speedup_vs_sequential": seq_s / batch_s, "tuning": tuning, "device_status": status,
+            "note": "one launch per kernel for all 64 cases, each step replayed from a CUDA graph; "
+                    "sequential = the 64 cases one after another, same settings, device time summed"}
 
 
 def bump_cpu_rate(seconds: float = 4.0):
@@ -411,6 +467,8 @@ def main():
                                 "sample": f"{n} full iterations of the same workload, {el:.1f} s, "
                                           f"{thr} threads (one per block), C++ -O3 restatement"}
     gc.close()
+    if world == 1 and not args.no_batch:
+        line["batched"] = batched_gpu(solver, max(5, min(args.steps, 20)), args.warmup)
     if world == 1 and not args.no_converge:
         conv = {"workload": CONV_WORKLOAD, "target_drop": CONV_TARGET,
                 "fp64": converge_gpu(solver, False), "mixed": converge_gpu(solver, True)}
