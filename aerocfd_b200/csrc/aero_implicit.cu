@@ -258,6 +258,11 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
 }
+// Bulk prefetch of global memory into L2 (no completion to track); both the
+// address and the size are multiples of 16 bytes.
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
 // Barrier 1 over the first n threads (the consumer warps), returning the OR of
 // `pred` over them; orders memory like __syncthreads.
 __device__ __forceinline__ bool consumers_sync_or(bool pred, int n) {
@@ -509,17 +514,33 @@ __global__ void k_lusgs_sweep_staged(const BlockView* __restrict__ blocks, int n
 
 // The same sweeps with the records read from global memory, for blocks whose
 // planes do not fit the shared-memory stages; the previous plane's dq is read
-// back from dqs / dq (written before the last __syncthreads).
+// back from dqs / dq (written before the last __syncthreads).  Thread 0 keeps
+// the records of the next kAhead planes on their way into L2 with bulk
+// prefetches.
 __global__ void k_lusgs_sweep_global(const BlockView* __restrict__ blocks, int nst, unsigned* status) {
   const BlockView& B = blocks[blockIdx.x];
   const int H = B.nplanes;
   const long* poff = B.poff;
+  constexpr int kAhead = 3;  // planes prefetched into L2 ahead of the sweep
+  // records, scalars (and, backward, dq*) of step st of a pass into L2
+  auto prefetch = [&](bool fwd, int st) {
+    if (st >= H) return;
+    int h = fwd ? st : H - 1 - st;
+    long b = poff[h];
+    unsigned cnt = (unsigned)(poff[h + 1] - b);
+    bulk_prefetch_l2((fwd ? B.rec_f : B.rec_b) + kRec * b, cnt * kRec * 8u);
+    bulk_prefetch_l2(B.sca + kSca * b, cnt * kSca * 8u);
+    if (!fwd) bulk_prefetch_l2(B.dqs + 8 * b, cnt * 64u);
+  };
   for (int pass = 0; pass < 2; ++pass) {
     const bool fwd = pass == 0;
+    if (threadIdx.x == 0)
+      for (int x = 0; x < kAhead; ++x) prefetch(fwd, x);
     for (int st = 0; st < H; ++st) {
       int h = fwd ? st : H - 1 - st;
       long base = poff[h];
       int cnt = (int)(poff[h + 1] - base);
+      if (threadIdx.x == 0) prefetch(fwd, st + kAhead);
       const double* rec = (fwd ? B.rec_f : B.rec_b) + kRec * base;
       const double* sca = B.sca + kSca * base;
       const double* dsv = B.dqs + 8 * base;
