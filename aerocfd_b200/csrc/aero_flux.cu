@@ -316,6 +316,66 @@ __global__ void k_inviscid_mixed_32(const BlockView* __restrict__ blocks, CaseCo
 __global__ void k_inviscid_mixed_64(const BlockView* __restrict__ blocks, CaseConsts cc) { inviscid_body<true, 64>(blocks, cc); }
 __global__ void k_inviscid_mixed_128(const BlockView* __restrict__ blocks, CaseConsts cc) { inviscid_body<true, 128>(blocks, cc); }
 
+// Face-based variant of the same residual: every face flux once.
+// k_inviscid_faces: thread = one face along direction d = blockIdx.z, the face
+// between node n and its neighbour up in d, for every n of the updated box
+// grown by one node down in d; the flux goes to FVH plane 5*d + c (the viscous
+// scratch, free until viscous_flux).  k_inviscid_combine then forms
+// rhsi = -dF; rhsi -= dG; rhsi -= dH as the per-node kernels do.
+template <bool MIXED>
+__device__ __forceinline__ void faces_body(const BlockView* __restrict__ blocks, CaseConsts cc) {
+  const BlockView& B = blocks[blockIdx.y];
+  const int d = blockIdx.z;
+  if (d >= (cc.dimension == IFLAG_3D ? 3 : 2)) return;
+  const Box& b1 = B.b1;
+  Box e = b1;
+  if (d == 0) e.is -= 1; else if (d == 1) e.js -= 1; else e.ks -= 1;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= e.size()) return;
+  int i = e.is + (int)(t % e.nx());
+  long r = t / e.nx();
+  int j = e.js + (int)(r % e.ny());
+  int k = e.ks + (int)(r / e.ny());
+  long n = B.at(i, j, k);
+  const long st = d == 0 ? 1 : (d == 1 ? (long)B.nx : (long)B.nx * B.ny);
+  const int pos = d == 0 ? i : (d == 1 ? j : k);
+  const int lo = d == 0 ? B.b.is : (d == 1 ? B.b.js : B.b.ks);
+  const int hi = d == 0 ? B.b.ie : (d == 1 ? B.b.je : B.b.ke);
+  double f[5];
+  if (MIXED)
+    face_flux_mixed(B, d + 1, n, pos, lo, hi, st, cc.gamma, f);
+  else
+    face_flux(B, d + 1, n, pos, lo, hi, st, cc.gamma, f);
+  double* out = B.f[F_FVH] + (long)(5 * d) * B.plane + n;
+#pragma unroll
+  for (int c = 0; c < 5; ++c) out[(long)c * B.plane] = f[c];
+}
+__global__ void k_inviscid_faces(const BlockView* __restrict__ blocks, CaseConsts cc) { faces_body<false>(blocks, cc); }
+__global__ void k_inviscid_faces_mixed(const BlockView* __restrict__ blocks, CaseConsts cc) { faces_body<true>(blocks, cc); }
+
+__global__ void k_inviscid_combine(const BlockView* __restrict__ blocks, CaseConsts cc) {
+  const BlockView& B = blocks[blockIdx.y];
+  const Box& b1 = B.b1;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b1.size()) return;
+  int i = b1.is + (int)(t % b1.nx());
+  long r = t / b1.nx();
+  int j = b1.js + (int)(r % b1.ny());
+  int k = b1.ks + (int)(r / b1.ny());
+  long n = B.at(i, j, k);
+  const long st[3] = {1, (long)B.nx, (long)B.nx * B.ny};
+  const int ndir = cc.dimension == IFLAG_3D ? 3 : 2;
+  const double* F = B.f[F_FVH];
+  const long P = B.plane;
+#pragma unroll
+  for (int c = 0; c < 5; ++c) {
+    double acc = -(F[(long)c * P + n] - F[(long)c * P + n - st[0]]);
+    acc = acc - (F[(long)(5 + c) * P + n] - F[(long)(5 + c) * P + n - st[1]]);
+    if (ndir == 3) acc = acc - (F[(long)(10 + c) * P + n] - F[(long)(10 + c) * P + n - st[2]]);
+    B.v(F_RHSI, c + 1, n) = acc;
+  }
+}
+
 // Zero-fills one field over the full box of every block (the reference's
 // `rhsi = 0.d0`, sub_inviscid1.f90:40, and similar whole-array assignments).
 __global__ void k_fill(const BlockView* __restrict__ blocks, int fid, int nc, double val) {

@@ -60,6 +60,10 @@ __global__ void k_inviscid_128(const BlockView* __restrict__ blocks, CaseConsts 
 __global__ void k_inviscid_mixed_32(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_inviscid_mixed_64(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_inviscid_mixed_128(const BlockView* __restrict__ blocks, CaseConsts cc);
+// face-based variant: face fluxes into FVH planes, then the node combine
+__global__ void k_inviscid_faces(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_inviscid_faces_mixed(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_inviscid_combine(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_viscous_a(const BlockView* __restrict__ blocks, CaseConsts cc, int store_dudx_tao);
 __global__ void k_viscous_a_mixed(const BlockView* __restrict__ blocks, CaseConsts cc, int store_dudx_tao);
 __global__ void k_viscous_b(const BlockView* __restrict__ blocks, CaseConsts cc);

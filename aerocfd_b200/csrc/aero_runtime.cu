@@ -7,6 +7,7 @@
 // host arrays only on request.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -97,6 +98,7 @@ struct State {
   double totalnodes = 0;
   long max_box = 0, max_b0 = 0, max_b1 = 0, max_ext = 0;
   Box max_b1_box{1, 0, 1, 0, 1, 0};  // largest updated extent per direction over the blocks
+  long max_b1_face = 0;               // largest face of an updated box (nodes)
   int max_ops = 0;       // most physical-BC subfaces in one block
   long max_face = 0;     // most nodes in one physical-BC subface
   std::map<const double*, std::pair<int, int>> registry;  // host array -> (block, field)
@@ -111,7 +113,7 @@ struct State {
   bool mixed = false;  // aero_set_precision(1): FP32 increments in the flux kernels
   // launch shapes (aero_autotune); none of them changes the arithmetic
   struct Tune {
-    int inv_tile = 64;  // nodes per CTA of the inviscid flux
+    int inv_tile = 64;  // nodes per CTA of the inviscid flux; 0: face-based kernels
     int ew = 256;       // threads per CTA of the element-wise kernels
     int visc = 128;     // threads per CTA of k_viscous_a
     int mats = 128;     // threads per CTA of k_lusgs_mats
@@ -423,13 +425,22 @@ int launch_getpri(const BlockView* views, int nblk, long maxN, const CaseConsts&
   CKL();
   return AERO_OK;
 }
-int launch_inviscid(const BlockView* views, int nblk, long maxN, long maxN1, const CaseConsts& cc) {
+int launch_inviscid(const BlockView* views, int nblk, long maxN, long maxN1, long maxFace, const CaseConsts& cc) {
   PROF(P_FILL, (k_fill<<<dim3(cdiv(maxN, g.tune.ew), nblk), g.tune.ew, 0, g.stream>>>(views, F_RHSI, 5, 0.0)));
   CKL();
   const int tile = g.tune.inv_tile;
-  auto kern = g.mixed ? (tile == 32 ? k_inviscid_mixed_32 : tile == 128 ? k_inviscid_mixed_128 : k_inviscid_mixed_64)
-                      : (tile == 32 ? k_inviscid_32 : tile == 128 ? k_inviscid_128 : k_inviscid_64);
-  PROF(P_INVISCID, (kern<<<dim3(cdiv(maxN1, tile), nblk), dim3(tile, 3), 0, g.stream>>>(views, cc)));
+  if (tile == 0) {  // face-based: each face once, then the combine
+    // faces per direction <= updated box grown by one node in that direction
+    long maxF = maxN1 + maxFace;
+    PROF(P_INVISCID, ((g.mixed ? k_inviscid_faces_mixed : k_inviscid_faces)<<<dim3(cdiv(maxF, 128), nblk, 3), 128, 0,
+                                                                             g.stream>>>(views, cc)));
+    CKL();
+    PROF(P_INVISCID, (k_inviscid_combine<<<dim3(cdiv(maxN1, g.tune.ew), nblk), g.tune.ew, 0, g.stream>>>(views, cc)));
+  } else {
+    auto kern = g.mixed ? (tile == 32 ? k_inviscid_mixed_32 : tile == 128 ? k_inviscid_mixed_128 : k_inviscid_mixed_64)
+                        : (tile == 32 ? k_inviscid_32 : tile == 128 ? k_inviscid_128 : k_inviscid_64);
+    PROF(P_INVISCID, (kern<<<dim3(cdiv(maxN1, tile), nblk), dim3(tile, 3), 0, g.stream>>>(views, cc)));
+  }
   CKL();
   return AERO_OK;
 }
@@ -615,7 +626,7 @@ int do_iteration_crank() {
     if ((rc = do_average1())) return rc;
     if ((rc = do_average2())) return rc;
     if ((rc = do_getpri_all())) return rc;
-    if ((rc = launch_inviscid(g.d_blocks, nb, g.max_box, g.max_b1, g.cc))) return rc;
+    if ((rc = launch_inviscid(g.d_blocks, nb, g.max_box, g.max_b1, g.max_b1_face, g.cc))) return rc;
     if (viscous_on() && (rc = launch_viscous(g.d_blocks, nb, g.max_b0, g.cc, 0))) return rc;
     if ((rc = launch_crank(g.d_blocks, nb, g.max_box, g.max_b1, &g.max_b1_box, g.cc))) return rc;
   }
@@ -634,7 +645,7 @@ int do_iteration(bool want_dt_minmax) {
   int nb = (int)g.blocks.size();
   int rc;
   if ((rc = do_getpri_all())) return rc;
-  if ((rc = launch_inviscid(g.d_blocks, nb, g.max_box, g.max_b1, g.cc))) return rc;
+  if ((rc = launch_inviscid(g.d_blocks, nb, g.max_box, g.max_b1, g.max_b1_face, g.cc))) return rc;
   if (viscous_on() && (rc = launch_viscous(g.d_blocks, nb, g.max_b0, g.cc, 0))) return rc;
   if ((rc = launch_find_dt(g.d_blocks, nb, g.max_box, g.cc))) return rc;
   if (want_dt_minmax && (rc = launch_dt_minmax(g.d_blocks, nb - 1, g.d_out + 7))) return rc;
@@ -779,6 +790,11 @@ int aero_finalize(void) {
   cudaStreamDestroy(g.stream); g.stream = nullptr;
   g.inited = false;
   g.configured = false;
+  // execution options of the finished run
+  g.mixed = false;
+  g.tune = State::Tune{};
+  g.graph_want = false;
+  g.tuning = State{}.tuning;
   return AERO_OK;
 }
 
@@ -866,7 +882,7 @@ int aero_autotune(int iters) {
     return AERO_OK;
   };
   struct Knob { int* v; std::vector<int> cand; };
-  std::vector<Knob> knobs = {{&g.tune.inv_tile, {32, 64, 128}}, {&g.tune.ew, {128, 256, 512}},
+  std::vector<Knob> knobs = {{&g.tune.inv_tile, {0, 32, 64, 128}}, {&g.tune.ew, {128, 256, 512}},
                              {&g.tune.visc, {64, 128, 256}}, {&g.tune.mats, {64, 128, 256}},
                              {&g.tune.nst_max, {2, 3, 4}}};
   for (Knob& k : knobs) {
@@ -897,6 +913,27 @@ int aero_autotune(int iters) {
 }
 
 const char* aero_tuning(void) { return g.tuning.c_str(); }
+
+int aero_set_tuning(int inv_tile, int ew, int visc, int mats, int nst_max) {
+  int rc = need_init();
+  if (rc) return rc;
+  auto in = [](int v, std::initializer_list<int> ok) { return std::find(ok.begin(), ok.end(), v) != ok.end(); };
+  if (!in(inv_tile, {0, 32, 64, 128}) || !in(ew, {128, 256, 512}) || !in(visc, {64, 128, 256}) ||
+      !in(mats, {64, 128, 256}) || !in(nst_max, {2, 3, 4}))
+    return fail(AERO_ERR_ARG, "launch shape %d/%d/%d/%d/%d is not one the autotuner offers", inv_tile, ew, visc, mats,
+                nst_max);
+  g.tune.inv_tile = inv_tile;
+  g.tune.ew = ew;
+  g.tune.visc = visc;
+  g.tune.mats = mats;
+  g.tune.nst_max = nst_max;
+  graph_release();
+  char buf[160];
+  std::snprintf(buf, sizeof buf, "inviscid_tile=%d elementwise_threads=%d viscous_threads=%d mats_threads=%d sweep_stages<=%d",
+                inv_tile, ew, visc, mats, nst_max);
+  g.tuning = buf;
+  return AERO_OK;
+}
 
 int aero_set_precision(int mode) {
   if (mode != 0 && mode != 1) return fail(AERO_ERR_ARG, "precision mode %d is not 0 (FP64) or 1 (mixed)", mode);
@@ -1006,6 +1043,7 @@ int aero_finish_setup(void) {
   size_t total = 0;
   g.max_box = g.max_b0 = g.max_b1 = g.max_ext = 0;
   g.max_b1_box = Box{1, 0, 1, 0, 1, 0};
+  g.max_b1_face = 0;
   g.totalnodes = 0;
   long max_b1 = 0;
   for (auto& H : g.blocks) {
@@ -1018,6 +1056,8 @@ int aero_finish_setup(void) {
     Box e{H.b1.is - 1, H.b1.ie + 1, H.b1.js - 1, H.b1.je + 1, H.b1.ks - 1, H.b1.ke + 1};
     g.max_ext = std::max(g.max_ext, e.size());
     g.totalnodes += (double)H.b0.size();
+    g.max_b1_face = std::max({g.max_b1_face, (long)H.b1.ny() * H.b1.nz(), (long)H.b1.nx() * H.b1.nz(),
+                              (long)H.b1.nx() * H.b1.ny()});
     g.max_b1_box.ie = std::max(g.max_b1_box.ie, H.b1.nx());
     g.max_b1_box.je = std::max(g.max_b1_box.je, H.b1.ny());
     g.max_b1_box.ke = std::max(g.max_b1_box.ke, H.b1.nz());
@@ -1158,7 +1198,8 @@ int aero_inviscid_flux_1(double* rhsi, const double* q, const double* dxidx, con
   BlockTarget t;
   if ((rc = resolve(b, b0, b1, args, t))) return rc;
   CaseConsts cc = consts_with(*gamma, g.cc.cv, g.cc.re);
-  if ((rc = launch_inviscid(t.d_view, 1, b.size(), b1.size(), cc))) return rc;
+  long maxFace = std::max({(long)b1.ny() * b1.nz(), (long)b1.nx() * b1.nz(), (long)b1.nx() * b1.ny()});
+  if ((rc = launch_inviscid(t.d_view, 1, b.size(), b1.size(), maxFace, cc))) return rc;
   return finish(t, args);
 }
 

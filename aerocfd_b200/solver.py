@@ -130,6 +130,10 @@ class GpuCase:
         self.L.aero_tuning.restype = ctypes.c_char_p
         return self.L.aero_tuning().decode()
 
+    def set_tuning(self, inv_tile: int = 64, ew: int = 256, visc: int = 128, mats: int = 128, nst_max: int = 4) -> None:
+        _lib.check(self.L.aero_set_tuning(ctypes.c_int(inv_tile), ctypes.c_int(ew), ctypes.c_int(visc),
+                                          ctypes.c_int(mats), ctypes.c_int(nst_max)), "aero_set_tuning")
+
     def set_precision(self, mixed: bool) -> None:
         """aero_set_precision: 0 = FP64 reference arithmetic, 1 = mixed."""
         _lib.check(self.L.aero_set_precision(ctypes.c_int(1 if mixed else 0)), "aero_set_precision")

@@ -75,6 +75,8 @@ enum {
 
 /* ---- runtime ----------------------------------------------------------- */
 int aero_init(int device);
+/* Releases everything; the execution options (aero_set_precision,
+ * aero_use_graphs, launch shapes) return to their defaults. */
 int aero_finalize(void);
 /* Text of the last error (valid until the next call). */
 const char* aero_last_error(void);
@@ -243,6 +245,10 @@ int aero_step_timed(int nsteps, int flush_l2, double* device_ms);
 int aero_use_graphs(int on);
 int aero_autotune(int iters);
 const char* aero_tuning(void);
+/* Sets the launch shapes directly (e.g. to apply a saved tuning): inviscid
+ * tile 0 (face-based kernels), 32, 64 or 128; element-wise threads 128, 256,
+ * 512; viscous and block-record threads 64, 128, 256; sweep stages 2..4. */
+int aero_set_tuning(int inv_tile, int ew, int visc, int mats, int nst_max);
 
 /* ---- instrumentation ---------------------------------------------------
  * aero_profile(1) starts timing every kernel launch with CUDA events on the
