@@ -250,6 +250,13 @@ const char* aero_tuning(void);
  * 512; viscous and block-record threads 64, 128, 256; sweep stages 2..4. */
 int aero_set_tuning(int inv_tile, int ew, int visc, int mats, int nst_max);
 
+/* ---- warm-start network (no counterpart in the reference) --------------
+ * aero_mlp_gemm: c[M x N] = a[M x K] * b[N x K]^T on the tcgen05 tensor cores,
+ * a and b BF16 bit patterns (row-major), c FP32, host arrays; M and N
+ * multiples of 128, K a multiple of 64; splits > 1 splits K over CTAs and
+ * adds the partial tiles in a fixed order. */
+int aero_mlp_gemm(const unsigned short* a, const unsigned short* b, float* c, int M, int N, int K, int splits);
+
 /* ---- instrumentation ---------------------------------------------------
  * aero_profile(1) starts timing every kernel launch with CUDA events on the
  * library's stream (and zeroes the totals); aero_profile(0) stops.
