@@ -256,6 +256,24 @@ int aero_set_tuning(int inv_tile, int ew, int visc, int mats, int nst_max);
  * multiples of 128, K a multiple of 64; splits > 1 splits K over CTAs and
  * adds the partial tiles in a fixed order. */
 int aero_mlp_gemm(const unsigned short* a, const unsigned short* b, float* c, int M, int N, int K, int splits);
+/* The network: n_in inputs (<= 128), depth hidden SiLU layers of `width`
+ * (a multiple of 128), n_out outputs (<= 128); BF16 weights and activations,
+ * FP32 accumulation, FP32 master weights trained with Adam on the mean
+ * squared error over mini-batches of `batch` rows (a multiple of 512).
+ * Parameters are laid out layer by layer as W [nout x nin] (row-major, with
+ * the padded sizes 128 for the input and output layers) then b [nout].
+ * x, t, y are host arrays, row-major (n x n_in, n x n_out). */
+int aero_mlp_create(int n_in, int n_out, int width, int depth, int batch, unsigned long long seed);
+int aero_mlp_destroy(void);
+int aero_mlp_param_count(long long* count);
+int aero_mlp_get_params(float* out);
+/* loss and gradients of one batch (n <= batch rows), parameters unchanged */
+int aero_mlp_gradients(const float* x, const float* t, int n, float* loss, float* grad);
+/* steps Adam steps on shuffled mini-batches; loss_hist (may be NULL) gets the
+ * batch loss of every step */
+int aero_mlp_train(const float* x, const float* t, long long n, int steps, float lr, unsigned long long seed,
+                   float* loss_hist);
+int aero_mlp_predict(const float* x, long long n, float* y);
 
 /* ---- instrumentation ---------------------------------------------------
  * aero_profile(1) starts timing every kernel launch with CUDA events on the
