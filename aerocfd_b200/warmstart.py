@@ -1,0 +1,186 @@
+"""Learned warm start for families of cases (no counterpart in the reference).
+
+A small MLP (aero_mlp_*: BF16 weights, FP32 accumulation, tcgen05 GEMMs) is
+trained on converged fields the solver generates for seeded members of a case
+family, and predicts the primitive variables of a new member from its
+parameters and node coordinates; the solver then starts from that field instead
+of the freestream.  The freestream start stays the fallback and the judge of
+the result: a warm-started run is iterated to the same residual level as the
+cold one and their wall forces are compared.
+
+The family here is the bump channel (a fixed grid of ni x nj x nk, bump height
+h ~ U[0.05, 0.12], Mach ~ U[0.3, 0.7]) with farfield (Riemann-invariant)
+boundaries on the inflow, outflow and top faces: its steady state is unique
+and the scheme converges to machine zero from any start, which the warm start
+is judged against.  (With the fixed inflow and extrapolated outflow of the
+reference's own channel set-up the converged pressure level depends on the
+start, so no start can be judged by its converged forces.)  Node inputs are
+(x, y, wall distance, h, M), outputs the freestream-normalised perturbations of
+(rho, u, v, p).
+"""
+from __future__ import annotations
+
+import ctypes
+import time
+from typing import Dict, List, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib, grids
+from .case import BC_FARFIELD, Case, Config, IFLAG_EULERSOLVER
+
+GAMMA = 1.4
+
+
+def family(n: int, seed: int, ni: int = 97, nj: int = 49, nk: int = 5) -> List[Tuple[Case, float, float]]:
+    """n bump channels with seeded (h, M): (case, h, M)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for c in range(n):
+        h = float(rng.uniform(0.05, 0.12))
+        ma = float(rng.uniform(0.3, 0.7))
+        cfg = Config(solver=IFLAG_EULERSOLVER, ma=ma, re=1.0e6, cfl=5.0)
+        case = grids.bump_channel(ni, nj, nk, h=h, cfg=cfg, name=f"bump_h{h:.3f}_m{ma:.3f}")
+        for sf in case.blocks[0].subfaces:
+            if sf.face in (1, 2, 4):
+                sf.blk_t = BC_FARFIELD
+        out.append((case, h, ma))
+    return out
+
+
+def features(case: Case, h: float, ma: float) -> np.ndarray:
+    """Per physical node of the first k-plane: x/3, y, y - y_wall(x), h/0.12,
+    (M - 0.5)/0.2 (float32, nj*ni rows, i fastest)."""
+    b = case.blocks[0]
+    s = b.sl(b.box0)
+    x = b.fields["x"][s][0]
+    y = b.fields["y"][s][0]
+    dist = y - y[0:1, :]
+    nj, ni = x.shape
+    f = np.stack([x / 3.0, y, dist, np.full_like(x, h / 0.12), np.full_like(x, (ma - 0.5) / 0.2)], -1)
+    return f.reshape(nj * ni, 5).astype(np.float32)
+
+
+def targets(case: Case) -> np.ndarray:
+    """(rho - 1, u - 1, v, p/p0 - 1) on the first k-plane of the physical
+    nodes (the freestream is rho = u = 1, v = 0, p = p0 = 1/(gamma M^2))."""
+    b = case.blocks[0]
+    s = b.sl(b.box0)
+    pri = b.fields["pri_v"][s][0]
+    p0 = 1.0 / GAMMA / case.cfg.ma ** 2
+    t = np.stack([pri[..., 0] - 1.0, pri[..., 1] - 1.0, pri[..., 2], pri[..., 4] / p0 - 1.0], -1)
+    return t.reshape(-1, 4).astype(np.float32)
+
+
+def set_state(case: Case, pred: np.ndarray) -> None:
+    """Conservative variables of every node of the case from predicted
+    perturbations on the first k-plane (copied along k; ghost nodes take the
+    nearest physical node's value before the start-up BCs overwrite them)."""
+    b = case.blocks[0]
+    ma = case.cfg.ma
+    p0 = 1.0 / GAMMA / ma ** 2
+    nk, nj, ni = b.nk, b.nj, b.ni
+    pr = pred.reshape(nj, ni, 4).astype(np.float64)
+    rho = 1.0 + pr[..., 0]
+    u = 1.0 + pr[..., 1]
+    v = pr[..., 2]
+    p = p0 * (1.0 + pr[..., 3])
+    q = np.stack([rho, rho * u, rho * v, np.zeros_like(rho), p / (GAMMA - 1.0) + 0.5 * rho * (u * u + v * v)], -1)
+    full = b.fields["q"]
+    is_, ie, js, je, ks, ke = b.box
+    ii = np.clip(np.arange(is_, ie + 1), 1, ni) - 1
+    jj = np.clip(np.arange(js, je + 1), 1, nj) - 1
+    full[...] = q[jj][:, ii][None, :, :, :]
+
+
+class Network:
+    """aero_mlp_* through the C-ABI."""
+
+    def __init__(self, n_in=5, n_out=4, width=256, depth=8, batch=8192, seed=1):
+        self.L = _lib.load()
+        _lib.check(self.L.aero_mlp_create(n_in, n_out, width, depth, batch, ctypes.c_ulonglong(seed)), "aero_mlp_create")
+        self.shape = (n_in, n_out, width, depth, batch)
+
+    def train(self, x: np.ndarray, t: np.ndarray, steps: int, lr: float = 1e-3, seed: int = 2) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        hist = np.zeros(steps, dtype=np.float32)
+        p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        _lib.check(self.L.aero_mlp_train(p(x), p(t), ctypes.c_longlong(len(x)), steps, ctypes.c_float(lr),
+                                         ctypes.c_ulonglong(seed), p(hist)), "aero_mlp_train")
+        return hist
+
+    def predict(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.zeros((len(x), self.shape[1]), dtype=np.float32)
+        p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        _lib.check(self.L.aero_mlp_predict(p(x), ctypes.c_longlong(len(x)), p(y)), "aero_mlp_predict")
+        return y
+
+    def close(self) -> None:
+        self.L.aero_mlp_destroy()
+
+
+def run_batch(solver, members: Sequence[Tuple[Case, float, float]], iters: int, chunk: int = 50,
+              warm: Dict[int, np.ndarray] = None, mixed: bool = False):
+    """Runs the members as one batch for `iters` iterations; warm maps member
+    index -> predicted field (else a freestream start).  Returns the per-member
+    density residual after iteration 1 and after every further chunk (row r is
+    iteration 1 + r*chunk), the wall time and the batch case (host arrays
+    synchronised)."""
+    cases = [m[0] for m in members]
+    batch, params = grids.batch_case(cases)
+    gc = solver.GpuCase(batch, block_params=params)
+    try:
+        gc.compute_geometry()
+        gc.init_flowfield()
+        if warm:
+            gc.sync_to_host(solver.ALL)
+            for i, pred in warm.items():
+                set_state(Case("member", cases[i].cfg, [batch.blocks[i]]), pred)
+            gc.sync_to_device(solver.mask("q"))
+        gc.start()
+        gc.set_precision(mixed)
+        gc.use_graphs(True)
+        t0 = time.perf_counter()
+        gc.step(1, history=False)
+        res = [gc.residual_blocks()[:, 0]]  # iteration 1
+        for _ in range(iters // chunk):
+            gc.step(chunk, history=False)
+            res.append(gc.residual_blocks()[:, 0])
+        wall = time.perf_counter() - t0
+        gc.sync_to_host(solver.ALL)
+        return np.array(res), wall, batch
+    finally:
+        gc.close()
+
+
+def member(batch: Case, i: int, cfg: Config) -> Case:
+    """Block i of a batch as a stand-alone single-block case (arrays copied)."""
+    from .case import Block
+    b = batch.blocks[i]
+    nb = Block(1, b.ni, b.nj, b.nk, b.subfaces, cfg.buffer_length, cfg.dimension)
+    for k, v in b.fields.items():
+        nb.fields[k][...] = v
+    return Case(f"member{i}", cfg, [nb])
+
+
+def first_below(hist: np.ndarray, level: np.ndarray, chunk: int) -> np.ndarray:
+    """Iteration (chunk resolution) at which each member's residual first falls
+    below its level (rows as run_batch returns them); -1 if never."""
+    out = np.full(hist.shape[1], -1)
+    for m in range(hist.shape[1]):
+        hit = np.nonzero(hist[:, m] <= level[m])[0]
+        if len(hit):
+            out[m] = 1 + hit[0] * chunk
+    return out
+
+
+def wall_force(solver, case: Case) -> np.ndarray:
+    """Pressure + viscous force on the walls (clcd_output) of a solved case."""
+    gc = solver.GpuCase(case)
+    try:
+        gc.sync_to_device(solver.ALL)
+        return gc.clcd_output(1.0)
+    finally:
+        gc.close()
