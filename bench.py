@@ -28,7 +28,9 @@ channel, FP64 and mixed, with the CPU restatement's time estimated from its
 iteration rate; a milestone the scheme does not reach is null) and `batched`
 (64 bump channels of uneven size in one batch, mixed precision, CUDA-graph
 replay, autotuned launch shapes, against the same 64 cases run one after
-another).
+another) and `warm_start` (iterations and wall time to residual drops of
+1e-4, 1e-6, 1e-8 from freestream vs from the learned prediction on held-out
+members of a bump family, with cl / cd of both converged runs).
 """
 from __future__ import annotations
 
@@ -80,6 +82,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-converge", action="store_true", help="skip the time-to-1e-8 runs")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-case batch")
+    ap.add_argument("--no-warm-start", action="store_true", help="skip the learned warm start")
     return ap.parse_args()
 
 
@@ -189,6 +192,55 @@ def batched_gpu(solver, steps: int, warmup: int):
             "speedup_vs_sequential": seq_s / batch_s, "tuning": tuning, "device_status": status,
             "note": "one launch per kernel for all 64 cases, each step replayed from a CUDA graph; "
                     "sequential = the 64 cases one after another, same settings, device time summed"}
+
+
+def warm_start_gpu(solver, n_train: int = 48, n_test: int = 8, ni: int = 97, nj: int = 49):
+    """Learned warm start on the bump family (97 x 49 x 5, farfield channel,
+    h ~ U[0.05,0.12], M ~ U[0.3,0.7]): training fields from n_train members run
+    3000 iterations as one batch, an 8 x 256 BF16 MLP trained on them with the
+    tcgen05 kernels, then n_test held-out members from freestream (cold) and
+    from the prediction (warm), both as a batch, to a 1e-8 drop of the cold
+    run's iteration-1 density residual; forces compared at the end."""
+    from aerocfd_b200 import warmstart as W
+    fam = W.family(n_train + n_test, seed=11, ni=ni, nj=nj, nk=5)
+    train, test = fam[:n_train], fam[n_train:]
+    t0 = time.perf_counter()
+    _, gen_s, batch = W.run_batch(solver, train, 3000, chunk=500)
+    X = np.concatenate([W.features(c, h, m) for c, h, m in train])
+    T = np.concatenate([W.targets(W.member(batch, i, c.cfg)) for i, (c, h, m) in enumerate(train)])
+    net = W.Network(width=256, depth=8, batch=8192, seed=3)
+    try:
+        t1 = time.perf_counter()
+        loss = net.train(X, T, steps=4000, lr=1e-3)
+        train_s = time.perf_counter() - t1
+        warm = {i: net.predict(W.features(c, h, m)) for i, (c, h, m) in enumerate(test)}
+    finally:
+        net.close()
+    iters, chunk = 6000, 50
+    hc, cold_s, bc = W.run_batch(solver, test, iters, chunk=chunk)
+    hw, warm_s, bw = W.run_batch(solver, test, iters, chunk=chunk, warm=warm)
+    out = {"family": f"bump_farfield_{ni}x{nj}x5", "train_members": n_train, "test_members": n_test,
+           "network": "8 x 256 SiLU MLP, BF16 weights/activations, FP32 accumulation, tcgen05 GEMMs",
+           "samples": int(len(X)), "train_steps": 4000, "train_s": train_s, "data_generation_s": gen_s,
+           "loss_first_last": [float(loss[:10].mean()), float(loss[-10:].mean())]}
+    for drop in (1e-4, 1e-6, 1e-8):
+        level = hc[0] * drop
+        ic, iw = W.first_below(hc, level, chunk), W.first_below(hw, level, chunk)
+        ok = (ic > 0) & (iw > 0)
+        out[f"{drop:.0e}"] = {"cold_iterations_mean": float(ic[ok].mean()) if ok.any() else None,
+                              "warm_iterations_mean": float(iw[ok].mean()) if ok.any() else None,
+                              "cold_wall_s": float(cold_s * ic[ok].max() / iters) if ok.any() else None,
+                              "warm_wall_s": float(warm_s * iw[ok].max() / iters) if ok.any() else None,
+                              "members_reached": int(ok.sum())}
+    out["iteration1_residual_ratio_warm_over_cold"] = float(np.mean(hw[0] / hc[0]))
+    diffs = []
+    for i, (c, h, m) in enumerate(test):
+        fc = W.wall_force(solver, W.member(bc, i, c.cfg))
+        fw = W.wall_force(solver, W.member(bw, i, c.cfg))
+        diffs.append(float(np.max(np.abs(fw[[6, 7]] - fc[[6, 7]]) / np.abs(fc[[6, 7]]))))
+    out["cl_cd_max_rel_diff"] = max(diffs)
+    out["total_s"] = time.perf_counter() - t0
+    return out
 
 
 def bump_cpu_rate(seconds: float = 4.0):
@@ -472,6 +524,8 @@ def main():
     gc.close()
     if world == 1 and not args.no_batch:
         line["batched"] = batched_gpu(solver, max(5, min(args.steps, 20)), args.warmup)
+    if world == 1 and not args.no_warm_start:
+        line["warm_start"] = warm_start_gpu(solver)
     if world == 1 and not args.no_converge:
         conv = {"workload": CONV_WORKLOAD, "target_drop": CONV_TARGET,
                 "fp64": converge_gpu(solver, False), "mixed": converge_gpu(solver, True)}
