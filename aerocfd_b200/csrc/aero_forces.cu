@@ -144,4 +144,34 @@ __global__ void k_forces_final(const double* __restrict__ part, int npart, CaseC
   }
 }
 
+// surface_output (sub_output_surface.f90:8-118): x, y, z and the pressure
+// coefficient cp = (p - p0) / qinf, p0 = d_0 t_0 / gamma / ma^2 and
+// qinf = 0.5 d_0 u_0^2 (:25-26), at every node of every wall subface, in the
+// reference's write order (block, subface, then k, j, i).  One thread per
+// node writes its four values contiguously, so the host copy is the file's
+// row order.
+__global__ void k_surface_cp(const BlockView* __restrict__ blocks, const SurfZone* __restrict__ zones, int nzone,
+                             long nnode, CaseConsts cc_launch, double* __restrict__ out) {
+  long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nnode) return;
+  int z = 0;
+  while (z + 1 < nzone && zones[z + 1].off <= q) ++z;
+  const SurfZone& Z = zones[z];
+  const BlockView& B = blocks[Z.block];
+  const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
+  long r = q - Z.off;
+  int i = Z.is + (int)(r % Z.nx);
+  r /= Z.nx;
+  int j = Z.js + (int)(r % Z.ny);
+  int k = Z.ks + (int)(r / Z.ny);
+  long n = B.at(i, j, k);
+  double p0 = cc.p_0;  // formed as d_0 * t_0 / gamma / ma / ma, as at :25
+  double qinf = 0.5 * cc.d_0 * p2(cc.u_0);
+  double p = B.v(F_PRI, 5, n);
+  out[4 * q + 0] = B.s(F_X, n);
+  out[4 * q + 1] = B.s(F_Y, n);
+  out[4 * q + 2] = B.s(F_Z, n);
+  out[4 * q + 3] = (p - p0) / qinf;
+}
+
 }  // namespace aero

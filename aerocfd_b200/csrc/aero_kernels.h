@@ -41,6 +41,16 @@ struct WallFace {
   long qoff;
 };
 
+// One wall subface of surface_output: its node box and the offset of its
+// first node in the output.
+struct SurfZone {
+  int block, face;
+  int is, js, ks, nx, ny, nz;
+  long off;
+};
+
+__global__ void k_surface_cp(const BlockView* __restrict__ blocks, const SurfZone* __restrict__ zones, int nzone,
+                             long nnode, CaseConsts cc_launch, double* __restrict__ out);
 __global__ void k_getpri(const BlockView* __restrict__ blocks, CaseConsts cc, unsigned* status);
 __global__ void k_forces(const BlockView* __restrict__ blocks, const WallFace* __restrict__ walls, int nwall,
                          long nquad, CaseConsts cc, double* __restrict__ part);

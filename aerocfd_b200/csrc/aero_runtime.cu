@@ -88,6 +88,11 @@ struct State {
   int nwall = 0;
   long nquad = 0;
   double* d_fpart = nullptr;
+  std::vector<SurfZone> surf;     // surface_output: wall subfaces (all nodes) and the x, y, z, cp rows
+  SurfZone* d_surf = nullptr;
+  long nsurf = 0;
+  int nsurf_live = 0;
+  double* d_surf_out = nullptr;
   CaseConsts* d_ccb = nullptr;   // per-block case constants (batches)
   double* d_resid_blocks = nullptr;  // 7 per block (aero_residual_blocks)
   double* d_out = nullptr;   // residual (7) + dt min/max (2)
@@ -767,6 +772,10 @@ static void release_case() {
   cudaFree(g.d_part); g.d_part = nullptr;
   cudaFree(g.d_walls); g.d_walls = nullptr;
   cudaFree(g.d_fpart); g.d_fpart = nullptr;
+  cudaFree(g.d_surf); g.d_surf = nullptr;
+  cudaFree(g.d_surf_out); g.d_surf_out = nullptr;
+  g.surf.clear();
+  g.nsurf = 0;
   cudaFree(g.d_ccb); g.d_ccb = nullptr;
   graph_release();
   cudaFree(g.d_resid_blocks); g.d_resid_blocks = nullptr;
@@ -1145,6 +1154,30 @@ int aero_finish_setup(void) {
       CK(cudaMalloc(&g.d_fpart, (size_t)cdiv(q, 256) * 6 * sizeof(double)));
     }
   }
+  // wall subfaces of surface_output: every node of the subface, lines included;
+  // zones without nodes keep their header but own no node index
+  {
+    g.surf.clear();
+    std::vector<SurfZone> live;
+    long q = 0;
+    for (int m = 0; m < nb; ++m)
+      for (const SubRow& r : g.blocks[m].subs) {
+        if (r.blk_t != BC_WALL) continue;
+        SurfZone z{m, r.face, r.is, r.js, r.ks, r.ie - r.is + 1, r.je - r.js + 1, r.ke - r.ks + 1, q};
+        g.surf.push_back(z);
+        if (z.nx > 0 && z.ny > 0 && z.nz > 0) {
+          live.push_back(z);
+          q += (long)z.nx * z.ny * z.nz;
+        }
+      }
+    g.nsurf = q;
+    g.nsurf_live = (int)live.size();
+    if (!live.empty()) {
+      CK(cudaMalloc(&g.d_surf, live.size() * sizeof(SurfZone)));
+      CK(cudaMemcpyAsync(g.d_surf, live.data(), live.size() * sizeof(SurfZone), cudaMemcpyHostToDevice, g.stream));
+      CK(cudaMalloc(&g.d_surf_out, (size_t)q * 4 * sizeof(double)));
+    }
+  }
   CK(cudaStreamSynchronize(g.stream));
   g.setup = true;
   return AERO_OK;
@@ -1372,6 +1405,37 @@ int aero_clcd_output(double sref, double* out8) {
   CK(cudaMemcpyAsync(g.h_out, g.d_out, 8 * sizeof(double), cudaMemcpyDeviceToHost, g.stream));
   CK(cudaStreamSynchronize(g.stream));
   std::memcpy(out8, g.h_out, 8 * sizeof(double));
+  return AERO_OK;
+}
+
+int aero_surface_count(long long* n_nodes, int* n_zones) {
+  int rc = need_setup();
+  if (rc) return rc;
+  if (!n_nodes || !n_zones) return fail(AERO_ERR_ARG, "null output pointer");
+  *n_nodes = g.nsurf;
+  *n_zones = (int)g.surf.size();
+  return AERO_OK;
+}
+
+int aero_surface_output(double* xyzcp, int* zones) {
+  int rc = need_setup();
+  if (rc) return rc;
+  if ((g.nsurf && !xyzcp) || (!g.surf.empty() && !zones)) return fail(AERO_ERR_ARG, "null output pointer");
+  for (size_t z = 0; z < g.surf.size(); ++z) {
+    const SurfZone& Z = g.surf[z];
+    int* o = zones + 5 * z;
+    o[0] = Z.block + 1;
+    o[1] = Z.face;
+    o[2] = Z.nx;
+    o[3] = Z.ny;
+    o[4] = Z.nz;
+  }
+  if (!g.nsurf) return AERO_OK;
+  PROF(P_FORCES, (k_surface_cp<<<cdiv(g.nsurf, 256), 256, 0, g.stream>>>(g.d_blocks, g.d_surf, g.nsurf_live,
+                                                                         g.nsurf, g.cc, g.d_surf_out)));
+  CKL();
+  CK(cudaMemcpyAsync(xyzcp, g.d_surf_out, (size_t)g.nsurf * 4 * sizeof(double), cudaMemcpyDeviceToHost, g.stream));
+  CK(cudaStreamSynchronize(g.stream));
   return AERO_OK;
 }
 

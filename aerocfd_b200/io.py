@@ -316,6 +316,39 @@ def write_flowfield(path: str, case: Case) -> None:
                 f.write(" ".join(f"{v:.17e}" for v in row) + "\n")
 
 
+def surface_path(timestep: int, rank: int = 0, directory: str = "result") -> str:
+    """The reference's surface file name (sub_output_surface.f90:30)."""
+    return os.path.join(directory, f"surfcp_{timestep:06d}_{rank:04d}.dat")
+
+
+def write_surface(path: str, zones: np.ndarray, rows: np.ndarray) -> None:
+    """surface_output's file (sub_output_surface.f90:32-113): per wall subface
+    a Tecplot point-format zone header and its x, y, z, cp rows, in the order
+    ``GpuCase.surface_output`` returns them; 17 significant digits."""
+    off = 0
+    with open(path, "w") as f:
+        for _, _, idim, jdim, kdim in np.asarray(zones).tolist():
+            f.write(" variables = x,y,z,cp\n")
+            f.write(f" zone i= {idim} j= {jdim} k= {kdim} datapacking=point\n")
+            n = idim * jdim * kdim if min(idim, jdim, kdim) > 0 else 0
+            for row in rows[off:off + n]:
+                f.write(" ".join(f"{v:.17e}" for v in row) + "\n")
+            off += n
+
+
+def read_surface(path: str) -> List[Tuple[Tuple[int, int, int], np.ndarray]]:
+    """Zones of a surface file: ((idim, jdim, kdim), rows x 4) each."""
+    out = []
+    r = _Reader(path)
+    while r.pos < len(r.lines) and r.lines[r.pos].strip():
+        r.skip(1)
+        head = r.read(7)
+        dims = (int(head[2]), int(head[4]), int(head[6]))
+        n = dims[0] * dims[1] * dims[2] if min(dims) > 0 else 0
+        out.append((dims, r.read_array(4 * n).reshape(n, 4)))
+    return out
+
+
 def read_restart(path: str, case: Case) -> None:
     """The restart branch of sub_init_flowfield.f90:117-268 (iflag_init = 1,
     3-D): reads a flowfield file written by flowfield_output and sets, on the

@@ -144,6 +144,16 @@ class GpuCase:
         _lib.check(self.L.aero_clcd_output(ctypes.c_double(sref), _p(out)), "aero_clcd_output")
         return out
 
+    def surface_output(self):
+        """surface_output on the device: zones (n x 5: block 1-based, face,
+        idim, jdim, kdim) and rows (m x 4: x, y, z, cp) of every wall subface."""
+        nn, nz = ctypes.c_longlong(0), ctypes.c_int(0)
+        _lib.check(self.L.aero_surface_count(ctypes.byref(nn), ctypes.byref(nz)), "aero_surface_count")
+        rows = np.zeros((nn.value, 4))
+        zones = np.zeros((nz.value, 5), dtype=np.int32)
+        _lib.check(self.L.aero_surface_output(_p(rows), ctypes.c_void_p(zones.ctypes.data)), "aero_surface_output")
+        return zones, rows
+
     def status(self) -> int:
         s = ctypes.c_uint(0)
         _lib.check(self.L.aero_get_status(ctypes.byref(s)), "aero_get_status")

@@ -84,6 +84,20 @@ module aerocfd_gpu
       real(c_double) :: out8(8)
     end function
 
+    ! sub_output_surface.f90:8 (surface_output): node and zone counts, then
+    ! xyzcp(4, n_nodes) and zones(5, n_zones) = block, face, idim, jdim, kdim
+    integer(c_int) function aero_surface_count(n_nodes, n_zones) bind(C, name="aero_surface_count")
+      import :: c_int, c_long_long
+      integer(c_long_long) :: n_nodes
+      integer(c_int) :: n_zones
+    end function
+
+    integer(c_int) function aero_surface_output(xyzcp, zones) bind(C, name="aero_surface_output")
+      import :: c_int, c_double
+      real(c_double) :: xyzcp(*)
+      integer(c_int) :: zones(*)
+    end function
+
     integer(c_int) function aero_finish_setup() bind(C, name="aero_finish_setup")
       import :: c_int
     end function

@@ -208,6 +208,15 @@ int aero_residual(double* out7);
  * reference area.  The per-element arithmetic is the reference's; the sums
  * over elements run in a fixed parallel order. */
 int aero_clcd_output(double sref, double* out8);
+/* sub_output_surface.f90:8-118 (surface_output): the rows the reference writes
+ * to result/surfcp_<timestep>_<rank>.dat.  aero_surface_count gives the number
+ * of wall-subface nodes and of wall subfaces (zones); aero_surface_output fills
+ * xyzcp (4 doubles per node: x, y, z, cp = (p - p0) / qinf, block by block,
+ * subface by subface in bcinfo order, then k, j, i) and zones (5 ints per
+ * zone: block (1-based), face, idim, jdim, kdim of the zone header) from the
+ * device's current pri_v and coordinates. */
+int aero_surface_count(long long* n_nodes, int* n_zones);
+int aero_surface_output(double* xyzcp, int* zones);
 /* sub_init_flowfield.f90:29-111 (freestream start) on all registered blocks */
 int aero_init_flowfield(void);
 /* sub_init_walldist.f90:9 (wall distance of every physical node) */

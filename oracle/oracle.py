@@ -143,6 +143,34 @@ class OracleCase:
         self.L.oracle_clcd_output(ctypes.c_double(sref), _p(out))
         return out
 
+    def surface_output(self):
+        """surface_output (sub_output_surface.f90:24-113) over the case's host
+        arrays: zones (block 1-based, face, idim, jdim, kdim) of every wall
+        subface in block and bcinfo order, and its rows x, y, z,
+        cp = (p - p0)/qinf in k, j, i order, p0 = d_0 t_0/gamma/ma/ma and
+        qinf = 0.5 d_0 u_0**2 (:25-26)."""
+        gamma, d_0, u_0, t_0 = 1.4, 1.0, 1.0, 1.0
+        ma = self.case.cfg.ma
+        p0 = d_0 * t_0 / gamma / ma / ma
+        qinf = 0.5 * d_0 * u_0 ** 2
+        zones, rows = [], []
+        for m, b in enumerate(self.case.blocks):
+            for sf in b.subfaces:
+                if sf.blk_t != -20:
+                    continue
+                box = (sf.is_, sf.ie, sf.js, sf.je, sf.ks, sf.ke)
+                dims = (sf.ie - sf.is_ + 1, sf.je - sf.js + 1, sf.ke - sf.ks + 1)
+                zones.append((m + 1, sf.face) + dims)
+                if min(dims) <= 0:
+                    continue
+                s = b.sl(box)
+                p = b.fields["pri_v"][s][..., 4]
+                cp = (p - p0) / qinf
+                cols = [b.fields["x"][s], b.fields["y"][s], b.fields["z"][s], cp]
+                rows.append(np.stack([c.ravel() for c in cols], axis=1))
+        out = np.concatenate(rows) if rows else np.zeros((0, 4))
+        return np.array(zones, dtype=np.int64).reshape(-1, 5), out
+
     def last_dt_minmax(self) -> np.ndarray:
         out = np.zeros(4)
         self.L.oracle_last_dt_minmax(_p(out))

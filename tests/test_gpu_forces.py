@@ -74,3 +74,29 @@ def test_clcd_output_matches_oracle(gpu, oracle_mod, make):
     div = 2.0  # 1 / (0.5 * rho * u^2 * sref) with rho = u = sref = 1
     sc = div * (scale[0] + scale[1] + scale[3] + scale[4])
     assert np.all(np.abs(got[6:8] - ref[6:8]) <= TOL * sc), (got[6:8], ref[6:8])
+
+
+@pytest.mark.parametrize("make", [cavity, naca_small])
+def test_surface_output_matches_oracle(gpu, oracle_mod, make):
+    """surface_output: zone headers equal and every x, y, z, cp bit-identical
+    (cp is one subtraction and one division per node)."""
+    co, cg = make(), make()
+    oc = oracle_mod.OracleCase(co)
+    oc.geometry()
+    oc.init_flowfield()
+    perturb(co, seed=4, amp=0.02)
+    oc.start()
+    oc.iterate(2)
+    for bo, bg in zip(co.blocks, cg.blocks):
+        for name, _ in FIELDS:
+            bg.fields[name][...] = bo.fields[name]
+    zref, rref = oc.surface_output()
+    gc = gpu.GpuCase(cg)
+    try:
+        gc.sync_to_device(gpu.ALL)
+        zgot, rgot = gc.surface_output()
+    finally:
+        gc.close()
+    assert np.array_equal(zgot, zref)
+    assert rgot.shape == rref.shape and len(rgot) > 0
+    assert np.array_equal(rgot, rref), np.abs(rgot - rref).max()

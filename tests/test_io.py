@@ -111,3 +111,17 @@ def test_flowfield_restart_round_trip(tmp_path, oracle_mod):
         assert np.array_equal(pb[..., 6], np.sqrt(pb[..., 4]) / ma)
         assert np.all(b.fields["dt"][s] == cb.cfg.dt) and np.all(b.fields["amu"][s][..., 0] == 1.0)
         assert not b.fields["rhs"][s].any()
+
+
+def test_surface_file_round_trip(tmp_path):
+    """write_surface / read_surface: headers and values survive exactly,
+    including a zone without nodes."""
+    rng = np.random.default_rng(0)
+    zones = np.array([[1, 3, 5, 1, 3], [2, 4, 0, 1, 3], [2, 5, 2, 4, 1]])
+    rows = rng.standard_normal((15 + 8, 4)) * 10.0 ** rng.integers(-8, 8, (23, 4))
+    path = tmp_path / "surfcp.dat"
+    io.write_surface(str(path), zones, rows)
+    back = io.read_surface(str(path))
+    assert [z for z, _ in back] == [(5, 1, 3), (0, 1, 3), (2, 4, 1)]
+    assert np.array_equal(np.concatenate([r for _, r in back]), rows)
+    assert io.surface_path(12, 3) == "result/surfcp_000012_0003.dat"
