@@ -585,6 +585,169 @@ __global__ void k_lusgs_sweep_global(const BlockView* __restrict__ blocks, int n
   (void)status;
 }
 
+namespace {
+
+__device__ __forceinline__ unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ unsigned cluster_size() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
+
+// One row of one node of a plane, as lusgs_rows computes it, with the values
+// written during the sweep (previous plane, dq*) loaded from L2: they come
+// from other SMs, and a line cached in this SM's L1 before they were written
+// would be stale.
+template <bool FWD>
+__device__ __forceinline__ double lusgs_row_l2(const double* rec, const double* sca, const double* dsv, int cnt,
+                                               int t, int row, const double* prev, long pst, int wst) {
+  double packed = rec[75 * cnt + t];
+  double acc[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    int w = nbr_local(packed, d);
+    double sd = 0.0;
+    if (w >= 0) {
+      const double* x = prev + (long)w * wst;
+      const double* mr = rec + (25 * d + 5 * row) * cnt + t;
+      sd = mr[0] * __ldcg(x);
+      sd = sd + mr[cnt] * __ldcg(x + pst);
+      sd = sd + mr[2 * cnt] * __ldcg(x + 2 * pst);
+      sd = sd + mr[3 * cnt] * __ldcg(x + 3 * pst);
+      sd = sd + mr[4 * cnt] * __ldcg(x + 4 * pst);
+    }
+    acc[d] = sd;
+  }
+  const double diag = sca[5 * cnt + t], invj = sca[6 * cnt + t];
+  const double rdiag = sca[7 * cnt + t], rinvj = sca[8 * cnt + t];
+  if (FWD) return div_rn(div_rn(sca[row * cnt + t] + (acc[0] + acc[1] + acc[2]), diag, rdiag), invj, rinvj);
+  return __ldcg(dsv + row * cnt + t) - div_rn(div_rn(acc[0] + acc[1] + acc[2], invj, rinvj), diag, rdiag);
+}
+
+}  // namespace
+
+// The records of one row of one node, loaded ahead of the plane barrier (they
+// were written before the sweep started).
+struct RowRecs {
+  double packed, m[15], rhs, diag, invj, rdiag, rinvj;
+  int row, node;
+};
+__device__ __forceinline__ void load_row_recs(const double* rec, const double* sca, int cnt, int t, RowRecs& r) {
+  r.row = t / cnt;
+  r.node = t - r.row * cnt;
+  const double* rn = rec + r.node;
+  r.packed = rn[75 * cnt];
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+#pragma unroll
+    for (int c = 0; c < 5; ++c) r.m[5 * d + c] = rn[(25 * d + 5 * r.row + c) * cnt];
+  const double* sn = sca + r.node;
+  r.rhs = sn[r.row * cnt];
+  r.diag = sn[5 * cnt];
+  r.invj = sn[6 * cnt];
+  r.rdiag = sn[7 * cnt];
+  r.rinvj = sn[8 * cnt];
+}
+// lusgs_rows' arithmetic for one row from preloaded records; the previous
+// plane's dq and dq* are loaded from L2 (written by other SMs during the sweep).
+template <bool FWD>
+__device__ __forceinline__ double row_from_recs(const RowRecs& r, const double* prev, long pst, int wst,
+                                                const double* dsv, int cnt) {
+  double acc[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    int w = nbr_local(r.packed, d);
+    double sd = 0.0;
+    if (w >= 0) {
+      const double* x = prev + (long)w * wst;
+      sd = r.m[5 * d] * __ldcg(x);
+      sd = sd + r.m[5 * d + 1] * __ldcg(x + pst);
+      sd = sd + r.m[5 * d + 2] * __ldcg(x + 2 * pst);
+      sd = sd + r.m[5 * d + 3] * __ldcg(x + 3 * pst);
+      sd = sd + r.m[5 * d + 4] * __ldcg(x + 4 * pst);
+    }
+    acc[d] = sd;
+  }
+  if (FWD) return div_rn(div_rn(r.rhs + (acc[0] + acc[1] + acc[2]), r.diag, r.rdiag), r.invj, r.rinvj);
+  return __ldcg(dsv + r.row * cnt + r.node) -
+         div_rn(div_rn(acc[0] + acc[1] + acc[2], r.invj, r.rinvj), r.diag, r.rdiag);
+}
+
+// The global-memory sweeps of one block spread over a thread-block cluster
+// (grid x = blocks x cluster size, cluster dims (CL,1,1)): the CL CTAs of a
+// cluster share every plane, one thread per row of a node (t < 5*cnt, row
+// t / cnt, consecutive threads on consecutive nodes of one row), and meet at a
+// cluster barrier between planes, which orders each plane's dq stores before
+// the next plane's loads.  The barrier is split: between its arrive and its
+// wait each thread loads the records of its first row of the next plane, so
+// only the neighbours' dq loads remain on the path from plane to plane.  All
+// CTAs of a cluster are resident together and every thread takes the same 2H
+// barriers, so the barrier always completes.  The arithmetic per row is
+// lusgs_rows'.
+__global__ void __launch_bounds__(512, 1) k_lusgs_sweep_cluster(const BlockView* __restrict__ blocks) {
+  const unsigned ncta = cluster_size();
+  const BlockView& B = blocks[blockIdx.x / ncta];
+  const int H = B.nplanes;
+  const long* poff = B.poff;
+  const int G = (int)(ncta * blockDim.x);
+  const int g = (int)(cluster_rank() * blockDim.x + threadIdx.x);
+  // records of this thread's first row of global step gs (forward: gs < H)
+  RowRecs pre;
+  auto preload = [&](int gs) {
+    if (gs >= 2 * H) return;
+    const bool fwd = gs < H;
+    const int h = fwd ? gs : 2 * H - 1 - gs;
+    const long base = poff[h];
+    const int cnt = (int)(poff[h + 1] - base);
+    if (g < 5 * cnt) load_row_recs((fwd ? B.rec_f : B.rec_b) + kRec * base, B.sca + kSca * base, cnt, g, pre);
+  };
+  preload(0);
+  for (int gs = 0; gs < 2 * H; ++gs) {
+    const bool fwd = gs < H;
+    const int h = fwd ? gs : 2 * H - 1 - gs;
+    const long base = poff[h];
+    const int cnt = (int)(poff[h + 1] - base);
+    const double* rec = (fwd ? B.rec_f : B.rec_b) + kRec * base;
+    const double* sca = B.sca + kSca * base;
+    const double* dsv = B.dqs + 8 * base;
+    const double* prev = sca;
+    long pst = 0;
+    int wst = 0;
+    if (fwd && h > 0) {
+      prev = B.dqs + 8 * poff[h - 1];
+      pst = poff[h] - poff[h - 1];
+      wst = 1;
+    } else if (!fwd && h + 1 < H) {
+      prev = B.dq + 5 * poff[h + 1];
+      pst = 1;
+      wst = 5;
+    }
+    if (g < 5 * cnt) {
+      double v = fwd ? row_from_recs<true>(pre, prev, pst, wst, dsv, cnt)
+                     : row_from_recs<false>(pre, prev, pst, wst, dsv, cnt);
+      if (fwd)
+        B.dqs[8 * base + pre.row * cnt + pre.node] = v;
+      else
+        B.dq[5 * (base + pre.node) + pre.row] = v;
+    }
+    for (int t = g + G; t < 5 * cnt; t += G) {
+      const int row = t / cnt;
+      const int node = t - row * cnt;
+      if (fwd)
+        B.dqs[8 * base + row * cnt + node] = lusgs_row_l2<true>(rec, sca, dsv, cnt, node, row, prev, pst, wst);
+      else
+        B.dq[5 * (base + node) + row] = lusgs_row_l2<false>(rec, sca, dsv, cnt, node, row, prev, pst, wst);
+    }
+    asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+    preload(gs + 1);
+    asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+  }
+}
+
 // q = q + dq on every updated node (sub_timeadvancement_1stimplicit.f90:568-574).
 __global__ void k_lusgs_update(const BlockView* __restrict__ blocks) {
   const BlockView& B = blocks[blockIdx.y];

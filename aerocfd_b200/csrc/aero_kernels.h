@@ -90,6 +90,7 @@ __global__ void k_sa_recs(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_sweep(const BlockView* __restrict__ blocks);
 __global__ void k_lusgs_sweep_staged(const BlockView* __restrict__ blocks, int nst, unsigned* status);
 __global__ void k_lusgs_sweep_global(const BlockView* __restrict__ blocks, int nst, unsigned* status);
+__global__ void k_lusgs_sweep_cluster(const BlockView* __restrict__ blocks);
 __global__ void k_lusgs_update(const BlockView* __restrict__ blocks);
 __global__ void k_physical_bc(const BlockView* __restrict__ blocks, const BcOp* __restrict__ ops,
                               const int* __restrict__ op_start, int o, CaseConsts cc);

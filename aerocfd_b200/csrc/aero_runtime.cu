@@ -123,6 +123,7 @@ struct State {
     int visc = 128;     // threads per CTA of k_viscous_a
     int mats = 128;     // threads per CTA of k_lusgs_mats
     int nst_max = 4;    // most shared-memory stages of the staged sweep
+    int sweep_cl = 0;   // CTAs per block of the global-memory sweep (0, 1: one CTA; 2..8: a cluster)
   } tune;
   // CUDA graph of one time step (aero_use_graphs)
   bool graph_want = false;
@@ -131,7 +132,8 @@ struct State {
   double* d_tmax = nullptr;
   size_t t_tmax = 0;
   std::string err;
-  std::string tuning = "inviscid_tile=64 elementwise_threads=256 viscous_threads=128 mats_threads=128 sweep_stages<=4";
+  std::string tuning = "inviscid_tile=64 elementwise_threads=256 viscous_threads=128 mats_threads=128 sweep_stages<=4 "
+                       "sweep_cluster=1";
 };
 
 State g;
@@ -496,7 +498,27 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
   // consumer threads: one per row of every node of the largest plane
   auto consumers_for = [](int p) { return (5 * std::max(p, 1) + 31) / 32 * 32; };
   if (nst >= 2 && consumers_for(pmax) + 32 > staged_max_threads) nst = 0;
-  if (nst >= 2) {
+  if (g.tune.sweep_cl >= 2) {
+    // one cluster of sweep_cl CTAs per block, one thread per row of every
+    // node of the largest plane (at most 512 per CTA; more rows loop)
+    const int cl = g.tune.sweep_cl;
+    int threads = (int)std::min<long>(512, std::max<long>(64, ((5L * pmax + cl - 1) / cl + 31) / 32 * 32));
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3((unsigned)(nblk * cl));
+    lc.blockDim = dim3((unsigned)threads);
+    lc.dynamicSmemBytes = 0;
+    lc.stream = g.stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)cl;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    cudaError_t le = cudaSuccess;
+    PROF(P_LUSGS_SWEEP, (le = cudaLaunchKernelEx(&lc, k_lusgs_sweep_cluster, views)));
+    CK(le);
+  } else if (nst >= 2) {
     int consumers = consumers_for(pmax);
     size_t smem = offs + ring + nst * stage + (2 * nst + 1) * 8;
     static size_t set_staged = 0;
@@ -845,6 +867,15 @@ int aero_use_graphs(int on) {
   return AERO_OK;
 }
 
+void set_tuning_text() {
+  char buf[200];
+  std::snprintf(buf, sizeof buf,
+                "inviscid_tile=%d elementwise_threads=%d viscous_threads=%d mats_threads=%d sweep_stages<=%d "
+                "sweep_cluster=%d",
+                g.tune.inv_tile, g.tune.ew, g.tune.visc, g.tune.mats, g.tune.nst_max, std::max(1, g.tune.sweep_cl));
+  g.tuning = buf;
+}
+
 int aero_autotune(int iters) {
   int rc = need_setup();
   if (rc) return rc;
@@ -893,7 +924,7 @@ int aero_autotune(int iters) {
   struct Knob { int* v; std::vector<int> cand; };
   std::vector<Knob> knobs = {{&g.tune.inv_tile, {0, 32, 64, 128}}, {&g.tune.ew, {128, 256, 512}},
                              {&g.tune.visc, {64, 128, 256}}, {&g.tune.mats, {64, 128, 256}},
-                             {&g.tune.nst_max, {2, 3, 4}}};
+                             {&g.tune.nst_max, {2, 3, 4}}, {&g.tune.sweep_cl, {0, 2, 4, 8}}};
   for (Knob& k : knobs) {
     int best = *k.v;
     double best_ms = 1e300;
@@ -914,10 +945,7 @@ int aero_autotune(int iters) {
   g.graph_want = graphs;
   if (rc) return rc;
   if (rc2) return rc2;
-  char buf[160];
-  std::snprintf(buf, sizeof buf, "inviscid_tile=%d elementwise_threads=%d viscous_threads=%d mats_threads=%d sweep_stages<=%d",
-                g.tune.inv_tile, g.tune.ew, g.tune.visc, g.tune.mats, g.tune.nst_max);
-  g.tuning = buf;
+  set_tuning_text();
   return AERO_OK;
 }
 
@@ -937,10 +965,18 @@ int aero_set_tuning(int inv_tile, int ew, int visc, int mats, int nst_max) {
   g.tune.mats = mats;
   g.tune.nst_max = nst_max;
   graph_release();
-  char buf[160];
-  std::snprintf(buf, sizeof buf, "inviscid_tile=%d elementwise_threads=%d viscous_threads=%d mats_threads=%d sweep_stages<=%d",
-                inv_tile, ew, visc, mats, nst_max);
-  g.tuning = buf;
+  set_tuning_text();
+  return AERO_OK;
+}
+
+int aero_set_sweep_cluster(int ctas) {
+  int rc = need_init();
+  if (rc) return rc;
+  if (ctas != 1 && ctas != 2 && ctas != 4 && ctas != 8)
+    return fail(AERO_ERR_ARG, "sweep cluster of %d CTAs is not 1, 2, 4 or 8", ctas);
+  g.tune.sweep_cl = ctas == 1 ? 0 : ctas;
+  graph_release();
+  set_tuning_text();
   return AERO_OK;
 }
 

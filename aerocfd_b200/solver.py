@@ -134,6 +134,10 @@ class GpuCase:
         _lib.check(self.L.aero_set_tuning(ctypes.c_int(inv_tile), ctypes.c_int(ew), ctypes.c_int(visc),
                                           ctypes.c_int(mats), ctypes.c_int(nst_max)), "aero_set_tuning")
 
+    def set_sweep_cluster(self, ctas: int) -> None:
+        """aero_set_sweep_cluster: CTAs per block of the LU-SGS sweep (1, 2, 4, 8)."""
+        _lib.check(self.L.aero_set_sweep_cluster(ctypes.c_int(ctas)), "aero_set_sweep_cluster")
+
     def set_precision(self, mixed: bool) -> None:
         """aero_set_precision: 0 = FP64 reference arithmetic, 1 = mixed."""
         _lib.check(self.L.aero_set_precision(ctypes.c_int(1 if mixed else 0)), "aero_set_precision")

@@ -248,7 +248,8 @@ int aero_step_timed(int nsteps, int flush_l2, double* device_ms);
  * first use; results are those of the launches it replays.
  * aero_autotune(iters): times iters steps for each candidate launch shape
  * (inviscid-flux CTA tile, element-wise / viscous / block-record thread
- * counts, sweep stages), keeps the fastest of each in turn, and restores the
+ * counts, sweep stages, CTAs per block of the LU-SGS sweep), keeps the fastest
+ * of each in turn, and restores the
  * solution state (q, nut, q0, dt, amu) it started from; the arithmetic is the
  * same for every shape.  aero_tuning() describes the shapes in use. */
 int aero_use_graphs(int on);
@@ -258,6 +259,11 @@ const char* aero_tuning(void);
  * tile 0 (face-based kernels), 32, 64 or 128; element-wise threads 128, 256,
  * 512; viscous and block-record threads 64, 128, 256; sweep stages 2..4. */
 int aero_set_tuning(int inv_tile, int ew, int visc, int mats, int nst_max);
+/* CTAs that share each block's LU-SGS sweep: 1 (one CTA per block, the
+ * records staged in shared memory when its planes fit) or a thread-block
+ * cluster of 2, 4 or 8 CTAs meeting at a cluster barrier between hyperplanes.
+ * The arithmetic is the same for every choice. */
+int aero_set_sweep_cluster(int ctas);
 
 /* ---- warm-start network (no counterpart in the reference) --------------
  * aero_mlp_gemm: c[M x N] = a[M x K] * b[N x K]^T on the tcgen05 tensor cores,
