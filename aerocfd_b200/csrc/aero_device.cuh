@@ -62,6 +62,8 @@ struct BlockView {
   double* sca;           // 8 per node: rhs(5), diag, inv_j, unused
   int* nbr;              // 6 per node: hyperplane-major positions of those neighbours (-1: outside)
   long* nat;             // natural (box) index of the node
+  double* sa_rec;        // kSaRec per node: SA sweep records (plane-local layout)
+  double* sa_dq;         // 1 per node: SA forward-sweep increment
   double* dqs;           // 8 per node: dq* (forward result), padded to 64 bytes
   double* dq;            // 5 per node: dq (backward result)
   // Case constants of this block when blocks of different cases share one
@@ -80,6 +82,26 @@ struct BlockView {
 constexpr int kRec = 76;
 // LU-SGS per-node scalars: rhs(5), diag, inv_j, 1/diag, 1/inv_j, unused.
 constexpr int kSca = 10;
+// SA sweep records per node: 0.5*(U+|U|) x3, 0.5*(U-|U|) x3, sa_rhs, diag,
+// packed forward and backward neighbours.
+constexpr int kSaRec = 10;
+
+// Three plane-local indices (+1; 0 = no neighbour) in one 64-bit word: the
+// neighbours' positions in their hyperplane relative to its first node.
+constexpr int kNbrBits = 21;
+__device__ __forceinline__ double pack_nbrs(const int* nb, long prev_base) {
+  unsigned long long u = 0;
+#pragma unroll
+  for (int e = 0; e < 3; ++e) {
+    unsigned long long f = nb[e] < 0 ? 0ull : (unsigned long long)(nb[e] - prev_base + 1);
+    u |= f << (kNbrBits * e);
+  }
+  return __longlong_as_double((long long)u);
+}
+__device__ __forceinline__ int nbr_local(double packed, int e) {
+  unsigned long long u = (unsigned long long)__double_as_longlong(packed);
+  return (int)((u >> (kNbrBits * e)) & ((1ull << kNbrBits) - 1)) - 1;
+}
 
 
 // ---------------------------------------------------------------- arithmetic

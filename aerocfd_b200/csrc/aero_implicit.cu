@@ -142,21 +142,6 @@ __device__ __forceinline__ long rec_at(const BlockView& B, long pos, int h, int 
   long cnt = B.poff[h + 1] - base;
   return stride * base + x * cnt + (pos - base);
 }
-// Three plane-local indices (+1; 0 = no neighbour) in one 64-bit word.
-constexpr int kNbrBits = 21;
-__device__ __forceinline__ double pack_nbrs(const int* nb, long prev_base) {
-  unsigned long long u = 0;
-#pragma unroll
-  for (int e = 0; e < 3; ++e) {
-    unsigned long long f = nb[e] < 0 ? 0ull : (unsigned long long)(nb[e] - prev_base + 1);
-    u |= f << (kNbrBits * e);
-  }
-  return __longlong_as_double((long long)u);
-}
-__device__ __forceinline__ int nbr_local(double packed, int e) {
-  unsigned long long u = (unsigned long long)__double_as_longlong(packed);
-  return (int)((u >> (kNbrBits * e)) & ((1ull << kNbrBits) - 1)) - 1;
-}
 
 // The off-diagonal blocks of both sweeps, off the critical path.  For every
 // updated node (the provider) and direction d: A = calc_jm at the provider,

@@ -63,6 +63,11 @@ struct State {
   bool inited = false;
   int device = 0;
   cudaStream_t stream = nullptr;
+  // second stream of a steady iteration: sa_model runs on it beside implicit1st
+  // (neither reads what the other writes), forked after find_dt and joined
+  // before the boundary conditions
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool configured = false;
   int iflags[8] = {};
   double params[7] = {};
@@ -187,12 +192,13 @@ struct ProfScope {
     }
   }
 };
-#define PROF(id, launch)                 \
+#define PROF_ON(id, st, launch)          \
   do {                                   \
-    ProfScope ps_(id, g.stream);         \
+    ProfScope ps_(id, st);               \
     launch;                              \
-    ps_.end(g.stream);                   \
+    ps_.end(st);                         \
   } while (0)
+#define PROF(id, launch) PROF_ON(id, g.stream, launch)
 
 void prof_collect() {
   if (gp.marks.empty()) return;
@@ -264,11 +270,11 @@ void fill_view(BlockView& v, const Box& b, const Box& b0, const Box& b1, long pl
 }
 
 // LU-SGS workspace of one view (see BlockView): one device allocation holding
-// poff, rec_f, rec_b, sca, dqs, dq, nat, nbr.
+// poff, rec_f, rec_b, sca, dqs, dq, sa_rec, sa_dq, nat, nbr.
 size_t workspace_bytes(const Box& b1, int H) {
   size_t N1 = (size_t)b1.size();
-  return (size_t)(H + 1) * sizeof(long) + N1 * (2 * kRec + kSca + 8 + 5) * sizeof(double) + N1 * sizeof(long) +
-         N1 * 6 * sizeof(int) + 256;
+  return (size_t)(H + 1) * sizeof(long) + N1 * (2 * kRec + kSca + 8 + 5 + kSaRec + 1) * sizeof(double) +
+         N1 * sizeof(long) + N1 * 6 * sizeof(int) + 256;
 }
 int attach_workspace(BlockView& v, void* ws, const std::vector<long>& poff, int pmax) {
   size_t N1 = (size_t)v.b1.size();
@@ -280,6 +286,8 @@ int attach_workspace(BlockView& v, void* ws, const std::vector<long>& poff, int 
   v.sca = (double*)p; p += N1 * kSca * sizeof(double);
   v.dqs = (double*)p; p += N1 * 8 * sizeof(double);
   v.dq = (double*)p; p += N1 * 5 * sizeof(double);
+  v.sa_rec = (double*)p; p += N1 * kSaRec * sizeof(double);
+  v.sa_dq = (double*)p; p += N1 * sizeof(double);
   v.nat = (long*)p; p += N1 * sizeof(long);
   v.poff = (long*)p; p += poff.size() * sizeof(long);
   v.nbr = (int*)p;
@@ -549,19 +557,22 @@ int launch_index(const BlockView* views, int nblk, long maxN1) {
   return AERO_OK;
 }
 
-// sa_model (sub_tur_sa.f90:7-122) on nblk views; needs the hyperplane index.
-int launch_sa(const BlockView* views, int nblk, long maxN, long maxN1, int pmax, const CaseConsts& cc) {
-  PROF(P_FILL, (k_sa_length<<<dim3(cdiv(maxN, 256), nblk), 256, 0, g.stream>>>(views)));
+// sa_model (sub_tur_sa.f90:7-122) on nblk views, on stream st (the library's
+// stream when null); needs the hyperplane index.
+int launch_sa(const BlockView* views, int nblk, long maxN, long maxN1, int pmax, const CaseConsts& cc,
+              cudaStream_t st = nullptr) {
+  if (!st) st = g.stream;
+  PROF_ON(P_FILL, st, (k_sa_length<<<dim3(cdiv(maxN, 256), nblk), 256, 0, st>>>(views)));
   CKL();
-  PROF(P_SA_A, (k_sa_a<<<dim3(cdiv(maxN1, 256), nblk), 256, 0, g.stream>>>(views, cc)));
+  PROF_ON(P_SA_A, st, (k_sa_a<<<dim3(cdiv(maxN1, 256), nblk), 256, 0, st>>>(views, cc)));
   CKL();
-  PROF(P_SA_B, (k_sa_b<<<dim3(cdiv(maxN1, 128), nblk), 128, 0, g.stream>>>(views, cc)));
+  PROF_ON(P_SA_B, st, (k_sa_b<<<dim3(cdiv(maxN1, 128), nblk), 128, 0, st>>>(views, cc)));
   CKL();
-  PROF(P_SA_RECS, (k_sa_recs<<<dim3(cdiv(maxN1, 256), nblk), 256, 0, g.stream>>>(views, cc)));
+  PROF_ON(P_SA_RECS, st, (k_sa_recs<<<dim3(cdiv(maxN1, 256), nblk), 256, 0, st>>>(views, cc)));
   CKL();
   size_t smem = (size_t)2 * std::max(pmax, 1) * sizeof(double);
   int threads = (int)std::min<long>(1024, std::max<long>(64, (pmax + 31) / 32 * 32));
-  PROF(P_SA_SWEEP, (k_sa_sweep<<<nblk, threads, smem, g.stream>>>(views)));
+  PROF_ON(P_SA_SWEEP, st, (k_sa_sweep<<<nblk, threads, smem, st>>>(views)));
   CKL();
   return AERO_OK;
 }
@@ -676,8 +687,18 @@ int do_iteration(bool want_dt_minmax) {
   if (viscous_on() && (rc = launch_viscous(g.d_blocks, nb, g.max_b0, g.cc, 0))) return rc;
   if ((rc = launch_find_dt(g.d_blocks, nb, g.max_box, g.cc))) return rc;
   if (want_dt_minmax && (rc = launch_dt_minmax(g.d_blocks, nb - 1, g.d_out + 7))) return rc;
+  // sa_model reads pri_v, amu, dudx, vor, dt and the metrics and writes nut,
+  // sa_rhs and its own scratch; implicit1st reads none of those it writes and
+  // writes only q and its own scratch: the two run side by side
+  const bool sa = sa_on();
+  if (sa) {
+    CK(cudaEventRecord(g.ev_fork, g.stream));
+    CK(cudaStreamWaitEvent(g.stream2, g.ev_fork, 0));
+    if ((rc = launch_sa(g.d_blocks, nb, g.max_box, g.max_b1, g.pmax_all, g.cc, g.stream2))) return rc;
+    CK(cudaEventRecord(g.ev_join, g.stream2));
+  }
   if ((rc = launch_implicit(g.d_blocks, nb, g.max_ext, g.max_b1, g.pmax_all, g.hmax_all, g.cc))) return rc;
-  if (sa_on() && (rc = launch_sa(g.d_blocks, nb, g.max_box, g.max_b1, g.pmax_all, g.cc))) return rc;
+  if (sa) CK(cudaStreamWaitEvent(g.stream, g.ev_join, 0));
   if ((rc = do_physical_bc())) return rc;
   if ((rc = do_halo())) return rc;
   if ((rc = do_average1())) return rc;
@@ -765,6 +786,9 @@ int aero_init(int device) {
   if (g.inited) return AERO_OK;
   CK(cudaSetDevice(device));
   CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&g.stream2, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&g.ev_fork, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&g.ev_join, cudaEventDisableTiming));
   CK(cudaMalloc(&g.d_status, sizeof(unsigned)));
   CK(cudaMemset(g.d_status, 0, sizeof(unsigned)));
   CK(cudaMalloc(&g.d_out, 16 * sizeof(double)));
@@ -819,6 +843,9 @@ int aero_finalize(void) {
   cudaFree(g.d_out); g.d_out = nullptr;
   cudaFreeHost(g.h_out); g.h_out = nullptr;
   cudaStreamDestroy(g.stream); g.stream = nullptr;
+  cudaStreamDestroy(g.stream2); g.stream2 = nullptr;
+  cudaEventDestroy(g.ev_fork); g.ev_fork = nullptr;
+  cudaEventDestroy(g.ev_join); g.ev_join = nullptr;
   g.inited = false;
   g.configured = false;
   // execution options of the finished run

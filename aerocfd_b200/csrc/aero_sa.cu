@@ -160,18 +160,26 @@ __global__ void k_sa_b(const BlockView* __restrict__ blocks, CaseConsts cc_launc
   B.s(F_DIASD, n) = fmin(spn + sdn, 0.0);
 }
 
-// sa_lusgs diagonal and upwind coefficients of every updated node, stored in
-// the node's hyperplane-major record: rec_f[0..2] = 0.5*(U+|U|) per
-// direction, rec_f[3..5] = 0.5*(U-|U|), rec_f[6] = sa_rhs, rec_f[7] = diag
-// (sub_tur_sa.f90:676-750, :762-778).
+// sa_lusgs diagonal and upwind coefficients of every updated node
+// (sub_tur_sa.f90:676-750, :762-778) in the plane-local layout of the sweep:
+// the records of hyperplane h form one chunk at kSaRec*poff[h], element x of
+// plane-local node t at x*cnt + t, so a warp's loads are consecutive words.
+// x = 0..2: 0.5*(U+|U|) per direction, 3..5: 0.5*(U-|U|), 6: sa_rhs, 7: diag,
+// 8 / 9: the packed forward / backward neighbours.
 __global__ void k_sa_recs(const BlockView* __restrict__ blocks, CaseConsts cc_launch) {
   const BlockView& B = blocks[blockIdx.y];
   const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
   const Box& b1 = B.b1;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= b1.size()) return;
-  long pos = t;  // the record of the t-th node in hyperplane-major order
+  long pos = t;  // the t-th node in hyperplane-major order
   long n = B.nat[pos];
+  long r = n / B.nx;
+  const int i = B.b.is + (int)(n - r * B.nx);
+  const int j = B.b.js + (int)(r % B.ny);
+  const int k = B.b.ks + (int)(r / B.ny);
+  const int h = (i - b1.is) + (j - b1.js) + (k - b1.ks);
+  const long base = B.poff[h], cnt = B.poff[h + 1] - base;
   double phi = (cc.cfl >= 1.0e3 && cc.time == IFLAG_STEADY) ? 0.0 : 1.0;
   double u = B.v(F_PRI, 2, n), v = B.v(F_PRI, 3, n), w = B.v(F_PRI, 4, n);
   double x0 = B.v(F_DXIDX, 1, n), y0 = B.v(F_DXIDX, 2, n), z0 = B.v(F_DXIDX, 3, n);
@@ -185,60 +193,114 @@ __global__ void k_sa_recs(const BlockView* __restrict__ blocks, CaseConsts cc_la
   double cw = x0 * u + y0 * v + z0 * w;
   double tm = 4.0 * d2 * B.s(F_NUT, n) / cc.re;
   double diag = 1.0 / B.s(F_DT, n) * phi + fabs(cu) + fabs(cv) + fabs(cw) + tm - B.s(F_DIASD, n);
-  double* rec = B.rec_f + kRec * pos;
+  double* rec = B.sa_rec + kSaRec * base + (pos - base);
   rec[0] = 0.5 * (cu + fabs(cu));
-  rec[1] = 0.5 * (cv + fabs(cv));
-  rec[2] = 0.5 * (cw + fabs(cw));
-  rec[3] = 0.5 * (cu - fabs(cu));
-  rec[4] = 0.5 * (cv - fabs(cv));
-  rec[5] = 0.5 * (cw - fabs(cw));
-  rec[6] = B.s(F_SARHS, n);
-  rec[7] = diag;
+  rec[cnt] = 0.5 * (cv + fabs(cv));
+  rec[2 * cnt] = 0.5 * (cw + fabs(cw));
+  rec[3 * cnt] = 0.5 * (cu - fabs(cu));
+  rec[4 * cnt] = 0.5 * (cv - fabs(cv));
+  rec[5 * cnt] = 0.5 * (cw - fabs(cw));
+  rec[6 * cnt] = B.s(F_SARHS, n);
+  rec[7 * cnt] = diag;
+  const int* nb = B.nbr + 6 * pos;
+  rec[8 * cnt] = pack_nbrs(nb, h > 0 ? B.poff[h - 1] : 0);
+  rec[9 * cnt] = pack_nbrs(nb + 3, h + 1 < B.nplanes ? B.poff[h + 1] : 0);
 }
 
+namespace {
+
+struct SaFwd {
+  double a[3], rhs, diag, packed;
+};
+struct SaBwd {
+  double b[3], diag, packed, dqs;
+  long nat;
+};
+__device__ __forceinline__ void sa_load_fwd(const BlockView& B, int h, int t, SaFwd& f) {
+  const long base = B.poff[h];
+  const int cnt = (int)(B.poff[h + 1] - base);
+  const double* r = B.sa_rec + kSaRec * base + t;
+  f.a[0] = r[0];
+  f.a[1] = r[cnt];
+  f.a[2] = r[2 * cnt];
+  f.rhs = r[6 * cnt];
+  f.diag = r[7 * cnt];
+  f.packed = r[8 * cnt];
+}
+__device__ __forceinline__ void sa_load_bwd(const BlockView& B, int h, int t, SaBwd& f) {
+  const long base = B.poff[h];
+  const int cnt = (int)(B.poff[h + 1] - base);
+  const double* r = B.sa_rec + kSaRec * base + t;
+  f.b[0] = r[3 * cnt];
+  f.b[1] = r[4 * cnt];
+  f.b[2] = r[5 * cnt];
+  f.diag = r[7 * cnt];
+  f.packed = r[9 * cnt];
+  f.dqs = B.sa_dq[base + t];
+  f.nat = B.nat[base + t];
+}
+
+}  // namespace
+
 // Scalar LU-SGS sweeps of the SA equation and nut += dnut, one CTA per block,
-// one thread per node of a hyperplane (sub_tur_sa.f90:759-818).
-__global__ void k_sa_sweep(const BlockView* __restrict__ blocks) {
+// one thread per node of a hyperplane (sub_tur_sa.f90:759-818).  Each thread
+// loads the records of its node of the next plane while it computes the
+// current one, so the plane-to-plane path is the shared-memory neighbours,
+// one division and the barrier.
+__global__ void __launch_bounds__(1024) k_sa_sweep(const BlockView* __restrict__ blocks) {
   const BlockView& B = blocks[blockIdx.x];
   extern __shared__ double sdn[];  // two planes of pmax values
   const int P = B.pmax;
   const int H = B.nplanes;
-  for (int h = 0; h < H; ++h) {
-    long base = B.poff[h];
-    int cnt = (int)(B.poff[h + 1] - base);
-    long pbase = h > 0 ? B.poff[h - 1] : 0;
-    double* prev = sdn + P * ((h + 1) & 1);
-    double* cur = sdn + P * (h & 1);
-    for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
-      long pos = base + t;
-      const double* rec = B.rec_f + kRec * pos;
-      const int* nb = B.nbr + 6 * pos;
-      double tt[3];
+  const int T = blockDim.x, tid = threadIdx.x;
+  auto cnt_of = [&](int h) { return (int)(B.poff[h + 1] - B.poff[h]); };
+  {
+    SaFwd nx{};
+    if (H > 0 && tid < cnt_of(0)) sa_load_fwd(B, 0, tid, nx);
+    for (int h = 0; h < H; ++h) {
+      const SaFwd cu = nx;
+      if (h + 1 < H && tid < cnt_of(h + 1)) sa_load_fwd(B, h + 1, tid, nx);
+      const long base = B.poff[h];
+      const int cnt = (int)(B.poff[h + 1] - base);
+      const double* prev = sdn + P * ((h + 1) & 1);
+      double* cur = sdn + P * (h & 1);
+      for (int t = tid; t < cnt; t += T) {
+        SaFwd f = cu;
+        if (t != tid) sa_load_fwd(B, h, t, f);
+        double tt[3];
 #pragma unroll
-      for (int d = 0; d < 3; ++d) tt[d] = nb[d] < 0 ? 0.0 : rec[d] * prev[nb[d] - pbase];
-      double v = (rec[6] + (tt[0] + tt[1] + tt[2])) / rec[7];
-      cur[t] = v;
-      B.dqs[pos] = v;
+        for (int d = 0; d < 3; ++d) {
+          int w = nbr_local(f.packed, d);
+          tt[d] = w < 0 ? 0.0 : f.a[d] * prev[w];
+        }
+        double v = (f.rhs + (tt[0] + tt[1] + tt[2])) / f.diag;
+        cur[t] = v;
+        B.sa_dq[base + t] = v;
+      }
+      __syncthreads();
     }
-    __syncthreads();
   }
+  SaBwd nx{};
+  if (H > 0 && tid < cnt_of(H - 1)) sa_load_bwd(B, H - 1, tid, nx);
   for (int h = H - 1; h >= 0; --h) {
-    long base = B.poff[h];
-    int cnt = (int)(B.poff[h + 1] - base);
-    long pbase = h + 1 < H ? B.poff[h + 1] : 0;
-    double* prev = sdn + P * ((h + 1) & 1);
+    const SaBwd cu = nx;
+    if (h > 0 && tid < cnt_of(h - 1)) sa_load_bwd(B, h - 1, tid, nx);
+    const long base = B.poff[h];
+    const int cnt = (int)(B.poff[h + 1] - base);
+    const double* prev = sdn + P * ((h + 1) & 1);
     double* cur = sdn + P * (h & 1);
-    for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
-      long pos = base + t;
-      const double* rec = B.rec_f + kRec * pos;
-      const int* nb = B.nbr + 6 * pos + 3;
+    for (int t = tid; t < cnt; t += T) {
+      SaBwd f = cu;
+      if (t != tid) sa_load_bwd(B, h, t, f);
       double tt[3];
 #pragma unroll
-      for (int d = 0; d < 3; ++d) tt[d] = nb[d] < 0 ? 0.0 : rec[3 + d] * prev[nb[d] - pbase];
-      double v = B.dqs[pos] - (tt[0] + tt[1] + tt[2]) / rec[7];
+      for (int d = 0; d < 3; ++d) {
+        int w = nbr_local(f.packed, d);
+        tt[d] = w < 0 ? 0.0 : f.b[d] * prev[w];
+      }
+      double v = f.dqs - (tt[0] + tt[1] + tt[2]) / f.diag;
       cur[t] = v;
-      long n = B.nat[pos];
-      B.s(F_NUT, n) = B.s(F_NUT, n) + v;
+      B.s(F_NUT, f.nat) = B.s(F_NUT, f.nat) + v;
     }
     __syncthreads();
   }
