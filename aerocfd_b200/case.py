@@ -21,6 +21,22 @@ IFLAG_STEADY, IFLAG_UNSTEADY = 0, 1
 IFLAG_1STIMPLICIT, IFLAG_2NDCRANK = 2, 3
 IFLAG_LAMINAR, IFLAG_SA = 0, 2
 IFLAG_3RDWENO = 4
+# Extension schemes: the reference defines these flag values (module_flags.f90:
+# 68, 71) but stops on them (main.f90:636-653); here iflag_inviscid = 5 is
+# Steger-Warming splitting with WENO5 and 8 is WCNS5 with the Roe flux.
+IFLAG_5THWENO, IFLAG_5THWCNS = 5, 8
+SCHEME_NAMES = {IFLAG_3RDWENO: "roe_weno3", IFLAG_5THWENO: "sw_weno5", IFLAG_5THWCNS: "wcns5_roe"}
+
+
+def buffer_length_for(inviscid: int) -> int:
+    """Ghost layers of a block interface for the inviscid scheme: 2 for the
+    3rd-order WENO (GetBufferLength, main.f90:636-653), 3 for the 5th-order
+    extension schemes (their stencils reach three nodes past a face)."""
+    if inviscid == IFLAG_3RDWENO:
+        return 2
+    if inviscid in (IFLAG_5THWENO, IFLAG_5THWCNS):
+        return 3
+    raise ValueError("Buffer length is not correct, please check the iflag_inviscid!")
 BC_INFLOW, BC_OUTFLOW, BC_SYMM, BC_WALL, BC_FARFIELD = -50, -40, -30, -20, -10
 
 # Field table shared with include/aerocfd_gpu.h (AERO_F_*): name, components.
@@ -130,7 +146,6 @@ class Config:
     timeadvance: int = IFLAG_1STIMPLICIT
     turbulence: int = IFLAG_LAMINAR
     des: int = 0
-    buffer_length: int = 2
     inviscid: int = IFLAG_3RDWENO
     ma: float = 0.5
     re: float = 1.0e6
@@ -139,6 +154,11 @@ class Config:
     cfl: float = 5.0
     dt: float = 1.0
     nutinf: float = 1.341946   # module_tursa.f90:11
+
+    @property
+    def buffer_length(self) -> int:
+        """bufferLength, derived from iflag_inviscid as main.f90:81 does."""
+        return buffer_length_for(self.inviscid)
 
     def iflags(self) -> np.ndarray:
         return np.array([self.dimension, self.solver, self.time, self.timeadvance,

@@ -45,6 +45,7 @@ struct CaseConsts {
   double gamma, cv, re, tinf, prl, prt, cfl;
   double d_0, u_0, p_0, c_0, aoa, nutinf;
   int dimension, solver, time, turbulence, des, bufferLength;
+  int inviscid;  // iflag_inviscid: 4 Roe + WENO3, 5 Steger-Warming + WENO5, 8 WCNS5 + Roe
 };
 
 // Everything a kernel needs to address one block's fields.
@@ -89,6 +90,7 @@ constexpr int kSaRec = 10;
 // Three plane-local indices (+1; 0 = no neighbour) in one 64-bit word: the
 // neighbours' positions in their hyperplane relative to its first node.
 constexpr int kNbrBits = 21;
+#ifdef __CUDACC__
 __device__ __forceinline__ double pack_nbrs(const int* nb, long prev_base) {
   unsigned long long u = 0;
 #pragma unroll
@@ -102,6 +104,7 @@ __device__ __forceinline__ int nbr_local(double packed, int e) {
   unsigned long long u = (unsigned long long)__double_as_longlong(packed);
   return (int)((u >> (kNbrBits * e)) & ((1ull << kNbrBits) - 1)) - 1;
 }
+#endif
 
 
 // ---------------------------------------------------------------- arithmetic
@@ -147,6 +150,7 @@ enum {
   IFLAG_2D = 2, IFLAG_3D = 3, IFLAG_NSSOLVER = 0, IFLAG_EULERSOLVER = 1,
   IFLAG_STEADY = 0, IFLAG_UNSTEADY = 1, IFLAG_LAMINAR = 0, IFLAG_SA = 2,
   IFLAG_1STIMPLICIT = 2, IFLAG_2NDCRANK = 3,
+  IFLAG_3RDWENO = 4, IFLAG_5THWENO = 5, IFLAG_5THWCNS = 8,
   IFLAG_DES97 = 1, IFLAG_DDES = 2,
   BC_INFLOW = -50, BC_OUTFLOW = -40, BC_SYMM = -30, BC_WALL = -20, BC_FARFIELD = -10,
 };

@@ -376,6 +376,219 @@ __global__ void k_inviscid_combine(const BlockView* __restrict__ blocks, CaseCon
   }
 }
 
+// ------------------------------------------- extension inviscid schemes
+// The reference defines iflag_5thweno = 5 and iflag_5thwcns = 8
+// (module_flags.f90:68, 71) but has no code for them (GetBufferLength stops on
+// any scheme but the 3rd-order WENO, main.f90:636-653).  These are the
+// published methods, on three ghost layers, in FP64:
+//  * 5: Steger-Warming flux-vector splitting (J. Comput. Phys. 40, 1981) of
+//    the contravariant flux at the nodes, the split fluxes reconstructed at
+//    the faces with the WENO5 of Jiang & Shu (J. Comput. Phys. 126, 1996);
+//  * 8: WCNS5 (Deng & Zhang, J. Comput. Phys. 165, 2000): 5th-order weighted
+//    nonlinear interpolation of the conservative variables to the faces
+//    (linear weights 1/16, 10/16, 5/16, Jiang-Shu smoothness indicators), the
+//    reference's Roe flux there, and the 4th-order hybrid face/node
+//    difference F'_i = 4/3 (F_i+1/2 - F_i-1/2) - 1/6 (F_i+1 - F_i-1), written
+//    as the face flux G = 4/3 F_i+1/2 - (F_i + F_i+1)/6 so that the combine
+//    kernel's difference applies.  For uniform flow G equals the reference's
+//    face flux, so freestream preservation is the reference scheme's.
+// Near a physical boundary, where a stencil would leave the box, the WENO5
+// reconstructions drop to WENO3 and then 1st order, and WCNS5 uses the
+// reference's WENO3 + Roe face.
+namespace {
+
+constexpr double kEps5 = 1.0e-6;
+
+// WENO5 value at the right edge of v2 from v0..v4 (Jiang & Shu).
+__device__ __forceinline__ double weno5_edge(double v0, double v1, double v2, double v3, double v4) {
+  double b0 = 13.0 / 12.0 * p2(v0 - 2.0 * v1 + v2) + 0.25 * p2(v0 - 4.0 * v1 + 3.0 * v2);
+  double b1 = 13.0 / 12.0 * p2(v1 - 2.0 * v2 + v3) + 0.25 * p2(v1 - v3);
+  double b2 = 13.0 / 12.0 * p2(v2 - 2.0 * v3 + v4) + 0.25 * p2(3.0 * v2 - 4.0 * v3 + v4);
+  double a0 = 0.1 / p2(kEps5 + b0);
+  double a1 = 0.6 / p2(kEps5 + b1);
+  double a2 = 0.3 / p2(kEps5 + b2);
+  double q0 = (2.0 * v0 - 7.0 * v1 + 11.0 * v2) / 6.0;
+  double q1 = (-v1 + 5.0 * v2 + 2.0 * v3) / 6.0;
+  double q2 = (2.0 * v2 + 5.0 * v3 - v4) / 6.0;
+  return (a0 * q0 + a1 * q1 + a2 * q2) / (a0 + a1 + a2);
+}
+// WENO3 value at the right edge of v1 from v0..v2 (Jiang & Shu).
+__device__ __forceinline__ double weno3_edge(double v0, double v1, double v2) {
+  double b0 = p2(v1 - v0);
+  double b1 = p2(v2 - v1);
+  double a0 = (1.0 / 3.0) / p2(kEps5 + b0);
+  double a1 = (2.0 / 3.0) / p2(kEps5 + b1);
+  double q0 = (3.0 * v1 - v0) / 2.0;
+  double q1 = (v1 + v2) / 2.0;
+  return (a0 * q0 + a1 * q1) / (a0 + a1);
+}
+// WCNS5 interpolation at the right edge of v2 from v0..v4 (Deng & Zhang).
+__device__ __forceinline__ double wcns5_edge(double v0, double v1, double v2, double v3, double v4) {
+  double b0 = 13.0 / 12.0 * p2(v0 - 2.0 * v1 + v2) + 0.25 * p2(v0 - 4.0 * v1 + 3.0 * v2);
+  double b1 = 13.0 / 12.0 * p2(v1 - 2.0 * v2 + v3) + 0.25 * p2(v1 - v3);
+  double b2 = 13.0 / 12.0 * p2(v2 - 2.0 * v3 + v4) + 0.25 * p2(3.0 * v2 - 4.0 * v3 + v4);
+  double a0 = 0.0625 / p2(kEps5 + b0);
+  double a1 = 0.625 / p2(kEps5 + b1);
+  double a2 = 0.3125 / p2(kEps5 + b2);
+  double q0 = (3.0 * v0 - 10.0 * v1 + 15.0 * v2) / 8.0;
+  double q1 = (-v1 + 6.0 * v2 + 3.0 * v3) / 8.0;
+  double q2 = (3.0 * v2 + 6.0 * v3 - v4) / 8.0;
+  return (a0 * q0 + a1 * q1 + a2 * q2) / (a0 + a1 + a2);
+}
+
+// Steger-Warming part of the contravariant flux along `coord` at node n
+// (metric K = grad xi * inv_j): PLUS takes the eigenvalues' positive parts,
+// otherwise the negative parts.
+template <bool PLUS>
+__device__ __forceinline__ void sw_part(const BlockView& B, int coord, long n, double gamma, double f[5]) {
+  double rho = B.v(F_Q, 1, n);
+  double u = B.v(F_Q, 2, n) / rho, v = B.v(F_Q, 3, n) / rho, w = B.v(F_Q, 4, n) / rho;
+  double q2 = 0.5 * (u * u + v * v + w * w);
+  double p = (B.v(F_Q, 5, n) - rho * q2) * (gamma - 1.0);
+  double c = sqrt(gamma * p / rho);
+  const int c1 = 3 * coord - 2;
+  double ij = B.s(F_INVJ, n);
+  double kx = B.v(F_DXIDX, c1, n) * ij, ky = B.v(F_DXIDX, c1 + 1, n) * ij, kz = B.v(F_DXIDX, c1 + 2, n) * ij;
+  double kn = sqrt(kx * kx + ky * ky + kz * kz);
+  double nx = kx / kn, ny = ky / kn, nz = kz / kn;
+  double uu = kx * u + ky * v + kz * w;
+  double ub = nx * u + ny * v + nz * w;
+  double l1 = uu, l4 = uu + c * kn, l5 = uu - c * kn;
+  if (PLUS) {
+    l1 = 0.5 * (l1 + fabs(l1));
+    l4 = 0.5 * (l4 + fabs(l4));
+    l5 = 0.5 * (l5 + fabs(l5));
+  } else {
+    l1 = 0.5 * (l1 - fabs(l1));
+    l4 = 0.5 * (l4 - fabs(l4));
+    l5 = 0.5 * (l5 - fabs(l5));
+  }
+  double h = c * c / (gamma - 1.0) + q2;
+  double coef = rho / (2.0 * gamma);
+  double a1 = 2.0 * (gamma - 1.0) * l1;
+  f[0] = coef * (a1 + l4 + l5);
+  f[1] = coef * (a1 * u + l4 * (u + c * nx) + l5 * (u - c * nx));
+  f[2] = coef * (a1 * v + l4 * (v + c * ny) + l5 * (v - c * ny));
+  f[3] = coef * (a1 * w + l4 * (w + c * nz) + l5 * (w - c * nz));
+  f[4] = coef * (a1 * q2 + l4 * (h + c * ub) + l5 * (h - c * ub));
+}
+
+// Contravariant flux along `coord` at node n with the node's metric, the
+// left-state expressions of roe_face.
+__device__ __forceinline__ void node_flux(const BlockView& B, int coord, long n, double gamma, double f[5]) {
+  double d = B.v(F_Q, 1, n);
+  double u = B.v(F_Q, 2, n) / d, v = B.v(F_Q, 3, n) / d, w = B.v(F_Q, 4, n) / d;
+  double p = (B.v(F_Q, 5, n) - 0.5 * (p2(B.v(F_Q, 2, n)) + p2(B.v(F_Q, 3, n)) + p2(B.v(F_Q, 4, n))) / d) *
+             (gamma - 1.0);
+  const int c1 = 3 * coord - 2;
+  double ij = B.s(F_INVJ, n);
+  double kx = B.v(F_DXIDX, c1, n) * ij, ky = B.v(F_DXIDX, c1 + 1, n) * ij, kz = B.v(F_DXIDX, c1 + 2, n) * ij;
+  double h = gamma * p / ((gamma - 1.0) * d) + 0.5 * (p2(u) + p2(v) + p2(w));
+  double uu = u * kx + v * ky + w * kz;
+  f[0] = d * uu;
+  f[1] = d * u * uu + kx * p;
+  f[2] = d * v * uu + ky * p;
+  f[3] = d * w * uu + kz * p;
+  f[4] = d * h * uu;
+}
+
+// The face pos+1/2 of node n along direction d (blockIdx.z) for every n of the
+// updated box grown by one node down in d, as faces_body: the geometry of one
+// thread.
+struct FaceAt {
+  long n, st;
+  int pos, lo, hi;
+};
+__device__ __forceinline__ bool face_at(const BlockView& B, int d, FaceAt& F) {
+  Box e = B.b1;
+  if (d == 0) e.is -= 1; else if (d == 1) e.js -= 1; else e.ks -= 1;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= e.size()) return false;
+  int i = e.is + (int)(t % e.nx());
+  long r = t / e.nx();
+  int j = e.js + (int)(r % e.ny());
+  int k = e.ks + (int)(r / e.ny());
+  F.n = B.at(i, j, k);
+  F.st = d == 0 ? 1 : (d == 1 ? (long)B.nx : (long)B.nx * B.ny);
+  F.pos = d == 0 ? i : (d == 1 ? j : k);
+  F.lo = d == 0 ? B.b.is : (d == 1 ? B.b.js : B.b.ks);
+  F.hi = d == 0 ? B.b.ie : (d == 1 ? B.b.je : B.b.ke);
+  return true;
+}
+
+}  // namespace
+
+// Steger-Warming + WENO5 face fluxes into FVH planes 5*d + c (then
+// k_inviscid_combine).  F+ at pos+1/2 from nodes pos-2..pos+2, F- from
+// pos-1..pos+3.
+__global__ void k_faces_sw_weno5(const BlockView* __restrict__ blocks, CaseConsts cc) {
+  const BlockView& B = blocks[blockIdx.y];
+  const int d = blockIdx.z;
+  FaceAt F;
+  if (!face_at(B, d, F)) return;
+  const int pos = F.pos, lo = F.lo, hi = F.hi;
+  const long n = F.n, st = F.st;
+  double out[5];
+  {
+    double v[5][5] = {};  // F+ at pos-2..pos+2 (those inside the box)
+#pragma unroll
+    for (int x = 0; x < 5; ++x)
+      if (pos - 2 + x >= lo && pos - 2 + x <= hi) sw_part<true>(B, d + 1, n + (x - 2) * st, cc.gamma, v[x]);
+    const bool five = pos - 2 >= lo && pos + 2 <= hi, three = pos - 1 >= lo && pos + 1 <= hi;
+#pragma unroll
+    for (int c = 0; c < 5; ++c)
+      out[c] = five ? weno5_edge(v[0][c], v[1][c], v[2][c], v[3][c], v[4][c])
+                    : (three ? weno3_edge(v[1][c], v[2][c], v[3][c]) : v[2][c]);
+  }
+  {
+    double v[5][5] = {};  // F- at pos-1..pos+3
+#pragma unroll
+    for (int x = 0; x < 5; ++x)
+      if (pos - 1 + x >= lo && pos - 1 + x <= hi) sw_part<false>(B, d + 1, n + (x - 1) * st, cc.gamma, v[x]);
+    const bool five = pos - 1 >= lo && pos + 3 <= hi, three = pos >= lo && pos + 2 <= hi;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      double fm = five ? weno5_edge(v[4][c], v[3][c], v[2][c], v[1][c], v[0][c])
+                       : (three ? weno3_edge(v[3][c], v[2][c], v[1][c]) : v[2][c]);
+      out[c] = out[c] + fm;
+    }
+  }
+  double* o = B.f[F_FVH] + (long)(5 * d) * B.plane + n;
+#pragma unroll
+  for (int c = 0; c < 5; ++c) o[(long)c * B.plane] = out[c];
+}
+
+// WCNS5 face fluxes G into FVH planes 5*d + c (then k_inviscid_combine).
+__global__ void k_faces_wcns5(const BlockView* __restrict__ blocks, CaseConsts cc) {
+  const BlockView& B = blocks[blockIdx.y];
+  const int d = blockIdx.z;
+  FaceAt F;
+  if (!face_at(B, d, F)) return;
+  const int pos = F.pos;
+  const long n = F.n, st = F.st;
+  double out[5];
+  if (pos - 2 >= F.lo && pos + 3 <= F.hi) {
+    double ul[5], ur[5], fh[5], fa[5], fb[5];
+#pragma unroll
+    for (int c = 1; c <= 5; ++c) {
+      double u0 = B.v(F_Q, c, n - 2 * st), u1 = B.v(F_Q, c, n - st), u2 = B.v(F_Q, c, n);
+      double u3 = B.v(F_Q, c, n + st), u4 = B.v(F_Q, c, n + 2 * st), u5 = B.v(F_Q, c, n + 3 * st);
+      ul[c - 1] = wcns5_edge(u0, u1, u2, u3, u4);
+      ur[c - 1] = wcns5_edge(u5, u4, u3, u2, u1);
+    }
+    roe_face(B, d + 1, n, n + st, ul, ur, cc.gamma, fh);
+    node_flux(B, d + 1, n, cc.gamma, fa);
+    node_flux(B, d + 1, n + st, cc.gamma, fb);
+#pragma unroll
+    for (int c = 0; c < 5; ++c) out[c] = 4.0 / 3.0 * fh[c] - (fa[c] + fb[c]) / 6.0;
+  } else {
+    face_flux(B, d + 1, n, pos, F.lo, F.hi, st, cc.gamma, out);
+  }
+  double* o = B.f[F_FVH] + (long)(5 * d) * B.plane + n;
+#pragma unroll
+  for (int c = 0; c < 5; ++c) o[(long)c * B.plane] = out[c];
+}
+
 // Zero-fills one field over the full box of every block (the reference's
 // `rhsi = 0.d0`, sub_inviscid1.f90:40, and similar whole-array assignments).
 __global__ void k_fill(const BlockView* __restrict__ blocks, int fid, int nc, double val) {

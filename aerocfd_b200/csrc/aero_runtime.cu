@@ -444,7 +444,14 @@ int launch_inviscid(const BlockView* views, int nblk, long maxN, long maxN1, lon
   PROF(P_FILL, (k_fill<<<dim3(cdiv(maxN, g.tune.ew), nblk), g.tune.ew, 0, g.stream>>>(views, F_RHSI, 5, 0.0)));
   CKL();
   const int tile = g.tune.inv_tile;
-  if (tile == 0) {  // face-based: each face once, then the combine
+  if (cc.inviscid == IFLAG_5THWENO || cc.inviscid == IFLAG_5THWCNS) {
+    // extension schemes (FP64 in both precision modes): faces, then the combine
+    long maxF = maxN1 + maxFace;
+    auto faces = cc.inviscid == IFLAG_5THWENO ? k_faces_sw_weno5 : k_faces_wcns5;
+    PROF(P_INVISCID, (faces<<<dim3(cdiv(maxF, 128), nblk, 3), 128, 0, g.stream>>>(views, cc)));
+    CKL();
+    PROF(P_INVISCID, (k_inviscid_combine<<<dim3(cdiv(maxN1, g.tune.ew), nblk), g.tune.ew, 0, g.stream>>>(views, cc)));
+  } else if (tile == 0) {  // face-based: each face once, then the combine
     // faces per direction <= updated box grown by one node in that direction
     long maxF = maxN1 + maxFace;
     PROF(P_INVISCID, ((g.mixed ? k_inviscid_faces_mixed : k_inviscid_faces)<<<dim3(cdiv(maxF, 128), nblk, 3), 128, 0,
@@ -722,6 +729,7 @@ CaseConsts consts_from(const int* iflags, const double* params) {
   c.aoa = params[3] * pi / 180.0;
   c.dimension = iflags[0]; c.solver = iflags[1]; c.time = iflags[2];
   c.turbulence = iflags[4]; c.des = iflags[5]; c.bufferLength = iflags[6];
+  c.inviscid = iflags[7];
   return c;
 }
 
@@ -1039,8 +1047,12 @@ int aero_configure(const int* iflags, const double* params) {
                 "unsteady 2nd-order Crank-Nicolson (1/3)", iflags[2], iflags[3]);
   if (iflags[4] != IFLAG_LAMINAR && iflags[4] != IFLAG_SA)
     return fail(AERO_ERR_ARG, "Wrong turbulence model type is input!!! (%d)", iflags[4]);
-  if (iflags[6] != 2 || iflags[7] != 4)
-    return fail(AERO_ERR_ARG, "bufferLength=%d/iflag_inviscid=%d: only the 3rd-order WENO (2 layers)", iflags[6], iflags[7]);
+  const bool scheme_ok = (iflags[7] == IFLAG_3RDWENO && iflags[6] == 2) ||
+                         ((iflags[7] == IFLAG_5THWENO || iflags[7] == IFLAG_5THWCNS) && iflags[6] == 3);
+  if (!scheme_ok)
+    return fail(AERO_ERR_ARG,
+                "bufferLength=%d/iflag_inviscid=%d: supported are the 3rd-order WENO with 2 layers and "
+                "WENO5 (5) or WCNS5 (8) with 3", iflags[6], iflags[7]);
   if (iflags[5] != 0) return fail(AERO_ERR_ARG, "iflag_des=%d: DES97/DDES are not supported on the GPU", iflags[5]);
   std::memcpy(g.iflags, iflags, sizeof g.iflags);
   std::memcpy(g.params, params, sizeof g.params);
@@ -1294,9 +1306,47 @@ int aero_inviscid_flux_1(double* rhsi, const double* q, const double* dxidx, con
   BlockTarget t;
   if ((rc = resolve(b, b0, b1, args, t))) return rc;
   CaseConsts cc = consts_with(*gamma, g.cc.cv, g.cc.re);
+  cc.inviscid = IFLAG_3RDWENO;  // this routine is the reference's Roe + WENO3 flux
   long maxFace = std::max({(long)b1.ny() * b1.nz(), (long)b1.nx() * b1.nz(), (long)b1.nx() * b1.ny()});
   if ((rc = launch_inviscid(t.d_view, 1, b.size(), b1.size(), maxFace, cc))) return rc;
   return finish(t, args);
+}
+
+// The extension schemes with inviscid_flux_1's argument list (no counterpart
+// in the reference): scheme IFLAG_5THWENO or IFLAG_5THWCNS.
+static int inviscid_ext(int scheme, double* rhsi, const double* q, const double* dxidx, const double* inv_j,
+                        const int* is, const int* ie, const int* js, const int* je, const int* ks, const int* ke,
+                        const int* is0, const int* ie0, const int* js0, const int* je0, const int* ks0,
+                        const int* ke0, const int* is1, const int* ie1, const int* js1, const int* je1,
+                        const int* ks1, const int* ke1, const double* gamma) {
+  int rc = need_init();
+  if (rc) return rc;
+  Box b = box_of(is, ie, js, je, ks, ke), b0 = box_of(is0, ie0, js0, je0, ks0, ke0),
+      b1 = box_of(is1, ie1, js1, je1, ks1, ke1);
+  std::vector<Arg> args = {{F_Q, q, false}, {F_DXIDX, dxidx, false}, {F_INVJ, inv_j, false}, {F_RHSI, rhsi, true}};
+  BlockTarget t;
+  if ((rc = resolve(b, b0, b1, args, t))) return rc;
+  CaseConsts cc = consts_with(*gamma, g.cc.cv, g.cc.re);
+  cc.inviscid = scheme;
+  long maxFace = std::max({(long)b1.ny() * b1.nz(), (long)b1.nx() * b1.nz(), (long)b1.nx() * b1.ny()});
+  if ((rc = launch_inviscid(t.d_view, 1, b.size(), b1.size(), maxFace, cc))) return rc;
+  return finish(t, args);
+}
+int aero_inviscid_flux_weno5(double* rhsi, const double* q, const double* dxidx, const double* inv_j,
+                             const int* is, const int* ie, const int* js, const int* je, const int* ks,
+                             const int* ke, const int* is0, const int* ie0, const int* js0, const int* je0,
+                             const int* ks0, const int* ke0, const int* is1, const int* ie1, const int* js1,
+                             const int* je1, const int* ks1, const int* ke1, const double* gamma) {
+  return inviscid_ext(IFLAG_5THWENO, rhsi, q, dxidx, inv_j, is, ie, js, je, ks, ke, is0, ie0, js0, je0, ks0,
+                      ke0, is1, ie1, js1, je1, ks1, ke1, gamma);
+}
+int aero_inviscid_flux_wcns5(double* rhsi, const double* q, const double* dxidx, const double* inv_j,
+                             const int* is, const int* ie, const int* js, const int* je, const int* ks,
+                             const int* ke, const int* is0, const int* ie0, const int* js0, const int* je0,
+                             const int* ks0, const int* ke0, const int* is1, const int* ie1, const int* js1,
+                             const int* je1, const int* ks1, const int* ke1, const double* gamma) {
+  return inviscid_ext(IFLAG_5THWCNS, rhsi, q, dxidx, inv_j, is, ie, js, je, ks, ke, is0, ie0, js0, je0, ks0,
+                      ke0, is1, ie1, js1, je1, ks1, ke1, gamma);
 }
 
 int aero_viscous_flux(double* rhsv, const double* pri_v, double* amu, double* vor, double* dudx,

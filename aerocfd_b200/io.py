@@ -29,7 +29,7 @@ from typing import Iterator, List, Sequence, Tuple
 
 import numpy as np
 
-from .case import Block, Case, Config, Subface, IFLAG_3D
+from .case import Block, Case, Config, Subface, IFLAG_3D, buffer_length_for
 
 _TOKEN = re.compile(r"'[^']*'|\"[^\"]*\"|[^\s,]+")
 
@@ -138,12 +138,12 @@ class Control:
         ("restartfile", str), ("nfile", int), ("restart_timestep", int))
 
     def config(self, nutinf: float = 1.341946) -> Config:
-        """The library's Config (bufferLength from GetBufferLength, main.f90:636-653)."""
-        if self.iflag_inviscid != 4:
-            raise ValueError("Buffer length is not correct, please check the iflag_inviscid!")
+        """The library's Config (bufferLength from iflag_inviscid, as GetBufferLength,
+        main.f90:636-653, does for the 3rd-order WENO)."""
+        buffer_length_for(self.iflag_inviscid)  # rejects what the reference rejects
         return Config(dimension=self.iflag_dimension, solver=self.iflag_solver, time=self.iflag_time,
                       timeadvance=self.iflag_timeadvance, turbulence=self.iflag_turbulence, des=self.iflag_des,
-                      buffer_length=2, inviscid=self.iflag_inviscid, ma=self.ma, re=self.re, tinf=self.tinf,
+                      inviscid=self.iflag_inviscid, ma=self.ma, re=self.re, tinf=self.tinf,
                       aoa_deg=self.aoa, cfl=self.cfl, dt=self.dt, nutinf=nutinf)
 
 

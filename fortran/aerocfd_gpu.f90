@@ -98,6 +98,12 @@ module aerocfd_gpu
       integer(c_int) :: zones(*)
     end function
 
+    ! CTAs per block of the LU-SGS sweep: 1, 2, 4 or 8 (no counterpart in the reference)
+    integer(c_int) function aero_set_sweep_cluster(ctas) bind(C, name="aero_set_sweep_cluster")
+      import :: c_int
+      integer(c_int), value :: ctas
+    end function
+
     integer(c_int) function aero_finish_setup() bind(C, name="aero_finish_setup")
       import :: c_int
     end function
@@ -123,6 +129,24 @@ module aerocfd_gpu
     ! sub_inviscid1.f90:8
     integer(c_int) function aero_inviscid_flux_1(rhsi, q, dxidx, inv_j, is, ie, js, je, ks, ke, &
         is0, ie0, js0, je0, ks0, ke0, is1, ie1, js1, je1, ks1, ke1, gamma) bind(C, name="aero_inviscid_flux_1")
+      import :: c_int, c_double
+      integer(c_int) :: is, ie, js, je, ks, ke, is0, ie0, js0, je0, ks0, ke0, is1, ie1, js1, je1, ks1, ke1
+      real(c_double) :: rhsi(5, is:ie, js:je, ks:ke), q(5, is:ie, js:je, ks:ke)
+      real(c_double) :: dxidx(9, is:ie, js:je, ks:ke), inv_j(is:ie, js:je, ks:ke), gamma
+    end function
+
+    ! Steger-Warming splitting + WENO5 (no counterpart in the reference: iflag_inviscid = 5, bufferLength = 3)
+    integer(c_int) function aero_inviscid_flux_weno5(rhsi, q, dxidx, inv_j, is, ie, js, je, ks, ke, &
+        is0, ie0, js0, je0, ks0, ke0, is1, ie1, js1, je1, ks1, ke1, gamma) bind(C, name="aero_inviscid_flux_weno5")
+      import :: c_int, c_double
+      integer(c_int) :: is, ie, js, je, ks, ke, is0, ie0, js0, je0, ks0, ke0, is1, ie1, js1, je1, ks1, ke1
+      real(c_double) :: rhsi(5, is:ie, js:je, ks:ke), q(5, is:ie, js:je, ks:ke)
+      real(c_double) :: dxidx(9, is:ie, js:je, ks:ke), inv_j(is:ie, js:je, ks:ke), gamma
+    end function
+
+    ! WCNS5 + Roe flux (no counterpart in the reference: iflag_inviscid = 8, bufferLength = 3)
+    integer(c_int) function aero_inviscid_flux_wcns5(rhsi, q, dxidx, inv_j, is, ie, js, je, ks, ke, &
+        is0, ie0, js0, je0, ks0, ke0, is1, ie1, js1, je1, ks1, ke1, gamma) bind(C, name="aero_inviscid_flux_wcns5")
       import :: c_int, c_double
       integer(c_int) :: is, ie, js, je, ks, ke, is0, ie0, js0, je0, ks0, ke0, is1, ie1, js1, je1, ks1, ke1
       real(c_double) :: rhsi(5, is:ie, js:je, ks:ke), q(5, is:ie, js:je, ks:ke)

@@ -132,6 +132,26 @@ int aero_inviscid_flux_1(double* rhsi, const double* q, const double* dxidx, con
                          const int* js0, const int* je0, const int* ks0, const int* ke0,
                          const int* is1, const int* ie1, const int* js1, const int* je1,
                          const int* ks1, const int* ke1, const double* gamma);
+/* Extension schemes with inviscid_flux_1's argument list (no counterpart in
+ * the reference, which defines iflag_inviscid = 5 and 8 in module_flags.f90:68,
+ * 71 but stops on them in GetBufferLength, main.f90:636-653): Steger-Warming
+ * flux-vector splitting with WENO5 reconstruction, and WCNS5 interpolation with
+ * the Roe flux and a 4th-order hybrid face/node difference.  Both need three
+ * ghost layers at block interfaces (bufferLength = 3); near physical
+ * boundaries they fall back to lower-order stencils.  aero_configure with
+ * iflag_inviscid = 5 or 8 and bufferLength = 3 makes aero_step use them. */
+int aero_inviscid_flux_weno5(double* rhsi, const double* q, const double* dxidx, const double* inv_j,
+                             const int* is, const int* ie, const int* js, const int* je,
+                             const int* ks, const int* ke, const int* is0, const int* ie0,
+                             const int* js0, const int* je0, const int* ks0, const int* ke0,
+                             const int* is1, const int* ie1, const int* js1, const int* je1,
+                             const int* ks1, const int* ke1, const double* gamma);
+int aero_inviscid_flux_wcns5(double* rhsi, const double* q, const double* dxidx, const double* inv_j,
+                             const int* is, const int* ie, const int* js, const int* je,
+                             const int* ks, const int* ke, const int* is0, const int* ie0,
+                             const int* js0, const int* je0, const int* ks0, const int* ke0,
+                             const int* is1, const int* ie1, const int* js1, const int* je1,
+                             const int* ks1, const int* ke1, const double* gamma);
 /* sub_viscous.f90:9-12 */
 int aero_viscous_flux(double* rhsv, const double* pri_v, double* amu, double* vor, double* dudx,
                       double* tao, const double* dxidx, const double* inv_j, const double* tinf,

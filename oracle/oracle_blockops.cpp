@@ -220,6 +220,207 @@ void inviscid_flux_1(V rhsi, V q, V dxidx, V inv_j, const Box& b, const Box& b0,
   }
 }
 
+// ------------------------------------------- extension inviscid schemes
+// iflag_inviscid = 5 (Steger-Warming splitting + WENO5) and 8 (WCNS5 + Roe):
+// flag values of the reference (module_flags.f90:68, 71) that it stops on
+// (main.f90:636-653), so there is no reference code to follow.  Restated from
+// the published methods: Steger & Warming, J. Comput. Phys. 40 (1981) 263;
+// Jiang & Shu, J. Comput. Phys. 126 (1996) 202; Deng & Zhang, J. Comput.
+// Phys. 165 (2000) 22.  Three ghost layers at interfaces; near a physical
+// boundary WENO5 drops to WENO3 and then 1st order, and WCNS5 to the
+// reference's WENO3 + Roe face.  The WCNS5 face flux is
+// G = 4/3 F(i+1/2) - (F(i) + F(i+1))/6 with node fluxes F(i), the 4th-order
+// hybrid face/node difference in conservative form.
+namespace {
+
+const double kEps5 = 1.0e-6;
+
+double w5_edge(double v0, double v1, double v2, double v3, double v4) {
+  double b0 = 13.0 / 12.0 * p2(v0 - 2.0 * v1 + v2) + 0.25 * p2(v0 - 4.0 * v1 + 3.0 * v2);
+  double b1 = 13.0 / 12.0 * p2(v1 - 2.0 * v2 + v3) + 0.25 * p2(v1 - v3);
+  double b2 = 13.0 / 12.0 * p2(v2 - 2.0 * v3 + v4) + 0.25 * p2(3.0 * v2 - 4.0 * v3 + v4);
+  double a0 = 0.1 / p2(kEps5 + b0), a1 = 0.6 / p2(kEps5 + b1), a2 = 0.3 / p2(kEps5 + b2);
+  double q0 = (2.0 * v0 - 7.0 * v1 + 11.0 * v2) / 6.0;
+  double q1 = (-v1 + 5.0 * v2 + 2.0 * v3) / 6.0;
+  double q2 = (2.0 * v2 + 5.0 * v3 - v4) / 6.0;
+  return (a0 * q0 + a1 * q1 + a2 * q2) / (a0 + a1 + a2);
+}
+
+double w3_edge(double v0, double v1, double v2) {
+  double b0 = p2(v1 - v0), b1 = p2(v2 - v1);
+  double a0 = (1.0 / 3.0) / p2(kEps5 + b0), a1 = (2.0 / 3.0) / p2(kEps5 + b1);
+  double q0 = (3.0 * v1 - v0) / 2.0, q1 = (v1 + v2) / 2.0;
+  return (a0 * q0 + a1 * q1) / (a0 + a1);
+}
+
+double c5_edge(double v0, double v1, double v2, double v3, double v4) {
+  double b0 = 13.0 / 12.0 * p2(v0 - 2.0 * v1 + v2) + 0.25 * p2(v0 - 4.0 * v1 + 3.0 * v2);
+  double b1 = 13.0 / 12.0 * p2(v1 - 2.0 * v2 + v3) + 0.25 * p2(v1 - v3);
+  double b2 = 13.0 / 12.0 * p2(v2 - 2.0 * v3 + v4) + 0.25 * p2(3.0 * v2 - 4.0 * v3 + v4);
+  double a0 = 0.0625 / p2(kEps5 + b0), a1 = 0.625 / p2(kEps5 + b1), a2 = 0.3125 / p2(kEps5 + b2);
+  double q0 = (3.0 * v0 - 10.0 * v1 + 15.0 * v2) / 8.0;
+  double q1 = (-v1 + 6.0 * v2 + 3.0 * v3) / 8.0;
+  double q2 = (3.0 * v2 + 6.0 * v3 - v4) / 8.0;
+  return (a0 * q0 + a1 * q1 + a2 * q2) / (a0 + a1 + a2);
+}
+
+// Steger-Warming split contravariant flux (positive or negative eigenvalue
+// parts) at node (i,j,k) along coord, metric K = grad xi * inv_j.
+void sw_flux(bool plus, V q, V dxidx, V inv_j, int coord, int i, int j, int k, double gamma, double f[5]) {
+  double rho = q(1, i, j, k);
+  double u = q(2, i, j, k) / rho, v = q(3, i, j, k) / rho, w = q(4, i, j, k) / rho;
+  double q2 = 0.5 * (u * u + v * v + w * w);
+  double p = (q(5, i, j, k) - rho * q2) * (gamma - 1.0);
+  double c = std::sqrt(gamma * p / rho);
+  int c1 = 3 * coord - 2;
+  double ij = inv_j(i, j, k);
+  double kx = dxidx(c1, i, j, k) * ij, ky = dxidx(c1 + 1, i, j, k) * ij, kz = dxidx(c1 + 2, i, j, k) * ij;
+  double kn = std::sqrt(kx * kx + ky * ky + kz * kz);
+  double nx = kx / kn, ny = ky / kn, nz = kz / kn;
+  double uu = kx * u + ky * v + kz * w;
+  double ub = nx * u + ny * v + nz * w;
+  double lam[3] = {uu, uu + c * kn, uu - c * kn};
+  for (double& l : lam) l = plus ? 0.5 * (l + std::fabs(l)) : 0.5 * (l - std::fabs(l));
+  double h = c * c / (gamma - 1.0) + q2;
+  double coef = rho / (2.0 * gamma);
+  double a1 = 2.0 * (gamma - 1.0) * lam[0];
+  f[0] = coef * (a1 + lam[1] + lam[2]);
+  f[1] = coef * (a1 * u + lam[1] * (u + c * nx) + lam[2] * (u - c * nx));
+  f[2] = coef * (a1 * v + lam[1] * (v + c * ny) + lam[2] * (v - c * ny));
+  f[3] = coef * (a1 * w + lam[1] * (w + c * nz) + lam[2] * (w - c * nz));
+  f[4] = coef * (a1 * q2 + lam[1] * (h + c * ub) + lam[2] * (h - c * ub));
+}
+
+// Physical contravariant flux at node (i,j,k) with its own metric.
+void phys_flux(V q, V dxidx, V inv_j, int coord, int i, int j, int k, double gamma, double f[5]) {
+  double d = q(1, i, j, k);
+  double u = q(2, i, j, k) / d, v = q(3, i, j, k) / d, w = q(4, i, j, k) / d;
+  double p = (q(5, i, j, k) - 0.5 * (p2(q(2, i, j, k)) + p2(q(3, i, j, k)) + p2(q(4, i, j, k))) / d) *
+             (gamma - 1.0);
+  int c1 = 3 * coord - 2;
+  double ij = inv_j(i, j, k);
+  double kx = dxidx(c1, i, j, k) * ij, ky = dxidx(c1 + 1, i, j, k) * ij, kz = dxidx(c1 + 2, i, j, k) * ij;
+  double h = gamma * p / ((gamma - 1.0) * d) + 0.5 * (p2(u) + p2(v) + p2(w));
+  double uu = u * kx + v * ky + w * kz;
+  f[0] = d * uu;
+  f[1] = d * u * uu + kx * p;
+  f[2] = d * v * uu + ky * p;
+  f[3] = d * w * uu + kz * p;
+  f[4] = d * h * uu;
+}
+
+// rhsi from face fluxes flux(i) = F(i+1/2) along coord, as sub_inviscid1.f90:82-88.
+void difference_faces(V rhsi, Tmp& flux, const Box& b1, int coord) {
+  int di = coord == 1, dj = coord == 2, dk = coord == 3;
+  for (int k = b1.ks; k <= b1.ke; ++k)
+    for (int j = b1.js; j <= b1.je; ++j)
+      for (int i = b1.is; i <= b1.ie; ++i)
+        for (int n = 1; n <= 5; ++n) {
+          double d = flux(n, i, j, k) - flux(n, i - di, j - dj, k - dk);
+          if (coord == 1)
+            rhsi(n, i, j, k) = -d;
+          else
+            rhsi(n, i, j, k) = rhsi(n, i, j, k) - d;
+        }
+}
+
+}  // namespace
+
+void inviscid_flux_sw_weno5(V rhsi, V q, V dxidx, V inv_j, const Box& b, const Box& b1, double gamma) {
+  for (long n = 0; n < 5 * b.size(); ++n) rhsi.p[n] = 0.0;
+  int ndir = g_flags.dimension == IFLAG_3D ? 3 : 2;
+  for (int coord = 1; coord <= ndir; ++coord) {
+    Tmp flux(5, b);
+    int di = coord == 1, dj = coord == 2, dk = coord == 3;
+    int lo = coord == 1 ? b.is : (coord == 2 ? b.js : b.ks);
+    int hi = coord == 1 ? b.ie : (coord == 2 ? b.je : b.ke);
+    for (int k = b1.ks - dk; k <= b1.ke; ++k)
+      for (int j = b1.js - dj; j <= b1.je; ++j)
+        for (int i = b1.is - di; i <= b1.ie; ++i) {
+          int pos = coord == 1 ? i : (coord == 2 ? j : k);
+          double fp[5][5], fm[5][5];  // node pos-2+x (plus), pos-1+x (minus)
+          for (int x = 0; x < 5; ++x) {
+            int o = x - 2;
+            if (pos + o >= lo && pos + o <= hi)
+              sw_flux(true, q, dxidx, inv_j, coord, i + o * di, j + o * dj, k + o * dk, gamma, fp[x]);
+            o = x - 1;
+            if (pos + o >= lo && pos + o <= hi)
+              sw_flux(false, q, dxidx, inv_j, coord, i + o * di, j + o * dj, k + o * dk, gamma, fm[x]);
+          }
+          bool p5 = pos - 2 >= lo && pos + 2 <= hi, p3 = pos - 1 >= lo && pos + 1 <= hi;
+          bool m5 = pos - 1 >= lo && pos + 3 <= hi, m3 = pos >= lo && pos + 2 <= hi;
+          for (int n = 0; n < 5; ++n) {
+            double a = p5 ? w5_edge(fp[0][n], fp[1][n], fp[2][n], fp[3][n], fp[4][n])
+                          : (p3 ? w3_edge(fp[1][n], fp[2][n], fp[3][n]) : fp[2][n]);
+            double m = m5 ? w5_edge(fm[4][n], fm[3][n], fm[2][n], fm[1][n], fm[0][n])
+                          : (m3 ? w3_edge(fm[3][n], fm[2][n], fm[1][n]) : fm[2][n]);
+            flux(n + 1, i, j, k) = a + m;
+          }
+        }
+    difference_faces(rhsi, flux, b1, coord);
+  }
+}
+
+void inviscid_flux_wcns5(V rhsi, V q, V dxidx, V inv_j, const Box& b, const Box& b1, double gamma) {
+  for (long n = 0; n < 5 * b.size(); ++n) rhsi.p[n] = 0.0;
+  int ndir = g_flags.dimension == IFLAG_3D ? 3 : 2;
+  for (int coord = 1; coord <= ndir; ++coord) {
+    Tmp ul(5, b), ur(5, b), ql(5, b), qr(5, b), flux(5, b);
+    thirdorder_weno(ur.view, q, b, b1, coord, 1);
+    thirdorder_weno(ul.view, q, b, b1, coord, -1);
+    int di = coord == 1, dj = coord == 2, dk = coord == 3;
+    int lo = coord == 1 ? b.is : (coord == 2 ? b.js : b.ks);
+    int hi = coord == 1 ? b.ie : (coord == 2 ? b.je : b.ke);
+    auto wcns = [&](int i, int j, int k) {
+      int pos = coord == 1 ? i : (coord == 2 ? j : k);
+      return pos - 2 >= lo && pos + 3 <= hi;
+    };
+    for (int k = b1.ks - dk; k <= b1.ke; ++k)
+      for (int j = b1.js - dj; j <= b1.je; ++j)
+        for (int i = b1.is - di; i <= b1.ie; ++i) {
+          if (wcns(i, j, k))
+            for (int n = 1; n <= 5; ++n) {
+              double u[6];
+              for (int x = 0; x < 6; ++x) u[x] = q(n, i + (x - 2) * di, j + (x - 2) * dj, k + (x - 2) * dk);
+              ul(n, i, j, k) = c5_edge(u[0], u[1], u[2], u[3], u[4]);
+              ur(n, i, j, k) = c5_edge(u[5], u[4], u[3], u[2], u[1]);
+            }
+          ql(1, i, j, k) = ul(1, i, j, k);
+          ql(2, i, j, k) = ul(2, i, j, k) / ul(1, i, j, k);
+          ql(3, i, j, k) = ul(3, i, j, k) / ul(1, i, j, k);
+          ql(4, i, j, k) = ul(4, i, j, k) / ul(1, i, j, k);
+          ql(5, i, j, k) = (ul(5, i, j, k) - 0.5 * (p2(ul(2, i, j, k)) + p2(ul(3, i, j, k)) +
+                                                    p2(ul(4, i, j, k))) / ul(1, i, j, k)) * (gamma - 1.0);
+          qr(1, i, j, k) = ur(1, i, j, k);
+          qr(2, i, j, k) = ur(2, i, j, k) / ur(1, i, j, k);
+          qr(3, i, j, k) = ur(3, i, j, k) / ur(1, i, j, k);
+          qr(4, i, j, k) = ur(4, i, j, k) / ur(1, i, j, k);
+          qr(5, i, j, k) = (ur(5, i, j, k) - 0.5 * (p2(ur(2, i, j, k)) + p2(ur(3, i, j, k)) +
+                                                    p2(ur(4, i, j, k))) / ur(1, i, j, k)) * (gamma - 1.0);
+        }
+    roe_3d(ql.view, qr.view, flux.view, dxidx, inv_j, gamma, b, b1, coord);
+    for (int k = b1.ks - dk; k <= b1.ke; ++k)
+      for (int j = b1.js - dj; j <= b1.je; ++j)
+        for (int i = b1.is - di; i <= b1.ie; ++i) {
+          if (!wcns(i, j, k)) continue;
+          double fa[5], fb[5];
+          phys_flux(q, dxidx, inv_j, coord, i, j, k, gamma, fa);
+          phys_flux(q, dxidx, inv_j, coord, i + di, j + dj, k + dk, gamma, fb);
+          for (int n = 0; n < 5; ++n) flux(n + 1, i, j, k) = 4.0 / 3.0 * flux(n + 1, i, j, k) - (fa[n] + fb[n]) / 6.0;
+        }
+    difference_faces(rhsi, flux, b1, coord);
+  }
+}
+
+void inviscid_flux(V rhsi, V q, V dxidx, V inv_j, const Box& b, const Box& b0, const Box& b1, double gamma) {
+  if (g_flags.inviscid == IFLAG_5THWENO)
+    inviscid_flux_sw_weno5(rhsi, q, dxidx, inv_j, b, b1, gamma);
+  else if (g_flags.inviscid == IFLAG_5THWCNS)
+    inviscid_flux_wcns5(rhsi, q, dxidx, inv_j, b, b1, gamma);
+  else
+    inviscid_flux_1(rhsi, q, dxidx, inv_j, b, b0, b1, gamma);
+}
+
 // sub_viscous.f90:9-378 (3-D branch).
 void viscous_flux(V rhsv, V pri_v, V amu, V vor, V dudx, V tao, V dxidx, V inv_j, double tinf,
                   double prl, double prt, double gamma, double cv, double re, const Box& b,

@@ -8,6 +8,10 @@ long get_primitivevariables(int mm, V pri_v, V q, double gamma, double cv, const
 void thirdorder_weno(V df, V f, const Box& b, const Box& r0, int coord, int direction);
 void roe_3d(V ql, V qr, V flux, V dxidx, V inv_j, double gamma, const Box& b, const Box& r0,
             int coord);
+void inviscid_flux_sw_weno5(V rhsi, V q, V dxidx, V inv_j, const Box& b, const Box& b1, double gamma);
+void inviscid_flux_wcns5(V rhsi, V q, V dxidx, V inv_j, const Box& b, const Box& b1, double gamma);
+// inviscid_flux_1 or the extension scheme g_flags.inviscid names
+void inviscid_flux(V rhsi, V q, V dxidx, V inv_j, const Box& b, const Box& b0, const Box& b1, double gamma);
 void inviscid_flux_1(V rhsi, V q, V dxidx, V inv_j, const Box& b, const Box& b0, const Box& b1,
                      double gamma);
 void viscous_flux(V rhsv, V pri_v, V amu, V vor, V dudx, V tao, V dxidx, V inv_j, double tinf,

@@ -645,7 +645,7 @@ static void block_update(Block& B, int m, double* dtmax, double* dtmin, double* 
   const Consts& c = g_consts;
   const Box &b = B.b, &b0 = B.b0, &b1 = B.b1;
   get_primitivevariables(m, B.v(F_PRI), B.v(F_Q), c.gamma, c.cv, b);
-  inviscid_flux_1(B.v(F_RHSI), B.v(F_Q), B.v(F_DXIDX), B.v(F_INVJ), b, b0, b1, c.gamma);
+  inviscid_flux(B.v(F_RHSI), B.v(F_Q), B.v(F_DXIDX), B.v(F_INVJ), b, b0, b1, c.gamma);
   if (g_flags.solver == IFLAG_NSSOLVER)
     viscous_flux(B.v(F_RHSV), B.v(F_PRI), B.v(F_AMU), B.v(F_VOR), B.v(F_DUDX), B.v(F_TAO),
                  B.v(F_DXIDX), B.v(F_INVJ), c.tinf, c.prl, c.prt, c.gamma, c.cv, c.re, b, b0, b1);
@@ -680,7 +680,7 @@ void iterate_crank(int nsteps, double* resid_hist) {
         if (!B.used) continue;
         const Box &b = B.b, &b0 = B.b0, &b1 = B.b1;
         get_primitivevariables(0, B.v(F_PRI), B.v(F_Q), c.gamma, c.cv, b);
-        inviscid_flux_1(B.v(F_RHSI), B.v(F_Q), B.v(F_DXIDX), B.v(F_INVJ), b, b0, b1, c.gamma);
+        inviscid_flux(B.v(F_RHSI), B.v(F_Q), B.v(F_DXIDX), B.v(F_INVJ), b, b0, b1, c.gamma);
         if (g_flags.solver == IFLAG_NSSOLVER)
           viscous_flux(B.v(F_RHSV), B.v(F_PRI), B.v(F_AMU), B.v(F_VOR), B.v(F_DUDX), B.v(F_TAO), B.v(F_DXIDX),
                        B.v(F_INVJ), c.tinf, c.prl, c.prt, c.gamma, c.cv, c.re, b, b0, b1);
@@ -820,6 +820,20 @@ void oracle_inviscid_flux_1(double* rhsi, double* q, double* dxidx, double* inv_
                             ARGS6(z), ARGS6(o), const double* gamma) {
   Box b = BOX6(), b0 = BOX6(z), b1 = BOX6(o);
   inviscid_flux_1(V{rhsi, 5, b}, V{q, 5, b}, V{dxidx, 9, b}, V{inv_j, 1, b}, b, b0, b1, *gamma);
+}
+
+void oracle_inviscid_flux_weno5(double* rhsi, double* q, double* dxidx, double* inv_j, ARGS6(),
+                                ARGS6(z), ARGS6(o), const double* gamma) {
+  Box b = BOX6(), b1 = BOX6(o);
+  (void)zis; (void)zie; (void)zjs; (void)zje; (void)zks; (void)zke;
+  inviscid_flux_sw_weno5(V{rhsi, 5, b}, V{q, 5, b}, V{dxidx, 9, b}, V{inv_j, 1, b}, b, b1, *gamma);
+}
+
+void oracle_inviscid_flux_wcns5(double* rhsi, double* q, double* dxidx, double* inv_j, ARGS6(),
+                                ARGS6(z), ARGS6(o), const double* gamma) {
+  Box b = BOX6(), b1 = BOX6(o);
+  (void)zis; (void)zie; (void)zjs; (void)zje; (void)zks; (void)zke;
+  inviscid_flux_wcns5(V{rhsi, 5, b}, V{q, 5, b}, V{dxidx, 9, b}, V{inv_j, 1, b}, b, b1, *gamma);
 }
 
 void oracle_viscous_flux(double* rhsv, double* pri_v, double* amu, double* vor, double* dudx,

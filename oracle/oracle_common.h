@@ -86,6 +86,7 @@ enum {
   IFLAG_NSSOLVER = 0, IFLAG_EULERSOLVER = 1,
   IFLAG_STEADY = 0, IFLAG_UNSTEADY = 1,
   IFLAG_1STIMPLICIT = 2, IFLAG_2NDCRANK = 3,
+  IFLAG_3RDWENO = 4, IFLAG_5THWENO = 5, IFLAG_5THWCNS = 8,
   IFLAG_LAMINAR = 0, IFLAG_SA = 2,
   IFLAG_DES97 = 1, IFLAG_DDES = 2,
   BC_INFLOW = -50, BC_OUTFLOW = -40, BC_SYMM = -30, BC_WALL = -20, BC_FARFIELD = -10,

@@ -287,3 +287,77 @@ def test_iteration_reduces_residual_on_bump(oracle_mod):
     h = oc.iterate(40)
     assert np.all(np.isfinite(h))
     assert h[-1, 0] < 0.5 * h[0, 0]
+
+
+# ------------------------------------------- extension inviscid schemes
+def _cartesian_line(oracle_mod, n, inviscid, ny=9, nz=9, amp=0.2):
+    """A Cartesian n x ny x nz box of spacing h with physical faces only, the
+    flow varying along x alone: rho = 1 + 0.2 sin(pi x / 2), u = 0.5, v = w = 0,
+    p = 1/1.4.  Returns the oracle's rhsi / inv_j on the centre line and the
+    exact -dF/dx there (the metric gives the face flux h^2 F, so
+    rhsi / inv_j approximates -dF/dx)."""
+    cfg = Config(ma=0.5, inviscid=inviscid)
+    subs = [Subface(f, f, *box, BC_SYMM) for f, box in enumerate(
+        [(1, 1, 1, ny, 1, nz), (n, n, 1, ny, 1, nz), (1, n, 1, 1, 1, nz), (1, n, ny, ny, 1, nz),
+         (1, n, 1, ny, 1, 1), (1, n, 1, ny, nz, nz)], start=1)]
+    blk = Block(1, n, ny, nz, subs, cfg.buffer_length, cfg.dimension)
+    case = Case("line", cfg, [blk])
+    oc = oracle_mod.OracleCase(case)  # configures the oracle's flags
+    h = 1.0 / (n - 1)
+    x = (np.arange(n) * h)[None, None, :] * np.ones((nz, ny, 1))
+    f = blk.fields
+    rho = 1.0 + amp * np.sin(np.pi * x / 2.0)
+    u, p, gam = 0.5, 1.0 / 1.4, 1.4
+    f["q"][..., 0] = rho
+    f["q"][..., 1] = rho * u
+    f["q"][..., 2] = 0.0
+    f["q"][..., 3] = 0.0
+    f["q"][..., 4] = p / (gam - 1.0) + 0.5 * rho * u * u
+    f["dxidx"][...] = 0.0
+    for c in (0, 4, 8):
+        f["dxidx"][..., c] = 1.0 / h
+    f["inv_j"][...] = h ** 3
+    name = {5: "weno5", 8: "wcns5"}[inviscid]
+    getattr(oc.L, f"oracle_inviscid_flux_{name}")(_p(f["rhsi"]), _p(f["q"]), _p(f["dxidx"]), _p(f["inv_j"]),
+                                                  *oracle_mod.box_args(blk.box), *oracle_mod.box_args(blk.box0),
+                                                  *oracle_mod.box_args(blk.box1), _d(1.4))
+    jc, kc = ny // 2, nz // 2
+    got = f["rhsi"][kc, jc, :, :] / h ** 3
+    xs = x[0, 0, :]
+    drho = amp * np.pi / 2.0 * np.cos(np.pi * xs / 2.0)
+    exact = -np.stack([drho * u, drho * u * u, 0 * xs, 0 * xs, 0.5 * drho * u ** 3], axis=1)
+    return got, exact, f["rhsi"]
+
+
+@pytest.mark.parametrize("inviscid,order", [(5, 4.0), (8, 3.6)])
+def test_extension_scheme_order_of_accuracy(oracle_mod, inviscid, order):
+    """Steger-Warming + WENO5 (5th order) and WCNS5 with the hybrid 4th-order
+    difference, on smooth monotone data away from the boundary closures: the
+    error of -dF/dx falls at least at the stated rate when h halves."""
+    errs = []
+    for n in (33, 65):
+        got, exact, _ = _cartesian_line(oracle_mod, n, inviscid)
+        sl = slice(5, n - 5)
+        errs.append(np.max(np.abs(got[sl] - exact[sl])))
+    rate = np.log2(errs[0] / errs[1])
+    print("errors", errs, "observed order", rate)
+    assert rate >= order
+
+
+@pytest.mark.parametrize("inviscid", [5, 8])
+def test_extension_schemes_keep_uniform_flow_on_cartesian_grid(oracle_mod, inviscid):
+    """Uniform flow on a Cartesian box: the interior faces see identical
+    stencils, so the residual is zero there to the last bit."""
+    got, exact, rhsi = _cartesian_line(oracle_mod, 21, inviscid, amp=0.0)
+    assert np.all(np.isfinite(rhsi))
+    assert np.all(got[5:-5] == 0.0)
+
+
+def test_buffer_length_follows_the_scheme():
+    """bufferLength is derived from iflag_inviscid (main.f90:81): 2 for the
+    3rd-order WENO, 3 for the 5th-order extension schemes, an error otherwise."""
+    assert Config(inviscid=4).buffer_length == 2
+    assert Config(inviscid=5).buffer_length == 3
+    assert Config(inviscid=8).buffer_length == 3
+    with pytest.raises(ValueError):
+        Config(inviscid=6).buffer_length
