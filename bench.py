@@ -84,6 +84,7 @@ def parse():
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-case batch")
     ap.add_argument("--no-warm-start", action="store_true", help="skip the learned warm start")
     ap.add_argument("--no-plate", action="store_true", help="skip the SA flat plate")
+    ap.add_argument("--no-schemes", action="store_true", help="skip the WENO5 / WCNS5 workloads")
     return ap.parse_args()
 
 
@@ -279,6 +280,55 @@ def sa_plate_gpu(solver, steps: int, warmup: int, its: int = 3000, chunk: int = 
                                                                          float(cf["fp64"].max())]}
     out["note"] = ("the 1e-8 drop is not reached within a bench run: the drop after 8000 iterations is "
                    "about 1.7e-4 at CFL 5 to 20")
+    return out
+
+
+def schemes_gpu(solver, steps: int, warmup: int):
+    """The scheme-named workloads: the Euler bump 97 x 49 x 5 with
+    Steger-Warming + WENO5 (CFL 5, 500 iterations) and the laminar NACA0012
+    O-grid 4 x 129 x 65 x 3 with WCNS5 + Roe (CFL 2, 3000 iterations), each
+    beside the same case with the reference's Roe + WENO3: device-timed
+    throughput (L2 flushed before every step), the density-residual drop over
+    the run and, for the aerofoil, cl and cd at its end."""
+    import torch
+    from aerocfd_b200 import _lib, grids
+    from aerocfd_b200.case import Config, IFLAG_EULERSOLVER, IFLAG_NSSOLVER, SCHEME_NAMES
+    out = {}
+    runs = [("bump_97x49x5_euler_m0.5_cfl5", 500,
+             lambda inv: grids.bump_channel(cfg=Config(solver=IFLAG_EULERSOLVER, ma=0.5, re=1.0e6, cfl=5.0,
+                                                       inviscid=inv)), (5, 4)),
+            ("naca0012_ogrid_4x129x65x3_laminar", 3000,
+             lambda inv: grids.naca_ogrid(cfg=Config(solver=IFLAG_NSSOLVER, ma=0.5, re=5000.0, aoa_deg=2.0, cfl=2.0,
+                                                     inviscid=inv)), (8, 4))]
+    ms = ctypes.c_double(0.0)
+    for name, its, make, schemes in runs:
+        res = {}
+        for inv in schemes:
+            case = make(inv)
+            gc = solver.GpuCase(case)
+            try:
+                gc.compute_geometry()
+                gc.init_flowfield()
+                gc.start()
+                gc.use_graphs(True)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                h = gc.step(its)
+                el = time.perf_counter() - t0
+                clcd = gc.clcd_output(1.0)[6:8] if inv != 5 else None
+                gc.step(warmup, history=False)
+                _lib.check(gc.L.aero_step_timed(ctypes.c_int(steps), ctypes.c_int(1), ctypes.byref(ms)), "scheme")
+                r = {"value": case.nodes * steps / (ms.value / 1e3) / 1e6, "unit": "Mcell-iter/s",
+                     "ms_per_step": ms.value / steps, "iterations": its, "wall_s": el,
+                     "drop": float(h[-1, 0] / h[0, 0]), "device_status": gc.status()}
+                if clcd is not None:
+                    r["cl"], r["cd"] = float(clcd[0]), float(clcd[1])
+                res[SCHEME_NAMES[inv]] = r
+            finally:
+                gc.close()
+        out[name] = res
+    out["note"] = ("iflag_inviscid 5 and 8 have no code in the reference (it stops on them); both run in FP64 in "
+                   "either precision mode")
     return out
 
 
@@ -612,6 +662,8 @@ def main():
     gc.close()
     if world == 1 and not args.no_batch:
         line["batched"] = batched_gpu(solver, max(5, min(args.steps, 20)), args.warmup)
+    if world == 1 and not args.no_schemes:
+        line["schemes"] = schemes_gpu(solver, max(5, min(args.steps, 20)), args.warmup)
     if world == 1 and not args.no_plate:
         line["sa_plate"] = sa_plate_gpu(solver, max(5, min(args.steps, 20)), args.warmup)
     if world == 1 and not args.no_warm_start:
