@@ -143,14 +143,44 @@ __device__ __forceinline__ long rec_at(const BlockView& B, long pos, int h, int 
   return stride * base + x * cnt + (pos - base);
 }
 
+// Record formats: the 5x5 blocks in FP64 (76 words per node: 75 entries and
+// the packed neighbours at 75*cnt) or, in mixed precision, in FP32 (80
+// floats per node: 75 entries, the packed neighbours as one 64-bit word at
+// float offset 76*cnt, 3 unused), so a plane's chunk stays a multiple of 16
+// bytes for the bulk copies.  Products and sums are FP64 either way.
+template <typename R>
+struct RecFmt;
+template <>
+struct RecFmt<double> {
+  static constexpr int kWords = kRec;
+  __device__ static double packed(const double* chunk, int cnt, int t) { return chunk[75 * cnt + t]; }
+  __device__ static void set_packed(double* chunk, int cnt, long t, double v) { chunk[75 * cnt + t] = v; }
+};
+template <>
+struct RecFmt<float> {
+  static constexpr int kWords = 80;
+  __device__ static double packed(const float* chunk, int cnt, int t) {
+    return reinterpret_cast<const double*>(chunk + 76 * cnt)[t];
+  }
+  __device__ static void set_packed(float* chunk, int cnt, long t, double v) {
+    reinterpret_cast<double*>(chunk + 76 * cnt)[t] = v;
+  }
+};
+template <typename R>
+__device__ __forceinline__ R* recs(const BlockView& B, bool fwd) {
+  return reinterpret_cast<R*>(fwd ? B.rec_f : B.rec_b);
+}
+
 // The off-diagonal blocks of both sweeps, off the critical path.  For every
 // updated node (the provider) and direction d: A = calc_jm at the provider,
 // S+ = 0.5*(A + r*I)*inv_j goes to the forward record of the node one step up
 // in d, S- = 0.5*(A - r*I)*inv_j to the backward record of the node one step
 // down (sub_timeadvancement_1stimplicit.f90:283-301, :459-477, same
 // operations).  Each node also stores rhs, diag and inv_j, and the packed
-// positions of its forward and backward neighbours.
-__global__ void k_lusgs_mats(const BlockView* __restrict__ blocks, CaseConsts cc) {
+// positions of its forward and backward neighbours.  R is the record format.
+template <typename R>
+__device__ __forceinline__ void lusgs_mats_body(const BlockView* __restrict__ blocks, CaseConsts cc) {
+  constexpr int W = RecFmt<R>::kWords;
   const BlockView& B = blocks[blockIdx.y];
   const Box& b1 = B.b1;
   // thread t: direction d = t / N1 and provider position p = t % N1 in the
@@ -178,8 +208,9 @@ __global__ void k_lusgs_mats(const BlockView* __restrict__ blocks, CaseConsts cc
     sc[6 * cnt] = invj;
     sc[7 * cnt] = 1.0 / diag;
     sc[8 * cnt] = 1.0 / invj;
-    B.rec_f[kRec * base + 75 * cnt + lt] = pack_nbrs(nb, h > 0 ? B.poff[h - 1] : 0);
-    B.rec_b[kRec * base + 75 * cnt + lt] = pack_nbrs(nb + 3, h + 1 < B.nplanes ? B.poff[h + 1] : 0);
+    RecFmt<R>::set_packed(recs<R>(B, true) + W * base, (int)cnt, lt, pack_nbrs(nb, h > 0 ? B.poff[h - 1] : 0));
+    RecFmt<R>::set_packed(recs<R>(B, false) + W * base, (int)cnt, lt,
+                          pack_nbrs(nb + 3, h + 1 < B.nplanes ? B.poff[h + 1] : 0));
   }
   const int up = nb[3 + d];    // forward consumer: the neighbour one step up in d
   const int down = nb[d];      // backward consumer: one step down
@@ -191,22 +222,28 @@ __global__ void k_lusgs_mats(const BlockView* __restrict__ blocks, CaseConsts cc
   double invj = B.s(F_INVJ, n);
   if (up >= 0) {
     long base = B.poff[h + 1], cnt = B.poff[h + 2] - base;
-    double* dst = B.rec_f + kRec * base + 25 * d * cnt + (up - base);
+    R* dst = recs<R>(B, true) + W * base + 25 * d * cnt + (up - base);
 #pragma unroll
     for (int x = 0; x < 25; ++x) {
       double v = (x % 6 == 0) ? A[x] + rad : A[x];
-      dst[x * cnt] = 0.5 * v * invj;
+      dst[x * cnt] = (R)(0.5 * v * invj);
     }
   }
   if (down >= 0) {
     long base = B.poff[h - 1], cnt = B.poff[h] - base;
-    double* dst = B.rec_b + kRec * base + 25 * d * cnt + (down - base);
+    R* dst = recs<R>(B, false) + W * base + 25 * d * cnt + (down - base);
 #pragma unroll
     for (int x = 0; x < 25; ++x) {
       double v = (x % 6 == 0) ? A[x] - rad : A[x];
-      dst[x * cnt] = 0.5 * v * invj;
+      dst[x * cnt] = (R)(0.5 * v * invj);
     }
   }
+}
+__global__ void k_lusgs_mats(const BlockView* __restrict__ blocks, CaseConsts cc) {
+  lusgs_mats_body<double>(blocks, cc);
+}
+__global__ void k_lusgs_mats_f32(const BlockView* __restrict__ blocks, CaseConsts cc) {
+  lusgs_mats_body<float>(blocks, cc);
 }
 
 // ---------------------------------------------------------------- sweeps
@@ -260,12 +297,13 @@ __device__ __forceinline__ bool consumers_sync_or(bool pred, int n) {
   return r != 0;
 }
 
-__device__ __forceinline__ double row_dot5(const double* m, int mst, const double* x, int xst) {
-  double s = m[0] * x[0];
-  s = s + m[mst] * x[xst];
-  s = s + m[2 * mst] * x[2 * xst];
-  s = s + m[3 * mst] * x[3 * xst];
-  s = s + m[4 * mst] * x[4 * xst];
+template <typename R>
+__device__ __forceinline__ double row_dot5(const R* m, int mst, const double* x, int xst) {
+  double s = (double)m[0] * x[0];
+  s = s + (double)m[mst] * x[xst];
+  s = s + (double)m[2 * mst] * x[2 * xst];
+  s = s + (double)m[3 * mst] * x[3 * xst];
+  s = s + (double)m[4 * mst] * x[4 * xst];
   return s;
 }
 
@@ -278,11 +316,11 @@ constexpr long kSpinLimit = 1L << 20;  // bounded mbarrier wait (well under a se
 // reciprocals).  rec/sca/dsv point at the plane's chunks (element stride
 // cnt); prev holds the previous plane's dq, component c of node w at
 // prev[c*pst + w*wst].
-template <bool FWD>
-__device__ __forceinline__ void lusgs_rows(const double* rec, const double* sca, const double* dsv, int cnt,
+template <bool FWD, typename R>
+__device__ __forceinline__ void lusgs_rows(const R* rec, const double* sca, const double* dsv, int cnt,
                                            int t, int r0, int nr, const double* prev, long pst, int wst,
                                            double out[3]) {
-  double packed = rec[75 * cnt + t];
+  double packed = RecFmt<R>::packed(rec, cnt, t);
   double x[3][5];
   bool has[3];
 #pragma unroll
@@ -323,18 +361,20 @@ __device__ __forceinline__ void lusgs_rows(const double* rec, const double* sca,
 // fence and the `fwd_done` mbarrier.  Every wait is bounded: a consumer that
 // gives up makes all consumers stop at the next plane barrier and raise
 // ST_TIMEOUT; the producer then waits (bounded) for its copies in flight.
-__global__ void k_lusgs_sweep_staged(const BlockView* __restrict__ blocks, int nst, unsigned* status) {
+template <typename R>
+__device__ __forceinline__ void lusgs_staged_body(const BlockView* __restrict__ blocks, int nst, unsigned* status) {
+  constexpr int RD = RecFmt<R>::kWords * (int)sizeof(R) / 8;  // record words per node, in doubles
   const BlockView& B = blocks[blockIdx.x];
   extern __shared__ __align__(16) unsigned char smem[];
   const int P = B.pmax;
   const int H = B.nplanes;
   const int C = blockDim.x - 32;  // consumer threads
   // shared layout: plane offsets (H+1, padded to 16 B) | ring (2 planes x 5*P)
-  // | nst stages (P*(kRec+kSca+8)) | mbarriers
+  // | nst stages (P*(RD+kSca+8) doubles: records, scalars, dq*) | mbarriers
   long* poff = (long*)smem;
   double* ring = (double*)(poff + ((H + 2) & ~1));
   double* stage0 = ring + 10 * P;
-  const int sdoubles = P * (kRec + kSca + 8);
+  const int sdoubles = P * (RD + kSca + 8);
   unsigned long long* full = (unsigned long long*)(stage0 + nst * sdoubles);
   unsigned long long* empty = full + nst;
   unsigned long long* fwd_done = empty + nst;
@@ -374,10 +414,10 @@ __global__ void k_lusgs_sweep_staged(const BlockView* __restrict__ blocks, int n
       unsigned long long* bar = &full[gs % nst];
       if (gs >= nst && !wait_bar(&empty[gs % nst], (unsigned)((gs / nst - 1) & 1))) return false;
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_expect_tx(bar, cnt * (kRec + kSca + (fwd ? 0 : 8)) * 8u);
-      bulk_g2s(stg, (fwd ? B.rec_f : B.rec_b) + kRec * base, cnt * kRec * 8u, bar);
-      bulk_g2s(stg + P * kRec, B.sca + kSca * base, cnt * kSca * 8u, bar);
-      if (!fwd && with_dqs) bulk_g2s(stg + P * (kRec + kSca), B.dqs + 8 * base, cnt * 64u, bar);
+      mbar_expect_tx(bar, cnt * (RD + kSca + (fwd ? 0 : 8)) * 8u);
+      bulk_g2s(stg, recs<R>(B, fwd) + RecFmt<R>::kWords * base, cnt * RD * 8u, bar);
+      bulk_g2s(stg + P * RD, B.sca + kSca * base, cnt * kSca * 8u, bar);
+      if (!fwd && with_dqs) bulk_g2s(stg + P * (RD + kSca), B.dqs + 8 * base, cnt * 64u, bar);
       ++issued;
       return true;
     };
@@ -385,7 +425,7 @@ __global__ void k_lusgs_sweep_staged(const BlockView* __restrict__ blocks, int n
       int h = 2 * H - 1 - gs;
       long base = poff[h];
       unsigned cnt = (unsigned)(poff[h + 1] - base);
-      bulk_g2s(stage_of(gs) + P * (kRec + kSca), B.dqs + 8 * base, cnt * 64u, &full[gs % nst]);
+      bulk_g2s(stage_of(gs) + P * (RD + kSca), B.dqs + 8 * base, cnt * 64u, &full[gs % nst]);
     };
     for (int gs = 0; gs < H && ok; ++gs) ok = issue(gs, true);
     int head = nst < H ? nst : H;
@@ -440,22 +480,22 @@ __global__ void k_lusgs_sweep_staged(const BlockView* __restrict__ blocks, int n
       // t / cnt through a float reciprocal: exact here since t < 5*cnt <= 5*P
       int row = (int)(((float)t + 0.5f) * (1.0f / (float)cnt));
       int node = t - row * cnt;
-      const double* rec = stg + node;
-      const double* sca = stg + P * kRec + node;
-      double packed = rec[75 * cnt];
+      const R* rec = reinterpret_cast<const R*>(stg) + node;
+      const double* sca = stg + P * RD + node;
+      double packed = RecFmt<R>::packed(reinterpret_cast<const R*>(stg), cnt, node);
       double acc[3];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         int w = nbr_local(packed, d);
         double sd = 0.0;
         if (w >= 0) {
-          const double* mr = rec + (25 * d + 5 * row) * cnt;
+          const R* mr = rec + (25 * d + 5 * row) * cnt;
           const double* x = prev + 5 * w;
-          sd = mr[0] * x[0];
-          sd = sd + mr[cnt] * x[1];
-          sd = sd + mr[2 * cnt] * x[2];
-          sd = sd + mr[3 * cnt] * x[3];
-          sd = sd + mr[4 * cnt] * x[4];
+          sd = (double)mr[0] * x[0];
+          sd = sd + (double)mr[cnt] * x[1];
+          sd = sd + (double)mr[2 * cnt] * x[2];
+          sd = sd + (double)mr[3 * cnt] * x[3];
+          sd = sd + (double)mr[4 * cnt] * x[4];
         }
         acc[d] = sd;
       }
@@ -465,7 +505,7 @@ __global__ void k_lusgs_sweep_staged(const BlockView* __restrict__ blocks, int n
                    sca[8 * cnt]);
         g_dqs[8 * base + row * cnt + node] = v;
       } else {
-        double ds = stg[P * (kRec + kSca) + row * cnt + node];
+        double ds = stg[P * (RD + kSca) + row * cnt + node];
         v = ds - div_rn(div_rn(acc[0] + acc[1] + acc[2], sca[6 * cnt], sca[8 * cnt]), sca[5 * cnt], sca[7 * cnt]);
         g_dq[5 * (base + node) + row] = v;
       }
@@ -497,12 +537,21 @@ __global__ void k_lusgs_sweep_staged(const BlockView* __restrict__ blocks, int n
   }
 }
 
+__global__ void k_lusgs_sweep_staged(const BlockView* __restrict__ blocks, int nst, unsigned* status) {
+  lusgs_staged_body<double>(blocks, nst, status);
+}
+__global__ void k_lusgs_sweep_staged_f32(const BlockView* __restrict__ blocks, int nst, unsigned* status) {
+  lusgs_staged_body<float>(blocks, nst, status);
+}
+
 // The same sweeps with the records read from global memory, for blocks whose
 // planes do not fit the shared-memory stages; the previous plane's dq is read
 // back from dqs / dq (written before the last __syncthreads).  Thread 0 keeps
 // the records of the next kAhead planes on their way into L2 with bulk
 // prefetches.
-__global__ void k_lusgs_sweep_global(const BlockView* __restrict__ blocks, int nst, unsigned* status) {
+template <typename R>
+__device__ __forceinline__ void lusgs_global_body(const BlockView* __restrict__ blocks) {
+  constexpr int W = RecFmt<R>::kWords;
   const BlockView& B = blocks[blockIdx.x];
   const int H = B.nplanes;
   const long* poff = B.poff;
@@ -513,7 +562,7 @@ __global__ void k_lusgs_sweep_global(const BlockView* __restrict__ blocks, int n
     int h = fwd ? st : H - 1 - st;
     long b = poff[h];
     unsigned cnt = (unsigned)(poff[h + 1] - b);
-    bulk_prefetch_l2((fwd ? B.rec_f : B.rec_b) + kRec * b, cnt * kRec * 8u);
+    bulk_prefetch_l2(recs<R>(B, fwd) + W * b, cnt * (unsigned)(W * sizeof(R)));
     bulk_prefetch_l2(B.sca + kSca * b, cnt * kSca * 8u);
     if (!fwd) bulk_prefetch_l2(B.dqs + 8 * b, cnt * 64u);
   };
@@ -526,7 +575,7 @@ __global__ void k_lusgs_sweep_global(const BlockView* __restrict__ blocks, int n
       long base = poff[h];
       int cnt = (int)(poff[h + 1] - base);
       if (threadIdx.x == 0) prefetch(fwd, st + kAhead);
-      const double* rec = (fwd ? B.rec_f : B.rec_b) + kRec * base;
+      const R* rec = recs<R>(B, fwd) + W * base;
       const double* sca = B.sca + kSca * base;
       const double* dsv = B.dqs + 8 * base;
       // previous plane: forward dq* (plane-local chunk, component stride = its
@@ -549,9 +598,9 @@ __global__ void k_lusgs_sweep_global(const BlockView* __restrict__ blocks, int n
         int r0 = half ? 3 : 0, nr = half ? 2 : 3;
         double v[3];
         if (fwd)
-          lusgs_rows<true>(rec, sca, dsv, cnt, node, r0, nr, prev, pst, wst, v);
+          lusgs_rows<true, R>(rec, sca, dsv, cnt, node, r0, nr, prev, pst, wst, v);
         else
-          lusgs_rows<false>(rec, sca, dsv, cnt, node, r0, nr, prev, pst, wst, v);
+          lusgs_rows<false, R>(rec, sca, dsv, cnt, node, r0, nr, prev, pst, wst, v);
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
           if (k < nr) {
@@ -566,8 +615,16 @@ __global__ void k_lusgs_sweep_global(const BlockView* __restrict__ blocks, int n
       __syncthreads();
     }
   }
+}
+__global__ void k_lusgs_sweep_global(const BlockView* __restrict__ blocks, int nst, unsigned* status) {
   (void)nst;
   (void)status;
+  lusgs_global_body<double>(blocks);
+}
+__global__ void k_lusgs_sweep_global_f32(const BlockView* __restrict__ blocks, int nst, unsigned* status) {
+  (void)nst;
+  (void)status;
+  lusgs_global_body<float>(blocks);
 }
 
 namespace {
@@ -587,10 +644,10 @@ __device__ __forceinline__ unsigned cluster_size() {
 // written during the sweep (previous plane, dq*) loaded from L2: they come
 // from other SMs, and a line cached in this SM's L1 before they were written
 // would be stale.
-template <bool FWD>
-__device__ __forceinline__ double lusgs_row_l2(const double* rec, const double* sca, const double* dsv, int cnt,
+template <bool FWD, typename R>
+__device__ __forceinline__ double lusgs_row_l2(const R* rec, const double* sca, const double* dsv, int cnt,
                                                int t, int row, const double* prev, long pst, int wst) {
-  double packed = rec[75 * cnt + t];
+  double packed = RecFmt<R>::packed(rec, cnt, t);
   double acc[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -598,12 +655,12 @@ __device__ __forceinline__ double lusgs_row_l2(const double* rec, const double* 
     double sd = 0.0;
     if (w >= 0) {
       const double* x = prev + (long)w * wst;
-      const double* mr = rec + (25 * d + 5 * row) * cnt + t;
-      sd = mr[0] * __ldcg(x);
-      sd = sd + mr[cnt] * __ldcg(x + pst);
-      sd = sd + mr[2 * cnt] * __ldcg(x + 2 * pst);
-      sd = sd + mr[3 * cnt] * __ldcg(x + 3 * pst);
-      sd = sd + mr[4 * cnt] * __ldcg(x + 4 * pst);
+      const R* mr = rec + (25 * d + 5 * row) * cnt + t;
+      sd = (double)mr[0] * __ldcg(x);
+      sd = sd + (double)mr[cnt] * __ldcg(x + pst);
+      sd = sd + (double)mr[2 * cnt] * __ldcg(x + 2 * pst);
+      sd = sd + (double)mr[3 * cnt] * __ldcg(x + 3 * pst);
+      sd = sd + (double)mr[4 * cnt] * __ldcg(x + 4 * pst);
     }
     acc[d] = sd;
   }
@@ -621,15 +678,16 @@ struct RowRecs {
   double packed, m[15], rhs, diag, invj, rdiag, rinvj;
   int row, node;
 };
-__device__ __forceinline__ void load_row_recs(const double* rec, const double* sca, int cnt, int t, RowRecs& r) {
+template <typename R>
+__device__ __forceinline__ void load_row_recs(const R* rec, const double* sca, int cnt, int t, RowRecs& r) {
   r.row = t / cnt;
   r.node = t - r.row * cnt;
-  const double* rn = rec + r.node;
-  r.packed = rn[75 * cnt];
+  const R* rn = rec + r.node;
+  r.packed = RecFmt<R>::packed(rec, cnt, r.node);
 #pragma unroll
   for (int d = 0; d < 3; ++d)
 #pragma unroll
-    for (int c = 0; c < 5; ++c) r.m[5 * d + c] = rn[(25 * d + 5 * r.row + c) * cnt];
+    for (int c = 0; c < 5; ++c) r.m[5 * d + c] = (double)rn[(25 * d + 5 * r.row + c) * cnt];
   const double* sn = sca + r.node;
   r.rhs = sn[r.row * cnt];
   r.diag = sn[5 * cnt];
@@ -673,7 +731,9 @@ __device__ __forceinline__ double row_from_recs(const RowRecs& r, const double* 
 // CTAs of a cluster are resident together and every thread takes the same 2H
 // barriers, so the barrier always completes.  The arithmetic per row is
 // lusgs_rows'.
-__global__ void __launch_bounds__(512, 1) k_lusgs_sweep_cluster(const BlockView* __restrict__ blocks) {
+template <typename R>
+__device__ __forceinline__ void lusgs_cluster_body(const BlockView* __restrict__ blocks) {
+  constexpr int W = RecFmt<R>::kWords;
   const unsigned ncta = cluster_size();
   const BlockView& B = blocks[blockIdx.x / ncta];
   const int H = B.nplanes;
@@ -688,7 +748,7 @@ __global__ void __launch_bounds__(512, 1) k_lusgs_sweep_cluster(const BlockView*
     const int h = fwd ? gs : 2 * H - 1 - gs;
     const long base = poff[h];
     const int cnt = (int)(poff[h + 1] - base);
-    if (g < 5 * cnt) load_row_recs((fwd ? B.rec_f : B.rec_b) + kRec * base, B.sca + kSca * base, cnt, g, pre);
+    if (g < 5 * cnt) load_row_recs(recs<R>(B, fwd) + W * base, B.sca + kSca * base, cnt, g, pre);
   };
   preload(0);
   for (int gs = 0; gs < 2 * H; ++gs) {
@@ -696,7 +756,7 @@ __global__ void __launch_bounds__(512, 1) k_lusgs_sweep_cluster(const BlockView*
     const int h = fwd ? gs : 2 * H - 1 - gs;
     const long base = poff[h];
     const int cnt = (int)(poff[h + 1] - base);
-    const double* rec = (fwd ? B.rec_f : B.rec_b) + kRec * base;
+    const R* rec = recs<R>(B, fwd) + W * base;
     const double* sca = B.sca + kSca * base;
     const double* dsv = B.dqs + 8 * base;
     const double* prev = sca;
@@ -723,14 +783,20 @@ __global__ void __launch_bounds__(512, 1) k_lusgs_sweep_cluster(const BlockView*
       const int row = t / cnt;
       const int node = t - row * cnt;
       if (fwd)
-        B.dqs[8 * base + row * cnt + node] = lusgs_row_l2<true>(rec, sca, dsv, cnt, node, row, prev, pst, wst);
+        B.dqs[8 * base + row * cnt + node] = lusgs_row_l2<true, R>(rec, sca, dsv, cnt, node, row, prev, pst, wst);
       else
-        B.dq[5 * (base + node) + row] = lusgs_row_l2<false>(rec, sca, dsv, cnt, node, row, prev, pst, wst);
+        B.dq[5 * (base + node) + row] = lusgs_row_l2<false, R>(rec, sca, dsv, cnt, node, row, prev, pst, wst);
     }
     asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
     preload(gs + 1);
     asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
   }
+}
+__global__ void __launch_bounds__(512, 1) k_lusgs_sweep_cluster(const BlockView* __restrict__ blocks) {
+  lusgs_cluster_body<double>(blocks);
+}
+__global__ void __launch_bounds__(512, 1) k_lusgs_sweep_cluster_f32(const BlockView* __restrict__ blocks) {
+  lusgs_cluster_body<float>(blocks);
 }
 
 // q = q + dq on every updated node (sub_timeadvancement_1stimplicit.f90:568-574).

@@ -85,6 +85,7 @@ __global__ void k_dt_minmax(const BlockView* __restrict__ blocks, int m, const d
 __global__ void k_lusgs_prep(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_plane_index(const BlockView* __restrict__ blocks);
 __global__ void k_lusgs_mats(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_lusgs_mats_f32(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_length(const BlockView* __restrict__ blocks);
 __global__ void k_sa_a(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_b(const BlockView* __restrict__ blocks, CaseConsts cc);
@@ -93,6 +94,10 @@ __global__ void k_sa_sweep(const BlockView* __restrict__ blocks);
 __global__ void k_lusgs_sweep_staged(const BlockView* __restrict__ blocks, int nst, unsigned* status);
 __global__ void k_lusgs_sweep_global(const BlockView* __restrict__ blocks, int nst, unsigned* status);
 __global__ void k_lusgs_sweep_cluster(const BlockView* __restrict__ blocks);
+// the same with the off-diagonal blocks stored in FP32 (mixed precision)
+__global__ void k_lusgs_sweep_staged_f32(const BlockView* __restrict__ blocks, int nst, unsigned* status);
+__global__ void k_lusgs_sweep_global_f32(const BlockView* __restrict__ blocks, int nst, unsigned* status);
+__global__ void k_lusgs_sweep_cluster_f32(const BlockView* __restrict__ blocks);
 __global__ void k_lusgs_update(const BlockView* __restrict__ blocks);
 __global__ void k_physical_bc(const BlockView* __restrict__ blocks, const BcOp* __restrict__ ops,
                               const int* __restrict__ op_start, int o, CaseConsts cc);

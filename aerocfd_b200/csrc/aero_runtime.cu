@@ -489,9 +489,13 @@ int launch_dt_minmax(const BlockView* views, int m, double* d_out2) {
 }
 int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, int pmax, int hmax,
                     const CaseConsts& cc) {
+  // mixed precision stores the off-diagonal blocks in FP32 (products and sums
+  // stay FP64); f selects that variant of every kernel that touches them
+  const int f = g.mixed ? 1 : 0;
   PROF(P_LUSGS_PREP, (k_lusgs_prep<<<dim3(cdiv(maxExt, g.tune.ew), nblk), g.tune.ew, 0, g.stream>>>(views, cc)));
   CKL();
-  PROF(P_LUSGS_MATS, (k_lusgs_mats<<<dim3(cdiv(3 * maxN1, g.tune.mats), nblk), g.tune.mats, 0, g.stream>>>(views, cc)));
+  PROF(P_LUSGS_MATS, ((f ? k_lusgs_mats_f32 : k_lusgs_mats)<<<dim3(cdiv(3 * maxN1, g.tune.mats), nblk), g.tune.mats, 0,
+                                                             g.stream>>>(views, cc)));
   CKL();
   // Staged sweep: plane offsets + ring of two planes + nst staged planes
   // (records, scalars, dq*) + 2*nst+1 mbarriers, as many stages as fit
@@ -499,20 +503,22 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
   // plus one producer warp.
   if (pmax >= (1 << 21) - 1) return fail(AERO_ERR_ARG, "hyperplane of %d nodes exceeds the LU-SGS index range", pmax);
   const size_t kSmemMax = 227 * 1024;
+  const size_t rec_words = f ? 40 : kRec;  // record words per node, in doubles
   size_t offs = (size_t)((hmax + 2) & ~1) * sizeof(long);
   size_t ring = (size_t)2 * 5 * std::max(pmax, 1) * sizeof(double);
-  size_t stage = (size_t)std::max(pmax, 1) * (kRec + kSca + 8) * sizeof(double);
+  size_t stage = (size_t)std::max(pmax, 1) * (rec_words + kSca + 8) * sizeof(double);
   int nst = g.tune.nst_max;
   while (nst >= 2 && offs + ring + nst * stage + (2 * nst + 1) * 8 > kSmemMax) --nst;
-  static int staged_max_threads = 0;  // limited by the kernel's registers
-  if (!staged_max_threads) {
+  auto staged = f ? k_lusgs_sweep_staged_f32 : k_lusgs_sweep_staged;
+  static int staged_max_threads[2] = {0, 0};  // limited by the kernel's registers
+  if (!staged_max_threads[f]) {
     cudaFuncAttributes fa;
-    CK(cudaFuncGetAttributes(&fa, k_lusgs_sweep_staged));
-    staged_max_threads = fa.maxThreadsPerBlock;
+    CK(cudaFuncGetAttributes(&fa, staged));
+    staged_max_threads[f] = fa.maxThreadsPerBlock;
   }
   // consumer threads: one per row of every node of the largest plane
   auto consumers_for = [](int p) { return (5 * std::max(p, 1) + 31) / 32 * 32; };
-  if (nst >= 2 && consumers_for(pmax) + 32 > staged_max_threads) nst = 0;
+  if (nst >= 2 && consumers_for(pmax) + 32 > staged_max_threads[f]) nst = 0;
   if (g.tune.sweep_cl >= 2) {
     // one cluster of sweep_cl CTAs per block, one thread per row of every
     // node of the largest plane (at most 512 per CTA; more rows loop)
@@ -531,26 +537,27 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
     lc.attrs = at;
     lc.numAttrs = 1;
     cudaError_t le = cudaSuccess;
-    PROF(P_LUSGS_SWEEP, (le = cudaLaunchKernelEx(&lc, k_lusgs_sweep_cluster, views)));
+    PROF(P_LUSGS_SWEEP, (le = cudaLaunchKernelEx(&lc, f ? k_lusgs_sweep_cluster_f32 : k_lusgs_sweep_cluster, views)));
     CK(le);
   } else if (nst >= 2) {
     int consumers = consumers_for(pmax);
     size_t smem = offs + ring + nst * stage + (2 * nst + 1) * 8;
-    static size_t set_staged = 0;
-    if (smem > 48 * 1024 && smem > set_staged) {
-      CK(cudaFuncSetAttribute(k_lusgs_sweep_staged, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      set_staged = smem;
+    static size_t set_staged[2] = {0, 0};
+    if (smem > 48 * 1024 && smem > set_staged[f]) {
+      CK(cudaFuncSetAttribute(staged, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      set_staged[f] = smem;
     }
-    PROF(P_LUSGS_SWEEP, (k_lusgs_sweep_staged<<<nblk, consumers + 32, smem, g.stream>>>(views, nst, g.d_status)));
+    PROF(P_LUSGS_SWEEP, (staged<<<nblk, consumers + 32, smem, g.stream>>>(views, nst, g.d_status)));
   } else {
-    static int global_max_threads = 0;  // limited by the kernel's registers
-    if (!global_max_threads) {
+    auto global = f ? k_lusgs_sweep_global_f32 : k_lusgs_sweep_global;
+    static int global_max_threads[2] = {0, 0};  // limited by the kernel's registers
+    if (!global_max_threads[f]) {
       cudaFuncAttributes fa;
-      CK(cudaFuncGetAttributes(&fa, k_lusgs_sweep_global));
-      global_max_threads = fa.maxThreadsPerBlock / 32 * 32;
+      CK(cudaFuncGetAttributes(&fa, global));
+      global_max_threads[f] = fa.maxThreadsPerBlock / 32 * 32;
     }
-    int threads = (int)std::min<long>(global_max_threads, std::max<long>(64, (2L * pmax + 31) / 32 * 32));
-    PROF(P_LUSGS_SWEEP, (k_lusgs_sweep_global<<<nblk, threads, 0, g.stream>>>(views, 1, g.d_status)));
+    int threads = (int)std::min<long>(global_max_threads[f], std::max<long>(64, (2L * pmax + 31) / 32 * 32));
+    PROF(P_LUSGS_SWEEP, (global<<<nblk, threads, 0, g.stream>>>(views, 1, g.d_status)));
   }
   CKL();
   PROF(P_LUSGS_UPDATE, (k_lusgs_update<<<dim3(cdiv(maxN1, g.tune.ew), nblk), g.tune.ew, 0, g.stream>>>(views)));

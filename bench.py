@@ -598,8 +598,8 @@ def main():
     dq = qmx - q64
     mixed = {"value": nodes * args.steps * world / mixed_s / 1e6, "unit": "Mcell-iter/s",
              "ms_per_step": 1e3 * mixed_s / args.steps,
-             "dtype": "f32 WENO corrections / Roe dissipation / viscous stresses; f64 state, metrics, "
-                      "Jacobians, LU-SGS, dt, residual",
+             "dtype": "f32 WENO corrections / Roe dissipation / viscous stresses / stored LU-SGS off-diagonal "
+                      "blocks; f64 state, metrics, rhs, implicit diagonal, sweep products, dt, residual",
              "error_vs_fp64": {"iterations": kerr, "q_max_rel": float(np.max(np.abs(dq)) / np.max(np.abs(q64))),
                                "q_l2_rel": float(np.linalg.norm(dq) / np.linalg.norm(q64)),
                                "resid_rho_rel": float(abs(hmx[-1, 0] - h64[-1, 0]) / abs(h64[-1, 0]))}}

@@ -94,8 +94,10 @@ int aero_configure(const int* iflags, const double* params);
  * FP64 throughout).  mode 0 (default): FP64 in the reference's operation order.
  * mode 1 (mixed): the WENO3 corrections, the Roe dissipation and the viscous
  * stresses and fluxes in FP32, each formed from FP64 differences around FP64
- * base states; metrics, Jacobians, the implicit diagonal and sweeps, the time
- * step, the viscosity and the residual stay FP64.  Applies to later calls. */
+ * base states, and the off-diagonal 5x5 blocks of the LU-SGS sweeps stored in
+ * FP32 (their products and sums are FP64); metrics, the grid Jacobian, rhs,
+ * the implicit diagonal, dq, the time step, the viscosity and the residual
+ * stay FP64.  Applies to later calls. */
 int aero_set_precision(int mode);
 /* Batches (no counterpart in the reference, which runs one case per job):
  * gives block m its own Control.in values (params[7] as aero_configure) so
