@@ -799,6 +799,171 @@ __global__ void __launch_bounds__(512, 1) k_lusgs_sweep_cluster_f32(const BlockV
   lusgs_cluster_body<float>(blocks);
 }
 
+namespace {
+
+// Shared-memory address of CTA `rank` of the cluster for a local address.
+__device__ __forceinline__ unsigned map_rank(unsigned local, unsigned rank) {
+  unsigned r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local), "r"(rank));
+  return r;
+}
+// Bulk copy from this CTA's shared memory into another CTA's of the cluster,
+// completion counted in bytes on the destination CTA's mbarrier (no
+// multicast).  Addresses 16-byte aligned, size a multiple of 16.
+__device__ __forceinline__ void bulk_to_cluster(unsigned dst, unsigned src, unsigned bytes, unsigned mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   dst),
+               "r"(src), "r"(bytes), "r"(mbar)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+  long spins = 0;
+  while (!mbar_try_wait(bar, parity))
+    if (++spins > kSpinLimit) return false;
+  return true;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// lusgs_rows' arithmetic for one row from preloaded records, the previous
+// plane's values read from this CTA's ring in row-major item order
+// (row c of node w at c*cnt_prev + w).
+template <bool FWD>
+__device__ __forceinline__ double row_from_ring(const RowRecs& r, const double* prev, int cnt_prev, const double* dsv,
+                                                int cnt) {
+  double acc[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    int w = nbr_local(r.packed, d);
+    double sd = 0.0;
+    if (w >= 0) {
+      const double* x = prev + w;
+      sd = r.m[5 * d] * x[0];
+      sd = sd + r.m[5 * d + 1] * x[cnt_prev];
+      sd = sd + r.m[5 * d + 2] * x[2 * cnt_prev];
+      sd = sd + r.m[5 * d + 3] * x[3 * cnt_prev];
+      sd = sd + r.m[5 * d + 4] * x[4 * cnt_prev];
+    }
+    acc[d] = sd;
+  }
+  if (FWD) return div_rn(div_rn(r.rhs + (acc[0] + acc[1] + acc[2]), r.diag, r.rdiag), r.invj, r.rinvj);
+  return __ldcg(dsv + r.row * cnt + r.node) -
+         div_rn(div_rn(acc[0] + acc[1] + acc[2], r.invj, r.rinvj), r.diag, r.rdiag);
+}
+
+}  // namespace
+
+// The cluster sweeps with the plane-to-plane exchange by bulk copies between
+// the CTAs' shared memories.  Item t of a plane (row t / cnt of node t % cnt)
+// belongs to thread t of the cluster (5 * pmax <= cluster threads), so CTA r
+// computes the contiguous slice [r*T, (r+1)*T) of the plane's values.  Each CTA
+// writes its slice into a two-plane ring in its own shared memory (row-major
+// item order), and after a CTA barrier lane r of warp 0 copies the slice into
+// the same place in CTA r with cp.async.bulk, the bytes counted on the receiver's mbarrier
+// for that ring half; a CTA arms its mbarrier with the bytes it expects and its
+// threads wait (bounded) for the previous plane's bytes before reading the
+// neighbours from local shared memory.  No cluster barrier or global memory
+// is on the plane-to-plane path; one cluster barrier at the pass boundary
+// publishes the forward dq* (global) to the backward pass, and a last one keeps
+// every CTA resident until the copies into it have landed.  A CTA copies plane
+// gs+2 into a ring half only after every CTA has sent it plane gs+1, i.e. after
+// all have finished reading that half.  A wait that runs out raises ST_TIMEOUT
+// and the sweep runs on to the end.  The arithmetic per row is lusgs_rows'.
+template <typename R>
+__device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ blocks, unsigned* status) {
+  constexpr int W = RecFmt<R>::kWords;
+  extern __shared__ __align__(16) double xring[];  // 2 halves x (G + 2) doubles
+  __shared__ __align__(8) unsigned long long xbar[2];
+  const unsigned ncta = cluster_size(), me = cluster_rank();
+  const BlockView& B = blocks[blockIdx.x / ncta];
+  const int H = B.nplanes;
+  const long* poff = B.poff;
+  const int T = (int)blockDim.x;
+  const int G = (int)ncta * T;
+  const int HS = G + 2;
+  const int g = (int)me * T + (int)threadIdx.x;
+  if (threadIdx.x == 0) {
+    mbar_init(&xbar[0], 1);
+    mbar_init(&xbar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  cluster_sync_all();  // every CTA's mbarriers exist before any copy targets them
+  const unsigned ring_local = smem_u32(xring), bar_local = smem_u32(xbar);
+  auto plane_of = [&](int gs) { return gs < H ? gs : 2 * H - 1 - gs; };
+  auto count_of = [&](int gs) {
+    const int h = plane_of(gs);
+    return (int)(poff[h + 1] - poff[h]);
+  };
+  auto slice_bytes = [&](int cnt, unsigned r) -> unsigned {
+    const int n = min(T, 5 * cnt - (int)r * T);
+    return n <= 0 ? 0u : (unsigned)((n * 8 + 15) & ~15);
+  };
+  RowRecs pre;
+  auto preload = [&](int gs) {
+    if (gs >= 2 * H) return;
+    const bool fwd = gs < H;
+    const long base = poff[plane_of(gs)];
+    const int cnt = count_of(gs);
+    if (g < 5 * cnt) load_row_recs(recs<R>(B, fwd) + W * base, B.sca + kSca * base, cnt, g, pre);
+  };
+  bool ok = true;
+  preload(0);
+  for (int gs = 0; gs < 2 * H; ++gs) {
+    const bool fwd = gs < H;
+    const long base = poff[plane_of(gs)];
+    const int cnt = count_of(gs);
+    if (threadIdx.x == 0) {  // arm this plane's half: the bytes of the other CTAs' slices
+      unsigned expect = 0;
+      for (unsigned r = 0; r < ncta; ++r)
+        if (r != me) expect += slice_bytes(cnt, r);
+      mbar_expect_tx(&xbar[gs & 1], expect);
+    }
+    int cnt_prev = 0;
+    if (gs > 0) {
+      cnt_prev = count_of(gs - 1);
+      if (!mbar_wait_bounded(&xbar[(gs - 1) & 1], (unsigned)(((gs - 1) >> 1) & 1))) ok = false;
+    }
+    if (gs == H) cluster_sync_all();  // the forward dq* stores, for dsv
+    const double* prev = xring + ((gs - 1) & 1) * HS;
+    double* cur = xring + (gs & 1) * HS;
+    if (g < 5 * cnt) {
+      const double* dsv = B.dqs + 8 * base;
+      const double v = fwd ? row_from_ring<true>(pre, prev, cnt_prev, dsv, cnt)
+                           : row_from_ring<false>(pre, prev, cnt_prev, dsv, cnt);
+      cur[g] = v;
+      if (fwd)
+        B.dqs[8 * base + pre.row * cnt + pre.node] = v;
+      else
+        B.dq[5 * (base + pre.node) + pre.row] = v;
+    }
+    // the slice is complete once every thread has written and fenced its value;
+    // lane r of warp 0 then copies it to CTA r
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x < ncta && threadIdx.x != me) {
+      const unsigned bytes = slice_bytes(cnt, me);
+      const unsigned off = (unsigned)(((gs & 1) * HS + (int)me * T) * sizeof(double));
+      const unsigned boff = (unsigned)((gs & 1) * sizeof(unsigned long long));
+      if (bytes)
+        bulk_to_cluster(map_rank(ring_local + off, threadIdx.x), ring_local + off, bytes,
+                        map_rank(bar_local + boff, threadIdx.x));
+    }
+    preload(gs + 1);
+  }
+  // the last plane's bytes, then no CTA leaves while a copy into it may be in flight
+  if (H > 0 && !mbar_wait_bounded(&xbar[(2 * H - 1) & 1], (unsigned)(((2 * H - 1) >> 1) & 1))) ok = false;
+  cluster_sync_all();
+  if (!ok && status) atomicOr(status, (unsigned)ST_TIMEOUT);
+}
+__global__ void __launch_bounds__(512, 1) k_lusgs_sweep_bulk(const BlockView* __restrict__ blocks, unsigned* status) {
+  lusgs_bulk_body<double>(blocks, status);
+}
+__global__ void __launch_bounds__(512, 1) k_lusgs_sweep_bulk_f32(const BlockView* __restrict__ blocks,
+                                                                 unsigned* status) {
+  lusgs_bulk_body<float>(blocks, status);
+}
+
 // q = q + dq on every updated node (sub_timeadvancement_1stimplicit.f90:568-574).
 __global__ void k_lusgs_update(const BlockView* __restrict__ blocks) {
   const BlockView& B = blocks[blockIdx.y];

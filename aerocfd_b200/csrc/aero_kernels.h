@@ -98,6 +98,9 @@ __global__ void k_lusgs_sweep_cluster(const BlockView* __restrict__ blocks);
 __global__ void k_lusgs_sweep_staged_f32(const BlockView* __restrict__ blocks, int nst, unsigned* status);
 __global__ void k_lusgs_sweep_global_f32(const BlockView* __restrict__ blocks, int nst, unsigned* status);
 __global__ void k_lusgs_sweep_cluster_f32(const BlockView* __restrict__ blocks);
+// cluster sweeps exchanging plane values by bulk copies between shared memories
+__global__ void k_lusgs_sweep_bulk(const BlockView* __restrict__ blocks, unsigned* status);
+__global__ void k_lusgs_sweep_bulk_f32(const BlockView* __restrict__ blocks, unsigned* status);
 __global__ void k_lusgs_update(const BlockView* __restrict__ blocks);
 __global__ void k_physical_bc(const BlockView* __restrict__ blocks, const BcOp* __restrict__ ops,
                               const int* __restrict__ op_start, int o, CaseConsts cc);

@@ -129,6 +129,7 @@ struct State {
     int mats = 128;     // threads per CTA of k_lusgs_mats
     int nst_max = 4;    // most shared-memory stages of the staged sweep
     int sweep_cl = 0;   // CTAs per block of the global-memory sweep (0, 1: one CTA; 2..8: a cluster)
+    int sweep_x = 0;    // cluster exchange: 0 through L2, 1 bulk copies between shared memories (when it fits)
   } tune;
   // CUDA graph of one time step (aero_use_graphs)
   bool graph_want = false;
@@ -138,7 +139,7 @@ struct State {
   size_t t_tmax = 0;
   std::string err;
   std::string tuning = "inviscid_tile=64 elementwise_threads=256 viscous_threads=128 mats_threads=128 sweep_stages<=4 "
-                       "sweep_cluster=1";
+                       "sweep_cluster=1 sweep_exchange=l2";
 };
 
 State g;
@@ -519,7 +520,35 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
   // consumer threads: one per row of every node of the largest plane
   auto consumers_for = [](int p) { return (5 * std::max(p, 1) + 31) / 32 * 32; };
   if (nst >= 2 && consumers_for(pmax) + 32 > staged_max_threads[f]) nst = 0;
-  if (g.tune.sweep_cl >= 2) {
+  const bool bulk = g.tune.sweep_cl >= 2 && g.tune.sweep_x == 1 && 5L * pmax <= 512L * g.tune.sweep_cl;
+  if (bulk) {
+    // one cluster per block, one thread per row of every node of the largest
+    // plane; the plane values travel between the CTAs' shared memories
+    const int cl = g.tune.sweep_cl;
+    int threads = (int)std::max<long>(64, ((5L * pmax + cl - 1) / cl + 31) / 32 * 32);
+    const size_t smem = (size_t)2 * ((size_t)cl * threads + 2) * sizeof(double);
+    auto kern = f ? k_lusgs_sweep_bulk_f32 : k_lusgs_sweep_bulk;
+    static size_t set_bulk[2] = {0, 0};
+    if (smem > 48 * 1024 && smem > set_bulk[f]) {
+      CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      set_bulk[f] = smem;
+    }
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3((unsigned)(nblk * cl));
+    lc.blockDim = dim3((unsigned)threads);
+    lc.dynamicSmemBytes = smem;
+    lc.stream = g.stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)cl;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    cudaError_t le = cudaSuccess;
+    PROF(P_LUSGS_SWEEP, (le = cudaLaunchKernelEx(&lc, kern, views, g.d_status)));
+    CK(le);
+  } else if (g.tune.sweep_cl >= 2) {
     // one cluster of sweep_cl CTAs per block, one thread per row of every
     // node of the largest plane (at most 512 per CTA; more rows loop)
     const int cl = g.tune.sweep_cl;
@@ -913,8 +942,9 @@ void set_tuning_text() {
   char buf[200];
   std::snprintf(buf, sizeof buf,
                 "inviscid_tile=%d elementwise_threads=%d viscous_threads=%d mats_threads=%d sweep_stages<=%d "
-                "sweep_cluster=%d",
-                g.tune.inv_tile, g.tune.ew, g.tune.visc, g.tune.mats, g.tune.nst_max, std::max(1, g.tune.sweep_cl));
+                "sweep_cluster=%d sweep_exchange=%s",
+                g.tune.inv_tile, g.tune.ew, g.tune.visc, g.tune.mats, g.tune.nst_max, std::max(1, g.tune.sweep_cl),
+                g.tune.sweep_x ? "shared" : "l2");
   g.tuning = buf;
 }
 
@@ -966,7 +996,8 @@ int aero_autotune(int iters) {
   struct Knob { int* v; std::vector<int> cand; };
   std::vector<Knob> knobs = {{&g.tune.inv_tile, {0, 32, 64, 128}}, {&g.tune.ew, {128, 256, 512}},
                              {&g.tune.visc, {64, 128, 256}}, {&g.tune.mats, {64, 128, 256}},
-                             {&g.tune.nst_max, {2, 3, 4}}, {&g.tune.sweep_cl, {0, 2, 4, 8}}};
+                             {&g.tune.nst_max, {2, 3, 4}}, {&g.tune.sweep_cl, {0, 2, 4, 8}},
+                             {&g.tune.sweep_x, {0, 1}}};
   for (Knob& k : knobs) {
     int best = *k.v;
     double best_ms = 1e300;
@@ -1006,6 +1037,16 @@ int aero_set_tuning(int inv_tile, int ew, int visc, int mats, int nst_max) {
   g.tune.visc = visc;
   g.tune.mats = mats;
   g.tune.nst_max = nst_max;
+  graph_release();
+  set_tuning_text();
+  return AERO_OK;
+}
+
+int aero_set_sweep_exchange(int mode) {
+  int rc = need_init();
+  if (rc) return rc;
+  if (mode != 0 && mode != 1) return fail(AERO_ERR_ARG, "sweep exchange %d is not 0 (L2) or 1 (shared memory)", mode);
+  g.tune.sweep_x = mode;
   graph_release();
   set_tuning_text();
   return AERO_OK;

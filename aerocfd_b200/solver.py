@@ -138,6 +138,11 @@ class GpuCase:
         """aero_set_sweep_cluster: CTAs per block of the LU-SGS sweep (1, 2, 4, 8)."""
         _lib.check(self.L.aero_set_sweep_cluster(ctypes.c_int(ctas)), "aero_set_sweep_cluster")
 
+    def set_sweep_exchange(self, shared: bool) -> None:
+        """aero_set_sweep_exchange: plane values of a cluster sweep through L2
+        (False) or by bulk copies between the CTAs' shared memories (True)."""
+        _lib.check(self.L.aero_set_sweep_exchange(ctypes.c_int(1 if shared else 0)), "aero_set_sweep_exchange")
+
     def set_precision(self, mixed: bool) -> None:
         """aero_set_precision: 0 = FP64 reference arithmetic, 1 = mixed."""
         _lib.check(self.L.aero_set_precision(ctypes.c_int(1 if mixed else 0)), "aero_set_precision")

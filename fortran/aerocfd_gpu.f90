@@ -104,6 +104,13 @@ module aerocfd_gpu
       integer(c_int), value :: ctas
     end function
 
+    ! plane-value exchange of a cluster sweep: 0 through L2, 1 bulk copies
+    ! between shared memories (no counterpart in the reference)
+    integer(c_int) function aero_set_sweep_exchange(mode) bind(C, name="aero_set_sweep_exchange")
+      import :: c_int
+      integer(c_int), value :: mode
+    end function
+
     integer(c_int) function aero_finish_setup() bind(C, name="aero_finish_setup")
       import :: c_int
     end function

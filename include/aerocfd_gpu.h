@@ -286,6 +286,12 @@ int aero_set_tuning(int inv_tile, int ew, int visc, int mats, int nst_max);
  * cluster of 2, 4 or 8 CTAs meeting at a cluster barrier between hyperplanes.
  * The arithmetic is the same for every choice. */
 int aero_set_sweep_cluster(int ctas);
+/* How a cluster's CTAs pass each hyperplane's values to the next plane: 0
+ * (default) through L2 with a cluster barrier per plane, 1 by bulk copies
+ * between the CTAs' shared memories counted on mbarriers (used when every row
+ * of the largest plane has its own thread: 5 x plane nodes <= 512 x CTAs).
+ * The arithmetic is the same either way. */
+int aero_set_sweep_exchange(int mode);
 
 /* ---- warm-start network (no counterpart in the reference) --------------
  * aero_mlp_gemm: c[M x N] = a[M x K] * b[N x K]^T on the tcgen05 tensor cores,

@@ -130,20 +130,23 @@ def test_every_launch_shape_gives_the_same_bits(gpu, make):
 def test_sweep_cluster_gives_the_same_bits(gpu, make):
     """The LU-SGS sweep on one CTA per block (staged in shared memory, or from
     global memory when the planes are too large: the 129 x 65 x 9 bump) and
-    on clusters of 2, 4 and 8 CTAs per block: identical histories and states,
-    in FP64 and mixed precision."""
+    on clusters of 2, 4 and 8 CTAs per block passing plane values through L2
+    or by bulk copies between shared memories: identical histories and
+    states, in FP64 and mixed precision."""
     for mixed in (False, True):
         ref = None
-        for ctas in (1, 2, 4, 8):
+        for ctas, shared in ((1, False), (2, False), (4, False), (8, False), (2, True), (4, True), (8, True)):
             case = make()
             gc = gpu.GpuCase(case)
             try:
                 gc.set_sweep_cluster(ctas)
+                gc.set_sweep_exchange(shared)
                 gc.set_precision(mixed)
                 gc.compute_geometry()
                 gc.init_flowfield()
                 gc.start()
                 h = gc.step(4)
+                assert gc.status() == 0, (ctas, shared)
                 gc.sync_to_host(gpu.mask("q", "nut"))
                 out = (h, [b.fields["q"].copy() for b in case.blocks], [b.fields["nut"].copy() for b in case.blocks])
             finally:
@@ -151,6 +154,7 @@ def test_sweep_cluster_gives_the_same_bits(gpu, make):
             if ref is None:
                 ref = out
                 continue
-            assert np.array_equal(out[0], ref[0]), (mixed, ctas)
+            assert np.array_equal(out[0], ref[0]), (mixed, ctas, shared)
             for a, b in zip(out[1] + out[2], ref[1] + ref[2]):
-                assert np.array_equal(a, b), (mixed, ctas)
+                assert np.array_equal(a, b), (mixed, ctas, shared)
+
