@@ -993,21 +993,27 @@ int aero_autotune(int iters) {
     ms = f;
     return AERO_OK;
   };
+  // the sweep's cluster size and exchange are one knob (value 2 * ctas +
+  // exchange), since the shared-memory exchange is only eligible for some sizes
+  int sweep_mode = 2 * g.tune.sweep_cl + g.tune.sweep_x;
   struct Knob { int* v; std::vector<int> cand; };
   std::vector<Knob> knobs = {{&g.tune.inv_tile, {0, 32, 64, 128}}, {&g.tune.ew, {128, 256, 512}},
                              {&g.tune.visc, {64, 128, 256}}, {&g.tune.mats, {64, 128, 256}},
-                             {&g.tune.nst_max, {2, 3, 4}}, {&g.tune.sweep_cl, {0, 2, 4, 8}},
-                             {&g.tune.sweep_x, {0, 1}}};
+                             {&g.tune.nst_max, {2, 3, 4}}, {&sweep_mode, {0, 4, 8, 16, 5, 9, 17}}};
   for (Knob& k : knobs) {
     int best = *k.v;
     double best_ms = 1e300;
     for (int c : k.cand) {
       *k.v = c;
+      g.tune.sweep_cl = sweep_mode / 2;
+      g.tune.sweep_x = sweep_mode % 2;
       double ms = 0;
       if ((rc = time_steps(ms))) break;
       if (ms < best_ms) { best_ms = ms; best = c; }
     }
     *k.v = best;
+    g.tune.sweep_cl = sweep_mode / 2;
+    g.tune.sweep_x = sweep_mode % 2;
     if (rc) break;
   }
   cudaEventDestroy(a);
