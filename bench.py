@@ -72,6 +72,38 @@ KERNEL_TRAFFIC = {"k_lusgs_sweep": 42.97e6 + 0.09e6}
 ITER_BYTES = 240
 
 
+def init_replicas(world: int, local: int, backend: str = "nccl"):
+    """One process per GPU (torchrun): the process group used only for the
+    barrier around the timed region and the max over ranks; None at N = 1."""
+    if world <= 1:
+        return None
+    import datetime
+    import torch
+    import torch.distributed as dist
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+    return dist
+
+
+def max_over_ranks(x: float, dist) -> float:
+    """The largest value of x over the ranks (the job's time is its slowest
+    replica's); x itself without a process group."""
+    if dist is None:
+        return x
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(nodes: int, steps: int, world: int, seconds: float) -> float:
+    """Mcell-iter/s of the whole job: every replica advances `nodes` nodes
+    `steps` times in `seconds` (the max over ranks)."""
+    return nodes * steps * world / seconds / 1e6
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -499,12 +531,7 @@ def main():
         return 0
 
     import torch
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        torch.cuda.set_device(local)
+    dist = init_replicas(world, local)
 
     from aerocfd_b200 import _lib, solver
     case = make_case()
@@ -529,13 +556,9 @@ def main():
     torch.cuda.synchronize()
     cnt1 = ctypes.c_ulonglong(0)
     L.aero_launch_count(ctypes.byref(cnt1))
-    dev_s = ms.value / 1e3
-    if dist:
-        t = torch.tensor([dev_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_s = float(t.item())
+    dev_s = max_over_ranks(ms.value / 1e3, dist)
     nodes = case.nodes
-    value = nodes * args.steps * world / dev_s / 1e6
+    value = whole_job_rate(nodes, args.steps, world, dev_s)
 
     # ---- per-kernel profile (separate pass) for the roofline
     L.aero_profile(ctypes.c_int(1))
@@ -574,11 +597,7 @@ def main():
     gc.step(3, history=False)
     torch.cuda.synchronize()
     _lib.check(L.aero_step_timed(ctypes.c_int(args.steps), ctypes.c_int(1), ctypes.byref(ms)), "mixed timed")
-    mixed_s = ms.value / 1e3
-    if dist:
-        t = torch.tensor([mixed_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        mixed_s = float(t.item())
+    mixed_s = max_over_ranks(ms.value / 1e3, dist)
     gc.set_precision(False)
     gc.sync_to_host(solver.ALL)
     snap = [{k: v.copy() for k, v in b.fields.items()} for b in case.blocks]
@@ -596,7 +615,7 @@ def main():
     gc.sync_to_host(solver.mask("q"))
     qmx = np.concatenate([b.fields["q"].ravel() for b in case.blocks])
     dq = qmx - q64
-    mixed = {"value": nodes * args.steps * world / mixed_s / 1e6, "unit": "Mcell-iter/s",
+    mixed = {"value": whole_job_rate(nodes, args.steps, world, mixed_s), "unit": "Mcell-iter/s",
              "ms_per_step": 1e3 * mixed_s / args.steps,
              "dtype": "f32 WENO corrections / Roe dissipation / viscous stresses / stored LU-SGS off-diagonal "
                       "blocks; f64 state, metrics, rhs, implicit diagonal, sweep products, dt, residual",
@@ -619,12 +638,8 @@ def main():
         gc.sync_to_device(mq)
         _lib.check(L.aero_step(ctypes.c_int(1), res.ctypes.data_as(ctypes.c_void_p), None), "aero_step")
         gc.sync_to_host(mq)
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = nodes * args.steps * world / e2e_s / 1e6
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
+    e2e = whole_job_rate(nodes, args.steps, world, e2e_s)
 
     status = gc.status()
     if status:
