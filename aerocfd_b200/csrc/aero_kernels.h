@@ -86,7 +86,7 @@ __global__ void k_lusgs_prep(const BlockView* __restrict__ blocks, CaseConsts cc
 __global__ void k_plane_index(const BlockView* __restrict__ blocks);
 __global__ void k_lusgs_mats(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_lusgs_mats_f32(const BlockView* __restrict__ blocks, CaseConsts cc);
-__global__ void k_sa_length(const BlockView* __restrict__ blocks);
+__global__ void k_sa_length(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_a(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_b(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_recs(const BlockView* __restrict__ blocks, CaseConsts cc);

@@ -605,7 +605,7 @@ int launch_index(const BlockView* views, int nblk, long maxN1) {
 int launch_sa(const BlockView* views, int nblk, long maxN, long maxN1, int pmax, const CaseConsts& cc,
               cudaStream_t st = nullptr) {
   if (!st) st = g.stream;
-  PROF_ON(P_FILL, st, (k_sa_length<<<dim3(cdiv(maxN, 256), nblk), 256, 0, st>>>(views)));
+  PROF_ON(P_FILL, st, (k_sa_length<<<dim3(cdiv(maxN, 256), nblk), 256, 0, st>>>(views, cc)));
   CKL();
   PROF_ON(P_SA_A, st, (k_sa_a<<<dim3(cdiv(maxN1, 256), nblk), 256, 0, st>>>(views, cc)));
   CKL();
@@ -621,6 +621,8 @@ int launch_sa(const BlockView* views, int nblk, long maxN, long maxN1, int pmax,
 }
 
 bool viscous_on() { return g.cc.solver == IFLAG_NSSOLVER; }
+// DDES reads dudx, which the viscous kernel then stores
+int ddes_on() { return g.cc.turbulence == IFLAG_SA && g.cc.des == IFLAG_DDES ? 1 : 0; }
 bool sa_on() { return g.cc.turbulence == IFLAG_SA && g.cc.solver == IFLAG_NSSOLVER; }
 
 int do_physical_bc() {
@@ -708,7 +710,7 @@ int do_iteration_crank() {
     if ((rc = do_average2())) return rc;
     if ((rc = do_getpri_all())) return rc;
     if ((rc = launch_inviscid(g.d_blocks, nb, g.max_box, g.max_b1, g.max_b1_face, g.cc))) return rc;
-    if (viscous_on() && (rc = launch_viscous(g.d_blocks, nb, g.max_b0, g.cc, 0))) return rc;
+    if (viscous_on() && (rc = launch_viscous(g.d_blocks, nb, g.max_b0, g.cc, ddes_on()))) return rc;
     if ((rc = launch_crank(g.d_blocks, nb, g.max_box, g.max_b1, &g.max_b1_box, g.cc))) return rc;
   }
   PROF(P_CRANK, (k_update_q0<<<dim3(cdiv(g.max_b0, 256), nb), 256, 0, g.stream>>>(g.d_blocks)));
@@ -727,7 +729,7 @@ int do_iteration(bool want_dt_minmax) {
   int rc;
   if ((rc = do_getpri_all())) return rc;
   if ((rc = launch_inviscid(g.d_blocks, nb, g.max_box, g.max_b1, g.max_b1_face, g.cc))) return rc;
-  if (viscous_on() && (rc = launch_viscous(g.d_blocks, nb, g.max_b0, g.cc, 0))) return rc;
+  if (viscous_on() && (rc = launch_viscous(g.d_blocks, nb, g.max_b0, g.cc, ddes_on()))) return rc;
   if ((rc = launch_find_dt(g.d_blocks, nb, g.max_box, g.cc))) return rc;
   if (want_dt_minmax && (rc = launch_dt_minmax(g.d_blocks, nb - 1, g.d_out + 7))) return rc;
   // sa_model reads pri_v, amu, dudx, vor, dt and the metrics and writes nut,
@@ -1107,7 +1109,8 @@ int aero_configure(const int* iflags, const double* params) {
     return fail(AERO_ERR_ARG,
                 "bufferLength=%d/iflag_inviscid=%d: supported are the 3rd-order WENO with 2 layers and "
                 "WENO5 (5) or WCNS5 (8) with 3", iflags[6], iflags[7]);
-  if (iflags[5] != 0) return fail(AERO_ERR_ARG, "iflag_des=%d: DES97/DDES are not supported on the GPU", iflags[5]);
+  if (iflags[5] != 0 && iflags[5] != IFLAG_DES97 && iflags[5] != IFLAG_DDES)
+    return fail(AERO_ERR_ARG, "iflag_des=%d is not 0, 1 (DES97) or 2 (DDES)", iflags[5]);
   std::memcpy(g.iflags, iflags, sizeof g.iflags);
   std::memcpy(g.params, params, sizeof g.params);
   g.cc = consts_from(iflags, params);
@@ -1655,10 +1658,8 @@ int aero_sa_model(double* nut, double* sa_rhs, const double* dt, const double* p
                   const int* ke, const int* is0, const int* ie0, const int* js0, const int* je0,
                   const int* ks0, const int* ke0, const int* is1, const int* ie1, const int* js1,
                   const int* je1, const int* ks1, const int* ke1) {
-  (void)dudx; (void)spac;
   int rc = need_init();
   if (rc) return rc;
-  if (g.cc.des != 0) return fail(AERO_ERR_ARG, "sa_model: DES97/DDES length scales are not supported");
   Box b = box_of(is, ie, js, je, ks, ke), b0 = box_of(is0, ie0, js0, je0, ks0, ke0),
       b1 = box_of(is1, ie1, js1, je1, ks1, ke1);
   std::vector<Arg> args = {{F_NUT, nut, true},     {F_SARHS, sa_rhs, true}, {F_DT, dt, false},
@@ -1666,6 +1667,8 @@ int aero_sa_model(double* nut, double* sa_rhs, const double* dt, const double* p
                            {F_DXIDX, dxidx, false}, {F_INVJ, inv_j, false}, {F_ALPHA, alpha, false},
                            {F_BETA, beta, false},  {F_GAMMA, gamma, false}, {F_LENGTH, length, true},
                            {F_DIST, dist, false}};
+  if (g.cc.des == IFLAG_DES97 || g.cc.des == IFLAG_DDES) args.push_back({F_SPACING, spac, false});
+  if (g.cc.des == IFLAG_DDES) args.push_back({F_DUDX, dudx, false});
   BlockTarget t;
   if ((rc = resolve(b, b0, b1, args, t))) return rc;
   CaseConsts cc = consts_with(g.cc.gamma, g.cc.cv, *re);

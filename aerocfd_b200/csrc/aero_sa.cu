@@ -307,11 +307,42 @@ __global__ void __launch_bounds__(1024) k_sa_sweep(const BlockView* __restrict__
 }
 
 // length = dist over the full box (sub_tur_sa.f90:51-57; no DES).
-__global__ void k_sa_length(const BlockView* __restrict__ blocks) {
+// With iflag_des = 1 (DES97) length = min(dist, cdes*spacing); with 2 (DDES)
+// length = dist - fd*max(0, dist - cdes*spacing), fd = 1 - tanh((8 rd)^3),
+// rd = (nu + nut) / (|S'| Re kar^2 dist^2) with |S'| formed from the
+// off-diagonal velocity gradients (sub_tur_sa.f90:51-97).  The reference
+// declares dudx as (3, is:ie, js:je, ks:ke, 3) over its (9, ...) array, so
+// dudx(a, node, c) reads word (a-1) + 3*node + 3*N*(c-1) of the (9, node)
+// layout, N the box size; that is reproduced.
+__global__ void k_sa_length(const BlockView* __restrict__ blocks, CaseConsts cc_launch) {
   const BlockView& B = blocks[blockIdx.y];
+  const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
   long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= B.b.size()) return;
-  B.s(F_LENGTH, n) = B.s(F_DIST, n);
+  const long N = B.b.size();
+  if (n >= N) return;
+  const double cdes = 0.65;
+  double dist0 = B.s(F_DIST, n);
+  double len = dist0;
+  if (cc.des == IFLAG_DES97) {
+    double a = cdes * B.s(F_SPACING, n);
+    len = a < dist0 ? a : dist0;  // min(dist0, cdes*spac0)
+  } else if (cc.des == IFLAG_DDES) {
+    auto g3 = [&](int a, int c) {
+      long w = (a - 1) + 3 * n + 3 * N * (c - 1);  // word of the (9, node) array
+      long node = w / 9;
+      return B.v(F_DUDX, (int)(w - 9 * node) + 1, node);
+    };
+    double uy = g3(1, 2), uz = g3(1, 3), vx = g3(2, 1), vz = g3(2, 3), wx = g3(3, 1), wy = g3(3, 2);
+    double d0 = B.v(F_PRI, 1, n), nut0 = B.s(F_NUT, n), nu0 = B.v(F_AMU, 1, n) / d0;
+    double spac0 = B.s(F_SPACING, n);
+    double temp = p2(uy) + p2(uz) + p2(vx) + p2(vz) + p2(wx) + p2(wy);
+    temp = sqrt(temp);
+    double rd = (nu0 + nut0) / (temp * cc.re * SA_KAR2 * p2(dist0));
+    double fd = 1.0 - tanh(p3(8.0 * rd));
+    double e = dist0 - cdes * spac0;
+    len = dist0 - fd * (0.0 < e ? e : 0.0);
+  }
+  B.s(F_LENGTH, n) = len;
   B.s(F_SARHS, n) = 0.0;
 }
 

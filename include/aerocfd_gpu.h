@@ -179,7 +179,9 @@ int aero_implicit1st(double* q, const double* dt, const double* pri_v, double* r
                      const int* je1, const int* ks1, const int* ke1, const double* gamma,
                      const double* cfl, const double* xx, const double* yy, const double* zz);
 
-/* sub_tur_sa.f90:7-11 (no DES; dudx and spac are accepted and unused) */
+/* sub_tur_sa.f90:7-11, with the DES97 (iflag_des = 1) and DDES (2) length
+ * scales of :51-97; spac is read by both, dudx by DDES (through the
+ * reference's (3, ..., 3) view of the (9, ...) array). */
 int aero_sa_model(double* nut, double* sa_rhs, const double* dt, const double* pri_v, const double* amu,
                   const double* dudx, const double* vor, const double* dxidx, const double* inv_j,
                   const double* alpha, const double* beta, const double* gamma, double* length,

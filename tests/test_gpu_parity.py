@@ -244,6 +244,44 @@ def test_sa_model_transient(gpu, oracle_mod):
     gc.close()
 
 
+def plate_des(des):
+    return lambda: grids.flat_plate(ni=33, nj=25, nk=9, dy_wall=1e-4, cfg=Config(
+        solver=IFLAG_NSSOLVER, turbulence=2, des=des, ma=0.2, re=1.0e5, cfl=2.0, nutinf=3.0))
+
+
+@pytest.mark.parametrize("des", [1, 2])
+def test_sa_model_des_transient(gpu, oracle_mod, des):
+    """sa_model with the DES97 (1) and DDES (2) length scales through the
+    drop-in entry point; DDES reads dudx through the reference's (3, ..., 3)
+    reshape of the (9, ...) array."""
+    oc, co, cg = prepared(plate_des(des), oracle_mod, seed=12)
+    oc.iterate(1)
+    gc = gpu.GpuCase(cg)
+    try:
+        b = co.blocks[0]  # upstream block: cdes * spacing < wall distance at some nodes
+        F = b.fields
+        f = {k: v.copy() for k, v in F.items()}
+        c = co.cfg
+        ob = oracle_mod.box_args
+        names = ("nut", "sa_rhs", "dt", "pri_v", "amu", "dudx", "vor", "dxidx", "inv_j", "alpha", "beta",
+                 "ggamma", "length", "dist", "spacing")
+        assert gc.L.aero_sa_model(*[_p(f[k]) for k in names], _d(c.re), _d(c.cfl),
+                                  *[_i(v) for v in b.box + b.box0 + b.box1]) == 0
+        oc.L.oracle_sa_model(*[_p(F[k]) for k in names], _d(c.re), _d(c.cfl), *ob(b.box), *ob(b.box0),
+                             *ob(b.box1))
+        assert not np.array_equal(F["length"], F["dist"])  # the length scale is in use
+        for k in ("length", "sa_rhs", "nut"):
+            assert relerr(f[k], F[k]) <= TOL, (k, relerr(f[k], F[k]))
+    finally:
+        gc.close()
+
+
+@pytest.mark.parametrize("des", [1, 2])
+def test_flat_plate_des_iterations(gpu, oracle_mod, des):
+    """Whole iterations of the SA plate with DES97 / DDES length scales."""
+    run_parity(plate_des(des), oracle_mod, gpu, nsteps=3)
+
+
 def test_flat_plate_sa_iterations(gpu, oracle_mod):
     """SA RANS, 2x2x2 blocks: edge/corner interfaces, wall + symmetry on one
     face row, farfield, SA clip and eddy viscosity."""
