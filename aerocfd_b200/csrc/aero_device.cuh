@@ -20,12 +20,14 @@ enum FieldId {
   F_X, F_Y, F_Z, F_DIST, F_ALPHA, F_BETA, F_GAMMA, F_DUDX, F_TAO, F_VOR, F_LENGTH, F_SPACING, F_Q0,
   // device-only scratch
   F_RA, F_RB, F_RC, F_DIAG, F_FVH, F_DIASD, F_SAS,
+  F_FIH,  // inviscid face fluxes of the face-based kernels (5 per direction)
   F_NUM
 };
 __host__ __device__ constexpr int field_nc(int f) {
   return f == F_Q ? 5 : f == F_PRI ? 7 : f == F_RHSI ? 5 : f == F_RHSV ? 5 : f == F_RHS ? 5
        : f == F_DXIDX ? 9 : f == F_AMU ? 3 : f == F_ALPHA ? 3 : f == F_BETA ? 3 : f == F_GAMMA ? 3
-       : f == F_DUDX ? 9 : f == F_TAO ? 6 : f == F_FVH ? 15 : f == F_SAS ? 7 : f == F_Q0 ? 10 : 1;
+       : f == F_DUDX ? 9 : f == F_TAO ? 6 : f == F_FVH ? 15 : f == F_SAS ? 7 : f == F_Q0 ? 10
+       : f == F_FIH ? 15 : 1;
 }
 constexpr int kNumPublicFields = F_Q0 + 1;
 

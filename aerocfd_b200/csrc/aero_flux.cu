@@ -319,8 +319,8 @@ __global__ void k_inviscid_mixed_128(const BlockView* __restrict__ blocks, CaseC
 // Face-based variant of the same residual: every face flux once.
 // k_inviscid_faces: thread = one face along direction d = blockIdx.z, the face
 // between node n and its neighbour up in d, for every n of the updated box
-// grown by one node down in d; the flux goes to FVH plane 5*d + c (the viscous
-// scratch, free until viscous_flux).  k_inviscid_combine then forms
+// grown by one node down in d; the flux goes to plane 5*d + c of the FIH
+// scratch (its own, so the viscous kernels may run at the same time).  k_inviscid_combine then forms
 // rhsi = -dF; rhsi -= dG; rhsi -= dH as the per-node kernels do.
 template <bool MIXED>
 __device__ __forceinline__ void faces_body(const BlockView* __restrict__ blocks, CaseConsts cc) {
@@ -346,7 +346,7 @@ __device__ __forceinline__ void faces_body(const BlockView* __restrict__ blocks,
     face_flux_mixed(B, d + 1, n, pos, lo, hi, st, cc.gamma, f);
   else
     face_flux(B, d + 1, n, pos, lo, hi, st, cc.gamma, f);
-  double* out = B.f[F_FVH] + (long)(5 * d) * B.plane + n;
+  double* out = B.f[F_FIH] + (long)(5 * d) * B.plane + n;
 #pragma unroll
   for (int c = 0; c < 5; ++c) out[(long)c * B.plane] = f[c];
 }
@@ -365,7 +365,7 @@ __global__ void k_inviscid_combine(const BlockView* __restrict__ blocks, CaseCon
   long n = B.at(i, j, k);
   const long st[3] = {1, (long)B.nx, (long)B.nx * B.ny};
   const int ndir = cc.dimension == IFLAG_3D ? 3 : 2;
-  const double* F = B.f[F_FVH];
+  const double* F = B.f[F_FIH];
   const long P = B.plane;
 #pragma unroll
   for (int c = 0; c < 5; ++c) {
@@ -518,7 +518,7 @@ __device__ __forceinline__ bool face_at(const BlockView& B, int d, FaceAt& F) {
 
 }  // namespace
 
-// Steger-Warming + WENO5 face fluxes into FVH planes 5*d + c (then
+// Steger-Warming + WENO5 face fluxes into FIH planes 5*d + c (then
 // k_inviscid_combine).  F+ at pos+1/2 from nodes pos-2..pos+2, F- from
 // pos-1..pos+3.
 __global__ void k_faces_sw_weno5(const BlockView* __restrict__ blocks, CaseConsts cc) {
@@ -553,12 +553,12 @@ __global__ void k_faces_sw_weno5(const BlockView* __restrict__ blocks, CaseConst
       out[c] = out[c] + fm;
     }
   }
-  double* o = B.f[F_FVH] + (long)(5 * d) * B.plane + n;
+  double* o = B.f[F_FIH] + (long)(5 * d) * B.plane + n;
 #pragma unroll
   for (int c = 0; c < 5; ++c) o[(long)c * B.plane] = out[c];
 }
 
-// WCNS5 face fluxes G into FVH planes 5*d + c (then k_inviscid_combine).
+// WCNS5 face fluxes G into FIH planes 5*d + c (then k_inviscid_combine).
 __global__ void k_faces_wcns5(const BlockView* __restrict__ blocks, CaseConsts cc) {
   const BlockView& B = blocks[blockIdx.y];
   const int d = blockIdx.z;
@@ -584,7 +584,7 @@ __global__ void k_faces_wcns5(const BlockView* __restrict__ blocks, CaseConsts c
   } else {
     face_flux(B, d + 1, n, pos, F.lo, F.hi, st, cc.gamma, out);
   }
-  double* o = B.f[F_FVH] + (long)(5 * d) * B.plane + n;
+  double* o = B.f[F_FIH] + (long)(5 * d) * B.plane + n;
 #pragma unroll
   for (int c = 0; c < 5; ++c) o[(long)c * B.plane] = out[c];
 }

@@ -63,11 +63,12 @@ struct State {
   bool inited = false;
   int device = 0;
   cudaStream_t stream = nullptr;
-  // second stream of a steady iteration: sa_model runs on it beside implicit1st
-  // (neither reads what the other writes), forked after find_dt and joined
-  // before the boundary conditions
+  // second stream of a steady iteration: inviscid_flux_1 runs on it beside
+  // viscous_flux and find_dt, and sa_model beside implicit1st (in each pair
+  // neither reads what the other writes); each is forked and joined with events
   cudaStream_t stream2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_fork2 = nullptr, ev_join2 = nullptr;  // inviscid beside viscous + find_dt
   bool configured = false;
   int iflags[8] = {};
   double params[7] = {};
@@ -441,28 +442,31 @@ int launch_getpri(const BlockView* views, int nblk, long maxN, const CaseConsts&
   CKL();
   return AERO_OK;
 }
-int launch_inviscid(const BlockView* views, int nblk, long maxN, long maxN1, long maxFace, const CaseConsts& cc) {
-  PROF(P_FILL, (k_fill<<<dim3(cdiv(maxN, g.tune.ew), nblk), g.tune.ew, 0, g.stream>>>(views, F_RHSI, 5, 0.0)));
+// inviscid_flux_1 on nblk views, on stream st (the library's stream when null).
+int launch_inviscid(const BlockView* views, int nblk, long maxN, long maxN1, long maxFace, const CaseConsts& cc,
+                    cudaStream_t st = nullptr) {
+  if (!st) st = g.stream;
+  PROF_ON(P_FILL, st, (k_fill<<<dim3(cdiv(maxN, g.tune.ew), nblk), g.tune.ew, 0, st>>>(views, F_RHSI, 5, 0.0)));
   CKL();
   const int tile = g.tune.inv_tile;
   if (cc.inviscid == IFLAG_5THWENO || cc.inviscid == IFLAG_5THWCNS) {
     // extension schemes (FP64 in both precision modes): faces, then the combine
     long maxF = maxN1 + maxFace;
     auto faces = cc.inviscid == IFLAG_5THWENO ? k_faces_sw_weno5 : k_faces_wcns5;
-    PROF(P_INVISCID, (faces<<<dim3(cdiv(maxF, 128), nblk, 3), 128, 0, g.stream>>>(views, cc)));
+    PROF_ON(P_INVISCID, st, (faces<<<dim3(cdiv(maxF, 128), nblk, 3), 128, 0, st>>>(views, cc)));
     CKL();
-    PROF(P_INVISCID, (k_inviscid_combine<<<dim3(cdiv(maxN1, g.tune.ew), nblk), g.tune.ew, 0, g.stream>>>(views, cc)));
+    PROF_ON(P_INVISCID, st, (k_inviscid_combine<<<dim3(cdiv(maxN1, g.tune.ew), nblk), g.tune.ew, 0, st>>>(views, cc)));
   } else if (tile == 0) {  // face-based: each face once, then the combine
     // faces per direction <= updated box grown by one node in that direction
     long maxF = maxN1 + maxFace;
-    PROF(P_INVISCID, ((g.mixed ? k_inviscid_faces_mixed : k_inviscid_faces)<<<dim3(cdiv(maxF, 128), nblk, 3), 128, 0,
-                                                                             g.stream>>>(views, cc)));
+    PROF_ON(P_INVISCID, st, ((g.mixed ? k_inviscid_faces_mixed : k_inviscid_faces)<<<dim3(cdiv(maxF, 128), nblk, 3),
+                                                                                    128, 0, st>>>(views, cc)));
     CKL();
-    PROF(P_INVISCID, (k_inviscid_combine<<<dim3(cdiv(maxN1, g.tune.ew), nblk), g.tune.ew, 0, g.stream>>>(views, cc)));
+    PROF_ON(P_INVISCID, st, (k_inviscid_combine<<<dim3(cdiv(maxN1, g.tune.ew), nblk), g.tune.ew, 0, st>>>(views, cc)));
   } else {
     auto kern = g.mixed ? (tile == 32 ? k_inviscid_mixed_32 : tile == 128 ? k_inviscid_mixed_128 : k_inviscid_mixed_64)
                         : (tile == 32 ? k_inviscid_32 : tile == 128 ? k_inviscid_128 : k_inviscid_64);
-    PROF(P_INVISCID, (kern<<<dim3(cdiv(maxN1, tile), nblk), dim3(tile, 3), 0, g.stream>>>(views, cc)));
+    PROF_ON(P_INVISCID, st, (kern<<<dim3(cdiv(maxN1, tile), nblk), dim3(tile, 3), 0, st>>>(views, cc)));
   }
   CKL();
   return AERO_OK;
@@ -728,10 +732,17 @@ int do_iteration(bool want_dt_minmax) {
   int nb = (int)g.blocks.size();
   int rc;
   if ((rc = do_getpri_all())) return rc;
-  if ((rc = launch_inviscid(g.d_blocks, nb, g.max_box, g.max_b1, g.max_b1_face, g.cc))) return rc;
+  // inviscid_flux_1 (rhsi and its face scratch) beside viscous_flux and
+  // find_dt (rhsv, amu, vor, dudx, tao, their scratch, dt): neither side reads
+  // what the other writes
+  CK(cudaEventRecord(g.ev_fork2, g.stream));
+  CK(cudaStreamWaitEvent(g.stream2, g.ev_fork2, 0));
+  if ((rc = launch_inviscid(g.d_blocks, nb, g.max_box, g.max_b1, g.max_b1_face, g.cc, g.stream2))) return rc;
+  CK(cudaEventRecord(g.ev_join2, g.stream2));
   if (viscous_on() && (rc = launch_viscous(g.d_blocks, nb, g.max_b0, g.cc, ddes_on()))) return rc;
   if ((rc = launch_find_dt(g.d_blocks, nb, g.max_box, g.cc))) return rc;
   if (want_dt_minmax && (rc = launch_dt_minmax(g.d_blocks, nb - 1, g.d_out + 7))) return rc;
+  CK(cudaStreamWaitEvent(g.stream, g.ev_join2, 0));
   // sa_model reads pri_v, amu, dudx, vor, dt and the metrics and writes nut,
   // sa_rhs and its own scratch; implicit1st reads none of those it writes and
   // writes only q and its own scratch: the two run side by side
@@ -835,6 +846,8 @@ int aero_init(int device) {
   CK(cudaStreamCreateWithFlags(&g.stream2, cudaStreamNonBlocking));
   CK(cudaEventCreateWithFlags(&g.ev_fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&g.ev_join, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&g.ev_fork2, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&g.ev_join2, cudaEventDisableTiming));
   CK(cudaMalloc(&g.d_status, sizeof(unsigned)));
   CK(cudaMemset(g.d_status, 0, sizeof(unsigned)));
   CK(cudaMalloc(&g.d_out, 16 * sizeof(double)));
@@ -892,6 +905,8 @@ int aero_finalize(void) {
   cudaStreamDestroy(g.stream2); g.stream2 = nullptr;
   cudaEventDestroy(g.ev_fork); g.ev_fork = nullptr;
   cudaEventDestroy(g.ev_join); g.ev_join = nullptr;
+  cudaEventDestroy(g.ev_fork2); g.ev_fork2 = nullptr;
+  cudaEventDestroy(g.ev_join2); g.ev_join2 = nullptr;
   g.inited = false;
   g.configured = false;
   // execution options of the finished run
