@@ -4,17 +4,17 @@ A small MLP (aero_mlp_*: BF16 weights, FP32 accumulation, tcgen05 GEMMs) is
 trained on converged fields the solver generates for seeded members of a case
 family, and predicts the primitive variables of a new member from its
 parameters and node coordinates; the solver then starts from that field instead
-of the freestream.  The freestream start stays the fallback and the judge of
-the result: a warm-started run is iterated to the same residual level as the
-cold one and their wall forces are compared.
+of the freestream.  The freestream start stays the fallback and the yardstick
+for the result: a warm-started run is iterated to the same residual level as
+the cold one and their wall forces are compared.
 
 The family here is the bump channel (a fixed grid of ni x nj x nk, bump height
 h ~ U[0.05, 0.12], Mach ~ U[0.3, 0.7]) with farfield (Riemann-invariant)
 boundaries on the inflow, outflow and top faces: its steady state is unique
 and the scheme converges to machine zero from any start, which the warm start
-is judged against.  (With the fixed inflow and extrapolated outflow of the
+is compared against.  (With the fixed inflow and extrapolated outflow of the
 reference's own channel set-up the converged pressure level depends on the
-start, so no start can be judged by its converged forces.)  Node inputs are
+start, so converged forces cannot tell two starts apart.)  Node inputs are
 (x, y, wall distance, h, M), outputs the freestream-normalised perturbations of
 (rho, u, v, p).
 """
