@@ -516,12 +516,53 @@ __device__ __forceinline__ bool face_at(const BlockView& B, int d, FaceAt& F) {
   return true;
 }
 
+// Mixed precision of the extension schemes: every reconstructed value is the
+// FP64 centre value plus an FP32 correction built from FP64 differences
+// (q_k - v2 and the smoothness indicators rewritten in differences), so the
+// FP32 rounding scales with the jumps.  a = v0-v1, b = v1-v2, c = v3-v2,
+// e = v4-v3 around the centre v2; `lin` selects the WENO5 reconstruction
+// (d = 0.1, 0.6, 0.3) or the WCNS5 interpolation (d = 1/16, 10/16, 5/16).
+template <bool WCNS>
+__device__ __forceinline__ double edge5_corr(double v0, double v1, double v2, double v3, double v4) {
+  const float eps = 1.0e-6f;
+  float a = (float)(v0 - v1), b = (float)(v1 - v2), c = (float)(v3 - v2), e = (float)(v4 - v3);
+  float s0 = a - b, t0 = a - 3.0f * b;
+  float s1 = b + c, t1 = b - c;
+  float s2 = e - c, t2 = e - 3.0f * c;
+  float b0 = 13.0f / 12.0f * s0 * s0 + 0.25f * t0 * t0;
+  float b1 = 13.0f / 12.0f * s1 * s1 + 0.25f * t1 * t1;
+  float b2 = 13.0f / 12.0f * s2 * s2 + 0.25f * t2 * t2;
+  float a0 = (WCNS ? 0.0625f : 0.1f) / ((eps + b0) * (eps + b0));
+  float a1 = (WCNS ? 0.625f : 0.6f) / ((eps + b1) * (eps + b1));
+  float a2 = (WCNS ? 0.3125f : 0.3f) / ((eps + b2) * (eps + b2));
+  float q0, q1, q2;
+  if (WCNS) {
+    q0 = (3.0f * a - 7.0f * b) / 8.0f;
+    q1 = (3.0f * c - b) / 8.0f;
+    q2 = (5.0f * c - e) / 8.0f;
+  } else {
+    q0 = (2.0f * a - 5.0f * b) / 6.0f;
+    q1 = (2.0f * c - b) / 6.0f;
+    q2 = (4.0f * c - e) / 6.0f;
+  }
+  return (double)((a0 * q0 + a1 * q1 + a2 * q2) / (a0 + a1 + a2));
+}
+// WENO3 (Jiang & Shu) at the right edge of v1 as v1 + FP32 correction.
+__device__ __forceinline__ double edge3_corr(double v0, double v1, double v2) {
+  const float eps = 1.0e-6f;
+  float a = (float)(v1 - v0), c = (float)(v2 - v1);
+  float a0 = (1.0f / 3.0f) / ((eps + a * a) * (eps + a * a));
+  float a1 = (2.0f / 3.0f) / ((eps + c * c) * (eps + c * c));
+  return (double)((a0 * (0.5f * a) + a1 * (0.5f * c)) / (a0 + a1));
+}
+
 }  // namespace
 
 // Steger-Warming + WENO5 face fluxes into FIH planes 5*d + c (then
 // k_inviscid_combine).  F+ at pos+1/2 from nodes pos-2..pos+2, F- from
 // pos-1..pos+3.
-__global__ void k_faces_sw_weno5(const BlockView* __restrict__ blocks, CaseConsts cc) {
+template <bool MIXED>
+__device__ __forceinline__ void sw_weno5_body(const BlockView* __restrict__ blocks, CaseConsts cc) {
   const BlockView& B = blocks[blockIdx.y];
   const int d = blockIdx.z;
   FaceAt F;
@@ -536,9 +577,14 @@ __global__ void k_faces_sw_weno5(const BlockView* __restrict__ blocks, CaseConst
       if (pos - 2 + x >= lo && pos - 2 + x <= hi) sw_part<true>(B, d + 1, n + (x - 2) * st, cc.gamma, v[x]);
     const bool five = pos - 2 >= lo && pos + 2 <= hi, three = pos - 1 >= lo && pos + 1 <= hi;
 #pragma unroll
-    for (int c = 0; c < 5; ++c)
-      out[c] = five ? weno5_edge(v[0][c], v[1][c], v[2][c], v[3][c], v[4][c])
-                    : (three ? weno3_edge(v[1][c], v[2][c], v[3][c]) : v[2][c]);
+    for (int c = 0; c < 5; ++c) {
+      if (MIXED)
+        out[c] = v[2][c] + (five ? edge5_corr<false>(v[0][c], v[1][c], v[2][c], v[3][c], v[4][c])
+                                 : (three ? edge3_corr(v[1][c], v[2][c], v[3][c]) : 0.0));
+      else
+        out[c] = five ? weno5_edge(v[0][c], v[1][c], v[2][c], v[3][c], v[4][c])
+                      : (three ? weno3_edge(v[1][c], v[2][c], v[3][c]) : v[2][c]);
+    }
   }
   {
     double v[5][5] = {};  // F- at pos-1..pos+3
@@ -548,8 +594,13 @@ __global__ void k_faces_sw_weno5(const BlockView* __restrict__ blocks, CaseConst
     const bool five = pos - 1 >= lo && pos + 3 <= hi, three = pos >= lo && pos + 2 <= hi;
 #pragma unroll
     for (int c = 0; c < 5; ++c) {
-      double fm = five ? weno5_edge(v[4][c], v[3][c], v[2][c], v[1][c], v[0][c])
-                       : (three ? weno3_edge(v[3][c], v[2][c], v[1][c]) : v[2][c]);
+      double fm;
+      if (MIXED)
+        fm = v[2][c] + (five ? edge5_corr<false>(v[4][c], v[3][c], v[2][c], v[1][c], v[0][c])
+                             : (three ? edge3_corr(v[3][c], v[2][c], v[1][c]) : 0.0));
+      else
+        fm = five ? weno5_edge(v[4][c], v[3][c], v[2][c], v[1][c], v[0][c])
+                  : (three ? weno3_edge(v[3][c], v[2][c], v[1][c]) : v[2][c]);
       out[c] = out[c] + fm;
     }
   }
@@ -557,9 +608,16 @@ __global__ void k_faces_sw_weno5(const BlockView* __restrict__ blocks, CaseConst
 #pragma unroll
   for (int c = 0; c < 5; ++c) o[(long)c * B.plane] = out[c];
 }
+__global__ void k_faces_sw_weno5(const BlockView* __restrict__ blocks, CaseConsts cc) {
+  sw_weno5_body<false>(blocks, cc);
+}
+__global__ void k_faces_sw_weno5_mixed(const BlockView* __restrict__ blocks, CaseConsts cc) {
+  sw_weno5_body<true>(blocks, cc);
+}
 
 // WCNS5 face fluxes G into FIH planes 5*d + c (then k_inviscid_combine).
-__global__ void k_faces_wcns5(const BlockView* __restrict__ blocks, CaseConsts cc) {
+template <bool MIXED>
+__device__ __forceinline__ void wcns5_body(const BlockView* __restrict__ blocks, CaseConsts cc) {
   const BlockView& B = blocks[blockIdx.y];
   const int d = blockIdx.z;
   FaceAt F;
@@ -573,20 +631,34 @@ __global__ void k_faces_wcns5(const BlockView* __restrict__ blocks, CaseConsts c
     for (int c = 1; c <= 5; ++c) {
       double u0 = B.v(F_Q, c, n - 2 * st), u1 = B.v(F_Q, c, n - st), u2 = B.v(F_Q, c, n);
       double u3 = B.v(F_Q, c, n + st), u4 = B.v(F_Q, c, n + 2 * st), u5 = B.v(F_Q, c, n + 3 * st);
-      ul[c - 1] = wcns5_edge(u0, u1, u2, u3, u4);
-      ur[c - 1] = wcns5_edge(u5, u4, u3, u2, u1);
+      if (MIXED) {
+        ul[c - 1] = u2 + edge5_corr<true>(u0, u1, u2, u3, u4);
+        ur[c - 1] = u3 + edge5_corr<true>(u5, u4, u3, u2, u1);
+      } else {
+        ul[c - 1] = wcns5_edge(u0, u1, u2, u3, u4);
+        ur[c - 1] = wcns5_edge(u5, u4, u3, u2, u1);
+      }
     }
-    roe_face(B, d + 1, n, n + st, ul, ur, cc.gamma, fh);
+    if (MIXED)
+      roe_face_mixed(B, d + 1, n, n + st, ul, ur, cc.gamma, fh);
+    else
+      roe_face(B, d + 1, n, n + st, ul, ur, cc.gamma, fh);
     node_flux(B, d + 1, n, cc.gamma, fa);
     node_flux(B, d + 1, n + st, cc.gamma, fb);
 #pragma unroll
     for (int c = 0; c < 5; ++c) out[c] = 4.0 / 3.0 * fh[c] - (fa[c] + fb[c]) / 6.0;
+  } else if (MIXED) {
+    face_flux_mixed(B, d + 1, n, pos, F.lo, F.hi, st, cc.gamma, out);
   } else {
     face_flux(B, d + 1, n, pos, F.lo, F.hi, st, cc.gamma, out);
   }
   double* o = B.f[F_FIH] + (long)(5 * d) * B.plane + n;
 #pragma unroll
   for (int c = 0; c < 5; ++c) o[(long)c * B.plane] = out[c];
+}
+__global__ void k_faces_wcns5(const BlockView* __restrict__ blocks, CaseConsts cc) { wcns5_body<false>(blocks, cc); }
+__global__ void k_faces_wcns5_mixed(const BlockView* __restrict__ blocks, CaseConsts cc) {
+  wcns5_body<true>(blocks, cc);
 }
 
 // Zero-fills one field over the full box of every block (the reference's

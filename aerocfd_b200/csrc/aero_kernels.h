@@ -76,6 +76,8 @@ __global__ void k_inviscid_faces_mixed(const BlockView* __restrict__ blocks, Cas
 __global__ void k_inviscid_combine(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_faces_sw_weno5(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_faces_wcns5(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_faces_sw_weno5_mixed(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_faces_wcns5_mixed(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_viscous_a(const BlockView* __restrict__ blocks, CaseConsts cc, int store_dudx_tao);
 __global__ void k_viscous_a_mixed(const BlockView* __restrict__ blocks, CaseConsts cc, int store_dudx_tao);
 __global__ void k_viscous_b(const BlockView* __restrict__ blocks, CaseConsts cc);

@@ -450,9 +450,10 @@ int launch_inviscid(const BlockView* views, int nblk, long maxN, long maxN1, lon
   CKL();
   const int tile = g.tune.inv_tile;
   if (cc.inviscid == IFLAG_5THWENO || cc.inviscid == IFLAG_5THWCNS) {
-    // extension schemes (FP64 in both precision modes): faces, then the combine
+    // extension schemes: faces, then the combine
     long maxF = maxN1 + maxFace;
-    auto faces = cc.inviscid == IFLAG_5THWENO ? k_faces_sw_weno5 : k_faces_wcns5;
+    auto faces = cc.inviscid == IFLAG_5THWENO ? (g.mixed ? k_faces_sw_weno5_mixed : k_faces_sw_weno5)
+                                              : (g.mixed ? k_faces_wcns5_mixed : k_faces_wcns5);
     PROF_ON(P_INVISCID, st, (faces<<<dim3(cdiv(maxF, 128), nblk, 3), 128, 0, st>>>(views, cc)));
     CKL();
     PROF_ON(P_INVISCID, st, (k_inviscid_combine<<<dim3(cdiv(maxN1, g.tune.ew), nblk), g.tune.ew, 0, st>>>(views, cc)));

@@ -359,8 +359,7 @@ def schemes_gpu(solver, steps: int, warmup: int):
             finally:
                 gc.close()
         out[name] = res
-    out["note"] = ("iflag_inviscid 5 and 8 have no code in the reference (it stops on them); both run in FP64 in "
-                   "either precision mode")
+    out["note"] = "iflag_inviscid 5 and 8 have no code in the reference (it stops on them); FP64 here"
     return out
 
 

@@ -107,3 +107,41 @@ def test_freestream_preservation_of_wcns5(gpu, oracle_mod):
     print("max |rhsi| of a uniform state:", out)
     assert np.isfinite(out["weno5"])
     assert out["wcns5"] <= 10.0 * out["1"] + 1e-15
+
+
+@pytest.mark.parametrize("scheme", sorted(SCHEMES))
+@pytest.mark.parametrize("where", ["bump", "naca"])
+def test_mixed_extension_schemes_close_to_fp64(gpu, scheme, where):
+    """Mixed precision of the extension schemes (reconstructions as the FP64
+    centre value plus an FP32 correction; the mixed Roe flux for WCNS5):
+    10 iterations from one state against FP64, with the bounds of the
+    3rd-order scheme's mixed test (q 1e-6, residual history 1e-3)."""
+    make = bump(scheme) if where == "bump" else naca(scheme)
+    case = make()
+    gc = gpu.GpuCase(case)
+    try:
+        gc.compute_geometry()
+        gc.init_flowfield()
+        gc.start()
+        gc.step(3, history=False)
+        gc.sync_to_host(gpu.ALL)
+        snap = [{k: v.copy() for k, v in b.fields.items()} for b in case.blocks]
+        out = {}
+        for mixed in (False, True):
+            for b, sn in zip(case.blocks, snap):
+                for k, v in sn.items():
+                    b.fields[k][...] = v
+            gc.sync_to_device(gpu.ALL)
+            gc.set_precision(mixed)
+            h = gc.step(10)
+            gc.sync_to_host(gpu.mask("q"))
+            out[mixed] = (h, np.concatenate([b.fields["q"].ravel().copy() for b in case.blocks]))
+        gc.set_precision(False)
+        (h64, q64), (hmx, qmx) = out[False], out[True]
+        eq = float(np.max(np.abs(qmx - q64)) / np.max(np.abs(q64)))
+        rh = float(np.max(np.abs(hmx[:, :5] - h64[:, :5]) / np.max(np.abs(h64[:, :5]), axis=1, keepdims=True)))
+        print(f"{SCHEMES[scheme]} {where}: mixed vs fp64 q {eq:.2e}, residual history {rh:.2e}")
+        assert 0 < eq <= 1e-6 and rh <= 1e-3
+        assert gc.status() == 0
+    finally:
+        gc.close()
