@@ -69,6 +69,9 @@ struct State {
   cudaStream_t stream2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaEvent_t ev_fork2 = nullptr, ev_join2 = nullptr;  // inviscid beside viscous + find_dt
+  // dynamic shared memory limits already raised on this device (cudaFuncSetAttribute
+  // is per device), per sweep kernel [FP64 records, FP32 records]
+  size_t smem_staged[2] = {0, 0}, smem_bulk[2] = {0, 0};
   bool configured = false;
   int iflags[8] = {};
   double params[7] = {};
@@ -533,10 +536,9 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
     int threads = (int)std::max<long>(64, ((5L * pmax + cl - 1) / cl + 31) / 32 * 32);
     const size_t smem = (size_t)2 * ((size_t)cl * threads + 2) * sizeof(double);
     auto kern = f ? k_lusgs_sweep_bulk_f32 : k_lusgs_sweep_bulk;
-    static size_t set_bulk[2] = {0, 0};
-    if (smem > 48 * 1024 && smem > set_bulk[f]) {
+    if (smem > 48 * 1024 && smem > g.smem_bulk[f]) {
       CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      set_bulk[f] = smem;
+      g.smem_bulk[f] = smem;
     }
     cudaLaunchConfig_t lc = {};
     lc.gridDim = dim3((unsigned)(nblk * cl));
@@ -576,10 +578,9 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
   } else if (nst >= 2) {
     int consumers = consumers_for(pmax);
     size_t smem = offs + ring + nst * stage + (2 * nst + 1) * 8;
-    static size_t set_staged[2] = {0, 0};
-    if (smem > 48 * 1024 && smem > set_staged[f]) {
+    if (smem > 48 * 1024 && smem > g.smem_staged[f]) {
       CK(cudaFuncSetAttribute(staged, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      set_staged[f] = smem;
+      g.smem_staged[f] = smem;
     }
     PROF(P_LUSGS_SWEEP, (staged<<<nblk, consumers + 32, smem, g.stream>>>(views, nst, g.d_status)));
   } else {
@@ -843,6 +844,7 @@ const char* aero_last_error(void) { return g.err.c_str(); }
 int aero_init(int device) {
   if (g.inited) return AERO_OK;
   CK(cudaSetDevice(device));
+  for (int f = 0; f < 2; ++f) g.smem_staged[f] = g.smem_bulk[f] = 0;
   CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
   CK(cudaStreamCreateWithFlags(&g.stream2, cudaStreamNonBlocking));
   CK(cudaEventCreateWithFlags(&g.ev_fork, cudaEventDisableTiming));
