@@ -215,34 +215,77 @@ __device__ __forceinline__ void lusgs_mats_body(const BlockView* __restrict__ bl
   const int up = nb[3 + d];    // forward consumer: the neighbour one step up in d
   const int down = nb[d];      // backward consumer: one step down
   if (up < 0 && down < 0) return;
-  double A[25];
-  calc_jm(B, n, 3 * d + 1, cc.gamma, A);
-  const int radf[3] = {F_RA, F_RB, F_RC};
-  double rad = B.s(radf[d], n);
-  double invj = B.s(F_INVJ, n);
+  // calc_jm's common terms (sub_timeadvancement_jac.f90:17-62); every entry is
+  // then formed, and written to both records, one at a time, which keeps few
+  // values live
+  const int cb = 3 * d + 1;
+  const double gamma = cc.gamma;
+  const double rho = B.v(F_Q, 1, n), mu0 = B.v(F_Q, 2, n), mv0 = B.v(F_Q, 3, n);
+  const double mw0 = B.v(F_Q, 4, n), e0 = B.v(F_Q, 5, n);
+  const double dxidx = B.v(F_DXIDX, cb, n), dxidy = B.v(F_DXIDX, cb + 1, n), dxidz = B.v(F_DXIDX, cb + 2, n);
+  const double a2 = gamma - 1.0, a3 = gamma - 2.0;
+  const double uu = (dxidx * mu0 + dxidy * mv0 + dxidz * mw0) / rho;
+  const double phi = 0.5 * a2 * (p2(mu0) + p2(mv0) + p2(mw0)) / p2(rho);
+  const double a1 = gamma * e0 / rho - phi;
+  const double rad = B.s(d == 0 ? F_RA : (d == 1 ? F_RB : F_RC), n);
+  const double invj = B.s(F_INVJ, n);
+  R* dup = nullptr;
+  R* ddn = nullptr;
+  long cup = 0, cdn = 0;
   if (up >= 0) {
-    long base = B.poff[h + 1], cnt = B.poff[h + 2] - base;
-    R* dst = recs<R>(B, true) + W * base + 25 * d * cnt + (up - base);
-#pragma unroll
-    for (int x = 0; x < 25; ++x) {
-      double v = (x % 6 == 0) ? A[x] + rad : A[x];
-      dst[x * cnt] = (R)(0.5 * v * invj);
-    }
+    long base = B.poff[h + 1];
+    cup = B.poff[h + 2] - base;
+    dup = recs<R>(B, true) + W * base + 25 * d * cup + (up - base);
   }
   if (down >= 0) {
-    long base = B.poff[h - 1], cnt = B.poff[h] - base;
-    R* dst = recs<R>(B, false) + W * base + 25 * d * cnt + (down - base);
+    long base = B.poff[h - 1];
+    cdn = B.poff[h] - base;
+    ddn = recs<R>(B, false) + W * base + 25 * d * cdn + (down - base);
+  }
 #pragma unroll
-    for (int x = 0; x < 25; ++x) {
-      double v = (x % 6 == 0) ? A[x] - rad : A[x];
-      dst[x * cnt] = (R)(0.5 * v * invj);
+  for (int x = 0; x < 25; ++x) {
+    double a;  // calc_jm's a(x/5+1, x%5+1), the same operations
+    switch (x) {
+      case 0: a = 0.0; break;
+      case 1: a = dxidx; break;
+      case 2: a = dxidy; break;
+      case 3: a = dxidz; break;
+      case 4: a = 0.0; break;
+      case 5: a = phi * dxidx - uu * mu0 / rho; break;
+      case 6: a = uu - a3 * dxidx * mu0 / rho; break;
+      case 7: a = dxidy * mu0 / rho - a2 * dxidx * mv0 / rho; break;
+      case 8: a = dxidz * mu0 / rho - a2 * dxidx * mw0 / rho; break;
+      case 9: a = a2 * dxidx; break;
+      case 10: a = phi * dxidy - uu * mv0 / rho; break;
+      case 11: a = dxidx * mv0 / rho - a2 * dxidy * mu0 / rho; break;
+      case 12: a = uu - a3 * dxidy * mv0 / rho; break;
+      case 13: a = dxidz * mv0 / rho - a2 * dxidy * mw0 / rho; break;
+      case 14: a = a2 * dxidy; break;
+      case 15: a = phi * dxidz - uu * mw0 / rho; break;
+      case 16: a = dxidx * mw0 / rho - a2 * dxidz * mu0 / rho; break;
+      case 17: a = dxidy * mw0 / rho - a2 * dxidz * mv0 / rho; break;
+      case 18: a = uu - a3 * dxidz * mw0 / rho; break;
+      case 19: a = a2 * dxidz; break;
+      case 20: a = (phi - a1) * uu; break;
+      case 21: a = a1 * dxidx - a2 * uu * mu0 / rho; break;
+      case 22: a = a1 * dxidy - a2 * uu * mv0 / rho; break;
+      case 23: a = a1 * dxidz - a2 * uu * mw0 / rho; break;
+      default: a = gamma * uu; break;
+    }
+    if (dup) {
+      double v = (x % 6 == 0) ? a + rad : a;
+      dup[x * cup] = (R)(0.5 * v * invj);
+    }
+    if (ddn) {
+      double v = (x % 6 == 0) ? a - rad : a;
+      ddn[x * cdn] = (R)(0.5 * v * invj);
     }
   }
 }
-__global__ void k_lusgs_mats(const BlockView* __restrict__ blocks, CaseConsts cc) {
+__global__ void __launch_bounds__(256, 4) k_lusgs_mats(const BlockView* __restrict__ blocks, CaseConsts cc) {
   lusgs_mats_body<double>(blocks, cc);
 }
-__global__ void k_lusgs_mats_f32(const BlockView* __restrict__ blocks, CaseConsts cc) {
+__global__ void __launch_bounds__(256, 4) k_lusgs_mats_f32(const BlockView* __restrict__ blocks, CaseConsts cc) {
   lusgs_mats_body<float>(blocks, cc);
 }
 
