@@ -125,15 +125,39 @@ __device__ __forceinline__ double p6(double x) { double x2 = x * x; double x3 = 
 // remainder, so values outside [2^-960, 2^960] (and a = 0, whose sign the
 // corrections would lose) take the IEEE division.  The result is bit-identical
 // to a / b.
-__device__ __forceinline__ double div_rn(double a, double b, double rb) {
+__device__ __forceinline__ double div_newton(double a, double b, double rb) {
   double q = a * rb;
   double r = fma(-q, b, a);
   q = fma(r, rb, q);
   r = fma(-q, b, a);
-  q = fma(r, rb, q);
+  return fma(r, rb, q);
+}
+__device__ __forceinline__ double div_rn(double a, double b, double rb) {
+  double q = div_newton(a, b, rb);
   double aa = fabs(a), ab = fabs(b), aq = fabs(q);
   if (!(aa > 0x1p-960 && aa < 0x1p960 && ab > 0x1p-960 && ab < 0x1p960 && aq > 0x1p-960 && aq < 0x1p960))
     q = a / b;
+  return q;
+}
+
+// The two divisions of a sweep row, (a / b1) / b2, with the stored
+// reciprocals rb1, rb2.  div_rn's corrections are exact while a, b and the
+// quotient lie within (2^-960, 2^960).  With both divisors within
+// (2^-200, 2^200) (divisors_ok, tested per node before the row's plane
+// starts) and |a| within (2^-500, 2^500), the first quotient lies within
+// (2^-700, 2^700) and the second within (2^-900, 2^900), so only a is tested
+// on the plane-to-plane chain.  Every other case, zero included, takes the
+// IEEE divisions in a function of its own, which keeps the division's long
+// code out of the sweep loop.  The result equals a / b1 / b2 bit for bit.
+inline __device__ __noinline__ double div2_ieee(double a, double b1, double b2) { return a / b1 / b2; }
+__device__ __forceinline__ bool divisors_ok(double b1, double b2) {
+  const double x1 = fabs(b1), x2 = fabs(b2);
+  return x1 > 0x1p-200 && x1 < 0x1p200 && x2 > 0x1p-200 && x2 < 0x1p200;
+}
+__device__ __forceinline__ double div2_rn(double a, double b1, double rb1, double b2, double rb2, bool bok) {
+  double q = div_newton(div_newton(a, b1, rb1), b2, rb2);
+  const double aa = fabs(a);
+  if (!(bok && aa > 0x1p-500 && aa < 0x1p500)) q = div2_ieee(a, b1, b2);
   return q;
 }
 

@@ -328,18 +328,6 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
 __device__ __forceinline__ void bulk_prefetch_l2(const void* src, unsigned bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
 }
-// Barrier 1 over the first n threads (the consumer warps), returning the OR of
-// `pred` over them; orders memory like __syncthreads.
-__device__ __forceinline__ bool consumers_sync_or(bool pred, int n) {
-  unsigned r;
-  asm volatile(
-      "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, 1, %2, p;\n selp.u32 %0, 1, 0, q;\n}"
-      : "=r"(r)
-      : "r"((unsigned)pred), "r"(n)
-      : "memory");
-  return r != 0;
-}
-
 template <typename R>
 __device__ __forceinline__ double row_dot5(const R* m, int mst, const double* x, int xst) {
   double s = (double)m[0] * x[0];
@@ -375,6 +363,7 @@ __device__ __forceinline__ void lusgs_rows(const R* rec, const double* sca, cons
   }
   const double diag = sca[5 * cnt + t], invj = sca[6 * cnt + t];
   const double rdiag = sca[7 * cnt + t], rinvj = sca[8 * cnt + t];
+  const bool bok = divisors_ok(diag, invj);
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     if (k < nr) {
@@ -384,9 +373,9 @@ __device__ __forceinline__ void lusgs_rows(const R* rec, const double* sca, cons
       for (int d = 0; d < 3; ++d)
         acc[d] = has[d] ? row_dot5(rec + (25 * d + 5 * row) * cnt + t, cnt, x[d], 1) : 0.0;
       if (FWD)
-        out[k] = div_rn(div_rn(sca[row * cnt + t] + (acc[0] + acc[1] + acc[2]), diag, rdiag), invj, rinvj);
+        out[k] = div2_rn(sca[row * cnt + t] + (acc[0] + acc[1] + acc[2]), diag, rdiag, invj, rinvj, bok);
       else
-        out[k] = dsv[row * cnt + t] - div_rn(div_rn(acc[0] + acc[1] + acc[2], invj, rinvj), diag, rdiag);
+        out[k] = dsv[row * cnt + t] - div2_rn(acc[0] + acc[1] + acc[2], invj, rinvj, diag, rdiag, bok);
     }
   }
 }
@@ -421,10 +410,13 @@ __device__ __forceinline__ void lusgs_staged_body(const BlockView* __restrict__ 
   unsigned long long* full = (unsigned long long*)(stage0 + nst * sdoubles);
   unsigned long long* empty = full + nst;
   unsigned long long* fwd_done = empty + nst;
-  __shared__ volatile int abort_flag;
+  __shared__ volatile int abort_flag;     // read by the producer
+  __shared__ volatile int abort_slot[2];  // consumers: slot k&1 is set before barrier k, read after it
   for (int x = threadIdx.x; x <= H; x += blockDim.x) poff[x] = B.poff[x];
   if (threadIdx.x == 0) {
     abort_flag = 0;
+    abort_slot[0] = 0;
+    abort_slot[1] = 0;
     for (int x = 0; x < nst; ++x) {
       mbar_init(&full[x], 1);
       mbar_init(&empty[x], C / 32);
@@ -494,84 +486,135 @@ __device__ __forceinline__ void lusgs_staged_body(const BlockView* __restrict__ 
   // Thread t < 5*cnt of a plane computes row t / cnt of node t % cnt (a warp
   // mostly covers consecutive nodes of one row, so its shared-memory reads
   // are consecutive words); warps beyond 5*cnt only take the barrier.  The
-  // ring holds the previous plane's dq node-major (5 per node).
+  // ring holds the previous plane's dq node-major (5 per node).  Everything
+  // of a plane that does not depend on the previous plane (its offsets, the
+  // wait for its copies, the row mapping, the thread's block rows, rhs or
+  // dq*, diagonal and J^-1) is loaded into registers before the barrier that
+  // ends the previous plane, so only the neighbours' dq, the block products
+  // and the two divisions remain between two barriers.
   const int lane = threadIdx.x & 31;
   double* const g_dqs = B.dqs;
   double* const g_dq = B.dq;
   const double* prev = ring + 5 * P;
   double* cur = ring;
-  int ls = 0;  // stage of the current step and its phase parity
-  unsigned lph = 0;
-  for (int gs = 0; gs < 2 * H; ++gs) {
+  struct PlaneRegs {
+    long base;
+    int cnt, row, node;
+    bool act, timeout;
+    int w[3];
+    R m[3][5];
+    double rhs, diag, invj, rdiag, rinvj;  // rhs: rhs (forward) or dq* (backward)
+    bool bok;                              // divisors_ok(diag, invj)
+  };
+  auto preload = [&](int gs, int ls, unsigned lph, PlaneRegs& q) {
     const bool fwd = gs < H;
     const int h = fwd ? gs : 2 * H - 1 - gs;
-    const long base = poff[h];
-    const int cnt = (int)(poff[h + 1] - base);
-    const double* stg = stage0 + ls * sdoubles;
-    bool timeout = false;
-    {
-      long spins = 0;
-      while (!mbar_try_wait(&full[ls], lph)) {
-        if (++spins > kSpinLimit) {
-          timeout = true;
-          break;
-        }
+    q.base = poff[h];
+    q.cnt = (int)(poff[h + 1] - q.base);
+    q.timeout = false;
+    long spins = 0;
+    while (!mbar_try_wait(&full[ls], lph)) {
+      if (++spins > kSpinLimit) {
+        q.timeout = true;
+        break;
       }
     }
     const int t = threadIdx.x;
-    if (!timeout && t < 5 * cnt) {
-      // t / cnt through a float reciprocal: exact here since t < 5*cnt <= 5*P
-      int row = (int)(((float)t + 0.5f) * (1.0f / (float)cnt));
-      int node = t - row * cnt;
-      const R* rec = reinterpret_cast<const R*>(stg) + node;
-      const double* sca = stg + P * RD + node;
-      double packed = RecFmt<R>::packed(reinterpret_cast<const R*>(stg), cnt, node);
+    q.act = !q.timeout && t < 5 * q.cnt;
+    if (!q.act) return;
+    const int cnt = q.cnt;
+    // t / cnt through a float reciprocal: exact here since t < 5*cnt <= 5*P
+    const int row = (int)(((float)t + 0.5f) * (1.0f / (float)cnt));
+    const int node = t - row * cnt;
+    q.row = row;
+    q.node = node;
+    const double* stg = stage0 + ls * sdoubles;
+    const R* rec = reinterpret_cast<const R*>(stg) + node;
+    const double* sca = stg + P * RD + node;
+    const double packed = RecFmt<R>::packed(reinterpret_cast<const R*>(stg), cnt, node);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int w = nbr_local(packed, d);
+      q.w[d] = w;
+      if (w >= 0) {
+        const R* mr = rec + (25 * d + 5 * row) * cnt;
+#pragma unroll
+        for (int c = 0; c < 5; ++c) q.m[d][c] = mr[c * cnt];
+      }
+    }
+    q.rhs = fwd ? sca[row * cnt] : stg[P * (RD + kSca) + row * cnt + node];
+    q.diag = sca[5 * cnt];
+    q.invj = sca[6 * cnt];
+    q.rdiag = sca[7 * cnt];
+    q.rinvj = sca[8 * cnt];
+    q.bok = divisors_ok(q.diag, q.invj);
+  };
+  PlaneRegs q;
+  int ls = 0;  // stage of the current step and its phase parity
+  unsigned lph = 0;
+  // barrier k (k = 0 before plane 0, k = gs+1 after plane gs) follows the
+  // preload of plane k; a thread whose wait gave up sets slot k&1 before it,
+  // and every consumer reads that slot after it.  A thread one plane ahead
+  // can only write the other slot, so all consumers take the same decision.
+  auto give_up = [&](int k) {
+    abort_slot[k & 1] = 1;
+    abort_flag = 1;
+  };
+  preload(0, 0, 0u, q);
+  if (q.timeout) give_up(0);
+  asm volatile("bar.sync 1, %0;" ::"r"(C) : "memory");
+  for (int gs = 0; gs < 2 * H; ++gs) {
+    if (abort_slot[gs & 1]) {
+      if (threadIdx.x == 0 && status) atomicOr(status, (unsigned)ST_TIMEOUT);
+      return;
+    }
+    const bool fwd = gs < H;
+    if (q.act) {
       double acc[3];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        int w = nbr_local(packed, d);
         double sd = 0.0;
-        if (w >= 0) {
-          const R* mr = rec + (25 * d + 5 * row) * cnt;
-          const double* x = prev + 5 * w;
-          sd = (double)mr[0] * x[0];
-          sd = sd + (double)mr[cnt] * x[1];
-          sd = sd + (double)mr[2 * cnt] * x[2];
-          sd = sd + (double)mr[3 * cnt] * x[3];
-          sd = sd + (double)mr[4 * cnt] * x[4];
+        if (q.w[d] >= 0) {
+          const double* x = prev + 5 * q.w[d];
+          sd = (double)q.m[d][0] * x[0];
+          sd = sd + (double)q.m[d][1] * x[1];
+          sd = sd + (double)q.m[d][2] * x[2];
+          sd = sd + (double)q.m[d][3] * x[3];
+          sd = sd + (double)q.m[d][4] * x[4];
         }
         acc[d] = sd;
       }
       double v;
       if (fwd) {
-        v = div_rn(div_rn(sca[row * cnt] + (acc[0] + acc[1] + acc[2]), sca[5 * cnt], sca[7 * cnt]), sca[6 * cnt],
-                   sca[8 * cnt]);
-        g_dqs[8 * base + row * cnt + node] = v;
+        v = div2_rn(q.rhs + (acc[0] + acc[1] + acc[2]), q.diag, q.rdiag, q.invj, q.rinvj, q.bok);
+        g_dqs[8 * q.base + q.row * q.cnt + q.node] = v;
       } else {
-        double ds = stg[P * (RD + kSca) + row * cnt + node];
-        v = ds - div_rn(div_rn(acc[0] + acc[1] + acc[2], sca[6 * cnt], sca[8 * cnt]), sca[5 * cnt], sca[7 * cnt]);
-        g_dq[5 * (base + node) + row] = v;
+        v = q.rhs - div2_rn(acc[0] + acc[1] + acc[2], q.invj, q.rinvj, q.diag, q.rdiag, q.bok);
+        g_dq[5 * (q.base + q.node) + q.row] = v;
       }
-      cur[5 * node + row] = v;
+      cur[5 * q.node + q.row] = v;
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[ls]);
     if (gs == H - 1) {
       // every thread orders its dq* stores before the backward bulk copies
-      // read them; the producer waits for all consumer warps
+      // read them; the producer waits for all consumer warps (before any
+      // consumer waits for a backward stage, whose dq* copy needs this)
       asm volatile("fence.proxy.async.global;" ::: "memory");
       __syncwarp();
       if (lane == 0) mbar_arrive(fwd_done);
-    }
-    if (consumers_sync_or(timeout, C)) {
-      abort_flag = 1;
-      if (threadIdx.x == 0 && status) atomicOr(status, (unsigned)ST_TIMEOUT);
-      return;
     }
     if (++ls == nst) {
       ls = 0;
       lph ^= 1u;
     }
+    if (gs + 1 < 2 * H) {
+      preload(gs + 1, ls, lph, q);
+      if (q.timeout) give_up(gs + 1);
+    }
+    // the barrier orders this plane's ring writes before the next plane's
+    // reads, and a timeout flag before every consumer's check
+    asm volatile("bar.sync 1, %0;" ::"r"(C) : "memory");
     // the first plane of each pass has no neighbours in the previous one, so
     // the ring needs no reset between passes
     const double* tmp = prev;
@@ -709,8 +752,9 @@ __device__ __forceinline__ double lusgs_row_l2(const R* rec, const double* sca, 
   }
   const double diag = sca[5 * cnt + t], invj = sca[6 * cnt + t];
   const double rdiag = sca[7 * cnt + t], rinvj = sca[8 * cnt + t];
-  if (FWD) return div_rn(div_rn(sca[row * cnt + t] + (acc[0] + acc[1] + acc[2]), diag, rdiag), invj, rinvj);
-  return __ldcg(dsv + row * cnt + t) - div_rn(div_rn(acc[0] + acc[1] + acc[2], invj, rinvj), diag, rdiag);
+  const bool bok = divisors_ok(diag, invj);
+  if (FWD) return div2_rn(sca[row * cnt + t] + (acc[0] + acc[1] + acc[2]), diag, rdiag, invj, rinvj, bok);
+  return __ldcg(dsv + row * cnt + t) - div2_rn(acc[0] + acc[1] + acc[2], invj, rinvj, diag, rdiag, bok);
 }
 
 }  // namespace
@@ -720,6 +764,7 @@ __device__ __forceinline__ double lusgs_row_l2(const R* rec, const double* sca, 
 struct RowRecs {
   double packed, m[15], rhs, diag, invj, rdiag, rinvj;
   int row, node;
+  bool bok;  // divisors_ok(diag, invj)
 };
 template <typename R>
 __device__ __forceinline__ void load_row_recs(const R* rec, const double* sca, int cnt, int t, RowRecs& r) {
@@ -737,6 +782,7 @@ __device__ __forceinline__ void load_row_recs(const R* rec, const double* sca, i
   r.invj = sn[6 * cnt];
   r.rdiag = sn[7 * cnt];
   r.rinvj = sn[8 * cnt];
+  r.bok = divisors_ok(r.diag, r.invj);
 }
 // lusgs_rows' arithmetic for one row from preloaded records; the previous
 // plane's dq and dq* are loaded from L2 (written by other SMs during the sweep).
@@ -758,9 +804,9 @@ __device__ __forceinline__ double row_from_recs(const RowRecs& r, const double* 
     }
     acc[d] = sd;
   }
-  if (FWD) return div_rn(div_rn(r.rhs + (acc[0] + acc[1] + acc[2]), r.diag, r.rdiag), r.invj, r.rinvj);
+  if (FWD) return div2_rn(r.rhs + (acc[0] + acc[1] + acc[2]), r.diag, r.rdiag, r.invj, r.rinvj, r.bok);
   return __ldcg(dsv + r.row * cnt + r.node) -
-         div_rn(div_rn(acc[0] + acc[1] + acc[2], r.invj, r.rinvj), r.diag, r.rdiag);
+         div2_rn(acc[0] + acc[1] + acc[2], r.invj, r.rinvj, r.diag, r.rdiag, r.bok);
 }
 
 // The global-memory sweeps of one block spread over a thread-block cluster
@@ -890,9 +936,9 @@ __device__ __forceinline__ double row_from_ring(const RowRecs& r, const double* 
     }
     acc[d] = sd;
   }
-  if (FWD) return div_rn(div_rn(r.rhs + (acc[0] + acc[1] + acc[2]), r.diag, r.rdiag), r.invj, r.rinvj);
+  if (FWD) return div2_rn(r.rhs + (acc[0] + acc[1] + acc[2]), r.diag, r.rdiag, r.invj, r.rinvj, r.bok);
   return __ldcg(dsv + r.row * cnt + r.node) -
-         div_rn(div_rn(acc[0] + acc[1] + acc[2], r.invj, r.rinvj), r.diag, r.rdiag);
+         div2_rn(acc[0] + acc[1] + acc[2], r.invj, r.rinvj, r.diag, r.rdiag, r.bok);
 }
 
 }  // namespace
