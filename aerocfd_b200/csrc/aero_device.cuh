@@ -90,11 +90,13 @@ constexpr int kSca = 10;
 constexpr int kSaRec = 10;
 
 // Three plane-local indices (+1; 0 = no neighbour) in one 64-bit word: the
-// neighbours' positions in their hyperplane relative to its first node.
+// neighbours' positions in their hyperplane relative to its first node.  Bit
+// 63, unused by the indices, marks an LU-SGS node whose divisors fall outside
+// div2_rn's fast range.
 constexpr int kNbrBits = 21;
 #ifdef __CUDACC__
-__device__ __forceinline__ double pack_nbrs(const int* nb, long prev_base) {
-  unsigned long long u = 0;
+__device__ __forceinline__ double pack_nbrs(const int* nb, long prev_base, bool slow_div = false) {
+  unsigned long long u = slow_div ? 1ull << 63 : 0ull;
 #pragma unroll
   for (int e = 0; e < 3; ++e) {
     unsigned long long f = nb[e] < 0 ? 0ull : (unsigned long long)(nb[e] - prev_base + 1);
@@ -106,6 +108,7 @@ __device__ __forceinline__ int nbr_local(double packed, int e) {
   unsigned long long u = (unsigned long long)__double_as_longlong(packed);
   return (int)((u >> (kNbrBits * e)) & ((1ull << kNbrBits) - 1)) - 1;
 }
+__device__ __forceinline__ bool nbr_slow_div(double packed) { return __double2hiint(packed) < 0; }
 #endif
 
 
@@ -143,8 +146,8 @@ __device__ __forceinline__ double div_rn(double a, double b, double rb) {
 // The two divisions of a sweep row, (a / b1) / b2, with the stored
 // reciprocals rb1, rb2.  div_rn's corrections are exact while a, b and the
 // quotient lie within (2^-960, 2^960).  With both divisors within
-// (2^-200, 2^200) (divisors_ok, tested per node before the row's plane
-// starts) and |a| within (2^-500, 2^500), the first quotient lies within
+// (2^-200, 2^200) (divisors_ok, tested once per node when its records are
+// made) and |a| within (2^-500, 2^500), the first quotient lies within
 // (2^-700, 2^700) and the second within (2^-900, 2^900), so only a is tested
 // on the plane-to-plane chain.  Every other case, zero included, takes the
 // IEEE divisions in a function of its own, which keeps the division's long

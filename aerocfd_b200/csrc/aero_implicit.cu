@@ -208,9 +208,11 @@ __device__ __forceinline__ void lusgs_mats_body(const BlockView* __restrict__ bl
     sc[6 * cnt] = invj;
     sc[7 * cnt] = 1.0 / diag;
     sc[8 * cnt] = 1.0 / invj;
-    RecFmt<R>::set_packed(recs<R>(B, true) + W * base, (int)cnt, lt, pack_nbrs(nb, h > 0 ? B.poff[h - 1] : 0));
+    const bool slow = !divisors_ok(diag, invj);
+    RecFmt<R>::set_packed(recs<R>(B, true) + W * base, (int)cnt, lt,
+                          pack_nbrs(nb, h > 0 ? B.poff[h - 1] : 0, slow));
     RecFmt<R>::set_packed(recs<R>(B, false) + W * base, (int)cnt, lt,
-                          pack_nbrs(nb + 3, h + 1 < B.nplanes ? B.poff[h + 1] : 0));
+                          pack_nbrs(nb + 3, h + 1 < B.nplanes ? B.poff[h + 1] : 0, slow));
   }
   const int up = nb[3 + d];    // forward consumer: the neighbour one step up in d
   const int down = nb[d];      // backward consumer: one step down
@@ -328,6 +330,11 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
 __device__ __forceinline__ void bulk_prefetch_l2(const void* src, unsigned bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
 }
+// Row t / cnt of item t < 5*cnt of a plane, by comparisons (no division).
+__device__ __forceinline__ int row_of(int t, int cnt) {
+  return (t >= cnt) + (t >= 2 * cnt) + (t >= 3 * cnt) + (t >= 4 * cnt);
+}
+
 template <typename R>
 __device__ __forceinline__ double row_dot5(const R* m, int mst, const double* x, int xst) {
   double s = (double)m[0] * x[0];
@@ -363,7 +370,7 @@ __device__ __forceinline__ void lusgs_rows(const R* rec, const double* sca, cons
   }
   const double diag = sca[5 * cnt + t], invj = sca[6 * cnt + t];
   const double rdiag = sca[7 * cnt + t], rinvj = sca[8 * cnt + t];
-  const bool bok = divisors_ok(diag, invj);
+  const bool bok = !nbr_slow_div(packed);
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     if (k < nr) {
@@ -504,7 +511,7 @@ __device__ __forceinline__ void lusgs_staged_body(const BlockView* __restrict__ 
     int w[3];
     R m[3][5];
     double rhs, diag, invj, rdiag, rinvj;  // rhs: rhs (forward) or dq* (backward)
-    bool bok;                              // divisors_ok(diag, invj)
+    bool bok;                              // divisors in div2_rn's fast range
   };
   auto preload = [&](int gs, int ls, unsigned lph, PlaneRegs& q) {
     const bool fwd = gs < H;
@@ -523,8 +530,7 @@ __device__ __forceinline__ void lusgs_staged_body(const BlockView* __restrict__ 
     q.act = !q.timeout && t < 5 * q.cnt;
     if (!q.act) return;
     const int cnt = q.cnt;
-    // t / cnt through a float reciprocal: exact here since t < 5*cnt <= 5*P
-    const int row = (int)(((float)t + 0.5f) * (1.0f / (float)cnt));
+    const int row = row_of(t, cnt);
     const int node = t - row * cnt;
     q.row = row;
     q.node = node;
@@ -547,7 +553,7 @@ __device__ __forceinline__ void lusgs_staged_body(const BlockView* __restrict__ 
     q.invj = sca[6 * cnt];
     q.rdiag = sca[7 * cnt];
     q.rinvj = sca[8 * cnt];
-    q.bok = divisors_ok(q.diag, q.invj);
+    q.bok = !nbr_slow_div(packed);
   };
   PlaneRegs q;
   int ls = 0;  // stage of the current step and its phase parity
@@ -752,7 +758,7 @@ __device__ __forceinline__ double lusgs_row_l2(const R* rec, const double* sca, 
   }
   const double diag = sca[5 * cnt + t], invj = sca[6 * cnt + t];
   const double rdiag = sca[7 * cnt + t], rinvj = sca[8 * cnt + t];
-  const bool bok = divisors_ok(diag, invj);
+  const bool bok = !nbr_slow_div(packed);
   if (FWD) return div2_rn(sca[row * cnt + t] + (acc[0] + acc[1] + acc[2]), diag, rdiag, invj, rinvj, bok);
   return __ldcg(dsv + row * cnt + t) - div2_rn(acc[0] + acc[1] + acc[2], invj, rinvj, diag, rdiag, bok);
 }
@@ -764,11 +770,11 @@ __device__ __forceinline__ double lusgs_row_l2(const R* rec, const double* sca, 
 struct RowRecs {
   double packed, m[15], rhs, diag, invj, rdiag, rinvj;
   int row, node;
-  bool bok;  // divisors_ok(diag, invj)
+  bool bok;  // divisors in div2_rn's fast range
 };
 template <typename R>
 __device__ __forceinline__ void load_row_recs(const R* rec, const double* sca, int cnt, int t, RowRecs& r) {
-  r.row = t / cnt;
+  r.row = row_of(t, cnt);
   r.node = t - r.row * cnt;
   const R* rn = rec + r.node;
   r.packed = RecFmt<R>::packed(rec, cnt, r.node);
@@ -782,7 +788,7 @@ __device__ __forceinline__ void load_row_recs(const R* rec, const double* sca, i
   r.invj = sn[6 * cnt];
   r.rdiag = sn[7 * cnt];
   r.rinvj = sn[8 * cnt];
-  r.bok = divisors_ok(r.diag, r.invj);
+  r.bok = !nbr_slow_div(r.packed);
 }
 // lusgs_rows' arithmetic for one row from preloaded records; the previous
 // plane's dq and dq* are loaded from L2 (written by other SMs during the sweep).
@@ -869,7 +875,7 @@ __device__ __forceinline__ void lusgs_cluster_body(const BlockView* __restrict__
         B.dq[5 * (base + pre.node) + pre.row] = v;
     }
     for (int t = g + G; t < 5 * cnt; t += G) {
-      const int row = t / cnt;
+      const int row = row_of(t, cnt);
       const int node = t - row * cnt;
       if (fwd)
         B.dqs[8 * base + row * cnt + node] = lusgs_row_l2<true, R>(rec, sca, dsv, cnt, node, row, prev, pst, wst);

@@ -134,6 +134,40 @@ def test_viscous_dt_implicit_transient(gpu, oracle_mod):
     gc.close()
 
 
+def test_implicit_slow_divisors_transient(gpu, oracle_mod):
+    """LU-SGS with J^-1 scaled by 2^-230 on every other node: those rows take
+    the IEEE divisions (divisors outside the fast range), the others the
+    corrected reciprocal products; both must match the oracle's divisions."""
+    oc, co, cg = prepared(bump_ns, oracle_mod, seed=5)
+    gc = gpu.GpuCase(cg)
+    b = co.blocks[0]
+    oc.getpri_all()
+    F = b.fields
+    c = co.cfg
+    consts = oc.consts()
+    ob = oracle_mod.box_args
+    oc.L.oracle_viscous_flux(*[_p(F[k]) for k in ("rhsv", "pri_v", "amu", "vor", "dudx", "tao", "dxidx", "inv_j")],
+                             _d(c.tinf), _d(0.72), _d(0.9), _d(1.4), _d(consts[5]), _d(c.re),
+                             *ob(b.box), *ob(b.box0), *ob(b.box1), _i(1))
+    oo = [ctypes.c_double(0) for _ in range(4)]
+    cfl_o = ctypes.c_double(c.cfl)
+    oc.L.oracle_find_dt(_p(F["dt"]), *[ctypes.byref(x) for x in oo], _p(F["pri_v"]), _p(F["amu"]),
+                        _p(F["dxidx"]), _d(c.re), ctypes.byref(cfl_o), *ob(b.box), _i(0), _i(0), _i(1))
+    tiny = np.zeros(F["inv_j"].shape, dtype=bool)
+    tiny.flat[::2] = True
+    F["inv_j"][tiny] *= 2.0 ** -230
+    f = {k: v.copy() for k, v in F.items()}
+    args = ("q", "dt", "pri_v", "rhs", "rhsi", "rhsv", "dxidx", "inv_j")
+    assert gc.L.aero_implicit1st(*[_p(f[k]) for k in args], *[_i(v) for v in b.box + b.box0 + b.box1],
+                                 _d(1.4), _d(c.cfl), _p(f["x"]), _p(f["y"]), _p(f["z"])) == 0
+    oc.L.oracle_implicit1st(*[_p(F[k]) for k in args], *ob(b.box), *ob(b.box0), *ob(b.box1), _d(1.4),
+                            _d(c.cfl), _p(F["x"]), _p(F["y"]), _p(F["z"]))
+    assert np.all(np.isfinite(f["q"]))
+    assert relerr(f["q"], F["q"]) <= TOL
+    assert relerr(f["rhs"], F["rhs"]) <= TOL
+    gc.close()
+
+
 # ------------------------------------------------------- whole iterations
 def run_parity(make, oracle_mod, gpu, nsteps, seed=0, check_every=1):
     oc, co, cg = prepared(make, oracle_mod, seed=seed)
