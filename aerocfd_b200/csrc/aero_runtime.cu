@@ -1333,17 +1333,58 @@ int aero_finish_setup(void) {
   return AERO_OK;
 }
 
+// Every registered array of the mask, in batches that share the staging
+// buffer (up to 64 MiB, or one array if larger): uploads issue all of a
+// batch's host-to-device copies back to back and then the transposes,
+// downloads the transposes and then all copies, so the copy engine streams
+// the batch without waiting on a kernel between arrays.
 static int sync_fields(unsigned long long mask, bool to_device) {
   int rc = need_setup();
   if (rc) return rc;
+  struct Item {
+    double* host;
+    double* dev;
+    long n;
+    int nc;
+    long plane;
+    size_t off;
+  };
+  std::vector<Item> items;
   for (int m = 0; m < (int)g.blocks.size(); ++m) {
     HostBlock& H = g.blocks[m];
-    for (int f = 0; f < kNumPublicFields; ++f) {
-      if (!(mask & (1ull << f)) || !H.host[f]) continue;
-      rc = to_device ? upload(H.host[f], g.views[m].f[f], H.b.size(), field_nc(f), H.plane)
-                     : download(H.host[f], g.views[m].f[f], H.b.size(), field_nc(f), H.plane);
-      if (rc) return rc;
+    for (int f = 0; f < kNumPublicFields; ++f)
+      if ((mask & (1ull << f)) && H.host[f]) items.push_back({H.host[f], g.views[m].f[f], H.b.size(), field_nc(f), H.plane, 0});
+  }
+  const size_t cap = (size_t)8 << 20;  // doubles per batch
+  for (size_t i = 0; i < items.size();) {
+    size_t j = i, total = 0;
+    while (j < items.size()) {
+      size_t len = ((size_t)items[j].n * items[j].nc + 31) / 32 * 32;  // 256-byte aligned slots
+      if (j > i && total + len > cap) break;
+      items[j].off = total;
+      total += len;
+      ++j;
     }
+    if ((rc = ensure_staging(total))) return rc;
+    for (int pass = 0; pass < 2; ++pass) {
+      for (size_t k = i; k < j; ++k) {
+        const Item& it = items[k];
+        double* st = g.d_staging + it.off;
+        const size_t bytes = (size_t)it.n * it.nc * sizeof(double);
+        if (to_device && pass == 0) {
+          CK(cudaMemcpyAsync(st, it.host, bytes, cudaMemcpyHostToDevice, g.stream));
+        } else if (to_device) {
+          PROF(P_TRANSFER, (k_aos_to_soa<<<cdiv(it.n, 256), 256, 0, g.stream>>>(st, it.dev, it.n, it.nc, it.plane)));
+          CKL();
+        } else if (pass == 0) {
+          PROF(P_TRANSFER, (k_soa_to_aos<<<cdiv(it.n, 256), 256, 0, g.stream>>>(it.dev, st, it.n, it.nc, it.plane)));
+          CKL();
+        } else {
+          CK(cudaMemcpyAsync(it.host, st, bytes, cudaMemcpyDeviceToHost, g.stream));
+        }
+      }
+    }
+    i = j;
   }
   CK(cudaStreamSynchronize(g.stream));
   return AERO_OK;
