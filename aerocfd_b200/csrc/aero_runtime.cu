@@ -69,6 +69,7 @@ struct State {
   cudaStream_t stream2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaEvent_t ev_fork2 = nullptr, ev_join2 = nullptr;  // inviscid beside viscous + find_dt
+  std::vector<cudaEvent_t> xfer_ev;  // host transfers: one per array of a batch, plus one
   // dynamic shared memory limits already raised on this device (cudaFuncSetAttribute
   // is per device), per sweep kernel [FP64 records, FP32 records]
   size_t smem_staged[2] = {0, 0}, smem_bulk[2] = {0, 0};
@@ -910,6 +911,8 @@ int aero_finalize(void) {
   cudaEventDestroy(g.ev_join); g.ev_join = nullptr;
   cudaEventDestroy(g.ev_fork2); g.ev_fork2 = nullptr;
   cudaEventDestroy(g.ev_join2); g.ev_join2 = nullptr;
+  for (cudaEvent_t e : g.xfer_ev) cudaEventDestroy(e);
+  g.xfer_ev.clear();
   g.inited = false;
   g.configured = false;
   // execution options of the finished run
@@ -1334,10 +1337,11 @@ int aero_finish_setup(void) {
 }
 
 // Every registered array of the mask, in batches that share the staging
-// buffer (up to 64 MiB, or one array if larger): uploads issue all of a
-// batch's host-to-device copies back to back and then the transposes,
-// downloads the transposes and then all copies, so the copy engine streams
-// the batch without waiting on a kernel between arrays.
+// buffer (up to 64 MiB, or one array if larger).  The copies of a batch run
+// back to back on the main stream and the transposes on the second stream,
+// each array's transpose chained to its own copy by an event: an upload
+// transposes array k while array k+1 is still crossing the bus, a download
+// copies array k while array k+1 is transposed.
 static int sync_fields(unsigned long long mask, bool to_device) {
   int rc = need_setup();
   if (rc) return rc;
@@ -1366,23 +1370,43 @@ static int sync_fields(unsigned long long mask, bool to_device) {
       ++j;
     }
     if ((rc = ensure_staging(total))) return rc;
-    for (int pass = 0; pass < 2; ++pass) {
-      for (size_t k = i; k < j; ++k) {
-        const Item& it = items[k];
-        double* st = g.d_staging + it.off;
-        const size_t bytes = (size_t)it.n * it.nc * sizeof(double);
-        if (to_device && pass == 0) {
-          CK(cudaMemcpyAsync(st, it.host, bytes, cudaMemcpyHostToDevice, g.stream));
-        } else if (to_device) {
-          PROF(P_TRANSFER, (k_aos_to_soa<<<cdiv(it.n, 256), 256, 0, g.stream>>>(st, it.dev, it.n, it.nc, it.plane)));
-          CKL();
-        } else if (pass == 0) {
-          PROF(P_TRANSFER, (k_soa_to_aos<<<cdiv(it.n, 256), 256, 0, g.stream>>>(it.dev, st, it.n, it.nc, it.plane)));
-          CKL();
-        } else {
-          CK(cudaMemcpyAsync(it.host, st, bytes, cudaMemcpyDeviceToHost, g.stream));
-        }
+    while (g.xfer_ev.size() < j - i + 1) {
+      cudaEvent_t e = nullptr;
+      CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      g.xfer_ev.push_back(e);
+    }
+    cudaEvent_t* ev = g.xfer_ev.data();
+    const size_t last = j - i;  // the event joining the two streams
+    if (!to_device) {
+      // the transposes wait for everything before them on the main stream
+      CK(cudaEventRecord(ev[last], g.stream));
+      CK(cudaStreamWaitEvent(g.stream2, ev[last], 0));
+    }
+    for (size_t k = i; k < j; ++k) {
+      const Item& it = items[k];
+      double* st = g.d_staging + it.off;
+      const size_t bytes = (size_t)it.n * it.nc * sizeof(double);
+      if (to_device) {
+        CK(cudaMemcpyAsync(st, it.host, bytes, cudaMemcpyHostToDevice, g.stream));
+        CK(cudaEventRecord(ev[k - i], g.stream));
+        CK(cudaStreamWaitEvent(g.stream2, ev[k - i], 0));
+        PROF_ON(P_TRANSFER, g.stream2,
+                (k_aos_to_soa<<<cdiv(it.n, 256), 256, 0, g.stream2>>>(st, it.dev, it.n, it.nc, it.plane)));
+        CKL();
+      } else {
+        PROF_ON(P_TRANSFER, g.stream2,
+                (k_soa_to_aos<<<cdiv(it.n, 256), 256, 0, g.stream2>>>(it.dev, st, it.n, it.nc, it.plane)));
+        CKL();
+        CK(cudaEventRecord(ev[k - i], g.stream2));
+        CK(cudaStreamWaitEvent(g.stream, ev[k - i], 0));
+        CK(cudaMemcpyAsync(it.host, st, bytes, cudaMemcpyDeviceToHost, g.stream));
       }
+    }
+    if (to_device) {
+      // later work on the main stream (and the next batch's copies into the
+      // staging buffer) waits for the transposes
+      CK(cudaEventRecord(ev[last], g.stream2));
+      CK(cudaStreamWaitEvent(g.stream, ev[last], 0));
     }
     i = j;
   }
