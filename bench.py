@@ -65,8 +65,8 @@ KERNEL_BYTES = {
     "k_getpri": 12 * 8,        # q read; pri write
 }
 # DRAM bytes (read + write) per launch of the dominant kernel on this workload,
-# from one ncu capture (profiles/k_lusgs_sweep_staged_naca0012.md).
-KERNEL_TRAFFIC = {"k_lusgs_sweep": 42.97e6 + 0.09e6}
+# from one ncu capture of it (--set full, cold cache under replay).
+KERNEL_TRAFFIC = {"k_lusgs_sweep": 42.97e6 + 0.04e6}
 # The whole iteration's compulsory footprint for Euler/laminar FP64: read q,
 # dxidx, inv_j, write q, dq* write+read = 30 words per node.
 ITER_BYTES = 240
