@@ -400,7 +400,7 @@ __device__ __forceinline__ void lusgs_rows(const R* rec, const double* sca, cons
 // fence and the `fwd_done` mbarrier.  Every wait is bounded: a consumer that
 // gives up makes all consumers stop at the next plane barrier and raise
 // ST_TIMEOUT; the producer then waits (bounded) for its copies in flight.
-template <typename R, bool kPreloadRows>
+template <typename R>
 __device__ __forceinline__ void lusgs_staged_body(const BlockView* __restrict__ blocks, int nst, unsigned* status) {
   constexpr int RD = RecFmt<R>::kWords * (int)sizeof(R) / 8;  // record words per node, in doubles
   const BlockView& B = blocks[blockIdx.x];
@@ -509,7 +509,6 @@ __device__ __forceinline__ void lusgs_staged_body(const BlockView* __restrict__ 
     int cnt, row, node;
     bool act, timeout;
     int w[3];
-    R m[3][5];
     double rhs, diag, invj, rdiag, rinvj;  // rhs: rhs (forward) or dq* (backward)
     bool bok;                              // divisors in div2_rn's fast range
   };
@@ -539,15 +538,7 @@ __device__ __forceinline__ void lusgs_staged_body(const BlockView* __restrict__ 
     const double* sca = stg + P * RD + node;
     const double packed = RecFmt<R>::packed(reinterpret_cast<const R*>(stg), cnt, node);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      const int w = nbr_local(packed, d);
-      q.w[d] = w;
-      if (kPreloadRows && w >= 0) {
-        const R* mr = rec + (25 * d + 5 * row) * cnt;
-#pragma unroll
-        for (int c = 0; c < 5; ++c) q.m[d][c] = mr[c * cnt];
-      }
-    }
+    for (int d = 0; d < 3; ++d) q.w[d] = nbr_local(packed, d);
     q.rhs = fwd ? sca[row * cnt] : stg[P * (RD + kSca) + row * cnt + node];
     q.diag = sca[5 * cnt];
     q.invj = sca[6 * cnt];
@@ -576,7 +567,6 @@ __device__ __forceinline__ void lusgs_staged_body(const BlockView* __restrict__ 
     }
     const bool fwd = gs < H;
     if (q.act) {
-      // without the preload, the block rows come from this plane's stage now
       const R* rec = reinterpret_cast<const R*>(stage0 + ls * sdoubles) + q.node;
       double acc[3];
 #pragma unroll
@@ -584,16 +574,12 @@ __device__ __forceinline__ void lusgs_staged_body(const BlockView* __restrict__ 
         double sd = 0.0;
         if (q.w[d] >= 0) {
           const double* x = prev + 5 * q.w[d];
-          if (!kPreloadRows) {
-            const R* mr = rec + (25 * d + 5 * q.row) * q.cnt;
-#pragma unroll
-            for (int c = 0; c < 5; ++c) q.m[d][c] = mr[c * q.cnt];
-          }
-          sd = (double)q.m[d][0] * x[0];
-          sd = sd + (double)q.m[d][1] * x[1];
-          sd = sd + (double)q.m[d][2] * x[2];
-          sd = sd + (double)q.m[d][3] * x[3];
-          sd = sd + (double)q.m[d][4] * x[4];
+          const R* mr = rec + (25 * d + 5 * q.row) * q.cnt;
+          sd = (double)mr[0] * x[0];
+          sd = sd + (double)mr[q.cnt] * x[1];
+          sd = sd + (double)mr[2 * q.cnt] * x[2];
+          sd = sd + (double)mr[3 * q.cnt] * x[3];
+          sd = sd + (double)mr[4 * q.cnt] * x[4];
         }
         acc[d] = sd;
       }
@@ -636,24 +622,15 @@ __device__ __forceinline__ void lusgs_staged_body(const BlockView* __restrict__ 
   }
 }
 
-__global__ void k_lusgs_sweep_staged(const BlockView* __restrict__ blocks, int nst, unsigned* status) {
-  lusgs_staged_body<double, true>(blocks, nst, status);
-}
-__global__ void k_lusgs_sweep_staged_f32(const BlockView* __restrict__ blocks, int nst, unsigned* status) {
-  lusgs_staged_body<float, true>(blocks, nst, status);
-}
-// The same sweeps within 64 registers per thread, so that one CTA can hold the
-// 5 rows of every node of planes up to 198 nodes (1024 threads); used when the
-// first kernels' register count does not allow that many threads.  The block
-// rows are read from the stage after the plane barrier instead of being held
-// in registers across it.
+// 64 registers per thread at most, so that one CTA can hold the 5 rows of
+// every node of planes up to 198 nodes (1024 threads).
 __global__ void __launch_bounds__(1024, 1)
-    k_lusgs_sweep_staged_wide(const BlockView* __restrict__ blocks, int nst, unsigned* status) {
-  lusgs_staged_body<double, false>(blocks, nst, status);
+    k_lusgs_sweep_staged(const BlockView* __restrict__ blocks, int nst, unsigned* status) {
+  lusgs_staged_body<double>(blocks, nst, status);
 }
 __global__ void __launch_bounds__(1024, 1)
-    k_lusgs_sweep_staged_wide_f32(const BlockView* __restrict__ blocks, int nst, unsigned* status) {
-  lusgs_staged_body<float, false>(blocks, nst, status);
+    k_lusgs_sweep_staged_f32(const BlockView* __restrict__ blocks, int nst, unsigned* status) {
+  lusgs_staged_body<float>(blocks, nst, status);
 }
 
 // The same sweeps with the records read from global memory, for blocks whose

@@ -98,9 +98,6 @@ __global__ void k_lusgs_sweep_global(const BlockView* __restrict__ blocks, int n
 __global__ void k_lusgs_sweep_cluster(const BlockView* __restrict__ blocks);
 // the same with the off-diagonal blocks stored in FP32 (mixed precision)
 __global__ void k_lusgs_sweep_staged_f32(const BlockView* __restrict__ blocks, int nst, unsigned* status);
-// the staged sweeps limited to 64 registers (planes up to 198 nodes in one CTA)
-__global__ void k_lusgs_sweep_staged_wide(const BlockView* __restrict__ blocks, int nst, unsigned* status);
-__global__ void k_lusgs_sweep_staged_wide_f32(const BlockView* __restrict__ blocks, int nst, unsigned* status);
 __global__ void k_lusgs_sweep_global_f32(const BlockView* __restrict__ blocks, int nst, unsigned* status);
 __global__ void k_lusgs_sweep_cluster_f32(const BlockView* __restrict__ blocks);
 // cluster sweeps exchanging plane values by bulk copies between shared memories

@@ -72,7 +72,7 @@ struct State {
   std::vector<cudaEvent_t> xfer_ev;  // host transfers: one per array of a batch, plus one
   // dynamic shared memory limits already raised on this device (cudaFuncSetAttribute
   // is per device), per sweep kernel [FP64 records, FP32 records]
-  size_t smem_staged[4] = {0, 0, 0, 0}, smem_bulk[2] = {0, 0};  // staged: [f + 2 * wide]
+  size_t smem_staged[2] = {0, 0}, smem_bulk[2] = {0, 0};
   bool configured = false;
   int iflags[8] = {};
   double params[7] = {};
@@ -519,23 +519,16 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
   size_t stage = (size_t)std::max(pmax, 1) * (rec_words + kSca + 8) * sizeof(double);
   int nst = g.tune.nst_max;
   while (nst >= 2 && offs + ring + nst * stage + (2 * nst + 1) * 8 > kSmemMax) --nst;
-  // the staged kernel, or its 64-register form when the plane needs more
-  // threads than the first one's registers allow (index f + 2 * wide)
-  using SweepKernel = void (*)(const BlockView*, int, unsigned*);
-  const SweepKernel staged_kernels[4] = {k_lusgs_sweep_staged, k_lusgs_sweep_staged_f32, k_lusgs_sweep_staged_wide,
-                                         k_lusgs_sweep_staged_wide_f32};
-  static int staged_max_threads[4] = {0, 0, 0, 0};  // limited by the kernels' registers
-  for (int x = f; x < 4; x += 2)
-    if (!staged_max_threads[x]) {
-      cudaFuncAttributes fa;
-      CK(cudaFuncGetAttributes(&fa, staged_kernels[x]));
-      staged_max_threads[x] = fa.maxThreadsPerBlock;
-    }
+  auto staged = f ? k_lusgs_sweep_staged_f32 : k_lusgs_sweep_staged;
+  static int staged_max_threads[2] = {0, 0};  // limited by the kernel's registers
+  if (!staged_max_threads[f]) {
+    cudaFuncAttributes fa;
+    CK(cudaFuncGetAttributes(&fa, staged));
+    staged_max_threads[f] = fa.maxThreadsPerBlock;
+  }
   // consumer threads: one per row of every node of the largest plane
   auto consumers_for = [](int p) { return (5 * std::max(p, 1) + 31) / 32 * 32; };
-  const int sk = consumers_for(pmax) + 32 <= staged_max_threads[f] ? f : f + 2;
-  auto staged = staged_kernels[sk];
-  if (nst >= 2 && consumers_for(pmax) + 32 > staged_max_threads[sk]) nst = 0;
+  if (nst >= 2 && consumers_for(pmax) + 32 > staged_max_threads[f]) nst = 0;
   const bool bulk = g.tune.sweep_cl >= 2 && g.tune.sweep_x == 1 && 5L * pmax <= 512L * g.tune.sweep_cl;
   if (bulk) {
     // one cluster per block, one thread per row of every node of the largest
@@ -586,9 +579,9 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
   } else if (nst >= 2) {
     int consumers = consumers_for(pmax);
     size_t smem = offs + ring + nst * stage + (2 * nst + 1) * 8;
-    if (smem > 48 * 1024 && smem > g.smem_staged[sk]) {
+    if (smem > 48 * 1024 && smem > g.smem_staged[f]) {
       CK(cudaFuncSetAttribute(staged, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      g.smem_staged[sk] = smem;
+      g.smem_staged[f] = smem;
     }
     PROF(P_LUSGS_SWEEP, (staged<<<nblk, consumers + 32, smem, g.stream>>>(views, nst, g.d_status)));
   } else {
@@ -852,8 +845,7 @@ const char* aero_last_error(void) { return g.err.c_str(); }
 int aero_init(int device) {
   if (g.inited) return AERO_OK;
   CK(cudaSetDevice(device));
-  for (int x = 0; x < 4; ++x) g.smem_staged[x] = 0;
-  for (int f = 0; f < 2; ++f) g.smem_bulk[f] = 0;
+  for (int f = 0; f < 2; ++f) g.smem_staged[f] = g.smem_bulk[f] = 0;
   CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
   CK(cudaStreamCreateWithFlags(&g.stream2, cudaStreamNonBlocking));
   CK(cudaEventCreateWithFlags(&g.ev_fork, cudaEventDisableTiming));
