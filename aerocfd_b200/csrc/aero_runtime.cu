@@ -69,6 +69,7 @@ struct State {
   cudaStream_t stream2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaEvent_t ev_fork2 = nullptr, ev_join2 = nullptr;  // inviscid beside viscous + find_dt
+  cudaEvent_t ev_prep = nullptr, ev_resid = nullptr;   // residual norm beside the LU-SGS sweeps
   std::vector<cudaEvent_t> xfer_ev;  // host transfers: one per array of a batch, plus one
   // dynamic shared memory limits already raised on this device (cudaFuncSetAttribute
   // is per device), per sweep kernel [FP64 records, FP32 records]
@@ -498,12 +499,13 @@ int launch_dt_minmax(const BlockView* views, int m, double* d_out2) {
   return AERO_OK;
 }
 int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, int pmax, int hmax,
-                    const CaseConsts& cc) {
+                    const CaseConsts& cc, cudaEvent_t after_prep = nullptr) {
   // mixed precision stores the off-diagonal blocks in FP32 (products and sums
   // stay FP64); f selects that variant of every kernel that touches them
   const int f = g.mixed ? 1 : 0;
   PROF(P_LUSGS_PREP, (k_lusgs_prep<<<dim3(cdiv(maxExt, g.tune.ew), nblk), g.tune.ew, 0, g.stream>>>(views, cc)));
   CKL();
+  if (after_prep) CK(cudaEventRecord(after_prep, g.stream));
   PROF(P_LUSGS_MATS, ((f ? k_lusgs_mats_f32 : k_lusgs_mats)<<<dim3(cdiv(3 * maxN1, g.tune.mats), nblk), g.tune.mats, 0,
                                                              g.stream>>>(views, cc)));
   CKL();
@@ -666,12 +668,13 @@ int do_average2() {
   CKL();
   return AERO_OK;
 }
-int do_residual(double* d_out7) {
+int do_residual(double* d_out7, cudaStream_t st = nullptr) {
+  if (!st) st = g.stream;
   int nb = (int)g.blocks.size();
-  PROF(P_RESID_PART, (k_residual_partial<<<dim3(g.resid_ctas, nb), 256, 0, g.stream>>>(g.d_blocks, g.d_part, sa_on())));
+  PROF_ON(P_RESID_PART, st, (k_residual_partial<<<dim3(g.resid_ctas, nb), 256, 0, st>>>(g.d_blocks, g.d_part, sa_on())));
   CKL();
-  PROF(P_RESID_FINAL, (k_residual_final<<<1, 256, 0, g.stream>>>(g.d_part, (long)g.resid_ctas * nb,
-                                                                  g.totalnodes, d_out7, g.d_status)));
+  PROF_ON(P_RESID_FINAL, st, (k_residual_final<<<1, 256, 0, st>>>(g.d_part, (long)g.resid_ctas * nb,
+                                                                    g.totalnodes, d_out7, g.d_status)));
   CKL();
   return AERO_OK;
 }
@@ -730,7 +733,11 @@ int do_iteration_crank() {
   return AERO_OK;
 }
 
-int do_iteration(bool want_dt_minmax) {
+// With resid_beside, the residual norm of the iteration (rhs, dt, inv_j and
+// sa_rhs, none of which is written after k_lusgs_prep and sa_model's rhs) is
+// computed on the second stream beside the LU-SGS sweeps, into g.d_out, and
+// g.ev_resid marks its end.
+int do_iteration(bool want_dt_minmax, bool resid_beside = false) {
   if (crank_on()) return do_iteration_crank();
   int nb = (int)g.blocks.size();
   int rc;
@@ -756,7 +763,14 @@ int do_iteration(bool want_dt_minmax) {
     if ((rc = launch_sa(g.d_blocks, nb, g.max_box, g.max_b1, g.pmax_all, g.cc, g.stream2))) return rc;
     CK(cudaEventRecord(g.ev_join, g.stream2));
   }
-  if ((rc = launch_implicit(g.d_blocks, nb, g.max_ext, g.max_b1, g.pmax_all, g.hmax_all, g.cc))) return rc;
+  if ((rc = launch_implicit(g.d_blocks, nb, g.max_ext, g.max_b1, g.pmax_all, g.hmax_all, g.cc,
+                            resid_beside ? g.ev_prep : nullptr)))
+    return rc;
+  if (resid_beside) {
+    CK(cudaStreamWaitEvent(g.stream2, g.ev_prep, 0));
+    if ((rc = do_residual(g.d_out, g.stream2))) return rc;
+    CK(cudaEventRecord(g.ev_resid, g.stream2));
+  }
   if (sa) CK(cudaStreamWaitEvent(g.stream, g.ev_join, 0));
   if ((rc = do_physical_bc())) return rc;
   if ((rc = do_halo())) return rc;
@@ -786,12 +800,16 @@ CaseConsts consts_from(const int* iflags, const double* params) {
 }
 
 // One time step as aero_step runs it: the iteration, the closing primitives
-// and the residual norm (into g.d_out).
+// and the residual norm (into g.d_out; beside the sweeps for the implicit
+// update, after the step for the dual-time one).
 int step_once() {
   int rc;
-  if ((rc = do_iteration(false))) return rc;
+  const bool beside = !crank_on();
+  if ((rc = do_iteration(false, beside))) return rc;
   if ((rc = do_getpri_all())) return rc;
-  return do_residual(g.d_out);
+  if (!beside) return do_residual(g.d_out);
+  CK(cudaStreamWaitEvent(g.stream, g.ev_resid, 0));
+  return AERO_OK;
 }
 
 void graph_release() {
@@ -852,6 +870,8 @@ int aero_init(int device) {
   CK(cudaEventCreateWithFlags(&g.ev_join, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&g.ev_fork2, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&g.ev_join2, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&g.ev_prep, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&g.ev_resid, cudaEventDisableTiming));
   CK(cudaMalloc(&g.d_status, sizeof(unsigned)));
   CK(cudaMemset(g.d_status, 0, sizeof(unsigned)));
   CK(cudaMalloc(&g.d_out, 16 * sizeof(double)));
@@ -911,6 +931,8 @@ int aero_finalize(void) {
   cudaEventDestroy(g.ev_join); g.ev_join = nullptr;
   cudaEventDestroy(g.ev_fork2); g.ev_fork2 = nullptr;
   cudaEventDestroy(g.ev_join2); g.ev_join2 = nullptr;
+  cudaEventDestroy(g.ev_prep); g.ev_prep = nullptr;
+  cudaEventDestroy(g.ev_resid); g.ev_resid = nullptr;
   for (cudaEvent_t e : g.xfer_ev) cudaEventDestroy(e);
   g.xfer_ev.clear();
   g.inited = false;
