@@ -493,12 +493,12 @@ __device__ __forceinline__ void lusgs_staged_body(const BlockView* __restrict__ 
   // Thread t < 5*cnt of a plane computes row t / cnt of node t % cnt (a warp
   // mostly covers consecutive nodes of one row, so its shared-memory reads
   // are consecutive words); warps beyond 5*cnt only take the barrier.  The
-  // ring holds the previous plane's dq node-major (5 per node).  Everything
-  // of a plane that does not depend on the previous plane (its offsets, the
-  // wait for its copies, the row mapping, the thread's block rows, rhs or
-  // dq*, diagonal and J^-1) is loaded into registers before the barrier that
-  // ends the previous plane, so only the neighbours' dq, the block products
-  // and the two divisions remain between two barriers.
+  // ring holds the previous plane's dq node-major (5 per node).  The plane's
+  // offsets, the wait for its copies, the row mapping, the neighbour
+  // positions, rhs or dq*, diagonal and J^-1 are loaded into registers before
+  // the barrier that ends the previous plane; the thread's 15 block entries
+  // are read from the stage after it (holding them across the barrier costs
+  // more registers than it saves).
   const int lane = threadIdx.x & 31;
   double* const g_dqs = B.dqs;
   double* const g_dq = B.dq;
@@ -534,7 +534,6 @@ __device__ __forceinline__ void lusgs_staged_body(const BlockView* __restrict__ 
     q.row = row;
     q.node = node;
     const double* stg = stage0 + ls * sdoubles;
-    const R* rec = reinterpret_cast<const R*>(stg) + node;
     const double* sca = stg + P * RD + node;
     const double packed = RecFmt<R>::packed(reinterpret_cast<const R*>(stg), cnt, node);
 #pragma unroll
