@@ -62,9 +62,10 @@ struct BlockView {
   long* poff;            // nplanes+1 plane offsets
   double* rec_f;         // kRec per node: forward blocks from the i-1, j-1, k-1 neighbours
   double* rec_b;         // kRec per node: backward blocks from the i+1, j+1, k+1 neighbours
-  double* sca;           // 8 per node: rhs(5), diag, inv_j, unused
+  double* sca;           // kSca per node: rhs(5), diag, inv_j, 1/diag, 1/inv_j, unused
   int* nbr;              // 6 per node: hyperplane-major positions of those neighbours (-1: outside)
   long* nat;             // natural (box) index of the node
+  int* pidx;             // per updated-box node in box order: its hyperplane-major position
   double* sa_rec;        // kSaRec per node: SA sweep records (plane-local layout)
   double* sa_dq;         // 1 per node: SA forward-sweep increment
   double* dqs;           // 8 per node: dq* (forward result), padded to 64 bytes

@@ -118,6 +118,7 @@ __global__ void k_plane_index(const BlockView* __restrict__ blocks) {
   const int lim[3] = {nx1, ny1, nz1};
   long pos = plane_pos(B, a, b, c);
   B.nat[pos] = B.at(b1.is + a, b1.js + b, b1.ks + c);
+  B.pidx[u] = (int)pos;
 #pragma unroll
   for (int e = 0; e < 3; ++e) {
     int lo[3] = {a, b, c}, hi[3] = {a, b, c};
@@ -1056,13 +1057,22 @@ __global__ void __launch_bounds__(512, 1) k_lusgs_sweep_bulk_f32(const BlockView
 }
 
 // q = q + dq on every updated node (sub_timeadvancement_1stimplicit.f90:568-574).
+// q += dq over the updated box, walked in box order so that q is read and
+// written along its rows; dq (hyperplane-major, 5 per node) is gathered
+// through the position index.
 __global__ void k_lusgs_update(const BlockView* __restrict__ blocks) {
   const BlockView& B = blocks[blockIdx.y];
-  long pos = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (pos >= B.b1.size()) return;
-  long n = B.nat[pos];
+  const Box& b1 = B.b1;
+  long u = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= b1.size()) return;
+  int i = b1.is + (int)(u % b1.nx());
+  long r = u / b1.nx();
+  int j = b1.js + (int)(r % b1.ny());
+  int k = b1.ks + (int)(r / b1.ny());
+  long n = B.at(i, j, k);
+  const double* dq = B.dq + 5L * B.pidx[u];
 #pragma unroll
-  for (int x = 1; x <= 5; ++x) B.v(F_Q, x, n) = B.v(F_Q, x, n) + B.dq[5 * pos + x - 1];
+  for (int x = 1; x <= 5; ++x) B.v(F_Q, x, n) = B.v(F_Q, x, n) + dq[x - 1];
 }
 
 }  // namespace aero

@@ -277,11 +277,11 @@ void fill_view(BlockView& v, const Box& b, const Box& b0, const Box& b1, long pl
 }
 
 // LU-SGS workspace of one view (see BlockView): one device allocation holding
-// poff, rec_f, rec_b, sca, dqs, dq, sa_rec, sa_dq, nat, nbr.
+// poff, rec_f, rec_b, sca, dqs, dq, sa_rec, sa_dq, nat, nbr, pidx.
 size_t workspace_bytes(const Box& b1, int H) {
   size_t N1 = (size_t)b1.size();
   return (size_t)(H + 1) * sizeof(long) + N1 * (2 * kRec + kSca + 8 + 5 + kSaRec + 1) * sizeof(double) +
-         N1 * sizeof(long) + N1 * 6 * sizeof(int) + 256;
+         N1 * sizeof(long) + N1 * 7 * sizeof(int) + 256;
 }
 int attach_workspace(BlockView& v, void* ws, const std::vector<long>& poff, int pmax) {
   size_t N1 = (size_t)v.b1.size();
@@ -298,6 +298,7 @@ int attach_workspace(BlockView& v, void* ws, const std::vector<long>& poff, int 
   v.nat = (long*)p; p += N1 * sizeof(long);
   v.poff = (long*)p; p += poff.size() * sizeof(long);
   v.nbr = (int*)p;
+  v.pidx = v.nbr + 6 * N1;
   CK(cudaMemcpyAsync(v.poff, poff.data(), poff.size() * sizeof(long), cudaMemcpyHostToDevice, g.stream));
   return AERO_OK;
 }
