@@ -346,7 +346,12 @@ __device__ __forceinline__ double row_dot5(const R* m, int mst, const double* x,
   return s;
 }
 
-constexpr long kSpinLimit = 1L << 20;  // bounded mbarrier wait (well under a second)
+// Bounded mbarrier waits (well under a second).  The staged sweep takes its
+// budget as an argument (aero_set_poll_budget; this is the default and the
+// largest), except for the producer's final wait for its own copies in
+// flight, which always has the full budget so that no copy lands after the
+// CTA has left.
+constexpr long kSpinLimit = 1L << 20;
 
 // Rows r0 .. r0+nr-1 (nr <= 3) of plane-local node `t` of one plane of the
 // sweep: each row of the three neighbour blocks times the neighbours' dq,
@@ -402,7 +407,8 @@ __device__ __forceinline__ void lusgs_rows(const R* rec, const double* sca, cons
 // gives up makes all consumers stop at the next plane barrier and raise
 // ST_TIMEOUT; the producer then waits (bounded) for its copies in flight.
 template <typename R>
-__device__ __forceinline__ void lusgs_staged_body(const BlockView* __restrict__ blocks, int nst, unsigned* status) {
+__device__ __forceinline__ void lusgs_staged_body(const BlockView* __restrict__ blocks, int nst, unsigned* status,
+                                                  long spin_limit, int stall_plane) {
   constexpr int RD = RecFmt<R>::kWords * (int)sizeof(R) / 8;  // record words per node, in doubles
   const BlockView& B = blocks[blockIdx.x];
   extern __shared__ __align__(16) unsigned char smem[];
@@ -440,7 +446,7 @@ __device__ __forceinline__ void lusgs_staged_body(const BlockView* __restrict__ 
     auto wait_bar = [&](unsigned long long* bar, unsigned parity) {
       long spins = 0;
       while (!mbar_try_wait(bar, parity)) {
-        if (abort_flag || ++spins > kSpinLimit) return false;
+        if (abort_flag || ++spins > spin_limit) return false;
       }
       return true;
     };
@@ -449,6 +455,10 @@ __device__ __forceinline__ void lusgs_staged_body(const BlockView* __restrict__ 
     // issue the copies of global step gs (forward: gs < H); with_dqs = false
     // leaves the backward dq* copy for later
     auto issue = [&](int gs, bool with_dqs) {
+      // fault injection: the copies of this forward plane are never issued,
+      // so the consumers' waits for it run out (the producer drains what it
+      // did issue and leaves)
+      if (gs == stall_plane) return false;
       bool fwd = gs < H;
       int h = fwd ? gs : 2 * H - 1 - gs;
       long base = poff[h];
@@ -521,7 +531,7 @@ __device__ __forceinline__ void lusgs_staged_body(const BlockView* __restrict__ 
     q.timeout = false;
     long spins = 0;
     while (!mbar_try_wait(&full[ls], lph)) {
-      if (++spins > kSpinLimit) {
+      if (++spins > spin_limit) {
         q.timeout = true;
         break;
       }
@@ -625,12 +635,14 @@ __device__ __forceinline__ void lusgs_staged_body(const BlockView* __restrict__ 
 // 64 registers per thread at most, so that one CTA can hold the 5 rows of
 // every node of planes up to 198 nodes (1024 threads).
 __global__ void __launch_bounds__(1024, 1)
-    k_lusgs_sweep_staged(const BlockView* __restrict__ blocks, int nst, unsigned* status) {
-  lusgs_staged_body<double>(blocks, nst, status);
+    k_lusgs_sweep_staged(const BlockView* __restrict__ blocks, int nst, unsigned* status, long spin_limit,
+                         int stall_plane) {
+  lusgs_staged_body<double>(blocks, nst, status, spin_limit, stall_plane);
 }
 __global__ void __launch_bounds__(1024, 1)
-    k_lusgs_sweep_staged_f32(const BlockView* __restrict__ blocks, int nst, unsigned* status) {
-  lusgs_staged_body<float>(blocks, nst, status);
+    k_lusgs_sweep_staged_f32(const BlockView* __restrict__ blocks, int nst, unsigned* status, long spin_limit,
+                             int stall_plane) {
+  lusgs_staged_body<float>(blocks, nst, status, spin_limit, stall_plane);
 }
 
 // The same sweeps with the records read from global memory, for blocks whose

@@ -93,11 +93,13 @@ __global__ void k_sa_a(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_b(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_recs(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_sweep(const BlockView* __restrict__ blocks);
-__global__ void k_lusgs_sweep_staged(const BlockView* __restrict__ blocks, int nst, unsigned* status);
+__global__ void k_lusgs_sweep_staged(const BlockView* __restrict__ blocks, int nst, unsigned* status,
+                                     long spin_limit, int stall_plane);
 __global__ void k_lusgs_sweep_global(const BlockView* __restrict__ blocks, int nst, unsigned* status);
 __global__ void k_lusgs_sweep_cluster(const BlockView* __restrict__ blocks);
 // the same with the off-diagonal blocks stored in FP32 (mixed precision)
-__global__ void k_lusgs_sweep_staged_f32(const BlockView* __restrict__ blocks, int nst, unsigned* status);
+__global__ void k_lusgs_sweep_staged_f32(const BlockView* __restrict__ blocks, int nst, unsigned* status,
+                                         long spin_limit, int stall_plane);
 __global__ void k_lusgs_sweep_global_f32(const BlockView* __restrict__ blocks, int nst, unsigned* status);
 __global__ void k_lusgs_sweep_cluster_f32(const BlockView* __restrict__ blocks);
 // cluster sweeps exchanging plane values by bulk copies between shared memories

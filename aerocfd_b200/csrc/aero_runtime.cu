@@ -59,6 +59,10 @@ std::vector<long> plane_offsets(const Box& b1, int& pmax) {
   return off;
 }
 
+// Largest (and default) number of polls of each wait of the staged LU-SGS
+// sweep, the kernel's own bound.
+constexpr long kPollBudgetMax = 1L << 20;
+
 struct State {
   bool inited = false;
   int device = 0;
@@ -74,6 +78,8 @@ struct State {
   // dynamic shared memory limits already raised on this device (cudaFuncSetAttribute
   // is per device), per sweep kernel [FP64 records, FP32 records]
   size_t smem_staged[2] = {0, 0}, smem_bulk[2] = {0, 0};
+  long spin_limit = kPollBudgetMax;  // polls of each staged-sweep wait (aero_set_poll_budget)
+  int stall_plane = -1;              // forward plane whose copies are withheld (aero_inject_sweep_stall)
   bool configured = false;
   int iflags[8] = {};
   double params[7] = {};
@@ -586,7 +592,8 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
       CK(cudaFuncSetAttribute(staged, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       g.smem_staged[f] = smem;
     }
-    PROF(P_LUSGS_SWEEP, (staged<<<nblk, consumers + 32, smem, g.stream>>>(views, nst, g.d_status)));
+    PROF(P_LUSGS_SWEEP, (staged<<<nblk, consumers + 32, smem, g.stream>>>(views, nst, g.d_status, g.spin_limit,
+                                                                          g.stall_plane)));
   } else {
     auto global = f ? k_lusgs_sweep_global_f32 : k_lusgs_sweep_global;
     static int global_max_threads[2] = {0, 0};  // limited by the kernel's registers
@@ -940,6 +947,8 @@ int aero_finalize(void) {
   g.configured = false;
   // execution options of the finished run
   g.mixed = false;
+  g.spin_limit = kPollBudgetMax;
+  g.stall_plane = -1;
   g.tune = State::Tune{};
   g.graph_want = false;
   g.tuning = State{}.tuning;
@@ -1091,6 +1100,25 @@ int aero_set_tuning(int inv_tile, int ew, int visc, int mats, int nst_max) {
   g.tune.nst_max = nst_max;
   graph_release();
   set_tuning_text();
+  return AERO_OK;
+}
+
+int aero_set_poll_budget(long long polls) {
+  int rc = need_init();
+  if (rc) return rc;
+  if (polls < 0 || polls > kPollBudgetMax)
+    return fail(AERO_ERR_ARG, "poll budget %lld is outside 0..%ld", polls, kPollBudgetMax);
+  g.spin_limit = (long)polls;
+  graph_release();
+  return AERO_OK;
+}
+
+int aero_inject_sweep_stall(int plane) {
+  int rc = need_init();
+  if (rc) return rc;
+  if (plane < -1) return fail(AERO_ERR_ARG, "stall plane %d is neither -1 nor a plane index", plane);
+  g.stall_plane = plane;
+  graph_release();
   return AERO_OK;
 }
 

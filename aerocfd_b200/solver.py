@@ -143,6 +143,18 @@ class GpuCase:
         (False) or by bulk copies between the CTAs' shared memories (True)."""
         _lib.check(self.L.aero_set_sweep_exchange(ctypes.c_int(1 if shared else 0)), "aero_set_sweep_exchange")
 
+    def set_poll_budget(self, polls: int) -> None:
+        """aero_set_poll_budget: polls of each bounded wait of the staged LU-SGS
+        sweep (0..2**20, the default); a wait that gives up raises
+        AERO_ST_TIMEOUT in the status word."""
+        _lib.check(self.L.aero_set_poll_budget(ctypes.c_longlong(polls)), "aero_set_poll_budget")
+
+    def inject_sweep_stall(self, plane: int) -> None:
+        """aero_inject_sweep_stall: test hook; the staged LU-SGS sweep never
+        issues the copies of forward hyperplane `plane` (-1: off), so its
+        waits run out and the status word gets AERO_ST_TIMEOUT."""
+        _lib.check(self.L.aero_inject_sweep_stall(ctypes.c_int(plane)), "aero_inject_sweep_stall")
+
     def set_precision(self, mixed: bool) -> None:
         """aero_set_precision: 0 = FP64 reference arithmetic, 1 = mixed."""
         _lib.check(self.L.aero_set_precision(ctypes.c_int(1 if mixed else 0)), "aero_set_precision")

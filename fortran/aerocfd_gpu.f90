@@ -111,6 +111,19 @@ module aerocfd_gpu
       integer(c_int), value :: mode
     end function
 
+    ! polls of each bounded wait of the staged LU-SGS sweep (fault-injection
+    ! hook; default and largest 1048576)
+    integer(c_int) function aero_set_poll_budget(polls) bind(C, name="aero_set_poll_budget")
+      import :: c_int, c_long_long
+      integer(c_long_long), value :: polls
+    end function
+
+    ! fault injection: copies of forward hyperplane `plane` withheld (-1: off)
+    integer(c_int) function aero_inject_sweep_stall(plane) bind(C, name="aero_inject_sweep_stall")
+      import :: c_int
+      integer(c_int), value :: plane
+    end function
+
     integer(c_int) function aero_finish_setup() bind(C, name="aero_finish_setup")
       import :: c_int
     end function

@@ -45,6 +45,8 @@ extern "C" {
 /* device status word bits (aero_get_status) */
 #define AERO_ST_NEG_DENSITY 1u        /* sub_getpri_v.f90:54-56 would print  */
 #define AERO_ST_NONFINITE_RESIDUAL 2u /* NaN/Inf in the residual norm        */
+#define AERO_ST_TIMEOUT 8u            /* an LU-SGS sweep wait ran out of polls
+                                         (that iteration's update is incomplete) */
 
 /* ---- field ids (module_block.f90:20-91 arrays) ------------------------- */
 enum {
@@ -294,6 +296,17 @@ int aero_set_sweep_cluster(int ctas);
  * of the largest plane has its own thread: 5 x plane nodes <= 512 x CTAs).
  * The arithmetic is the same either way. */
 int aero_set_sweep_exchange(int mode);
+/* Polls each bounded wait of the staged LU-SGS sweep (one CTA per block)
+ * makes before it gives up, 0..1048576 (the default); each poll may suspend
+ * the waiting thread for a short, system-dependent time.  A wait that gives
+ * up ends the sweep with AERO_ST_TIMEOUT in the status word and leaves the
+ * context usable. */
+int aero_set_poll_budget(long long polls);
+/* Fault injection for tests: in every staged LU-SGS sweep the copies of
+ * forward hyperplane `plane` (0-based) are never issued, so the waits for
+ * them run out and the sweep ends with AERO_ST_TIMEOUT; -1 (default) turns it
+ * off.  The iteration's update is then incomplete. */
+int aero_inject_sweep_stall(int plane);
 
 /* ---- warm-start network (no counterpart in the reference) --------------
  * aero_mlp_gemm: c[M x N] = a[M x K] * b[N x K]^T on the tcgen05 tensor cores,
