@@ -52,17 +52,17 @@ __device__ __forceinline__ void unit_normal(const BlockView& B, long n, int dir,
   }
 }
 
-// sub_bc.f90:26-62 for the o-th subface of every block (launched once per
-// subface index o, in bcinfo order, so a later subface overwrites shared edge
-// nodes and reads what an earlier one wrote, as in the serial reference).
-// The nodes of one subface are independent and spread over the grid's x.
+// sub_bc.f90:26-62 for the ops of one dependency level (grid y: the level's
+// entries), launched level after level: an op that must see what another op
+// of its block wrote, or must overwrite it, sits in a later level, as the
+// serial reference orders them.  The nodes of one subface are independent
+// and spread over the grid's x.
 __global__ void k_physical_bc(const BlockView* __restrict__ blocks, const BcOp* __restrict__ ops,
-                              const int* __restrict__ op_start, int o, CaseConsts cc_launch) {
-  const BlockView& B = blocks[blockIdx.y];
+                              const BcEntry* __restrict__ list, int first, CaseConsts cc_launch) {
+  const BcEntry e = list[first + blockIdx.y];
+  const BlockView& B = blocks[e.blk];
   const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
-  int idx = op_start[blockIdx.y] + o;
-  if (idx >= op_start[blockIdx.y + 1]) return;
-  const BcOp op = ops[idx];
+  const BcOp op = ops[e.op];
   bool tur = cc.turbulence >= 1;
   double gamma = cc.gamma;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;

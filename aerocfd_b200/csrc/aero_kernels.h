@@ -12,6 +12,10 @@ struct BcOp {
   int face;
   Box sb;  // subface box exactly as the BC routine receives it
 };
+// One op of a physical-BC launch: the op and its block.
+struct BcEntry {
+  int op, blk;
+};
 
 // One ghost node of the halo and the interior node it copies.
 struct HaloEntry {
@@ -107,7 +111,7 @@ __global__ void k_lusgs_sweep_bulk(const BlockView* __restrict__ blocks, unsigne
 __global__ void k_lusgs_sweep_bulk_f32(const BlockView* __restrict__ blocks, unsigned* status);
 __global__ void k_lusgs_update(const BlockView* __restrict__ blocks);
 __global__ void k_physical_bc(const BlockView* __restrict__ blocks, const BcOp* __restrict__ ops,
-                              const int* __restrict__ op_start, int o, CaseConsts cc);
+                              const BcEntry* __restrict__ list, int first, CaseConsts cc);
 __global__ void k_sa_clip(const BlockView* __restrict__ blocks);
 __global__ void k_halo(const BlockView* __restrict__ blocks, const HaloEntry* __restrict__ map,
                        long nmap, int mode);

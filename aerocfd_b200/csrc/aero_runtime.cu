@@ -92,7 +92,11 @@ struct State {
   BlockView* d_blocks = nullptr;
   std::vector<BlockView> views;
   BcOp* d_bc_ops = nullptr;
-  int* d_bc_start = nullptr;
+  // physical-BC launches: the entries of dependency level L are
+  // d_bc_list[bc_lstart[L] .. bc_lstart[L+1]), the largest face bc_lface[L]
+  BcEntry* d_bc_list = nullptr;
+  std::vector<int> bc_lstart;
+  std::vector<long> bc_lface;
   HaloEntry* d_halo = nullptr;
   long nhalo = 0;
   AvgSrc* d_avg_src = nullptr;
@@ -121,8 +125,6 @@ struct State {
   long max_box = 0, max_b0 = 0, max_b1 = 0, max_ext = 0;
   Box max_b1_box{1, 0, 1, 0, 1, 0};  // largest updated extent per direction over the blocks
   long max_b1_face = 0;               // largest face of an updated box (nodes)
-  int max_ops = 0;       // most physical-BC subfaces in one block
-  long max_face = 0;     // most nodes in one physical-BC subface
   std::map<const double*, std::pair<int, int>> registry;  // host array -> (block, field)
   // transient mode pool
   double* t_arena = nullptr;
@@ -644,9 +646,10 @@ bool sa_on() { return g.cc.turbulence == IFLAG_SA && g.cc.solver == IFLAG_NSSOLV
 
 int do_physical_bc() {
   int nb = (int)g.blocks.size();
-  for (int o = 0; o < g.max_ops; ++o) {
-    PROF(P_BC, (k_physical_bc<<<dim3(cdiv(g.max_face, 128), nb), 128, 0, g.stream>>>(
-                    g.d_blocks, g.d_bc_ops, g.d_bc_start, o, g.cc)));
+  for (size_t L = 0; L + 1 < g.bc_lstart.size(); ++L) {
+    const int first = g.bc_lstart[L], count = g.bc_lstart[L + 1] - first;
+    PROF(P_BC, (k_physical_bc<<<dim3(cdiv(g.bc_lface[L], 128), count), 128, 0, g.stream>>>(
+                    g.d_blocks, g.d_bc_ops, g.d_bc_list, first, g.cc)));
     CKL();
   }
   if (sa_on()) {
@@ -901,7 +904,9 @@ static void release_case() {
   cudaFree(g.arena); g.arena = nullptr;
   cudaFree(g.d_blocks); g.d_blocks = nullptr;
   cudaFree(g.d_bc_ops); g.d_bc_ops = nullptr;
-  cudaFree(g.d_bc_start); g.d_bc_start = nullptr;
+  cudaFree(g.d_bc_list); g.d_bc_list = nullptr;
+  g.bc_lstart.clear();
+  g.bc_lface.clear();
   cudaFree(g.d_halo); g.d_halo = nullptr;
   cudaFree(g.d_avg_src); g.d_avg_src = nullptr;
   cudaFree(g.d_avg_dst); g.d_avg_dst = nullptr;
@@ -1306,20 +1311,36 @@ int aero_finish_setup(void) {
   CK(cudaMalloc(&g.d_blocks, nb * sizeof(BlockView)));
   CK(cudaMemcpyAsync(g.d_blocks, g.views.data(), nb * sizeof(BlockView), cudaMemcpyHostToDevice, g.stream));
   // tables
-  g.max_ops = 0;
-  g.max_face = 1;
-  for (int m = 0; m < nb; ++m) g.max_ops = std::max(g.max_ops, topo.bc_start[m + 1] - topo.bc_start[m]);
-  for (const BcOp& op : topo.bc_ops) {
-    int dir = (op.face - 1) / 2;
-    long n = dir == 0 ? (long)op.sb.ny() * op.sb.nz() : dir == 1 ? (long)op.sb.nx() * op.sb.nz()
-                                                                  : (long)op.sb.nx() * op.sb.ny();
-    g.max_face = std::max(g.max_face, n);
-  }
   CK(cudaMalloc(&g.d_bc_ops, std::max<size_t>(1, topo.bc_ops.size()) * sizeof(BcOp)));
-  CK(cudaMalloc(&g.d_bc_start, topo.bc_start.size() * sizeof(int)));
   if (!topo.bc_ops.empty())
     CK(cudaMemcpyAsync(g.d_bc_ops, topo.bc_ops.data(), topo.bc_ops.size() * sizeof(BcOp), cudaMemcpyHostToDevice, g.stream));
-  CK(cudaMemcpyAsync(g.d_bc_start, topo.bc_start.data(), topo.bc_start.size() * sizeof(int), cudaMemcpyHostToDevice, g.stream));
+  {
+    // launch lists by dependency level
+    auto face_nodes = [](const BcOp& op) {
+      int dir = (op.face - 1) / 2;
+      return dir == 0 ? (long)op.sb.ny() * op.sb.nz() : dir == 1 ? (long)op.sb.nx() * op.sb.nz()
+                                                                  : (long)op.sb.nx() * op.sb.ny();
+    };
+    int nlev = 0;
+    for (int l : topo.bc_level) nlev = std::max(nlev, l + 1);
+    std::vector<BcEntry> list;
+    g.bc_lstart.assign(1, 0);
+    g.bc_lface.clear();
+    for (int L = 0; L < nlev; ++L) {
+      long face = 1;
+      for (int m = 0; m < nb; ++m)
+        for (int idx = topo.bc_start[m]; idx < topo.bc_start[m + 1]; ++idx)
+          if (topo.bc_level[idx] == L) {
+            list.push_back({idx, m});
+            face = std::max(face, face_nodes(topo.bc_ops[idx]));
+          }
+      g.bc_lstart.push_back((int)list.size());
+      g.bc_lface.push_back(face);
+    }
+    CK(cudaMalloc(&g.d_bc_list, std::max<size_t>(1, list.size()) * sizeof(BcEntry)));
+    if (!list.empty())
+      CK(cudaMemcpyAsync(g.d_bc_list, list.data(), list.size() * sizeof(BcEntry), cudaMemcpyHostToDevice, g.stream));
+  }
   g.nhalo = (long)topo.halo.size();
   g.navg_src = (long)topo.avg_src.size();
   g.navg_dst = (long)topo.avg_dst.size();

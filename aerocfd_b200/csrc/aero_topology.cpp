@@ -11,11 +11,67 @@
 // gives the shared interface nodes of average1 (sub_bc_updatebufferaverage.f90).
 #include "aero_topology.h"
 
+#include <algorithm>
 #include <cstdio>
 #include <map>
 #include <tuple>
 
 namespace aero {
+
+namespace {
+
+// Node layers one physical-BC op writes (its face layer) and reads (up to
+// three layers inward along the face normal: no-slip extrapolates from
+// three, outflow, symmetry and farfield read one, inflow none), as index
+// boxes; the metrics it reads are never written by a BC.
+struct Layers {
+  int w[2][3], r[2][3];
+  bool reads;
+};
+Layers bc_layers(const BcOp& op) {
+  const int dir = (op.face - 1) / 2;
+  const int s = op.face % 2 == 1 ? 1 : -1;
+  const int lo[3] = {op.sb.is, op.sb.js, op.sb.ks}, hi[3] = {op.sb.ie, op.sb.je, op.sb.ke};
+  Layers L;
+  for (int d = 0; d < 3; ++d) {
+    L.w[0][d] = L.r[0][d] = lo[d];
+    L.w[1][d] = L.r[1][d] = hi[d];
+  }
+  const int f = s > 0 ? lo[dir] : hi[dir];
+  const int depth = op.type == BCT_NOSLIP ? 3 : (op.type == BCT_INFLOW ? 0 : 1);
+  L.w[0][dir] = L.w[1][dir] = f;
+  L.reads = depth > 0;
+  L.r[0][dir] = std::min(f + s, f + s * depth);
+  L.r[1][dir] = std::max(f + s, f + s * depth);
+  return L;
+}
+bool meet(const int a[2][3], const int b[2][3]) {
+  for (int d = 0; d < 3; ++d)
+    if (a[1][d] < b[0][d] || b[1][d] < a[0][d]) return false;
+  return true;
+}
+
+}  // namespace
+
+// Dependency levels of each block's physical-BC ops.  The reference applies a
+// block's subfaces one after another; an op must follow an earlier op of its
+// block when their written layers meet or one reads what the other writes.
+// Its level is one more than the highest level of such earlier ops, so the
+// ops of one level touch disjoint nodes, read nothing another writes, and can
+// run in one launch with the serial result.
+void bc_levels(Topology& out) {
+  out.bc_level.assign(out.bc_ops.size(), 0);
+  for (size_t m = 0; m + 1 < out.bc_start.size(); ++m) {
+    for (int i = out.bc_start[m]; i < out.bc_start[m + 1]; ++i) {
+      const Layers Li = bc_layers(out.bc_ops[i]);
+      for (int j = out.bc_start[m]; j < i; ++j) {
+        const Layers Lj = bc_layers(out.bc_ops[j]);
+        bool dep = meet(Lj.w, Li.w) || (Li.reads && meet(Lj.w, Li.r)) || (Lj.reads && meet(Lj.r, Li.w));
+        if (dep) out.bc_level[i] = std::max(out.bc_level[i], out.bc_level[j] + 1);
+      }
+    }
+  }
+}
 
 namespace {
 
@@ -244,6 +300,7 @@ std::string build_topology(const std::vector<TopoBlock>& blocks, int buffer_leng
     }
     out.bc_start.push_back((int)out.bc_ops.size());
   }
+  bc_levels(out);
   return std::string();
 }
 

@@ -29,6 +29,7 @@ struct Topology {
   std::vector<AvgDst> avg_dst;
   std::vector<BcOp> bc_ops;        // per block, bcinfo order
   std::vector<int> bc_start;       // nblock+1 offsets into bc_ops
+  std::vector<int> bc_level;       // per op: dependency level within its block (see bc_levels)
 };
 
 // Builds all tables; returns an empty string on success or the reason the
