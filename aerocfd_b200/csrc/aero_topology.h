@@ -37,4 +37,8 @@ struct Topology {
 std::string build_topology(const std::vector<TopoBlock>& blocks, int buffer_length, int solver,
                            Topology& out);
 
+// Fills out.bc_level from out.bc_ops and out.bc_start: each op's dependency
+// level within its block (build_topology calls it).
+void bc_levels(Topology& out);
+
 }  // namespace aero
