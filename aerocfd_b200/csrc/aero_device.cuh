@@ -19,7 +19,7 @@ enum FieldId {
   F_Q = 0, F_PRI, F_RHSI, F_RHSV, F_RHS, F_DT, F_DXIDX, F_INVJ, F_AMU, F_NUT, F_SARHS,
   F_X, F_Y, F_Z, F_DIST, F_ALPHA, F_BETA, F_GAMMA, F_DUDX, F_TAO, F_VOR, F_LENGTH, F_SPACING, F_Q0,
   // device-only scratch
-  F_FVH, F_DIASD, F_SAS,
+  F_RA, F_RB, F_RC, F_DIAG, F_FVH, F_DIASD, F_SAS,
   F_FIH,  // inviscid face fluxes of the face-based kernels (5 per direction)
   F_NUM
 };

@@ -15,15 +15,39 @@
 
 namespace aero {
 
-// Spectral radius along direction d at node n, as
-// sub_timeadvancement_1stimplicit.f90:72-156 forms ra, rb, rc.
-__device__ __forceinline__ double spectral_radius(const BlockView& B, long n, int d) {
+// sub_timeadvancement_1stimplicit.f90:72-156: rhs on the updated nodes and the
+// spectral radii ra, rb, rc and the diagonal on the updated box grown by one.
+__global__ void k_lusgs_prep(const BlockView* __restrict__ blocks, CaseConsts cc_launch) {
+  const BlockView& B = blocks[blockIdx.y];
+  const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
+  const Box& b1 = B.b1;
+  Box e{b1.is - 1, b1.ie + 1, b1.js - 1, b1.je + 1, b1.ks - 1, b1.ke + 1};
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= e.size()) return;
+  int i = e.is + (int)(t % e.nx());
+  long r = t / e.nx();
+  int j = e.js + (int)(r % e.ny());
+  int k = e.ks + (int)(r / e.ny());
+  long n = B.at(i, j, k);
+  if (b1.contains(i, j, k)) {
+#pragma unroll
+    for (int c = 1; c <= 5; ++c) B.v(F_RHS, c, n) = B.v(F_RHSI, c, n) + B.v(F_RHSV, c, n);
+  }
+  double phi = cc.cfl >= 1.0e3 ? 0.0 : 1.0;
   double u = B.v(F_PRI, 2, n), v = B.v(F_PRI, 3, n), w = B.v(F_PRI, 4, n), c = B.v(F_PRI, 7, n);
-  double x0 = B.v(F_DXIDX, 3 * d + 1, n), y0 = B.v(F_DXIDX, 3 * d + 2, n), z0 = B.v(F_DXIDX, 3 * d + 3, n);
-  double temp = p2(x0) + p2(y0) + p2(z0);
-  temp = sqrt(temp);
-  double cu = x0 * u + y0 * v + z0 * w;
-  return fabs(cu) + fabs(c * temp);
+  double rr[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    double x0 = B.v(F_DXIDX, 3 * d + 1, n), y0 = B.v(F_DXIDX, 3 * d + 2, n), z0 = B.v(F_DXIDX, 3 * d + 3, n);
+    double temp = p2(x0) + p2(y0) + p2(z0);
+    temp = sqrt(temp);
+    double cu = x0 * u + y0 * v + z0 * w;
+    rr[d] = fabs(cu) + fabs(c * temp);
+  }
+  B.s(F_RA, n) = rr[0];
+  B.s(F_RB, n) = rr[1];
+  B.s(F_RC, n) = rr[2];
+  B.s(F_DIAG, n) = phi * 1.0 / B.s(F_DT, n) + rr[0] + rr[1] + rr[2];
 }
 
 // calc_jm (sub_timeadvancement_jac.f90:17-62) at node n with the metric row
@@ -153,13 +177,8 @@ __device__ __forceinline__ R* recs(const BlockView& B, bool fwd) {
 // S+ = 0.5*(A + r*I)*inv_j goes to the forward record of the node one step up
 // in d, S- = 0.5*(A - r*I)*inv_j to the backward record of the node one step
 // down (sub_timeadvancement_1stimplicit.f90:283-301, :459-477, same
-// operations).  The direction-0 thread of each node also forms rhs = rhsi +
-// rhsv (written back to rhs) and the diagonal from the three spectral radii
-// and dt (:72-156), and stores rhs, diag, inv_j, their reciprocals and the
-// packed positions of the node's forward and backward neighbours.  The
-// reference also forms the radii and the diagonal on the ring of nodes around
-// the updated box; there dq is zero, so nothing reads them.  R is the record
-// format.
+// operations).  Each node also stores rhs, diag and inv_j, and the packed
+// positions of its forward and backward neighbours.  R is the record format.
 template <typename R>
 __device__ __forceinline__ void lusgs_mats_body(const BlockView* __restrict__ blocks, CaseConsts cc) {
   constexpr int W = RecFmt<R>::kWords;
@@ -184,15 +203,8 @@ __device__ __forceinline__ void lusgs_mats_body(const BlockView* __restrict__ bl
     long base = B.poff[h], cnt = B.poff[h + 1] - base, lt = p - base;
     double* sc = B.sca + kSca * base + lt;
 #pragma unroll
-    for (int x = 1; x <= 5; ++x) {
-      const double rhs = B.v(F_RHSI, x, n) + B.v(F_RHSV, x, n);
-      B.v(F_RHS, x, n) = rhs;
-      sc[(x - 1) * cnt] = rhs;
-    }
-    const CaseConsts& cb = B.ccb ? *B.ccb : cc;
-    const double phi = cb.cfl >= 1.0e3 ? 0.0 : 1.0;
-    const double r0 = spectral_radius(B, n, 0), r1 = spectral_radius(B, n, 1), r2 = spectral_radius(B, n, 2);
-    double diag = phi * 1.0 / B.s(F_DT, n) + r0 + r1 + r2, invj = B.s(F_INVJ, n);
+    for (int x = 0; x < 5; ++x) sc[x * cnt] = B.v(F_RHS, x + 1, n);
+    double diag = B.s(F_DIAG, n), invj = B.s(F_INVJ, n);
     sc[5 * cnt] = diag;
     sc[6 * cnt] = invj;
     sc[7 * cnt] = 1.0 / diag;
@@ -218,7 +230,7 @@ __device__ __forceinline__ void lusgs_mats_body(const BlockView* __restrict__ bl
   const double uu = (dxidx * mu0 + dxidy * mv0 + dxidz * mw0) / rho;
   const double phi = 0.5 * a2 * (p2(mu0) + p2(mv0) + p2(mw0)) / p2(rho);
   const double a1 = gamma * e0 / rho - phi;
-  const double rad = spectral_radius(B, n, d);
+  const double rad = B.s(d == 0 ? F_RA : (d == 1 ? F_RB : F_RC), n);
   const double invj = B.s(F_INVJ, n);
   R* dup = nullptr;
   R* ddn = nullptr;

@@ -73,7 +73,7 @@ struct State {
   cudaStream_t stream2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaEvent_t ev_fork2 = nullptr, ev_join2 = nullptr;  // inviscid beside viscous + find_dt
-  cudaEvent_t ev_rhs = nullptr, ev_resid = nullptr;    // residual norm beside the LU-SGS sweeps
+  cudaEvent_t ev_prep = nullptr, ev_resid = nullptr;   // residual norm beside the LU-SGS sweeps
   std::vector<cudaEvent_t> xfer_ev;  // host transfers: one per array of a batch, plus one
   // dynamic shared memory limits already raised on this device (cudaFuncSetAttribute
   // is per device), per sweep kernel [FP64 records, FP32 records]
@@ -122,7 +122,7 @@ struct State {
   double* d_staging = nullptr;
   size_t staging_doubles = 0;
   double totalnodes = 0;
-  long max_box = 0, max_b0 = 0, max_b1 = 0;
+  long max_box = 0, max_b0 = 0, max_b1 = 0, max_ext = 0;
   Box max_b1_box{1, 0, 1, 0, 1, 0};  // largest updated extent per direction over the blocks
   long max_b1_face = 0;               // largest face of an updated box (nodes)
   std::map<const double*, std::pair<int, int>> registry;  // host array -> (block, field)
@@ -162,13 +162,13 @@ State g;
 // Per-kernel CUDA-event timing on the library's stream (aero_profile_*), and a
 // count of every kernel this library launches (aero_launch_count).
 enum ProfId {
-  P_GETPRI, P_FILL, P_INVISCID, P_VISC_A, P_VISC_B, P_FIND_DT, P_DT_MINMAX,
+  P_GETPRI, P_FILL, P_INVISCID, P_VISC_A, P_VISC_B, P_FIND_DT, P_DT_MINMAX, P_LUSGS_PREP,
   P_LUSGS_MATS, P_LUSGS_SWEEP, P_LUSGS_UPDATE, P_SA_A, P_SA_B, P_SA_RECS, P_SA_SWEEP, P_INDEX, P_BC, P_SA_CLIP, P_HALO, P_AVG_GATHER, P_AVG_APPLY, P_RESID_PART, P_RESID_FINAL,
   P_TRANSFER, P_GEOMETRY, P_FORCES, P_CRANK, P_NUM
 };
 const char* kProfName[P_NUM] = {
     "k_getpri", "k_fill", "k_inviscid", "k_viscous_a", "k_viscous_b", "k_find_dt", "k_dt_minmax",
-    "k_lusgs_mats", "k_lusgs_sweep", "k_lusgs_update", "k_sa_a", "k_sa_b", "k_sa_recs", "k_sa_sweep",
+    "k_lusgs_prep", "k_lusgs_mats", "k_lusgs_sweep", "k_lusgs_update", "k_sa_a", "k_sa_b", "k_sa_recs", "k_sa_sweep",
     "k_plane_index", "k_physical_bc", "k_sa_clip", "k_halo", "k_avg_gather",
     "k_avg_apply", "k_residual_partial", "k_residual_final", "k_transfer", "k_geometry", "k_forces", "k_crank"};
 struct Prof {
@@ -507,17 +507,17 @@ int launch_dt_minmax(const BlockView* views, int m, double* d_out2) {
   CKL();
   return AERO_OK;
 }
-// implicit1st on nblk views; after_rhs (if given) is recorded once rhs is
-// final (after k_lusgs_mats, which forms it).
-int launch_implicit(const BlockView* views, int nblk, long maxN1, int pmax, int hmax, const CaseConsts& cc,
-                    cudaEvent_t after_rhs = nullptr) {
+int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, int pmax, int hmax,
+                    const CaseConsts& cc, cudaEvent_t after_prep = nullptr) {
   // mixed precision stores the off-diagonal blocks in FP32 (products and sums
   // stay FP64); f selects that variant of every kernel that touches them
   const int f = g.mixed ? 1 : 0;
+  PROF(P_LUSGS_PREP, (k_lusgs_prep<<<dim3(cdiv(maxExt, g.tune.ew), nblk), g.tune.ew, 0, g.stream>>>(views, cc)));
+  CKL();
+  if (after_prep) CK(cudaEventRecord(after_prep, g.stream));
   PROF(P_LUSGS_MATS, ((f ? k_lusgs_mats_f32 : k_lusgs_mats)<<<dim3(cdiv(3 * maxN1, g.tune.mats), nblk), g.tune.mats, 0,
                                                              g.stream>>>(views, cc)));
   CKL();
-  if (after_rhs) CK(cudaEventRecord(after_rhs, g.stream));
   // Staged sweep: plane offsets + ring of two planes + nst staged planes
   // (records, scalars, dq*) + 2*nst+1 mbarriers, as many stages as fit
   // (2..4); one consumer thread per row of every node of the largest plane
@@ -745,7 +745,7 @@ int do_iteration_crank() {
 }
 
 // With resid_beside, the residual norm of the iteration (rhs, dt, inv_j and
-// sa_rhs, none of which is written after k_lusgs_mats and sa_model's rhs) is
+// sa_rhs, none of which is written after k_lusgs_prep and sa_model's rhs) is
 // computed on the second stream beside the LU-SGS sweeps, into g.d_out, and
 // g.ev_resid marks its end.
 int do_iteration(bool want_dt_minmax, bool resid_beside = false) {
@@ -774,11 +774,11 @@ int do_iteration(bool want_dt_minmax, bool resid_beside = false) {
     if ((rc = launch_sa(g.d_blocks, nb, g.max_box, g.max_b1, g.pmax_all, g.cc, g.stream2))) return rc;
     CK(cudaEventRecord(g.ev_join, g.stream2));
   }
-  if ((rc = launch_implicit(g.d_blocks, nb, g.max_b1, g.pmax_all, g.hmax_all, g.cc,
-                            resid_beside ? g.ev_rhs : nullptr)))
+  if ((rc = launch_implicit(g.d_blocks, nb, g.max_ext, g.max_b1, g.pmax_all, g.hmax_all, g.cc,
+                            resid_beside ? g.ev_prep : nullptr)))
     return rc;
   if (resid_beside) {
-    CK(cudaStreamWaitEvent(g.stream2, g.ev_rhs, 0));
+    CK(cudaStreamWaitEvent(g.stream2, g.ev_prep, 0));
     if ((rc = do_residual(g.d_out, g.stream2))) return rc;
     CK(cudaEventRecord(g.ev_resid, g.stream2));
   }
@@ -881,7 +881,7 @@ int aero_init(int device) {
   CK(cudaEventCreateWithFlags(&g.ev_join, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&g.ev_fork2, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&g.ev_join2, cudaEventDisableTiming));
-  CK(cudaEventCreateWithFlags(&g.ev_rhs, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&g.ev_prep, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&g.ev_resid, cudaEventDisableTiming));
   CK(cudaMalloc(&g.d_status, sizeof(unsigned)));
   CK(cudaMemset(g.d_status, 0, sizeof(unsigned)));
@@ -944,7 +944,7 @@ int aero_finalize(void) {
   cudaEventDestroy(g.ev_join); g.ev_join = nullptr;
   cudaEventDestroy(g.ev_fork2); g.ev_fork2 = nullptr;
   cudaEventDestroy(g.ev_join2); g.ev_join2 = nullptr;
-  cudaEventDestroy(g.ev_rhs); g.ev_rhs = nullptr;
+  cudaEventDestroy(g.ev_prep); g.ev_prep = nullptr;
   cudaEventDestroy(g.ev_resid); g.ev_resid = nullptr;
   for (cudaEvent_t e : g.xfer_ev) cudaEventDestroy(e);
   g.xfer_ev.clear();
@@ -1259,7 +1259,7 @@ int aero_finish_setup(void) {
   if (!why.empty()) return fail(AERO_ERR_ARG, "%s", why.c_str());
   // arena
   size_t total = 0;
-  g.max_box = g.max_b0 = g.max_b1 = 0;
+  g.max_box = g.max_b0 = g.max_b1 = g.max_ext = 0;
   g.max_b1_box = Box{1, 0, 1, 0, 1, 0};
   g.max_b1_face = 0;
   g.totalnodes = 0;
@@ -1271,6 +1271,8 @@ int aero_finish_setup(void) {
     g.max_box = std::max(g.max_box, H.b.size());
     g.max_b0 = std::max(g.max_b0, H.b0.size());
     max_b1 = std::max(max_b1, H.b1.size());
+    Box e{H.b1.is - 1, H.b1.ie + 1, H.b1.js - 1, H.b1.je + 1, H.b1.ks - 1, H.b1.ke + 1};
+    g.max_ext = std::max(g.max_ext, e.size());
     g.totalnodes += (double)H.b0.size();
     g.max_b1_face = std::max({g.max_b1_face, (long)H.b1.ny() * H.b1.nz(), (long)H.b1.nx() * H.b1.nz(),
                               (long)H.b1.nx() * H.b1.ny()});
@@ -1630,8 +1632,9 @@ int aero_implicit1st(double* q, const double* dt, const double* pri_v, double* r
   if ((rc = resolve(b, b0, b1, args, t))) return rc;
   CaseConsts cc = consts_with(*gamma, g.cc.cv, g.cc.re);
   cc.cfl = *cfl;
+  Box e{b1.is - 1, b1.ie + 1, b1.js - 1, b1.je + 1, b1.ks - 1, b1.ke + 1};
   if (!t.resident && (rc = launch_index(t.d_view, 1, b1.size()))) return rc;
-  if ((rc = launch_implicit(t.d_view, 1, b1.size(), t.view.pmax, t.view.nplanes, cc))) return rc;
+  if ((rc = launch_implicit(t.d_view, 1, e.size(), b1.size(), t.view.pmax, t.view.nplanes, cc))) return rc;
   return finish(t, args);
 }
 

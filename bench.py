@@ -60,7 +60,8 @@ KERNEL_BYTES = {
     "k_viscous_a": 30 * 8,     # pri(u,v,w,t),amu2,dxidx,inv_j read; amu1,amu3,vor,fv/gv/hv write
     "k_viscous_b": 17 * 8,     # fv/gv/hv read; rhsv write
     "k_find_dt": 23 * 8,       # dxidx,pri(d,u,v,w,c),amu3 read; dt write
-    "k_lusgs_mats": 35 * 8,    # q,dxidx,inv_j,pri(u,v,w,c),dt,rhsi,rhsv read; rhs write (the blocks it writes are workspace)
+    "k_lusgs_prep": 22 * 8,    # pri(u,v,w,c),dxidx,dt,rhsi,rhsv read; ra,rb,rc,diag,rhs write
+    "k_lusgs_mats": 24 * 8,    # q,dxidx,inv_j,ra,rb,rc,rhs,diag read (the blocks it writes are workspace)
     "k_getpri": 12 * 8,        # q read; pri write
 }
 # DRAM bytes (read + write) per launch of the dominant kernel on this workload,
