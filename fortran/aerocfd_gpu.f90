@@ -249,6 +249,169 @@ module aerocfd_gpu
       import :: c_ptr
       type(c_ptr) :: aero_last_error
     end function
+
+    ! device status word (AERO_ST_* bits raised since the last call; clears them)
+    integer(c_int) function aero_get_status(status) bind(C, name="aero_get_status")
+      import :: c_int
+      integer(c_int) :: status
+    end function
+
+    ! sub_tur_sa.f90:7 (sa_model; main.f90:415, :538).  The arrays are passed
+    ! by address as the reference passes them: dxidx and dudx are the blocks'
+    ! (9, ...) arrays that sa_model views as (3, ..., 3).
+    integer(c_int) function aero_sa_model(nut, sa_rhs, dt, pri_v, amu, dudx, vor, dxidx, inv_j, alpha, beta, &
+        gamma, length, dist, spac, re, cfl, is, ie, js, je, ks, ke, is0, ie0, js0, je0, ks0, ke0, &
+        is1, ie1, js1, je1, ks1, ke1) bind(C, name="aero_sa_model")
+      import :: c_int, c_double
+      integer(c_int) :: is, ie, js, je, ks, ke, is0, ie0, js0, je0, ks0, ke0, is1, ie1, js1, je1, ks1, ke1
+      real(c_double) :: nut(*), sa_rhs(*), dt(*), pri_v(*), amu(*), dudx(*), vor(*), dxidx(*), inv_j(*)
+      real(c_double) :: alpha(*), beta(*), gamma(*), length(*), dist(*), spac(*), re, cfl
+    end function
+
+    ! module-state routines of the registered set (main.f90:142-318, :446)
+    integer(c_int) function aero_compute_geometry(with_walldist) bind(C, name="aero_compute_geometry")
+      import :: c_int
+      integer(c_int), value :: with_walldist
+    end function
+
+    integer(c_int) function aero_init_flowfield() bind(C, name="aero_init_flowfield")
+      import :: c_int
+    end function
+
+    integer(c_int) function aero_getpri_all() bind(C, name="aero_getpri_all")
+      import :: c_int
+    end function
+
+    ! per-block residual norms of the last aero_step (7 per block)
+    integer(c_int) function aero_residual_blocks(out7_per_block) bind(C, name="aero_residual_blocks")
+      import :: c_int, c_double
+      real(c_double) :: out7_per_block(7, *)
+    end function
+
+    ! a block's own Control.in values (batches of independent cases)
+    integer(c_int) function aero_set_block_params(m, params) bind(C, name="aero_set_block_params")
+      import :: c_int, c_double
+      integer(c_int), value :: m
+      real(c_double) :: params(7)
+    end function
+
+    ! execution options (no counterpart in the reference)
+    integer(c_int) function aero_set_precision(mode) bind(C, name="aero_set_precision")
+      import :: c_int
+      integer(c_int), value :: mode
+    end function
+
+    integer(c_int) function aero_use_graphs(on) bind(C, name="aero_use_graphs")
+      import :: c_int
+      integer(c_int), value :: on
+    end function
+
+    integer(c_int) function aero_autotune(iters) bind(C, name="aero_autotune")
+      import :: c_int
+      integer(c_int), value :: iters
+    end function
+
+    integer(c_int) function aero_set_tuning(inv_tile, ew, visc, mats, nst_max) bind(C, name="aero_set_tuning")
+      import :: c_int
+      integer(c_int), value :: inv_tile, ew, visc, mats, nst_max
+    end function
+
+    function aero_tuning() bind(C, name="aero_tuning")
+      import :: c_ptr
+      type(c_ptr) :: aero_tuning
+    end function
+
+    ! benchmarking and profiling
+    integer(c_int) function aero_step_timed(nsteps, flush_l2, device_ms) bind(C, name="aero_step_timed")
+      import :: c_int, c_double
+      integer(c_int), value :: nsteps, flush_l2
+      real(c_double) :: device_ms
+    end function
+
+    integer(c_int) function aero_launch_count(count) bind(C, name="aero_launch_count")
+      import :: c_int, c_long_long
+      integer(c_long_long) :: count
+    end function
+
+    integer(c_int) function aero_profile(enable) bind(C, name="aero_profile")
+      import :: c_int
+      integer(c_int), value :: enable
+    end function
+
+    integer(c_int) function aero_profile_read(ms, counts, n) bind(C, name="aero_profile_read")
+      import :: c_int, c_double, c_long_long
+      real(c_double) :: ms(*)
+      integer(c_long_long) :: counts(*)
+      integer(c_int), value :: n
+    end function
+
+    function aero_profile_name(id) bind(C, name="aero_profile_name")
+      import :: c_int, c_ptr
+      integer(c_int), value :: id
+      type(c_ptr) :: aero_profile_name
+    end function
+
+    ! residual norms from caller-owned device arrays (arrays of device
+    ! addresses, one per block), allocating nothing
+    integer(c_int) function aero_residual_device_noalloc(nblocks, rhs, dt, inv_j, sa_rhs, boxes, totalnodes, &
+        out7, stream) bind(C, name="aero_residual_device_noalloc")
+      import :: c_int, c_double, c_ptr
+      integer(c_int), value :: nblocks
+      type(c_ptr) :: rhs(*), dt(*), inv_j(*), sa_rhs(*)
+      integer(c_int) :: boxes(*)
+      real(c_double), value :: totalnodes
+      real(c_double) :: out7(7)
+      type(c_ptr), value :: stream
+    end function
+
+    ! warm-start network on the tcgen05 tensor cores (no counterpart in the
+    ! reference); BF16 operands as 16-bit integers
+    integer(c_int) function aero_mlp_create(n_in, n_out, width, depth, batch, seed) bind(C, name="aero_mlp_create")
+      import :: c_int, c_long_long
+      integer(c_int), value :: n_in, n_out, width, depth, batch
+      integer(c_long_long), value :: seed
+    end function
+
+    integer(c_int) function aero_mlp_destroy() bind(C, name="aero_mlp_destroy")
+      import :: c_int
+    end function
+
+    integer(c_int) function aero_mlp_gemm(a, b, c, m, n, k, splits) bind(C, name="aero_mlp_gemm")
+      import :: c_int, c_short, c_float
+      integer(c_short) :: a(*), b(*)
+      real(c_float) :: c(*)
+      integer(c_int), value :: m, n, k, splits
+    end function
+
+    integer(c_int) function aero_mlp_param_count(count) bind(C, name="aero_mlp_param_count")
+      import :: c_int, c_long_long
+      integer(c_long_long) :: count
+    end function
+
+    integer(c_int) function aero_mlp_get_params(out) bind(C, name="aero_mlp_get_params")
+      import :: c_int, c_float
+      real(c_float) :: out(*)
+    end function
+
+    integer(c_int) function aero_mlp_gradients(x, t, n, loss, grad) bind(C, name="aero_mlp_gradients")
+      import :: c_int, c_float
+      real(c_float) :: x(*), t(*), loss, grad(*)
+      integer(c_int), value :: n
+    end function
+
+    integer(c_int) function aero_mlp_train(x, t, n, steps, lr, seed, loss_hist) bind(C, name="aero_mlp_train")
+      import :: c_int, c_float, c_long_long
+      real(c_float) :: x(*), t(*), loss_hist(*)
+      integer(c_long_long), value :: n, seed
+      integer(c_int), value :: steps
+      real(c_float), value :: lr
+    end function
+
+    integer(c_int) function aero_mlp_predict(x, n, y) bind(C, name="aero_mlp_predict")
+      import :: c_int, c_float, c_long_long
+      real(c_float) :: x(*), y(*)
+      integer(c_long_long), value :: n
+    end function
   end interface
 
 contains

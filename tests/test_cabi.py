@@ -26,6 +26,20 @@ def test_header_declares_drop_in_and_module_routines():
         assert name in syms
 
 
+def test_fortran_module_binds_every_header_symbol():
+    """fortran/aerocfd_gpu.f90 (source only here: no Fortran compiler) gives
+    every C entry point a bind(C) interface under its own name, and keeps to
+    free-form source's 132-column lines."""
+    import re
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "fortran", "aerocfd_gpu.f90")
+    text = open(path).read()
+    bound = set(re.findall(r'bind\(C,\s*name="(aero_[a-z0-9_]+)"\)', text))
+    missing = [s for s in _lib.header_symbols() if s not in bound]
+    assert not missing, f"no Fortran interface for: {missing}"
+    assert not bound - set(_lib.header_symbols()), "Fortran binds a name the header does not declare"
+    assert max(len(line) for line in text.splitlines()) <= 132
+
+
 def test_library_exports_every_header_symbol(lib):
     out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True,
                          text=True, check=True).stdout
