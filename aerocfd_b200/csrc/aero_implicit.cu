@@ -926,6 +926,8 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsig
     if (++spins > kSpinLimit) return false;
   return true;
 }
+// "no wait has run out" in the bulk sweep's failure stamp
+constexpr unsigned kNoFailure = 0xffffffffu;
 __device__ __forceinline__ void cluster_sync_all() {
   asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
@@ -972,13 +974,28 @@ __device__ __forceinline__ double row_from_ring(const RowRecs& r, const double* 
 // publishes the forward dq* (global) to the backward pass, and a last one keeps
 // every CTA resident until the copies into it have landed.  A CTA copies plane
 // gs+2 into a ring half only after every CTA has sent it plane gs+1, i.e. after
-// all have finished reading that half.  A wait that runs out raises ST_TIMEOUT
-// and the sweep runs on to the end.  The arithmetic per row is lusgs_rows'.
+// all have finished reading that half.  The arithmetic per row is lusgs_rows'.
+//
+// Failure (a wait that runs out) is contained by these rules:
+//  * a CTA arms a ring half for plane gs only while none of its waits has run
+//    out, so the half's previous phase (plane gs-2) was seen complete: no half
+//    is ever re-armed over an incomplete phase;
+//  * once a wait has run out the CTA sends nothing more.  Its peers then run
+//    out waiting for its next slice and stop too, so every copy into a CTA
+//    belongs to a plane that CTA has armed (no bytes are counted on the wrong
+//    phase) and the whole cluster ends in the failed state;
+//  * at the end every CTA publishes whether it failed; if any did, each waits
+//    again (bounded) for its armed phases and then idles for a bounded time
+//    after the last cluster barrier, so copies issued before that barrier land
+//    before any CTA leaves.  Without a failure every CTA has seen every byte
+//    sent to it before the last barrier, so no copy is in flight at exit.
+// The sweep raises ST_TIMEOUT; its values are then meaningless.
 template <typename R>
 __device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ blocks, unsigned* status) {
   constexpr int W = RecFmt<R>::kWords;
   extern __shared__ __align__(16) double xring[];  // 2 halves x (G + 2) doubles
   __shared__ __align__(8) unsigned long long xbar[2];
+  __shared__ unsigned s_failed;  // a wait of this CTA ran out (any thread)
   const unsigned ncta = cluster_size(), me = cluster_rank();
   const BlockView& B = blocks[blockIdx.x / ncta];
   const int H = B.nplanes;
@@ -988,6 +1005,7 @@ __device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ bl
   const int HS = G + 2;
   const int g = (int)me * T + (int)threadIdx.x;
   if (threadIdx.x == 0) {
+    s_failed = kNoFailure;
     mbar_init(&xbar[0], 1);
     mbar_init(&xbar[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -1011,22 +1029,35 @@ __device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ bl
     const int cnt = count_of(gs);
     if (g < 5 * cnt) load_row_recs(recs<R>(B, fwd) + W * base, B.sca + kSca * base, cnt, g, pre);
   };
-  bool ok = true;
+  // failures are stamped with the plane whose wait ran out (the smallest
+  // such plane is kept), so a test for "a wait of plane <= p ran out" is
+  // exact whatever later planes other warps have reached
+  volatile unsigned* failed_at = &s_failed;
+  auto failed_by = [&](int p) { return p >= 0 && *failed_at <= (unsigned)p; };
+  auto fail_at = [&](int p) { atomicMin(&s_failed, (unsigned)p); };
+  int armed0 = -1, armed1 = -1;  // thread 0: the last plane armed on ring half 0 / 1
   preload(0);
   for (int gs = 0; gs < 2 * H; ++gs) {
     const bool fwd = gs < H;
     const long base = poff[plane_of(gs)];
     const int cnt = count_of(gs);
-    if (threadIdx.x == 0) {  // arm this plane's half: the bytes of the other CTAs' slices
+    // arm this plane's half (the bytes of the other CTAs' slices) only if the
+    // half's previous phase (plane gs-2, waited for at plane gs-1) completed
+    if (threadIdx.x == 0 && !failed_by(gs - 1)) {
       unsigned expect = 0;
       for (unsigned r = 0; r < ncta; ++r)
         if (r != me) expect += slice_bytes(cnt, r);
       mbar_expect_tx(&xbar[gs & 1], expect);
+      if (gs & 1)
+        armed1 = gs;
+      else
+        armed0 = gs;
     }
     int cnt_prev = 0;
     if (gs > 0) {
       cnt_prev = count_of(gs - 1);
-      if (!mbar_wait_bounded(&xbar[(gs - 1) & 1], (unsigned)(((gs - 1) >> 1) & 1))) ok = false;
+      if (!failed_by(gs - 1) && !mbar_wait_bounded(&xbar[(gs - 1) & 1], (unsigned)(((gs - 1) >> 1) & 1)))
+        fail_at(gs);
     }
     if (gs == H) cluster_sync_all();  // the forward dq* stores, for dsv
     const double* prev = xring + ((gs - 1) & 1) * HS;
@@ -1042,10 +1073,11 @@ __device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ bl
         B.dq[5 * (base + pre.node) + pre.row] = v;
     }
     // the slice is complete once every thread has written and fenced its value;
-    // lane r of warp 0 then copies it to CTA r
+    // lane r of warp 0 then copies it to CTA r, unless a wait of this CTA up to
+    // this plane ran out (every such failure is recorded before the barrier)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
-    if (threadIdx.x < ncta && threadIdx.x != me) {
+    if (threadIdx.x < ncta && threadIdx.x != me && !failed_by(gs)) {
       const unsigned bytes = slice_bytes(cnt, me);
       const unsigned off = (unsigned)(((gs & 1) * HS + (int)me * T) * sizeof(double));
       const unsigned boff = (unsigned)((gs & 1) * sizeof(unsigned long long));
@@ -1055,10 +1087,39 @@ __device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ bl
     }
     preload(gs + 1);
   }
-  // the last plane's bytes, then no CTA leaves while a copy into it may be in flight
-  if (H > 0 && !mbar_wait_bounded(&xbar[(2 * H - 1) & 1], (unsigned)(((2 * H - 1) >> 1) & 1))) ok = false;
+  // the last plane's bytes
+  if (H > 0 && !failed_by(2 * H - 1) &&
+      !mbar_wait_bounded(&xbar[(2 * H - 1) & 1], (unsigned)(((2 * H - 1) >> 1) & 1)))
+    fail_at(2 * H);
+  __syncthreads();
+  // every CTA's outcome is final once all have reached the barrier; each
+  // reads the others' and no CTA leaves before all have read
   cluster_sync_all();
-  if (!ok && status) atomicOr(status, (unsigned)ST_TIMEOUT);
+  unsigned any = (s_failed != kNoFailure) ? 1u : 0u;
+  if (threadIdx.x < ncta && threadIdx.x != me) {
+    unsigned v;
+    asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(map_rank(smem_u32(&s_failed), threadIdx.x))
+                 : "memory");
+    any |= v != kNoFailure ? 1u : 0u;
+  }
+  any = __syncthreads_or(any);
+  cluster_sync_all();
+  if (any) {
+    // copies issued before the last barrier may still be landing in, or
+    // reading from, this CTA's shared memory: wait (bounded) for the phases
+    // this CTA armed, then idle for a bounded time before leaving
+    if (threadIdx.x == 0) {
+      for (int h = 0; h < 2; ++h) {
+        const int a = h ? armed1 : armed0;
+        if (a >= 0)
+          for (long s = 0; s < kSpinLimit && !mbar_try_wait(&xbar[h], (unsigned)((a >> 1) & 1)); ++s) {
+          }
+      }
+      for (int s = 0; s < 2000; ++s) __nanosleep(1000);
+      if (status) atomicOr(status, (unsigned)ST_TIMEOUT);
+    }
+    __syncthreads();
+  }
 }
 __global__ void __launch_bounds__(512, 1) k_lusgs_sweep_bulk(const BlockView* __restrict__ blocks, unsigned* status) {
   lusgs_bulk_body<double>(blocks, status);

@@ -116,6 +116,23 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(const uint16_t* __restrict__ 
     __syncthreads();
     if (abort_flag) break;
   }
+  if (abort_flag) {
+    // The MMAs committed last may still read the staged tiles and write the
+    // accumulator: wait once more, with a longer bound, for that commit
+    // (parity phase ^ 1, the one the loop gave up on) before the accumulator
+    // is freed.  If this wait runs out too, the status bit below is the only
+    // guarantee left: the dealloc then races the MMAs.
+    if (tid == 0) {
+      unsigned done = 0;
+      for (long spins = 0; !done && spins < 16 * kGemmSpin; ++spins)
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(done)
+            : "r"(smem_addr(&bar)), "r"(phase ^ 1u)
+            : "memory");
+    }
+    __syncthreads();
+  }
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (!abort_flag) {
     const int row = m0 + warp * 32 + lane;

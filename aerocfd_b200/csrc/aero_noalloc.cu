@@ -4,8 +4,12 @@
 //
 // The per-CTA partial sums that aero_residual keeps in a buffer allocated at
 // set-up live here in one file-scope device array of fixed size.  Its address
-// is looked up once per device (cudaGetSymbolAddress, with that device
-// current) on the first call made on that device; later calls reuse it.
+// is looked up (cudaGetSymbolAddress, with the device current) on the first
+// call made on a device and kept together with the CUDA context it belongs
+// to; a later call in the same context reuses it, and a call that finds
+// another context current (the primary context was reset and re-created,
+// which reloads the module at another address) looks it up again.  A lookup
+// that fails is not kept: the next call tries again.
 //
 // Scratch contents: slot p holds the six partial sums of CTA p of the current
 // call.  Every slot the final reduction reads is written by the partial kernel
@@ -84,12 +88,59 @@ __global__ void k_residual_partial_ref(ResidBlocks rb, double* __restrict__ part
   }
 }
 
+// The scratch address of one device, valid in the context whose unique ID
+// (cuCtxGetId: never reused within a process, unlike a context handle, which
+// a re-created primary context may get again) is `ctx_id`.
 struct DeviceScratch {
-  std::once_flag once;
-  cudaError_t rc = cudaSuccess;
+  unsigned long long ctx_id = 0;
   double* part = nullptr;
 };
 DeviceScratch s_dev[kMaxDevices];
+std::mutex s_dev_mu;
+
+// cuCtxGetCurrent and cuCtxGetId through the runtime's driver entry point
+// table (the library does not link libcuda itself); CUresult is an int-sized
+// enum, 0 = success.
+typedef int (*CtxGetCurrentFn)(void**);
+typedef int (*CtxGetIdFn)(void*, unsigned long long*);
+void* driver_fn(const char* name) {
+  void* p = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess)
+    return nullptr;
+  return p;
+}
+
+// Unique ID of the current context (0 when none is current or on failure).
+unsigned long long current_ctx_id() {
+  static CtxGetCurrentFn get = (CtxGetCurrentFn)driver_fn("cuCtxGetCurrent");
+  static CtxGetIdFn get_id = (CtxGetIdFn)driver_fn("cuCtxGetId");
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get || !get_id || get(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
+
+// Device address of s_part for device `dev` in the current context.
+cudaError_t scratch_address(int dev, double** part) {
+  std::lock_guard<std::mutex> lock(s_dev_mu);
+  DeviceScratch& S = s_dev[dev];
+  unsigned long long id = current_ctx_id();
+  if (id && S.part && S.ctx_id == id) {
+    *part = S.part;
+    return cudaSuccess;
+  }
+  // on a first call no context may be current yet: cudaGetSymbolAddress makes
+  // the device's primary context current, and the ID is read after it
+  double* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress((void**)&p, s_part);
+  if (e != cudaSuccess) return e;  // not kept: the next call tries again
+  if (!(id = current_ctx_id())) return cudaErrorDeviceUninitialized;
+  S.ctx_id = id;
+  S.part = p;
+  *part = p;
+  return cudaSuccess;
+}
 
 bool valid_box(const int* x) { return x[0] <= x[1] && x[2] <= x[3] && x[4] <= x[5]; }
 bool inside(const int* in, const int* out) {
@@ -143,14 +194,14 @@ extern "C" int aero_residual_device_noalloc(int nblocks, const double* const* rh
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return set_last_error(AERO_ERR_CUDA, cudaGetErrorString(e));
   if (dev < 0 || dev >= kMaxDevices) return set_last_error(AERO_ERR_ARG, "aero_residual_device_noalloc: device ordinal out of range");
-  DeviceScratch& S = s_dev[dev];
-  std::call_once(S.once, [&S] { S.rc = cudaGetSymbolAddress((void**)&S.part, s_part); });
-  if (S.rc != cudaSuccess) return set_last_error(AERO_ERR_CUDA, cudaGetErrorString(S.rc));
+  double* part = nullptr;
+  if ((e = scratch_address(dev, &part)) != cudaSuccess)
+    return set_last_error(AERO_ERR_CUDA, cudaGetErrorString(e));
 
   cudaStream_t st = (cudaStream_t)stream;
-  k_residual_partial_ref<<<dim3((unsigned)ctas, nblocks), kThreads, 0, st>>>(rb, S.part);
+  k_residual_partial_ref<<<dim3((unsigned)ctas, nblocks), kThreads, 0, st>>>(rb, part);
   if ((e = cudaGetLastError()) != cudaSuccess) return set_last_error(AERO_ERR_CUDA, cudaGetErrorString(e));
-  k_residual_final<<<1, 256, 0, st>>>(S.part, ctas * nblocks, totalnodes, out7, nullptr);
+  k_residual_final<<<1, 256, 0, st>>>(part, ctas * nblocks, totalnodes, out7, nullptr);
   if ((e = cudaGetLastError()) != cudaSuccess) return set_last_error(AERO_ERR_CUDA, cudaGetErrorString(e));
   return AERO_OK;
 }

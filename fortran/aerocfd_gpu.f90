@@ -352,16 +352,19 @@ module aerocfd_gpu
     end function
 
     ! residual norms from caller-owned device arrays (arrays of device
-    ! addresses, one per block), allocating nothing
+    ! addresses, one per block), allocating nothing; sa_rhs is c_loc of an
+    ! array of device addresses or c_null_ptr (laminar), out7 the DEVICE
+    ! address of 7 doubles (c_devloc of a CUDA Fortran device array, or
+    ! acc_deviceptr under OpenACC), stream a cudaStream_t or c_null_ptr
     integer(c_int) function aero_residual_device_noalloc(nblocks, rhs, dt, inv_j, sa_rhs, boxes, totalnodes, &
         out7, stream) bind(C, name="aero_residual_device_noalloc")
       import :: c_int, c_double, c_ptr
       integer(c_int), value :: nblocks
-      type(c_ptr) :: rhs(*), dt(*), inv_j(*), sa_rhs(*)
+      type(c_ptr) :: rhs(*), dt(*), inv_j(*)
+      type(c_ptr), value :: sa_rhs
       integer(c_int) :: boxes(*)
       real(c_double), value :: totalnodes
-      real(c_double) :: out7(7)
-      type(c_ptr), value :: stream
+      type(c_ptr), value :: out7, stream
     end function
 
     ! warm-start network on the tcgen05 tensor cores (no counterpart in the
@@ -400,8 +403,9 @@ module aerocfd_gpu
     end function
 
     integer(c_int) function aero_mlp_train(x, t, n, steps, lr, seed, loss_hist) bind(C, name="aero_mlp_train")
-      import :: c_int, c_float, c_long_long
-      real(c_float) :: x(*), t(*), loss_hist(*)
+      import :: c_int, c_float, c_long_long, c_ptr
+      real(c_float) :: x(*), t(*)
+      type(c_ptr), value :: loss_hist
       integer(c_long_long), value :: n, seed
       integer(c_int), value :: steps
       real(c_float), value :: lr

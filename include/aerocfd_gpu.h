@@ -370,8 +370,10 @@ int aero_launch_count(unsigned long long* count);
  * ceil(largest updated box / 256) <= AERO_NOALLOC_MAX_PARTS (about 4.2 million
  * updated nodes in equal blocks); larger calls return AERO_ERR_ARG before any
  * device work.  The partial sums live in one fixed device array per device;
- * the first call on a device looks its address up (make that first call
- * outside any stream capture), and nothing in it has to start at zero.  Calls
+ * the first call in each CUDA context of a device looks its address up (make
+ * that first call outside any stream capture; a context re-created after a
+ * device reset gets a fresh lookup, and a failed lookup is retried by the
+ * next call), and nothing in it has to start at zero.  Calls
  * whose kernels can overlap on one device (other streams, other host threads)
  * share that array and race: order them on one stream. */
 #define AERO_NOALLOC_MAX_BLOCKS 32

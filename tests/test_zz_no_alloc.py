@@ -98,3 +98,66 @@ def test_noalloc_rejects_out_of_range_calls():
     bad = np.array([1, 9, 1, 9, 1, 9, 0, 8, 2, 8, 2, 8], dtype=np.int32)
     assert _call(L, 1, one, one, one, None, bad, 1.0, 1, 0) == 1
     assert b"bad box" in L.aero_last_error()
+
+
+def _reference_norms(blocks, totalnodes):
+    """sub_output_residual.f90:27-56 in exact arithmetic (math.fsum) over the
+    updated box of every block: sqrt(sum((rhs_n dt / inv_j)^2) / totalnodes)
+    and, with sa_rhs, sqrt(sum((sa_rhs dt)^2) / totalnodes)."""
+    import math
+    out = np.zeros(7)
+    for c in range(6):
+        terms = []
+        for rhs, dt, invj, sa, bx in blocks:
+            i0, j0, k0 = bx[6] - bx[0], bx[8] - bx[2], bx[10] - bx[4]
+            i1, j1, k1 = bx[7] - bx[0] + 1, bx[9] - bx[2] + 1, bx[11] - bx[4] + 1
+            d = dt[k0:k1, j0:j1, i0:i1]
+            if c < 5:
+                terms.append(((rhs[k0:k1, j0:j1, i0:i1, c] * d / invj[k0:k1, j0:j1, i0:i1]) ** 2).ravel())
+            elif sa is not None:
+                terms.append(((sa[k0:k1, j0:j1, i0:i1] * d) ** 2).ravel())
+        out[c] = math.sqrt(math.fsum(np.concatenate(terms)) / totalnodes) if terms else 0.0
+    return out
+
+
+@pytest.mark.gpu
+def test_noalloc_residual_uneven_blocks_large_then_small_call():
+    """Blocks of different sizes (so the partial-sum grid has CTAs past the
+    end of the smaller blocks), one large call followed by a smaller one
+    (which leaves stale partial sums of the first call in the shared
+    scratch): each result equals the exact norm of its own arrays to 1e-13."""
+    torch = pytest.importorskip("torch")
+    from aerocfd_b200 import build
+    build.build()
+    L = _lib.load()
+    rng = np.random.default_rng(7)
+
+    def make_block(ni, nj, nk, with_sa):
+        # full box 1..n with one ghost layer outside the updated box 2..n-1
+        bx = [1, ni, 1, nj, 1, nk, 2, ni - 1, 2, nj - 1, 2, nk - 1]
+        rhs = rng.standard_normal((nk, nj, ni, 5))
+        dt = rng.uniform(0.1, 2.0, (nk, nj, ni))
+        invj = rng.uniform(0.5, 3.0, (nk, nj, ni))
+        sa = rng.standard_normal((nk, nj, ni)) if with_sa else None
+        return rhs, dt, invj, sa, bx
+
+    calls = [[make_block(70, 45, 22, True), make_block(17, 9, 5, True), make_block(33, 65, 3, True)],
+             [make_block(12, 7, 4, True), make_block(9, 30, 6, True)]]
+    stream = torch.cuda.current_stream().cuda_stream
+    for blocks in calls:
+        dev = [[torch.from_numpy(np.ascontiguousarray(a)).to("cuda:0") for a in blk[:4]] for blk in blocks]
+        boxes = np.array([v for blk in blocks for v in blk[4]], dtype=np.int32)
+        totalnodes = float(sum((b[4][1] - b[4][0] - 1) * (b[4][3] - b[4][2] - 1) * (b[4][5] - b[4][4] - 1)
+                               for b in blocks))
+        ref = _reference_norms(blocks, totalnodes)
+        out = torch.empty(7, dtype=torch.float64, device="cuda:0")
+        out.fill_(float("nan"))
+        rc = _call(L, len(blocks), [d[0].data_ptr() for d in dev], [d[1].data_ptr() for d in dev],
+                   [d[2].data_ptr() for d in dev], [d[3].data_ptr() for d in dev], boxes, totalnodes,
+                   out.data_ptr(), stream)
+        assert rc == 0, L.aero_last_error()
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        assert got[6] == 0.0
+        err = np.abs(got[:6] - ref[:6]) / np.abs(ref[:6])
+        assert np.all(err <= TOL), (got, ref)
