@@ -1,11 +1,14 @@
 #!/usr/bin/env python
 """Throughput of aerocfd's residual-and-update iteration on B200.
 
-Workload: the laminar Navier-Stokes 4-block O-grid around an analytic NACA0012
-(4 x 129x65x3 nodes, farfield radius 20 chords, wall spacing 1e-4 chord,
-M=0.5, Re=5000, AoA=2 deg), synthetic and generated in-process, started from
-freestream.  Scheme: the reference's Roe flux on WENO3 states with 2nd-order
-central viscous terms and the 1st-order implicit LU-SGS update, FP64.
+Workload (the headline line): the turbulent flat plate with Spalart-Allmaras,
+193 x 129 x 33 nodes as 8 blocks of 25 x 129 x 33 along x (851,400 nodes),
+wall spacing 5e-6 (y+ about 1 at Re_L 5e6), wall-normal ratio 1.1,
+leading-edge clustering, M 0.2, Re_L 5e6, nu_t,inf = 3 nu_inf, CFL 5,
+synthetic and generated in-process, started from freestream.  Scheme: the
+reference's Roe flux on WENO3 states, 2nd-order central viscous terms, the
+1st-order implicit LU-SGS update and the SA model with its scalar LU-SGS,
+FP64 (the reference's arithmetic).
 
 A step is one iteration of main.f90:343-447 for every block plus the residual
 norm of sub_output_residual.f90 (the reference computes it every iteration).
@@ -13,24 +16,26 @@ norm of sub_output_residual.f90 (the reference computes it every iteration).
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 value: Mcell-iter/s (nodes x steps / device time), inputs resident on the GPU,
-L2 flushed before every timed step.  e2e: the same metric through the C-ABI
-with the solution held on the host: every step copies q host->device, runs
-the iteration and copies q and the residual back.  --impl reference times the
-CPU restatement of the reference's algorithm (the reference is Fortran + MPI
-and cannot be compiled in this image) on the host cores, one thread per block
+L2 flushed before every timed step (the case's arrays, 0.9 GB, exceed L2 as
+well).  e2e: the same metric through the C-ABI with the solution (q and nu_t)
+held on the host: every step copies them host->device, runs the iteration and
+copies them and the residual back.  --impl reference times the CPU
+restatement of the reference's algorithm (the reference is Fortran + MPI and
+cannot be compiled in this image) on the host cores, one thread per block
 like one MPI rank per block.
 
-Extra objects on the line: `mixed` (the same device-timed metric with
+Extra objects on the line: `mixed` (the device-timed metric with
 aero_set_precision(1), and the mixed solution's max / L2 error against FP64
-after 50 iterations from one state) and `convergence` (wall time to each drop
-milestone 1e-3 .. 1e-8 of the density residual on the 97x49x5 Euler bump
-channel, FP64 and mixed, with the CPU restatement's time estimated from its
-iteration rate; a milestone the scheme does not reach is null) and `batched`
-(64 bump channels of uneven size in one batch, mixed precision, CUDA-graph
-replay, autotuned launch shapes, against the same 64 cases run one after
-another) and `warm_start` (iterations and wall time to residual drops of
-1e-4, 1e-6, 1e-8 from freestream vs from the learned prediction on held-out
-members of a bump family, with cl / cd of both converged runs).
+after 50 iterations from one state), `naca` (the laminar NACA0012 O-grid
+4 x 129 x 65 x 3, M 0.5, Re 5000, AoA 2, CFL 2: the same measurements, its own
+roofline, e2e and CPU sample), `convergence` (wall time to each drop milestone
+1e-3 .. 1e-8 of the density residual on the 97x49x5 Euler bump channel with
+the reference's Roe + WENO3 and with Steger-Warming + WENO5, FP64 and mixed),
+`batched` (64 bump channels of uneven size in one batch, mixed precision,
+CUDA-graph replay, autotuned launch shapes, against the same 64 cases run one
+after another, with its error against an FP64 run of the same batch),
+`schemes`, `sa_plate` (3000 iterations of the headline case from freestream
+in FP64 and mixed: residual drop and skin-friction error) and `warm_start`.
 """
 from __future__ import annotations
 
@@ -49,11 +54,14 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = "naca0012_ogrid_4x129x65x3_laminar_fp64"
+WORKLOAD = "sa_flat_plate_193x129x33_8blocks_m0.2_re5e6_cfl5_fp64"
+NACA_WORKLOAD = "naca0012_ogrid_4x129x65x3_laminar_fp64"
 HBM_FALLBACK = 6650.0
 
 # Algorithmic bytes per processed node of each kernel class (FP64): every
-# array the kernel must read once plus every array it must write once.
+# array the kernel must read once plus every array it must write once (the
+# LU-SGS records and other scratch a kernel writes for a later one are not
+# credited).
 KERNEL_BYTES = {
     "k_lusgs_sweep": 49 * 8,   # q,dxidx,inv_j,ra,rb,rc,diag,rhs read; dq*,dq w+r; q w
     "k_inviscid": 20 * 8,      # q,dxidx,inv_j read; rhsi write
@@ -63,13 +71,21 @@ KERNEL_BYTES = {
     "k_lusgs_prep": 22 * 8,    # pri(u,v,w,c),dxidx,dt,rhsi,rhsv read; ra,rb,rc,diag,rhs write
     "k_lusgs_mats": 24 * 8,    # q,dxidx,inv_j,ra,rb,rc,rhs,diag read (the blocks it writes are workspace)
     "k_getpri": 12 * 8,        # q read; pri write
+    "k_sa_sweep": 21 * 8,      # pri(u,v,w),dxidx,inv_j,nut,dt,sa_rhs,diag read; dnut* w+r; dnut w; nut w
+    "k_sa_a": 19 * 8,          # pri(u,v,w),dxidx,inv_j,nut,vor,length read; sa_rhs write (+ its source terms)
 }
-# DRAM bytes (read + write) per launch of the dominant kernel on this workload,
-# from one ncu capture of it (--set full, cold cache under replay).
-KERNEL_TRAFFIC = {"k_lusgs_sweep": 42.97e6 + 0.04e6}
-# The whole iteration's compulsory footprint for Euler/laminar FP64: read q,
-# dxidx, inv_j, write q, dq* write+read = 30 words per node.
+# The node box each kernel class runs over.
+KERNEL_BOX = {"k_lusgs_sweep": "box1", "k_inviscid": "box1", "k_viscous_a": "box0", "k_viscous_b": "box0",
+              "k_residual_partial": "box1", "k_lusgs_mats": "box1", "k_sa_sweep": "box1", "k_sa_a": "box1"}
+# DRAM bytes (read + write) per launch of the dominant kernel of each
+# workload, from one ncu capture of it (cold cache under replay).
+KERNEL_TRAFFIC = {(WORKLOAD, "k_lusgs_sweep"): 1083.8e6 + 62.0e6,
+                  (NACA_WORKLOAD, "k_lusgs_sweep"): 42.97e6 + 0.04e6}
+# The whole iteration's compulsory footprint (FP64): read q, dxidx, inv_j,
+# write q, dq* write+read = 30 words per node; SA adds nut r/w, dist, the
+# alpha/beta/gamma tensors and dnut* w/r = 44 words.
 ITER_BYTES = 240
+ITER_BYTES_SA = 352
 
 
 def init_replicas(world: int, local: int, backend: str = "nccl"):
@@ -115,8 +131,9 @@ def parse():
     ap.add_argument("--no-converge", action="store_true", help="skip the time-to-1e-8 runs")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-case batch")
     ap.add_argument("--no-warm-start", action="store_true", help="skip the learned warm start")
-    ap.add_argument("--no-plate", action="store_true", help="skip the SA flat plate")
+    ap.add_argument("--no-plate", action="store_true", help="skip the plate's 3000-iteration runs")
     ap.add_argument("--no-schemes", action="store_true", help="skip the WENO5 / WCNS5 workloads")
+    ap.add_argument("--no-naca", action="store_true", help="skip the NACA0012 O-grid workload")
     return ap.parse_args()
 
 
@@ -129,33 +146,47 @@ def peaks():
 
 
 def make_case():
+    """The headline workload: the SA flat plate, 8 blocks of 25 x 129 x 33."""
+    from aerocfd_b200 import grids
+    from aerocfd_b200.case import Config, IFLAG_NSSOLVER
+    cfg = Config(solver=IFLAG_NSSOLVER, turbulence=2, ma=0.2, re=5.0e6, cfl=5.0, nutinf=3.0)
+    return grids.flat_plate(nbi=8, nbj=1, nbk=1, cfg=cfg)
+
+
+def make_naca():
+    """The laminar NACA0012 O-grid 4 x 129 x 65 x 3 (M 0.5, Re 5000, AoA 2,
+    CFL 2)."""
     from aerocfd_b200 import grids
     return grids.naca_ogrid()
 
 
 CONV_WORKLOAD = "bump_channel_97x49x5_euler_m0.5_cfl5"
 CONV_TARGET = 1e-8
-CONV_MILESTONES = (1e-3, 1e-4, 1e-5, 1e-6, 1e-8)
+CONV_MILESTONES = (1e-3, 1e-4, 1e-5, 1e-6, 1e-7, 1e-8)
 
 
-def make_bump():
+def make_bump(inviscid: int = 4):
+    """BASELINE config 1's channel and flow: 97 x 49 x 5, Euler, M 0.5, CFL 5;
+    inviscid 4 = the reference's Roe + WENO3, 5 = Steger-Warming + WENO5."""
     from aerocfd_b200 import grids
-    return grids.bump_channel()
+    from aerocfd_b200.case import Config, IFLAG_EULERSOLVER
+    return grids.bump_channel(cfg=Config(solver=IFLAG_EULERSOLVER, ma=0.5, re=1.0e6, cfl=5.0, inviscid=inviscid))
 
 
-def converge_gpu(solver, mixed: bool, chunk: int = 500, its: int = 12000):
+def converge_gpu(solver, mixed: bool, inviscid: int = 4, chunk: int = 500, its: int = 20000):
     """Wall time to each drop milestone of the density residual (relative to
     iteration 1) on the Euler bump channel, freestream start, over `its`
     iterations; the time to a milestone is the run's time per iteration times
     the iteration that first reached it."""
     import torch
-    case = make_bump()
+    case = make_bump(inviscid)
     gc = solver.GpuCase(case)
     try:
         gc.compute_geometry()
         gc.init_flowfield()
         gc.start()
         gc.set_precision(mixed)
+        gc.use_graphs(True)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         hs = [gc.step(chunk) for _ in range(its // chunk)]
@@ -170,7 +201,9 @@ def converge_gpu(solver, mixed: bool, chunk: int = 500, its: int = 12000):
         hit = np.nonzero(d <= m)[0]
         first[f"{m:.0e}"] = int(hit[0]) + 1 if len(hit) else None
     per_it = el / len(d)
+    # where the history stops falling: the best drop and the iteration of it
     return {"iterations_run": len(d), "wall_s_run": el, "final_drop": float(d[-1]), "min_drop": float(d.min()),
+            "iteration_of_min_drop": int(np.argmin(d)) + 1,
             "iterations_to": first,
             "wall_s_to": {k: (v * per_it if v else None) for k, v in first.items()},
             "device_status": status}
@@ -179,12 +212,97 @@ def converge_gpu(solver, mixed: bool, chunk: int = 500, its: int = 12000):
 BATCH_WORKLOAD = "bump_batch_64_uneven_euler_mixed"
 
 
+def profile_kernels(L, steps: int):
+    """Per-kernel-class device time of `steps` steps (aero_profile: CUDA events
+    around every launch on the stream it is launched on), with each class's
+    share of the summed kernel time."""
+    ms = ctypes.c_double(0.0)
+    from aerocfd_b200 import _lib
+    L.aero_profile(ctypes.c_int(1))
+    _lib.check(L.aero_step_timed(ctypes.c_int(steps), ctypes.c_int(1), ctypes.byref(ms)), "profile")
+    L.aero_profile(ctypes.c_int(0))
+    kms = (ctypes.c_double * 32)()
+    kct = (ctypes.c_longlong * 32)()
+    nk = L.aero_profile_read(kms, kct, ctypes.c_int(32))
+    L.aero_profile_name.restype = ctypes.c_char_p
+    kernels = {}
+    for i in range(nk):
+        if kct[i]:
+            kernels[L.aero_profile_name(ctypes.c_int(i)).decode()] = {"ms_total": kms[i], "launches": int(kct[i])}
+    tot = max(1e-12, sum(x["ms_total"] for x in kernels.values()))
+    for k in kernels:
+        kernels[k]["share"] = kernels[k]["ms_total"] / tot
+    return kernels, ms.value / steps
+
+
+def box_nodes(case, boxname: str) -> int:
+    tot = 0
+    for b in case.blocks:
+        bx = getattr(b, boxname)
+        tot += (bx[1] - bx[0] + 1) * (bx[3] - bx[2] + 1) * (bx[5] - bx[4] + 1)
+    return tot
+
+
+def roofline_of(case, kernels, workload: str):
+    """The dominant kernel class's achieved HBM rate: its algorithmic bytes
+    per launch (KERNEL_BYTES x the nodes it runs over) / its event-timed
+    average launch duration, against the measured copy bandwidth."""
+    hbm, hbm_kind = peaks()
+    dom = max(kernels, key=lambda k: kernels[k]["ms_total"])
+    per_launch_ms = kernels[dom]["ms_total"] / kernels[dom]["launches"]
+    n_units = box_nodes(case, KERNEL_BOX.get(dom, "box"))
+    alg_bytes = KERNEL_BYTES.get(dom, ITER_BYTES) * n_units
+    achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
+    return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm, "peak_kind": hbm_kind, "traffic": KERNEL_TRAFFIC.get((workload, dom)),
+            "alg_bytes_per_launch": alg_bytes, "units_per_launch": n_units,
+            "bytes_per_unit": KERNEL_BYTES.get(dom, ITER_BYTES), "ms_per_launch": per_launch_ms}
+
+
+def snapshot(case):
+    return [{k: v.copy() for k, v in b.fields.items()} for b in case.blocks]
+
+
+def restore(gc, case, snap, solver):
+    for b, sn in zip(case.blocks, snap):
+        for k, v in sn.items():
+            b.fields[k][...] = v
+    gc.sync_to_device(solver.ALL)
+
+
+def mixed_error(gc, case, solver, its: int = 50):
+    """Max and L2 error of the mixed-precision solution against FP64 after
+    `its` iterations from the same state (q, and nu_t with SA), and of the
+    density residual at the last of them; the FP64 mode is left set."""
+    names = ("q", "nut") if case.cfg.turbulence else ("q",)
+    gc.set_precision(False)
+    gc.sync_to_host(solver.ALL)
+    snap = snapshot(case)
+    h64 = gc.step(its)
+    gc.sync_to_host(solver.mask(*names))
+    ref = {k: np.concatenate([b.fields[k].ravel().copy() for b in case.blocks]) for k in names}
+    restore(gc, case, snap, solver)
+    gc.set_precision(True)
+    hmx = gc.step(its)
+    gc.set_precision(False)
+    gc.sync_to_host(solver.mask(*names))
+    out = {"iterations": its}
+    for k in names:
+        got = np.concatenate([b.fields[k].ravel() for b in case.blocks])
+        d = got - ref[k]
+        out[f"{k}_max_rel"] = float(np.max(np.abs(d)) / np.max(np.abs(ref[k])))
+        out[f"{k}_l2_rel"] = float(np.linalg.norm(d) / np.linalg.norm(ref[k]))
+    out["resid_rho_rel"] = float(abs(hmx[-1, 0] - h64[-1, 0]) / abs(h64[-1, 0]))
+    restore(gc, case, snap, solver)
+    return out
+
+
 def batched_gpu(solver, steps: int, warmup: int):
     """64 bump channels of uneven size (seed 0: ni ~ U{65..257}, nj ~ U{33..97},
     nk = 5, h ~ U[0.05,0.12], M ~ U[0.3,0.7]), mixed precision, as one batch
     with CUDA-graph replay and autotuned launch shapes, against the same cases
-    run one after another with the same settings.  Device time, L2 flushed
-    before every timed step."""
+    run one after another with the same settings, and the same batch in FP64.
+    Device time, L2 flushed before every timed step."""
     import torch
     from aerocfd_b200 import _lib, grids
     cases = grids.bump_batch(64, seed=0)
@@ -192,18 +310,34 @@ def batched_gpu(solver, steps: int, warmup: int):
     batch, params = grids.batch_case(cases)
     gc = solver.GpuCase(batch, block_params=params)
     ms = ctypes.c_double(0.0)
+    out = {"workload": BATCH_WORKLOAD, "cases": 64, "nodes": nodes, "steps": steps}
     try:
         gc.compute_geometry()
         gc.init_flowfield()
         gc.start()
         gc.set_precision(True)
-        tuning = gc.autotune(3)
+        out["tuning"] = gc.autotune(3)
         gc.use_graphs(True)
-        gc.step(warmup, history=False)
-        torch.cuda.synchronize()
-        _lib.check(gc.L.aero_step_timed(ctypes.c_int(steps), ctypes.c_int(1), ctypes.byref(ms)), "batch timed")
-        batch_s = ms.value / 1e3
-        status = gc.status()
+        for mixed in (True, False):
+            gc.set_precision(mixed)
+            gc.step(warmup, history=False)
+            torch.cuda.synchronize()
+            _lib.check(gc.L.aero_step_timed(ctypes.c_int(steps), ctypes.c_int(1), ctypes.byref(ms)), "batch timed")
+            if mixed:
+                batch_s = ms.value / 1e3
+                out.update({"value": nodes * steps / batch_s / 1e6, "unit": "Mcell-iter/s",
+                            "ms_per_step": 1e3 * batch_s / steps})
+            else:
+                out["fp64"] = {"value": nodes * steps / (ms.value / 1e3) / 1e6, "ms_per_step": ms.value / steps}
+        gc.set_precision(True)
+        kernels, step_ms = profile_kernels(gc.L, max(5, steps // 2))
+        out["kernels"] = kernels
+        out["roofline"] = roofline_of(batch, kernels, BATCH_WORKLOAD)
+        out["iteration_roofline"] = {"bytes_per_node_iter": ITER_BYTES,
+                                     "achieved_gbs": ITER_BYTES * nodes / (out["ms_per_step"] / 1e3) / 1e9,
+                                     "frac": ITER_BYTES * nodes / (out["ms_per_step"] / 1e3) / 1e9 / peaks()[0]}
+        out["error_vs_fp64"] = mixed_error(gc, batch, solver, 50)
+        out["device_status"] = gc.status()
     finally:
         gc.close()
     seq_s = 0.0
@@ -220,12 +354,11 @@ def batched_gpu(solver, steps: int, warmup: int):
             seq_s += ms.value / 1e3
         finally:
             g1.close()
-    return {"workload": BATCH_WORKLOAD, "cases": 64, "nodes": nodes, "steps": steps,
-            "value": nodes * steps / batch_s / 1e6, "unit": "Mcell-iter/s", "ms_per_step": 1e3 * batch_s / steps,
-            "sequential_value": nodes * steps / seq_s / 1e6, "sequential_ms_per_step": 1e3 * seq_s / steps,
-            "speedup_vs_sequential": seq_s / batch_s, "tuning": tuning, "device_status": status,
-            "note": "one launch per kernel for all 64 cases, each step replayed from a CUDA graph; "
-                    "sequential = the 64 cases one after another, same settings, device time summed"}
+    out.update({"sequential_value": nodes * steps / seq_s / 1e6, "sequential_ms_per_step": 1e3 * seq_s / steps,
+                "speedup_vs_sequential": seq_s / batch_s,
+                "note": "one launch per kernel for all 64 cases, each step replayed from a CUDA graph; "
+                        "sequential = the 64 cases one after another, same settings, device time summed"})
+    return out
 
 
 PLATE_WORKLOAD = "sa_flat_plate_193x129x33_8blocks_m0.2_re5e6_cfl5"
@@ -247,47 +380,23 @@ def plate_cf(case) -> np.ndarray:
     return np.array(out)
 
 
-def sa_plate_gpu(solver, steps: int, warmup: int, its: int = 3000, chunk: int = 500):
-    """Turbulent flat plate (SA), 193 x 129 x 33 nodes in 8 blocks of
-    25 x 129 x 33 along x, wall spacing 5e-6 (y+ ~ 1 at Re_L 5e6), ratio 1.1,
-    M 0.2, nu_t,inf = 3 nu_inf, CFL 5: device-timed throughput in FP64 and
-    mixed precision, then `its` iterations from the freestream in each, with
-    the residual drop and the skin friction of the mixed run against FP64."""
+def sa_plate_gpu(solver, its: int = 3000, chunk: int = 500):
+    """The headline plate run from the freestream for `its` iterations in
+    FP64 and in mixed precision (autotuned shapes, CUDA graphs): the residual
+    drop of each, the wall time, and the skin friction of the mixed run
+    against FP64 (the config's 1e-8 drop needs far more iterations than a
+    bench run)."""
     import torch
-    from aerocfd_b200 import _lib, grids
-    from aerocfd_b200.case import Config, IFLAG_NSSOLVER
-    cfg = Config(solver=IFLAG_NSSOLVER, turbulence=2, ma=0.2, re=5.0e6, cfl=5.0, nutinf=3.0)
-    case = grids.flat_plate(nbi=8, nbj=1, nbk=1, cfg=cfg)
+    case = make_case()
     gc = solver.GpuCase(case)
-    ms = ctypes.c_double(0.0)
-    out = {"workload": PLATE_WORKLOAD, "blocks": len(case.blocks), "nodes": case.nodes, "steps": steps}
+    out = {"workload": PLATE_WORKLOAD, "blocks": len(case.blocks), "nodes": case.nodes}
+    cf = {}
     try:
         gc.compute_geometry()
         gc.init_flowfield()
         gc.start()
         out["tuning"] = gc.autotune(3)
         gc.use_graphs(True)
-        for mixed in (False, True):
-            gc.set_precision(mixed)
-            gc.step(warmup, history=False)
-            torch.cuda.synchronize()
-            _lib.check(gc.L.aero_step_timed(ctypes.c_int(steps), ctypes.c_int(1), ctypes.byref(ms)), "plate timed")
-            key = "mixed" if mixed else "fp64"
-            out[key] = {"value": case.nodes * steps / (ms.value / 1e3) / 1e6, "unit": "Mcell-iter/s",
-                        "ms_per_step": ms.value / steps}
-        # per-kernel shares (FP64), a separate pass
-        gc.set_precision(False)
-        gc.L.aero_profile(ctypes.c_int(1))
-        _lib.check(gc.L.aero_step_timed(ctypes.c_int(10), ctypes.c_int(1), ctypes.byref(ms)), "plate profile")
-        gc.L.aero_profile(ctypes.c_int(0))
-        kms = (ctypes.c_double * 32)()
-        kct = (ctypes.c_longlong * 32)()
-        nk = gc.L.aero_profile_read(kms, kct, ctypes.c_int(32))
-        gc.L.aero_profile_name.restype = ctypes.c_char_p
-        tot = sum(kms[i] for i in range(nk) if kct[i])
-        out["kernel_shares"] = {gc.L.aero_profile_name(ctypes.c_int(i)).decode(): round(kms[i] / tot, 4)
-                                for i in range(nk) if kct[i]}
-        cf = {}
         for mixed in (False, True):
             gc.init_flowfield()
             gc.start()
@@ -298,8 +407,8 @@ def sa_plate_gpu(solver, steps: int, warmup: int, its: int = 3000, chunk: int = 
             el = time.perf_counter() - t0
             d = h[:, 0] / h[0, 0]
             key = "mixed" if mixed else "fp64"
-            out[key].update({"iterations_run": len(d), "wall_s_run": el, "final_drop": float(d[-1]),
-                             "nut_final_drop": float(h[-1, 5] / h[0, 5])})
+            out[key] = {"iterations_run": len(d), "wall_s_run": el, "final_drop": float(d[-1]),
+                        "min_drop": float(d.min()), "nut_final_drop": float(h[-1, 5] / h[0, 5])}
             gc.sync_to_host(solver.ALL)
             cf[key] = plate_cf(case)
         out["device_status"] = gc.status()
@@ -392,15 +501,23 @@ def warm_start_gpu(solver, n_train: int = 48, n_test: int = 8, ni: int = 97, nj:
            "network": "8 x 256 SiLU MLP, BF16 weights/activations, FP32 accumulation, tcgen05 GEMMs",
            "samples": int(len(X)), "train_steps": 4000, "train_s": train_s, "data_generation_s": gen_s,
            "loss_first_last": [float(loss[:10].mean()), float(loss[-10:].mean())]}
+    out["iterations_run"] = iters
     for drop in (1e-4, 1e-6, 1e-8):
+        # every member is reported: the iteration at which it first reached
+        # the level, or null when it did not within the run; the batch's wall
+        # time to the level is the time until its slowest member reached it,
+        # null unless every member did
         level = hc[0] * drop
         ic, iw = W.first_below(hc, level, chunk), W.first_below(hw, level, chunk)
-        ok = (ic > 0) & (iw > 0)
-        out[f"{drop:.0e}"] = {"cold_iterations_mean": float(ic[ok].mean()) if ok.any() else None,
-                              "warm_iterations_mean": float(iw[ok].mean()) if ok.any() else None,
-                              "cold_wall_s": float(cold_s * ic[ok].max() / iters) if ok.any() else None,
-                              "warm_wall_s": float(warm_s * iw[ok].max() / iters) if ok.any() else None,
-                              "members_reached": int(ok.sum())}
+        both = (ic > 0) & (iw > 0)
+        out[f"{drop:.0e}"] = {
+            "cold_iterations": [int(v) if v > 0 else None for v in ic],
+            "warm_iterations": [int(v) if v > 0 else None for v in iw],
+            "cold_members_reached": int((ic > 0).sum()), "warm_members_reached": int((iw > 0).sum()),
+            "cold_iterations_mean_of_both_reached": float(ic[both].mean()) if both.any() else None,
+            "warm_iterations_mean_of_both_reached": float(iw[both].mean()) if both.any() else None,
+            "cold_wall_s_all_members": float(cold_s * ic.max() / iters) if (ic > 0).all() else None,
+            "warm_wall_s_all_members": float(warm_s * iw.max() / iters) if (iw > 0).all() else None}
     out["iteration1_residual_ratio_warm_over_cold"] = float(np.mean(hw[0] / hc[0]))
     diffs = []
     for i, (c, h, m) in enumerate(test):
@@ -479,11 +596,12 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
-def cpu_reference(seconds: float, steps: int = 0, warmup: int = 0):
-    """Times the CPU restatement (oracle/, -O3, one thread per block)."""
+def cpu_reference(make, seconds: float, steps: int = 0, warmup: int = 0):
+    """Times the CPU restatement (oracle/, -O3, one thread per block, the
+    reference's one MPI rank per block) on the case `make` builds."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle  # CPU baseline only
-    case = make_case()
+    case = make()
     oc = oracle.OracleCase(case, fast=True)
     oc.geometry()
     oc.init_flowfield()
@@ -505,6 +623,100 @@ def cpu_reference(seconds: float, steps: int = 0, warmup: int = 0):
     return case.nodes * n / el / 1e6, n, el, threads
 
 
+def measure(solver, case, workload: str, args, world: int, local: int, dist, clocks: bool = False):
+    """Device-timed, profiled, mixed-precision and end-to-end measurements of
+    one workload; returns the line's fields (value, ms_per_step, roofline,
+    kernels, mixed, e2e, ...)."""
+    import torch
+    from aerocfd_b200 import _lib
+    gc = solver.GpuCase(case, device=local)
+    L = gc.L
+    try:
+        gc.compute_geometry()
+        gc.init_flowfield()
+        gc.start()
+        tuning = gc.autotune(3)   # launch shapes only; the state is restored
+        gc.use_graphs(True)       # every step replayed from one CUDA graph
+        gc.step(args.warmup, history=False)
+
+        # ---- device-timed steps (resident inputs, L2 flushed before each step)
+        cnt0 = ctypes.c_ulonglong(0)
+        L.aero_launch_count(ctypes.byref(cnt0))
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ms = ctypes.c_double(0.0)
+        clk = ClockSampler(local) if clocks else None
+        if clk:
+            clk.__enter__()
+        try:
+            _lib.check(L.aero_step_timed(ctypes.c_int(args.steps), ctypes.c_int(1), ctypes.byref(ms)),
+                       "aero_step_timed")
+            torch.cuda.synchronize()
+        finally:
+            if clk:
+                clk.__exit__(None, None, None)
+        cnt1 = ctypes.c_ulonglong(0)
+        L.aero_launch_count(ctypes.byref(cnt1))
+        dev_s = max_over_ranks(ms.value / 1e3, dist)
+        nodes = case.nodes
+        out = {"value": whole_job_rate(nodes, args.steps, world, dev_s), "ms_per_step": 1e3 * dev_s / args.steps,
+               "gpu_launches": int(cnt1.value - cnt0.value), "tuning": tuning}
+        if clk:
+            out["clocks"] = clk.summary()
+
+        # ---- per-kernel profile (separate pass) for the roofline
+        kernels, _ = profile_kernels(L, max(5, min(args.steps, 20)))
+        out["kernels"] = kernels
+        out["roofline"] = roofline_of(case, kernels, workload)
+        hbm = peaks()[0]
+        ib = ITER_BYTES_SA if case.cfg.turbulence else ITER_BYTES
+        gbs = ib * nodes / (dev_s / args.steps) / 1e9
+        out["iteration_roofline"] = {"bytes_per_node_iter": ib, "achieved_gbs": gbs, "frac": gbs / hbm}
+
+        # ---- mixed precision: device-timed throughput, and its error against
+        # FP64 after the same iterations from the same state
+        gc.set_precision(True)
+        gc.step(3, history=False)
+        torch.cuda.synchronize()
+        _lib.check(L.aero_step_timed(ctypes.c_int(args.steps), ctypes.c_int(1), ctypes.byref(ms)), "mixed timed")
+        mixed_s = max_over_ranks(ms.value / 1e3, dist)
+        out["mixed"] = {
+            "value": whole_job_rate(nodes, args.steps, world, mixed_s), "unit": "Mcell-iter/s",
+            "ms_per_step": 1e3 * mixed_s / args.steps,
+            "dtype": "f32 WENO corrections / Roe dissipation / viscous stresses / SA source, advection and "
+                     "diffusion terms / stored LU-SGS off-diagonal blocks; f64 state, metrics, rhs, implicit "
+                     "diagonals, sweep products, dt, residual",
+            "error_vs_fp64": mixed_error(gc, case, solver, 50)}
+
+        # ---- end-to-end through the C-ABI with the solution held on the host
+        names = ("q", "nut") if case.cfg.turbulence else ("q",)
+        mq = solver.mask(*names)
+        sbytes = sum(b.fields[k].nbytes for b in case.blocks for k in names)
+        gc.sync_to_host(mq)
+        res = np.zeros(7)
+        for _ in range(2):
+            gc.sync_to_device(mq)
+            gc.step(1)
+            gc.sync_to_host(mq)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            gc.sync_to_device(mq)
+            _lib.check(L.aero_step(ctypes.c_int(1), res.ctypes.data_as(ctypes.c_void_p), None), "aero_step")
+            gc.sync_to_host(mq)
+        e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
+        out["e2e"] = {"value": whole_job_rate(nodes, args.steps, world, e2e_s), "unit": "Mcell-iter/s",
+                      "h2d_bytes_per_step": sbytes, "d2h_bytes_per_step": sbytes + 56,
+                      "fields": list(names)}
+        out["device_status"] = gc.status()
+    finally:
+        gc.close()
+    return out
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -512,16 +724,21 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.warmup < 3:
         args.warmup = 3
+    case = make_case()
+    config = {"workload": WORKLOAD, "blocks": len(case.blocks), "nodes": case.nodes,
+              "grid": "193x129x33 as 8 blocks of 25x129x33 along x, wall spacing 5e-6, ratio 1.1",
+              "ma": case.cfg.ma, "re": case.cfg.re, "nutinf_over_nuinf": case.cfg.nutinf, "cfl": case.cfg.cfl,
+              "scheme": "roe_weno3 + central viscous + spalart-allmaras + lu-sgs (reference path)"}
 
     if args.impl == "reference":
         if rank != 0:
             return 0
-        v, n, el, thr = cpu_reference(0.0, steps=args.steps, warmup=args.warmup)
+        v, n, el, thr = cpu_reference(make_case, 0.0, steps=args.steps, warmup=args.warmup)
         line = {"metric": "Mcell-iter/s", "value": v, "unit": "Mcell-iter/s", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / n,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic", "impl": "reference",
-                "config": {"workload": WORKLOAD, "blocks": 4, "nodes": make_case().nodes},
+                "data": "synthetic (analytic flat-plate grid, freestream start)", "impl": "reference",
+                "config": config,
                 "cpu_baseline": {"value": v, "unit": "Mcell-iter/s", "cores": thr, "kind": "port",
                                  "sample": f"{n} full iterations of the workload on {thr} threads "
                                            f"(one per block), C++ -O3 restatement"},
@@ -529,169 +746,56 @@ def main():
         print(json.dumps(line))
         return 0
 
-    import torch
     dist = init_replicas(world, local)
-
-    from aerocfd_b200 import _lib, solver
-    case = make_case()
-    gc = solver.GpuCase(case, device=local)
-    L = gc.L
-    gc.compute_geometry()
-    gc.init_flowfield()
-    gc.start()
-    tuning = gc.autotune(3)   # launch shapes only; the state is restored
-    gc.use_graphs(True)       # every step replayed from one CUDA graph
-    gc.step(args.warmup, history=False)
-
-    # ---- device-timed steps (resident inputs, L2 flushed before each step)
-    cnt0 = ctypes.c_ulonglong(0)
-    L.aero_launch_count(ctypes.byref(cnt0))
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    ms = ctypes.c_double(0.0)
-    with ClockSampler(local) as clk:
-        _lib.check(L.aero_step_timed(ctypes.c_int(args.steps), ctypes.c_int(1), ctypes.byref(ms)), "aero_step_timed")
-    torch.cuda.synchronize()
-    cnt1 = ctypes.c_ulonglong(0)
-    L.aero_launch_count(ctypes.byref(cnt1))
-    dev_s = max_over_ranks(ms.value / 1e3, dist)
-    nodes = case.nodes
-    value = whole_job_rate(nodes, args.steps, world, dev_s)
-
-    # ---- per-kernel profile (separate pass) for the roofline
-    L.aero_profile(ctypes.c_int(1))
-    prof_steps = max(5, min(args.steps, 20))
-    _lib.check(L.aero_step_timed(ctypes.c_int(prof_steps), ctypes.c_int(1), ctypes.byref(ms)), "profile")
-    L.aero_profile(ctypes.c_int(0))
-    kms = (ctypes.c_double * 32)()
-    kct = (ctypes.c_longlong * 32)()
-    nk = L.aero_profile_read(kms, kct, ctypes.c_int(32))
-    L.aero_profile_name.restype = ctypes.c_char_p
-    kernels = {}
-    for i in range(nk):
-        if kct[i]:
-            kernels[L.aero_profile_name(ctypes.c_int(i)).decode()] = {"ms_total": kms[i], "launches": int(kct[i])}
-    dom = max(kernels, key=lambda k: kernels[k]["ms_total"])
-    hbm, hbm_kind = peaks()
-    per_launch_ms = kernels[dom]["ms_total"] / kernels[dom]["launches"]
-    def count(boxname):
-        tot = 0
-        for b in case.blocks:
-            bx = getattr(b, boxname)
-            tot += (bx[1] - bx[0] + 1) * (bx[3] - bx[2] + 1) * (bx[5] - bx[4] + 1)
-        return tot
-    box_of_kernel = {"k_lusgs_sweep": "box1", "k_inviscid": "box1", "k_viscous_a": "box0",
-                     "k_viscous_b": "box0", "k_residual_partial": "box1"}
-    n_units = count(box_of_kernel.get(dom, "box"))
-    alg_bytes = KERNEL_BYTES.get(dom, ITER_BYTES) * n_units
-    achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
-    step_ms_prof = ms.value / prof_steps
-    for k in kernels:
-        kernels[k]["share"] = kernels[k]["ms_total"] / max(1e-12, sum(x["ms_total"] for x in kernels.values()))
-
-    # ---- mixed precision: device-timed throughput, and its error against
-    # FP64 after the same iterations from the same state
-    gc.set_precision(True)
-    gc.step(3, history=False)
-    torch.cuda.synchronize()
-    _lib.check(L.aero_step_timed(ctypes.c_int(args.steps), ctypes.c_int(1), ctypes.byref(ms)), "mixed timed")
-    mixed_s = max_over_ranks(ms.value / 1e3, dist)
-    gc.set_precision(False)
-    gc.sync_to_host(solver.ALL)
-    snap = [{k: v.copy() for k, v in b.fields.items()} for b in case.blocks]
-    kerr = 50
-    h64 = gc.step(kerr)
-    gc.sync_to_host(solver.mask("q"))
-    q64 = np.concatenate([b.fields["q"].ravel().copy() for b in case.blocks])
-    for b, sn in zip(case.blocks, snap):
-        for k, v in sn.items():
-            b.fields[k][...] = v
-    gc.sync_to_device(solver.ALL)
-    gc.set_precision(True)
-    hmx = gc.step(kerr)
-    gc.set_precision(False)
-    gc.sync_to_host(solver.mask("q"))
-    qmx = np.concatenate([b.fields["q"].ravel() for b in case.blocks])
-    dq = qmx - q64
-    mixed = {"value": whole_job_rate(nodes, args.steps, world, mixed_s), "unit": "Mcell-iter/s",
-             "ms_per_step": 1e3 * mixed_s / args.steps,
-             "dtype": "f32 WENO corrections / Roe dissipation / viscous stresses / stored LU-SGS off-diagonal "
-                      "blocks; f64 state, metrics, rhs, implicit diagonal, sweep products, dt, residual",
-             "error_vs_fp64": {"iterations": kerr, "q_max_rel": float(np.max(np.abs(dq)) / np.max(np.abs(q64))),
-                               "q_l2_rel": float(np.linalg.norm(dq) / np.linalg.norm(q64)),
-                               "resid_rho_rel": float(abs(hmx[-1, 0] - h64[-1, 0]) / abs(h64[-1, 0]))}}
-
-    # ---- end-to-end through the C-ABI with host-held q
-    qbytes = sum(b.fields["q"].nbytes for b in case.blocks)
-    mq = solver.mask("q")
-    gc.sync_to_host(mq)
-    res = np.zeros(7)
-    for _ in range(2):
-        gc.sync_to_device(mq); gc.step(1); gc.sync_to_host(mq)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        gc.sync_to_device(mq)
-        _lib.check(L.aero_step(ctypes.c_int(1), res.ctypes.data_as(ctypes.c_void_p), None), "aero_step")
-        gc.sync_to_host(mq)
-    e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
-    e2e = whole_job_rate(nodes, args.steps, world, e2e_s)
-
-    status = gc.status()
-    if status:
-        print(f"warning: device status word {status} (non-finite residual or negative density)", file=sys.stderr)
-    line = {
-        "metric": "Mcell-iter/s", "value": value, "unit": "Mcell-iter/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dev_s / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (analytic NACA0012 O-grid, freestream start)",
-        "config": {"workload": WORKLOAD, "blocks": len(case.blocks), "nodes": nodes,
-                   "ma": case.cfg.ma, "re": case.cfg.re, "aoa_deg": case.cfg.aoa_deg, "cfl": case.cfg.cfl,
-                   "scheme": "roe_weno3 + central viscous + lu-sgs (reference path)",
-                   "l2": "flushed (256 MiB write) before every timed step",
-                   "execution": "each step replayed from a CUDA graph; launch shapes from the autotuner: " + tuning,
-                   "parallelism": f"replicas x{world}"},
-        "e2e": {"value": e2e, "unit": "Mcell-iter/s", "h2d_bytes_per_step": qbytes,
-                "d2h_bytes_per_step": qbytes + 56},
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "peak_kind": hbm_kind, "traffic": KERNEL_TRAFFIC.get(dom),
-                     "alg_bytes_per_launch": alg_bytes, "ms_per_launch": per_launch_ms},
-        "iteration_roofline": {"bytes_per_node_iter": ITER_BYTES,
-                               "achieved_gbs": ITER_BYTES * nodes / (dev_s / args.steps) / 1e9,
-                               "frac": ITER_BYTES * nodes / (dev_s / args.steps) / 1e9 / hbm},
-        "kernels": kernels,
-        "clocks": clk.summary(),
-        "gpu_launches": int(cnt1.value - cnt0.value),
-        "device_status": status,
-    }
-    line["mixed"] = mixed
+    from aerocfd_b200 import solver
+    m = measure(solver, case, WORKLOAD, args, world, local, dist, clocks=True)
+    if m["device_status"]:
+        print(f"warning: device status word {m['device_status']}", file=sys.stderr)
+    config.update({"l2": "flushed (256 MiB write) before every timed step; the case's arrays exceed L2",
+                   "execution": "each step replayed from a CUDA graph; launch shapes from the autotuner: "
+                                + m.pop("tuning"),
+                   "parallelism": f"replicas x{world}"})
+    line = {"metric": "Mcell-iter/s", "value": m.pop("value"), "unit": "Mcell-iter/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": m.pop("ms_per_step"),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (analytic flat-plate grid, freestream start)", "config": config}
+    line.update(m)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, n, el, thr = cpu_reference(args.cpu_sample_seconds)
+        v, n, el, thr = cpu_reference(make_case, args.cpu_sample_seconds)
         line["cpu_baseline"] = {"value": v, "unit": "Mcell-iter/s", "cores": thr, "kind": "port",
                                 "sample": f"{n} full iterations of the same workload, {el:.1f} s, "
                                           f"{thr} threads (one per block), C++ -O3 restatement"}
-    gc.close()
+    if world == 1 and not args.no_naca:
+        naca = make_naca()
+        nm = measure(solver, naca, NACA_WORKLOAD, args, world, local, dist)
+        nm.update({"workload": NACA_WORKLOAD, "blocks": len(naca.blocks), "nodes": naca.nodes,
+                   "unit": "Mcell-iter/s"})
+        if not args.no_cpu_baseline:
+            v, n, el, thr = cpu_reference(make_naca, args.cpu_sample_seconds / 2)
+            nm["cpu_baseline"] = {"value": v, "unit": "Mcell-iter/s", "cores": thr, "kind": "port",
+                                  "sample": f"{n} full iterations, {el:.1f} s, {thr} threads (one per block)"}
+        line["naca"] = nm
     if world == 1 and not args.no_batch:
         line["batched"] = batched_gpu(solver, max(5, min(args.steps, 20)), args.warmup)
     if world == 1 and not args.no_schemes:
         line["schemes"] = schemes_gpu(solver, max(5, min(args.steps, 20)), args.warmup)
     if world == 1 and not args.no_plate:
-        line["sa_plate"] = sa_plate_gpu(solver, max(5, min(args.steps, 20)), args.warmup)
+        line["sa_plate"] = sa_plate_gpu(solver)
     if world == 1 and not args.no_warm_start:
         line["warm_start"] = warm_start_gpu(solver)
     if world == 1 and not args.no_converge:
         conv = {"workload": CONV_WORKLOAD, "target_drop": CONV_TARGET,
-                "fp64": converge_gpu(solver, False), "mixed": converge_gpu(solver, True)}
+                "roe_weno3": {"fp64": converge_gpu(solver, False, 4), "mixed": converge_gpu(solver, True, 4)},
+                "sw_weno5": {"fp64": converge_gpu(solver, False, 5), "mixed": converge_gpu(solver, True, 5)}}
         if not args.no_cpu_baseline:
             rate = bump_cpu_rate()
             conv["cpu_reference"] = {
                 "its_per_s": rate, "cores": 1, "kind": "port",
-                "wall_s_to_est": {k: (v / rate if v else None) for k, v in conv["fp64"]["iterations_to"].items()},
-                "note": "oracle iteration rate x the FP64 GPU iteration counts (the FP64 path reproduces the "
-                        "oracle's iterates); 1 thread = the reference's layout for a 1-block case"}
+                "wall_s_to_est": {k: (v / rate if v else None)
+                                  for k, v in conv["roe_weno3"]["fp64"]["iterations_to"].items()},
+                "note": "oracle iteration rate (measured, Roe + WENO3) x the FP64 GPU iteration counts (the FP64 "
+                        "path reproduces the oracle's iterates); 1 thread = the reference's layout for a "
+                        "1-block case"}
         line["convergence"] = conv
     if rank == 0:
         print(json.dumps(line))
