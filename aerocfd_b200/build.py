@@ -22,8 +22,9 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 SOURCES = ["aero_flux.cu", "aero_implicit.cu", "aero_bc.cu", "aero_transfer.cu",
            "aero_runtime.cu", "aero_topology.cpp", "aero_geometry.cu", "aero_sa.cu",
-           "aero_noalloc.cu", "aero_forces.cu", "aero_crank.cu", "aero_mlp.cu"]
-HEADERS = ["aero_device.cuh", "aero_kernels.h", "aero_topology.h", "aero_mlp_gemm.cuh"]
+           "aero_noalloc.cu", "aero_forces.cu", "aero_crank.cu", "aero_mlp.cu", "aero_crmath.cu"]
+HEADERS = ["aero_device.cuh", "aero_kernels.h", "aero_topology.h", "aero_mlp_gemm.cuh", "aero_crmath.h",
+           "aero_crmath_tables.h"]
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC",

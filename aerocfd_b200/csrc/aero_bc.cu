@@ -74,8 +74,8 @@ __global__ void k_physical_bc(const BlockView* __restrict__ blocks, const BcOp* 
   int dir = di ? 0 : (dj ? 1 : 2);
   if (op.type == BCT_INFLOW) {  // sub_bc_-50_inflow.f90:21-40
     B.v(F_Q, 1, n) = cc.d_0;
-    B.v(F_Q, 2, n) = cc.d_0 * cc.u_0 * cos(cc.aoa);
-    B.v(F_Q, 3, n) = cc.d_0 * cc.u_0 * sin(cc.aoa);
+    B.v(F_Q, 2, n) = cc.d_0 * cc.u_0 * cc.cos_aoa;
+    B.v(F_Q, 3, n) = cc.d_0 * cc.u_0 * cc.sin_aoa;
     B.v(F_Q, 4, n) = 0.0;
     B.v(F_Q, 5, n) = cc.p_0 / (gamma - 1.0) + 0.5 * p2(cc.u_0);
     if (tur) B.s(F_NUT, n) = cc.nutinf;
@@ -101,8 +101,8 @@ __global__ void k_physical_bc(const BlockView* __restrict__ blocks, const BcOp* 
     B.v(F_Q, 5, n) = (11.0 * B.v(F_Q, 5, n1) - 7.0 * B.v(F_Q, 5, n2) + 2.0 * B.v(F_Q, 5, n3)) / 6.0;
     if (tur) B.s(F_NUT, n) = 0.0;
   } else if (op.type == BCT_FARFIELD) {  // sub_bc_-10_farfield.f90:30-106
-    double u_inf = cc.u_0 * cos(cc.aoa), v_inf = cc.u_0 * sin(cc.aoa), w_inf = 0.0;
-    double s_inf = cc.p_0 / pow(cc.d_0, gamma);
+    double u_inf = cc.u_0 * cc.cos_aoa, v_inf = cc.u_0 * cc.sin_aoa, w_inf = 0.0;
+    double s_inf = cc.p_0 / crm::pow(cc.d_0, gamma);
     double c_inf = cc.c_0;
     double x0, y0, z0;
     unit_normal(B, n, dir, s, x0, y0, z0);
@@ -112,7 +112,7 @@ __global__ void k_physical_bc(const BlockView* __restrict__ blocks, const BcOp* 
     double w_p = B.v(F_Q, 4, n1) / d_p;
     double p_p = (B.v(F_Q, 5, n1) - 0.5 * d_p * (p2(u_p) + p2(v_p) + p2(w_p))) * (gamma - 1.0);
     double c_p = sqrt(gamma * p_p / d_p);
-    double s_p = p_p / pow(d_p, gamma);
+    double s_p = p_p / crm::pow(d_p, gamma);
     double vn_inf = u_inf * x0 + v_inf * y0 + w_inf * z0;
     double vn_p = u_p * x0 + v_p * y0 + w_p * z0;
     double rm = vn_inf - 2.0 * c_inf / (gamma - 1.0);
@@ -125,8 +125,8 @@ __global__ void k_physical_bc(const BlockView* __restrict__ blocks, const BcOp* 
     double u_b = u_ref + (vn_b - u_ref_t) * x0;
     double v_b = v_ref + (vn_b - u_ref_t) * y0;
     double w_b = w_ref + (vn_b - u_ref_t) * z0;
-    double d_b = pow(c_p * c_p / (gamma * s_b), 1.0 / (gamma - 1.0));
-    double p_b = s_b * pow(d_b, gamma);
+    double d_b = crm::pow(c_p * c_p / (gamma * s_b), 1.0 / (gamma - 1.0));
+    double p_b = s_b * crm::pow(d_b, gamma);
     B.v(F_Q, 1, n) = d_b;
     B.v(F_Q, 2, n) = d_b * u_b;
     B.v(F_Q, 3, n) = d_b * v_b;

@@ -12,6 +12,8 @@
 #pragma once
 #include <cstdint>
 
+#include "aero_crmath.h"
+
 namespace aero {
 
 // Field ids of the C-ABI (AERO_F_* in include/aerocfd_gpu.h).
@@ -46,6 +48,9 @@ struct Box {
 struct CaseConsts {
   double gamma, cv, re, tinf, prl, prt, cfl;
   double d_0, u_0, p_0, c_0, aoa, nutinf;
+  // cos(aoa) and sin(aoa) from the host's libm (the reference's cos and sin
+  // on its CPU), so every kernel uses the same values as the CPU path
+  double cos_aoa, sin_aoa;
   int dimension, solver, time, turbulence, des, bufferLength;
   int inviscid;  // iflag_inviscid: 4 Roe + WENO3, 5 Steger-Warming + WENO5, 8 WCNS5 + Roe
 };
@@ -88,7 +93,7 @@ constexpr int kRec = 76;
 constexpr int kSca = 10;
 // SA sweep records per node: 0.5*(U+|U|) x3, 0.5*(U-|U|) x3, sa_rhs, diag,
 // packed forward and backward neighbours.
-constexpr int kSaRec = 10;
+constexpr int kSaRec = 12;
 
 // Three plane-local indices (+1; 0 = no neighbour) in one 64-bit word: the
 // neighbours' positions in their hyperplane relative to its first node.  Bit
@@ -141,6 +146,17 @@ __device__ __forceinline__ double div_rn(double a, double b, double rb) {
   double aa = fabs(a), ab = fabs(b), aq = fabs(q);
   if (!(aa > 0x1p-960 && aa < 0x1p960 && ab > 0x1p-960 && ab < 0x1p960 && aq > 0x1p-960 && aq < 0x1p960))
     q = a / b;
+  return q;
+}
+// div_rn with the IEEE division of the rare out-of-range case in a function
+// of its own, which keeps the division's long code (and its registers) out of
+// a sweep loop.  Bit-identical to a / b, as div_rn.
+inline __device__ __noinline__ double div1_ieee(double a, double b) { return a / b; }
+__device__ __forceinline__ double div_rn_lean(double a, double b, double rb) {
+  double q = div_newton(a, b, rb);
+  double aa = fabs(a), ab = fabs(b), aq = fabs(q);
+  if (!(aa > 0x1p-960 && aa < 0x1p960 && ab > 0x1p-960 && ab < 0x1p960 && aq > 0x1p-960 && aq < 0x1p960))
+    q = div1_ieee(a, b);
   return q;
 }
 

@@ -711,7 +711,7 @@ __global__ void k_viscous_a(const BlockView* __restrict__ blocks, CaseConsts cc_
     gw[d] = cdiff(pw, n, st[d], pos[d], lo[d], hi[d]);
   }
   double u0 = pu[n], v0 = pv[n], w0 = pw[n], t0 = pt[n];
-  double amu1 = (1.0 + 124.0 / cc.tinf) / (t0 + 124.0 / cc.tinf) * pow(t0, 1.5);
+  double amu1 = (1.0 + 124.0 / cc.tinf) / (t0 + 124.0 / cc.tinf) * crm::pow(t0, 1.5);
   double amu2 = B.v(F_AMU, 2, n);
   double amu3 = amu1 + amu2;
   B.v(F_AMU, 1, n) = amu1;
@@ -792,7 +792,7 @@ __global__ void k_viscous_a_mixed(const BlockView* __restrict__ blocks, CaseCons
     gw[d] = (float)cdiff(pw, n, st[d], pos[d], lo[d], hi[d]);
   }
   double t0 = pt[n];
-  double amu1 = (1.0 + 124.0 / cc.tinf) / (t0 + 124.0 / cc.tinf) * pow(t0, 1.5);
+  double amu1 = (1.0 + 124.0 / cc.tinf) / (t0 + 124.0 / cc.tinf) * crm::pow(t0, 1.5);
   double amu2 = B.v(F_AMU, 2, n);
   double amu3d = amu1 + amu2;
   B.v(F_AMU, 1, n) = amu1;

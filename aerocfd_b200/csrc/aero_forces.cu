@@ -139,8 +139,8 @@ __global__ void k_forces_final(const double* __restrict__ part, int npart, CaseC
       out8[x] = fp[x];
       out8[3 + x] = fv[x];
     }
-    out8[6] = ((fp[1] + fv[1]) * cos(cc.aoa) - (fp[0] + fv[0]) * sin(cc.aoa)) * div;
-    out8[7] = ((fp[1] + fv[1]) * sin(cc.aoa) + (fp[0] + fv[0]) * cos(cc.aoa)) * div;
+    out8[6] = ((fp[1] + fv[1]) * cc.cos_aoa - (fp[0] + fv[0]) * cc.sin_aoa) * div;
+    out8[7] = ((fp[1] + fv[1]) * cc.sin_aoa + (fp[0] + fv[0]) * cc.cos_aoa) * div;
   }
 }
 

@@ -15,8 +15,39 @@
 
 namespace aero {
 
-// sub_timeadvancement_1stimplicit.f90:72-156: rhs on the updated nodes and the
-// spectral radii ra, rb, rc and the diagonal on the updated box grown by one.
+// sub_timeadvancement_1stimplicit.f90:108-156, first half: the spectral
+// radii ra, rb, rc on the updated box grown by one.  They need only the
+// primitives and the metrics, so they (and the off-diagonal blocks made from
+// them) can be formed while the fluxes and the time step are computed.
+__global__ void k_lusgs_radii(const BlockView* __restrict__ blocks) {
+  const BlockView& B = blocks[blockIdx.y];
+  const Box& b1 = B.b1;
+  Box e{b1.is - 1, b1.ie + 1, b1.js - 1, b1.je + 1, b1.ks - 1, b1.ke + 1};
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= e.size()) return;
+  int i = e.is + (int)(t % e.nx());
+  long r = t / e.nx();
+  int j = e.js + (int)(r % e.ny());
+  int k = e.ks + (int)(r / e.ny());
+  long n = B.at(i, j, k);
+  double u = B.v(F_PRI, 2, n), v = B.v(F_PRI, 3, n), w = B.v(F_PRI, 4, n), c = B.v(F_PRI, 7, n);
+  double rr[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    double x0 = B.v(F_DXIDX, 3 * d + 1, n), y0 = B.v(F_DXIDX, 3 * d + 2, n), z0 = B.v(F_DXIDX, 3 * d + 3, n);
+    double temp = p2(x0) + p2(y0) + p2(z0);
+    temp = sqrt(temp);
+    double cu = x0 * u + y0 * v + z0 * w;
+    rr[d] = fabs(cu) + fabs(c * temp);
+  }
+  B.s(F_RA, n) = rr[0];
+  B.s(F_RB, n) = rr[1];
+  B.s(F_RC, n) = rr[2];
+}
+
+// sub_timeadvancement_1stimplicit.f90:72-156, second half: rhs = rhsi + rhsv
+// on the updated nodes and diag = phi/dt + ra + rb + rc on the grown box
+// (phi = 0 if cfl >= 1000), from the radii k_lusgs_radii stored.
 __global__ void k_lusgs_prep(const BlockView* __restrict__ blocks, CaseConsts cc_launch) {
   const BlockView& B = blocks[blockIdx.y];
   const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
@@ -34,20 +65,7 @@ __global__ void k_lusgs_prep(const BlockView* __restrict__ blocks, CaseConsts cc
     for (int c = 1; c <= 5; ++c) B.v(F_RHS, c, n) = B.v(F_RHSI, c, n) + B.v(F_RHSV, c, n);
   }
   double phi = cc.cfl >= 1.0e3 ? 0.0 : 1.0;
-  double u = B.v(F_PRI, 2, n), v = B.v(F_PRI, 3, n), w = B.v(F_PRI, 4, n), c = B.v(F_PRI, 7, n);
-  double rr[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    double x0 = B.v(F_DXIDX, 3 * d + 1, n), y0 = B.v(F_DXIDX, 3 * d + 2, n), z0 = B.v(F_DXIDX, 3 * d + 3, n);
-    double temp = p2(x0) + p2(y0) + p2(z0);
-    temp = sqrt(temp);
-    double cu = x0 * u + y0 * v + z0 * w;
-    rr[d] = fabs(cu) + fabs(c * temp);
-  }
-  B.s(F_RA, n) = rr[0];
-  B.s(F_RB, n) = rr[1];
-  B.s(F_RC, n) = rr[2];
-  B.s(F_DIAG, n) = phi * 1.0 / B.s(F_DT, n) + rr[0] + rr[1] + rr[2];
+  B.s(F_DIAG, n) = phi * 1.0 / B.s(F_DT, n) + B.s(F_RA, n) + B.s(F_RB, n) + B.s(F_RC, n);
 }
 
 // calc_jm (sub_timeadvancement_jac.f90:17-62) at node n with the metric row
@@ -177,8 +195,8 @@ __device__ __forceinline__ R* recs(const BlockView& B, bool fwd) {
 // S+ = 0.5*(A + r*I)*inv_j goes to the forward record of the node one step up
 // in d, S- = 0.5*(A - r*I)*inv_j to the backward record of the node one step
 // down (sub_timeadvancement_1stimplicit.f90:283-301, :459-477, same
-// operations).  Each node also stores rhs, diag and inv_j, and the packed
-// positions of its forward and backward neighbours.  R is the record format.
+// operations).  They need q, the metrics, inv_j and the radii only, so they
+// are formed beside the flux and time-step kernels.  R is the record format.
 template <typename R>
 __device__ __forceinline__ void lusgs_mats_body(const BlockView* __restrict__ blocks, CaseConsts cc) {
   constexpr int W = RecFmt<R>::kWords;
@@ -199,22 +217,6 @@ __device__ __forceinline__ void lusgs_mats_body(const BlockView* __restrict__ bl
   int k = B.b.ks + (int)(r / B.ny);
   const int h = (i - b1.is) + (j - b1.js) + (k - b1.ks);
   const int* nb = B.nbr + 6 * p;
-  if (d == 0) {
-    long base = B.poff[h], cnt = B.poff[h + 1] - base, lt = p - base;
-    double* sc = B.sca + kSca * base + lt;
-#pragma unroll
-    for (int x = 0; x < 5; ++x) sc[x * cnt] = B.v(F_RHS, x + 1, n);
-    double diag = B.s(F_DIAG, n), invj = B.s(F_INVJ, n);
-    sc[5 * cnt] = diag;
-    sc[6 * cnt] = invj;
-    sc[7 * cnt] = 1.0 / diag;
-    sc[8 * cnt] = 1.0 / invj;
-    const bool slow = !divisors_ok(diag, invj);
-    RecFmt<R>::set_packed(recs<R>(B, true) + W * base, (int)cnt, lt,
-                          pack_nbrs(nb, h > 0 ? B.poff[h - 1] : 0, slow));
-    RecFmt<R>::set_packed(recs<R>(B, false) + W * base, (int)cnt, lt,
-                          pack_nbrs(nb + 3, h + 1 < B.nplanes ? B.poff[h + 1] : 0, slow));
-  }
   const int up = nb[3 + d];    // forward consumer: the neighbour one step up in d
   const int down = nb[d];      // backward consumer: one step down
   if (up < 0 && down < 0) return;
@@ -291,6 +293,42 @@ __global__ void __launch_bounds__(256, 4) k_lusgs_mats(const BlockView* __restri
 __global__ void __launch_bounds__(256, 4) k_lusgs_mats_f32(const BlockView* __restrict__ blocks, CaseConsts cc) {
   lusgs_mats_body<float>(blocks, cc);
 }
+
+// The per-node part of the sweep records, once rhs and diag are known: rhs,
+// diag, inv_j and their reciprocals in the plane-local scalar layout, and the
+// packed positions of each node's forward and backward neighbours (with the
+// flag that sends its divisions to the IEEE path), one thread per updated
+// node in hyperplane-major order.  R is the record format.
+template <typename R>
+__device__ __forceinline__ void lusgs_sca_body(const BlockView* __restrict__ blocks) {
+  constexpr int W = RecFmt<R>::kWords;
+  const BlockView& B = blocks[blockIdx.y];
+  const Box& b1 = B.b1;
+  long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= b1.size()) return;
+  long n = B.nat[p];
+  long r = n / B.nx;
+  int i = B.b.is + (int)(n - r * B.nx);
+  int j = B.b.js + (int)(r % B.ny);
+  int k = B.b.ks + (int)(r / B.ny);
+  const int h = (i - b1.is) + (j - b1.js) + (k - b1.ks);
+  const int* nb = B.nbr + 6 * p;
+  long base = B.poff[h], cnt = B.poff[h + 1] - base, lt = p - base;
+  double* sc = B.sca + kSca * base + lt;
+#pragma unroll
+  for (int x = 0; x < 5; ++x) sc[x * cnt] = B.v(F_RHS, x + 1, n);
+  double diag = B.s(F_DIAG, n), invj = B.s(F_INVJ, n);
+  sc[5 * cnt] = diag;
+  sc[6 * cnt] = invj;
+  sc[7 * cnt] = 1.0 / diag;
+  sc[8 * cnt] = 1.0 / invj;
+  const bool slow = !divisors_ok(diag, invj);
+  RecFmt<R>::set_packed(recs<R>(B, true) + W * base, (int)cnt, lt, pack_nbrs(nb, h > 0 ? B.poff[h - 1] : 0, slow));
+  RecFmt<R>::set_packed(recs<R>(B, false) + W * base, (int)cnt, lt,
+                        pack_nbrs(nb + 3, h + 1 < B.nplanes ? B.poff[h + 1] : 0, slow));
+}
+__global__ void k_lusgs_sca(const BlockView* __restrict__ blocks) { lusgs_sca_body<double>(blocks); }
+__global__ void k_lusgs_sca_f32(const BlockView* __restrict__ blocks) { lusgs_sca_body<float>(blocks); }
 
 // ---------------------------------------------------------------- sweeps
 namespace {
@@ -1029,6 +1067,25 @@ __device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ bl
     const int cnt = count_of(gs);
     if (g < 5 * cnt) load_row_recs(recs<R>(B, fwd) + W * base, B.sca + kSca * base, cnt, g, pre);
   };
+  // L2 prefetch of plane gs's records and scalars (and, backward, dq*): each
+  // CTA asks for its 1/ncta share of each chunk, so the whole chunk is in L2
+  // before preload() reads it a plane later.  Every chunk starts and ends on a
+  // 16-byte boundary (W * sizeof(R), kSca * 8 and 8 * 8 bytes per node are
+  // multiples of 16), and so does every share.
+  auto prefetch = [&](int gs) {
+    if (gs >= 2 * H || threadIdx.x != 32) return;
+    const bool fwd = gs < H;
+    const long base = poff[plane_of(gs)];
+    const long cnt = count_of(gs);
+    auto share = [&](const void* chunk, long bytes) {
+      const long part = ((bytes + ncta - 1) / ncta + 15) & ~15L;
+      const long off = part * me;
+      if (off < bytes) bulk_prefetch_l2((const char*)chunk + off, (unsigned)min(part, bytes - off));
+    };
+    share(recs<R>(B, fwd) + W * base, (long)W * sizeof(R) * cnt);
+    share(B.sca + kSca * base, (long)kSca * 8 * cnt);
+    if (!fwd) share(B.dqs + 8 * base, 64L * cnt);
+  };
   // failures are stamped with the plane whose wait ran out (the smallest
   // such plane is kept), so a test for "a wait of plane <= p ran out" is
   // exact whatever later planes other warps have reached
@@ -1036,6 +1093,7 @@ __device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ bl
   auto failed_by = [&](int p) { return p >= 0 && *failed_at <= (unsigned)p; };
   auto fail_at = [&](int p) { atomicMin(&s_failed, (unsigned)p); };
   int armed0 = -1, armed1 = -1;  // thread 0: the last plane armed on ring half 0 / 1
+  prefetch(1);
   preload(0);
   for (int gs = 0; gs < 2 * H; ++gs) {
     const bool fwd = gs < H;
@@ -1085,6 +1143,7 @@ __device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ bl
         bulk_to_cluster(map_rank(ring_local + off, threadIdx.x), ring_local + off, bytes,
                         map_rank(bar_local + boff, threadIdx.x));
     }
+    prefetch(gs + 2);
     preload(gs + 1);
   }
   // the last plane's bytes

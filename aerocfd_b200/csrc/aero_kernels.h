@@ -88,7 +88,10 @@ __global__ void k_viscous_b(const BlockView* __restrict__ blocks, CaseConsts cc)
 __global__ void k_find_dt(const BlockView* __restrict__ blocks, CaseConsts cc, double* cta_max);
 __global__ void k_dt_minmax(const BlockView* __restrict__ blocks, int m, const double* cta_max,
                             int ncta, int cta_size, double* out2);
+__global__ void k_lusgs_radii(const BlockView* __restrict__ blocks);
 __global__ void k_lusgs_prep(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_lusgs_sca(const BlockView* __restrict__ blocks);
+__global__ void k_lusgs_sca_f32(const BlockView* __restrict__ blocks);
 __global__ void k_plane_index(const BlockView* __restrict__ blocks);
 __global__ void k_lusgs_mats(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_lusgs_mats_f32(const BlockView* __restrict__ blocks, CaseConsts cc);

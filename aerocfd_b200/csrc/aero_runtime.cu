@@ -74,6 +74,10 @@ struct State {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaEvent_t ev_fork2 = nullptr, ev_join2 = nullptr;  // inviscid beside viscous + find_dt
   cudaEvent_t ev_prep = nullptr, ev_resid = nullptr;   // residual norm beside the LU-SGS sweeps
+  // third stream: the LU-SGS radii and off-diagonal blocks beside the flux and
+  // time-step kernels (they read q, the primitives and the metrics only)
+  cudaStream_t stream3 = nullptr;
+  cudaEvent_t ev_join3 = nullptr;
   std::vector<cudaEvent_t> xfer_ev;  // host transfers: one per array of a batch, plus one
   // dynamic shared memory limits already raised on this device (cudaFuncSetAttribute
   // is per device), per sweep kernel [FP64 records, FP32 records]
@@ -90,6 +94,7 @@ struct State {
   double* arena = nullptr;
   size_t arena_doubles = 0;
   BlockView* d_blocks = nullptr;
+  BlockView* d_blocks_chain = nullptr;  // the views, longest sweep chain first
   std::vector<BlockView> views;
   BcOp* d_bc_ops = nullptr;
   // physical-BC launches: the entries of dependency level L are
@@ -135,6 +140,12 @@ struct State {
   int pmax_all = 0;
   int hmax_all = 0;
   bool mixed = false;  // aero_set_precision(1): FP32 increments in the flux kernels
+  // rhsi holds 0 on every node outside the updated boxes of the registered
+  // blocks (set by init_flowfield and by every full fill; cleared when the
+  // caller uploads rhsi).  The inviscid kernels write only updated nodes and
+  // nothing else writes rhsi, so while it holds the whole-iteration path skips
+  // inviscid_flux_1's full-box zeroing.
+  bool rhsi_ghosts_zero = false;
   // launch shapes (aero_autotune); none of them changes the arithmetic
   struct Tune {
     int inv_tile = 64;  // nodes per CTA of the inviscid flux; 0: face-based kernels
@@ -285,27 +296,37 @@ void fill_view(BlockView& v, const Box& b, const Box& b0, const Box& b1, long pl
 }
 
 // LU-SGS workspace of one view (see BlockView): one device allocation holding
-// poff, rec_f, rec_b, sca, dqs, dq, sa_rec, sa_dq, nat, nbr, pidx.
+// poff, rec_f, rec_b, sca, dqs, dq, sa_rec, sa_dq, nat, nbr, pidx, each array
+// starting on a 256-byte boundary (the sweeps' bulk copies and L2 prefetches
+// of plane chunks need 16-byte aligned starts).
+constexpr size_t kWsAlign = 256;
+constexpr int kWsArrays = 11;
+size_t ws_round(size_t bytes) { return (bytes + kWsAlign - 1) / kWsAlign * kWsAlign; }
 size_t workspace_bytes(const Box& b1, int H) {
   size_t N1 = (size_t)b1.size();
   return (size_t)(H + 1) * sizeof(long) + N1 * (2 * kRec + kSca + 8 + 5 + kSaRec + 1) * sizeof(double) +
-         N1 * sizeof(long) + N1 * 7 * sizeof(int) + 256;
+         N1 * sizeof(long) + N1 * 7 * sizeof(int) + (kWsArrays + 1) * kWsAlign;
 }
 int attach_workspace(BlockView& v, void* ws, const std::vector<long>& poff, int pmax) {
   size_t N1 = (size_t)v.b1.size();
   char* p = (char*)ws;
+  auto take = [&](size_t bytes) {
+    char* at = p;
+    p += ws_round(bytes);
+    return at;
+  };
   v.nplanes = (int)poff.size() - 1;
   v.pmax = pmax;
-  v.rec_f = (double*)p; p += N1 * kRec * sizeof(double);
-  v.rec_b = (double*)p; p += N1 * kRec * sizeof(double);
-  v.sca = (double*)p; p += N1 * kSca * sizeof(double);
-  v.dqs = (double*)p; p += N1 * 8 * sizeof(double);
-  v.dq = (double*)p; p += N1 * 5 * sizeof(double);
-  v.sa_rec = (double*)p; p += N1 * kSaRec * sizeof(double);
-  v.sa_dq = (double*)p; p += N1 * sizeof(double);
-  v.nat = (long*)p; p += N1 * sizeof(long);
-  v.poff = (long*)p; p += poff.size() * sizeof(long);
-  v.nbr = (int*)p;
+  v.rec_f = (double*)take(N1 * kRec * sizeof(double));
+  v.rec_b = (double*)take(N1 * kRec * sizeof(double));
+  v.sca = (double*)take(N1 * kSca * sizeof(double));
+  v.dqs = (double*)take(N1 * 8 * sizeof(double));
+  v.dq = (double*)take(N1 * 5 * sizeof(double));
+  v.sa_rec = (double*)take(N1 * kSaRec * sizeof(double));
+  v.sa_dq = (double*)take(N1 * sizeof(double));
+  v.nat = (long*)take(N1 * sizeof(long));
+  v.poff = (long*)take(poff.size() * sizeof(long));
+  v.nbr = (int*)take(N1 * 7 * sizeof(int));
   v.pidx = v.nbr + 6 * N1;
   CK(cudaMemcpyAsync(v.poff, poff.data(), poff.size() * sizeof(long), cudaMemcpyHostToDevice, g.stream));
   return AERO_OK;
@@ -457,11 +478,15 @@ int launch_getpri(const BlockView* views, int nblk, long maxN, const CaseConsts&
   return AERO_OK;
 }
 // inviscid_flux_1 on nblk views, on stream st (the library's stream when null).
+// fill = false skips the full-box zeroing of rhsi (sub_inviscid1.f90:32-48),
+// for registered blocks whose rhsi is already 0 outside the updated boxes.
 int launch_inviscid(const BlockView* views, int nblk, long maxN, long maxN1, long maxFace, const CaseConsts& cc,
-                    cudaStream_t st = nullptr) {
+                    cudaStream_t st = nullptr, bool fill = true) {
   if (!st) st = g.stream;
-  PROF_ON(P_FILL, st, (k_fill<<<dim3(cdiv(maxN, g.tune.ew), nblk), g.tune.ew, 0, st>>>(views, F_RHSI, 5, 0.0)));
-  CKL();
+  if (fill) {
+    PROF_ON(P_FILL, st, (k_fill<<<dim3(cdiv(maxN, g.tune.ew), nblk), g.tune.ew, 0, st>>>(views, F_RHSI, 5, 0.0)));
+    CKL();
+  }
   const int tile = g.tune.inv_tile;
   if (cc.inviscid == IFLAG_5THWENO || cc.inviscid == IFLAG_5THWCNS) {
     // extension schemes: faces, then the combine
@@ -507,16 +532,41 @@ int launch_dt_minmax(const BlockView* views, int m, double* d_out2) {
   CKL();
   return AERO_OK;
 }
+// The part of implicit1st that needs only q, the primitives and the metrics:
+// the spectral radii and the off-diagonal blocks of the sweeps, on stream st
+// (the library's stream when null).  A steady iteration runs it on its own
+// stream beside the flux and time-step kernels.
+int launch_implicit_blocks(const BlockView* views, int nblk, long maxExt, long maxN1, const CaseConsts& cc,
+                           cudaStream_t st = nullptr) {
+  if (!st) st = g.stream;
+  const int f = g.mixed ? 1 : 0;
+  PROF_ON(P_LUSGS_PREP, st, (k_lusgs_radii<<<dim3(cdiv(maxExt, g.tune.ew), nblk), g.tune.ew, 0, st>>>(views)));
+  CKL();
+  PROF_ON(P_LUSGS_MATS, st, ((f ? k_lusgs_mats_f32 : k_lusgs_mats)<<<dim3(cdiv(3 * maxN1, g.tune.mats), nblk),
+                                                                    g.tune.mats, 0, st>>>(views, cc)));
+  CKL();
+  return AERO_OK;
+}
+
+// The rest of implicit1st after launch_implicit_blocks: rhs and the diagonal,
+// the per-node sweep scalars, the forward and backward sweeps and q += dq.
+// with_blocks also runs launch_implicit_blocks first, on the same stream.
+// sweep_views (null: views) is the view array the sweep kernels index: the
+// same blocks, possibly in another order.
 int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, int pmax, int hmax,
-                    const CaseConsts& cc, cudaEvent_t after_prep = nullptr) {
+                    const CaseConsts& cc, cudaEvent_t after_prep = nullptr, bool with_blocks = true,
+                    const BlockView* sweep_views = nullptr) {
+  const BlockView* sv = sweep_views ? sweep_views : views;
   // mixed precision stores the off-diagonal blocks in FP32 (products and sums
   // stay FP64); f selects that variant of every kernel that touches them
   const int f = g.mixed ? 1 : 0;
+  int rc;
+  if (with_blocks && (rc = launch_implicit_blocks(views, nblk, maxExt, maxN1, cc))) return rc;
   PROF(P_LUSGS_PREP, (k_lusgs_prep<<<dim3(cdiv(maxExt, g.tune.ew), nblk), g.tune.ew, 0, g.stream>>>(views, cc)));
   CKL();
   if (after_prep) CK(cudaEventRecord(after_prep, g.stream));
-  PROF(P_LUSGS_MATS, ((f ? k_lusgs_mats_f32 : k_lusgs_mats)<<<dim3(cdiv(3 * maxN1, g.tune.mats), nblk), g.tune.mats, 0,
-                                                             g.stream>>>(views, cc)));
+  PROF(P_LUSGS_MATS, ((f ? k_lusgs_sca_f32 : k_lusgs_sca)<<<dim3(cdiv(maxN1, g.tune.ew), nblk), g.tune.ew, 0,
+                                                           g.stream>>>(views)));
   CKL();
   // Staged sweep: plane offsets + ring of two planes + nst staged planes
   // (records, scalars, dq*) + 2*nst+1 mbarriers, as many stages as fit
@@ -565,7 +615,7 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
     lc.attrs = at;
     lc.numAttrs = 1;
     cudaError_t le = cudaSuccess;
-    PROF(P_LUSGS_SWEEP, (le = cudaLaunchKernelEx(&lc, kern, views, g.d_status)));
+    PROF(P_LUSGS_SWEEP, (le = cudaLaunchKernelEx(&lc, kern, sv, g.d_status)));
     CK(le);
   } else if (g.tune.sweep_cl >= 2) {
     // one cluster of sweep_cl CTAs per block, one thread per row of every
@@ -585,7 +635,7 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
     lc.attrs = at;
     lc.numAttrs = 1;
     cudaError_t le = cudaSuccess;
-    PROF(P_LUSGS_SWEEP, (le = cudaLaunchKernelEx(&lc, f ? k_lusgs_sweep_cluster_f32 : k_lusgs_sweep_cluster, views)));
+    PROF(P_LUSGS_SWEEP, (le = cudaLaunchKernelEx(&lc, f ? k_lusgs_sweep_cluster_f32 : k_lusgs_sweep_cluster, sv)));
     CK(le);
   } else if (nst >= 2) {
     int consumers = consumers_for(pmax);
@@ -594,8 +644,8 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
       CK(cudaFuncSetAttribute(staged, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       g.smem_staged[f] = smem;
     }
-    PROF(P_LUSGS_SWEEP, (staged<<<nblk, consumers + 32, smem, g.stream>>>(views, nst, g.d_status, g.spin_limit,
-                                                                          g.stall_plane)));
+    PROF(P_LUSGS_SWEEP, (staged<<<nblk, consumers + 32, smem, g.stream>>>(sv, nst, g.d_status, g.spin_limit,
+                                                                       g.stall_plane)));
   } else {
     auto global = f ? k_lusgs_sweep_global_f32 : k_lusgs_sweep_global;
     static int global_max_threads[2] = {0, 0};  // limited by the kernel's registers
@@ -605,7 +655,7 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
       global_max_threads[f] = fa.maxThreadsPerBlock / 32 * 32;
     }
     int threads = (int)std::min<long>(global_max_threads[f], std::max<long>(64, (2L * pmax + 31) / 32 * 32));
-    PROF(P_LUSGS_SWEEP, (global<<<nblk, threads, 0, g.stream>>>(views, 1, g.d_status)));
+    PROF(P_LUSGS_SWEEP, (global<<<nblk, threads, 0, g.stream>>>(sv, 1, g.d_status)));
   }
   CKL();
   PROF(P_LUSGS_UPDATE, (k_lusgs_update<<<dim3(cdiv(maxN1, g.tune.ew), nblk), g.tune.ew, 0, g.stream>>>(views)));
@@ -730,7 +780,10 @@ int do_iteration_crank() {
     if ((rc = do_average1())) return rc;
     if ((rc = do_average2())) return rc;
     if ((rc = do_getpri_all())) return rc;
-    if ((rc = launch_inviscid(g.d_blocks, nb, g.max_box, g.max_b1, g.max_b1_face, g.cc))) return rc;
+    if ((rc = launch_inviscid(g.d_blocks, nb, g.max_box, g.max_b1, g.max_b1_face, g.cc, nullptr,
+                              !g.rhsi_ghosts_zero)))
+      return rc;
+    g.rhsi_ghosts_zero = true;
     if (viscous_on() && (rc = launch_viscous(g.d_blocks, nb, g.max_b0, g.cc, ddes_on()))) return rc;
     if ((rc = launch_crank(g.d_blocks, nb, g.max_box, g.max_b1, &g.max_b1_box, g.cc))) return rc;
   }
@@ -758,8 +811,17 @@ int do_iteration(bool want_dt_minmax, bool resid_beside = false) {
   // what the other writes
   CK(cudaEventRecord(g.ev_fork2, g.stream));
   CK(cudaStreamWaitEvent(g.stream2, g.ev_fork2, 0));
-  if ((rc = launch_inviscid(g.d_blocks, nb, g.max_box, g.max_b1, g.max_b1_face, g.cc, g.stream2))) return rc;
+  if ((rc = launch_inviscid(g.d_blocks, nb, g.max_box, g.max_b1, g.max_b1_face, g.cc, g.stream2,
+                            !g.rhsi_ghosts_zero)))
+    return rc;
+  g.rhsi_ghosts_zero = true;
   CK(cudaEventRecord(g.ev_join2, g.stream2));
+  // the LU-SGS radii and off-diagonal blocks (q, primitives, metrics) beside
+  // both: nothing before the sweeps writes what they read or reads what they
+  // write
+  CK(cudaStreamWaitEvent(g.stream3, g.ev_fork2, 0));
+  if ((rc = launch_implicit_blocks(g.d_blocks, nb, g.max_ext, g.max_b1, g.cc, g.stream3))) return rc;
+  CK(cudaEventRecord(g.ev_join3, g.stream3));
   if (viscous_on() && (rc = launch_viscous(g.d_blocks, nb, g.max_b0, g.cc, ddes_on()))) return rc;
   if ((rc = launch_find_dt(g.d_blocks, nb, g.max_box, g.cc))) return rc;
   if (want_dt_minmax && (rc = launch_dt_minmax(g.d_blocks, nb - 1, g.d_out + 7))) return rc;
@@ -774,8 +836,9 @@ int do_iteration(bool want_dt_minmax, bool resid_beside = false) {
     if ((rc = launch_sa(g.d_blocks, nb, g.max_box, g.max_b1, g.pmax_all, g.cc, g.stream2))) return rc;
     CK(cudaEventRecord(g.ev_join, g.stream2));
   }
+  CK(cudaStreamWaitEvent(g.stream, g.ev_join3, 0));
   if ((rc = launch_implicit(g.d_blocks, nb, g.max_ext, g.max_b1, g.pmax_all, g.hmax_all, g.cc,
-                            resid_beside ? g.ev_prep : nullptr)))
+                            resid_beside ? g.ev_prep : nullptr, false, g.d_blocks_chain)))
     return rc;
   if (resid_beside) {
     CK(cudaStreamWaitEvent(g.stream2, g.ev_prep, 0));
@@ -804,6 +867,8 @@ CaseConsts consts_from(const int* iflags, const double* params) {
   c.c_0 = std::sqrt(t_0) / ma;
   c.cv = 1.0 / c.gamma / (c.gamma - 1.0) / ma / ma;
   c.aoa = params[3] * pi / 180.0;
+  c.cos_aoa = std::cos(c.aoa);
+  c.sin_aoa = std::sin(c.aoa);
   c.dimension = iflags[0]; c.solver = iflags[1]; c.time = iflags[2];
   c.turbulence = iflags[4]; c.des = iflags[5]; c.bufferLength = iflags[6];
   c.inviscid = iflags[7];
@@ -877,6 +942,8 @@ int aero_init(int device) {
   for (int f = 0; f < 2; ++f) g.smem_staged[f] = g.smem_bulk[f] = 0;
   CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
   CK(cudaStreamCreateWithFlags(&g.stream2, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&g.stream3, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&g.ev_join3, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&g.ev_fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&g.ev_join, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&g.ev_fork2, cudaEventDisableTiming));
@@ -901,8 +968,10 @@ static void release_case() {
   }
   g.blocks.clear();
   g.registry.clear();
+  g.rhsi_ghosts_zero = false;
   cudaFree(g.arena); g.arena = nullptr;
   cudaFree(g.d_blocks); g.d_blocks = nullptr;
+  cudaFree(g.d_blocks_chain); g.d_blocks_chain = nullptr;
   cudaFree(g.d_bc_ops); g.d_bc_ops = nullptr;
   cudaFree(g.d_bc_list); g.d_bc_list = nullptr;
   g.bc_lstart.clear();
@@ -940,6 +1009,8 @@ int aero_finalize(void) {
   cudaFreeHost(g.h_out); g.h_out = nullptr;
   cudaStreamDestroy(g.stream); g.stream = nullptr;
   cudaStreamDestroy(g.stream2); g.stream2 = nullptr;
+  cudaStreamDestroy(g.stream3); g.stream3 = nullptr;
+  cudaEventDestroy(g.ev_join3); g.ev_join3 = nullptr;
   cudaEventDestroy(g.ev_fork); g.ev_fork = nullptr;
   cudaEventDestroy(g.ev_join); g.ev_join = nullptr;
   cudaEventDestroy(g.ev_fork2); g.ev_fork2 = nullptr;
@@ -1310,6 +1381,16 @@ int aero_finish_setup(void) {
   }
   CK(cudaMalloc(&g.d_blocks, nb * sizeof(BlockView)));
   CK(cudaMemcpyAsync(g.d_blocks, g.views.data(), nb * sizeof(BlockView), cudaMemcpyHostToDevice, g.stream));
+  // the same views with the longest hyperplane chains first, for the LU-SGS
+  // sweeps: when a batch's sweep CTAs outnumber the SMs, the blocks whose
+  // sweeps take longest are the first to be given SMs
+  {
+    std::vector<BlockView> chain(g.views);
+    std::stable_sort(chain.begin(), chain.end(),
+                     [](const BlockView& a, const BlockView& b) { return a.nplanes > b.nplanes; });
+    CK(cudaMalloc(&g.d_blocks_chain, nb * sizeof(BlockView)));
+    CK(cudaMemcpyAsync(g.d_blocks_chain, chain.data(), nb * sizeof(BlockView), cudaMemcpyHostToDevice, g.stream));
+  }
   // tables
   CK(cudaMalloc(&g.d_bc_ops, std::max<size_t>(1, topo.bc_ops.size()) * sizeof(BcOp)));
   if (!topo.bc_ops.empty())
@@ -1417,6 +1498,12 @@ int aero_finish_setup(void) {
 static int sync_fields(unsigned long long mask, bool to_device) {
   int rc = need_setup();
   if (rc) return rc;
+  if (to_device && (mask & (1ull << F_RHSI)) && g.rhsi_ghosts_zero) {
+    // the uploaded rhsi may be non-zero outside the updated boxes: the next
+    // iteration zeroes it again (a captured step without that fill is stale)
+    g.rhsi_ghosts_zero = false;
+    graph_release();
+  }
   struct Item {
     double* host;
     double* dev;
@@ -1801,6 +1888,7 @@ int aero_init_flowfield(void) {
       for (int x = 0; x < field_nc(fid); ++x)
         if ((rc = put(v.f[fid] + x * v.plane, 0.0))) return rc;
   }
+  g.rhsi_ghosts_zero = true;
   CK(cudaStreamSynchronize(g.stream));
   return AERO_OK;
 }

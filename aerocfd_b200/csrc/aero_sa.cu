@@ -130,8 +130,8 @@ __global__ void k_sa_b(const BlockView* __restrict__ blocks, CaseConsts cc_launc
   double r = nut0 * dv;  // the reference's r (sub_tur_sa.f90:579)
   r = fmin(r, 10.0);
   double g = r + SA_CW2 * (p6(r) - r);
-  double fw = g * pow((1.0 + 64.0) / (p6(g) + 64.0), 1.0 / 6.0);
-  double ft2 = SA_CT3 * exp(-SA_CT4 * p2(leix));
+  double fw = g * crm::pow((1.0 + 64.0) / (p6(g) + 64.0), 1.0 / 6.0);
+  double ft2 = SA_CT3 * crm::exp(-SA_CT4 * p2(leix));
   double aaa = SA_CB1 * ((1.0 - ft2) * fv2 + ft2) / SA_KAR2;
   double bbb = SA_CW1 * fw;
   double ccc = nut0 / p2(dist0);
@@ -151,8 +151,8 @@ __global__ void k_sa_b(const BlockView* __restrict__ blocks, CaseConsts cc_launc
   double rn = (s - sn * nut0) / dv;
   double gn = (1.0 + SA_CW2 * 6.0 * p5(r) - SA_CW2) * rn;
   const double cw3m6 = 0.015625;  // cw3**(-6)
-  double fwn = -((1.0 / 6.0) * pow((pow(g, -6.0) + cw3m6) / (1.0 + cw3m6), -7.0 / 6.0));
-  fwn = fwn / (1.0 + cw3m6) * (-(6.0 * pow(g, -7.0))) * gn;
+  double fwn = -((1.0 / 6.0) * crm::pow((crm::pow(g, -6.0) + cw3m6) / (1.0 + cw3m6), -7.0 / 6.0));
+  fwn = fwn / (1.0 + cw3m6) * (-(6.0 * crm::pow(g, -7.0))) * gn;
   double spn = SA_CB1 * (1.0 - ft2) * omega + SA_CB1 * (-ft2n) * omega * nut0;
   double sdn = (1.0 / re) * (SA_CB1 * (fv2 - ft2 * fv2 + ft2) / SA_KAR2 - SA_CW1 * fw) * 2.0 * nut0 / p2(dist0);
   sdn = (1.0 / re) * (SA_CB1 * (fv2n - ft2n * fv2 - ft2 * fv2n + ft2n) / SA_KAR2 - SA_CW1 * fwn) *
@@ -165,7 +165,8 @@ __global__ void k_sa_b(const BlockView* __restrict__ blocks, CaseConsts cc_launc
 // the records of hyperplane h form one chunk at kSaRec*poff[h], element x of
 // plane-local node t at x*cnt + t, so a warp's loads are consecutive words.
 // x = 0..2: 0.5*(U+|U|) per direction, 3..5: 0.5*(U-|U|), 6: sa_rhs, 7: diag,
-// 8 / 9: the packed forward / backward neighbours.
+// 8 / 9: the packed forward / backward neighbours, 10: 1/diag (the sweeps'
+// exact division by diag uses it), 11: unused (keeps 16-byte chunks).
 __global__ void k_sa_recs(const BlockView* __restrict__ blocks, CaseConsts cc_launch) {
   const BlockView& B = blocks[blockIdx.y];
   const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
@@ -205,15 +206,16 @@ __global__ void k_sa_recs(const BlockView* __restrict__ blocks, CaseConsts cc_la
   const int* nb = B.nbr + 6 * pos;
   rec[8 * cnt] = pack_nbrs(nb, h > 0 ? B.poff[h - 1] : 0);
   rec[9 * cnt] = pack_nbrs(nb + 3, h + 1 < B.nplanes ? B.poff[h + 1] : 0);
+  rec[10 * cnt] = 1.0 / diag;
 }
 
 namespace {
 
 struct SaFwd {
-  double a[3], rhs, diag, packed;
+  double a[3], rhs, diag, rdiag, packed;
 };
 struct SaBwd {
-  double b[3], diag, packed, dqs;
+  double b[3], diag, rdiag, packed, dqs;
   long nat;
 };
 __device__ __forceinline__ void sa_load_fwd(const BlockView& B, int h, int t, SaFwd& f) {
@@ -225,6 +227,7 @@ __device__ __forceinline__ void sa_load_fwd(const BlockView& B, int h, int t, Sa
   f.a[2] = r[2 * cnt];
   f.rhs = r[6 * cnt];
   f.diag = r[7 * cnt];
+  f.rdiag = r[10 * cnt];
   f.packed = r[8 * cnt];
 }
 __device__ __forceinline__ void sa_load_bwd(const BlockView& B, int h, int t, SaBwd& f) {
@@ -235,6 +238,7 @@ __device__ __forceinline__ void sa_load_bwd(const BlockView& B, int h, int t, Sa
   f.b[1] = r[4 * cnt];
   f.b[2] = r[5 * cnt];
   f.diag = r[7 * cnt];
+  f.rdiag = r[10 * cnt];
   f.packed = r[9 * cnt];
   f.dqs = B.sa_dq[base + t];
   f.nat = B.nat[base + t];
@@ -242,11 +246,22 @@ __device__ __forceinline__ void sa_load_bwd(const BlockView& B, int h, int t, Sa
 
 }  // namespace
 
+// L2 prefetch of the SA records of plane h (kSaRec * 8 bytes per node, a
+// multiple of 16, so the chunk starts and ends on 16-byte boundaries).
+__device__ __forceinline__ void sa_prefetch(const BlockView& B, int h) {
+  if (h < 0 || h >= B.nplanes) return;
+  const long base = B.poff[h];
+  const unsigned bytes = (unsigned)((B.poff[h + 1] - base) * kSaRec * 8);
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(B.sa_rec + kSaRec * base), "r"(bytes) : "memory");
+}
+
 // Scalar LU-SGS sweeps of the SA equation and nut += dnut, one CTA per block,
 // one thread per node of a hyperplane (sub_tur_sa.f90:759-818).  Each thread
 // loads the records of its node of the next plane while it computes the
-// current one, so the plane-to-plane path is the shared-memory neighbours,
-// one division and the barrier.
+// current one (one thread prefetches the plane after that into L2), so the
+// plane-to-plane path is the shared-memory neighbours, one division (div_rn_lean
+// with the reciprocal stored in the records: the correctly rounded quotient,
+// as a / b) and the barrier.
 __global__ void __launch_bounds__(1024) k_sa_sweep(const BlockView* __restrict__ blocks) {
   const BlockView& B = blocks[blockIdx.x];
   extern __shared__ double sdn[];  // two planes of pmax values
@@ -257,8 +272,10 @@ __global__ void __launch_bounds__(1024) k_sa_sweep(const BlockView* __restrict__
   {
     SaFwd nx{};
     if (H > 0 && tid < cnt_of(0)) sa_load_fwd(B, 0, tid, nx);
+    if (tid == 32) sa_prefetch(B, 1);
     for (int h = 0; h < H; ++h) {
       const SaFwd cu = nx;
+      if (tid == 32) sa_prefetch(B, h + 2);
       if (h + 1 < H && tid < cnt_of(h + 1)) sa_load_fwd(B, h + 1, tid, nx);
       const long base = B.poff[h];
       const int cnt = (int)(B.poff[h + 1] - base);
@@ -273,7 +290,7 @@ __global__ void __launch_bounds__(1024) k_sa_sweep(const BlockView* __restrict__
           int w = nbr_local(f.packed, d);
           tt[d] = w < 0 ? 0.0 : f.a[d] * prev[w];
         }
-        double v = (f.rhs + (tt[0] + tt[1] + tt[2])) / f.diag;
+        double v = div_rn_lean(f.rhs + (tt[0] + tt[1] + tt[2]), f.diag, f.rdiag);
         cur[t] = v;
         B.sa_dq[base + t] = v;
       }
@@ -282,8 +299,10 @@ __global__ void __launch_bounds__(1024) k_sa_sweep(const BlockView* __restrict__
   }
   SaBwd nx{};
   if (H > 0 && tid < cnt_of(H - 1)) sa_load_bwd(B, H - 1, tid, nx);
+  if (tid == 32) sa_prefetch(B, H - 2);
   for (int h = H - 1; h >= 0; --h) {
     const SaBwd cu = nx;
+    if (tid == 32) sa_prefetch(B, h - 2);
     if (h > 0 && tid < cnt_of(h - 1)) sa_load_bwd(B, h - 1, tid, nx);
     const long base = B.poff[h];
     const int cnt = (int)(B.poff[h + 1] - base);
@@ -298,7 +317,7 @@ __global__ void __launch_bounds__(1024) k_sa_sweep(const BlockView* __restrict__
         int w = nbr_local(f.packed, d);
         tt[d] = w < 0 ? 0.0 : f.b[d] * prev[w];
       }
-      double v = f.dqs - (tt[0] + tt[1] + tt[2]) / f.diag;
+      double v = f.dqs - div_rn_lean(tt[0] + tt[1] + tt[2], f.diag, f.rdiag);
       cur[t] = v;
       B.s(F_NUT, f.nat) = B.s(F_NUT, f.nat) + v;
     }

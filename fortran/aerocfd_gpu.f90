@@ -351,6 +351,14 @@ module aerocfd_gpu
       type(c_ptr) :: aero_profile_name
     end function
 
+    ! test hook: the device's correctly rounded pow (fn 0) and exp (fn 1)
+    integer(c_int) function aero_math_eval(fn, x, y, out, n) bind(C, name="aero_math_eval")
+      import :: c_int, c_double, c_long_long
+      integer(c_int), value :: fn
+      real(c_double) :: x(*), y(*), out(*)
+      integer(c_long_long), value :: n
+    end function
+
     ! residual norms from caller-owned device arrays (arrays of device
     ! addresses, one per block), allocating nothing; sa_rhs is c_loc of an
     ! array of device addresses or c_null_ptr (laminar), out7 the DEVICE

@@ -345,6 +345,15 @@ int aero_profile_read(double* ms, long long* counts, int n);
 const char* aero_profile_name(int id);
 int aero_launch_count(unsigned long long* count);
 
+/* ---- test hook: the device's exact elementary functions ----------------
+ * The FP64 kernels evaluate the reference's x**y and exp(x) with correctly
+ * rounded double-double implementations that give the same bits on the host
+ * (the CPU oracle uses them too).  aero_math_eval runs them on the device for
+ * n host values: fn 0 = pow(x[i], y[i]), fn 1 = exp(x[i]) (y unused), results
+ * in out (host).  It needs no aero_init; it allocates device memory for the
+ * call and synchronises.  No counterpart in the reference (a test hook). */
+int aero_math_eval(int fn, const double* x, const double* y, double* out, long long n);
+
 /* ---- residual of caller-owned device arrays, without allocation --------
  * No counterpart in the reference: it is the computation of
  * sub_output_residual.f90:8-67 (what aero_residual returns) for a caller that

@@ -16,11 +16,22 @@
 // the (component, i, j, k) column-major layout and the Fortran operation order
 // (left-to-right evaluation, x**2 -> x*x, integer powers by GCC's powi chain).
 // Build with -ffp-contract=off so no multiply-add is fused.
+//
+// x**y and exp(x): the reference gets them from the platform libm, which is
+// not specified to the last bit (glibc's pow and exp return a result one ulp
+// off the correctly rounded one on about 1 in 1,200 arguments; CUDA's differ on
+// others).  The oracle and the FP64 GPU kernels both call the correctly
+// rounded crm::pow / crm::exp of aerocfd_b200/csrc/aero_crmath.h (a header of
+// plain arithmetic, host and device), so that libm choices do not separate
+// them; tests/test_crmath.py checks those functions against exact values
+// (Python's decimal) and against glibc on the arguments the solver produces.
 #pragma once
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
+
+#include "../aerocfd_b200/csrc/aero_crmath.h"
 
 namespace oracle {
 
