@@ -61,6 +61,7 @@ __global__ void k_physical_bc(const BlockView* __restrict__ blocks, const BcOp* 
                               const BcEntry* __restrict__ list, int first, CaseConsts cc_launch) {
   const BcEntry e = list[first + blockIdx.y];
   const BlockView& B = blocks[e.blk];
+  if (B.retired()) return;
   const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
   const BcOp op = ops[e.op];
   bool tur = cc.turbulence >= 1;
@@ -140,6 +141,7 @@ __global__ void k_physical_bc(const BlockView* __restrict__ blocks, const BcOp* 
 // clip is overwritten by the upper clip of the unclipped value, as in :80-81.
 __global__ void k_sa_clip(const BlockView* __restrict__ blocks) {
   const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
   long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= B.b.size()) return;
   double d = B.v(F_PRI, 1, n);
@@ -207,6 +209,14 @@ __global__ void k_avg_apply(const BlockView* __restrict__ blocks, const AvgDst* 
   if (with_nut) D.s(F_NUT, a.n) = q[5];
 }
 
+// Retirement (aero_set_retirement): a block whose status word holds any bit
+// stops advancing; its live flag is set once per step, before any kernel of
+// the step reads it.
+__global__ void k_retire(const unsigned* __restrict__ bstat, int* __restrict__ live, int nb) {
+  int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m < nb) live[m] = bstat[m] == 0u ? 1 : 0;
+}
+
 // Residual norm, pass 1: per-CTA partial sums of (rhs*dt/inv_j)^2 (5 values)
 // and (sa_rhs*dt)^2 over the updated nodes (sub_output_residual.f90:32-44).
 __global__ void k_residual_partial(const BlockView* __restrict__ blocks, double* __restrict__ part,
@@ -215,7 +225,8 @@ __global__ void k_residual_partial(const BlockView* __restrict__ blocks, double*
   const Box& b1 = B.b1;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   double v[6] = {0, 0, 0, 0, 0, 0};
-  if (t < b1.size()) {
+  // a retired block contributes zeros (its partial slots are still written)
+  if (t < b1.size() && !B.retired()) {
     int i = b1.is + (int)(t % b1.nx());
     long r = t / b1.nx();
     int j = b1.js + (int)(r % b1.ny());
@@ -240,7 +251,10 @@ __global__ void k_residual_partial(const BlockView* __restrict__ blocks, double*
     for (int c = 0; c < 6; ++c) {
       double x = threadIdx.x < nw ? sm[c][threadIdx.x] : 0.0;
       for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-      if (threadIdx.x == 0) part[6 * ((long)blockIdx.y * gridDim.x + blockIdx.x) + c] = x;
+      if (threadIdx.x == 0) {
+        part[6 * ((long)blockIdx.y * gridDim.x + blockIdx.x) + c] = x;
+        if (!isfinite(x)) B.raise(ST_NONFINITE_RESIDUAL);  // this block's own bit
+      }
     }
   }
 }

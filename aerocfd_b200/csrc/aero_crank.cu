@@ -62,6 +62,7 @@ __device__ __forceinline__ void crank_a(const BlockView& B, int cb, long nb, dou
 // updated nodes.
 __global__ void k_crank_rhs(const BlockView* __restrict__ blocks) {
   const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
   const Box& b1 = B.b1;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= b1.size()) return;
@@ -86,6 +87,7 @@ __global__ void k_crank_rhs(const BlockView* __restrict__ blocks) {
 // reference; along i and j they cover the whole line.
 __global__ void k_crank_sweep(const BlockView* __restrict__ blocks, int d, double gamma) {
   const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
   const Box& b1 = B.b1;
   const int n1[3] = {b1.nx(), b1.ny(), b1.nz()};
   const int lo[3] = {b1.is, b1.js, b1.ks};
@@ -137,6 +139,7 @@ __global__ void k_crank_sweep(const BlockView* __restrict__ blocks, int d, doubl
 // :455-462: q += dq / inv_j on the updated nodes.
 __global__ void k_crank_update(const BlockView* __restrict__ blocks) {
   const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
   const Box& b1 = B.b1;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= b1.size()) return;
@@ -153,6 +156,7 @@ __global__ void k_crank_update(const BlockView* __restrict__ blocks) {
 // main.f90:692-711 on the physical nodes.
 __global__ void k_update_q0(const BlockView* __restrict__ blocks) {
   const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
   const Box& b0 = B.b0;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= b0.size()) return;

@@ -78,6 +78,22 @@ struct BlockView {
   // Case constants of this block when blocks of different cases share one
   // launch (a batch); nullptr: the launch's constants apply.
   const CaseConsts* ccb;
+  // Registered blocks: this block's own status word (the ST_* bits its
+  // kernels raised, besides the global word) and its live flag, refreshed from
+  // the status word at the start of every step while retirement is on
+  // (aero_set_retirement); a block whose flag is 0 is skipped by every kernel
+  // of the step, so its state stays as it was when it failed.  Both nullptr
+  // for the drop-in entry points' temporary views.
+  unsigned* bstat;
+  const int* live;
+  __device__ __forceinline__ bool retired() const { return live && *live == 0; }
+  __device__ __forceinline__ void raise(unsigned bits) const {
+#if defined(__CUDA_ARCH__)
+    if (bstat) atomicOr(bstat, bits);
+#else
+    (void)bits;  // host builds of this header (tests) never call it
+#endif
+  }
 
   __device__ __forceinline__ long at(int i, int j, int k) const {
     return (long)(i - b.is) + (long)nx * ((long)(j - b.js) + (long)ny * (long)(k - b.ks));

@@ -13,6 +13,7 @@ namespace aero {
 // sub_getpri_v.f90:19-62, over the full box of every block.
 __global__ void k_getpri(const BlockView* __restrict__ blocks, CaseConsts cc_launch, unsigned* status) {
   const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
   const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
   long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
   long N = B.b.size();
@@ -33,7 +34,10 @@ __global__ void k_getpri(const BlockView* __restrict__ blocks, CaseConsts cc_lau
   B.v(F_PRI, 5, n) = p;
   B.v(F_PRI, 6, n) = t;
   B.v(F_PRI, 7, n) = c;
-  if (d < 0.0 && status) atomicOr(status, (unsigned)ST_NEG_DENSITY);
+  if (d < 0.0) {
+    if (status) atomicOr(status, (unsigned)ST_NEG_DENSITY);
+    B.raise(ST_NEG_DENSITY);
+  }
 }
 
 // -------------------------------------------------------------- inviscid flux
@@ -59,16 +63,11 @@ __device__ __forceinline__ double weno_left(double u1, double u2, double u3) {
   return w1 * (-u1 / 2.0 + 3.0 * u2 / 2.0) + w2 * (u2 / 2.0 + u3 / 2.0);
 }
 
-// Roe flux at face (node n, node n+s) along `coord` from conservative left/right
-// states (sub_inviscid1.f90:58-74 then sub_inviscid_splitting.f90:65-162).
-__device__ __forceinline__ void roe_face(const BlockView& B, int coord, long n, long ns,
-                                         const double ulc[5], const double urc[5], double gamma,
-                                         double flux[5]) {
-  double dl = ulc[0], ul = ulc[1] / ulc[0], vl = ulc[2] / ulc[0], wl = ulc[3] / ulc[0];
-  double pl = (ulc[4] - 0.5 * (p2(ulc[1]) + p2(ulc[2]) + p2(ulc[3])) / ulc[0]) * (gamma - 1.0);
-  double dr = urc[0], ur = urc[1] / urc[0], vr = urc[2] / urc[0], wr = urc[3] / urc[0];
-  double pr = (urc[4] - 0.5 * (p2(urc[1]) + p2(urc[2]) + p2(urc[3])) / urc[0]) * (gamma - 1.0);
-
+// Roe flux at face (node n, node n+s) along `coord` from primitive left/right
+// states d, u, v, w, p (sub_inviscid_splitting.f90:65-162).
+__device__ __forceinline__ void roe_prim(const BlockView& B, int coord, long n, long ns, double dl, double ul,
+                                         double vl, double wl, double pl, double dr, double ur, double vr, double wr,
+                                         double pr, double gamma, double flux[5]) {
   int c1 = coord * 3 - 2;
   double ja = B.s(F_INVJ, n), jb = B.s(F_INVJ, ns);
   double dxidx1 = 0.5 * (B.v(F_DXIDX, c1, n) * ja + B.v(F_DXIDX, c1, ns) * jb);
@@ -129,6 +128,17 @@ __device__ __forceinline__ void roe_face(const BlockView& B, int coord, long n, 
   flux[2] = 0.5 * (fl2 + fr2 - temp * f2);
   flux[3] = 0.5 * (fl3 + fr3 - temp * f3);
   flux[4] = 0.5 * (fl4 + fr4 - temp * f4);
+}
+// The same from conservative left/right states, converted to primitives as
+// sub_inviscid1.f90:58-74 does.
+__device__ __forceinline__ void roe_face(const BlockView& B, int coord, long n, long ns,
+                                         const double ulc[5], const double urc[5], double gamma,
+                                         double flux[5]) {
+  double dl = ulc[0], ul = ulc[1] / ulc[0], vl = ulc[2] / ulc[0], wl = ulc[3] / ulc[0];
+  double pl = (ulc[4] - 0.5 * (p2(ulc[1]) + p2(ulc[2]) + p2(ulc[3])) / ulc[0]) * (gamma - 1.0);
+  double dr = urc[0], ur = urc[1] / urc[0], vr = urc[2] / urc[0], wr = urc[3] / urc[0];
+  double pr = (urc[4] - 0.5 * (p2(urc[1]) + p2(urc[2]) + p2(urc[3])) / urc[0]) * (gamma - 1.0);
+  roe_prim(B, coord, n, ns, dl, ul, vl, wl, pl, dr, ur, vr, wr, pr, gamma, flux);
 }
 
 // Flux through face pos+1/2 along `coord` starting at node (i,j,k); pos is the
@@ -262,6 +272,7 @@ __device__ __forceinline__ void face_flux_mixed(const BlockView& B, int coord, l
 template <bool MIXED, int TILE>
 __device__ __forceinline__ void inviscid_body(const BlockView* __restrict__ blocks, CaseConsts cc) {
   const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
   const Box& b1 = B.b1;
   __shared__ double dsm[3][5][TILE];
   long t = (long)blockIdx.x * TILE + threadIdx.x;
@@ -325,6 +336,7 @@ __global__ void k_inviscid_mixed_128(const BlockView* __restrict__ blocks, CaseC
 template <bool MIXED>
 __device__ __forceinline__ void faces_body(const BlockView* __restrict__ blocks, CaseConsts cc) {
   const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
   const int d = blockIdx.z;
   if (d >= (cc.dimension == IFLAG_3D ? 3 : 2)) return;
   const Box& b1 = B.b1;
@@ -355,6 +367,7 @@ __global__ void k_inviscid_faces_mixed(const BlockView* __restrict__ blocks, Cas
 
 __global__ void k_inviscid_combine(const BlockView* __restrict__ blocks, CaseConsts cc) {
   const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
   const Box& b1 = B.b1;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= b1.size()) return;
@@ -374,6 +387,57 @@ __global__ void k_inviscid_combine(const BlockView* __restrict__ blocks, CaseCon
     if (ndir == 3) acc = acc - (F[(long)(10 + c) * P + n] - F[(long)(10 + c) * P + n - st[2]]);
     B.v(F_RHSI, c + 1, n) = acc;
   }
+}
+
+// ----------------------------------- the reconstruction and the Riemann solver
+// thirdorder_weno (sub_inviscid_upwind.f90:1-179) and roe_3d
+// (sub_inviscid_splitting.f90:1-172) as stand-alone routines over one block
+// (view 0), for the drop-in entry points aero_thirdorder_weno / aero_roe_3d.
+// Face i stands for i+1/2 along coord, for the faces of r0 grown by one node
+// down along coord (the routines' loops); the states and fluxes are those of
+// face_flux and roe_face, the same operations.
+__device__ __forceinline__ bool face_node(const Box& r0, int coord, long t, int& i, int& j, int& k) {
+  Box e = r0;
+  if (coord == 1) e.is -= 1; else if (coord == 2) e.js -= 1; else e.ks -= 1;
+  if (t >= e.size()) return false;
+  i = e.is + (int)(t % e.nx());
+  long r = t / e.nx();
+  j = e.js + (int)(r % e.ny());
+  k = e.ks + (int)(r / e.ny());
+  return true;
+}
+// f in the F_Q slot, df (left state for direction -1, right for +1) in F_RHSI
+__global__ void k_weno3_states(const BlockView* __restrict__ blocks, int coord, int direction, Box r0) {
+  const BlockView& B = blocks[0];
+  int i, j, k;
+  if (!face_node(r0, coord, (long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+  const long n = B.at(i, j, k);
+  const long st = coord == 1 ? 1 : (coord == 2 ? (long)B.nx : (long)B.nx * B.ny);
+  const int pos = coord == 1 ? i : (coord == 2 ? j : k);
+  const int lo = coord == 1 ? B.b.is : (coord == 2 ? B.b.js : B.b.ks);
+  const int hi = coord == 1 ? B.b.ie : (coord == 2 ? B.b.je : B.b.ke);
+#pragma unroll
+  for (int c = 1; c <= 5; ++c) {
+    double v;
+    if (direction == 1)
+      v = pos == hi - 1 ? B.v(F_Q, c, n + st) : weno_right(B.v(F_Q, c, n), B.v(F_Q, c, n + st), B.v(F_Q, c, n + 2 * st));
+    else
+      v = pos == lo ? B.v(F_Q, c, n) : weno_left(B.v(F_Q, c, n - st), B.v(F_Q, c, n), B.v(F_Q, c, n + st));
+    B.v(F_RHSI, c, n) = v;
+  }
+}
+// primitive ql in the F_Q slot, qr in F_RHSI, the flux to F_RHSV
+__global__ void k_roe_states(const BlockView* __restrict__ blocks, int coord, Box r0, double gamma) {
+  const BlockView& B = blocks[0];
+  int i, j, k;
+  if (!face_node(r0, coord, (long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+  const long n = B.at(i, j, k);
+  const long st = coord == 1 ? 1 : (coord == 2 ? (long)B.nx : (long)B.nx * B.ny);
+  double f[5];
+  roe_prim(B, coord, n, n + st, B.v(F_Q, 1, n), B.v(F_Q, 2, n), B.v(F_Q, 3, n), B.v(F_Q, 4, n), B.v(F_Q, 5, n),
+           B.v(F_RHSI, 1, n), B.v(F_RHSI, 2, n), B.v(F_RHSI, 3, n), B.v(F_RHSI, 4, n), B.v(F_RHSI, 5, n), gamma, f);
+#pragma unroll
+  for (int c = 0; c < 5; ++c) B.v(F_RHSV, c + 1, n) = f[c];
 }
 
 // ------------------------------------------- extension inviscid schemes
@@ -564,6 +628,7 @@ __device__ __forceinline__ double edge3_corr(double v0, double v1, double v2) {
 template <bool MIXED>
 __device__ __forceinline__ void sw_weno5_body(const BlockView* __restrict__ blocks, CaseConsts cc) {
   const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
   const int d = blockIdx.z;
   FaceAt F;
   if (!face_at(B, d, F)) return;
@@ -619,6 +684,7 @@ __global__ void k_faces_sw_weno5_mixed(const BlockView* __restrict__ blocks, Cas
 template <bool MIXED>
 __device__ __forceinline__ void wcns5_body(const BlockView* __restrict__ blocks, CaseConsts cc) {
   const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
   const int d = blockIdx.z;
   FaceAt F;
   if (!face_at(B, d, F)) return;
@@ -665,6 +731,7 @@ __global__ void k_faces_wcns5_mixed(const BlockView* __restrict__ blocks, CaseCo
 // `rhsi = 0.d0`, sub_inviscid1.f90:40, and similar whole-array assignments).
 __global__ void k_fill(const BlockView* __restrict__ blocks, int fid, int nc, double val) {
   const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
   long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
   long N = B.b.size();
   if (n >= N || !B.f[fid]) return;
@@ -685,6 +752,7 @@ __device__ __forceinline__ double cdiff(const double* f, long n, long st, int po
 // fluxes fv,gv,hv (components 2..5 each) go to the FVH scratch field.
 __global__ void k_viscous_a(const BlockView* __restrict__ blocks, CaseConsts cc_launch, int store_dudx_tao) {
   const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
   const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
   const Box& b0 = B.b0;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -766,6 +834,7 @@ __global__ void k_viscous_a(const BlockView* __restrict__ blocks, CaseConsts cc_
 // and the contravariant fluxes are FP32.
 __global__ void k_viscous_a_mixed(const BlockView* __restrict__ blocks, CaseConsts cc_launch, int store_dudx_tao) {
   const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
   const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
   const Box& b0 = B.b0;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -846,6 +915,7 @@ __global__ void k_viscous_a_mixed(const BlockView* __restrict__ blocks, CaseCons
 // sub_viscous.f90:296-365: rhsv = (d fv/dxi + d gv/deta + d hv/dzeta)/re.
 __global__ void k_viscous_b(const BlockView* __restrict__ blocks, CaseConsts cc_launch) {
   const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
   const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
   const Box& b0 = B.b0;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -878,6 +948,7 @@ __global__ void k_viscous_b(const BlockView* __restrict__ blocks, CaseConsts cc_
 // reduction in k_dt_minmax.
 __global__ void k_find_dt(const BlockView* __restrict__ blocks, CaseConsts cc_launch, double* cta_max) {
   const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
   const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
   long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
   long N = B.b.size();

@@ -21,6 +21,7 @@ namespace aero {
 // them) can be formed while the fluxes and the time step are computed.
 __global__ void k_lusgs_radii(const BlockView* __restrict__ blocks) {
   const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
   const Box& b1 = B.b1;
   Box e{b1.is - 1, b1.ie + 1, b1.js - 1, b1.je + 1, b1.ks - 1, b1.ke + 1};
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -50,6 +51,7 @@ __global__ void k_lusgs_radii(const BlockView* __restrict__ blocks) {
 // (phi = 0 if cfl >= 1000), from the radii k_lusgs_radii stored.
 __global__ void k_lusgs_prep(const BlockView* __restrict__ blocks, CaseConsts cc_launch) {
   const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
   const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
   const Box& b1 = B.b1;
   Box e{b1.is - 1, b1.ie + 1, b1.js - 1, b1.je + 1, b1.ks - 1, b1.ke + 1};
@@ -201,6 +203,7 @@ template <typename R>
 __device__ __forceinline__ void lusgs_mats_body(const BlockView* __restrict__ blocks, CaseConsts cc) {
   constexpr int W = RecFmt<R>::kWords;
   const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
   const Box& b1 = B.b1;
   // thread t: direction d = t / N1 and provider position p = t % N1 in the
   // hyperplane-major order, so a warp's record stores go to consecutive
@@ -303,6 +306,7 @@ template <typename R>
 __device__ __forceinline__ void lusgs_sca_body(const BlockView* __restrict__ blocks) {
   constexpr int W = RecFmt<R>::kWords;
   const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
   const Box& b1 = B.b1;
   long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= b1.size()) return;
@@ -449,6 +453,7 @@ __device__ __forceinline__ void lusgs_staged_body(const BlockView* __restrict__ 
                                                   long spin_limit, int stall_plane) {
   constexpr int RD = RecFmt<R>::kWords * (int)sizeof(R) / 8;  // record words per node, in doubles
   const BlockView& B = blocks[blockIdx.x];
+  if (B.retired()) return;
   extern __shared__ __align__(16) unsigned char smem[];
   const int P = B.pmax;
   const int H = B.nplanes;
@@ -610,7 +615,10 @@ __device__ __forceinline__ void lusgs_staged_body(const BlockView* __restrict__ 
   asm volatile("bar.sync 1, %0;" ::"r"(C) : "memory");
   for (int gs = 0; gs < 2 * H; ++gs) {
     if (abort_slot[gs & 1]) {
-      if (threadIdx.x == 0 && status) atomicOr(status, (unsigned)ST_TIMEOUT);
+      if (threadIdx.x == 0) {
+        if (status) atomicOr(status, (unsigned)ST_TIMEOUT);
+        B.raise(ST_TIMEOUT);
+      }
       return;
     }
     const bool fwd = gs < H;
@@ -692,6 +700,7 @@ template <typename R>
 __device__ __forceinline__ void lusgs_global_body(const BlockView* __restrict__ blocks) {
   constexpr int W = RecFmt<R>::kWords;
   const BlockView& B = blocks[blockIdx.x];
+  if (B.retired()) return;
   const int H = B.nplanes;
   const long* poff = B.poff;
   constexpr int kAhead = 3;  // planes prefetched into L2 ahead of the sweep
@@ -878,6 +887,7 @@ __device__ __forceinline__ void lusgs_cluster_body(const BlockView* __restrict__
   constexpr int W = RecFmt<R>::kWords;
   const unsigned ncta = cluster_size();
   const BlockView& B = blocks[blockIdx.x / ncta];
+  if (B.retired()) return;
   const int H = B.nplanes;
   const long* poff = B.poff;
   const int G = (int)(ncta * blockDim.x);
@@ -1036,6 +1046,7 @@ __device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ bl
   __shared__ unsigned s_failed;  // a wait of this CTA ran out (any thread)
   const unsigned ncta = cluster_size(), me = cluster_rank();
   const BlockView& B = blocks[blockIdx.x / ncta];
+  if (B.retired()) return;
   const int H = B.nplanes;
   const long* poff = B.poff;
   const int T = (int)blockDim.x;
@@ -1176,6 +1187,7 @@ __device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ bl
       }
       for (int s = 0; s < 2000; ++s) __nanosleep(1000);
       if (status) atomicOr(status, (unsigned)ST_TIMEOUT);
+      B.raise(ST_TIMEOUT);
     }
     __syncthreads();
   }
@@ -1194,6 +1206,7 @@ __global__ void __launch_bounds__(512, 1) k_lusgs_sweep_bulk_f32(const BlockView
 // through the position index.
 __global__ void k_lusgs_update(const BlockView* __restrict__ blocks) {
   const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
   const Box& b1 = B.b1;
   long u = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= b1.size()) return;

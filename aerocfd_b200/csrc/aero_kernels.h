@@ -88,6 +88,9 @@ __global__ void k_viscous_b(const BlockView* __restrict__ blocks, CaseConsts cc)
 __global__ void k_find_dt(const BlockView* __restrict__ blocks, CaseConsts cc, double* cta_max);
 __global__ void k_dt_minmax(const BlockView* __restrict__ blocks, int m, const double* cta_max,
                             int ncta, int cta_size, double* out2);
+__global__ void k_weno3_states(const BlockView* __restrict__ blocks, int coord, int direction, Box r0);
+__global__ void k_roe_states(const BlockView* __restrict__ blocks, int coord, Box r0, double gamma);
+__global__ void k_retire(const unsigned* __restrict__ bstat, int* __restrict__ live, int nb);
 __global__ void k_lusgs_radii(const BlockView* __restrict__ blocks);
 __global__ void k_lusgs_prep(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_lusgs_sca(const BlockView* __restrict__ blocks);
@@ -98,6 +101,7 @@ __global__ void k_lusgs_mats_f32(const BlockView* __restrict__ blocks, CaseConst
 __global__ void k_sa_length(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_a(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_b(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_sa_b_mixed(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_recs(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_sweep(const BlockView* __restrict__ blocks);
 __global__ void k_lusgs_sweep_staged(const BlockView* __restrict__ blocks, int nst, unsigned* status,

@@ -121,6 +121,9 @@ struct State {
   double* d_surf_out = nullptr;
   CaseConsts* d_ccb = nullptr;   // per-block case constants (batches)
   double* d_resid_blocks = nullptr;  // 7 per block (aero_residual_blocks)
+  unsigned* d_bstat = nullptr;       // per-block status words (aero_get_block_status)
+  int* d_live = nullptr;             // per-block live flags (aero_set_retirement)
+  bool retire = false;               // refresh the live flags from the status words every step
   double* d_out = nullptr;   // residual (7) + dt min/max (2)
   double* h_out = nullptr;   // pinned
   unsigned* d_status = nullptr;
@@ -175,13 +178,14 @@ State g;
 enum ProfId {
   P_GETPRI, P_FILL, P_INVISCID, P_VISC_A, P_VISC_B, P_FIND_DT, P_DT_MINMAX, P_LUSGS_PREP,
   P_LUSGS_MATS, P_LUSGS_SWEEP, P_LUSGS_UPDATE, P_SA_A, P_SA_B, P_SA_RECS, P_SA_SWEEP, P_INDEX, P_BC, P_SA_CLIP, P_HALO, P_AVG_GATHER, P_AVG_APPLY, P_RESID_PART, P_RESID_FINAL,
-  P_TRANSFER, P_GEOMETRY, P_FORCES, P_CRANK, P_NUM
+  P_TRANSFER, P_GEOMETRY, P_FORCES, P_CRANK, P_LUSGS_RADII, P_LUSGS_SCA, P_NUM
 };
 const char* kProfName[P_NUM] = {
     "k_getpri", "k_fill", "k_inviscid", "k_viscous_a", "k_viscous_b", "k_find_dt", "k_dt_minmax",
     "k_lusgs_prep", "k_lusgs_mats", "k_lusgs_sweep", "k_lusgs_update", "k_sa_a", "k_sa_b", "k_sa_recs", "k_sa_sweep",
     "k_plane_index", "k_physical_bc", "k_sa_clip", "k_halo", "k_avg_gather",
-    "k_avg_apply", "k_residual_partial", "k_residual_final", "k_transfer", "k_geometry", "k_forces", "k_crank"};
+    "k_avg_apply", "k_residual_partial", "k_residual_final", "k_transfer", "k_geometry", "k_forces", "k_crank",
+    "k_lusgs_radii", "k_lusgs_sca"};
 struct Prof {
   bool on = false;
   std::vector<cudaEvent_t> pool;
@@ -190,6 +194,10 @@ struct Prof {
   double ms[P_NUM] = {};
   long count[P_NUM] = {};
   unsigned long long launches = 0;
+  // the launches of the last collected batch of marks: class, start and end in
+  // ms after the first of them (aero_profile_timeline)
+  std::vector<int> tl_id;
+  std::vector<double> tl_start, tl_end;
 } gp;
 
 cudaEvent_t prof_event() {
@@ -200,10 +208,11 @@ cudaEvent_t prof_event() {
   }
   return gp.pool[gp.used++];
 }
+int stream_index(cudaStream_t s);
 struct ProfScope {
   int id;
   cudaEvent_t a{}, b{};
-  ProfScope(int id_, cudaStream_t s) : id(id_) {
+  ProfScope(int id_, cudaStream_t s) : id(id_ + 100 * stream_index(s)) {
     ++gp.launches;
     if (gp.on) {
       a = prof_event();
@@ -226,14 +235,27 @@ struct ProfScope {
   } while (0)
 #define PROF(id, launch) PROF_ON(id, g.stream, launch)
 
+// 0 for the library's first stream, 1 and 2 for its second and third
+int stream_index(cudaStream_t s) { return s == g.stream2 ? 1 : (s == g.stream3 ? 2 : 0); }
+
 void prof_collect() {
   if (gp.marks.empty()) return;
   cudaStreamSynchronize(g.stream);
+  cudaDeviceSynchronize();  // marks on the other streams too
+  gp.tl_id.clear();
+  gp.tl_start.clear();
+  gp.tl_end.clear();
+  const cudaEvent_t t0 = gp.marks.front().second.first;
   for (auto& m : gp.marks) {
-    float t = 0.f;
+    float t = 0.f, a = 0.f, b = 0.f;
     cudaEventElapsedTime(&t, m.second.first, m.second.second);
-    gp.ms[m.first] += t;
-    gp.count[m.first] += 1;
+    gp.ms[m.first % 100] += t;
+    gp.count[m.first % 100] += 1;
+    cudaEventElapsedTime(&a, t0, m.second.first);
+    cudaEventElapsedTime(&b, t0, m.second.second);
+    gp.tl_id.push_back(m.first);
+    gp.tl_start.push_back(a);
+    gp.tl_end.push_back(b);
   }
   gp.marks.clear();
   gp.used = 0;
@@ -286,6 +308,8 @@ size_t view_doubles(long plane) {
 void fill_view(BlockView& v, const Box& b, const Box& b0, const Box& b1, long plane, double* base) {
   v.b = b; v.b0 = b0; v.b1 = b1;
   v.ccb = nullptr;
+  v.bstat = nullptr;
+  v.live = nullptr;
   v.nx = b.nx(); v.ny = b.ny();
   v.plane = plane;
   size_t off = 0;
@@ -540,7 +564,7 @@ int launch_implicit_blocks(const BlockView* views, int nblk, long maxExt, long m
                            cudaStream_t st = nullptr) {
   if (!st) st = g.stream;
   const int f = g.mixed ? 1 : 0;
-  PROF_ON(P_LUSGS_PREP, st, (k_lusgs_radii<<<dim3(cdiv(maxExt, g.tune.ew), nblk), g.tune.ew, 0, st>>>(views)));
+  PROF_ON(P_LUSGS_RADII, st, (k_lusgs_radii<<<dim3(cdiv(maxExt, g.tune.ew), nblk), g.tune.ew, 0, st>>>(views)));
   CKL();
   PROF_ON(P_LUSGS_MATS, st, ((f ? k_lusgs_mats_f32 : k_lusgs_mats)<<<dim3(cdiv(3 * maxN1, g.tune.mats), nblk),
                                                                     g.tune.mats, 0, st>>>(views, cc)));
@@ -565,7 +589,7 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
   PROF(P_LUSGS_PREP, (k_lusgs_prep<<<dim3(cdiv(maxExt, g.tune.ew), nblk), g.tune.ew, 0, g.stream>>>(views, cc)));
   CKL();
   if (after_prep) CK(cudaEventRecord(after_prep, g.stream));
-  PROF(P_LUSGS_MATS, ((f ? k_lusgs_sca_f32 : k_lusgs_sca)<<<dim3(cdiv(maxN1, g.tune.ew), nblk), g.tune.ew, 0,
+  PROF(P_LUSGS_SCA, ((f ? k_lusgs_sca_f32 : k_lusgs_sca)<<<dim3(cdiv(maxN1, g.tune.ew), nblk), g.tune.ew, 0,
                                                            g.stream>>>(views)));
   CKL();
   // Staged sweep: plane offsets + ring of two planes + nst staged planes
@@ -678,7 +702,7 @@ int launch_sa(const BlockView* views, int nblk, long maxN, long maxN1, int pmax,
   CKL();
   PROF_ON(P_SA_A, st, (k_sa_a<<<dim3(cdiv(maxN1, 256), nblk), 256, 0, st>>>(views, cc)));
   CKL();
-  PROF_ON(P_SA_B, st, (k_sa_b<<<dim3(cdiv(maxN1, 128), nblk), 128, 0, st>>>(views, cc)));
+  PROF_ON(P_SA_B, st, ((g.mixed ? k_sa_b_mixed : k_sa_b)<<<dim3(cdiv(maxN1, 128), nblk), 128, 0, st>>>(views, cc)));
   CKL();
   PROF_ON(P_SA_RECS, st, (k_sa_recs<<<dim3(cdiv(maxN1, 256), nblk), 256, 0, st>>>(views, cc)));
   CKL();
@@ -801,10 +825,21 @@ int do_iteration_crank() {
 // sa_rhs, none of which is written after k_lusgs_prep and sa_model's rhs) is
 // computed on the second stream beside the LU-SGS sweeps, into g.d_out, and
 // g.ev_resid marks its end.
+// With retirement on: every block whose status word is non-zero stops (its
+// live flag drops to 0 for the whole step).
+int do_retire() {
+  if (!g.retire) return AERO_OK;
+  const int nb = (int)g.blocks.size();
+  PROF(P_BC, (k_retire<<<cdiv(nb, 128), 128, 0, g.stream>>>(g.d_bstat, g.d_live, nb)));
+  CKL();
+  return AERO_OK;
+}
+
 int do_iteration(bool want_dt_minmax, bool resid_beside = false) {
+  int rc;
+  if ((rc = do_retire())) return rc;
   if (crank_on()) return do_iteration_crank();
   int nb = (int)g.blocks.size();
-  int rc;
   if ((rc = do_getpri_all())) return rc;
   // inviscid_flux_1 (rhsi and its face scratch) beside viscous_flux and
   // find_dt (rhsv, amu, vor, dudx, tao, their scratch, dt): neither side reads
@@ -990,6 +1025,9 @@ static void release_case() {
   cudaFree(g.d_ccb); g.d_ccb = nullptr;
   graph_release();
   cudaFree(g.d_resid_blocks); g.d_resid_blocks = nullptr;
+  cudaFree(g.d_bstat); g.d_bstat = nullptr;
+  cudaFree(g.d_live); g.d_live = nullptr;
+  g.retire = false;
   g.nwall = 0;
   g.nquad = 0;
   g.views.clear();
@@ -1237,6 +1275,41 @@ int aero_get_status(unsigned* status) {
   return AERO_OK;
 }
 
+int aero_get_block_status(unsigned* out) {
+  int rc = need_setup();
+  if (rc) return rc;
+  const int nb = (int)g.blocks.size();
+  CK(cudaMemcpyAsync(out, g.d_bstat, nb * sizeof(unsigned), cudaMemcpyDeviceToHost, g.stream));
+  CK(cudaStreamSynchronize(g.stream));
+  return AERO_OK;
+}
+
+int aero_clear_block_status(void) {
+  int rc = need_setup();
+  if (rc) return rc;
+  const int nb = (int)g.blocks.size();
+  std::vector<int> ones(nb, 1);
+  CK(cudaMemsetAsync(g.d_bstat, 0, nb * sizeof(unsigned), g.stream));
+  CK(cudaMemcpyAsync(g.d_live, ones.data(), nb * sizeof(int), cudaMemcpyHostToDevice, g.stream));
+  CK(cudaStreamSynchronize(g.stream));
+  return AERO_OK;
+}
+
+int aero_set_retirement(int on) {
+  int rc = need_setup();
+  if (rc) return rc;
+  if ((on != 0) == g.retire) return AERO_OK;
+  g.retire = on != 0;
+  graph_release();  // the captured step gains or loses the refresh
+  if (!g.retire) {
+    const int nb = (int)g.blocks.size();
+    std::vector<int> ones(nb, 1);
+    CK(cudaMemcpyAsync(g.d_live, ones.data(), nb * sizeof(int), cudaMemcpyHostToDevice, g.stream));
+    CK(cudaStreamSynchronize(g.stream));
+  }
+  return AERO_OK;
+}
+
 int aero_configure(const int* iflags, const double* params) {
   int rc = need_init();
   if (rc) return rc;
@@ -1378,6 +1451,19 @@ int aero_finish_setup(void) {
     CK(cudaMemcpyAsync(g.d_ccb, ccs.data(), nb * sizeof(CaseConsts), cudaMemcpyHostToDevice, g.stream));
     for (int m = 0; m < nb; ++m)
       if (g.blocks[m].own_params) g.views[m].ccb = g.d_ccb + m;
+  }
+  // per-block status words (zero) and live flags (one)
+  CK(cudaMalloc(&g.d_bstat, nb * sizeof(unsigned)));
+  CK(cudaMalloc(&g.d_live, nb * sizeof(int)));
+  CK(cudaMemsetAsync(g.d_bstat, 0, nb * sizeof(unsigned), g.stream));
+  {
+    std::vector<int> ones(nb, 1);
+    CK(cudaMemcpyAsync(g.d_live, ones.data(), nb * sizeof(int), cudaMemcpyHostToDevice, g.stream));
+    CK(cudaStreamSynchronize(g.stream));
+  }
+  for (int m = 0; m < nb; ++m) {
+    g.views[m].bstat = g.d_bstat + m;
+    g.views[m].live = g.d_live + m;
   }
   CK(cudaMalloc(&g.d_blocks, nb * sizeof(BlockView)));
   CK(cudaMemcpyAsync(g.d_blocks, g.views.data(), nb * sizeof(BlockView), cudaMemcpyHostToDevice, g.stream));
@@ -1608,6 +1694,58 @@ int aero_inviscid_flux_1(double* rhsi, const double* q, const double* dxidx, con
   cc.inviscid = IFLAG_3RDWENO;  // this routine is the reference's Roe + WENO3 flux
   long maxFace = std::max({(long)b1.ny() * b1.nz(), (long)b1.nx() * b1.nz(), (long)b1.nx() * b1.ny()});
   if ((rc = launch_inviscid(t.d_view, 1, b.size(), b1.size(), maxFace, cc))) return rc;
+  return finish(t, args);
+}
+
+// thirdorder_weno (sub_inviscid_upwind.f90:1): the WENO3 state at every face
+// of the caller's box is0..ke0 grown by one node down along coord, right
+// (direction 1) or left (direction -1) of the face; df keeps the caller's
+// values elsewhere.  Always transient (the reference calls it on scratch
+// arrays of inviscid_flux_1).
+int aero_thirdorder_weno(double* df, const double* f, const int* is, const int* ie, const int* js, const int* je,
+                         const int* ks, const int* ke, const int* is0, const int* ie0, const int* js0,
+                         const int* je0, const int* ks0, const int* ke0, const int* coord, const int* direction) {
+  int rc = need_init();
+  if (rc) return rc;
+  if (*coord < 1 || *coord > 3) return fail(AERO_ERR_ARG, "thirdorder_weno: coord %d is not 1, 2 or 3", *coord);
+  Box b = box_of(is, ie, js, je, ks, ke), r0 = box_of(is0, ie0, js0, je0, ks0, ke0);
+  std::vector<Arg> args = {{F_Q, f, false}, {F_RHSI, df, true}};
+  BlockTarget t;
+  if ((rc = resolve(b, r0, r0, args, t))) return rc;
+  if (t.resident) return fail(AERO_ERR_ARG, "thirdorder_weno works on unregistered arrays");
+  Box e = r0;
+  if (*coord == 1) e.is -= 1; else if (*coord == 2) e.js -= 1; else e.ks -= 1;
+  // direction 1: right states, -1: left states, anything else: nothing (the
+  // reference's if / else if)
+  if (e.size() > 0 && (*direction == 1 || *direction == -1)) {
+    k_weno3_states<<<cdiv(e.size(), 128), 128, 0, g.stream>>>(t.d_view, *coord, *direction, r0);
+    CKL();
+  }
+  return finish(t, args);
+}
+
+// roe_3d (sub_inviscid_splitting.f90:1): the Roe flux at every face of
+// is0..ke0 grown by one down along coord from primitive states ql, qr
+// (d, u, v, w, p); flux keeps the caller's values elsewhere.  Always transient.
+int aero_roe_3d(const double* ql, const double* qr, double* flux, const double* dxidx, const double* inv_j,
+                const double* gamma, const int* is, const int* ie, const int* js, const int* je, const int* ks,
+                const int* ke, const int* is0, const int* ie0, const int* js0, const int* je0, const int* ks0,
+                const int* ke0, const int* coord) {
+  int rc = need_init();
+  if (rc) return rc;
+  if (*coord < 1 || *coord > 3) return fail(AERO_ERR_ARG, "roe_3d: coord %d is not 1, 2 or 3", *coord);
+  Box b = box_of(is, ie, js, je, ks, ke), r0 = box_of(is0, ie0, js0, je0, ks0, ke0);
+  std::vector<Arg> args = {{F_Q, ql, false}, {F_RHSI, qr, false}, {F_RHSV, flux, true},
+                           {F_DXIDX, dxidx, false}, {F_INVJ, inv_j, false}};
+  BlockTarget t;
+  if ((rc = resolve(b, r0, r0, args, t))) return rc;
+  if (t.resident) return fail(AERO_ERR_ARG, "roe_3d works on unregistered arrays");
+  Box e = r0;
+  if (*coord == 1) e.is -= 1; else if (*coord == 2) e.js -= 1; else e.ks -= 1;
+  if (e.size() > 0) {
+    k_roe_states<<<cdiv(e.size(), 128), 128, 0, g.stream>>>(t.d_view, *coord, r0, *gamma);
+    CKL();
+  }
   return finish(t, args);
 }
 
@@ -2060,6 +2198,19 @@ int aero_profile_read(double* ms, long long* counts, int n) {
 }
 
 const char* aero_profile_name(int id) { return (id >= 0 && id < P_NUM) ? kProfName[id] : ""; }
+
+int aero_profile_timeline(int* ids, double* start_ms, double* end_ms, int n) {
+  int rc = need_init();
+  if (rc) return rc;
+  prof_collect();
+  const int m = (int)gp.tl_id.size();
+  for (int i = 0; i < n && i < m; ++i) {
+    ids[i] = gp.tl_id[i];
+    start_ms[i] = gp.tl_start[i];
+    end_ms[i] = gp.tl_end[i];
+  }
+  return m;
+}
 
 int aero_launch_count(unsigned long long* count) {
   *count = gp.launches;

@@ -36,6 +36,7 @@ __device__ __forceinline__ void node_of(const Box& bx, long t, int& i, int& j, i
 // scratch planes 0..6.
 __global__ void k_sa_a(const BlockView* __restrict__ blocks, CaseConsts cc_launch) {
   const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
   const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
   const Box& b1 = B.b1;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -67,6 +68,7 @@ __global__ void k_sa_a(const BlockView* __restrict__ blocks, CaseConsts cc_launc
 // linearisation diasd (sub_tur_sa.f90:152-208, :359-512, :561-625).
 __global__ void k_sa_b(const BlockView* __restrict__ blocks, CaseConsts cc_launch) {
   const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
   const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
   const Box& b1 = B.b1;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -160,6 +162,109 @@ __global__ void k_sa_b(const BlockView* __restrict__ blocks, CaseConsts cc_launc
   B.s(F_DIASD, n) = fmin(spn + sdn, 0.0);
 }
 
+// k_sa_b for mixed precision (aero_set_precision(1)): the same three terms
+// with their arithmetic in FP32 -- the advection products of FP32 contravariant
+// velocities with FP64 differences of nut, the diffusion products of FP64
+// differences of the scratch planes with FP32 metrics, and the production /
+// destruction closure (fv1, fv2, fw, ft2) -- summed into the FP64 sa_rhs in the
+// order of k_sa_b; diasd likewise.  nut, the metrics, the diagonal and the
+// sweep stay FP64 (the scalar LU-SGS sees only sa_rhs and diasd).
+__global__ void k_sa_b_mixed(const BlockView* __restrict__ blocks, CaseConsts cc_launch) {
+  const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
+  const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
+  const Box& b1 = B.b1;
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= b1.size()) return;
+  int i, j, k;
+  node_of(b1, t, i, j, k);
+  long n = B.at(i, j, k);
+  const long st[3] = {1, (long)B.nx, (long)B.nx * B.ny};
+  const int pos[3] = {i, j, k};
+  const int lo0[3] = {B.b0.is, B.b0.js, B.b0.ks}, hi0[3] = {B.b0.ie, B.b0.je, B.b0.ke};
+  const double* nut = B.f[F_NUT];
+  const double* S = B.f[F_SAS];
+  long P = B.plane;
+  bool three = cc.dimension == IFLAG_3D;
+  const float re = (float)cc.re;
+  float m[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) m[c] = (float)B.v(F_DXIDX, c + 1, n);
+  const float u = (float)B.v(F_PRI, 2, n), v = (float)B.v(F_PRI, 3, n), w = (float)B.v(F_PRI, 4, n);
+  const double nut0d = nut[n];
+  const float nut0 = (float)nut0d;
+  // sa_rhs1: first-order upwind advection
+  float adv[3] = {0.0f, 0.0f, 0.0f};
+  for (int d = 0; d < (three ? 3 : 2); ++d) {
+    float uu = m[3 * d] * u + m[3 * d + 1] * v + m[3 * d + 2] * w;
+    float dm = (float)(nut0d - nut[n - st[d]]), dp = (float)(nut[n + st[d]] - nut0d);
+    adv[d] = -(0.5f * (uu + fabsf(uu)) * dm + 0.5f * (uu - fabsf(uu)) * dp);
+  }
+  double rhs = (double)adv[0] + (double)adv[1] + (double)adv[2];
+  // sa_rhs2: diffusion
+  float ta = (float)d1(S + 3 * P, n, st[0], pos[0], lo0[0], hi0[0]);
+  float tb = (float)d1(S + 4 * P, n, st[1], pos[1], lo0[1], hi0[1]);
+  float tc = three ? (float)d1(S + 5 * P, n, st[2], pos[2], lo0[2], hi0[2]) : 0.0f;
+  float txi = (float)d1(S + 6 * P, n, st[0], pos[0], lo0[0], hi0[0]);
+  float teta = (float)d1(S + 6 * P, n, st[1], pos[1], lo0[1], hi0[1]);
+  float tzeta = three ? (float)d1(S + 6 * P, n, st[2], pos[2], lo0[2], hi0[2]) : 0.0f;
+  float tx = txi * m[0] + teta * m[3] + tzeta * m[6];
+  float ty = txi * m[1] + teta * m[4] + tzeta * m[7];
+  float tz = txi * m[2] + teta * m[5] + tzeta * m[8];
+  const float inv_j0 = (float)B.s(F_INVJ, n);
+  float deltanut = (ta + tb + tc) / inv_j0;
+  float gx = (float)S[0 * P + n], ge = (float)S[1 * P + n], gz = (float)S[2 * P + n];
+  float dnutdx = gx * m[0] + ge * m[3] + gz * m[6];
+  float dnutdy = gx * m[1] + ge * m[4] + gz * m[7];
+  float dnutdz = gx * m[2] + ge * m[5] + gz * m[8];
+  float temp = (float)S[6 * P + n];
+  const float rd = 1.0f / (re * (float)SA_DTA);
+  float diff = -((float)SA_CB2 * rd) * nut0 * deltanut + rd * (temp * deltanut + tx * dnutdx + ty * dnutdy + tz * dnutdz);
+  rhs = rhs + (double)diff;
+  // sa_rhs3: production / destruction
+  const float kar2 = (float)SA_KAR2, cv13 = (float)SA_CV13, cw2 = (float)SA_CW2, cb1 = (float)SA_CB1;
+  const float ct3 = (float)SA_CT3, ct4 = (float)SA_CT4, cw1 = (float)SA_CW1;
+  float nu0 = (float)(B.v(F_AMU, 1, n) / B.v(F_PRI, 1, n));
+  float omega = fabsf((float)B.s(F_VOR, n));
+  float dist2 = (float)p2(B.s(F_LENGTH, n));
+  float leix = fmaxf(nut0 / nu0, 0.001f);
+  float l3 = leix * leix * leix;
+  float fv1 = l3 / (l3 + cv13);
+  float fv2 = 1.0f - leix / (1.0f + leix * fv1);
+  float sv = omega + nut0 * fv2 / (re * kar2 * dist2);
+  sv = fmaxf(sv, 0.3f * omega);
+  float dv = fmaxf(sv * re * kar2 * dist2, 1.0e-6f);
+  float r = fminf(nut0 * dv, 10.0f);  // the reference's r (sub_tur_sa.f90:579)
+  float r2 = r * r, r6 = r2 * r2 * r2;
+  float g = r + cw2 * (r6 - r);
+  float g2 = g * g, g6 = g2 * g2 * g2;
+  float fw = g * powf(65.0f / (g6 + 64.0f), 1.0f / 6.0f);
+  float ft2 = ct3 * expf(-ct4 * leix * leix);
+  float aaa = cb1 * ((1.0f - ft2) * fv2 + ft2) / kar2;
+  float bbb = cw1 * fw;
+  float ccc = nut0 / dist2;
+  float sd = (aaa - bbb) * ccc / re * nut0;
+  float sp = cb1 * (1.0f - ft2) * omega * nut0;
+  rhs = rhs + (double)sd + (double)sp;
+  B.s(F_SARHS, n) = rhs;
+  float leixn = 1.0f / nu0;
+  float fv1n = (3.0f * leix * leix * leixn * (l3 + cv13) - l3 * (3.0f * leix * leix * leixn)) / ((l3 + cv13) * (l3 + cv13));
+  float fv2n = (leixn * (1.0f + leix * fv1) - leix * (leixn * fv1 + leix * fv1n)) / ((1.0f + leix * fv1) * (1.0f + leix * fv1));
+  float ft2n = -(2.0f * ct4 * leix * leixn * ft2);
+  float sn = 1.0f / (re * kar2 * dist2) * (fv2 + fv2n * nut0);
+  dv = fmaxf(sv * sv * (re * kar2 * dist2), 1.0e-6f);
+  float rn = (sv - sn * nut0) / dv;
+  float r5 = r2 * r2 * r;
+  float gn = (1.0f + cw2 * 6.0f * r5 - cw2) * rn;
+  const float cw3m6 = 0.015625f;
+  float fwn = -((1.0f / 6.0f) * powf((powf(g, -6.0f) + cw3m6) / (1.0f + cw3m6), -7.0f / 6.0f));
+  fwn = fwn / (1.0f + cw3m6) * (-(6.0f * powf(g, -7.0f))) * gn;
+  float spn = cb1 * (1.0f - ft2) * omega + cb1 * (-ft2n) * omega * nut0;
+  float sdn = (1.0f / re) * (cb1 * (fv2 - ft2 * fv2 + ft2) / kar2 - cw1 * fw) * 2.0f * nut0 / dist2;
+  sdn = (1.0f / re) * (cb1 * (fv2n - ft2n * fv2 - ft2 * fv2n + ft2n) / kar2 - cw1 * fwn) * (nut0 * nut0 / dist2) + sdn;
+  B.s(F_DIASD, n) = (double)fminf(spn + sdn, 0.0f);
+}
+
 // sa_lusgs diagonal and upwind coefficients of every updated node
 // (sub_tur_sa.f90:676-750, :762-778) in the plane-local layout of the sweep:
 // the records of hyperplane h form one chunk at kSaRec*poff[h], element x of
@@ -169,6 +274,7 @@ __global__ void k_sa_b(const BlockView* __restrict__ blocks, CaseConsts cc_launc
 // exact division by diag uses it), 11: unused (keeps 16-byte chunks).
 __global__ void k_sa_recs(const BlockView* __restrict__ blocks, CaseConsts cc_launch) {
   const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
   const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
   const Box& b1 = B.b1;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -264,6 +370,7 @@ __device__ __forceinline__ void sa_prefetch(const BlockView& B, int h) {
 // as a / b) and the barrier.
 __global__ void __launch_bounds__(1024) k_sa_sweep(const BlockView* __restrict__ blocks) {
   const BlockView& B = blocks[blockIdx.x];
+  if (B.retired()) return;
   extern __shared__ double sdn[];  // two planes of pmax values
   const int P = B.pmax;
   const int H = B.nplanes;
@@ -335,6 +442,7 @@ __global__ void __launch_bounds__(1024) k_sa_sweep(const BlockView* __restrict__
 // layout, N the box size; that is reproduced.
 __global__ void k_sa_length(const BlockView* __restrict__ blocks, CaseConsts cc_launch) {
   const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
   const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
   long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const long N = B.b.size();

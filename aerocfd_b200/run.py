@@ -42,6 +42,8 @@ def main(argv=None) -> int:
                     help="plane exchange of a cluster sweep (default: the autotuner's or L2)")
     ap.add_argument("--no-graphs", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes")
+    ap.add_argument("--tuning", type=int, nargs=5, metavar=("INV_TILE", "EW", "VISC", "MATS", "NST"),
+                    help="launch shapes as aero_set_tuning takes them (instead of the autotuner)")
     args = ap.parse_args(argv)
     case, params = make(args.case, args.inviscid)
     gc = solver.GpuCase(case, block_params=params) if params else solver.GpuCase(case)
@@ -50,7 +52,11 @@ def main(argv=None) -> int:
         gc.init_flowfield()
         gc.start()
         gc.set_precision(args.mixed)
-        tuning = "" if args.no_autotune else gc.autotune(3)
+        if args.tuning:
+            gc.set_tuning(*args.tuning)
+            tuning = ""
+        else:
+            tuning = "" if args.no_autotune else gc.autotune(3)
         if args.sweep_cluster:
             gc.set_sweep_cluster(args.sweep_cluster)
         if args.sweep_exchange:

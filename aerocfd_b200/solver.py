@@ -180,6 +180,20 @@ class GpuCase:
         _lib.check(self.L.aero_get_status(ctypes.byref(s)), "aero_get_status")
         return s.value
 
+    def block_status(self) -> np.ndarray:
+        """aero_get_block_status: every block's status word (not cleared)."""
+        out = np.zeros(len(self.case.blocks), dtype=np.uint32)
+        _lib.check(self.L.aero_get_block_status(ctypes.c_void_p(out.ctypes.data)), "aero_get_block_status")
+        return out
+
+    def clear_block_status(self) -> None:
+        _lib.check(self.L.aero_clear_block_status(), "aero_clear_block_status")
+
+    def set_retirement(self, on: bool = True) -> None:
+        """aero_set_retirement: blocks with a non-zero status word stop
+        advancing from the next step on."""
+        _lib.check(self.L.aero_set_retirement(ctypes.c_int(1 if on else 0)), "aero_set_retirement")
+
     def start(self) -> None:
         """main.f90:249-318 on the device: BCs, primitives, BCs, halo, averaging."""
         self.physical_bc()

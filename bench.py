@@ -534,7 +534,7 @@ def bump_cpu_rate(seconds: float = 4.0):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle  # CPU baseline only
     case = make_bump()
-    oc = oracle.OracleCase(case, fast=True)
+    oc = oracle.OracleCase(case, libm=True)
     oc.geometry()
     oc.init_flowfield()
     oc.start()
@@ -602,7 +602,7 @@ def cpu_reference(make, seconds: float, steps: int = 0, warmup: int = 0):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle  # CPU baseline only
     case = make()
-    oc = oracle.OracleCase(case, fast=True)
+    oc = oracle.OracleCase(case, libm=True)
     oc.geometry()
     oc.init_flowfield()
     oc.start()
@@ -741,7 +741,7 @@ def main():
                 "config": config,
                 "cpu_baseline": {"value": v, "unit": "Mcell-iter/s", "cores": thr, "kind": "port",
                                  "sample": f"{n} full iterations of the workload on {thr} threads "
-                                           f"(one per block), C++ -O3 restatement"},
+                                           f"(one per block), C++ -O3 restatement with glibc's pow/exp"},
                 "e2e": {"value": v, "unit": "Mcell-iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return 0

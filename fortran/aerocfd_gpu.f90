@@ -155,6 +155,21 @@ module aerocfd_gpu
       real(c_double) :: dxidx(9, is:ie, js:je, ks:ke), inv_j(is:ie, js:je, ks:ke), gamma
     end function
 
+    ! thirdorder_weno and roe_3d as routines of their own (unit tests)
+    integer(c_int) function aero_thirdorder_weno(df, f, is, ie, js, je, ks, ke, is0, ie0, js0, je0, ks0, ke0, &
+        coord, direction) bind(C, name="aero_thirdorder_weno")
+      import :: c_int, c_double
+      real(c_double) :: df(*), f(*)
+      integer(c_int) :: is, ie, js, je, ks, ke, is0, ie0, js0, je0, ks0, ke0, coord, direction
+    end function
+
+    integer(c_int) function aero_roe_3d(ql, qr, flux, dxidx, inv_j, gamma, is, ie, js, je, ks, ke, &
+        is0, ie0, js0, je0, ks0, ke0, coord) bind(C, name="aero_roe_3d")
+      import :: c_int, c_double
+      real(c_double) :: ql(*), qr(*), flux(*), dxidx(*), inv_j(*), gamma
+      integer(c_int) :: is, ie, js, je, ks, ke, is0, ie0, js0, je0, ks0, ke0, coord
+    end function
+
     ! Steger-Warming splitting + WENO5 (no counterpart in the reference: iflag_inviscid = 5, bufferLength = 3)
     integer(c_int) function aero_inviscid_flux_weno5(rhsi, q, dxidx, inv_j, is, ie, js, je, ks, ke, &
         is0, ie0, js0, je0, ks0, ke0, is1, ie1, js1, je1, ks1, ke1, gamma) bind(C, name="aero_inviscid_flux_weno5")
@@ -256,6 +271,21 @@ module aerocfd_gpu
       integer(c_int) :: status
     end function
 
+    ! per-block status words and retirement of failed blocks (batches)
+    integer(c_int) function aero_get_block_status(out) bind(C, name="aero_get_block_status")
+      import :: c_int
+      integer(c_int) :: out(*)
+    end function
+
+    integer(c_int) function aero_clear_block_status() bind(C, name="aero_clear_block_status")
+      import :: c_int
+    end function
+
+    integer(c_int) function aero_set_retirement(on) bind(C, name="aero_set_retirement")
+      import :: c_int
+      integer(c_int), value :: on
+    end function
+
     ! sub_tur_sa.f90:7 (sa_model; main.f90:415, :538).  The arrays are passed
     ! by address as the reference passes them: dxidx and dudx are the blocks'
     ! (9, ...) arrays that sa_model views as (3, ..., 3).
@@ -349,6 +379,13 @@ module aerocfd_gpu
       import :: c_int, c_ptr
       integer(c_int), value :: id
       type(c_ptr) :: aero_profile_name
+    end function
+
+    integer(c_int) function aero_profile_timeline(ids, start_ms, end_ms, n) bind(C, name="aero_profile_timeline")
+      import :: c_int, c_double
+      integer(c_int) :: ids(*)
+      real(c_double) :: start_ms(*), end_ms(*)
+      integer(c_int), value :: n
     end function
 
     ! test hook: the device's correctly rounded pow (fn 0) and exp (fn 1)

@@ -85,6 +85,24 @@ const char* aero_last_error(void);
 /* OR of the device status bits raised since the last call; clears them. */
 int aero_get_status(unsigned* status);
 
+/* Per-block status and retirement (batches of independent cases, where a
+ * case is one block; no counterpart in the reference, which stops the run).
+ * Every registered block has its own status word, raised with the same
+ * AERO_ST_* bits as the global one by that block's kernels (negative density
+ * in get_primitivevariables, a non-finite partial sum of its residual, a
+ * sweep wait that ran out).  aero_get_block_status copies the nblocks words
+ * (block m at out[m-1]) without clearing them; aero_clear_block_status clears
+ * them.  With aero_set_retirement(1) every step begins by retiring each block
+ * whose word is non-zero: no kernel of the step touches it, so its state stays
+ * as it was after the step that raised the bit, its residual norms count as 0
+ * (aero_residual, aero_residual_blocks) and the other blocks advance as if it
+ * were not there (their kernels never read another block, halos aside: retire
+ * a multi-block case as a whole).  Clearing a block's word brings it back at
+ * the next step; aero_set_retirement(0) (the default) brings every block back. */
+int aero_get_block_status(unsigned* out);
+int aero_clear_block_status(void);
+int aero_set_retirement(int on);
+
 /* ---- case set-up (replaces init_readcontrolfile / init_readbcinfo /
  *      init_allocatememory module state, main.f90:80-140) ---------------- */
 /* iflags[8]: iflag_dimension, iflag_solver, iflag_time, iflag_timeadvance,
@@ -136,6 +154,25 @@ int aero_inviscid_flux_1(double* rhsi, const double* q, const double* dxidx, con
                          const int* js0, const int* je0, const int* ks0, const int* ke0,
                          const int* is1, const int* ie1, const int* js1, const int* je1,
                          const int* ks1, const int* ke1, const double* gamma);
+
+/* thirdorder_weno(df,f,is..ke,is0..ke0,coord,direction)
+ * sub_inviscid_upwind.f90:1 -- the WENO3 states of inviscid_flux_1 as a
+ * routine of its own (for unit tests, as the reference's internal entry
+ * point): at every face i+1/2 of is0..ke0 grown by one node down along coord,
+ * df = the right state (direction 1) or the left state (direction -1; any
+ * other value writes nothing, as in the reference); df keeps its values at
+ * the other nodes.  Unregistered arrays only. */
+int aero_thirdorder_weno(double* df, const double* f, const int* is, const int* ie, const int* js, const int* je,
+                         const int* ks, const int* ke, const int* is0, const int* ie0, const int* js0,
+                         const int* je0, const int* ks0, const int* ke0, const int* coord, const int* direction);
+/* roe_3d(ql,qr,flux,dxidx,inv_j,gamma,is..ke,is0..ke0,coord)
+ * sub_inviscid_splitting.f90:1 -- the Roe flux with Harten's fix at the same
+ * faces from primitive states ql, qr (d, u, v, w, p); flux keeps its values
+ * at the other nodes.  Unregistered arrays only. */
+int aero_roe_3d(const double* ql, const double* qr, double* flux, const double* dxidx, const double* inv_j,
+                const double* gamma, const int* is, const int* ie, const int* js, const int* je, const int* ks,
+                const int* ke, const int* is0, const int* ie0, const int* js0, const int* je0, const int* ks0,
+                const int* ke0, const int* coord);
 /* Extension schemes with inviscid_flux_1's argument list (no counterpart in
  * the reference, which defines iflag_inviscid = 5 and 8 in module_flags.f90:68,
  * 71 but stops on them in GetBufferLength, main.f90:636-653): Steger-Warming
@@ -343,6 +380,14 @@ int aero_mlp_predict(const float* x, long long n, float* y);
 int aero_profile(int enable);
 int aero_profile_read(double* ms, long long* counts, int n);
 const char* aero_profile_name(int id);
+/* The launches timed since the previous read (in launch order): their class
+ * ids[i], and start_ms[i] / end_ms[i], the times of the events recorded on
+ * their own streams before and after them, in milliseconds after the first
+ * launch's start; ids[i] = class + 100 x the stream (0 the library's first
+ * stream, 1 and 2 its others).  Fills at most n entries and returns how many launches
+ * there were.  Kernels on the library's other streams overlap those on its
+ * first, so this is the time line of a step, not a sum of durations. */
+int aero_profile_timeline(int* ids, double* start_ms, double* end_ms, int n);
 int aero_launch_count(unsigned long long* count);
 
 /* ---- test hook: the device's exact elementary functions ----------------

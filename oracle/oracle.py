@@ -19,12 +19,15 @@ _LIBS = {}
 
 
 def build() -> None:
-    """Compiles both oracle variants (make, in this directory)."""
+    """Compiles the three oracle builds (make, in this directory)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
-def lib(fast: bool = False) -> ctypes.CDLL:
-    name = "liboracle_fast.so" if fast else "liboracle.so"
+def lib(fast: bool = False, libm: bool = False) -> ctypes.CDLL:
+    """The bounds-checked build (default), the -O3 build (fast) or the -O3
+    build with the platform libm's pow and exp (libm: the timed CPU
+    baseline; the others use the correctly rounded pow and exp the GPU uses)."""
+    name = "liboracle_libm.so" if libm else ("liboracle_fast.so" if fast else "liboracle.so")
     if name not in _LIBS:
         path = os.path.join(HERE, "_build", name)
         if not os.path.exists(path):
@@ -54,9 +57,9 @@ class OracleCase:
     """Registers a Case's host arrays with the oracle (the oracle works on them
     in place) and exposes the module-level routines."""
 
-    def __init__(self, case, fast: bool = False):
+    def __init__(self, case, fast: bool = False, libm: bool = False):
         self.case = case
-        self.L = lib(fast)
+        self.L = lib(fast, libm)
         L = self.L
         L.oracle_reset()
         L.oracle_configure(case.cfg.iflags().ctypes.data_as(ctypes.c_void_p),

@@ -465,7 +465,7 @@ void viscous_flux(V rhsv, V pri_v, V amu, V vor, V dudx, V tao, V dxidx, V inv_j
     for (int j = b0.js; j <= b0.je; ++j)
       for (int i = b0.is; i <= b0.ie; ++i) {
         double u0 = u(i, j, k), v0 = v(i, j, k), w0 = w(i, j, k), t0 = t(i, j, k);
-        amu(1, i, j, k) = (1.0 + 124.0 / tinf) / (t0 + 124.0 / tinf) * crm::pow(t0, 1.5);
+        amu(1, i, j, k) = (1.0 + 124.0 / tinf) / (t0 + 124.0 / tinf) * xpow(t0, 1.5);
         amu(3, i, j, k) = amu(1, i, j, k) + amu(2, i, j, k);
         double ki = gamma * cv * (amu(1, i, j, k) / prl + amu(2, i, j, k) / prt);
         double tx = txi(i, j, k) * dxidx(1, i, j, k) + teta(i, j, k) * dxidx(4, i, j, k) +
@@ -829,8 +829,8 @@ static void sa_rhs3(V sa_rhs, V nut, V pri_v, V amu, V vor, V length, V diasd, d
         double r = nut0 * div;
         r = std::min(r, 10.0);
         double g = r + SA_CW2 * (p6(r) - r);
-        double fw = g * crm::pow((1.0 + 64.0) / (p6(g) + 64.0), 1.0 / 6.0);
-        double ft2 = SA_CT3 * crm::exp(-SA_CT4 * p2(leix));
+        double fw = g * xpow((1.0 + 64.0) / (p6(g) + 64.0), 1.0 / 6.0);
+        double ft2 = SA_CT3 * xexp(-SA_CT4 * p2(leix));
         double aaa = SA_CB1 * ((1.0 - ft2) * fv2 + ft2) / SA_KAR2;
         double bbb = SA_CW1 * fw;
         double ccc = nut0 / p2(dist0);
@@ -850,8 +850,8 @@ static void sa_rhs3(V sa_rhs, V nut, V pri_v, V amu, V vor, V length, V diasd, d
         double rn = (s - sn * nut0) / div;
         double gn = (1.0 + SA_CW2 * 6.0 * p5(r) - SA_CW2) * rn;
         const double cw3m6 = 0.015625;  // cw3**(-6.d0), folded
-        double fwn = -((1.0 / 6.0) * crm::pow((crm::pow(g, -6.0) + cw3m6) / (1.0 + cw3m6), -7.0 / 6.0));
-        fwn = fwn / (1.0 + cw3m6) * (-(6.0 * crm::pow(g, -7.0))) * gn;
+        double fwn = -((1.0 / 6.0) * xpow((xpow(g, -6.0) + cw3m6) / (1.0 + cw3m6), -7.0 / 6.0));
+        fwn = fwn / (1.0 + cw3m6) * (-(6.0 * xpow(g, -7.0))) * gn;
         double spn = SA_CB1 * (1.0 - ft2) * omega + SA_CB1 * (-ft2n) * omega * nut0;
         double sdn = (1.0 / re) * (SA_CB1 * (fv2 - ft2 * fv2 + ft2) / SA_KAR2 - SA_CW1 * fw) * 2.0 * nut0 / p2(dist0);
         sdn = (1.0 / re) * (SA_CB1 * (fv2n - ft2n * fv2 - ft2 * fv2n + ft2n) / SA_KAR2 - SA_CW1 * fwn) *

@@ -161,7 +161,7 @@ static void bc_farfield(Block& B, const Box& sb, int face) {  // sub_bc_-10_farf
   double gamma = c.gamma;
   double d_inf = c.d_0, u_inf = c.u_0 * std::cos(c.aoa), v_inf = c.u_0 * std::sin(c.aoa), w_inf = 0.0;
   double p_inf = c.p_0;
-  double s_inf = c.p_0 / crm::pow(c.d_0, gamma);
+  double s_inf = c.p_0 / xpow(c.d_0, gamma);
   double c_inf = c.c_0;
   (void)d_inf; (void)p_inf;
   for_face(face, sb, [&](int i, int j, int k, int di, int dj, int dk, int s) {
@@ -181,7 +181,7 @@ static void bc_farfield(Block& B, const Box& sb, int face) {  // sub_bc_-10_farf
     double w_p = q(4, ii, jj, kk) / d_p;
     double p_p = (q(5, ii, jj, kk) - 0.5 * d_p * (p2(u_p) + p2(v_p) + p2(w_p))) * (gamma - 1.0);
     double c_p = std::sqrt(gamma * p_p / d_p);
-    double s_p = p_p / crm::pow(d_p, gamma);
+    double s_p = p_p / xpow(d_p, gamma);
     double vn_inf = u_inf * x0 + v_inf * y0 + w_inf * z0;
     double vn_p = u_p * x0 + v_p * y0 + w_p * z0;
     double rm = vn_inf - 2.0 * c_inf / (gamma - 1.0);
@@ -198,8 +198,8 @@ static void bc_farfield(Block& B, const Box& sb, int face) {  // sub_bc_-10_farf
     double u_b = u_ref + (vn_b - u_ref_t) * x0;
     double v_b = v_ref + (vn_b - u_ref_t) * y0;
     double w_b = w_ref + (vn_b - u_ref_t) * z0;
-    double d_b = crm::pow(c_p * c_p / (gamma * s_b), 1.0 / (gamma - 1.0));  // c_p, as the reference (:93)
-    double p_b = s_b * crm::pow(d_b, gamma);
+    double d_b = xpow(c_p * c_p / (gamma * s_b), 1.0 / (gamma - 1.0));  // c_p, as the reference (:93)
+    double p_b = s_b * xpow(d_b, gamma);
     q(1, i, j, k) = d_b;
     q(2, i, j, k) = d_b * u_b;
     q(3, i, j, k) = d_b * v_b;

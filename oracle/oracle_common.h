@@ -20,11 +20,14 @@
 // x**y and exp(x): the reference gets them from the platform libm, which is
 // not specified to the last bit (glibc's pow and exp return a result one ulp
 // off the correctly rounded one on about 1 in 1,200 arguments; CUDA's differ on
-// others).  The oracle and the FP64 GPU kernels both call the correctly
-// rounded crm::pow / crm::exp of aerocfd_b200/csrc/aero_crmath.h (a header of
-// plain arithmetic, host and device), so that libm choices do not separate
-// them; tests/test_crmath.py checks those functions against exact values
-// (Python's decimal) and against glibc on the arguments the solver produces.
+// others).  The oracle builds used as the checker and the FP64 GPU kernels
+// both call the correctly rounded crm::pow / crm::exp of
+// aerocfd_b200/csrc/aero_crmath.h (a header of plain arithmetic, host and
+// device), so that libm choices do not separate them; tests/test_crmath.py
+// checks those functions against exact values (Python's decimal) and against
+// glibc on the arguments the solver produces.  The build timed as the CPU
+// baseline (liboracle_libm.so) calls glibc's pow and exp instead, as the
+// reference does, so its speed is the reference's.
 #pragma once
 #include <cmath>
 #include <cstdio>
@@ -32,6 +35,26 @@
 #include <vector>
 
 #include "../aerocfd_b200/csrc/aero_crmath.h"
+
+namespace oracle {
+// x**y and exp(x) of the restatement: the shared correctly rounded functions,
+// or, in the build timed as the CPU baseline (ORACLE_PLATFORM_LIBM), the
+// platform libm that the reference's own build calls.
+inline double xpow(double x, double y) {
+#ifdef ORACLE_PLATFORM_LIBM
+  return std::pow(x, y);
+#else
+  return crm::pow(x, y);
+#endif
+}
+inline double xexp(double x) {
+#ifdef ORACLE_PLATFORM_LIBM
+  return std::exp(x);
+#else
+  return crm::exp(x);
+#endif
+}
+}  // namespace oracle
 
 namespace oracle {
 

@@ -158,3 +158,51 @@ def test_sweep_cluster_gives_the_same_bits(gpu, make):
             for a, b in zip(out[1] + out[2], ref[1] + ref[2]):
                 assert np.array_equal(a, b), (mixed, ctas, shared)
 
+
+
+def test_failed_case_is_retired_and_the_others_follow_their_own_cases(gpu, oracle_mod):
+    """A NaN planted on the host in one case of a running batch (between two
+    steps, at an interior node): the next step raises that block's own
+    non-finite-residual bit and no other block's; with retirement on, the
+    failed case is frozen from then on (its q keeps the bits it had after the
+    failing step, its residual counts as 0), and every other case still
+    follows the oracle's run of that case alone, to the end."""
+    ST_NONFINITE = 2
+    cases = small_batch()
+    nsteps = 7
+    hist = [run_oracle(oracle_mod, c, nsteps) for c in cases]
+    batch, gc = started_batch(gpu, small_batch())
+    bad = 2
+    try:
+        gc.set_retirement(True)
+        gc.step(2, history=False)
+        assert not gc.block_status().any()
+        gc.sync_to_host(gpu.mask("q"))
+        b = batch.blocks[bad]
+        i, j, k = b.box1[0] + 3, b.box1[2] + 2, b.box1[4] + 1
+        b.fields["q"][k - b.box[4], j - b.box[2], i - b.box[0], 0] = np.nan
+        gc.sync_to_device(gpu.mask("q"))
+        gc.step(1, history=False)
+        st = gc.block_status()
+        assert st[bad] & ST_NONFINITE, st
+        assert not np.delete(st, bad).any(), st
+        gc.sync_to_host(gpu.mask("q"))
+        frozen = b.fields["q"].copy()
+        assert np.isnan(frozen).any()
+        gc.step(nsteps - 3, history=False)
+        r = gc.residual_blocks()
+        assert np.array_equal(gc.block_status(), st)
+        gc.sync_to_host(gpu.mask("q"))
+        assert np.array_equal(b.fields["q"], frozen, equal_nan=True)
+        assert np.all(r[bad] == 0.0)
+        for m, c in enumerate(cases):
+            if m == bad:
+                continue
+            h = hist[m][-1, :5]
+            scale = np.maximum(np.abs(h), 1e-6 * np.abs(h).max())
+            assert np.max(np.abs(r[m, :5] - h) / scale) <= 1e-10, m
+            assert relerr(batch.blocks[m].fields["q"], c.blocks[0].fields["q"]) <= TOL, m
+        gc.clear_block_status()
+        assert not gc.block_status().any()
+    finally:
+        gc.close()

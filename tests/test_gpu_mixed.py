@@ -94,3 +94,33 @@ def test_mixed_fluxes_close_to_fp64(gpu):
             assert e[0] <= 1e-5, (k, e)
     finally:
         gc.close()
+
+
+def test_mixed_sa_plate_close_to_fp64(gpu):
+    """SA flat plate (2x2x2 blocks, wall spacing 1e-4): the mixed path, with
+    the SA advection, diffusion and production/destruction terms in FP32,
+    against FP64 after 10 iterations from one state: q and nu_t max error
+    1e-6 and 1e-5 of their maxima, residual history (mean flow and nu_t)
+    1e-3 relative."""
+    from aerocfd_b200.case import Config, IFLAG_NSSOLVER
+    make = lambda: grids.flat_plate(ni=33, nj=25, nk=9, dy_wall=1e-4, cfg=Config(
+        solver=IFLAG_NSSOLVER, turbulence=2, ma=0.2, re=1.0e5, cfl=2.0, nutinf=3.0))
+    case, gc = started(gpu, make, steps=5)
+    try:
+        snap = snapshot(gc, case, gpu)
+        h64 = gc.step(10)
+        gc.sync_to_host(gpu.mask("q", "nut"))
+        ref = {k: np.concatenate([b.fields[k].ravel().copy() for b in case.blocks]) for k in ("q", "nut")}
+        restore(gc, case, gpu, snap)
+        gc.set_precision(True)
+        hmx = gc.step(10)
+        gc.sync_to_host(gpu.mask("q", "nut"))
+        gc.set_precision(False)
+        eq = errs(np.concatenate([b.fields["q"].ravel() for b in case.blocks]), ref["q"])
+        en = errs(np.concatenate([b.fields["nut"].ravel() for b in case.blocks]), ref["nut"])
+        rh = np.max(np.abs(hmx[:, :6] - h64[:, :6]) / np.max(np.abs(h64[:, :6]), axis=0, keepdims=True))
+        print(f"SA mixed vs fp64 after 10 iterations: q {eq}, nut {en}, residual history {rh:.2e}")
+        assert eq[0] <= 1e-6 and en[0] <= 1e-5 and rh <= 1e-3
+        assert gc.status() == 0
+    finally:
+        gc.close()

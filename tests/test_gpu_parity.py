@@ -89,6 +89,51 @@ def test_getpri_and_inviscid_transient(gpu, oracle_mod):
     gc.close()
 
 
+@pytest.mark.parametrize("coord", [1, 2, 3])
+def test_thirdorder_weno_and_roe_3d_transient(gpu, oracle_mod, coord):
+    """thirdorder_weno and roe_3d as routines of their own (the reference's
+    internal entry points): right and left WENO3 states on every face of the
+    updated box grown by one, then the Roe flux from their primitives, bit for
+    bit against the oracle; nodes the routines do not write keep the
+    caller's values."""
+    oc, co, cg = prepared(bump_small, oracle_mod, seed=21)
+    gc = gpu.GpuCase(cg)
+    try:
+        b = co.blocks[0]
+        F = b.fields
+        ob = oracle_mod.box_args
+        rng = np.random.default_rng(coord)
+        states = {}
+        for direction in (1, -1):
+            fill = rng.standard_normal(F["q"].shape)
+            dg, do = fill.copy(), fill.copy()
+            assert gc.L.aero_thirdorder_weno(_p(dg), _p(F["q"]), *[_i(v) for v in b.box + b.box1], _i(coord),
+                                             _i(direction)) == 0
+            oc.L.oracle_thirdorder_weno(_p(do), _p(F["q"]), *ob(b.box), *ob(b.box1), _i(coord), _i(direction))
+            assert np.array_equal(dg, do), direction
+            assert (dg != fill).any()
+            states[direction] = dg
+        # primitives of the states (sub_inviscid1.f90:58-74), then the flux
+        prim = {}
+        for d, u in states.items():
+            p = np.empty_like(u)
+            p[..., 0] = u[..., 0]
+            p[..., 1:4] = u[..., 1:4] / u[..., 0:1]
+            p[..., 4] = (u[..., 4] - 0.5 * (u[..., 1] ** 2 + u[..., 2] ** 2 + u[..., 3] ** 2) / u[..., 0]) * 0.4
+            prim[d] = np.ascontiguousarray(p)
+        fill = rng.standard_normal(F["q"].shape)
+        fg, fo = fill.copy(), fill.copy()
+        with np.errstate(all="ignore"):
+            assert gc.L.aero_roe_3d(_p(prim[-1]), _p(prim[1]), _p(fg), _p(F["dxidx"]), _p(F["inv_j"]), _d(1.4),
+                                    *[_i(v) for v in b.box + b.box1], _i(coord)) == 0
+            oc.L.oracle_roe_3d(_p(prim[-1]), _p(prim[1]), _p(fo), _p(F["dxidx"]), _p(F["inv_j"]), _d(1.4),
+                               *ob(b.box), *ob(b.box1), _i(coord))
+        assert np.array_equal(fg, fo, equal_nan=True)
+        assert (fg != fill).any()
+    finally:
+        gc.close()
+
+
 def test_viscous_dt_implicit_transient(gpu, oracle_mod):
     oc, co, cg = prepared(bump_ns, oracle_mod, seed=3)
     gc = gpu.GpuCase(cg)
