@@ -6,7 +6,7 @@
 // iterated solver such one-ulp differences grow (the WENO weights amplify
 // them).  The FP64 kernels and the CPU oracle therefore both call the
 // functions of this header, which compute the result in double-double
-// arithmetic (relative error below 2^-94) and round it once, so they return
+// arithmetic (relative error below about 2^-94) and round it once, so they return
 // the correctly rounded value (which glibc's pow and exp also return except on
 // rare arguments within about 2^-14 ulp of a rounding boundary).  Every step
 // is an IEEE-754 operation that rounds correctly (+, -, *, fma; the callers
@@ -19,10 +19,10 @@
 //  * ln x: x = 2^k m, m in [1, 2); i = the top 8 bits of m's fraction;
 //    r = m c_i - 1 exactly (c_i ~ 1/m with 9 significant bits, one fma),
 //    |r| < 2^-8; ln x = k ln 2 - ln c_i + ln(1 + r), the last by its Taylor
-//    series to r^12 (terms from r^7 on in double, the rest in double-double);
+//    series to r^12 (terms from r^6 on in double, the rest in double-double);
 //  * exp z (z double-double): n = nearest integer to 64 z / ln 2,
 //    w = z - n ln(2)/64 (|w| < 2^-7), exp z = 2^(n div 64) 2^((n mod 64)/64)
-//    exp w, exp w by its Taylor series to w^11 (terms from w^6 on in double);
+//    exp w, exp w by its Taylor series to w^11 (terms from w^5 on in double);
 //  * pow(x, y) = exp(y ln x) for finite x > 0 and finite y with
 //    |y ln x| < 708.
 // Tables (aero_crmath_tables.h, from gen_crmath_tables.py) hold c_i, -ln c_i,
@@ -44,8 +44,9 @@
 namespace crm {
 
 // The tables, once for host code and (in CUDA translation units) once in
-// constant memory for device code; CRM_T(name) picks the copy of the side
-// being compiled.
+// device global memory for device code (not constant memory: the threads of
+// a warp index different entries, which constant memory would serialise);
+// CRM_T(name) picks the copy of the side being compiled.
 namespace host_tab {
 #define CRM_TABLE static const
 #define CRM_CONST static constexpr
@@ -55,7 +56,7 @@ namespace host_tab {
 }  // namespace host_tab
 #if defined(__CUDACC__)
 namespace dev_tab {
-#define CRM_TABLE static __constant__ const
+#define CRM_TABLE static __device__ const
 #define CRM_CONST static constexpr
 #include "aero_crmath_tables.h"
 #undef CRM_TABLE
@@ -157,6 +158,18 @@ CRM_FN dd mul_d(dd a, double b) {
   double lo = p.lo + a.lo * b;
   return fast_two_sum(p.hi, lo);
 }
+// a + b where |a.hi| >= |b.hi| (a Horner coefficient plus a much smaller
+// product): one fast two-sum instead of two two-sums.
+CRM_FN dd add_big(dd a, dd b) {
+  dd s = fast_two_sum(a.hi, b.hi);
+  double lo = s.lo + (a.lo + b.lo);
+  return fast_two_sum(s.hi, lo);
+}
+CRM_FN dd add_big_d(double a, dd b) {
+  dd s = fast_two_sum(a, b.hi);
+  double lo = s.lo + b.lo;
+  return fast_two_sum(s.hi, lo);
+}
 
 // ln x as a double-double, x finite and > 0.
 CRM_FN dd log_dd(double x) {
@@ -170,19 +183,22 @@ CRM_FN dd log_dd(double x) {
   const int i = (int)((u >> 44) & 255);
   const double m = from_bits((u & 0x000fffffffffffffULL) | 0x3ff0000000000000ULL);
   const double r = crm_fma(m, CRM_T(kLogInv)[i], -1.0);  // exact
-  // ln(1 + r) = sum_{n=1..12} (-1)^(n+1) r^n / n, Horner from n = 12
+  // ln(1 + r) = sum_{n=1..12} (-1)^(n+1) r^n / n, Horner from n = 12: the
+  // terms from r^6 on in double (their rounding is below 2^-103 of the
+  // result), the rest in double-double; every coefficient outweighs the
+  // product added to it (|r| < 2^-8), so each step is a fast two-sum
   double t = -1.0 / 12.0;
   t = t * r + 1.0 / 11.0;
   t = t * r - 1.0 / 10.0;
   t = t * r + 1.0 / 9.0;
   t = t * r - 1.0 / 8.0;
-  dd a = add(two_prod(t, r), dd{CRM_T(kInv7_hi), CRM_T(kInv7_lo)});
-  a = add(mul_d(a, r), dd{-CRM_T(kInv6_hi), -CRM_T(kInv6_lo)});
-  a = add(mul_d(a, r), dd{CRM_T(kInv5_hi), CRM_T(kInv5_lo)});
-  a = add_d(mul_d(a, r), -0.25);
-  a = add(mul_d(a, r), dd{CRM_T(kInv3_hi), CRM_T(kInv3_lo)});
-  a = add_d(mul_d(a, r), -0.5);
-  a = add_d(mul_d(a, r), 1.0);
+  t = t * r + 1.0 / 7.0;
+  t = t * r - 1.0 / 6.0;
+  dd a = add_big(dd{CRM_T(kInv5_hi), CRM_T(kInv5_lo)}, two_prod(t, r));
+  a = add_big_d(-0.25, mul_d(a, r));
+  a = add_big(dd{CRM_T(kInv3_hi), CRM_T(kInv3_lo)}, mul_d(a, r));
+  a = add_big_d(-0.5, mul_d(a, r));
+  a = add_big_d(1.0, mul_d(a, r));
   const dd lnr = mul_d(a, r);
   // k ln 2 (k * hi exact, k * mid exact as a pair)
   const double kd = (double)k;
@@ -203,19 +219,21 @@ CRM_FN double exp_dd_rounded(dd z) {
   const dd nm = two_prod(fn, CRM_T(kLn2Over64_mid));
   w = add(w, dd{-nm.hi, -nm.lo});
   w = add_d(w, -(fn * CRM_T(kLn2Over64_lo)));
-  // exp w = sum_{n=0..11} w^n / n!, Horner from n = 11
+  // exp w = sum_{n=0..11} w^n / n!, Horner from n = 11: the terms from w^5 on
+  // in double (their rounding is below 2^-97 of the result), the rest in
+  // double-double; w's low part matters only in the linear term
   double t = 1.0 / 39916800.0;
   t = t * w.hi + 1.0 / 3628800.0;
   t = t * w.hi + 1.0 / 362880.0;
   t = t * w.hi + 1.0 / 40320.0;
   t = t * w.hi + 1.0 / 5040.0;
   t = t * w.hi + 1.0 / 720.0;
-  dd a = add(mul(dd{t, 0.0}, w), dd{CRM_T(kInvFact5_hi), CRM_T(kInvFact5_lo)});
-  a = add(mul(a, w), dd{CRM_T(kInvFact4_hi), CRM_T(kInvFact4_lo)});
-  a = add(mul(a, w), dd{CRM_T(kInvFact3_hi), CRM_T(kInvFact3_lo)});
-  a = add_d(mul(a, w), 0.5);
-  a = add_d(mul(a, w), 1.0);
-  a = add_d(mul(a, w), 1.0);
+  t = t * w.hi + 1.0 / 120.0;
+  dd a = add_big(dd{CRM_T(kInvFact4_hi), CRM_T(kInvFact4_lo)}, two_prod(t, w.hi));
+  a = add_big(dd{CRM_T(kInvFact3_hi), CRM_T(kInvFact3_lo)}, mul_d(a, w.hi));
+  a = add_big_d(0.5, mul_d(a, w.hi));
+  a = add_big_d(1.0, mul_d(a, w.hi));
+  a = add_big_d(1.0, mul(a, w));
   const int j = n & 63;
   const int e = (n - j) / 64;  // exact floor division
   const dd r = mul(a, dd{CRM_T(kExp2)[j][0], CRM_T(kExp2)[j][1]});

@@ -104,6 +104,7 @@ __global__ void k_sa_b(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_b_mixed(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_recs(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_sweep(const BlockView* __restrict__ blocks);
+__global__ void k_sa_sweep_768(const BlockView* __restrict__ blocks);
 __global__ void k_lusgs_sweep_staged(const BlockView* __restrict__ blocks, int nst, unsigned* status,
                                      long spin_limit, int stall_plane);
 __global__ void k_lusgs_sweep_global(const BlockView* __restrict__ blocks, int nst, unsigned* status);

@@ -175,7 +175,14 @@ int gemm(const uint16_t* A, const uint16_t* B, float* C, int M, int N, int K, in
   int klen = ((ktiles + splits - 1) / splits) * kBK;
   splits = (K + klen - 1) / klen;
   dim3 grid(N / kBN, M / kBM, splits);
-  k_gemm_bf16<<<grid, 128, 0, st>>>(A, B, splits > 1 ? scratch : C, M, N, K, klen, status);
+  static int smem_dev = -1;  // device whose limit was raised (one device per process)
+  int dev = 0;
+  MCK(cudaGetDevice(&dev));
+  if (smem_dev != dev) {
+    MCK(cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
+    smem_dev = dev;
+  }
+  k_gemm_bf16<<<grid, 128, kGemmSmem, st>>>(A, B, splits > 1 ? scratch : C, M, N, K, klen, status);
   MCK(cudaGetLastError());
   if (splits > 1) {
     long n = (long)M * N;
@@ -189,6 +196,50 @@ int gemm(const uint16_t* A, const uint16_t* B, float* C, int M, int N, int K, in
 }  // namespace aero
 
 using namespace aero;
+
+extern "C" int aero_mlp_gemm_timed(int M, int N, int K, int reps, double* ms_per_gemm) {
+  if (M <= 0 || N <= 0 || K <= 0 || M % 128 || N % 128 || K % 64 || reps < 1 || !ms_per_gemm)
+    return set_last_error(AERO_ERR_ARG, "aero_mlp_gemm_timed: M, N multiples of 128, K a multiple of 64, reps >= 1");
+  uint16_t *dA = nullptr, *dB = nullptr;
+  float* dC = nullptr;
+  unsigned* dst = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  auto cleanup = [&] {
+    cudaFree(dA); cudaFree(dB); cudaFree(dC); cudaFree(dst);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+  };
+  size_t na = (size_t)M * K, nb = (size_t)N * K, nc = (size_t)M * N;
+  if (cudaMalloc(&dA, na * 2) || cudaMalloc(&dB, nb * 2) || cudaMalloc(&dC, nc * 4) || cudaMalloc(&dst, 4)) {
+    cleanup();
+    return set_last_error(AERO_ERR_NOMEM, "aero_mlp_gemm_timed: device allocation failed");
+  }
+  // operands: every byte 0x3c, i.e. BF16 0x3c3c (about 0.0115) everywhere; the
+  // values do not change the time
+  cudaMemset(dA, 0x3c, na * 2);
+  cudaMemset(dB, 0x3c, nb * 2);
+  cudaMemset(dst, 0, 4);
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  int rc = mlp::gemm(dA, dB, dC, M, N, K, 1, nullptr, dst, 0);  // warm-up
+  if (!rc) {
+    cudaEventRecord(e0, 0);
+    for (int r = 0; r < reps && !rc; ++r) rc = mlp::gemm(dA, dB, dC, M, N, K, 1, nullptr, dst, 0);
+    cudaEventRecord(e1, 0);
+  }
+  unsigned st = 0;
+  if (!rc) {
+    cudaError_t e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e == cudaSuccess) e = cudaMemcpy(&st, dst, 4, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) rc = set_last_error(AERO_ERR_CUDA, cudaGetErrorString(e));
+    else if (st) rc = set_last_error(AERO_ERR_DEVICE, "aero_mlp_gemm_timed: a tensor-core wait timed out");
+    *ms_per_gemm = ms / reps;
+  }
+  cleanup();
+  return rc;
+}
 
 extern "C" int aero_mlp_gemm(const uint16_t* a, const uint16_t* b, float* c, int M, int N, int K, int splits) {
   if (M <= 0 || N <= 0 || K <= 0 || M % 128 || N % 128 || K % 64 || splits < 1)

@@ -8,9 +8,10 @@
 // columns), A and B tiles of 128 x 64 BF16 staged in shared memory by the
 // threads in the canonical no-swizzle K-major layout (8-row x 16-byte core
 // matrices; LBO = 128 B between core matrices along K, SBO = 1024 B between
-// 8-row groups), four kind::f16 MMAs of K = 16 per tile issued by one thread,
-// completion through tcgen05.commit on an mbarrier, and the epilogue reading
-// tensor memory with tcgen05.ld (warp w reads lanes 32w..32w+31 = rows).
+// 8-row groups), two stages so that staging overlaps the MMAs, four kind::f16
+// MMAs of K = 16 per tile issued by one thread, completion through
+// tcgen05.commit on the stage's mbarrier, and the epilogue reading tensor
+// memory with tcgen05.ld (warp w reads lanes 32w..32w+31 = rows).
 // Every wait is bounded; the tensor memory is always released.
 #pragma once
 #include <cstdint>
@@ -39,19 +40,47 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
 }
 
 constexpr long kGemmSpin = 1L << 22;
+// Dynamic shared memory of k_gemm_bf16: two stages of A and B tiles (2 x 2 x
+// 16 KB) plus slack to align the first tile to 1024 bytes.
+constexpr int kGemmStages = 2;
+constexpr size_t kGemmSmem = (size_t)kGemmStages * (kBM + kBN) * kBK * sizeof(uint16_t) + 1024;
 
+__device__ __forceinline__ bool gemm_try_wait(uint32_t bar, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(done)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+__device__ __forceinline__ bool gemm_wait(uint32_t bar, unsigned parity, long budget) {
+  for (long spins = 0; spins < budget; ++spins)
+    if (gemm_try_wait(bar, parity)) return true;
+  return false;
+}
+
+// Two-stage pipeline: the threads stage K-tile t into shared-memory stage
+// t % 2 while the tensor cores still run the MMAs of tile t - 1 from the other
+// stage; before restaging a stage they wait for the commit of the MMAs that
+// read it two tiles earlier (tcgen05.commit arrives on that stage's mbarrier
+// once every MMA issued before it is done).
 __global__ void __launch_bounds__(128) k_gemm_bf16(const uint16_t* __restrict__ A, const uint16_t* __restrict__ B,
                                                   float* __restrict__ C, int M, int N, int K, int klen,
                                                   unsigned* status) {
-  __shared__ __align__(1024) uint16_t sA[kBM * kBK];
-  __shared__ __align__(1024) uint16_t sB[kBN * kBK];
-  __shared__ __align__(8) unsigned long long bar;
+  extern __shared__ uint8_t gemm_smem[];
+  __shared__ __align__(8) unsigned long long bar[kGemmStages];
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
   const int kbeg = blockIdx.z * klen, kend = min(K, kbeg + klen);
   float* Cs = C + (long)blockIdx.z * M * N;
+  // stage s: A tile at base + s * 32 KB, B tile 16 KB after it
+  const uint32_t raw = smem_addr(gemm_smem);
+  const uint32_t base_s = (raw + 1023u) & ~1023u;
+  uint8_t* base = gemm_smem + (base_s - raw);
+  const uint32_t stage_bytes = (kBM + kBN) * kBK * sizeof(uint16_t);
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
@@ -60,7 +89,8 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(const uint16_t* __restrict__ 
   }
   if (tid == 0) {
     abort_flag = 0;
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar)) : "memory");
+    for (int s = 0; s < kGemmStages; ++s)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar[s])) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -68,8 +98,24 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(const uint16_t* __restrict__ 
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_slot;
   const uint32_t idesc = idesc_bf16(kBM, kBN);
-  unsigned phase = 0;
-  for (int k0 = kbeg; k0 < kend; k0 += kBK) {
+  // per stage: parity of the next commit to wait for, and whether one is
+  // pending (scalars, so nothing goes to local memory)
+  unsigned ph0 = 0u, ph1 = 0u;
+  bool pend0 = false, pend1 = false;
+  int it = 0;
+  for (int k0 = kbeg; k0 < kend; k0 += kBK, ++it) {
+    const int s = it & 1;
+    uint16_t* sA = (uint16_t*)(base + s * stage_bytes);
+    uint16_t* sB = sA + kBM * kBK;
+    if (s ? pend1 : pend0) {  // the MMAs that read this stage two tiles ago
+      if (gemm_wait(smem_addr(&bar[s]), s ? ph1 : ph0, kGemmSpin)) {
+        if (s) { ph1 ^= 1u; pend1 = false; } else { ph0 ^= 1u; pend0 = false; }
+      } else {
+        abort_flag = 1;
+      }
+      __syncthreads();
+      if (abort_flag) break;
+    }
     // stage A and B: 128 rows x 8 chunks of 8 BF16 each, 8 chunks per thread
 #pragma unroll
     for (int x = 0; x < 8; ++x) {
@@ -95,41 +141,29 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(const uint16_t* __restrict__ 
             : "memory");
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                       smem_addr(&bar))
+                       smem_addr(&bar[s]))
                    : "memory");
     }
-    // wait for the MMAs (they read the staged tiles) before restaging
-    long spins = 0;
-    unsigned done = 0;
-    while (!done) {
-      asm volatile(
-          "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-          : "=r"(done)
-          : "r"(smem_addr(&bar)), "r"(phase)
-          : "memory");
-      if (!done && ++spins > kGemmSpin) {
-        abort_flag = 1;
-        break;
-      }
+    if (s) pend1 = true; else pend0 = true;
+  }
+  // every commit still pending: the last tile's covers all MMAs issued
+  if (!abort_flag) {
+    if (pend0) {
+      if (gemm_wait(smem_addr(&bar[0]), ph0, kGemmSpin)) pend0 = false; else abort_flag = 1;
     }
-    phase ^= 1u;
+    if (pend1) {
+      if (gemm_wait(smem_addr(&bar[1]), ph1, kGemmSpin)) pend1 = false; else abort_flag = 1;
+    }
     __syncthreads();
-    if (abort_flag) break;
   }
   if (abort_flag) {
-    // The MMAs committed last may still read the staged tiles and write the
-    // accumulator: wait once more, with a longer bound, for that commit
-    // (parity phase ^ 1, the one the loop gave up on) before the accumulator
-    // is freed.  If this wait runs out too, the status bit below is the only
-    // guarantee left: the dealloc then races the MMAs.
+    // MMAs committed on a stage whose wait ran out may still read the staged
+    // tiles and write the accumulator: wait once more, with a longer bound,
+    // for each pending commit before the accumulator is freed.  If such a
+    // wait runs out too, the status bit below is the only guarantee left.
     if (tid == 0) {
-      unsigned done = 0;
-      for (long spins = 0; !done && spins < 16 * kGemmSpin; ++spins)
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-            : "=r"(done)
-            : "r"(smem_addr(&bar)), "r"(phase ^ 1u)
-            : "memory");
+      if (pend0) gemm_wait(smem_addr(&bar[0]), ph0, 16 * kGemmSpin);
+      if (pend1) gemm_wait(smem_addr(&bar[1]), ph1, 16 * kGemmSpin);
     }
     __syncthreads();
   }

@@ -78,6 +78,9 @@ struct State {
   // time-step kernels (they read q, the primitives and the metrics only)
   cudaStream_t stream3 = nullptr;
   cudaEvent_t ev_join3 = nullptr;
+  // fourth stream: sa_model, forked after find_dt, beside the rest of the
+  // mean-flow iteration
+  cudaStream_t stream4 = nullptr;
   std::vector<cudaEvent_t> xfer_ev;  // host transfers: one per array of a batch, plus one
   // dynamic shared memory limits already raised on this device (cudaFuncSetAttribute
   // is per device), per sweep kernel [FP64 records, FP32 records]
@@ -235,8 +238,8 @@ struct ProfScope {
   } while (0)
 #define PROF(id, launch) PROF_ON(id, g.stream, launch)
 
-// 0 for the library's first stream, 1 and 2 for its second and third
-int stream_index(cudaStream_t s) { return s == g.stream2 ? 1 : (s == g.stream3 ? 2 : 0); }
+// 0 for the library's first stream, 1, 2 and 3 for its others
+int stream_index(cudaStream_t s) { return s == g.stream2 ? 1 : (s == g.stream3 ? 2 : (s == g.stream4 ? 3 : 0)); }
 
 void prof_collect() {
   if (gp.marks.empty()) return;
@@ -535,16 +538,27 @@ int launch_inviscid(const BlockView* views, int nblk, long maxN, long maxN1, lon
   CKL();
   return AERO_OK;
 }
-int launch_viscous(const BlockView* views, int nblk, long maxN0, const CaseConsts& cc, int store) {
-  const int vt = g.tune.visc, ew = g.tune.ew;
+// viscous_flux in two parts: part a (gradients, viscosity, vorticity, the
+// contravariant fluxes; everything find_dt and sa_model read) and part b (the
+// divergence of the fluxes into rhsv).
+int launch_viscous_a(const BlockView* views, int nblk, long maxN0, const CaseConsts& cc, int store) {
+  const int vt = g.tune.visc;
   if (g.mixed)
     PROF(P_VISC_A, (k_viscous_a_mixed<<<dim3(cdiv(maxN0, vt), nblk), vt, 0, g.stream>>>(views, cc, store)));
   else
     PROF(P_VISC_A, (k_viscous_a<<<dim3(cdiv(maxN0, vt), nblk), vt, 0, g.stream>>>(views, cc, store)));
   CKL();
+  return AERO_OK;
+}
+int launch_viscous_b(const BlockView* views, int nblk, long maxN0, const CaseConsts& cc) {
+  const int ew = g.tune.ew;
   PROF(P_VISC_B, (k_viscous_b<<<dim3(cdiv(maxN0, ew), nblk), ew, 0, g.stream>>>(views, cc)));
   CKL();
   return AERO_OK;
+}
+int launch_viscous(const BlockView* views, int nblk, long maxN0, const CaseConsts& cc, int store) {
+  int rc = launch_viscous_a(views, nblk, maxN0, cc, store);
+  return rc ? rc : launch_viscous_b(views, nblk, maxN0, cc);
 }
 int launch_find_dt(const BlockView* views, int nblk, long maxN, const CaseConsts& cc) {
   PROF(P_FIND_DT, (k_find_dt<<<dim3(cdiv(maxN, g.tune.ew), nblk), g.tune.ew, 0, g.stream>>>(views, cc, nullptr)));
@@ -708,7 +722,7 @@ int launch_sa(const BlockView* views, int nblk, long maxN, long maxN1, int pmax,
   CKL();
   size_t smem = (size_t)2 * std::max(pmax, 1) * sizeof(double);
   int threads = (int)std::min<long>(1024, std::max<long>(64, (pmax + 31) / 32 * 32));
-  PROF_ON(P_SA_SWEEP, st, (k_sa_sweep<<<nblk, threads, smem, st>>>(views)));
+  PROF_ON(P_SA_SWEEP, st, ((threads <= 768 ? k_sa_sweep_768 : k_sa_sweep)<<<nblk, threads, smem, st>>>(views)));
   CKL();
   return AERO_OK;
 }
@@ -857,28 +871,34 @@ int do_iteration(bool want_dt_minmax, bool resid_beside = false) {
   CK(cudaStreamWaitEvent(g.stream3, g.ev_fork2, 0));
   if ((rc = launch_implicit_blocks(g.d_blocks, nb, g.max_ext, g.max_b1, g.cc, g.stream3))) return rc;
   CK(cudaEventRecord(g.ev_join3, g.stream3));
-  if (viscous_on() && (rc = launch_viscous(g.d_blocks, nb, g.max_b0, g.cc, ddes_on()))) return rc;
+  // viscous part a, then find_dt (it reads the viscosity part a forms), then
+  // sa_model on a fourth stream: it reads pri_v, amu, dudx, vor, dt and the
+  // metrics and writes nut, sa_rhs and its own scratch, none of which the
+  // rest of the mean-flow iteration (viscous part b, implicit1st) reads or
+  // writes, so it runs beside all of them
+  if (viscous_on() && (rc = launch_viscous_a(g.d_blocks, nb, g.max_b0, g.cc, ddes_on()))) return rc;
   if ((rc = launch_find_dt(g.d_blocks, nb, g.max_box, g.cc))) return rc;
   if (want_dt_minmax && (rc = launch_dt_minmax(g.d_blocks, nb - 1, g.d_out + 7))) return rc;
-  CK(cudaStreamWaitEvent(g.stream, g.ev_join2, 0));
-  // sa_model reads pri_v, amu, dudx, vor, dt and the metrics and writes nut,
-  // sa_rhs and its own scratch; implicit1st reads none of those it writes and
-  // writes only q and its own scratch: the two run side by side
   const bool sa = sa_on();
   if (sa) {
     CK(cudaEventRecord(g.ev_fork, g.stream));
-    CK(cudaStreamWaitEvent(g.stream2, g.ev_fork, 0));
-    if ((rc = launch_sa(g.d_blocks, nb, g.max_box, g.max_b1, g.pmax_all, g.cc, g.stream2))) return rc;
-    CK(cudaEventRecord(g.ev_join, g.stream2));
+    CK(cudaStreamWaitEvent(g.stream4, g.ev_fork, 0));
+    if ((rc = launch_sa(g.d_blocks, nb, g.max_box, g.max_b1, g.pmax_all, g.cc, g.stream4))) return rc;
+    CK(cudaEventRecord(g.ev_join, g.stream4));
   }
+  if (viscous_on() && (rc = launch_viscous_b(g.d_blocks, nb, g.max_b0, g.cc))) return rc;
+  CK(cudaStreamWaitEvent(g.stream, g.ev_join2, 0));
   CK(cudaStreamWaitEvent(g.stream, g.ev_join3, 0));
   if ((rc = launch_implicit(g.d_blocks, nb, g.max_ext, g.max_b1, g.pmax_all, g.hmax_all, g.cc,
                             resid_beside ? g.ev_prep : nullptr, false, g.d_blocks_chain)))
     return rc;
   if (resid_beside) {
-    CK(cudaStreamWaitEvent(g.stream2, g.ev_prep, 0));
-    if ((rc = do_residual(g.d_out, g.stream2))) return rc;
-    CK(cudaEventRecord(g.ev_resid, g.stream2));
+    // the residual norm reads rhs (k_lusgs_prep), dt, inv_j and sa_rhs: with
+    // SA on the SA stream after its kernels, otherwise on the second stream
+    cudaStream_t rs = sa ? g.stream4 : g.stream2;
+    CK(cudaStreamWaitEvent(rs, g.ev_prep, 0));
+    if ((rc = do_residual(g.d_out, rs))) return rc;
+    CK(cudaEventRecord(g.ev_resid, rs));
   }
   if (sa) CK(cudaStreamWaitEvent(g.stream, g.ev_join, 0));
   if ((rc = do_physical_bc())) return rc;
@@ -978,6 +998,7 @@ int aero_init(int device) {
   CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
   CK(cudaStreamCreateWithFlags(&g.stream2, cudaStreamNonBlocking));
   CK(cudaStreamCreateWithFlags(&g.stream3, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&g.stream4, cudaStreamNonBlocking));
   CK(cudaEventCreateWithFlags(&g.ev_join3, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&g.ev_fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&g.ev_join, cudaEventDisableTiming));
@@ -1048,6 +1069,7 @@ int aero_finalize(void) {
   cudaStreamDestroy(g.stream); g.stream = nullptr;
   cudaStreamDestroy(g.stream2); g.stream2 = nullptr;
   cudaStreamDestroy(g.stream3); g.stream3 = nullptr;
+  cudaStreamDestroy(g.stream4); g.stream4 = nullptr;
   cudaEventDestroy(g.ev_join3); g.ev_join3 = nullptr;
   cudaEventDestroy(g.ev_fork); g.ev_fork = nullptr;
   cudaEventDestroy(g.ev_join); g.ev_join = nullptr;

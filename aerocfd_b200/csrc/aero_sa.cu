@@ -321,7 +321,7 @@ struct SaFwd {
   double a[3], rhs, diag, rdiag, packed;
 };
 struct SaBwd {
-  double b[3], diag, rdiag, packed, dqs;
+  double b[3], diag, rdiag, packed, dqs, nut;
   long nat;
 };
 __device__ __forceinline__ void sa_load_fwd(const BlockView& B, int h, int t, SaFwd& f) {
@@ -348,6 +348,7 @@ __device__ __forceinline__ void sa_load_bwd(const BlockView& B, int h, int t, Sa
   f.packed = r[9 * cnt];
   f.dqs = B.sa_dq[base + t];
   f.nat = B.nat[base + t];
+  f.nut = B.s(F_NUT, f.nat);  // loaded with the records, off the plane-to-plane chain
 }
 
 }  // namespace
@@ -368,7 +369,7 @@ __device__ __forceinline__ void sa_prefetch(const BlockView& B, int h) {
 // plane-to-plane path is the shared-memory neighbours, one division (div_rn_lean
 // with the reciprocal stored in the records: the correctly rounded quotient,
 // as a / b) and the barrier.
-__global__ void __launch_bounds__(1024) k_sa_sweep(const BlockView* __restrict__ blocks) {
+__device__ __forceinline__ void sa_sweep_body(const BlockView* __restrict__ blocks) {
   const BlockView& B = blocks[blockIdx.x];
   if (B.retired()) return;
   extern __shared__ double sdn[];  // two planes of pmax values
@@ -426,11 +427,16 @@ __global__ void __launch_bounds__(1024) k_sa_sweep(const BlockView* __restrict__
       }
       double v = f.dqs - div_rn_lean(tt[0] + tt[1] + tt[2], f.diag, f.rdiag);
       cur[t] = v;
-      B.s(F_NUT, f.nat) = B.s(F_NUT, f.nat) + v;
+      B.s(F_NUT, f.nat) = f.nut + v;
     }
     __syncthreads();
   }
 }
+
+// Two register budgets: up to 1024 threads (64 registers each) and up to 768
+// (80 registers, no spills), the launch picking the second when planes fit.
+__global__ void __launch_bounds__(1024) k_sa_sweep(const BlockView* __restrict__ blocks) { sa_sweep_body(blocks); }
+__global__ void __launch_bounds__(768) k_sa_sweep_768(const BlockView* __restrict__ blocks) { sa_sweep_body(blocks); }
 
 // length = dist over the full box (sub_tur_sa.f90:51-57; no DES).
 // With iflag_des = 1 (DES97) length = min(dist, cdes*spacing); with 2 (DDES)

@@ -192,23 +192,55 @@ def bump_batch(ncase: int = 64, seed: int = 0, nk: int = 5):
 
 
 def batch_case(cases, name: str = "batch"):
-    """Independent single-block cases as the blocks of one registered set (a
-    batch): returns the Case (blocks renumbered 1..n, each keeping its own
-    arrays) and {m: Config} with every block's own Control.in values, for
+    """Independent cases as the blocks of one registered set (a batch):
+    returns the Case (blocks renumbered 1..n in case order, each keeping its
+    own arrays; the interface partners of a multi-block case shifted with
+    them) and {m: Config} with every block's own Control.in values, for
     GpuCase(..., block_params=...).  The flags (solver, time advance, ...) of
     the first case apply to all."""
+    import dataclasses
     from .case import Block as _Block
     blocks, params = [], {}
-    for m, c in enumerate(cases, start=1):
-        if len(c.blocks) != 1:
-            raise ValueError(f"case {c.name} has {len(c.blocks)} blocks; a batch takes single-block cases")
-        b = c.blocks[0]
-        nb = _Block(m, b.ni, b.nj, b.nk, b.subfaces, c.cfg.buffer_length, c.cfg.dimension)
-        for k, v in b.fields.items():
+    off = 0
+    for c in cases:
+        for b in c.blocks:
+            subs = [dataclasses.replace(sf, blk_t=sf.blk_t + off if sf.blk_t > 0 else sf.blk_t)
+                    for sf in b.subfaces]
+            nb = _Block(off + b.m, b.ni, b.nj, b.nk, subs, c.cfg.buffer_length, c.cfg.dimension)
+            for k, v in b.fields.items():
+                nb.fields[k][...] = v
+            blocks.append(nb)
+            params[nb.m] = c.cfg
+        off += len(c.blocks)
+    blocks.sort(key=lambda b: b.m)
+    return Case(name, cases[0].cfg, blocks), params
+
+
+def batch_members(cases):
+    """The 0-based block range [first, last) of every case in the batch that
+    batch_case builds from `cases`."""
+    out, off = [], 0
+    for c in cases:
+        out.append((off, off + len(c.blocks)))
+        off += len(c.blocks)
+    return out
+
+
+def unbatch(batch: Case, cases, i: int) -> Case:
+    """Case i of a batch as a stand-alone case with its own numbering (arrays
+    copied from the batch's host arrays)."""
+    import dataclasses
+    from .case import Block as _Block
+    first, last = batch_members(cases)[i]
+    c = cases[i]
+    blocks = []
+    for b, src in zip(c.blocks, batch.blocks[first:last]):
+        nb = _Block(b.m, b.ni, b.nj, b.nk, [dataclasses.replace(sf) for sf in b.subfaces], c.cfg.buffer_length,
+                    c.cfg.dimension)
+        for k, v in src.fields.items():
             nb.fields[k][...] = v
         blocks.append(nb)
-        params[m] = c.cfg
-    return Case(name, cases[0].cfg, blocks), params
+    return Case(f"{c.name}_member{i}", c.cfg, blocks)
 
 
 def geometric_nodes(n: int, first: float, length: float) -> np.ndarray:

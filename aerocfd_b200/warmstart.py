@@ -184,3 +184,152 @@ def wall_force(solver, case: Case) -> np.ndarray:
         return gc.clcd_output(1.0)
     finally:
         gc.close()
+
+
+# ---------------------------------------------------------------------------
+# NACA 4-digit family with the SA model on the 4-block O-grid
+#
+# Family parameters (seeded): thickness t ~ U[0.08, 0.15], camber m ~
+# U[0, 0.04] at p ~ U[0.2, 0.6], angle of attack ~ U[-2, 6] deg, M ~
+# U[0.3, 0.7], Re ~ U[1e6, 1e7]; SA with nu_t,inf = 3 nu_inf.  Every member
+# has its own grid (the section shape changes it), so a batch of members is a
+# set of 4-block cases (grids.batch_case).  Node inputs: x, y, the distance to
+# the wall, and the six member parameters, scaled to O(1); outputs: the
+# perturbations of rho, u, v, p from the freestream and log(nu_t / nu_t,inf).
+
+NACA_IN, NACA_OUT = 9, 5
+
+
+def naca_family(n: int, seed: int, ni: int = 129, nj: int = 65, nk: int = 3, first: float = 5.0e-6,
+                cfl: float = 5.0):
+    """n members of the NACA family: [(case, params)], params a dict of the
+    member's t, m, p, aoa_deg, ma, re."""
+    from .case import IFLAG_NSSOLVER
+    rng = np.random.default_rng(seed)
+    out = []
+    for c in range(n):
+        prm = {"t": float(rng.uniform(0.08, 0.15)), "m": float(rng.uniform(0.0, 0.04)),
+               "p": float(rng.uniform(0.2, 0.6)), "aoa_deg": float(rng.uniform(-2.0, 6.0)),
+               "ma": float(rng.uniform(0.3, 0.7)), "re": float(rng.uniform(1.0e6, 1.0e7))}
+        cfg = Config(solver=IFLAG_NSSOLVER, turbulence=2, ma=prm["ma"], re=prm["re"], aoa_deg=prm["aoa_deg"],
+                     cfl=cfl, nutinf=3.0)
+        case = grids.naca_ogrid(ni=ni, nj=nj, nk=nk, t=prm["t"], m=prm["m"], p=prm["p"], first=first, cfg=cfg,
+                                name=f"naca_{c:03d}")
+        out.append((case, prm))
+    return out
+
+
+def _plane(b, name):
+    s = b.sl(b.box0)
+    return b.fields[name][s][0]
+
+
+def naca_features(case: Case, prm) -> np.ndarray:
+    """Per physical node of the first k-plane of every block (block order,
+    i fastest): x, y (chord units, y scaled by 1/2), log10 of the distance to
+    the nearest wall node, and the member parameters scaled to O(1)."""
+    wall = np.concatenate([np.stack([_plane(b, "x")[0], _plane(b, "y")[0]], -1) for b in case.blocks])
+    rows = []
+    for b in case.blocks:
+        x, y = _plane(b, "x"), _plane(b, "y")
+        pts = np.stack([x.ravel(), y.ravel()], -1)
+        d = np.full(len(pts), np.inf)
+        for c0 in range(0, len(wall), 256):
+            w = wall[c0:c0 + 256]
+            d = np.minimum(d, np.min(np.hypot(pts[:, None, 0] - w[None, :, 0], pts[:, None, 1] - w[None, :, 1]), 1))
+        n = len(pts)
+        par = [(prm["t"] - 0.115) / 0.035, prm["m"] / 0.02 - 1.0, (prm["p"] - 0.4) / 0.2,
+               (prm["aoa_deg"] - 2.0) / 4.0, (prm["ma"] - 0.5) / 0.2, (np.log10(prm["re"]) - 6.5) / 0.5]
+        f = np.stack([np.tanh(pts[:, 0] - 0.5), np.tanh(pts[:, 1]), np.log10(np.maximum(d, 1e-7)) / 3.0 + 1.0]
+                     + [np.full(n, v) for v in par], -1)
+        rows.append(f)
+    return np.concatenate(rows).astype(np.float32)
+
+
+def naca_targets(case: Case) -> np.ndarray:
+    """(rho - 1, u - cos aoa, v - sin aoa, p/p0 - 1, log(nu_t / nu_t,inf)) on
+    the first k-plane of the physical nodes of every block."""
+    cfg = case.cfg
+    a = np.deg2rad(cfg.aoa_deg)
+    p0 = 1.0 / GAMMA / cfg.ma ** 2
+    rows = []
+    for b in case.blocks:
+        pri = _plane(b, "pri_v")
+        nut = _plane(b, "nut")
+        t = np.stack([pri[..., 0] - 1.0, pri[..., 1] - np.cos(a), pri[..., 2] - np.sin(a), pri[..., 4] / p0 - 1.0,
+                      np.log(np.maximum(nut, 1e-12) / cfg.nutinf)], -1)
+        rows.append(t.reshape(-1, NACA_OUT))
+    return np.concatenate(rows).astype(np.float32)
+
+
+def naca_set_state(case: Case, pred: np.ndarray) -> None:
+    """q and nu_t of every node of every block from the predicted first-plane
+    values (copied along k; ghost nodes take the nearest physical node's value
+    before the start-up BCs and halos overwrite them)."""
+    cfg = case.cfg
+    a = np.deg2rad(cfg.aoa_deg)
+    p0 = 1.0 / GAMMA / cfg.ma ** 2
+    off = 0
+    for b in case.blocks:
+        nj, ni = b.nj, b.ni
+        pr = pred[off:off + nj * ni].reshape(nj, ni, NACA_OUT).astype(np.float64)
+        off += nj * ni
+        rho = np.maximum(1.0 + pr[..., 0], 0.05)
+        u = np.cos(a) + pr[..., 1]
+        v = np.sin(a) + pr[..., 2]
+        p = p0 * np.maximum(1.0 + pr[..., 3], 0.05)
+        nut = cfg.nutinf * np.exp(np.clip(pr[..., 4], -20.0, 20.0))
+        q = np.stack([rho, rho * u, rho * v, np.zeros_like(rho), p / (GAMMA - 1.0) + 0.5 * rho * (u * u + v * v)], -1)
+        is_, ie, js, je, ks, ke = b.box
+        ii = np.clip(np.arange(is_, ie + 1), 1, ni) - 1
+        jj = np.clip(np.arange(js, je + 1), 1, nj) - 1
+        b.fields["q"][...] = q[jj][:, ii][None, :, :, :]
+        b.fields["nut"][...] = nut[jj][:, ii][None, :, :]
+
+
+def case_residuals(batch: Case, cases, r_blocks: np.ndarray) -> np.ndarray:
+    """Each member's density residual norm from its blocks' norms (the norm
+    over the member's nodes: block sums weighted by their node counts)."""
+    out = []
+    for first, last in grids.batch_members(cases):
+        nodes = np.array([b.nodes for b in batch.blocks[first:last]], dtype=float)
+        out.append(np.sqrt(np.sum(r_blocks[first:last, 0] ** 2 * nodes) / np.sum(nodes)))
+    return np.array(out)
+
+
+def run_family_batch(solver, members, iters: int, chunk: int = 100, warm: Dict[int, np.ndarray] = None,
+                     mixed: bool = False):
+    """The members (multi-block cases) as one batch for `iters` iterations
+    from the freestream or, for the members in `warm`, from the predicted
+    field.  Returns each member's density residual after iteration 1 and after
+    every further chunk (rows), the wall time and the batch case (host arrays
+    synchronised)."""
+    cases = [m[0] for m in members]
+    batch, params = grids.batch_case(cases)
+    gc = solver.GpuCase(batch, block_params=params)
+    try:
+        gc.compute_geometry()
+        gc.init_flowfield()
+        if warm:
+            gc.sync_to_host(solver.ALL)
+            spans = grids.batch_members(cases)
+            for i, pred in warm.items():
+                first, last = spans[i]
+                naca_set_state(Case("member", cases[i].cfg, batch.blocks[first:last]), pred)
+            gc.sync_to_device(solver.mask("q", "nut"))
+        gc.start()
+        gc.set_precision(mixed)
+        gc.set_retirement(True)
+        gc.use_graphs(True)
+        t0 = time.perf_counter()
+        gc.step(1, history=False)
+        res = [case_residuals(batch, cases, gc.residual_blocks())]
+        for _ in range(iters // chunk):
+            gc.step(chunk, history=False)
+            res.append(case_residuals(batch, cases, gc.residual_blocks()))
+        wall = time.perf_counter() - t0
+        gc.sync_to_host(solver.ALL)
+        status = gc.block_status()
+        return np.array(res), wall, batch, status
+    finally:
+        gc.close()

@@ -529,6 +529,29 @@ def warm_start_gpu(solver, n_train: int = 48, n_test: int = 8, ni: int = 97, nj:
     return out
 
 
+def mlp_gemm_gpu():
+    """The warm-start network's tcgen05 BF16 GEMM (C = A B^T, FP32
+    accumulation) timed on its own: the network's layer shape (a batch of 8192
+    rows through a 256-wide layer) and a large square one, against the
+    measured cuBLAS BF16 peak (burst)."""
+    from aerocfd_b200 import _lib
+    L = _lib.load()
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak, kind = float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        peak, kind = 1590.0, "fallback"
+    out = {"peak_tflops": peak, "peak_kind": kind}
+    for name, (m, n, k, reps) in {"layer_8192x256x256": (8192, 256, 256, 200),
+                                  "square_8192": (8192, 8192, 8192, 10)}.items():
+        ms = ctypes.c_double(0.0)
+        _lib.check(L.aero_mlp_gemm_timed(ctypes.c_int(m), ctypes.c_int(n), ctypes.c_int(k), ctypes.c_int(reps),
+                                         ctypes.byref(ms)), "aero_mlp_gemm_timed")
+        tf = 2.0 * m * n * k / (ms.value / 1e3) / 1e12
+        out[name] = {"m": m, "n": n, "k": k, "ms": ms.value, "tflops": tf, "frac": tf / peak}
+    return out
+
+
 def bump_cpu_rate(seconds: float = 4.0):
     """Iterations per second of the CPU restatement on the bump case (1 block, 1 thread)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -783,6 +806,7 @@ def main():
         line["sa_plate"] = sa_plate_gpu(solver)
     if world == 1 and not args.no_warm_start:
         line["warm_start"] = warm_start_gpu(solver)
+        line["mlp_gemm"] = mlp_gemm_gpu()
     if world == 1 and not args.no_converge:
         conv = {"workload": CONV_WORKLOAD, "target_drop": CONV_TARGET,
                 "roe_weno3": {"fp64": converge_gpu(solver, False, 4), "mixed": converge_gpu(solver, True, 4)},

@@ -431,6 +431,12 @@ module aerocfd_gpu
       integer(c_int), value :: m, n, k, splits
     end function
 
+    integer(c_int) function aero_mlp_gemm_timed(m, n, k, reps, ms_per_gemm) bind(C, name="aero_mlp_gemm_timed")
+      import :: c_int, c_double
+      integer(c_int), value :: m, n, k, reps
+      real(c_double) :: ms_per_gemm
+    end function
+
     integer(c_int) function aero_mlp_param_count(count) bind(C, name="aero_mlp_param_count")
       import :: c_int, c_long_long
       integer(c_long_long) :: count

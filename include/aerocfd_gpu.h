@@ -351,6 +351,10 @@ int aero_inject_sweep_stall(int plane);
  * multiples of 128, K a multiple of 64; splits > 1 splits K over CTAs and
  * adds the partial tiles in a fixed order. */
 int aero_mlp_gemm(const unsigned short* a, const unsigned short* b, float* c, int M, int N, int K, int splits);
+/* The same GEMM on device operands of its own (constant values), reps times
+ * back to back after one warm-up; ms_per_gemm receives the mean device time
+ * of one, CUDA events on the default stream (benchmarking). */
+int aero_mlp_gemm_timed(int M, int N, int K, int reps, double* ms_per_gemm);
 /* The network: n_in inputs (<= 128), depth hidden SiLU layers of `width`
  * (a multiple of 128), n_out outputs (<= 128); BF16 weights and activations,
  * FP32 accumulation, FP32 master weights trained with Adam on the mean
