@@ -85,6 +85,7 @@ struct State {
   // dynamic shared memory limits already raised on this device (cudaFuncSetAttribute
   // is per device), per sweep kernel [FP64 records, FP32 records]
   size_t smem_staged[2] = {0, 0}, smem_bulk[2] = {0, 0};
+  bool np_cluster[2] = {false, false};  // bulk sweep: clusters of 16 CTAs allowed on this device
   long spin_limit = kPollBudgetMax;  // polls of each staged-sweep wait (aero_set_poll_budget)
   int stall_plane = -1;              // forward plane whose copies are withheld (aero_inject_sweep_stall)
   bool configured = false;
@@ -640,6 +641,10 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
       CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       g.smem_bulk[f] = smem;
     }
+    if (cl > 8 && !g.np_cluster[f]) {  // 16 CTAs: a non-portable cluster size
+      CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+      g.np_cluster[f] = true;
+    }
     cudaLaunchConfig_t lc = {};
     lc.gridDim = dim3((unsigned)(nblk * cl));
     lc.blockDim = dim3((unsigned)threads);
@@ -657,8 +662,9 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
     CK(le);
   } else if (g.tune.sweep_cl >= 2) {
     // one cluster of sweep_cl CTAs per block, one thread per row of every
-    // node of the largest plane (at most 512 per CTA; more rows loop)
-    const int cl = g.tune.sweep_cl;
+    // node of the largest plane (at most 512 per CTA; more rows loop); the
+    // exchange through L2 takes portable cluster sizes only (8 for 16)
+    const int cl = std::min(8, g.tune.sweep_cl);
     int threads = (int)std::min<long>(512, std::max<long>(64, ((5L * pmax + cl - 1) / cl + 31) / 32 * 32));
     cudaLaunchConfig_t lc = {};
     lc.gridDim = dim3((unsigned)(nblk * cl));
@@ -994,7 +1000,10 @@ const char* aero_last_error(void) { return g.err.c_str(); }
 int aero_init(int device) {
   if (g.inited) return AERO_OK;
   CK(cudaSetDevice(device));
-  for (int f = 0; f < 2; ++f) g.smem_staged[f] = g.smem_bulk[f] = 0;
+  for (int f = 0; f < 2; ++f) {
+    g.smem_staged[f] = g.smem_bulk[f] = 0;
+    g.np_cluster[f] = false;
+  }
   CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
   CK(cudaStreamCreateWithFlags(&g.stream2, cudaStreamNonBlocking));
   CK(cudaStreamCreateWithFlags(&g.stream3, cudaStreamNonBlocking));
@@ -1129,6 +1138,44 @@ int aero_use_graphs(int on) {
   return AERO_OK;
 }
 
+// Whether the bulk-exchange sweep can run as clusters of 16 CTAs: the
+// largest plane's rows fit 16 CTAs of at most 512 threads, and the device can
+// hold at least one such cluster (a non-portable cluster size).
+bool bulk_cluster16_fits() {
+  if (!g.setup || 5L * g.pmax_all > 512L * 16) return false;
+  const int cl = 16;
+  const int threads = (int)std::max<long>(64, ((5L * g.pmax_all + cl - 1) / cl + 31) / 32 * 32);
+  const size_t smem = (size_t)2 * ((size_t)cl * threads + 2) * sizeof(double);
+  for (int f = 0; f < 2; ++f) {
+    auto kern = f ? k_lusgs_sweep_bulk_f32 : k_lusgs_sweep_bulk;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) break;
+    g.np_cluster[f] = true;
+    if (smem > 48 * 1024 && smem > g.smem_bulk[f]) {
+      if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) break;
+      g.smem_bulk[f] = smem;
+    }
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3((unsigned)cl);
+    lc.blockDim = dim3((unsigned)threads);
+    lc.dynamicSmemBytes = smem;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)cl;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, kern, &lc) != cudaSuccess || n < 1) {
+      cudaGetLastError();
+      return false;
+    }
+    if (f == 1) return true;
+  }
+  cudaGetLastError();
+  return false;
+}
+
 void set_tuning_text() {
   char buf[200];
   std::snprintf(buf, sizeof buf,
@@ -1191,6 +1238,7 @@ int aero_autotune(int iters) {
   std::vector<Knob> knobs = {{&g.tune.inv_tile, {0, 32, 64, 128}}, {&g.tune.ew, {128, 256, 512}},
                              {&g.tune.visc, {64, 128, 256}}, {&g.tune.mats, {64, 128, 256}},
                              {&g.tune.nst_max, {2, 3, 4}}, {&sweep_mode, {0, 4, 8, 16, 5, 9, 17}}};
+  if (bulk_cluster16_fits()) knobs.back().cand.push_back(33);  // 16 CTAs, bulk exchange
   for (Knob& k : knobs) {
     int best = *k.v;
     double best_ms = 1e300;
@@ -1271,8 +1319,11 @@ int aero_set_sweep_exchange(int mode) {
 int aero_set_sweep_cluster(int ctas) {
   int rc = need_init();
   if (rc) return rc;
-  if (ctas != 1 && ctas != 2 && ctas != 4 && ctas != 8)
-    return fail(AERO_ERR_ARG, "sweep cluster of %d CTAs is not 1, 2, 4 or 8", ctas);
+  if (ctas != 1 && ctas != 2 && ctas != 4 && ctas != 8 && ctas != 16)
+    return fail(AERO_ERR_ARG, "sweep cluster of %d CTAs is not 1, 2, 4, 8 or 16", ctas);
+  if (ctas == 16 && !bulk_cluster16_fits())
+    return fail(AERO_ERR_ARG, "a cluster of 16 sweep CTAs does not fit this device or these blocks "
+                              "(16 CTAs take the bulk exchange only)");
   g.tune.sweep_cl = ctas == 1 ? 0 : ctas;
   graph_release();
   set_tuning_text();

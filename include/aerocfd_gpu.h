@@ -324,7 +324,9 @@ const char* aero_tuning(void);
 int aero_set_tuning(int inv_tile, int ew, int visc, int mats, int nst_max);
 /* CTAs that share each block's LU-SGS sweep: 1 (one CTA per block, the
  * records staged in shared memory when its planes fit) or a thread-block
- * cluster of 2, 4 or 8 CTAs meeting at a cluster barrier between hyperplanes.
+ * cluster of 2, 4 or 8 CTAs meeting at a cluster barrier between hyperplanes,
+ * or 16 CTAs (a non-portable cluster size, with the bulk-copy exchange only;
+ * accepted after aero_finish_setup when the device can hold such a cluster).
  * The arithmetic is the same for every choice. */
 int aero_set_sweep_cluster(int ctas);
 /* How a cluster's CTAs pass each hyperplane's values to the next plane: 0
