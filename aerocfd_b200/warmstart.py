@@ -201,7 +201,7 @@ NACA_IN, NACA_OUT = 9, 5
 
 
 def naca_family(n: int, seed: int, ni: int = 129, nj: int = 65, nk: int = 3, first: float = 5.0e-6,
-                cfl: float = 5.0):
+                cfl: float = 3.0):
     """n members of the NACA family: [(case, params)], params a dict of the
     member's t, m, p, aoa_deg, ma, re."""
     from .case import IFLAG_NSSOLVER
@@ -262,15 +262,14 @@ def naca_targets(case: Case) -> np.ndarray:
     return np.concatenate(rows).astype(np.float32)
 
 
-def naca_set_state(case: Case, pred: np.ndarray) -> None:
-    """q and nu_t of every node of every block from the predicted first-plane
-    values (copied along k; ghost nodes take the nearest physical node's value
-    before the start-up BCs and halos overwrite them)."""
-    cfg = case.cfg
+def naca_set_state(cfg: Config, blocks, pred: np.ndarray) -> None:
+    """q and nu_t of every node of the member's blocks from the predicted
+    first-plane values (copied along k; ghost nodes take the nearest physical
+    node's value before the start-up BCs and halos overwrite them)."""
     a = np.deg2rad(cfg.aoa_deg)
     p0 = 1.0 / GAMMA / cfg.ma ** 2
     off = 0
-    for b in case.blocks:
+    for b in blocks:
         nj, ni = b.nj, b.ni
         pr = pred[off:off + nj * ni].reshape(nj, ni, NACA_OUT).astype(np.float64)
         off += nj * ni
@@ -315,7 +314,7 @@ def run_family_batch(solver, members, iters: int, chunk: int = 100, warm: Dict[i
             spans = grids.batch_members(cases)
             for i, pred in warm.items():
                 first, last = spans[i]
-                naca_set_state(Case("member", cases[i].cfg, batch.blocks[first:last]), pred)
+                naca_set_state(cases[i].cfg, batch.blocks[first:last], pred)
             gc.sync_to_device(solver.mask("q", "nut"))
         gc.start()
         gc.set_precision(mixed)
@@ -329,7 +328,10 @@ def run_family_batch(solver, members, iters: int, chunk: int = 100, warm: Dict[i
             res.append(case_residuals(batch, cases, gc.residual_blocks()))
         wall = time.perf_counter() - t0
         gc.sync_to_host(solver.ALL)
-        status = gc.block_status()
+        # each member's status: the OR of its blocks' words (a retired member
+        # is frozen where it failed)
+        bst = gc.block_status()
+        status = np.array([np.bitwise_or.reduce(bst[a:e]) for a, e in grids.batch_members(cases)])
         return np.array(res), wall, batch, status
     finally:
         gc.close()

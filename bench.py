@@ -529,6 +529,71 @@ def warm_start_gpu(solver, n_train: int = 48, n_test: int = 8, ni: int = 97, nj:
     return out
 
 
+def warm_start_naca_gpu(solver, n_train: int = 48, n_test: int = 12, its_train: int = 3000, its_test: int = 3000,
+                        chunk: int = 100):
+    """Learned warm start on the NACA 4-digit family with SA (config 5's
+    parameter ranges: t 8-15 %, camber 0-4 % at 0.2-0.6, AoA -2..6 deg,
+    M 0.3-0.7, Re 1e6-1e7) on the 4-block O-grid 4 x 129 x 65 x 3 (wall
+    spacing 5e-6, CFL 3): n_train members run its_train iterations as one
+    batch give the training fields (members that fail, retired by their
+    block status, are left out), an 8 x 256 BF16 MLP is trained on them
+    with the tcgen05 kernels, and n_test held-out members run its_test
+    iterations from the freestream (cold, FP64), from the prediction (warm,
+    FP64) and from the prediction in mixed precision, each as one batch.
+    Reported per member: the iteration at which the density residual first
+    falls to each level (a drop relative to the cold run's iteration-1
+    residual), the wall time for the whole batch to get there, and cl, cd of
+    the cold and warm runs after its_test iterations."""
+    from aerocfd_b200 import grids, warmstart as W
+    fam = W.naca_family(n_train + n_test, seed=11)
+    train, test = fam[:n_train], fam[n_train:]
+    t0 = time.perf_counter()
+    _, gen_s, batch, st_train = W.run_family_batch(solver, train, its_train, chunk=chunk)
+    cases_tr = [c for c, _ in train]
+    ok = [i for i in range(n_train) if st_train[i] == 0]  # a member that failed gives no training data
+    X = np.concatenate([W.naca_features(*train[i]) for i in ok])
+    T = np.concatenate([W.naca_targets(grids.unbatch(batch, cases_tr, i)) for i in ok])
+    del batch
+    net = W.Network(n_in=W.NACA_IN, n_out=W.NACA_OUT, width=256, depth=8, batch=8192, seed=3)
+    try:
+        t1 = time.perf_counter()
+        loss = net.train(X, T, steps=4000, lr=1e-3)
+        train_s = time.perf_counter() - t1
+        warm = {i: net.predict(W.naca_features(c, p)) for i, (c, p) in enumerate(test)}
+    finally:
+        net.close()
+    runs = {"cold": W.run_family_batch(solver, test, its_test, chunk=chunk),
+            "warm": W.run_family_batch(solver, test, its_test, chunk=chunk, warm=warm),
+            "warm_mixed": W.run_family_batch(solver, test, its_test, chunk=chunk, warm=warm, mixed=True)}
+    hc = runs["cold"][0]
+    out = {"family": "naca4_sa_ogrid_4x129x65x3_cfl3", "train_members": n_train, "train_members_used": len(ok),
+           "test_members": n_test,
+           "iterations_train": its_train, "iterations_test": its_test,
+           "network": "8 x 256 SiLU MLP, BF16 weights/activations, FP32 accumulation, tcgen05 GEMMs",
+           "samples": int(len(X)), "train_steps": 4000, "train_s": train_s, "data_generation_s": gen_s,
+           "loss_first_last": [float(loss[:10].mean()), float(loss[-10:].mean())],
+           "iteration1_residual_ratio_warm_over_cold": float(np.mean(runs["warm"][0][0] / hc[0])),
+           "block_status_nonzero": {k: int((v[3] != 0).sum()) for k, v in runs.items()}}
+    levels = {}
+    for drop in (1e-1, 1e-2, 1e-3):
+        lv = hc[0] * drop
+        row = {}
+        for k, (h, wall, _, _) in runs.items():
+            it = W.first_below(h, lv, chunk)
+            row[k] = {"iterations": [int(v) if v > 0 else None for v in it], "members_reached": int((it > 0).sum()),
+                      "wall_s_all_members": float(wall * it.max() / its_test) if (it > 0).all() else None}
+        levels[f"{drop:.0e}"] = row
+    out["levels"] = levels
+    forces = []
+    for i in range(n_test):
+        fc = W.wall_force(solver, grids.unbatch(runs["cold"][2], [c for c, _ in test], i))
+        fw = W.wall_force(solver, grids.unbatch(runs["warm"][2], [c for c, _ in test], i))
+        forces.append({"cl_cold": float(fc[6]), "cl_warm": float(fw[6]), "cd_cold": float(fc[7]), "cd_warm": float(fw[7])})
+    out["forces_after_test_iterations"] = forces
+    out["total_s"] = time.perf_counter() - t0
+    return out
+
+
 def mlp_gemm_gpu():
     """The warm-start network's tcgen05 BF16 GEMM (C = A B^T, FP32
     accumulation) timed on its own: the network's layer shape (a batch of 8192
@@ -807,6 +872,7 @@ def main():
     if world == 1 and not args.no_warm_start:
         line["warm_start"] = warm_start_gpu(solver)
         line["mlp_gemm"] = mlp_gemm_gpu()
+        line["warm_start_naca_sa"] = warm_start_naca_gpu(solver)
     if world == 1 and not args.no_converge:
         conv = {"workload": CONV_WORKLOAD, "target_drop": CONV_TARGET,
                 "roe_weno3": {"fp64": converge_gpu(solver, False, 4), "mixed": converge_gpu(solver, True, 4)},
