@@ -191,17 +191,21 @@ __device__ __forceinline__ double weno_corr(double um, double u0, double up) {
 __device__ __forceinline__ void roe_face_mixed(const BlockView& B, int coord, long n, long ns,
                                                const double ulc[5], const double urc[5], double gamma,
                                                double flux[5]) {
-  double dl = ulc[0], ul = ulc[1] / ulc[0], vl = ulc[2] / ulc[0], wl = ulc[3] / ulc[0];
-  double pl = (ulc[4] - 0.5 * (p2(ulc[1]) + p2(ulc[2]) + p2(ulc[3])) / ulc[0]) * (gamma - 1.0);
-  double dr = urc[0], ur = urc[1] / urc[0], vr = urc[2] / urc[0], wr = urc[3] / urc[0];
-  double pr = (urc[4] - 0.5 * (p2(urc[1]) + p2(urc[2]) + p2(urc[3])) / urc[0]) * (gamma - 1.0);
+  // primitives with one FP64 reciprocal of the density per side (the FP64
+  // path divides each component, as the reference)
+  const double rl = 1.0 / ulc[0], rr = 1.0 / urc[0];
+  double dl = ulc[0], ul = ulc[1] * rl, vl = ulc[2] * rl, wl = ulc[3] * rl;
+  double pl = (ulc[4] - 0.5 * (p2(ulc[1]) + p2(ulc[2]) + p2(ulc[3])) * rl) * (gamma - 1.0);
+  double dr = urc[0], ur = urc[1] * rr, vr = urc[2] * rr, wr = urc[3] * rr;
+  double pr = (urc[4] - 0.5 * (p2(urc[1]) + p2(urc[2]) + p2(urc[3])) * rr) * (gamma - 1.0);
   int c1 = coord * 3 - 2;
   double ja = B.s(F_INVJ, n), jb = B.s(F_INVJ, ns);
   double dxidx1 = 0.5 * (B.v(F_DXIDX, c1, n) * ja + B.v(F_DXIDX, c1, ns) * jb);
   double dxidy1 = 0.5 * (B.v(F_DXIDX, c1 + 1, n) * ja + B.v(F_DXIDX, c1 + 1, ns) * jb);
   double dxidz1 = 0.5 * (B.v(F_DXIDX, c1 + 2, n) * ja + B.v(F_DXIDX, c1 + 2, ns) * jb);
-  double hl = gamma * pl / ((gamma - 1.0) * dl) + 0.5 * (p2(ul) + p2(vl) + p2(wl));
-  double hr = gamma * pr / ((gamma - 1.0) * dr) + 0.5 * (p2(ur) + p2(vr) + p2(wr));
+  const double gg = gamma / (gamma - 1.0);
+  double hl = gg * pl * rl + 0.5 * (p2(ul) + p2(vl) + p2(wl));
+  double hr = gg * pr * rr + 0.5 * (p2(ur) + p2(vr) + p2(wr));
   double uul = ul * dxidx1 + vl * dxidy1 + wl * dxidz1;
   double uur = ur * dxidx1 + vr * dxidy1 + wr * dxidz1;
   // central part (FP64)
