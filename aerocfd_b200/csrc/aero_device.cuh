@@ -65,6 +65,11 @@ struct BlockView {
   // node (nodes of plane h = (i-is1)+(j-js1)+(k-ks1) are contiguous):
   int nplanes, pmax;     // number of hyperplanes, largest plane
   long* poff;            // nplanes+1 plane offsets
+  // nplanes x (nz1+2) k-segment starts: entry h*(nz1+2) + c+1 counts the
+  // nodes of plane h with k-offset below c (c = -1 .. nz1), i.e. where the
+  // nodes of k-offset c begin inside the plane (a plane lists its nodes by
+  // k-offset, then j); the slab sweeps address their k-slabs by it
+  int* seg;
   double* rec_f;         // kRec per node: forward blocks from the i-1, j-1, k-1 neighbours
   double* rec_b;         // kRec per node: backward blocks from the i+1, j+1, k+1 neighbours
   double* sca;           // kSca per node: rhs(5), diag, inv_j, 1/diag, 1/inv_j, unused
@@ -221,5 +226,119 @@ enum {
 enum StatusBits : unsigned {
   ST_NEG_DENSITY = 1u, ST_NONFINITE_RESIDUAL = 2u, ST_NEG_PRESSURE = 4u, ST_TIMEOUT = 8u,
 };
+
+#ifdef __CUDACC__
+// ------------------------------------------- thread-block cluster primitives
+// (the slab sweeps: a CTA's progress counters and ring slots are written by
+// its neighbours in the cluster)
+namespace slab {
+__device__ __forceinline__ unsigned rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ unsigned size() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ unsigned local(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+// address of the same shared-memory word in CTA `r` of the cluster
+__device__ __forceinline__ unsigned map(unsigned addr, unsigned r) {
+  unsigned out;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(out) : "r"(addr), "r"(r));
+  return out;
+}
+// full cluster barrier (release / acquire): orders every shared::cluster
+// store issued before it
+__device__ __forceinline__ void sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// acquire load of a counter in this CTA's shared memory that other CTAs of
+// the cluster write
+__device__ __forceinline__ int load_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.cluster.shared::cta.u32 %0, [%1];" : "=r"(v) : "r"(local(p)) : "memory");
+  return v;
+}
+// release store of a counter into another CTA's shared memory: every store
+// this CTA's threads issued before a CTA barrier that precedes it is visible
+// to a thread that reads the counter with load_acquire
+__device__ __forceinline__ void store_release(unsigned remote, int v) {
+  asm volatile("st.release.cluster.shared::cluster.u32 [%0], %1;" ::"r"(remote), "r"(v) : "memory");
+}
+__device__ __forceinline__ void store_f64(unsigned remote, double v) {
+  asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(remote), "d"(v) : "memory");
+}
+// L2 prefetch of [p, p + bytes) widened to 16-byte boundaries; the caller
+// keeps the widened range inside one allocation
+__device__ __forceinline__ void prefetch_span(const void* p, long bytes) {
+  if (bytes <= 0) return;
+  const unsigned long long a = (unsigned long long)p & ~15ull;
+  const unsigned long long e = ((unsigned long long)p + (unsigned long long)bytes + 15ull) & ~15ull;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((unsigned)(e - a)) : "memory");
+}
+// Bounded wait until a counter of this CTA reaches v; false when it did not
+// within `limit` polls.
+__device__ __forceinline__ bool wait_for(const int* counter, int v, long limit) {
+  long spins = 0;
+  while (load_acquire(counter) < v)
+    if (++spins > limit) return false;
+  return true;
+}
+
+// The k-slab of one CTA of a slab sweep and its links to the neighbouring
+// slabs.  The block's k-offsets 0..nz1-1 split into ce = min(cluster size,
+// nz1) slabs, slab r = [r*nz1/ce, (r+1)*nz1/ce); CTAs ce.. of the cluster
+// idle.  Steps gs = 0..H-1 are the forward pass over planes h = gs, steps
+// H..2H-1 the backward pass over h = 2H-1-gs.  A node's k-1 (forward) or k+1
+// (backward) neighbour may lie in the slab below or above: the "upstream"
+// slab of the pass (below forward, above backward) delivers those values,
+// and this CTA delivers its own edge values to the "downstream" slab.
+struct Geom {
+  const int* segt;
+  int SW, nz1, nab, H, ce, me, c0, c1;
+  __device__ Geom(const BlockView& B, int ncta, int rank) {
+    segt = B.seg;
+    nz1 = B.b1.nz();
+    SW = nz1 + 2;
+    nab = B.b1.nx() + B.b1.ny() - 2;
+    H = B.nplanes;
+    ce = min(ncta, nz1);
+    me = rank;
+    c0 = c0_of(me);
+    c1 = c0_of(me + 1);
+  }
+  __device__ bool active() const { return me < ce; }
+  __device__ int c0_of(int r) const { return r * nz1 / ce; }
+  // nodes of plane h with k-offset below c (c = -1 .. nz1)
+  __device__ int seg(int h, int c) const { return segt[h * SW + c + 1]; }
+  // first plane-local index held in a ring slot of slab r for plane h: the
+  // k-segment below the slab (or the slab itself for r = 0)
+  __device__ int wl(int h, int r) const { return seg(h, max(c0_of(r) - 1, 0)); }
+  __device__ int plane(int gs) const { return gs < H ? gs : 2 * H - 1 - gs; }
+  __device__ bool has_lo() const { return me > 0 && me < ce; }
+  __device__ bool has_hi() const { return me + 1 < ce; }
+  // plane h holds nodes of k-offset c
+  __device__ bool holds(int h, int c) const { return h - c >= 0 && h - c <= nab; }
+  // step gs reads values of the upstream slab (the k-1 / k+1 neighbours of
+  // this slab's first / last k-segment)
+  __device__ bool need_up(int gs) const {
+    const int h = plane(gs);
+    return gs < H ? (has_lo() && h >= 1 && holds(h, c0)) : (has_hi() && h + 1 < H && holds(h, c1 - 1));
+  }
+  // step gs delivers values to the downstream slab; the same condition as
+  // the downstream CTA's need_up at step gs + 1
+  __device__ bool need_dn(int gs) const {
+    const int h = plane(gs);
+    return gs < H ? (has_hi() && h + 1 < H && holds(h, c1 - 1)) : (has_lo() && h >= 1 && holds(h, c0));
+  }
+  // this slab's edge k-segment the downstream slab reads at step gs
+  __device__ int c_dn(int gs) const { return gs < H ? c1 - 1 : c0; }
+  // the downstream CTA's rank at step gs
+  __device__ int rank_dn(int gs) const { return gs < H ? me + 1 : me - 1; }
+};
+}  // namespace slab
+#endif
 
 }  // namespace aero

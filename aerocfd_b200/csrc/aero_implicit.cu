@@ -175,6 +175,7 @@ template <>
 struct RecFmt<double> {
   static constexpr int kWords = kRec;
   __device__ static double packed(const double* chunk, int cnt, int t) { return chunk[75 * cnt + t]; }
+  __device__ static const double* packed_ptr(const double* chunk, int cnt) { return chunk + 75 * cnt; }
   __device__ static void set_packed(double* chunk, int cnt, long t, double v) { chunk[75 * cnt + t] = v; }
 };
 template <>
@@ -182,6 +183,9 @@ struct RecFmt<float> {
   static constexpr int kWords = 80;
   __device__ static double packed(const float* chunk, int cnt, int t) {
     return reinterpret_cast<const double*>(chunk + 76 * cnt)[t];
+  }
+  __device__ static const double* packed_ptr(const float* chunk, int cnt) {
+    return reinterpret_cast<const double*>(chunk + 76 * cnt);
   }
   __device__ static void set_packed(float* chunk, int cnt, long t, double v) {
     reinterpret_cast<double*>(chunk + 76 * cnt)[t] = v;
@@ -1198,6 +1202,214 @@ __global__ void __launch_bounds__(512, 1) k_lusgs_sweep_bulk(const BlockView* __
 __global__ void __launch_bounds__(512, 1) k_lusgs_sweep_bulk_f32(const BlockView* __restrict__ blocks,
                                                                  unsigned* status) {
   lusgs_bulk_body<float>(blocks, status);
+}
+
+// ------------------------------------------------------------ slab sweeps
+namespace {
+
+// The records of row `row` of plane-local node `node` (cnt nodes in the plane).
+template <typename R>
+__device__ __forceinline__ void load_node_row(const R* rec, const double* sca, int cnt, int row, int node,
+                                              RowRecs& r) {
+  r.row = row;
+  r.node = node;
+  const R* rn = rec + node;
+  r.packed = RecFmt<R>::packed(rec, cnt, node);
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+#pragma unroll
+    for (int c = 0; c < 5; ++c) r.m[5 * d + c] = (double)rn[(25 * d + 5 * row + c) * cnt];
+  const double* sn = sca + node;
+  r.rhs = sn[row * cnt];
+  r.diag = sn[5 * cnt];
+  r.invj = sn[6 * cnt];
+  r.rdiag = sn[7 * cnt];
+  r.rinvj = sn[8 * cnt];
+  r.bok = !nbr_slow_div(r.packed);
+}
+// lusgs_rows' arithmetic for one row from preloaded records, the previous
+// plane's values read from a ring slot (row c of plane-local node w at
+// prev[c*S + w - wl]).
+template <bool FWD>
+__device__ __forceinline__ double row_from_slot(const RowRecs& r, const double* prev, int wl, int S,
+                                                const double* dsv, int cnt) {
+  double acc[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    int w = nbr_local(r.packed, d);
+    double sd = 0.0;
+    if (w >= 0) {
+      const double* x = prev + (w - wl);
+      sd = r.m[5 * d] * x[0];
+      sd = sd + r.m[5 * d + 1] * x[S];
+      sd = sd + r.m[5 * d + 2] * x[2 * S];
+      sd = sd + r.m[5 * d + 3] * x[3 * S];
+      sd = sd + r.m[5 * d + 4] * x[4 * S];
+    }
+    acc[d] = sd;
+  }
+  if (FWD) return div2_rn(r.rhs + (acc[0] + acc[1] + acc[2]), r.diag, r.rdiag, r.invj, r.rinvj, r.bok);
+  return __ldcg(dsv + r.row * cnt + r.node) -
+         div2_rn(acc[0] + acc[1] + acc[2], r.invj, r.rinvj, r.diag, r.rdiag, r.bok);
+}
+
+}  // namespace
+
+// The forward and backward sweeps of one block pipelined over a cluster of
+// CTAs by k-slabs (grid x = blocks x cluster size, cluster dims (CL,1,1)).
+// CTA r owns the nodes of k-offsets [r*nz1/ce, (r+1)*nz1/ce) (slab::Geom); a
+// plane lists its nodes by k-offset, so a slab's part of every plane is one
+// contiguous range of plane-local indices, which the CTA computes one row of a
+// node per thread, in the hyperplane order of the serial sweep.  Within a
+// slab every neighbour a node needs from the previous plane is the CTA's own,
+// except the k-1 (forward) / k+1 (backward) neighbours of the slab's first /
+// last k-segment, which the CTA below / above computes: that CTA stores them
+// straight into this CTA's ring (st.shared::cluster) and then publishes its
+// progress (the last step it completed) with a release store into this CTA's
+// counter.  So a CTA waits only for the step before its own on one neighbour,
+// and the CTAs run as a pipeline, each a few planes behind its upstream
+// neighbour: the pass takes about H plane steps plus one neighbour latency per
+// slab, instead of a cluster-wide exchange on every plane.  The ring holds D
+// planes; a CTA writes into a neighbour's slot only after that neighbour has
+// finished the step that read the slot's previous plane (its counter, which
+// it publishes to both neighbours), so the ring never overflows.  No CTA can
+// wait forever on another: each wait is for a CTA at an earlier step, and
+// every wait is bounded.  A wait that runs out makes the CTA stop (its
+// neighbours then run out too), and the final cluster barrier keeps every CTA
+// resident until no neighbour can still store into it; no asynchronous copy
+// is used.  The arithmetic per row is lusgs_rows', so the result is the same
+// to the bit.
+template <typename R>
+__device__ __forceinline__ void lusgs_slab_body(const BlockView* __restrict__ blocks, unsigned* status, int S,
+                                                int D) {
+  constexpr int W = RecFmt<R>::kWords;
+  extern __shared__ __align__(16) double sring[];  // D slots x 5 rows x S
+  __shared__ int s_prog[2];  // last step completed by the CTA below / above
+  __shared__ int s_fail;
+  const int ncta = (int)slab::size();
+  const BlockView& B = blocks[blockIdx.x / ncta];
+  if (B.retired()) return;
+  const slab::Geom G(B, ncta, (int)slab::rank());
+  const long* poff = B.poff;
+  const int H = G.H, tid = (int)threadIdx.x;
+  if (tid == 0) {
+    s_prog[0] = -1;
+    s_prog[1] = -1;
+    s_fail = 0;
+  }
+  slab::sync();  // every CTA's counters are set before a neighbour writes them
+  if (G.active()) {
+    const unsigned ring_l = slab::local(sring);
+    // this CTA's progress lives in the CTA below as its "above" counter and in
+    // the CTA above as its "below" counter
+    const unsigned at_lo = G.has_lo() ? slab::map(slab::local(&s_prog[1]), G.me - 1) : 0u;
+    const unsigned at_hi = G.has_hi() ? slab::map(slab::local(&s_prog[0]), G.me + 1) : 0u;
+    const unsigned ring_lo = G.has_lo() ? slab::map(ring_l, G.me - 1) : 0u;
+    const unsigned ring_hi = G.has_hi() ? slab::map(ring_l, G.me + 1) : 0u;
+    RowRecs pre;  // the records of this thread's first row of the next step
+    auto preload = [&](int gs) {
+      if (gs >= 2 * H) return;
+      const bool fwd = gs < H;
+      const int h = G.plane(gs);
+      const long base = poff[h];
+      const int cnt = (int)(poff[h + 1] - base);
+      const int t0 = G.seg(h, G.c0), n = G.seg(h, G.c1) - t0;
+      if (tid < 5 * n) {
+        const int row = row_of(tid, n);
+        load_node_row(recs<R>(B, fwd) + W * base, B.sca + kSca * base, cnt, row, t0 + tid - row * n, pre);
+      }
+    };
+    // L2 prefetch, by warp 1, of the slab's part of step gs's chunks: every
+    // record entry, the packed neighbours, the scalars and (backward) dq*,
+    // each a run of n values inside its plane's chunk (chunks start and end
+    // on 16-byte boundaries, so the widened runs stay inside them)
+    auto prefetch = [&](int gs) {
+      if (gs >= 2 * H || (tid >> 5) != 1) return;
+      const bool fwd = gs < H;
+      const int h = G.plane(gs);
+      const long base = poff[h];
+      const int cnt = (int)(poff[h + 1] - base);
+      const int t0 = G.seg(h, G.c0), n = G.seg(h, G.c1) - t0;
+      if (n <= 0) return;
+      const R* rec = recs<R>(B, fwd) + W * base;
+      const int nrun = 76 + kSca + (fwd ? 0 : 5);
+      for (int x = (tid & 31); x < nrun; x += 32) {
+        if (x < 75)
+          slab::prefetch_span(rec + (long)x * cnt + t0, (long)n * (long)sizeof(R));
+        else if (x == 75)
+          slab::prefetch_span(RecFmt<R>::packed_ptr(rec, cnt) + t0, 8L * n);
+        else if (x < 76 + kSca)
+          slab::prefetch_span(B.sca + kSca * base + (long)(x - 76) * cnt + t0, 8L * n);
+        else
+          slab::prefetch_span(B.dqs + 8 * base + (long)(x - 76 - kSca) * cnt + t0, 8L * n);
+      }
+    };
+    constexpr int PF = 3;  // prefetch distance in steps
+    for (int gs = 0; gs < PF; ++gs) prefetch(gs);
+    preload(0);
+    for (int gs = 0; gs < 2 * H; ++gs) {
+      const bool fwd = gs < H;
+      const int h = G.plane(gs);
+      const long base = poff[h];
+      const int cnt = (int)(poff[h + 1] - base);
+      const int t0 = G.seg(h, G.c0), n = G.seg(h, G.c1) - t0;
+      const bool need_dn = G.need_dn(gs);
+      bool fail = false;
+      // the upstream slab's values of the previous step
+      if (G.need_up(gs)) fail = !slab::wait_for(&s_prog[fwd ? 0 : 1], gs - 1, kSpinLimit);
+      // room in the downstream slab's ring: it has finished step gs-D+1,
+      // the last to read the slot's previous plane
+      if (!fail && need_dn) fail = !slab::wait_for(&s_prog[fwd ? 1 : 0], gs - D + 1, kSpinLimit);
+      if (!fail) {
+        double* cur = sring + (gs % D) * 5 * S;
+        const double* prev = sring + ((gs + D - 1) % D) * 5 * S;
+        const int wlc = G.wl(h, G.me);
+        const int wlp = gs > 0 ? G.wl(G.plane(gs - 1), G.me) : 0;
+        // this slab's edge nodes the downstream slab reads, and where they go
+        const int e0 = need_dn ? G.seg(h, G.c_dn(gs)) : 0, e1 = need_dn ? G.seg(h, G.c_dn(gs) + 1) : 0;
+        const int wld = need_dn ? G.wl(h, G.rank_dn(gs)) : 0;
+        const unsigned slot_dn = (fwd ? ring_hi : ring_lo) + (unsigned)((gs % D) * 5 * S * 8);
+        const double* dsv = B.dqs + 8 * base;
+        auto item = [&](const RowRecs& r) {
+          const double v = fwd ? row_from_slot<true>(r, prev, wlp, S, dsv, cnt)
+                               : row_from_slot<false>(r, prev, wlp, S, dsv, cnt);
+          cur[r.row * S + (r.node - wlc)] = v;
+          if (r.node >= e0 && r.node < e1) slab::store_f64(slot_dn + (unsigned)((r.row * S + r.node - wld) * 8), v);
+          if (fwd)
+            B.dqs[8 * base + r.row * cnt + r.node] = v;
+          else
+            B.dq[5 * (base + r.node) + r.row] = v;
+        };
+        if (tid < 5 * n) item(pre);  // the launch gives every row of a slab's plane a thread
+      }
+      // every thread's values of this step are stored (locally and in the
+      // downstream ring) before thread 0 publishes the step
+      if (__syncthreads_or(fail ? 1 : 0)) {
+        if (tid == 0) s_fail = 1;
+        break;
+      }
+      if (tid == 0) {
+        if (G.has_lo()) slab::store_release(at_lo, gs);
+        if (G.has_hi()) slab::store_release(at_hi, gs);
+      }
+      prefetch(gs + PF);
+      preload(gs + 1);
+    }
+  }
+  __syncthreads();
+  slab::sync();  // no CTA leaves while a neighbour may still store into it
+  if (tid == 0 && s_fail) {
+    if (status) atomicOr(status, (unsigned)ST_TIMEOUT);
+    B.raise(ST_TIMEOUT);
+  }
+}
+__global__ void __launch_bounds__(512, 1) k_lusgs_sweep_slab(const BlockView* __restrict__ blocks, unsigned* status,
+                                                             int S, int D) {
+  lusgs_slab_body<double>(blocks, status, S, D);
+}
+__global__ void __launch_bounds__(512, 1) k_lusgs_sweep_slab_f32(const BlockView* __restrict__ blocks,
+                                                                 unsigned* status, int S, int D) {
+  lusgs_slab_body<float>(blocks, status, S, D);
 }
 
 // q = q + dq on every updated node (sub_timeadvancement_1stimplicit.f90:568-574).

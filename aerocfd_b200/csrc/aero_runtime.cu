@@ -59,6 +59,78 @@ std::vector<long> plane_offsets(const Box& b1, int& pmax) {
   return off;
 }
 
+// k-segment starts of every plane of an nx1 x ny1 x nz1 updated box
+// (BlockView::seg): entry h*(nz1+2) + c+1 = nodes of plane h with k-offset
+// below c, for c = -1 .. nz1.
+std::vector<int> plane_segments(const Box& b1) {
+  const int nx1 = b1.nx(), ny1 = b1.ny(), nz1 = b1.nz();
+  const int H = nx1 + ny1 + nz1 - 2, SW = nz1 + 2;
+  std::vector<int> seg((size_t)std::max(H, 0) * SW, 0);
+  for (int h = 0; h < H; ++h) {
+    int n = 0;
+    for (int c = 0; c < nz1; ++c) {
+      seg[(size_t)h * SW + c + 1] = n;
+      const int r = h - c;
+      const int bmin = std::max(0, r - (nx1 - 1)), bmax = std::min(ny1 - 1, r);
+      if (r >= 0 && bmax >= bmin) n += bmax - bmin + 1;
+    }
+    seg[(size_t)h * SW + nz1 + 1] = n;
+  }
+  return seg;
+}
+
+// Shape of the slab sweeps of one block over clusters of `ncta` CTAs: the
+// block's k-offsets 0..nz1-1 split into ce = min(ncta, nz1) slabs, slab r
+// holding [r*nz1/ce, (r+1)*nz1/ce).  width: the most nodes of one plane
+// between the start of the k-segment below a slab and the end of the one
+// above it (a CTA's ring slot); own: the most nodes of one plane inside a
+// slab.
+void slab_shape(const Box& b1, int ncta, int& width, int& own) {
+  const int nz1 = b1.nz(), H = b1.nx() + b1.ny() + nz1 - 2, SW = nz1 + 2;
+  const std::vector<int> seg = plane_segments(b1);
+  const int ce = std::max(1, std::min(ncta, nz1));
+  width = own = 0;
+  for (int r = 0; r < ce; ++r) {
+    const int c0 = r * nz1 / ce, c1 = (r + 1) * nz1 / ce;
+    for (int h = 0; h < H; ++h) {
+      const int* s = seg.data() + (size_t)h * SW + 1;  // s[c] for c = -1 .. nz1
+      width = std::max(width, s[std::min(c1 + 1, nz1)] - s[std::max(c0 - 1, 0)]);
+      own = std::max(own, s[c1] - s[c0]);
+    }
+  }
+}
+
+// Launch shape of a slab sweep (k_lusgs_sweep_slab: `rows` = 5 rows per node;
+// k_sa_sweep_slab: 1) over clusters of ncta CTAs for a set of blocks: ring
+// slot width S, threads T (one per row of a slab's plane) and ring depth D
+// (up to 8 planes in 200 KB of shared memory).  ok is false when a slab's
+// plane needs more than 512 threads or fewer than two planes fit.
+struct SlabFit {
+  bool ok = false;
+  int S = 0, T = 0, D = 0;
+};
+SlabFit slab_fit(const BlockView* hv, int nblk, int ncta, int rows) {
+  SlabFit f;
+  int width = 0, own = 0;
+  for (int m = 0; m < nblk; ++m) {
+    int w = 0, o = 0;
+    slab_shape(hv[m].b1, ncta, w, o);
+    width = std::max(width, w);
+    own = std::max(own, o);
+  }
+  if (rows * own > 512 || width <= 0) return f;
+  f.S = width;
+  f.T = std::max(64, (rows * own + 31) / 32 * 32);
+  const size_t slot = (size_t)rows * f.S * sizeof(double);
+  f.D = (int)std::min<size_t>(8, (size_t)(200 * 1024) / slot);
+  f.ok = f.D >= 2;
+  return f;
+}
+
+// slab_fit of the registered blocks (hv null; cached per setup) or of the
+// nblk host views hv.
+SlabFit slab_fit_for(const BlockView* hv, int nblk, int ncta, int rows);
+
 // Largest (and default) number of polls of each wait of the staged LU-SGS
 // sweep, the kernel's own bound.
 constexpr long kPollBudgetMax = 1L << 20;
@@ -86,6 +158,12 @@ struct State {
   // is per device), per sweep kernel [FP64 records, FP32 records]
   size_t smem_staged[2] = {0, 0}, smem_bulk[2] = {0, 0};
   bool np_cluster[2] = {false, false};  // bulk sweep: clusters of 16 CTAs allowed on this device
+  // slab sweeps (mean flow FP64 / FP32 records, SA): dynamic shared memory
+  // set so far, clusters of 16 allowed, and the launch shapes of the
+  // registered blocks per (cluster size, rows per node)
+  size_t smem_slab[3] = {0, 0, 0};
+  bool np_slab[3] = {false, false, false};
+  std::map<int, SlabFit> slab_fits;
   long spin_limit = kPollBudgetMax;  // polls of each staged-sweep wait (aero_set_poll_budget)
   int stall_plane = -1;              // forward plane whose copies are withheld (aero_inject_sweep_stall)
   bool configured = false;
@@ -161,7 +239,9 @@ struct State {
     int mats = 128;     // threads per CTA of k_lusgs_mats
     int nst_max = 4;    // most shared-memory stages of the staged sweep
     int sweep_cl = 0;   // CTAs per block of the global-memory sweep (0, 1: one CTA; 2..8: a cluster)
-    int sweep_x = 0;    // cluster exchange: 0 through L2, 1 bulk copies between shared memories (when it fits)
+    int sweep_x = 0;    // cluster exchange: 0 through L2, 1 bulk copies between shared memories (when it fits),
+                        // 2 pipelined k-slabs (when it fits; else 1)
+    int sa_cl = 0;      // CTAs per block of the SA sweep (0, 1: one CTA; 2..16: a cluster pipelined by k-slabs)
   } tune;
   // CUDA graph of one time step (aero_use_graphs)
   bool graph_want = false;
@@ -175,6 +255,16 @@ struct State {
 };
 
 State g;
+
+SlabFit slab_fit_for(const BlockView* hv, int nblk, int ncta, int rows) {
+  if (hv) return slab_fit(hv, nblk, ncta, rows);
+  const int key = ncta * 8 + rows;
+  auto it = g.slab_fits.find(key);
+  if (it != g.slab_fits.end()) return it->second;
+  SlabFit f = slab_fit(g.views.data(), (int)g.views.size(), ncta, rows);
+  g.slab_fits[key] = f;
+  return f;
+}
 
 // ---------------------------------------------------------------- profiling
 // Per-kernel CUDA-event timing on the library's stream (aero_profile_*), and a
@@ -324,16 +414,17 @@ void fill_view(BlockView& v, const Box& b, const Box& b0, const Box& b1, long pl
 }
 
 // LU-SGS workspace of one view (see BlockView): one device allocation holding
-// poff, rec_f, rec_b, sca, dqs, dq, sa_rec, sa_dq, nat, nbr, pidx, each array
+// poff, rec_f, rec_b, sca, dqs, dq, sa_rec, sa_dq, nat, nbr, pidx, seg, each array
 // starting on a 256-byte boundary (the sweeps' bulk copies and L2 prefetches
 // of plane chunks need 16-byte aligned starts).
 constexpr size_t kWsAlign = 256;
-constexpr int kWsArrays = 11;
+constexpr int kWsArrays = 12;
 size_t ws_round(size_t bytes) { return (bytes + kWsAlign - 1) / kWsAlign * kWsAlign; }
 size_t workspace_bytes(const Box& b1, int H) {
   size_t N1 = (size_t)b1.size();
   return (size_t)(H + 1) * sizeof(long) + N1 * (2 * kRec + kSca + 8 + 5 + kSaRec + 1) * sizeof(double) +
-         N1 * sizeof(long) + N1 * 7 * sizeof(int) + (kWsArrays + 1) * kWsAlign;
+         N1 * sizeof(long) + N1 * 7 * sizeof(int) + (size_t)H * (b1.nz() + 2) * sizeof(int) +
+         (kWsArrays + 1) * kWsAlign;
 }
 int attach_workspace(BlockView& v, void* ws, const std::vector<long>& poff, int pmax) {
   size_t N1 = (size_t)v.b1.size();
@@ -356,7 +447,11 @@ int attach_workspace(BlockView& v, void* ws, const std::vector<long>& poff, int 
   v.poff = (long*)take(poff.size() * sizeof(long));
   v.nbr = (int*)take(N1 * 7 * sizeof(int));
   v.pidx = v.nbr + 6 * N1;
+  const std::vector<int> seg = plane_segments(v.b1);
+  v.seg = (int*)take(seg.size() * sizeof(int));
   CK(cudaMemcpyAsync(v.poff, poff.data(), poff.size() * sizeof(long), cudaMemcpyHostToDevice, g.stream));
+  if (!seg.empty())
+    CK(cudaMemcpyAsync(v.seg, seg.data(), seg.size() * sizeof(int), cudaMemcpyHostToDevice, g.stream));
   return AERO_OK;
 }
 
@@ -592,9 +687,42 @@ int launch_implicit_blocks(const BlockView* views, int nblk, long maxExt, long m
 // with_blocks also runs launch_implicit_blocks first, on the same stream.
 // sweep_views (null: views) is the view array the sweep kernels index: the
 // same blocks, possibly in another order.
+// Launches kern over nblk clusters of cl CTAs (grid x = nblk * cl) of
+// `threads` threads with `smem` bytes of dynamic shared memory on stream st.
+template <typename K, typename... A>
+cudaError_t launch_clusters(K kern, int nblk, int cl, int threads, size_t smem, cudaStream_t st, A... args) {
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = dim3((unsigned)(nblk * cl));
+  lc.blockDim = dim3((unsigned)threads);
+  lc.dynamicSmemBytes = smem;
+  lc.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = (unsigned)cl;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  lc.attrs = at;
+  lc.numAttrs = 1;
+  return cudaLaunchKernelEx(&lc, kern, args...);
+}
+// The attributes a slab sweep kernel (index k of State::smem_slab) needs for
+// smem bytes of dynamic shared memory and clusters of cl CTAs.
+template <typename K>
+int prepare_slab(K kern, int k, size_t smem, int cl) {
+  if (smem > 48 * 1024 && smem > g.smem_slab[k]) {
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    g.smem_slab[k] = smem;
+  }
+  if (cl > 8 && !g.np_slab[k]) {  // 16 CTAs: a non-portable cluster size
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    g.np_slab[k] = true;
+  }
+  return AERO_OK;
+}
+
 int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, int pmax, int hmax,
                     const CaseConsts& cc, cudaEvent_t after_prep = nullptr, bool with_blocks = true,
-                    const BlockView* sweep_views = nullptr) {
+                    const BlockView* sweep_views = nullptr, const BlockView* host_views = nullptr) {
   const BlockView* sv = sweep_views ? sweep_views : views;
   // mixed precision stores the off-diagonal blocks in FP32 (products and sums
   // stay FP64); f selects that variant of every kernel that touches them
@@ -629,8 +757,22 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
   // consumer threads: one per row of every node of the largest plane
   auto consumers_for = [](int p) { return (5 * std::max(p, 1) + 31) / 32 * 32; };
   if (nst >= 2 && consumers_for(pmax) + 32 > staged_max_threads[f]) nst = 0;
-  const bool bulk = g.tune.sweep_cl >= 2 && g.tune.sweep_x == 1 && 5L * pmax <= 512L * g.tune.sweep_cl;
-  if (bulk) {
+  // slab sweep when every block's slab rows fit one CTA; else the bulk
+  // exchange when the planes fit the cluster
+  SlabFit sf;
+  const bool slabbed = g.tune.sweep_cl >= 2 && g.tune.sweep_x == 2 &&
+                       (sf = slab_fit_for(host_views, nblk, g.tune.sweep_cl, 5)).ok;
+  const bool bulk = !slabbed && g.tune.sweep_cl >= 2 && g.tune.sweep_x >= 1 && 5L * pmax <= 512L * g.tune.sweep_cl;
+  if (slabbed) {
+    // one cluster per block, each CTA one k-slab, pipelined plane by plane
+    const int cl = g.tune.sweep_cl;
+    const size_t smem = (size_t)sf.D * 5 * sf.S * sizeof(double);
+    auto kern = f ? k_lusgs_sweep_slab_f32 : k_lusgs_sweep_slab;
+    if ((rc = prepare_slab(kern, f, smem, cl))) return rc;
+    cudaError_t le = cudaSuccess;
+    PROF(P_LUSGS_SWEEP, (le = launch_clusters(kern, nblk, cl, sf.T, smem, g.stream, sv, g.d_status, sf.S, sf.D)));
+    CK(le);
+  } else if (bulk) {
     // one cluster per block, one thread per row of every node of the largest
     // plane; the plane values travel between the CTAs' shared memories
     const int cl = g.tune.sweep_cl;
@@ -716,7 +858,7 @@ int launch_index(const BlockView* views, int nblk, long maxN1) {
 // sa_model (sub_tur_sa.f90:7-122) on nblk views, on stream st (the library's
 // stream when null); needs the hyperplane index.
 int launch_sa(const BlockView* views, int nblk, long maxN, long maxN1, int pmax, const CaseConsts& cc,
-              cudaStream_t st = nullptr) {
+              cudaStream_t st = nullptr, const BlockView* host_views = nullptr) {
   if (!st) st = g.stream;
   PROF_ON(P_FILL, st, (k_sa_length<<<dim3(cdiv(maxN, 256), nblk), 256, 0, st>>>(views, cc)));
   CKL();
@@ -726,6 +868,19 @@ int launch_sa(const BlockView* views, int nblk, long maxN, long maxN1, int pmax,
   CKL();
   PROF_ON(P_SA_RECS, st, (k_sa_recs<<<dim3(cdiv(maxN1, 256), nblk), 256, 0, st>>>(views, cc)));
   CKL();
+  SlabFit sf;
+  if (g.tune.sa_cl >= 2 && (sf = slab_fit_for(host_views, nblk, g.tune.sa_cl, 1)).ok) {
+    // one cluster per block, each CTA one k-slab, pipelined plane by plane
+    const int cl = g.tune.sa_cl;
+    const size_t smem = (size_t)sf.D * sf.S * sizeof(double);
+    int rc = prepare_slab(k_sa_sweep_slab, 2, smem, cl);
+    if (rc) return rc;
+    cudaError_t le = cudaSuccess;
+    PROF_ON(P_SA_SWEEP, st, (le = launch_clusters(k_sa_sweep_slab, nblk, cl, sf.T, smem, st, views, g.d_status,
+                                                  sf.S, sf.D)));
+    CK(le);
+    return AERO_OK;
+  }
   size_t smem = (size_t)2 * std::max(pmax, 1) * sizeof(double);
   int threads = (int)std::min<long>(1024, std::max<long>(64, (pmax + 31) / 32 * 32));
   PROF_ON(P_SA_SWEEP, st, ((threads <= 768 ? k_sa_sweep_768 : k_sa_sweep)<<<nblk, threads, smem, st>>>(views)));
@@ -1176,13 +1331,51 @@ bool bulk_cluster16_fits() {
   return false;
 }
 
+// Whether a slab sweep can run as clusters of 16 CTAs on this device for the
+// registered blocks (rows = 5: the mean-flow sweep; 1: the SA sweep).
+bool slab_cluster16_fits(int rows) {
+  if (!g.setup) return false;
+  const SlabFit sf = slab_fit_for(nullptr, 0, 16, rows);
+  if (!sf.ok) return false;
+  const size_t smem = (size_t)sf.D * rows * sf.S * sizeof(double);
+  const int nk = rows == 5 ? 2 : 1;
+  for (int k = 0; k < nk; ++k) {
+    const int idx = rows == 5 ? k : 2;
+    void (*kern)(const BlockView*, unsigned*, int, int) =
+        rows == 5 ? (k ? k_lusgs_sweep_slab_f32 : k_lusgs_sweep_slab) : k_sa_sweep_slab;
+    if (prepare_slab(kern, idx, smem, 16) != AERO_OK) {
+      cudaGetLastError();
+      return false;
+    }
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(16u);
+    lc.blockDim = dim3((unsigned)sf.T);
+    lc.dynamicSmemBytes = smem;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = 16;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, kern, &lc) != cudaSuccess || n < 1) {
+      cudaGetLastError();
+      return false;
+    }
+  }
+  return true;
+}
+
+const char* exchange_name(int x) { return x == 2 ? "slab" : x == 1 ? "shared" : "l2"; }
+
 void set_tuning_text() {
-  char buf[200];
+  char buf[240];
   std::snprintf(buf, sizeof buf,
                 "inviscid_tile=%d elementwise_threads=%d viscous_threads=%d mats_threads=%d sweep_stages<=%d "
-                "sweep_cluster=%d sweep_exchange=%s",
+                "sweep_cluster=%d sweep_exchange=%s sa_sweep_cluster=%d",
                 g.tune.inv_tile, g.tune.ew, g.tune.visc, g.tune.mats, g.tune.nst_max, std::max(1, g.tune.sweep_cl),
-                g.tune.sweep_x ? "shared" : "l2");
+                exchange_name(g.tune.sweep_x), std::max(1, g.tune.sa_cl));
   g.tuning = buf;
 }
 
@@ -1231,28 +1424,34 @@ int aero_autotune(int iters) {
     ms = f;
     return AERO_OK;
   };
-  // the sweep's cluster size and exchange are one knob (value 2 * ctas +
-  // exchange), since the shared-memory exchange is only eligible for some sizes
-  int sweep_mode = 2 * g.tune.sweep_cl + g.tune.sweep_x;
+  // the sweep's cluster size and exchange are one knob (value 4 * ctas +
+  // exchange), since the exchanges are only eligible for some sizes
+  int sweep_mode = 4 * g.tune.sweep_cl + g.tune.sweep_x;
   struct Knob { int* v; std::vector<int> cand; };
   std::vector<Knob> knobs = {{&g.tune.inv_tile, {0, 32, 64, 128}}, {&g.tune.ew, {128, 256, 512}},
                              {&g.tune.visc, {64, 128, 256}}, {&g.tune.mats, {64, 128, 256}},
-                             {&g.tune.nst_max, {2, 3, 4}}, {&sweep_mode, {0, 4, 8, 16, 5, 9, 17}}};
-  if (bulk_cluster16_fits()) knobs.back().cand.push_back(33);  // 16 CTAs, bulk exchange
+                             {&g.tune.nst_max, {2, 3, 4}},
+                             {&sweep_mode, {0, 8, 16, 32, 9, 17, 33, 10, 18, 34}}};
+  if (bulk_cluster16_fits()) knobs.back().cand.push_back(65);   // 16 CTAs, bulk exchange
+  if (slab_cluster16_fits(5)) knobs.back().cand.push_back(66);  // 16 CTAs, slabs
+  if (sa_on()) {
+    knobs.push_back({&g.tune.sa_cl, {0, 2, 4, 8}});
+    if (slab_cluster16_fits(1)) knobs.back().cand.push_back(16);
+  }
   for (Knob& k : knobs) {
     int best = *k.v;
     double best_ms = 1e300;
     for (int c : k.cand) {
       *k.v = c;
-      g.tune.sweep_cl = sweep_mode / 2;
-      g.tune.sweep_x = sweep_mode % 2;
+      g.tune.sweep_cl = sweep_mode / 4;
+      g.tune.sweep_x = sweep_mode % 4;
       double ms = 0;
       if ((rc = time_steps(ms))) break;
       if (ms < best_ms) { best_ms = ms; best = c; }
     }
     *k.v = best;
-    g.tune.sweep_cl = sweep_mode / 2;
-    g.tune.sweep_x = sweep_mode % 2;
+    g.tune.sweep_cl = sweep_mode / 4;
+    g.tune.sweep_x = sweep_mode % 4;
     if (rc) break;
   }
   cudaEventDestroy(a);
@@ -1309,7 +1508,8 @@ int aero_inject_sweep_stall(int plane) {
 int aero_set_sweep_exchange(int mode) {
   int rc = need_init();
   if (rc) return rc;
-  if (mode != 0 && mode != 1) return fail(AERO_ERR_ARG, "sweep exchange %d is not 0 (L2) or 1 (shared memory)", mode);
+  if (mode < 0 || mode > 2)
+    return fail(AERO_ERR_ARG, "sweep exchange %d is not 0 (L2), 1 (shared memory) or 2 (pipelined k-slabs)", mode);
   g.tune.sweep_x = mode;
   graph_release();
   set_tuning_text();
@@ -1321,10 +1521,23 @@ int aero_set_sweep_cluster(int ctas) {
   if (rc) return rc;
   if (ctas != 1 && ctas != 2 && ctas != 4 && ctas != 8 && ctas != 16)
     return fail(AERO_ERR_ARG, "sweep cluster of %d CTAs is not 1, 2, 4, 8 or 16", ctas);
-  if (ctas == 16 && !bulk_cluster16_fits())
+  if (ctas == 16 && !bulk_cluster16_fits() && !slab_cluster16_fits(5))
     return fail(AERO_ERR_ARG, "a cluster of 16 sweep CTAs does not fit this device or these blocks "
-                              "(16 CTAs take the bulk exchange only)");
+                              "(16 CTAs take the bulk or the slab exchange only)");
   g.tune.sweep_cl = ctas == 1 ? 0 : ctas;
+  graph_release();
+  set_tuning_text();
+  return AERO_OK;
+}
+
+int aero_set_sa_sweep_cluster(int ctas) {
+  int rc = need_init();
+  if (rc) return rc;
+  if (ctas != 1 && ctas != 2 && ctas != 4 && ctas != 8 && ctas != 16)
+    return fail(AERO_ERR_ARG, "SA sweep cluster of %d CTAs is not 1, 2, 4, 8 or 16", ctas);
+  if (ctas == 16 && !slab_cluster16_fits(1))
+    return fail(AERO_ERR_ARG, "a cluster of 16 SA sweep CTAs does not fit this device or these blocks");
+  g.tune.sa_cl = ctas == 1 ? 0 : ctas;
   graph_release();
   set_tuning_text();
   return AERO_OK;
@@ -1503,6 +1716,7 @@ int aero_finish_setup(void) {
   g.arena_doubles = total;
   g.views.resize(nb);
   g.pmax_all = 0;
+  g.slab_fits.clear();
   g.hmax_all = 0;
   for (int m = 0; m < nb; ++m) {
     HostBlock& H = g.blocks[m];
@@ -1932,7 +2146,9 @@ int aero_implicit1st(double* q, const double* dt, const double* pri_v, double* r
   cc.cfl = *cfl;
   Box e{b1.is - 1, b1.ie + 1, b1.js - 1, b1.je + 1, b1.ks - 1, b1.ke + 1};
   if (!t.resident && (rc = launch_index(t.d_view, 1, b1.size()))) return rc;
-  if ((rc = launch_implicit(t.d_view, 1, e.size(), b1.size(), t.view.pmax, t.view.nplanes, cc))) return rc;
+  if ((rc = launch_implicit(t.d_view, 1, e.size(), b1.size(), t.view.pmax, t.view.nplanes, cc, nullptr, true,
+                            nullptr, &t.view)))
+    return rc;
   return finish(t, args);
 }
 
@@ -2128,7 +2344,7 @@ int aero_sa_model(double* nut, double* sa_rhs, const double* dt, const double* p
   CaseConsts cc = consts_with(g.cc.gamma, g.cc.cv, *re);
   cc.cfl = *cfl;
   if (!t.resident && (rc = launch_index(t.d_view, 1, b1.size()))) return rc;
-  if ((rc = launch_sa(t.d_view, 1, b.size(), b1.size(), t.view.pmax, cc))) return rc;
+  if ((rc = launch_sa(t.d_view, 1, b.size(), b1.size(), t.view.pmax, cc, nullptr, &t.view))) return rc;
   return finish(t, args);
 }
 

@@ -438,6 +438,130 @@ __device__ __forceinline__ void sa_sweep_body(const BlockView* __restrict__ bloc
 __global__ void __launch_bounds__(1024) k_sa_sweep(const BlockView* __restrict__ blocks) { sa_sweep_body(blocks); }
 __global__ void __launch_bounds__(768) k_sa_sweep_768(const BlockView* __restrict__ blocks) { sa_sweep_body(blocks); }
 
+// The SA sweeps pipelined over a cluster of CTAs by k-slabs, as
+// k_lusgs_sweep_slab pipelines the mean-flow sweeps (slab::Geom: CTA r owns
+// the nodes of one range of k-offsets; the CTA upstream of the pass stores the
+// values of its edge k-segment into this CTA's ring and publishes its step
+// with a release store; every wait is bounded, and the final cluster barrier
+// keeps every CTA resident until no neighbour can still store into it).  One
+// node per thread; the ring holds D planes of S values.  The arithmetic per
+// node is sa_sweep_body's, so the result is the same to the bit.
+__global__ void __launch_bounds__(512, 1) k_sa_sweep_slab(const BlockView* __restrict__ blocks, unsigned* status,
+                                                          int S, int D) {
+  extern __shared__ __align__(16) double sring[];  // D slots x S
+  __shared__ int s_prog[2];  // last step completed by the CTA below / above
+  __shared__ int s_fail;
+  const int ncta = (int)slab::size();
+  const BlockView& B = blocks[blockIdx.x / ncta];
+  if (B.retired()) return;
+  const slab::Geom G(B, ncta, (int)slab::rank());
+  const int H = G.H, tid = (int)threadIdx.x;
+  if (tid == 0) {
+    s_prog[0] = -1;
+    s_prog[1] = -1;
+    s_fail = 0;
+  }
+  slab::sync();  // every CTA's counters are set before a neighbour writes them
+  if (G.active()) {
+    const unsigned ring_l = slab::local(sring);
+    const unsigned at_lo = G.has_lo() ? slab::map(slab::local(&s_prog[1]), G.me - 1) : 0u;
+    const unsigned at_hi = G.has_hi() ? slab::map(slab::local(&s_prog[0]), G.me + 1) : 0u;
+    const unsigned ring_lo = G.has_lo() ? slab::map(ring_l, G.me - 1) : 0u;
+    const unsigned ring_hi = G.has_hi() ? slab::map(ring_l, G.me + 1) : 0u;
+    SaFwd pre_f{};
+    SaBwd pre_b{};
+    auto preload = [&](int gs) {
+      if (gs >= 2 * H) return;
+      const int h = G.plane(gs);
+      const int t0 = G.seg(h, G.c0), n = G.seg(h, G.c1) - t0;
+      if (tid < n) {
+        if (gs < H)
+          sa_load_fwd(B, h, t0 + tid, pre_f);
+        else
+          sa_load_bwd(B, h, t0 + tid, pre_b);
+      }
+    };
+    // L2 prefetch, by warp 1, of the slab's runs of step gs's records and
+    // (backward) of sa_dq and the natural indices
+    auto prefetch = [&](int gs) {
+      if (gs >= 2 * H || (tid >> 5) != 1) return;
+      const int h = G.plane(gs);
+      const long base = B.poff[h];
+      const int cnt = (int)(B.poff[h + 1] - base);
+      const int t0 = G.seg(h, G.c0), n = G.seg(h, G.c1) - t0;
+      if (n <= 0) return;
+      const int x = tid & 31;
+      if (x < kSaRec)
+        slab::prefetch_span(B.sa_rec + kSaRec * base + (long)x * cnt + t0, 8L * n);
+      else if (x == kSaRec && gs >= H)
+        slab::prefetch_span(B.sa_dq + base + t0, 8L * n);
+      else if (x == kSaRec + 1 && gs >= H)
+        slab::prefetch_span(B.nat + base + t0, 8L * n);
+    };
+    constexpr int PF = 3;  // prefetch distance in steps
+    for (int gs = 0; gs < PF; ++gs) prefetch(gs);
+    preload(0);
+    for (int gs = 0; gs < 2 * H; ++gs) {
+      const bool fwd = gs < H;
+      const int h = G.plane(gs);
+      const long base = B.poff[h];
+      const int t0 = G.seg(h, G.c0), n = G.seg(h, G.c1) - t0;
+      const bool need_dn = G.need_dn(gs);
+      bool fail = false;
+      if (G.need_up(gs)) fail = !slab::wait_for(&s_prog[fwd ? 0 : 1], gs - 1, 1L << 20);
+      if (!fail && need_dn) fail = !slab::wait_for(&s_prog[fwd ? 1 : 0], gs - D + 1, 1L << 20);
+      if (!fail) {
+        double* cur = sring + (gs % D) * S;
+        const double* prev = sring + ((gs + D - 1) % D) * S;
+        const int wlc = G.wl(h, G.me);
+        const int wlp = gs > 0 ? G.wl(G.plane(gs - 1), G.me) : 0;
+        const int e0 = need_dn ? G.seg(h, G.c_dn(gs)) : 0, e1 = need_dn ? G.seg(h, G.c_dn(gs) + 1) : 0;
+        const int wld = need_dn ? G.wl(h, G.rank_dn(gs)) : 0;
+        const unsigned slot_dn = (fwd ? ring_hi : ring_lo) + (unsigned)((gs % D) * S * 8);
+        if (tid < n) {  // the launch gives every node of a slab's plane a thread
+          const int t = t0 + tid;
+          double tt[3], v;
+          if (fwd) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              const int w = nbr_local(pre_f.packed, d);
+              tt[d] = w < 0 ? 0.0 : pre_f.a[d] * prev[w - wlp];
+            }
+            v = div_rn_lean(pre_f.rhs + (tt[0] + tt[1] + tt[2]), pre_f.diag, pre_f.rdiag);
+            B.sa_dq[base + t] = v;
+          } else {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              const int w = nbr_local(pre_b.packed, d);
+              tt[d] = w < 0 ? 0.0 : pre_b.b[d] * prev[w - wlp];
+            }
+            v = pre_b.dqs - div_rn_lean(tt[0] + tt[1] + tt[2], pre_b.diag, pre_b.rdiag);
+            B.s(F_NUT, pre_b.nat) = pre_b.nut + v;
+          }
+          cur[t - wlc] = v;
+          if (t >= e0 && t < e1) slab::store_f64(slot_dn + (unsigned)((t - wld) * 8), v);
+        }
+      }
+      if (__syncthreads_or(fail ? 1 : 0)) {
+        if (tid == 0) s_fail = 1;
+        break;
+      }
+      if (tid == 0) {
+        if (G.has_lo()) slab::store_release(at_lo, gs);
+        if (G.has_hi()) slab::store_release(at_hi, gs);
+      }
+      prefetch(gs + PF);
+      preload(gs + 1);
+    }
+  }
+  __syncthreads();
+  slab::sync();  // no CTA leaves while a neighbour may still store into it
+  if (tid == 0 && s_fail) {
+    if (status) atomicOr(status, (unsigned)ST_TIMEOUT);
+    B.raise(ST_TIMEOUT);
+  }
+}
+
 // length = dist over the full box (sub_tur_sa.f90:51-57; no DES).
 // With iflag_des = 1 (DES97) length = min(dist, cdes*spacing); with 2 (DDES)
 // length = dist - fd*max(0, dist - cdes*spacing), fd = 1 - tanh((8 rd)^3),

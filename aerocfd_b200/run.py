@@ -38,8 +38,9 @@ def main(argv=None) -> int:
     ap.add_argument("--inviscid", type=int, default=4, help="4 Roe + WENO3, 5 SW + WENO5, 8 WCNS5")
     ap.add_argument("--mixed", action="store_true")
     ap.add_argument("--sweep-cluster", type=int, default=0, help="CTAs per block of the LU-SGS sweep (0: autotune)")
-    ap.add_argument("--sweep-exchange", choices=["l2", "shared"], default=None,
+    ap.add_argument("--sweep-exchange", choices=["l2", "shared", "slab"], default=None,
                     help="plane exchange of a cluster sweep (default: the autotuner's or L2)")
+    ap.add_argument("--sa-sweep-cluster", type=int, default=0, help="CTAs per block of the SA sweep (0: autotune)")
     ap.add_argument("--no-graphs", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes")
     ap.add_argument("--tuning", type=int, nargs=5, metavar=("INV_TILE", "EW", "VISC", "MATS", "NST"),
@@ -60,7 +61,9 @@ def main(argv=None) -> int:
         if args.sweep_cluster:
             gc.set_sweep_cluster(args.sweep_cluster)
         if args.sweep_exchange:
-            gc.set_sweep_exchange(args.sweep_exchange == "shared")
+            gc.set_sweep_exchange(args.sweep_exchange)
+        if args.sa_sweep_cluster:
+            gc.set_sa_sweep_cluster(args.sa_sweep_cluster)
         gc.use_graphs(not args.no_graphs)
         gc.step(args.warmup, history=False)
         ms = ctypes.c_double(0.0)

@@ -135,13 +135,20 @@ class GpuCase:
                                           ctypes.c_int(mats), ctypes.c_int(nst_max)), "aero_set_tuning")
 
     def set_sweep_cluster(self, ctas: int) -> None:
-        """aero_set_sweep_cluster: CTAs per block of the LU-SGS sweep (1, 2, 4, 8)."""
+        """aero_set_sweep_cluster: CTAs per block of the LU-SGS sweep (1, 2, 4, 8, 16)."""
         _lib.check(self.L.aero_set_sweep_cluster(ctypes.c_int(ctas)), "aero_set_sweep_cluster")
 
-    def set_sweep_exchange(self, shared: bool) -> None:
-        """aero_set_sweep_exchange: plane values of a cluster sweep through L2
-        (False) or by bulk copies between the CTAs' shared memories (True)."""
-        _lib.check(self.L.aero_set_sweep_exchange(ctypes.c_int(1 if shared else 0)), "aero_set_sweep_exchange")
+    def set_sweep_exchange(self, mode) -> None:
+        """aero_set_sweep_exchange: how a cluster shares a sweep: "l2" (or
+        False), "shared" (or True: bulk copies between shared memories) or
+        "slab" (CTAs pipelined by k-slabs)."""
+        code = {"l2": 0, "shared": 1, "slab": 2}[mode] if isinstance(mode, str) else (1 if mode else 0)
+        _lib.check(self.L.aero_set_sweep_exchange(ctypes.c_int(code)), "aero_set_sweep_exchange")
+
+    def set_sa_sweep_cluster(self, ctas: int) -> None:
+        """aero_set_sa_sweep_cluster: CTAs per block of the SA sweep (1, 2, 4,
+        8, 16), pipelined by k-slabs."""
+        _lib.check(self.L.aero_set_sa_sweep_cluster(ctypes.c_int(ctas)), "aero_set_sa_sweep_cluster")
 
     def set_poll_budget(self, polls: int) -> None:
         """aero_set_poll_budget: polls of each bounded wait of the staged LU-SGS

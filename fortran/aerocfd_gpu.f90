@@ -105,10 +105,17 @@ module aerocfd_gpu
     end function
 
     ! plane-value exchange of a cluster sweep: 0 through L2, 1 bulk copies
-    ! between shared memories (no counterpart in the reference)
+    ! between shared memories, 2 pipelined k-slabs (no counterpart in the
+    ! reference)
     integer(c_int) function aero_set_sweep_exchange(mode) bind(C, name="aero_set_sweep_exchange")
       import :: c_int
       integer(c_int), value :: mode
+    end function
+
+    ! CTAs per block of the SA sweep, pipelined by k-slabs (1, 2, 4, 8, 16)
+    integer(c_int) function aero_set_sa_sweep_cluster(ctas) bind(C, name="aero_set_sa_sweep_cluster")
+      import :: c_int
+      integer(c_int), value :: ctas
     end function
 
     ! polls of each bounded wait of the staged LU-SGS sweep (fault-injection

@@ -324,17 +324,27 @@ const char* aero_tuning(void);
 int aero_set_tuning(int inv_tile, int ew, int visc, int mats, int nst_max);
 /* CTAs that share each block's LU-SGS sweep: 1 (one CTA per block, the
  * records staged in shared memory when its planes fit) or a thread-block
- * cluster of 2, 4 or 8 CTAs meeting at a cluster barrier between hyperplanes,
- * or 16 CTAs (a non-portable cluster size, with the bulk-copy exchange only;
- * accepted after aero_finish_setup when the device can hold such a cluster).
- * The arithmetic is the same for every choice. */
+ * cluster of 2, 4 or 8 CTAs, or 16 CTAs (a non-portable cluster size, with
+ * the bulk-copy or the slab exchange only; accepted after aero_finish_setup
+ * when the device can hold such a cluster).  The arithmetic is the same for
+ * every choice. */
 int aero_set_sweep_cluster(int ctas);
-/* How a cluster's CTAs pass each hyperplane's values to the next plane: 0
- * (default) through L2 with a cluster barrier per plane, 1 by bulk copies
- * between the CTAs' shared memories counted on mbarriers (used when every row
- * of the largest plane has its own thread: 5 x plane nodes <= 512 x CTAs).
- * The arithmetic is the same either way. */
+/* How a cluster's CTAs share a block's sweep: 0 (default) every CTA a part
+ * of each hyperplane, the values passed through L2 with a cluster barrier
+ * per plane; 1 the same with bulk copies between the CTAs' shared memories
+ * counted on mbarriers (used when every row of the largest plane has its own
+ * thread: 5 x plane nodes <= 512 x CTAs); 2 every CTA one range of k
+ * (a k-slab), the CTAs pipelined plane by plane, each passing only its edge
+ * k-segment's values to the next CTA (used when each slab's part of a plane
+ * has at most 102 nodes; else 1).  The arithmetic is the same for every
+ * choice. */
 int aero_set_sweep_exchange(int mode);
+/* CTAs that share each block's SA sweep: 1 (default; one CTA per block) or a
+ * cluster of 2, 4 or 8 CTAs pipelined by k-slabs as exchange 2 above (used
+ * when each slab's part of a plane has at most 512 nodes), or 16 (accepted
+ * after aero_finish_setup when the device can hold such a cluster).  The
+ * arithmetic is the same for every choice. */
+int aero_set_sa_sweep_cluster(int ctas);
 /* Polls each bounded wait of the staged LU-SGS sweep (one CTA per block)
  * makes before it gives up, 0..1048576 (the default); each poll may suspend
  * the waiting thread for a short, system-dependent time.  A wait that gives

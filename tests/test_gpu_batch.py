@@ -130,30 +130,37 @@ def test_every_launch_shape_gives_the_same_bits(gpu, make):
 def test_sweep_cluster_gives_the_same_bits(gpu, make):
     """The LU-SGS sweep on one CTA per block (staged in shared memory, or from
     global memory when the planes are too large: the 129 x 65 x 9 bump) and
-    on clusters of 2, 4 and 8 CTAs per block passing plane values through L2
-    or by bulk copies between shared memories, and on clusters of 16 CTAs
-    (bulk copies; a non-portable cluster size, taken where the device holds
-    one): identical histories and states, in FP64 and mixed precision."""
+    on clusters of 2, 4 and 8 CTAs per block passing plane values through L2,
+    by bulk copies between shared memories, or pipelined by k-slabs, and on
+    clusters of 16 CTAs (bulk copies or slabs; a non-portable cluster size,
+    taken where the device holds one); the SA sweep (the plate) on one CTA or
+    on clusters of k-slabs: identical histories and states, in FP64 and mixed
+    precision.  Slab clusters larger than a block's k-extent leave CTAs idle
+    (the aerofoil: one k-offset), and slabs too wide for one CTA fall back to
+    the bulk or the L2 exchange (the bump on 2 and 4 CTAs)."""
     from aerocfd_b200 import _lib
     for mixed in (False, True):
         ref = None
-        for ctas, shared in ((1, False), (2, False), (4, False), (8, False), (2, True), (4, True), (8, True),
-                             (16, True)):
+        for ctas, exch, sa_ctas in ((1, "l2", 1), (2, "l2", 1), (4, "l2", 1), (8, "l2", 1), (2, "shared", 1),
+                                    (4, "shared", 1), (8, "shared", 1), (16, "shared", 1), (2, "slab", 2),
+                                    (4, "slab", 4), (8, "slab", 8), (16, "slab", 16), (8, "slab", 1),
+                                    (1, "l2", 4)):
             case = make()
             gc = gpu.GpuCase(case)
             try:
                 try:
                     gc.set_sweep_cluster(ctas)
+                    gc.set_sa_sweep_cluster(sa_ctas)
                 except _lib.AeroError:
-                    assert ctas == 16  # the device holds no 16-CTA cluster
+                    assert 16 in (ctas, sa_ctas)  # the device holds no 16-CTA cluster
                     continue
-                gc.set_sweep_exchange(shared)
+                gc.set_sweep_exchange(exch)
                 gc.set_precision(mixed)
                 gc.compute_geometry()
                 gc.init_flowfield()
                 gc.start()
                 h = gc.step(4)
-                assert gc.status() == 0, (ctas, shared)
+                assert gc.status() == 0, (ctas, exch, sa_ctas)
                 gc.sync_to_host(gpu.mask("q", "nut"))
                 out = (h, [b.fields["q"].copy() for b in case.blocks], [b.fields["nut"].copy() for b in case.blocks])
             finally:
@@ -161,9 +168,9 @@ def test_sweep_cluster_gives_the_same_bits(gpu, make):
             if ref is None:
                 ref = out
                 continue
-            assert np.array_equal(out[0], ref[0]), (mixed, ctas, shared)
+            assert np.array_equal(out[0], ref[0]), (mixed, ctas, exch, sa_ctas)
             for a, b in zip(out[1] + out[2], ref[1] + ref[2]):
-                assert np.array_equal(a, b), (mixed, ctas, shared)
+                assert np.array_equal(a, b), (mixed, ctas, exch, sa_ctas)
 
 
 
