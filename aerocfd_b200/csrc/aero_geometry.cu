@@ -210,9 +210,12 @@ __global__ void k_wall_points(const BlockView* __restrict__ blocks, const AvgSrc
 // sub_init_walldist.f90:39-90: distance from each physical node to the nearest
 // wall node (brute force).  sqrt is monotone and correctly rounded, so the
 // square root of the smallest squared distance equals the smallest distance.
+// The wall nodes of block m's case are xyz entries [range[2m], range[2m] +
+// range[2m+1]).
 __global__ void k_walldist(const BlockView* __restrict__ blocks, const double* __restrict__ xyz,
-                           long nwall) {
+                           const long* __restrict__ range) {
   const BlockView& B = blocks[blockIdx.y];
+  const long first = range[2 * blockIdx.y], nwall = range[2 * blockIdx.y + 1];
   const Box& b0 = B.b0;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   extern __shared__ double tile[];
@@ -231,9 +234,9 @@ __global__ void k_walldist(const BlockView* __restrict__ blocks, const double* _
   for (long base = 0; base < nwall; base += blockDim.x) {
     long w = base + threadIdx.x;
     if (w < nwall) {
-      tile[3 * threadIdx.x + 0] = xyz[3 * w + 0];
-      tile[3 * threadIdx.x + 1] = xyz[3 * w + 1];
-      tile[3 * threadIdx.x + 2] = xyz[3 * w + 2];
+      tile[3 * threadIdx.x + 0] = xyz[3 * (first + w) + 0];
+      tile[3 * threadIdx.x + 1] = xyz[3 * (first + w) + 1];
+      tile[3 * threadIdx.x + 2] = xyz[3 * (first + w) + 2];
     }
     __syncthreads();
     long cnt = min((long)blockDim.x, nwall - base);

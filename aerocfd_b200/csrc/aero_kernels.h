@@ -148,6 +148,6 @@ __global__ void k_spacing(const BlockView* __restrict__ blocks);
 __global__ void k_wall_points(const BlockView* __restrict__ blocks, const AvgSrc* __restrict__ wall,
                               long nwall, double* __restrict__ xyz);
 __global__ void k_walldist(const BlockView* __restrict__ blocks, const double* __restrict__ xyz,
-                           long nwall);
+                           const long* __restrict__ range);
 
 }  // namespace aero

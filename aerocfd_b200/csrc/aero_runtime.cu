@@ -2380,22 +2380,51 @@ int aero_gridtransformation(double* dxidx, double* inv_j, double* alpha, double*
 int aero_init_walldist(void) {
   int rc = need_setup();
   if (rc) return rc;
-  // wall-subface nodes of every block (sub_init_readbcinfo.f90:286-388)
+  // Independent cases registered together (a batch) are the connected
+  // components of the block-interface graph; every node's distance is to the
+  // walls of its own case, as when that case runs alone (one case: all
+  // walls, as the reference).
+  const int nb = (int)g.blocks.size();
+  std::vector<int> root(nb);
+  for (int m = 0; m < nb; ++m) root[m] = m;
+  auto find = [&](int m) {
+    while (root[m] != m) m = root[m] = root[root[m]];
+    return m;
+  };
+  for (int m = 0; m < nb; ++m)
+    for (const SubRow& s : g.blocks[m].subs)
+      if (s.blk_t > 0 && s.blk_t <= nb) {
+        const int a = find(m), b = find(s.blk_t - 1);
+        if (a != b) root[std::max(a, b)] = std::min(a, b);
+      }
+  // wall-subface nodes of every block (sub_init_readbcinfo.f90:286-388),
+  // grouped by case; range[2m], range[2m+1]: first and count of block m's case
   std::vector<AvgSrc> wall;
-  for (int m = 0; m < (int)g.blocks.size(); ++m) {
-    const HostBlock& H = g.blocks[m];
-    for (const SubRow& s : H.subs) {
-      if (s.blk_t != BC_WALL) continue;
-      for (int k = s.ks; k <= s.ke; ++k)
-        for (int j = s.js; j <= s.je; ++j)
-          for (int i = s.is; i <= s.ie; ++i) {
-            int ii = s.face == 1 ? H.b0.is : s.face == 2 ? H.b0.ie : i;
-            int jj = s.face == 3 ? H.b0.js : s.face == 4 ? H.b0.je : j;
-            int kk = s.face == 5 ? H.b0.ks : s.face == 6 ? H.b0.ke : k;
-            long n = (long)(ii - H.b.is) + (long)H.b.nx() * ((long)(jj - H.b.js) + (long)H.b.ny() * (long)(kk - H.b.ks));
-            wall.push_back(AvgSrc{m, n});
-          }
+  std::vector<long> range(2 * (size_t)nb, 0);
+  for (int c = 0; c < nb; ++c) {
+    if (find(c) != c) continue;
+    const long first = (long)wall.size();
+    for (int m = 0; m < nb; ++m) {
+      if (find(m) != c) continue;
+      const HostBlock& H = g.blocks[m];
+      for (const SubRow& s : H.subs) {
+        if (s.blk_t != BC_WALL) continue;
+        for (int k = s.ks; k <= s.ke; ++k)
+          for (int j = s.js; j <= s.je; ++j)
+            for (int i = s.is; i <= s.ie; ++i) {
+              int ii = s.face == 1 ? H.b0.is : s.face == 2 ? H.b0.ie : i;
+              int jj = s.face == 3 ? H.b0.js : s.face == 4 ? H.b0.je : j;
+              int kk = s.face == 5 ? H.b0.ks : s.face == 6 ? H.b0.ke : k;
+              long n = (long)(ii - H.b.is) + (long)H.b.nx() * ((long)(jj - H.b.js) + (long)H.b.ny() * (long)(kk - H.b.ks));
+              wall.push_back(AvgSrc{m, n});
+            }
+      }
     }
+    for (int m = 0; m < nb; ++m)
+      if (find(m) == c) {
+        range[2 * m] = first;
+        range[2 * m + 1] = (long)wall.size() - first;
+      }
   }
   long nw = (long)wall.size();
   AvgSrc* d_wall = nullptr;
@@ -2407,11 +2436,16 @@ int aero_init_walldist(void) {
     PROF(P_GEOMETRY, (k_wall_points<<<cdiv(nw, 256), 256, 0, g.stream>>>(g.d_blocks, d_wall, nw, d_xyz)));
     CKL();
   }
-  PROF(P_GEOMETRY, (k_walldist<<<dim3(cdiv(g.max_b0, 256), (unsigned)g.blocks.size()), 256, 256 * 3 * sizeof(double), g.stream>>>( g.d_blocks, d_xyz, nw)));
+  long* d_range = nullptr;
+  CK(cudaMalloc(&d_range, range.size() * sizeof(long)));
+  CK(cudaMemcpyAsync(d_range, range.data(), range.size() * sizeof(long), cudaMemcpyHostToDevice, g.stream));
+  PROF(P_GEOMETRY, (k_walldist<<<dim3(cdiv(g.max_b0, 256), (unsigned)nb), 256, 256 * 3 * sizeof(double), g.stream>>>(
+                       g.d_blocks, d_xyz, d_range)));
   CKL();
   CK(cudaStreamSynchronize(g.stream));
   if (d_wall) CK(cudaFree(d_wall));
   if (d_xyz) CK(cudaFree(d_xyz));
+  CK(cudaFree(d_range));
   return AERO_OK;
 }
 
