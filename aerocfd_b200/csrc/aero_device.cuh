@@ -231,6 +231,8 @@ enum StatusBits : unsigned {
 // ------------------------------------------- thread-block cluster primitives
 // (the slab sweeps: a CTA's progress counters and ring slots are written by
 // its neighbours in the cluster)
+// Ring, inbox and staging slots (planes) of a slab sweep, at most.
+constexpr int kSlabSlots = 8;
 namespace slab {
 __device__ __forceinline__ unsigned rank() {
   unsigned r;
@@ -254,21 +256,59 @@ __device__ __forceinline__ unsigned map(unsigned addr, unsigned r) {
 __device__ __forceinline__ void sync() {
   asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
-// acquire load of a counter in this CTA's shared memory that other CTAs of
-// the cluster write
-__device__ __forceinline__ int load_acquire(const int* p) {
+// relaxed store of a counter into another CTA's shared memory (no fence: the
+// counters only say that a slot's earlier contents have been read)
+__device__ __forceinline__ void store_relaxed(unsigned remote, int v) {
+  asm volatile("st.relaxed.cluster.shared::cluster.u32 [%0], %1;" ::"r"(remote), "r"(v) : "memory");
+}
+__device__ __forceinline__ int load_relaxed(const int* p) {
   int v;
-  asm volatile("ld.acquire.cluster.shared::cta.u32 %0, [%1];" : "=r"(v) : "r"(local(p)) : "memory");
+  asm volatile("ld.relaxed.cluster.shared::cta.u32 %0, [%1];" : "=r"(v) : "r"(local(p)) : "memory");
   return v;
 }
-// release store of a counter into another CTA's shared memory: every store
-// this CTA's threads issued before a CTA barrier that precedes it is visible
-// to a thread that reads the counter with load_acquire
-__device__ __forceinline__ void store_release(unsigned remote, int v) {
-  asm volatile("st.release.cluster.shared::cluster.u32 [%0], %1;" ::"r"(remote), "r"(v) : "memory");
+// mbarriers of this CTA
+__device__ __forceinline__ void bar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(local(bar)), "r"(count) : "memory");
 }
-__device__ __forceinline__ void store_f64(unsigned remote, double v) {
-  asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(remote), "d"(v) : "memory");
+// this CTA's arrival on `bar` with `bytes` more to come from copies
+__device__ __forceinline__ void bar_expect(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(local(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool bar_try(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(local(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait for the phase of `bar` with this parity; false when it did not
+// complete within `limit` polls
+__device__ __forceinline__ bool bar_wait(unsigned long long* bar, unsigned parity, long limit) {
+  long spins = 0;
+  while (!bar_try(bar, parity))
+    if (++spins > limit) return false;
+  return true;
+}
+// bulk copy of `bytes` from this CTA's shared memory into another CTA's of the
+// cluster, counted in bytes on the receiver's mbarrier (no multicast); both
+// addresses 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void copy_to(unsigned dst, unsigned src, unsigned bytes, unsigned remote_bar) {
+  asm volatile("cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   dst),
+               "r"(src), "r"(bytes), "r"(remote_bar)
+               : "memory");
+}
+// this thread's shared-memory writes visible to the bulk copies it issues next
+__device__ __forceinline__ void fence_to_copies() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// Bounded wait until a counter of this CTA (written by a neighbour with
+// store_relaxed) reaches v; false when it did not within `limit` polls.
+__device__ __forceinline__ bool wait_for(const int* counter, int v, long limit) {
+  long spins = 0;
+  while (load_relaxed(counter) < v)
+    if (++spins > limit) return false;
+  return true;
 }
 // L2 prefetch of [p, p + bytes) widened to 16-byte boundaries; the caller
 // keeps the widened range inside one allocation
@@ -277,14 +317,6 @@ __device__ __forceinline__ void prefetch_span(const void* p, long bytes) {
   const unsigned long long a = (unsigned long long)p & ~15ull;
   const unsigned long long e = ((unsigned long long)p + (unsigned long long)bytes + 15ull) & ~15ull;
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((unsigned)(e - a)) : "memory");
-}
-// Bounded wait until a counter of this CTA reaches v; false when it did not
-// within `limit` polls.
-__device__ __forceinline__ bool wait_for(const int* counter, int v, long limit) {
-  long spins = 0;
-  while (load_acquire(counter) < v)
-    if (++spins > limit) return false;
-  return true;
 }
 
 // The k-slab of one CTA of a slab sweep and its links to the neighbouring
@@ -313,9 +345,6 @@ struct Geom {
   __device__ int c0_of(int r) const { return r * nz1 / ce; }
   // nodes of plane h with k-offset below c (c = -1 .. nz1)
   __device__ int seg(int h, int c) const { return segt[h * SW + c + 1]; }
-  // first plane-local index held in a ring slot of slab r for plane h: the
-  // k-segment below the slab (or the slab itself for r = 0)
-  __device__ int wl(int h, int r) const { return seg(h, max(c0_of(r) - 1, 0)); }
   __device__ int plane(int gs) const { return gs < H ? gs : 2 * H - 1 - gs; }
   __device__ bool has_lo() const { return me > 0 && me < ce; }
   __device__ bool has_hi() const { return me + 1 < ce; }
@@ -335,9 +364,39 @@ struct Geom {
   }
   // this slab's edge k-segment the downstream slab reads at step gs
   __device__ int c_dn(int gs) const { return gs < H ? c1 - 1 : c0; }
+  // the upstream slab's edge k-segment, whose values of step gs-1 step gs reads
+  __device__ int c_up(int gs) const { return gs < H ? c0 - 1 : c1; }
   // the downstream CTA's rank at step gs
   __device__ int rank_dn(int gs) const { return gs < H ? me + 1 : me - 1; }
 };
+
+// End of a slab sweep for every CTA of the cluster: the CTAs exchange their
+// failure flags (s_fail, shared); if any CTA failed, each idles for a bounded
+// time after the last cluster barrier, so that copies issued before that
+// barrier land before any CTA leaves, and a CTA that failed raises
+// ST_TIMEOUT for its block.
+__device__ __forceinline__ void finish(const int& s_fail, int ncta, unsigned* status, const BlockView& B) {
+  __syncthreads();
+  sync();
+  unsigned any = s_fail ? 1u : 0u;
+  if ((int)threadIdx.x < ncta && threadIdx.x != rank()) {
+    unsigned v;
+    asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(map(local(&s_fail), threadIdx.x)) : "memory");
+    any |= v != 0u ? 1u : 0u;
+  }
+  any = __syncthreads_or(any);
+  sync();
+  if (any) {
+    if (threadIdx.x == 0) {
+      for (int x = 0; x < 2000; ++x) __nanosleep(1000);
+      if (s_fail) {
+        if (status) atomicOr(status, (unsigned)ST_TIMEOUT);
+        B.raise(ST_TIMEOUT);
+      }
+    }
+    __syncthreads();
+  }
+}
 }  // namespace slab
 #endif
 

@@ -1227,24 +1227,28 @@ __device__ __forceinline__ void load_node_row(const R* rec, const double* sca, i
   r.rinvj = sn[8 * cnt];
   r.bok = !nbr_slow_div(r.packed);
 }
-// lusgs_rows' arithmetic for one row from preloaded records, the previous
-// plane's values read from a ring slot (row c of plane-local node w at
-// prev[c*S + w - wl]).
+// lusgs_rows' arithmetic for one row from preloaded records.  The previous
+// plane's values: row c of plane-local node w at own[c*So + w - o0] for the
+// slab's own nodes [o0, o0 + no), else (the k-neighbour in the upstream
+// slab's edge segment, which starts at eb) at edge[c*L + w - eb].
 template <bool FWD>
-__device__ __forceinline__ double row_from_slot(const RowRecs& r, const double* prev, int wl, int S,
-                                                const double* dsv, int cnt) {
+__device__ __forceinline__ double row_from_slab(const RowRecs& r, const double* own, int o0, int no, int So,
+                                                const double* edge, int eb, int L, const double* dsv, int cnt) {
   double acc[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     int w = nbr_local(r.packed, d);
     double sd = 0.0;
     if (w >= 0) {
-      const double* x = prev + (w - wl);
+      // the i and j neighbours share the node's k-offset, so they are the slab's own
+      const bool mine = d < 2 || (unsigned)(w - o0) < (unsigned)no;
+      const double* x = mine ? own + (w - o0) : edge + (w - eb);
+      const int st = mine ? So : L;
       sd = r.m[5 * d] * x[0];
-      sd = sd + r.m[5 * d + 1] * x[S];
-      sd = sd + r.m[5 * d + 2] * x[2 * S];
-      sd = sd + r.m[5 * d + 3] * x[3 * S];
-      sd = sd + r.m[5 * d + 4] * x[4 * S];
+      sd = sd + r.m[5 * d + 1] * x[st];
+      sd = sd + r.m[5 * d + 2] * x[2 * st];
+      sd = sd + r.m[5 * d + 3] * x[3 * st];
+      sd = sd + r.m[5 * d + 4] * x[4 * st];
     }
     acc[d] = sd;
   }
@@ -1263,27 +1267,37 @@ __device__ __forceinline__ double row_from_slot(const RowRecs& r, const double* 
 // node per thread, in the hyperplane order of the serial sweep.  Within a
 // slab every neighbour a node needs from the previous plane is the CTA's own,
 // except the k-1 (forward) / k+1 (backward) neighbours of the slab's first /
-// last k-segment, which the CTA below / above computes: that CTA stores them
-// straight into this CTA's ring (st.shared::cluster) and then publishes its
-// progress (the last step it completed) with a release store into this CTA's
-// counter.  So a CTA waits only for the step before its own on one neighbour,
-// and the CTAs run as a pipeline, each a few planes behind its upstream
-// neighbour: the pass takes about H plane steps plus one neighbour latency per
-// slab, instead of a cluster-wide exchange on every plane.  The ring holds D
-// planes; a CTA writes into a neighbour's slot only after that neighbour has
-// finished the step that read the slot's previous plane (its counter, which
-// it publishes to both neighbours), so the ring never overflows.  No CTA can
+// last k-segment, which belong to the edge k-segment of the slab below /
+// above (the pass's "upstream" slab).  After each plane a CTA stages its own
+// edge segment's values and copies them with one cp.async.bulk (no multicast)
+// into the downstream CTA's inbox, counted in bytes on the receiver's mbarrier
+// for that inbox slot; a CTA waits only on that mbarrier, for the step before
+// its own.  So the CTAs run as a pipeline, each a few planes behind its
+// upstream neighbour, and a pass takes about H plane steps plus one
+// neighbour latency per slab, with no cluster-wide exchange on any plane and
+// no memory fence on the plane-to-plane path.  Rings, inboxes and staging
+// areas hold D planes.  After each step a CTA tells both neighbours the last
+// step it completed (a relaxed store into their shared memory); a CTA copies
+// step gs into a neighbour's slot only after that neighbour has completed
+// step gs-D+1, which waited for the slot's previous copy, so no slot is
+// overwritten while in use and no mbarrier phase is armed twice.  No CTA can
 // wait forever on another: each wait is for a CTA at an earlier step, and
-// every wait is bounded.  A wait that runs out makes the CTA stop (its
-// neighbours then run out too), and the final cluster barrier keeps every CTA
-// resident until no neighbour can still store into it; no asynchronous copy
-// is used.  The arithmetic per row is lusgs_rows', so the result is the same
-// to the bit.
+// every wait is bounded.  A wait that runs out makes the CTA stop sending (its
+// neighbours then run out too); at the end the CTAs exchange their failure
+// flags, and if any failed each idles for a bounded time after the last
+// cluster barrier, so copies issued before that barrier land before any CTA
+// leaves.  Without a failure every copy into a CTA is waited for before the
+// last barrier.  The arithmetic per row is lusgs_rows', so the result is the
+// same to the bit.
 template <typename R>
-__device__ __forceinline__ void lusgs_slab_body(const BlockView* __restrict__ blocks, unsigned* status, int S,
-                                                int D) {
+__device__ __forceinline__ void lusgs_slab_body(const BlockView* __restrict__ blocks, unsigned* status, int So,
+                                                int L, int D) {
   constexpr int W = RecFmt<R>::kWords;
-  extern __shared__ __align__(16) double sring[];  // D slots x 5 rows x S
+  extern __shared__ __align__(16) double sdyn[];
+  double* stage = sdyn;                // D x 5 x L: this slab's edge values, copied downstream
+  double* inbox = stage + D * 5 * L;   // D x 5 x L: the upstream slab's edge values
+  double* ring = inbox + D * 5 * L;    // D x 5 x So: this slab's values
+  __shared__ __align__(8) unsigned long long full[kSlabSlots];  // inbox slot arrivals
   __shared__ int s_prog[2];  // last step completed by the CTA below / above
   __shared__ int s_fail;
   const int ncta = (int)slab::size();
@@ -1296,17 +1310,18 @@ __device__ __forceinline__ void lusgs_slab_body(const BlockView* __restrict__ bl
     s_prog[0] = -1;
     s_prog[1] = -1;
     s_fail = 0;
+    for (int x = 0; x < D; ++x) slab::bar_init(&full[x], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  slab::sync();  // every CTA's counters are set before a neighbour writes them
+  slab::sync();  // every CTA's counters and mbarriers exist before a neighbour touches them
+  const unsigned slot_bytes = (unsigned)(5 * L * sizeof(double));
   if (G.active()) {
-    const unsigned ring_l = slab::local(sring);
     // this CTA's progress lives in the CTA below as its "above" counter and in
     // the CTA above as its "below" counter
     const unsigned at_lo = G.has_lo() ? slab::map(slab::local(&s_prog[1]), G.me - 1) : 0u;
     const unsigned at_hi = G.has_hi() ? slab::map(slab::local(&s_prog[0]), G.me + 1) : 0u;
-    const unsigned ring_lo = G.has_lo() ? slab::map(ring_l, G.me - 1) : 0u;
-    const unsigned ring_hi = G.has_hi() ? slab::map(ring_l, G.me + 1) : 0u;
-    RowRecs pre;  // the records of this thread's first row of the next step
+    const unsigned inbox_l = slab::local(inbox), full_l = slab::local(full), stage_l = slab::local(stage);
+    RowRecs pre;  // the records of this thread's row of the next step
     auto preload = [&](int gs) {
       if (gs >= 2 * H) return;
       const bool fwd = gs < H;
@@ -1347,6 +1362,7 @@ __device__ __forceinline__ void lusgs_slab_body(const BlockView* __restrict__ bl
     constexpr int PF = 3;  // prefetch distance in steps
     for (int gs = 0; gs < PF; ++gs) prefetch(gs);
     preload(0);
+    unsigned parity = 0;  // bit x: parity of the next phase of full[x] to wait for
     for (int gs = 0; gs < 2 * H; ++gs) {
       const bool fwd = gs < H;
       const int h = G.plane(gs);
@@ -1354,62 +1370,64 @@ __device__ __forceinline__ void lusgs_slab_body(const BlockView* __restrict__ bl
       const int cnt = (int)(poff[h + 1] - base);
       const int t0 = G.seg(h, G.c0), n = G.seg(h, G.c1) - t0;
       const bool need_dn = G.need_dn(gs);
+      const int x = gs % D, xp = (gs + D - 1) % D;
       bool fail = false;
-      // the upstream slab's values of the previous step
-      if (G.need_up(gs)) fail = !slab::wait_for(&s_prog[fwd ? 0 : 1], gs - 1, kSpinLimit);
-      // room in the downstream slab's ring: it has finished step gs-D+1,
-      // the last to read the slot's previous plane
-      if (!fail && need_dn) fail = !slab::wait_for(&s_prog[fwd ? 1 : 0], gs - D + 1, kSpinLimit);
-      if (!fail) {
-        double* cur = sring + (gs % D) * 5 * S;
-        const double* prev = sring + ((gs + D - 1) % D) * 5 * S;
-        const int wlc = G.wl(h, G.me);
-        const int wlp = gs > 0 ? G.wl(G.plane(gs - 1), G.me) : 0;
-        // this slab's edge nodes the downstream slab reads, and where they go
-        const int e0 = need_dn ? G.seg(h, G.c_dn(gs)) : 0, e1 = need_dn ? G.seg(h, G.c_dn(gs) + 1) : 0;
-        const int wld = need_dn ? G.wl(h, G.rank_dn(gs)) : 0;
-        const unsigned slot_dn = (fwd ? ring_hi : ring_lo) + (unsigned)((gs % D) * 5 * S * 8);
-        const double* dsv = B.dqs + 8 * base;
-        auto item = [&](const RowRecs& r) {
-          const double v = fwd ? row_from_slot<true>(r, prev, wlp, S, dsv, cnt)
-                               : row_from_slot<false>(r, prev, wlp, S, dsv, cnt);
-          cur[r.row * S + (r.node - wlc)] = v;
-          if (r.node >= e0 && r.node < e1) slab::store_f64(slot_dn + (unsigned)((r.row * S + r.node - wld) * 8), v);
-          if (fwd)
-            B.dqs[8 * base + r.row * cnt + r.node] = v;
-          else
-            B.dq[5 * (base + r.node) + r.row] = v;
-        };
-        if (tid < 5 * n) item(pre);  // the launch gives every row of a slab's plane a thread
+      if (G.need_up(gs)) {
+        // the upstream slab's edge values of step gs-1, copied into inbox slot xp
+        if (tid == 0) slab::bar_expect(&full[xp], slot_bytes);
+        fail = !slab::bar_wait(&full[xp], (parity >> xp) & 1u, kSpinLimit);
+        parity ^= 1u << xp;
       }
-      // every thread's values of this step are stored (locally and in the
-      // downstream ring) before thread 0 publishes the step
+      // room downstream: it has completed step gs-D+1, which waited for the
+      // previous copy into slot x (so that copy also finished reading stage x)
+      if (!fail && need_dn) fail = !slab::wait_for(&s_prog[fwd ? 1 : 0], gs - D + 1, kSpinLimit);
+      if (!fail && tid < 5 * n) {  // the launch gives every row of a slab's plane a thread
+        const int hp = G.plane(gs > 0 ? gs - 1 : 0);
+        const int p0 = G.seg(hp, G.c0), np = G.seg(hp, G.c1) - p0;
+        const int eb = G.seg(hp, max(G.c_up(gs), 0));
+        const double* own = ring + xp * 5 * So;
+        const double* edge = inbox + xp * 5 * L;
+        const double* dsv = B.dqs + 8 * base;
+        const double v = fwd ? row_from_slab<true>(pre, own, p0, np, So, edge, eb, L, dsv, cnt)
+                             : row_from_slab<false>(pre, own, p0, np, So, edge, eb, L, dsv, cnt);
+        ring[x * 5 * So + pre.row * So + (pre.node - t0)] = v;
+        if (need_dn) {
+          const int e0 = G.seg(h, G.c_dn(gs));
+          if (pre.node >= e0 && pre.node < G.seg(h, G.c_dn(gs) + 1)) stage[x * 5 * L + pre.row * L + (pre.node - e0)] = v;
+        }
+        if (fwd)
+          B.dqs[8 * base + pre.row * cnt + pre.node] = v;
+        else
+          B.dq[5 * (base + pre.node) + pre.row] = v;
+      }
+      if (need_dn) slab::fence_to_copies();
       if (__syncthreads_or(fail ? 1 : 0)) {
         if (tid == 0) s_fail = 1;
         break;
       }
       if (tid == 0) {
-        if (G.has_lo()) slab::store_release(at_lo, gs);
-        if (G.has_hi()) slab::store_release(at_hi, gs);
+        if (need_dn) {
+          const unsigned r = (unsigned)G.rank_dn(gs);
+          const unsigned off = (unsigned)(x * 5 * L * sizeof(double));
+          slab::copy_to(slab::map(inbox_l + off, r), stage_l + off, slot_bytes,
+                        slab::map(full_l + (unsigned)(x * sizeof(unsigned long long)), r));
+        }
+        if (G.has_lo()) slab::store_relaxed(at_lo, gs);
+        if (G.has_hi()) slab::store_relaxed(at_hi, gs);
       }
       prefetch(gs + PF);
       preload(gs + 1);
     }
   }
-  __syncthreads();
-  slab::sync();  // no CTA leaves while a neighbour may still store into it
-  if (tid == 0 && s_fail) {
-    if (status) atomicOr(status, (unsigned)ST_TIMEOUT);
-    B.raise(ST_TIMEOUT);
-  }
+  slab::finish(s_fail, ncta, status, B);
 }
 __global__ void __launch_bounds__(512, 1) k_lusgs_sweep_slab(const BlockView* __restrict__ blocks, unsigned* status,
-                                                             int S, int D) {
-  lusgs_slab_body<double>(blocks, status, S, D);
+                                                             int So, int L, int D) {
+  lusgs_slab_body<double>(blocks, status, So, L, D);
 }
 __global__ void __launch_bounds__(512, 1) k_lusgs_sweep_slab_f32(const BlockView* __restrict__ blocks,
-                                                                 unsigned* status, int S, int D) {
-  lusgs_slab_body<float>(blocks, status, S, D);
+                                                                 unsigned* status, int So, int L, int D) {
+  lusgs_slab_body<float>(blocks, status, So, L, D);
 }
 
 // q = q + dq on every updated node (sub_timeadvancement_1stimplicit.f90:568-574).

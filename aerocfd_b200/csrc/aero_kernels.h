@@ -105,7 +105,7 @@ __global__ void k_sa_b_mixed(const BlockView* __restrict__ blocks, CaseConsts cc
 __global__ void k_sa_recs(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_sweep(const BlockView* __restrict__ blocks);
 __global__ void k_sa_sweep_768(const BlockView* __restrict__ blocks);
-__global__ void k_sa_sweep_slab(const BlockView* __restrict__ blocks, unsigned* status, int S, int D);
+__global__ void k_sa_sweep_slab(const BlockView* __restrict__ blocks, unsigned* status, int So, int L, int D);
 __global__ void k_lusgs_sweep_staged(const BlockView* __restrict__ blocks, int nst, unsigned* status,
                                      long spin_limit, int stall_plane);
 __global__ void k_lusgs_sweep_global(const BlockView* __restrict__ blocks, int nst, unsigned* status);
@@ -118,9 +118,10 @@ __global__ void k_lusgs_sweep_cluster_f32(const BlockView* __restrict__ blocks);
 // cluster sweeps exchanging plane values by bulk copies between shared memories
 __global__ void k_lusgs_sweep_bulk(const BlockView* __restrict__ blocks, unsigned* status);
 __global__ void k_lusgs_sweep_bulk_f32(const BlockView* __restrict__ blocks, unsigned* status);
-// cluster sweeps pipelined by k-slabs (ring of D slots of 5 x S values)
-__global__ void k_lusgs_sweep_slab(const BlockView* __restrict__ blocks, unsigned* status, int S, int D);
-__global__ void k_lusgs_sweep_slab_f32(const BlockView* __restrict__ blocks, unsigned* status, int S, int D);
+// cluster sweeps pipelined by k-slabs (D slots: rings of 5 x So values, edge
+// inboxes and staging areas of 5 x L values)
+__global__ void k_lusgs_sweep_slab(const BlockView* __restrict__ blocks, unsigned* status, int So, int L, int D);
+__global__ void k_lusgs_sweep_slab_f32(const BlockView* __restrict__ blocks, unsigned* status, int So, int L, int D);
 __global__ void k_lusgs_update(const BlockView* __restrict__ blocks);
 __global__ void k_physical_bc(const BlockView* __restrict__ blocks, const BcOp* __restrict__ ops,
                               const BcEntry* __restrict__ list, int first, CaseConsts cc);

@@ -81,51 +81,51 @@ std::vector<int> plane_segments(const Box& b1) {
 
 // Shape of the slab sweeps of one block over clusters of `ncta` CTAs: the
 // block's k-offsets 0..nz1-1 split into ce = min(ncta, nz1) slabs, slab r
-// holding [r*nz1/ce, (r+1)*nz1/ce).  width: the most nodes of one plane
-// between the start of the k-segment below a slab and the end of the one
-// above it (a CTA's ring slot); own: the most nodes of one plane inside a
-// slab.
-void slab_shape(const Box& b1, int ncta, int& width, int& own) {
+// holding [r*nz1/ce, (r+1)*nz1/ce).  own: the most nodes of one plane inside
+// a slab; edge: the most nodes of one k-segment of one plane (a slab's edge
+// segment, the values it passes to the next slab).
+void slab_shape(const Box& b1, int ncta, int& own, int& edge) {
   const int nz1 = b1.nz(), H = b1.nx() + b1.ny() + nz1 - 2, SW = nz1 + 2;
   const std::vector<int> seg = plane_segments(b1);
   const int ce = std::max(1, std::min(ncta, nz1));
-  width = own = 0;
-  for (int r = 0; r < ce; ++r) {
-    const int c0 = r * nz1 / ce, c1 = (r + 1) * nz1 / ce;
-    for (int h = 0; h < H; ++h) {
-      const int* s = seg.data() + (size_t)h * SW + 1;  // s[c] for c = -1 .. nz1
-      width = std::max(width, s[std::min(c1 + 1, nz1)] - s[std::max(c0 - 1, 0)]);
-      own = std::max(own, s[c1] - s[c0]);
-    }
+  own = edge = 0;
+  for (int h = 0; h < H; ++h) {
+    const int* s = seg.data() + (size_t)h * SW + 1;  // s[c] for c = -1 .. nz1
+    for (int c = 0; c < nz1; ++c) edge = std::max(edge, s[c + 1] - s[c]);
+    for (int r = 0; r < ce; ++r) own = std::max(own, s[(r + 1) * nz1 / ce] - s[r * nz1 / ce]);
   }
 }
 
 // Launch shape of a slab sweep (k_lusgs_sweep_slab: `rows` = 5 rows per node;
-// k_sa_sweep_slab: 1) over clusters of ncta CTAs for a set of blocks: ring
-// slot width S, threads T (one per row of a slab's plane) and ring depth D
-// (up to 8 planes in 200 KB of shared memory).  ok is false when a slab's
-// plane needs more than 512 threads or fewer than two planes fit.
+// k_sa_sweep_slab: 1) over clusters of ncta CTAs for a set of blocks: So
+// values per row of a ring slot, L per row of an edge slot (even, so every
+// copied slot is a multiple of 16 bytes), threads T (one per row of a slab's
+// plane) and slots D (up to kSlabSlots in 200 KB of shared memory).  ok is
+// false when a slab's plane needs more than 512 threads or fewer than two
+// slots fit.
 struct SlabFit {
   bool ok = false;
-  int S = 0, T = 0, D = 0;
+  int So = 0, L = 0, T = 0, D = 0;
 };
 SlabFit slab_fit(const BlockView* hv, int nblk, int ncta, int rows) {
   SlabFit f;
-  int width = 0, own = 0;
+  int own = 0, edge = 0;
   for (int m = 0; m < nblk; ++m) {
-    int w = 0, o = 0;
-    slab_shape(hv[m].b1, ncta, w, o);
-    width = std::max(width, w);
+    int o = 0, e = 0;
+    slab_shape(hv[m].b1, ncta, o, e);
     own = std::max(own, o);
+    edge = std::max(edge, e);
   }
-  if (rows * own > 512 || width <= 0) return f;
-  f.S = width;
+  if (rows * own > 512 || own <= 0) return f;
+  f.So = own;
+  f.L = (edge + 1) & ~1;
   f.T = std::max(64, (rows * own + 31) / 32 * 32);
-  const size_t slot = (size_t)rows * f.S * sizeof(double);
-  f.D = (int)std::min<size_t>(8, (size_t)(200 * 1024) / slot);
+  const size_t slot = (size_t)rows * (f.So + 2 * f.L) * sizeof(double);
+  f.D = (int)std::min<size_t>(kSlabSlots, (size_t)(200 * 1024) / slot);
   f.ok = f.D >= 2;
   return f;
 }
+size_t slab_smem(const SlabFit& f, int rows) { return (size_t)f.D * rows * (f.So + 2 * f.L) * sizeof(double); }
 
 // slab_fit of the registered blocks (hv null; cached per setup) or of the
 // nblk host views hv.
@@ -766,11 +766,12 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
   if (slabbed) {
     // one cluster per block, each CTA one k-slab, pipelined plane by plane
     const int cl = g.tune.sweep_cl;
-    const size_t smem = (size_t)sf.D * 5 * sf.S * sizeof(double);
+    const size_t smem = slab_smem(sf, 5);
     auto kern = f ? k_lusgs_sweep_slab_f32 : k_lusgs_sweep_slab;
     if ((rc = prepare_slab(kern, f, smem, cl))) return rc;
     cudaError_t le = cudaSuccess;
-    PROF(P_LUSGS_SWEEP, (le = launch_clusters(kern, nblk, cl, sf.T, smem, g.stream, sv, g.d_status, sf.S, sf.D)));
+    PROF(P_LUSGS_SWEEP,
+         (le = launch_clusters(kern, nblk, cl, sf.T, smem, g.stream, sv, g.d_status, sf.So, sf.L, sf.D)));
     CK(le);
   } else if (bulk) {
     // one cluster per block, one thread per row of every node of the largest
@@ -872,12 +873,12 @@ int launch_sa(const BlockView* views, int nblk, long maxN, long maxN1, int pmax,
   if (g.tune.sa_cl >= 2 && (sf = slab_fit_for(host_views, nblk, g.tune.sa_cl, 1)).ok) {
     // one cluster per block, each CTA one k-slab, pipelined plane by plane
     const int cl = g.tune.sa_cl;
-    const size_t smem = (size_t)sf.D * sf.S * sizeof(double);
+    const size_t smem = slab_smem(sf, 1);
     int rc = prepare_slab(k_sa_sweep_slab, 2, smem, cl);
     if (rc) return rc;
     cudaError_t le = cudaSuccess;
     PROF_ON(P_SA_SWEEP, st, (le = launch_clusters(k_sa_sweep_slab, nblk, cl, sf.T, smem, st, views, g.d_status,
-                                                  sf.S, sf.D)));
+                                                  sf.So, sf.L, sf.D)));
     CK(le);
     return AERO_OK;
   }
@@ -1337,11 +1338,11 @@ bool slab_cluster16_fits(int rows) {
   if (!g.setup) return false;
   const SlabFit sf = slab_fit_for(nullptr, 0, 16, rows);
   if (!sf.ok) return false;
-  const size_t smem = (size_t)sf.D * rows * sf.S * sizeof(double);
+  const size_t smem = slab_smem(sf, rows);
   const int nk = rows == 5 ? 2 : 1;
   for (int k = 0; k < nk; ++k) {
     const int idx = rows == 5 ? k : 2;
-    void (*kern)(const BlockView*, unsigned*, int, int) =
+    void (*kern)(const BlockView*, unsigned*, int, int, int) =
         rows == 5 ? (k ? k_lusgs_sweep_slab_f32 : k_lusgs_sweep_slab) : k_sa_sweep_slab;
     if (prepare_slab(kern, idx, smem, 16) != AERO_OK) {
       cudaGetLastError();

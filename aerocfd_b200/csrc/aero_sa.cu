@@ -440,15 +440,20 @@ __global__ void __launch_bounds__(768) k_sa_sweep_768(const BlockView* __restric
 
 // The SA sweeps pipelined over a cluster of CTAs by k-slabs, as
 // k_lusgs_sweep_slab pipelines the mean-flow sweeps (slab::Geom: CTA r owns
-// the nodes of one range of k-offsets; the CTA upstream of the pass stores the
-// values of its edge k-segment into this CTA's ring and publishes its step
-// with a release store; every wait is bounded, and the final cluster barrier
-// keeps every CTA resident until no neighbour can still store into it).  One
-// node per thread; the ring holds D planes of S values.  The arithmetic per
-// node is sa_sweep_body's, so the result is the same to the bit.
+// the nodes of one range of k-offsets; after each plane a CTA copies its edge
+// k-segment's values into the downstream CTA's inbox with one bulk copy,
+// counted on that CTA's mbarrier; relaxed progress counters keep the D-plane
+// slots from being overwritten while in use; every wait is bounded, and
+// slab::finish keeps every CTA resident until no copy can still land in it).
+// One node per thread.  The arithmetic per node is sa_sweep_body's, so the
+// result is the same to the bit.
 __global__ void __launch_bounds__(512, 1) k_sa_sweep_slab(const BlockView* __restrict__ blocks, unsigned* status,
-                                                          int S, int D) {
-  extern __shared__ __align__(16) double sring[];  // D slots x S
+                                                          int So, int L, int D) {
+  extern __shared__ __align__(16) double sdyn[];
+  double* stage = sdyn;            // D x L: this slab's edge values, copied downstream
+  double* inbox = stage + D * L;   // D x L: the upstream slab's edge values
+  double* ring = inbox + D * L;    // D x So: this slab's values
+  __shared__ __align__(8) unsigned long long full[kSlabSlots];
   __shared__ int s_prog[2];  // last step completed by the CTA below / above
   __shared__ int s_fail;
   const int ncta = (int)slab::size();
@@ -460,14 +465,15 @@ __global__ void __launch_bounds__(512, 1) k_sa_sweep_slab(const BlockView* __res
     s_prog[0] = -1;
     s_prog[1] = -1;
     s_fail = 0;
+    for (int x = 0; x < D; ++x) slab::bar_init(&full[x], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  slab::sync();  // every CTA's counters are set before a neighbour writes them
+  slab::sync();  // every CTA's counters and mbarriers exist before a neighbour touches them
+  const unsigned slot_bytes = (unsigned)(L * sizeof(double));
   if (G.active()) {
-    const unsigned ring_l = slab::local(sring);
     const unsigned at_lo = G.has_lo() ? slab::map(slab::local(&s_prog[1]), G.me - 1) : 0u;
     const unsigned at_hi = G.has_hi() ? slab::map(slab::local(&s_prog[0]), G.me + 1) : 0u;
-    const unsigned ring_lo = G.has_lo() ? slab::map(ring_l, G.me - 1) : 0u;
-    const unsigned ring_hi = G.has_hi() ? slab::map(ring_l, G.me + 1) : 0u;
+    const unsigned inbox_l = slab::local(inbox), full_l = slab::local(full), stage_l = slab::local(stage);
     SaFwd pre_f{};
     SaBwd pre_b{};
     auto preload = [&](int gs) {
@@ -501,65 +507,76 @@ __global__ void __launch_bounds__(512, 1) k_sa_sweep_slab(const BlockView* __res
     constexpr int PF = 3;  // prefetch distance in steps
     for (int gs = 0; gs < PF; ++gs) prefetch(gs);
     preload(0);
+    unsigned parity = 0;  // bit x: parity of the next phase of full[x] to wait for
     for (int gs = 0; gs < 2 * H; ++gs) {
       const bool fwd = gs < H;
       const int h = G.plane(gs);
       const long base = B.poff[h];
       const int t0 = G.seg(h, G.c0), n = G.seg(h, G.c1) - t0;
       const bool need_dn = G.need_dn(gs);
+      const int x = gs % D, xp = (gs + D - 1) % D;
       bool fail = false;
-      if (G.need_up(gs)) fail = !slab::wait_for(&s_prog[fwd ? 0 : 1], gs - 1, 1L << 20);
+      if (G.need_up(gs)) {
+        if (tid == 0) slab::bar_expect(&full[xp], slot_bytes);
+        fail = !slab::bar_wait(&full[xp], (parity >> xp) & 1u, 1L << 20);
+        parity ^= 1u << xp;
+      }
       if (!fail && need_dn) fail = !slab::wait_for(&s_prog[fwd ? 1 : 0], gs - D + 1, 1L << 20);
-      if (!fail) {
-        double* cur = sring + (gs % D) * S;
-        const double* prev = sring + ((gs + D - 1) % D) * S;
-        const int wlc = G.wl(h, G.me);
-        const int wlp = gs > 0 ? G.wl(G.plane(gs - 1), G.me) : 0;
-        const int e0 = need_dn ? G.seg(h, G.c_dn(gs)) : 0, e1 = need_dn ? G.seg(h, G.c_dn(gs) + 1) : 0;
-        const int wld = need_dn ? G.wl(h, G.rank_dn(gs)) : 0;
-        const unsigned slot_dn = (fwd ? ring_hi : ring_lo) + (unsigned)((gs % D) * S * 8);
-        if (tid < n) {  // the launch gives every node of a slab's plane a thread
-          const int t = t0 + tid;
-          double tt[3], v;
-          if (fwd) {
+      if (!fail && tid < n) {  // the launch gives every node of a slab's plane a thread
+        const int hp = G.plane(gs > 0 ? gs - 1 : 0);
+        const int p0 = G.seg(hp, G.c0), np = G.seg(hp, G.c1) - p0;
+        const int eb = G.seg(hp, max(G.c_up(gs), 0));
+        const double* own = ring + xp * So;
+        const double* edge = inbox + xp * L;
+        auto prev = [&](int w, int d) {
+          // the i and j neighbours share the node's k-offset, so they are the slab's own
+          return (d < 2 || (unsigned)(w - p0) < (unsigned)np) ? own[w - p0] : edge[w - eb];
+        };
+        const int t = t0 + tid;
+        double tt[3], v;
+        if (fwd) {
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-              const int w = nbr_local(pre_f.packed, d);
-              tt[d] = w < 0 ? 0.0 : pre_f.a[d] * prev[w - wlp];
-            }
-            v = div_rn_lean(pre_f.rhs + (tt[0] + tt[1] + tt[2]), pre_f.diag, pre_f.rdiag);
-            B.sa_dq[base + t] = v;
-          } else {
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-              const int w = nbr_local(pre_b.packed, d);
-              tt[d] = w < 0 ? 0.0 : pre_b.b[d] * prev[w - wlp];
-            }
-            v = pre_b.dqs - div_rn_lean(tt[0] + tt[1] + tt[2], pre_b.diag, pre_b.rdiag);
-            B.s(F_NUT, pre_b.nat) = pre_b.nut + v;
+          for (int d = 0; d < 3; ++d) {
+            const int w = nbr_local(pre_f.packed, d);
+            tt[d] = w < 0 ? 0.0 : pre_f.a[d] * prev(w, d);
           }
-          cur[t - wlc] = v;
-          if (t >= e0 && t < e1) slab::store_f64(slot_dn + (unsigned)((t - wld) * 8), v);
+          v = div_rn_lean(pre_f.rhs + (tt[0] + tt[1] + tt[2]), pre_f.diag, pre_f.rdiag);
+          B.sa_dq[base + t] = v;
+        } else {
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            const int w = nbr_local(pre_b.packed, d);
+            tt[d] = w < 0 ? 0.0 : pre_b.b[d] * prev(w, d);
+          }
+          v = pre_b.dqs - div_rn_lean(tt[0] + tt[1] + tt[2], pre_b.diag, pre_b.rdiag);
+          B.s(F_NUT, pre_b.nat) = pre_b.nut + v;
+        }
+        ring[x * So + tid] = v;
+        if (need_dn) {
+          const int e0 = G.seg(h, G.c_dn(gs));
+          if (t >= e0 && t < G.seg(h, G.c_dn(gs) + 1)) stage[x * L + (t - e0)] = v;
         }
       }
+      if (need_dn) slab::fence_to_copies();
       if (__syncthreads_or(fail ? 1 : 0)) {
         if (tid == 0) s_fail = 1;
         break;
       }
       if (tid == 0) {
-        if (G.has_lo()) slab::store_release(at_lo, gs);
-        if (G.has_hi()) slab::store_release(at_hi, gs);
+        if (need_dn) {
+          const unsigned r = (unsigned)G.rank_dn(gs);
+          const unsigned off = (unsigned)(x * L * sizeof(double));
+          slab::copy_to(slab::map(inbox_l + off, r), stage_l + off, slot_bytes,
+                        slab::map(full_l + (unsigned)(x * sizeof(unsigned long long)), r));
+        }
+        if (G.has_lo()) slab::store_relaxed(at_lo, gs);
+        if (G.has_hi()) slab::store_relaxed(at_hi, gs);
       }
       prefetch(gs + PF);
       preload(gs + 1);
     }
   }
-  __syncthreads();
-  slab::sync();  // no CTA leaves while a neighbour may still store into it
-  if (tid == 0 && s_fail) {
-    if (status) atomicOr(status, (unsigned)ST_TIMEOUT);
-    B.raise(ST_TIMEOUT);
-  }
+  slab::finish(s_fail, ncta, status, B);
 }
 
 // length = dist over the full box (sub_tur_sa.f90:51-57; no DES).
