@@ -1334,30 +1334,20 @@ __device__ __forceinline__ void lusgs_slab_body(const BlockView* __restrict__ bl
         load_node_row(recs<R>(B, fwd) + W * base, B.sca + kSca * base, cnt, row, t0 + tid - row * n, pre);
       }
     };
-    // L2 prefetch, by warp 1, of the slab's part of step gs's chunks: every
-    // record entry, the packed neighbours, the scalars and (backward) dq*,
-    // each a run of n values inside its plane's chunk (chunks start and end
-    // on 16-byte boundaries, so the widened runs stay inside them)
+    // L2 prefetch of step gs's whole chunks (records, scalars and, backward,
+    // dq*) by the pass's leading CTA (the one without an upstream slab: every
+    // other CTA reaches each step after it), one lane per chunk; the chunks
+    // start and end on 16-byte boundaries
+    const bool lead_f = G.me == 0, lead_b = G.me == G.ce - 1;
     auto prefetch = [&](int gs) {
-      if (gs >= 2 * H || (tid >> 5) != 1) return;
+      if (gs >= 2 * H || tid >= 35 || tid < 32) return;
       const bool fwd = gs < H;
-      const int h = G.plane(gs);
-      const long base = poff[h];
-      const int cnt = (int)(poff[h + 1] - base);
-      const int t0 = G.seg(h, G.c0), n = G.seg(h, G.c1) - t0;
-      if (n <= 0) return;
-      const R* rec = recs<R>(B, fwd) + W * base;
-      const int nrun = 76 + kSca + (fwd ? 0 : 5);
-      for (int x = (tid & 31); x < nrun; x += 32) {
-        if (x < 75)
-          slab::prefetch_span(rec + (long)x * cnt + t0, (long)n * (long)sizeof(R));
-        else if (x == 75)
-          slab::prefetch_span(RecFmt<R>::packed_ptr(rec, cnt) + t0, 8L * n);
-        else if (x < 76 + kSca)
-          slab::prefetch_span(B.sca + kSca * base + (long)(x - 76) * cnt + t0, 8L * n);
-        else
-          slab::prefetch_span(B.dqs + 8 * base + (long)(x - 76 - kSca) * cnt + t0, 8L * n);
-      }
+      if (!(fwd ? lead_f : lead_b)) return;
+      const long base = poff[G.plane(gs)];
+      const long cnt = poff[G.plane(gs) + 1] - base;
+      if (tid == 32) slab::prefetch_span(recs<R>(B, fwd) + W * base, (long)W * (long)sizeof(R) * cnt);
+      if (tid == 33) slab::prefetch_span(B.sca + kSca * base, 8L * kSca * cnt);
+      if (tid == 34 && !fwd) slab::prefetch_span(B.dqs + 8 * base, 64L * cnt);
     };
     constexpr int PF = 3;  // prefetch distance in steps
     for (int gs = 0; gs < PF; ++gs) prefetch(gs);

@@ -487,22 +487,19 @@ __global__ void __launch_bounds__(512, 1) k_sa_sweep_slab(const BlockView* __res
           sa_load_bwd(B, h, t0 + tid, pre_b);
       }
     };
-    // L2 prefetch, by warp 1, of the slab's runs of step gs's records and
-    // (backward) of sa_dq and the natural indices
+    // L2 prefetch of step gs's whole chunks (records and, backward, sa_dq and
+    // the natural indices) by the pass's leading CTA (the one without an
+    // upstream slab: every other CTA reaches each step after it)
+    const bool lead_f = G.me == 0, lead_b = G.me == G.ce - 1;
     auto prefetch = [&](int gs) {
-      if (gs >= 2 * H || (tid >> 5) != 1) return;
-      const int h = G.plane(gs);
-      const long base = B.poff[h];
-      const int cnt = (int)(B.poff[h + 1] - base);
-      const int t0 = G.seg(h, G.c0), n = G.seg(h, G.c1) - t0;
-      if (n <= 0) return;
-      const int x = tid & 31;
-      if (x < kSaRec)
-        slab::prefetch_span(B.sa_rec + kSaRec * base + (long)x * cnt + t0, 8L * n);
-      else if (x == kSaRec && gs >= H)
-        slab::prefetch_span(B.sa_dq + base + t0, 8L * n);
-      else if (x == kSaRec + 1 && gs >= H)
-        slab::prefetch_span(B.nat + base + t0, 8L * n);
+      if (gs >= 2 * H || tid >= 35 || tid < 32) return;
+      const bool fwd = gs < H;
+      if (!(fwd ? lead_f : lead_b)) return;
+      const long base = B.poff[G.plane(gs)];
+      const long cnt = B.poff[G.plane(gs) + 1] - base;
+      if (tid == 32) slab::prefetch_span(B.sa_rec + kSaRec * base, 8L * kSaRec * cnt);
+      if (tid == 33 && !fwd) slab::prefetch_span(B.sa_dq + base, 8L * cnt);
+      if (tid == 34 && !fwd) slab::prefetch_span(B.nat + base, 8L * cnt);
     };
     constexpr int PF = 3;  // prefetch distance in steps
     for (int gs = 0; gs < PF; ++gs) prefetch(gs);
