@@ -42,25 +42,32 @@ __global__ void k_getpri(const BlockView* __restrict__ blocks, CaseConsts cc_lau
 
 // -------------------------------------------------------------- inviscid flux
 // WENO3 weights and state (sub_inviscid_upwind.f90:32-41 right, :57-66 left).
-__device__ __forceinline__ double weno_right(double u1, double u2, double u3) {
+// The reference's four divisions per state are formed with fewer: the
+// smoothness weight of a difference d, 1 / (3 (eps + d^2)^2), is one
+// reciprocal (correctly rounded, as 1.0 / x), the reference's 2 / x is twice
+// it (exact: scaling by 2 commutes with rounding for these normal values,
+// x >= 3e-12), and the two normalisations w = a / (a1 + a2) share the
+// reciprocal of the sum through div_rn_lean, which equals the quotient to
+// the bit.  (d^2 is the same for d and -d, so weno_faces' shared weights are
+// the reference's s1 / s2 of either state.)
+__device__ __forceinline__ double weno_weight(double d) {
   const double eps = 1.0e-6;
-  double s1 = p2(u2 - u3);
-  double s2 = p2(u1 - u2);
-  double a1 = 1.0 / (3.0 * p2(eps + s1));
-  double a2 = 2.0 / (3.0 * p2(eps + s2));
-  double w1 = a1 / (a1 + a2);
-  double w2 = a2 / (a1 + a2);
-  return w1 * (-u3 / 2.0 + 3.0 * u2 / 2.0) + w2 * (u2 / 2.0 + u1 / 2.0);
+  return 1.0 / (3.0 * p2(eps + p2(d)));
+}
+// w1 (c1) + w2 (c2) with w = a / (a1 + a2)
+__device__ __forceinline__ double weno_mix(double a1, double a2, double c1, double c2) {
+  const double sum = a1 + a2, rs = 1.0 / sum;
+  return div_rn_lean(a1, sum, rs) * c1 + div_rn_lean(a2, sum, rs) * c2;
+}
+__device__ __forceinline__ double weno_right(double u1, double u2, double u3) {
+  const double a1 = weno_weight(u2 - u3);
+  const double a2 = 2.0 * weno_weight(u1 - u2);
+  return weno_mix(a1, a2, -u3 / 2.0 + 3.0 * u2 / 2.0, u2 / 2.0 + u1 / 2.0);
 }
 __device__ __forceinline__ double weno_left(double u1, double u2, double u3) {
-  const double eps = 1.0e-6;
-  double s1 = p2(u2 - u1);
-  double s2 = p2(u3 - u2);
-  double a1 = 1.0 / (3.0 * p2(eps + s1));
-  double a2 = 2.0 / (3.0 * p2(eps + s2));
-  double w1 = a1 / (a1 + a2);
-  double w2 = a2 / (a1 + a2);
-  return w1 * (-u1 / 2.0 + 3.0 * u2 / 2.0) + w2 * (u2 / 2.0 + u3 / 2.0);
+  const double a1 = weno_weight(u2 - u1);
+  const double a2 = 2.0 * weno_weight(u3 - u2);
+  return weno_mix(a1, a2, -u1 / 2.0 + 3.0 * u2 / 2.0, u2 / 2.0 + u3 / 2.0);
 }
 
 // Roe flux at face (node n, node n+s) along `coord` from primitive left/right
@@ -73,14 +80,18 @@ __device__ __forceinline__ void roe_prim(const BlockView& B, int coord, long n, 
   double dxidx1 = 0.5 * (B.v(F_DXIDX, c1, n) * ja + B.v(F_DXIDX, c1, ns) * jb);
   double dxidy1 = 0.5 * (B.v(F_DXIDX, c1 + 1, n) * ja + B.v(F_DXIDX, c1 + 1, ns) * jb);
   double dxidz1 = 0.5 * (B.v(F_DXIDX, c1 + 2, n) * ja + B.v(F_DXIDX, c1 + 2, ns) * jb);
+  // the divisions that share a divisor go through its reciprocal and
+  // div_rn_lean (each quotient the same to the bit)
   double temp = sqrt(p2(dxidx1) + p2(dxidy1) + p2(dxidz1));
-  double dxidx0 = dxidx1 / temp, dxidy0 = dxidy1 / temp, dxidz0 = dxidz1 / temp;
+  const double rtemp = 1.0 / temp;
+  double dxidx0 = div_rn_lean(dxidx1, temp, rtemp), dxidy0 = div_rn_lean(dxidy1, temp, rtemp);
+  double dxidz0 = div_rn_lean(dxidz1, temp, rtemp);
 
   double hl = gamma * pl / ((gamma - 1.0) * dl) + 0.5 * (p2(ul) + p2(vl) + p2(wl));
   double hr = gamma * pr / ((gamma - 1.0) * dr) + 0.5 * (p2(ur) + p2(vr) + p2(wr));
   double uul = ul * dxidx1 + vl * dxidy1 + wl * dxidz1;
   double uur = ur * dxidx1 + vr * dxidy1 + wr * dxidz1;
-  double ubarl = uul / temp, ubarr = uur / temp;
+  double ubarl = div_rn_lean(uul, temp, rtemp), ubarr = div_rn_lean(uur, temp, rtemp);
 
   double fl0 = dl * uul, fl1 = dl * ul * uul + dxidx1 * pl, fl2 = dl * vl * uul + dxidy1 * pl;
   double fl3 = dl * wl * uul + dxidz1 * pl, fl4 = dl * hl * uul;
@@ -89,29 +100,34 @@ __device__ __forceinline__ void roe_prim(const BlockView& B, int coord, long n, 
 
   double tmpp = sqrt(dr / dl);
   double avd = sqrt(dl * dr);
-  double avu = (ul + ur * tmpp) / (1.0 + tmpp);
-  double avv = (vl + vr * tmpp) / (1.0 + tmpp);
-  double avw = (wl + wr * tmpp) / (1.0 + tmpp);
-  double avh = (hl + hr * tmpp) / (1.0 + tmpp);
+  const double op = 1.0 + tmpp, rop = 1.0 / op;
+  double avu = div_rn_lean(ul + ur * tmpp, op, rop);
+  double avv = div_rn_lean(vl + vr * tmpp, op, rop);
+  double avw = div_rn_lean(wl + wr * tmpp, op, rop);
+  double avh = div_rn_lean(hl + hr * tmpp, op, rop);
   double ava = sqrt((gamma - 1.0) * (avh - 0.5 * (p2(avu) + p2(avv) + p2(avw))));
   double avuu = avu * dxidx0 + avv * dxidy0 + avw * dxidz0;
 
   const double delt = 0.06;
+  constexpr double kTwoDelt = 2.0 * 0.06, kRcpTwoDelt = 1.0 / (2.0 * 0.06);
   double lam[5] = {fabs(avuu - ava), fabs(avuu), fabs(avuu), fabs(avuu), fabs(avuu + ava)};
 #pragma unroll
   for (int m = 0; m < 5; ++m) {  // Harten entropy fix (sub_inviscid_splitting.f90:122-130)
     double tmp = copysign(1.0, delt - lam[m]);
     double tmp1 = 0.5 * (1.0 - tmp);
     double tmp2 = 0.5 * (1.0 + tmp);
-    double harten = (p2(lam[m]) + p2(delt)) / (2.0 * delt);
+    double harten = div_rn_lean(p2(lam[m]) + p2(delt), kTwoDelt, kRcpTwoDelt);
     lam[m] = tmp1 * lam[m] + tmp2 * harten;
   }
   double deltad = dr - dl, deltap = pr - pl;
   double deltau = ur - ul, deltav = vr - vl, deltaw = wr - wl;
   double deltauu = ubarr - ubarl;
-  double alpha1 = lam[1] * (deltad - deltap / p2(ava));
-  double alpha2 = lam[4] * (deltap + avd * ava * deltauu) / (2.0 * p2(ava));
-  double alpha3 = lam[0] * (deltap - avd * ava * deltauu) / (2.0 * p2(ava));
+  // p2(ava) and 2 p2(ava) (exactly twice it, so 1/(2 p2(ava)) is exactly half
+  // of 1/p2(ava)) as divisors
+  const double ava2 = p2(ava), rava2 = 1.0 / ava2;
+  double alpha1 = lam[1] * (deltad - div_rn_lean(deltap, ava2, rava2));
+  double alpha2 = div_rn_lean(lam[4] * (deltap + avd * ava * deltauu), 2.0 * ava2, 0.5 * rava2);
+  double alpha3 = div_rn_lean(lam[0] * (deltap - avd * ava * deltauu), 2.0 * ava2, 0.5 * rava2);
   double alpha4 = alpha1 + alpha2 + alpha3;
   double alpha5 = ava * (alpha2 - alpha3);
   double alpha6 = lam[1] * (avd * deltau - avd * deltauu * dxidx0);
@@ -134,10 +150,14 @@ __device__ __forceinline__ void roe_prim(const BlockView& B, int coord, long n, 
 __device__ __forceinline__ void roe_face(const BlockView& B, int coord, long n, long ns,
                                          const double ulc[5], const double urc[5], double gamma,
                                          double flux[5]) {
-  double dl = ulc[0], ul = ulc[1] / ulc[0], vl = ulc[2] / ulc[0], wl = ulc[3] / ulc[0];
-  double pl = (ulc[4] - 0.5 * (p2(ulc[1]) + p2(ulc[2]) + p2(ulc[3])) / ulc[0]) * (gamma - 1.0);
-  double dr = urc[0], ur = urc[1] / urc[0], vr = urc[2] / urc[0], wr = urc[3] / urc[0];
-  double pr = (urc[4] - 0.5 * (p2(urc[1]) + p2(urc[2]) + p2(urc[3])) / urc[0]) * (gamma - 1.0);
+  // the four divisions by the density of each side through its reciprocal
+  const double rl = 1.0 / ulc[0], rr = 1.0 / urc[0];
+  double dl = ulc[0], ul = div_rn_lean(ulc[1], dl, rl), vl = div_rn_lean(ulc[2], dl, rl);
+  double wl = div_rn_lean(ulc[3], dl, rl);
+  double pl = (ulc[4] - div_rn_lean(0.5 * (p2(ulc[1]) + p2(ulc[2]) + p2(ulc[3])), dl, rl)) * (gamma - 1.0);
+  double dr = urc[0], ur = div_rn_lean(urc[1], dr, rr), vr = div_rn_lean(urc[2], dr, rr);
+  double wr = div_rn_lean(urc[3], dr, rr);
+  double pr = (urc[4] - div_rn_lean(0.5 * (p2(urc[1]) + p2(urc[2]) + p2(urc[3])), dr, rr)) * (gamma - 1.0);
   roe_prim(B, coord, n, ns, dl, ul, vl, wl, pl, dr, ur, vr, wr, pr, gamma, flux);
 }
 
@@ -153,17 +173,20 @@ __device__ __forceinline__ void face_flux(const BlockView& B, int coord, long n,
   for (int c = 1; c <= 5; ++c) {
     double f0 = B.v(F_Q, c, n);
     double fp = B.v(F_Q, c, n + st);
+    // the weight of the face's own difference serves both states (the
+    // reference's s2 of each)
+    const double a_mid = (rone && lone) ? 0.0 : weno_weight(fp - f0);
     if (rone) {
       urc[c - 1] = fp;
     } else {
       double fpp = B.v(F_Q, c, n + 2 * st);
-      urc[c - 1] = weno_right(f0, fp, fpp);
+      urc[c - 1] = weno_mix(weno_weight(fp - fpp), 2.0 * a_mid, -fpp / 2.0 + 3.0 * fp / 2.0, fp / 2.0 + f0 / 2.0);
     }
     if (lone) {
       ulc[c - 1] = f0;
     } else {
       double fm = B.v(F_Q, c, n - st);
-      ulc[c - 1] = weno_left(fm, f0, fp);
+      ulc[c - 1] = weno_mix(weno_weight(f0 - fm), 2.0 * a_mid, -fm / 2.0 + 3.0 * f0 / 2.0, f0 / 2.0 + fp / 2.0);
     }
   }
   roe_face(B, coord, n, n + st, ulc, urc, gamma, flux);

@@ -236,9 +236,12 @@ __device__ __forceinline__ void lusgs_mats_body(const BlockView* __restrict__ bl
   const double mw0 = B.v(F_Q, 4, n), e0 = B.v(F_Q, 5, n);
   const double dxidx = B.v(F_DXIDX, cb, n), dxidy = B.v(F_DXIDX, cb + 1, n), dxidz = B.v(F_DXIDX, cb + 2, n);
   const double a2 = gamma - 1.0, a3 = gamma - 2.0;
-  const double uu = (dxidx * mu0 + dxidy * mv0 + dxidz * mw0) / rho;
+  // every division by rho through its reciprocal (div_rn_lean: the same bits)
+  const double rrho = 1.0 / rho;
+  auto dv = [&](double x) { return div_rn_lean(x, rho, rrho); };
+  const double uu = dv(dxidx * mu0 + dxidy * mv0 + dxidz * mw0);
   const double phi = 0.5 * a2 * (p2(mu0) + p2(mv0) + p2(mw0)) / p2(rho);
-  const double a1 = gamma * e0 / rho - phi;
+  const double a1 = dv(gamma * e0) - phi;
   const double rad = B.s(d == 0 ? F_RA : (d == 1 ? F_RB : F_RC), n);
   const double invj = B.s(F_INVJ, n);
   R* dup = nullptr;
@@ -263,25 +266,25 @@ __device__ __forceinline__ void lusgs_mats_body(const BlockView* __restrict__ bl
       case 2: a = dxidy; break;
       case 3: a = dxidz; break;
       case 4: a = 0.0; break;
-      case 5: a = phi * dxidx - uu * mu0 / rho; break;
-      case 6: a = uu - a3 * dxidx * mu0 / rho; break;
-      case 7: a = dxidy * mu0 / rho - a2 * dxidx * mv0 / rho; break;
-      case 8: a = dxidz * mu0 / rho - a2 * dxidx * mw0 / rho; break;
+      case 5: a = phi * dxidx - dv(uu * mu0); break;
+      case 6: a = uu - dv(a3 * dxidx * mu0); break;
+      case 7: a = dv(dxidy * mu0) - dv(a2 * dxidx * mv0); break;
+      case 8: a = dv(dxidz * mu0) - dv(a2 * dxidx * mw0); break;
       case 9: a = a2 * dxidx; break;
-      case 10: a = phi * dxidy - uu * mv0 / rho; break;
-      case 11: a = dxidx * mv0 / rho - a2 * dxidy * mu0 / rho; break;
-      case 12: a = uu - a3 * dxidy * mv0 / rho; break;
-      case 13: a = dxidz * mv0 / rho - a2 * dxidy * mw0 / rho; break;
+      case 10: a = phi * dxidy - dv(uu * mv0); break;
+      case 11: a = dv(dxidx * mv0) - dv(a2 * dxidy * mu0); break;
+      case 12: a = uu - dv(a3 * dxidy * mv0); break;
+      case 13: a = dv(dxidz * mv0) - dv(a2 * dxidy * mw0); break;
       case 14: a = a2 * dxidy; break;
-      case 15: a = phi * dxidz - uu * mw0 / rho; break;
-      case 16: a = dxidx * mw0 / rho - a2 * dxidz * mu0 / rho; break;
-      case 17: a = dxidy * mw0 / rho - a2 * dxidz * mv0 / rho; break;
-      case 18: a = uu - a3 * dxidz * mw0 / rho; break;
+      case 15: a = phi * dxidz - dv(uu * mw0); break;
+      case 16: a = dv(dxidx * mw0) - dv(a2 * dxidz * mu0); break;
+      case 17: a = dv(dxidy * mw0) - dv(a2 * dxidz * mv0); break;
+      case 18: a = uu - dv(a3 * dxidz * mw0); break;
       case 19: a = a2 * dxidz; break;
       case 20: a = (phi - a1) * uu; break;
-      case 21: a = a1 * dxidx - a2 * uu * mu0 / rho; break;
-      case 22: a = a1 * dxidy - a2 * uu * mv0 / rho; break;
-      case 23: a = a1 * dxidz - a2 * uu * mw0 / rho; break;
+      case 21: a = a1 * dxidx - dv(a2 * uu * mu0); break;
+      case 22: a = a1 * dxidy - dv(a2 * uu * mv0); break;
+      case 23: a = a1 * dxidz - dv(a2 * uu * mw0); break;
       default: a = gamma * uu; break;
     }
     if (dup) {
@@ -1207,10 +1210,18 @@ __global__ void __launch_bounds__(512, 1) k_lusgs_sweep_bulk_f32(const BlockView
 // ------------------------------------------------------------ slab sweeps
 namespace {
 
-// The records of row `row` of plane-local node `node` (cnt nodes in the plane).
+// What one row of one node of a slab sweep reads besides the previous plane:
+// its records, scalars and (backward) dq*.
+struct SlabRow {
+  double packed, m[15], rhs, diag, invj, rdiag, rinvj, dsv;
+  int row, node;
+  bool bok;  // divisors in div2_rn's fast range
+};
 template <typename R>
-__device__ __forceinline__ void load_node_row(const R* rec, const double* sca, int cnt, int row, int node,
-                                              RowRecs& r) {
+__device__ __forceinline__ void load_slab_row(const BlockView& B, bool fwd, long base, int cnt, int row, int node,
+                                              SlabRow& r) {
+  constexpr int W = RecFmt<R>::kWords;
+  const R* rec = recs<R>(B, fwd) + W * base;
   r.row = row;
   r.node = node;
   const R* rn = rec + node;
@@ -1219,12 +1230,14 @@ __device__ __forceinline__ void load_node_row(const R* rec, const double* sca, i
   for (int d = 0; d < 3; ++d)
 #pragma unroll
     for (int c = 0; c < 5; ++c) r.m[5 * d + c] = (double)rn[(25 * d + 5 * row + c) * cnt];
-  const double* sn = sca + node;
+  const double* sn = B.sca + kSca * base + node;
   r.rhs = sn[row * cnt];
   r.diag = sn[5 * cnt];
   r.invj = sn[6 * cnt];
   r.rdiag = sn[7 * cnt];
   r.rinvj = sn[8 * cnt];
+  // dq* of the node, written by this CTA in the forward pass (read from L2)
+  r.dsv = fwd ? 0.0 : __ldcg(B.dqs + 8 * base + row * cnt + node);
   r.bok = !nbr_slow_div(r.packed);
 }
 // lusgs_rows' arithmetic for one row from preloaded records.  The previous
@@ -1232,8 +1245,8 @@ __device__ __forceinline__ void load_node_row(const R* rec, const double* sca, i
 // slab's own nodes [o0, o0 + no), else (the k-neighbour in the upstream
 // slab's edge segment, which starts at eb) at edge[c*L + w - eb].
 template <bool FWD>
-__device__ __forceinline__ double row_from_slab(const RowRecs& r, const double* own, int o0, int no, int So,
-                                                const double* edge, int eb, int L, const double* dsv, int cnt) {
+__device__ __forceinline__ double row_from_slab(const SlabRow& r, const double* own, int o0, int no, int So,
+                                                const double* edge, int eb, int L) {
   double acc[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -1253,8 +1266,7 @@ __device__ __forceinline__ double row_from_slab(const RowRecs& r, const double* 
     acc[d] = sd;
   }
   if (FWD) return div2_rn(r.rhs + (acc[0] + acc[1] + acc[2]), r.diag, r.rdiag, r.invj, r.rinvj, r.bok);
-  return __ldcg(dsv + r.row * cnt + r.node) -
-         div2_rn(acc[0] + acc[1] + acc[2], r.invj, r.rinvj, r.diag, r.rdiag, r.bok);
+  return r.dsv - div2_rn(acc[0] + acc[1] + acc[2], r.invj, r.rinvj, r.diag, r.rdiag, r.bok);
 }
 
 }  // namespace
@@ -1273,23 +1285,23 @@ __device__ __forceinline__ double row_from_slab(const RowRecs& r, const double* 
 // into the downstream CTA's inbox, counted in bytes on the receiver's mbarrier
 // for that inbox slot; a CTA waits only on that mbarrier, for the step before
 // its own.  So the CTAs run as a pipeline, each a few planes behind its
-// upstream neighbour, and a pass takes about H plane steps plus one
-// neighbour latency per slab, with no cluster-wide exchange on any plane and
-// no memory fence on the plane-to-plane path.  Rings, inboxes and staging
-// areas hold D planes.  After each step a CTA tells both neighbours the last
-// step it completed (a relaxed store into their shared memory); a CTA copies
-// step gs into a neighbour's slot only after that neighbour has completed
-// step gs-D+1, which waited for the slot's previous copy, so no slot is
-// overwritten while in use and no mbarrier phase is armed twice.  No CTA can
-// wait forever on another: each wait is for a CTA at an earlier step, and
-// every wait is bounded.  A wait that runs out makes the CTA stop sending (its
-// neighbours then run out too); at the end the CTAs exchange their failure
-// flags, and if any failed each idles for a bounded time after the last
-// cluster barrier, so copies issued before that barrier land before any CTA
-// leaves.  Without a failure every copy into a CTA is waited for before the
-// last barrier.  The arithmetic per row is lusgs_rows', so the result is the
-// same to the bit.
-template <typename R>
+// upstream neighbour, with no cluster-wide exchange on any plane and no memory
+// fence on the plane-to-plane path; what remains per plane is the CTA's own
+// work and its record loads, which each thread issues DEPTH steps ahead (two
+// register sets for DEPTH 2, which the 256-thread variant has room for) after
+// the pass's leading CTA has prefetched the plane's chunks into L2.  Rings,
+// inboxes and staging areas hold D planes.  After each step a CTA tells both
+// neighbours the last step it completed (a relaxed store into their shared
+// memory); a CTA copies step gs into a neighbour's slot only after that
+// neighbour has completed step gs-D+1, which waited for the slot's previous
+// copy, so no slot is overwritten while in use and no mbarrier phase is armed
+// twice.  No CTA can wait forever on another: each wait is for a CTA at an
+// earlier step, and every wait is bounded.  A wait that runs out makes the
+// CTA stop sending (its neighbours then run out too); slab::finish then keeps
+// every CTA resident until no copy can still land in it.  Without a failure
+// every copy into a CTA is waited for before the last barrier.  The
+// arithmetic per row is lusgs_rows', so the result is the same to the bit.
+template <typename R, int DEPTH>
 __device__ __forceinline__ void lusgs_slab_body(const BlockView* __restrict__ blocks, unsigned* status, int So,
                                                 int L, int D) {
   constexpr int W = RecFmt<R>::kWords;
@@ -1321,17 +1333,14 @@ __device__ __forceinline__ void lusgs_slab_body(const BlockView* __restrict__ bl
     const unsigned at_lo = G.has_lo() ? slab::map(slab::local(&s_prog[1]), G.me - 1) : 0u;
     const unsigned at_hi = G.has_hi() ? slab::map(slab::local(&s_prog[0]), G.me + 1) : 0u;
     const unsigned inbox_l = slab::local(inbox), full_l = slab::local(full), stage_l = slab::local(stage);
-    RowRecs pre;  // the records of this thread's row of the next step
-    auto preload = [&](int gs) {
+    auto preload = [&](int gs, SlabRow& r) {
       if (gs >= 2 * H) return;
-      const bool fwd = gs < H;
       const int h = G.plane(gs);
       const long base = poff[h];
-      const int cnt = (int)(poff[h + 1] - base);
       const int t0 = G.seg(h, G.c0), n = G.seg(h, G.c1) - t0;
       if (tid < 5 * n) {
         const int row = row_of(tid, n);
-        load_node_row(recs<R>(B, fwd) + W * base, B.sca + kSca * base, cnt, row, t0 + tid - row * n, pre);
+        load_slab_row<R>(B, gs < H, base, (int)(poff[h + 1] - base), row, t0 + tid - row * n, r);
       }
     };
     // L2 prefetch of step gs's whole chunks (records, scalars and, backward,
@@ -1349,11 +1358,10 @@ __device__ __forceinline__ void lusgs_slab_body(const BlockView* __restrict__ bl
       if (tid == 33) slab::prefetch_span(B.sca + kSca * base, 8L * kSca * cnt);
       if (tid == 34 && !fwd) slab::prefetch_span(B.dqs + 8 * base, 64L * cnt);
     };
-    constexpr int PF = 3;  // prefetch distance in steps
-    for (int gs = 0; gs < PF; ++gs) prefetch(gs);
-    preload(0);
     unsigned parity = 0;  // bit x: parity of the next phase of full[x] to wait for
-    for (int gs = 0; gs < 2 * H; ++gs) {
+    // one plane step with the row preloaded in `pre`; false (in every thread)
+    // when a wait of this CTA ran out
+    auto step = [&](int gs, const SlabRow& pre) -> bool {
       const bool fwd = gs < H;
       const int h = G.plane(gs);
       const long base = poff[h];
@@ -1377,13 +1385,13 @@ __device__ __forceinline__ void lusgs_slab_body(const BlockView* __restrict__ bl
         const int eb = G.seg(hp, max(G.c_up(gs), 0));
         const double* own = ring + xp * 5 * So;
         const double* edge = inbox + xp * 5 * L;
-        const double* dsv = B.dqs + 8 * base;
-        const double v = fwd ? row_from_slab<true>(pre, own, p0, np, So, edge, eb, L, dsv, cnt)
-                             : row_from_slab<false>(pre, own, p0, np, So, edge, eb, L, dsv, cnt);
+        const double v = fwd ? row_from_slab<true>(pre, own, p0, np, So, edge, eb, L)
+                             : row_from_slab<false>(pre, own, p0, np, So, edge, eb, L);
         ring[x * 5 * So + pre.row * So + (pre.node - t0)] = v;
         if (need_dn) {
           const int e0 = G.seg(h, G.c_dn(gs));
-          if (pre.node >= e0 && pre.node < G.seg(h, G.c_dn(gs) + 1)) stage[x * 5 * L + pre.row * L + (pre.node - e0)] = v;
+          if (pre.node >= e0 && pre.node < G.seg(h, G.c_dn(gs) + 1))
+            stage[x * 5 * L + pre.row * L + (pre.node - e0)] = v;
         }
         if (fwd)
           B.dqs[8 * base + pre.row * cnt + pre.node] = v;
@@ -1393,7 +1401,7 @@ __device__ __forceinline__ void lusgs_slab_body(const BlockView* __restrict__ bl
       if (need_dn) slab::fence_to_copies();
       if (__syncthreads_or(fail ? 1 : 0)) {
         if (tid == 0) s_fail = 1;
-        break;
+        return false;
       }
       if (tid == 0) {
         if (need_dn) {
@@ -1405,19 +1413,43 @@ __device__ __forceinline__ void lusgs_slab_body(const BlockView* __restrict__ bl
         if (G.has_lo()) slab::store_relaxed(at_lo, gs);
         if (G.has_hi()) slab::store_relaxed(at_hi, gs);
       }
+      return true;
+    };
+    constexpr int PF = 4;  // prefetch distance in steps
+    for (int gs = 0; gs < PF; ++gs) prefetch(gs);
+    SlabRow r0, r1;
+    preload(0, r0);
+    if (DEPTH == 2) preload(1, r1);
+    for (int gs = 0; gs < 2 * H; gs += DEPTH) {
+      if (!step(gs, r0)) break;
       prefetch(gs + PF);
-      preload(gs + 1);
+      preload(gs + DEPTH, r0);
+      if (DEPTH == 2) {
+        if (gs + 1 >= 2 * H) break;
+        if (!step(gs + 1, r1)) break;
+        prefetch(gs + 1 + PF);
+        preload(gs + 3, r1);
+      }
     }
   }
   slab::finish(s_fail, ncta, status, B);
 }
 __global__ void __launch_bounds__(512, 1) k_lusgs_sweep_slab(const BlockView* __restrict__ blocks, unsigned* status,
                                                              int So, int L, int D) {
-  lusgs_slab_body<double>(blocks, status, So, L, D);
+  lusgs_slab_body<double, 1>(blocks, status, So, L, D);
 }
 __global__ void __launch_bounds__(512, 1) k_lusgs_sweep_slab_f32(const BlockView* __restrict__ blocks,
                                                                  unsigned* status, int So, int L, int D) {
-  lusgs_slab_body<float>(blocks, status, So, L, D);
+  lusgs_slab_body<float, 1>(blocks, status, So, L, D);
+}
+// Slabs whose planes have at most 51 nodes (256 rows): record loads two steps ahead.
+__global__ void __launch_bounds__(256, 1) k_lusgs_sweep_slab2(const BlockView* __restrict__ blocks,
+                                                              unsigned* status, int So, int L, int D) {
+  lusgs_slab_body<double, 2>(blocks, status, So, L, D);
+}
+__global__ void __launch_bounds__(256, 1) k_lusgs_sweep_slab2_f32(const BlockView* __restrict__ blocks,
+                                                                  unsigned* status, int So, int L, int D) {
+  lusgs_slab_body<float, 2>(blocks, status, So, L, D);
 }
 
 // q = q + dq on every updated node (sub_timeadvancement_1stimplicit.f90:568-574).

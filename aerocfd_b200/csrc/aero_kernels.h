@@ -122,6 +122,9 @@ __global__ void k_lusgs_sweep_bulk_f32(const BlockView* __restrict__ blocks, uns
 // inboxes and staging areas of 5 x L values)
 __global__ void k_lusgs_sweep_slab(const BlockView* __restrict__ blocks, unsigned* status, int So, int L, int D);
 __global__ void k_lusgs_sweep_slab_f32(const BlockView* __restrict__ blocks, unsigned* status, int So, int L, int D);
+// the same for slab planes of at most 256 rows, record loads two steps ahead
+__global__ void k_lusgs_sweep_slab2(const BlockView* __restrict__ blocks, unsigned* status, int So, int L, int D);
+__global__ void k_lusgs_sweep_slab2_f32(const BlockView* __restrict__ blocks, unsigned* status, int So, int L, int D);
 __global__ void k_lusgs_update(const BlockView* __restrict__ blocks);
 __global__ void k_physical_bc(const BlockView* __restrict__ blocks, const BcOp* __restrict__ ops,
                               const BcEntry* __restrict__ list, int first, CaseConsts cc);

@@ -161,8 +161,10 @@ struct State {
   // slab sweeps (mean flow FP64 / FP32 records, SA): dynamic shared memory
   // set so far, clusters of 16 allowed, and the launch shapes of the
   // registered blocks per (cluster size, rows per node)
-  size_t smem_slab[3] = {0, 0, 0};
-  bool np_slab[3] = {false, false, false};
+  // (index: 0 / 1 mean flow FP64 / FP32 records, 2 SA, 3 / 4 the mean-flow
+  // variants with loads two steps ahead)
+  size_t smem_slab[5] = {0, 0, 0, 0, 0};
+  bool np_slab[5] = {false, false, false, false, false};
   std::map<int, SlabFit> slab_fits;
   long spin_limit = kPollBudgetMax;  // polls of each staged-sweep wait (aero_set_poll_budget)
   int stall_plane = -1;              // forward plane whose copies are withheld (aero_inject_sweep_stall)
@@ -767,8 +769,10 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
     // one cluster per block, each CTA one k-slab, pipelined plane by plane
     const int cl = g.tune.sweep_cl;
     const size_t smem = slab_smem(sf, 5);
-    auto kern = f ? k_lusgs_sweep_slab_f32 : k_lusgs_sweep_slab;
-    if ((rc = prepare_slab(kern, f, smem, cl))) return rc;
+    // slab planes of at most 256 rows take the variant with loads two steps ahead
+    const bool deep = sf.T <= 256;
+    auto kern = deep ? (f ? k_lusgs_sweep_slab2_f32 : k_lusgs_sweep_slab2) : (f ? k_lusgs_sweep_slab_f32 : k_lusgs_sweep_slab);
+    if ((rc = prepare_slab(kern, f + (deep ? 3 : 0), smem, cl))) return rc;
     cudaError_t le = cudaSuccess;
     PROF(P_LUSGS_SWEEP,
          (le = launch_clusters(kern, nblk, cl, sf.T, smem, g.stream, sv, g.d_status, sf.So, sf.L, sf.D)));
@@ -1340,10 +1344,13 @@ bool slab_cluster16_fits(int rows) {
   if (!sf.ok) return false;
   const size_t smem = slab_smem(sf, rows);
   const int nk = rows == 5 ? 2 : 1;
+  const bool deep = rows == 5 && sf.T <= 256;
   for (int k = 0; k < nk; ++k) {
-    const int idx = rows == 5 ? k : 2;
+    const int idx = rows == 5 ? k + (deep ? 3 : 0) : 2;
     void (*kern)(const BlockView*, unsigned*, int, int, int) =
-        rows == 5 ? (k ? k_lusgs_sweep_slab_f32 : k_lusgs_sweep_slab) : k_sa_sweep_slab;
+        rows == 5 ? (deep ? (k ? k_lusgs_sweep_slab2_f32 : k_lusgs_sweep_slab2)
+                          : (k ? k_lusgs_sweep_slab_f32 : k_lusgs_sweep_slab))
+                  : k_sa_sweep_slab;
     if (prepare_slab(kern, idx, smem, 16) != AERO_OK) {
       cudaGetLastError();
       return false;

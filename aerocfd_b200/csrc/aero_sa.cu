@@ -445,8 +445,8 @@ __global__ void __launch_bounds__(768) k_sa_sweep_768(const BlockView* __restric
 // counted on that CTA's mbarrier; relaxed progress counters keep the D-plane
 // slots from being overwritten while in use; every wait is bounded, and
 // slab::finish keeps every CTA resident until no copy can still land in it).
-// One node per thread.  The arithmetic per node is sa_sweep_body's, so the
-// result is the same to the bit.
+// One node per thread, its records loaded two steps ahead.  The arithmetic
+// per node is sa_sweep_body's, so the result is the same to the bit.
 __global__ void __launch_bounds__(512, 1) k_sa_sweep_slab(const BlockView* __restrict__ blocks, unsigned* status,
                                                           int So, int L, int D) {
   extern __shared__ __align__(16) double sdyn[];
@@ -474,17 +474,18 @@ __global__ void __launch_bounds__(512, 1) k_sa_sweep_slab(const BlockView* __res
     const unsigned at_lo = G.has_lo() ? slab::map(slab::local(&s_prog[1]), G.me - 1) : 0u;
     const unsigned at_hi = G.has_hi() ? slab::map(slab::local(&s_prog[0]), G.me + 1) : 0u;
     const unsigned inbox_l = slab::local(inbox), full_l = slab::local(full), stage_l = slab::local(stage);
-    SaFwd pre_f{};
-    SaBwd pre_b{};
-    auto preload = [&](int gs) {
+    // the records of this thread's node, loaded two steps ahead (even and odd steps)
+    SaFwd pf[2] = {};
+    SaBwd pb[2] = {};
+    auto preload = [&](int gs, SaFwd& f, SaBwd& bw) {
       if (gs >= 2 * H) return;
       const int h = G.plane(gs);
       const int t0 = G.seg(h, G.c0), n = G.seg(h, G.c1) - t0;
       if (tid < n) {
         if (gs < H)
-          sa_load_fwd(B, h, t0 + tid, pre_f);
+          sa_load_fwd(B, h, t0 + tid, f);
         else
-          sa_load_bwd(B, h, t0 + tid, pre_b);
+          sa_load_bwd(B, h, t0 + tid, bw);
       }
     };
     // L2 prefetch of step gs's whole chunks (records and, backward, sa_dq and
@@ -501,11 +502,9 @@ __global__ void __launch_bounds__(512, 1) k_sa_sweep_slab(const BlockView* __res
       if (tid == 33 && !fwd) slab::prefetch_span(B.sa_dq + base, 8L * cnt);
       if (tid == 34 && !fwd) slab::prefetch_span(B.nat + base, 8L * cnt);
     };
-    constexpr int PF = 3;  // prefetch distance in steps
-    for (int gs = 0; gs < PF; ++gs) prefetch(gs);
-    preload(0);
     unsigned parity = 0;  // bit x: parity of the next phase of full[x] to wait for
-    for (int gs = 0; gs < 2 * H; ++gs) {
+    // one plane step; false (in every thread) when a wait of this CTA ran out
+    auto step = [&](int gs, const SaFwd& pre_f, const SaBwd& pre_b) -> bool {
       const bool fwd = gs < H;
       const int h = G.plane(gs);
       const long base = B.poff[h];
@@ -557,7 +556,7 @@ __global__ void __launch_bounds__(512, 1) k_sa_sweep_slab(const BlockView* __res
       if (need_dn) slab::fence_to_copies();
       if (__syncthreads_or(fail ? 1 : 0)) {
         if (tid == 0) s_fail = 1;
-        break;
+        return false;
       }
       if (tid == 0) {
         if (need_dn) {
@@ -569,8 +568,20 @@ __global__ void __launch_bounds__(512, 1) k_sa_sweep_slab(const BlockView* __res
         if (G.has_lo()) slab::store_relaxed(at_lo, gs);
         if (G.has_hi()) slab::store_relaxed(at_hi, gs);
       }
+      return true;
+    };
+    constexpr int PF = 4;  // prefetch distance in steps
+    for (int gs = 0; gs < PF; ++gs) prefetch(gs);
+    preload(0, pf[0], pb[0]);
+    preload(1, pf[1], pb[1]);
+    for (int gs = 0; gs < 2 * H; gs += 2) {
+      if (!step(gs, pf[0], pb[0])) break;
       prefetch(gs + PF);
-      preload(gs + 1);
+      preload(gs + 2, pf[0], pb[0]);
+      if (gs + 1 >= 2 * H) break;
+      if (!step(gs + 1, pf[1], pb[1])) break;
+      prefetch(gs + 1 + PF);
+      preload(gs + 3, pf[1], pb[1]);
     }
   }
   slab::finish(s_fail, ncta, status, B);

@@ -573,15 +573,23 @@ def warm_start_naca_gpu(solver, n_train: int = 48, n_test: int = 12, its_train: 
            "samples": int(len(X)), "train_steps": 4000, "train_s": train_s, "data_generation_s": gen_s,
            "loss_first_last": [float(loss[:10].mean()), float(loss[-10:].mean())],
            "iteration1_residual_ratio_warm_over_cold": float(np.mean(runs["warm"][0][0] / hc[0])),
-           "block_status_nonzero": {k: int((v[3] != 0).sum()) for k, v in runs.items()}}
+           "member_status": {k: [int(x) for x in v[3]] for k, v in runs.items()}}
     levels = {}
     for drop in (1e-1, 1e-2, 1e-3):
         lv = hc[0] * drop
         row = {}
-        for k, (h, wall, _, _) in runs.items():
+        for k, (h, wall, _, st) in runs.items():
             it = W.first_below(h, lv, chunk)
+            it[st != 0] = -1  # a failed member is retired (its residual then reads 0): it reached nothing
             row[k] = {"iterations": [int(v) if v > 0 else None for v in it], "members_reached": int((it > 0).sum()),
+                      "members_failed": int((st != 0).sum()),
                       "wall_s_all_members": float(wall * it.max() / its_test) if (it > 0).all() else None}
+        # members that both the cold run and the warm run brought to the level
+        both = [i for i in range(n_test) if row["cold"]["iterations"][i] and row["warm"]["iterations"][i]]
+        row["mean_iterations_both_reached"] = {
+            k: (float(np.mean([row[k]["iterations"][i] for i in both])) if both else None) for k in ("cold", "warm")}
+        row["members_warm_faster"] = int(sum(row["warm"]["iterations"][i] < row["cold"]["iterations"][i] for i in both))
+        row["members_both_reached"] = len(both)
         levels[f"{drop:.0e}"] = row
     out["levels"] = levels
     forces = []
