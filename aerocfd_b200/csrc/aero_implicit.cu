@@ -1236,7 +1236,8 @@ __device__ __forceinline__ void load_slab_row(const BlockView& B, bool fwd, long
   r.invj = sn[6 * cnt];
   r.rdiag = sn[7 * cnt];
   r.rinvj = sn[8 * cnt];
-  // dq* of the node, written by this CTA in the forward pass (read from L2)
+  // dq* of the node, written by this CTA in the forward pass (read from L2;
+  // complete once the forward pass has passed the node's plane)
   r.dsv = fwd ? 0.0 : __ldcg(B.dqs + 8 * base + row * cnt + node);
   r.bok = !nbr_slow_div(r.packed);
 }
@@ -1246,7 +1247,7 @@ __device__ __forceinline__ void load_slab_row(const BlockView& B, bool fwd, long
 // slab's edge segment, which starts at eb) at edge[c*L + w - eb].
 template <bool FWD>
 __device__ __forceinline__ double row_from_slab(const SlabRow& r, const double* own, int o0, int no, int So,
-                                                const double* edge, int eb, int L) {
+                                                const double* edge, int eb, int L, double dsv) {
   double acc[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -1266,7 +1267,7 @@ __device__ __forceinline__ double row_from_slab(const SlabRow& r, const double* 
     acc[d] = sd;
   }
   if (FWD) return div2_rn(r.rhs + (acc[0] + acc[1] + acc[2]), r.diag, r.rdiag, r.invj, r.rinvj, r.bok);
-  return r.dsv - div2_rn(acc[0] + acc[1] + acc[2], r.invj, r.rinvj, r.diag, r.rdiag, r.bok);
+  return dsv - div2_rn(acc[0] + acc[1] + acc[2], r.invj, r.rinvj, r.diag, r.rdiag, r.bok);
 }
 
 }  // namespace
@@ -1385,8 +1386,11 @@ __device__ __forceinline__ void lusgs_slab_body(const BlockView* __restrict__ bl
         const int eb = G.seg(hp, max(G.c_up(gs), 0));
         const double* own = ring + xp * 5 * So;
         const double* edge = inbox + xp * 5 * L;
-        const double v = fwd ? row_from_slab<true>(pre, own, p0, np, So, edge, eb, L)
-                             : row_from_slab<false>(pre, own, p0, np, So, edge, eb, L);
+        // dq* of the first backward plane (the forward pass's last) is written
+        // by the step before, after a two-step-ahead load of it was issued
+        const double dsv = (DEPTH > 1 && gs == H) ? __ldcg(B.dqs + 8 * base + pre.row * cnt + pre.node) : pre.dsv;
+        const double v = fwd ? row_from_slab<true>(pre, own, p0, np, So, edge, eb, L, dsv)
+                             : row_from_slab<false>(pre, own, p0, np, So, edge, eb, L, dsv);
         ring[x * 5 * So + pre.row * So + (pre.node - t0)] = v;
         if (need_dn) {
           const int e0 = G.seg(h, G.c_dn(gs));

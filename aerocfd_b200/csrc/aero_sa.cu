@@ -544,7 +544,10 @@ __global__ void __launch_bounds__(512, 1) k_sa_sweep_slab(const BlockView* __res
             const int w = nbr_local(pre_b.packed, d);
             tt[d] = w < 0 ? 0.0 : pre_b.b[d] * prev(w, d);
           }
-          v = pre_b.dqs - div_rn_lean(tt[0] + tt[1] + tt[2], pre_b.diag, pre_b.rdiag);
+          // sa_dq of the first backward plane (the forward pass's last) is
+          // written by the step before, after its two-step-ahead load was issued
+          const double dqs = gs == H ? __ldcg(B.sa_dq + base + t) : pre_b.dqs;
+          v = dqs - div_rn_lean(tt[0] + tt[1] + tt[2], pre_b.diag, pre_b.rdiag);
           B.s(F_NUT, pre_b.nat) = pre_b.nut + v;
         }
         ring[x * So + tid] = v;
