@@ -150,6 +150,7 @@ struct State {
   // time-step kernels (they read q, the primitives and the metrics only)
   cudaStream_t stream3 = nullptr;
   cudaEvent_t ev_join3 = nullptr;
+  cudaEvent_t ev_dt = nullptr;  // find_dt done: the SA records may start
   // fourth stream: sa_model, forked after find_dt, beside the rest of the
   // mean-flow iteration
   cudaStream_t stream4 = nullptr;
@@ -862,15 +863,22 @@ int launch_index(const BlockView* views, int nblk, long maxN1) {
 
 // sa_model (sub_tur_sa.f90:7-122) on nblk views, on stream st (the library's
 // stream when null); needs the hyperplane index.
+// parts: 1 the length scale and the right-hand side (sa_rhs1/2/3; they read
+// pri_v, amu, vor, dudx and the metrics), 2 the records and the sweeps (the
+// records also read dt); 3 both.
 int launch_sa(const BlockView* views, int nblk, long maxN, long maxN1, int pmax, const CaseConsts& cc,
-              cudaStream_t st = nullptr, const BlockView* host_views = nullptr) {
+              cudaStream_t st = nullptr, const BlockView* host_views = nullptr, int parts = 3) {
   if (!st) st = g.stream;
-  PROF_ON(P_FILL, st, (k_sa_length<<<dim3(cdiv(maxN, 256), nblk), 256, 0, st>>>(views, cc)));
-  CKL();
-  PROF_ON(P_SA_A, st, (k_sa_a<<<dim3(cdiv(maxN1, 256), nblk), 256, 0, st>>>(views, cc)));
-  CKL();
-  PROF_ON(P_SA_B, st, ((g.mixed ? k_sa_b_mixed : k_sa_b)<<<dim3(cdiv(maxN1, 128), nblk), 128, 0, st>>>(views, cc)));
-  CKL();
+  if (parts & 1) {
+    PROF_ON(P_FILL, st, (k_sa_length<<<dim3(cdiv(maxN, 256), nblk), 256, 0, st>>>(views, cc)));
+    CKL();
+    PROF_ON(P_SA_A, st, (k_sa_a<<<dim3(cdiv(maxN1, 256), nblk), 256, 0, st>>>(views, cc)));
+    CKL();
+    PROF_ON(P_SA_B, st,
+            ((g.mixed ? k_sa_b_mixed : k_sa_b)<<<dim3(cdiv(maxN1, 128), nblk), 128, 0, st>>>(views, cc)));
+    CKL();
+  }
+  if (!(parts & 2)) return AERO_OK;
   PROF_ON(P_SA_RECS, st, (k_sa_recs<<<dim3(cdiv(maxN1, 256), nblk), 256, 0, st>>>(views, cc)));
   CKL();
   SlabFit sf;
@@ -1037,19 +1045,25 @@ int do_iteration(bool want_dt_minmax, bool resid_beside = false) {
   CK(cudaStreamWaitEvent(g.stream3, g.ev_fork2, 0));
   if ((rc = launch_implicit_blocks(g.d_blocks, nb, g.max_ext, g.max_b1, g.cc, g.stream3))) return rc;
   CK(cudaEventRecord(g.ev_join3, g.stream3));
-  // viscous part a, then find_dt (it reads the viscosity part a forms), then
-  // sa_model on a fourth stream: it reads pri_v, amu, dudx, vor, dt and the
-  // metrics and writes nut, sa_rhs and its own scratch, none of which the
-  // rest of the mean-flow iteration (viscous part b, implicit1st) reads or
-  // writes, so it runs beside all of them
+  // viscous part a, then find_dt (it reads the viscosity part a forms);
+  // sa_model runs on a fourth stream: it reads pri_v, amu, dudx, vor, dt and
+  // the metrics and writes nut, sa_rhs and its own scratch, none of which the
+  // rest of the mean-flow iteration (find_dt, viscous part b, implicit1st)
+  // reads or writes, so it runs beside all of them, its right-hand side from
+  // viscous part a on and its records (which read dt) from find_dt on
   if (viscous_on() && (rc = launch_viscous_a(g.d_blocks, nb, g.max_b0, g.cc, ddes_on()))) return rc;
-  if ((rc = launch_find_dt(g.d_blocks, nb, g.max_box, g.cc))) return rc;
-  if (want_dt_minmax && (rc = launch_dt_minmax(g.d_blocks, nb - 1, g.d_out + 7))) return rc;
   const bool sa = sa_on();
   if (sa) {
     CK(cudaEventRecord(g.ev_fork, g.stream));
     CK(cudaStreamWaitEvent(g.stream4, g.ev_fork, 0));
-    if ((rc = launch_sa(g.d_blocks, nb, g.max_box, g.max_b1, g.pmax_all, g.cc, g.stream4))) return rc;
+    if ((rc = launch_sa(g.d_blocks, nb, g.max_box, g.max_b1, g.pmax_all, g.cc, g.stream4, nullptr, 1))) return rc;
+  }
+  if ((rc = launch_find_dt(g.d_blocks, nb, g.max_box, g.cc))) return rc;
+  if (want_dt_minmax && (rc = launch_dt_minmax(g.d_blocks, nb - 1, g.d_out + 7))) return rc;
+  if (sa) {
+    CK(cudaEventRecord(g.ev_dt, g.stream));
+    CK(cudaStreamWaitEvent(g.stream4, g.ev_dt, 0));
+    if ((rc = launch_sa(g.d_blocks, nb, g.max_box, g.max_b1, g.pmax_all, g.cc, g.stream4, nullptr, 2))) return rc;
     CK(cudaEventRecord(g.ev_join, g.stream4));
   }
   if (viscous_on() && (rc = launch_viscous_b(g.d_blocks, nb, g.max_b0, g.cc))) return rc;
@@ -1169,6 +1183,7 @@ int aero_init(int device) {
   CK(cudaStreamCreateWithFlags(&g.stream3, cudaStreamNonBlocking));
   CK(cudaStreamCreateWithFlags(&g.stream4, cudaStreamNonBlocking));
   CK(cudaEventCreateWithFlags(&g.ev_join3, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&g.ev_dt, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&g.ev_fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&g.ev_join, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&g.ev_fork2, cudaEventDisableTiming));
@@ -1241,6 +1256,7 @@ int aero_finalize(void) {
   cudaStreamDestroy(g.stream4); g.stream4 = nullptr;
   cudaEventDestroy(g.ev_join3); g.ev_join3 = nullptr;
   cudaEventDestroy(g.ev_fork); g.ev_fork = nullptr;
+  cudaEventDestroy(g.ev_dt); g.ev_dt = nullptr;
   cudaEventDestroy(g.ev_join); g.ev_join = nullptr;
   cudaEventDestroy(g.ev_fork2); g.ev_fork2 = nullptr;
   cudaEventDestroy(g.ev_join2); g.ev_join2 = nullptr;
