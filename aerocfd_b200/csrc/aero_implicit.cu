@@ -1344,28 +1344,20 @@ __device__ __forceinline__ void lusgs_slab_body(const BlockView* __restrict__ bl
         load_slab_row<R>(B, gs < H, base, (int)(poff[h + 1] - base), row, t0 + tid - row * n, r);
       }
     };
-    // L2 prefetch of step gs's chunks (records, scalars and, backward, dq*):
-    // each CTA asks for its 1/ce share of each chunk, split over the lanes of
-    // warp 1 (every share and piece starts and ends on a 16-byte boundary:
-    // the chunks do, and so do the rounded pieces); a CTA lags the pass's
-    // leading CTA by a few steps, so the distance covers that lag too
+    // L2 prefetch of step gs's whole chunks (records, scalars and, backward,
+    // dq*) by the pass's leading CTA (the one without an upstream slab: every
+    // other CTA reaches each step after it), one lane per chunk; the chunks
+    // start and end on 16-byte boundaries
+    const bool lead_f = G.me == 0, lead_b = G.me == G.ce - 1;
     auto prefetch = [&](int gs) {
-      if (gs >= 2 * H || (tid >> 5) != 1) return;
+      if (gs >= 2 * H || tid >= 35 || tid < 32) return;
       const bool fwd = gs < H;
+      if (!(fwd ? lead_f : lead_b)) return;
       const long base = poff[G.plane(gs)];
       const long cnt = poff[G.plane(gs) + 1] - base;
-      const int lane = tid & 31;
-      auto share = [&](const void* chunk, long bytes) {
-        const long part = ((bytes + G.ce - 1) / G.ce + 15) & ~15L;
-        const long off = part * G.me, len = min(part, bytes - off);
-        if (len <= 0) return;
-        const long piece = ((len + 31) / 32 + 15) & ~15L;
-        const long o = (long)lane * piece;
-        if (o < len) slab::prefetch_span((const char*)chunk + off + o, min(piece, len - o));
-      };
-      share(recs<R>(B, fwd) + W * base, (long)W * (long)sizeof(R) * cnt);
-      share(B.sca + kSca * base, 8L * kSca * cnt);
-      if (!fwd) share(B.dqs + 8 * base, 64L * cnt);
+      if (tid == 32) slab::prefetch_span(recs<R>(B, fwd) + W * base, (long)W * (long)sizeof(R) * cnt);
+      if (tid == 33) slab::prefetch_span(B.sca + kSca * base, 8L * kSca * cnt);
+      if (tid == 34 && !fwd) slab::prefetch_span(B.dqs + 8 * base, 64L * cnt);
     };
     unsigned parity = 0;  // bit x: parity of the next phase of full[x] to wait for
     // one plane step with the row preloaded in `pre`; false (in every thread)
@@ -1427,7 +1419,7 @@ __device__ __forceinline__ void lusgs_slab_body(const BlockView* __restrict__ bl
       }
       return true;
     };
-    constexpr int PF = 8;  // prefetch distance in steps
+    constexpr int PF = 4;  // prefetch distance in steps
     for (int gs = 0; gs < PF; ++gs) prefetch(gs);
     SlabRow r0, r1;
     preload(0, r0);

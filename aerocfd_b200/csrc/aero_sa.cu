@@ -488,29 +488,19 @@ __global__ void __launch_bounds__(512, 1) k_sa_sweep_slab(const BlockView* __res
           sa_load_bwd(B, h, t0 + tid, bw);
       }
     };
-    // L2 prefetch of step gs's chunks (records and, backward, sa_dq and the
-    // natural indices): each CTA asks for its 1/ce share of each chunk, split
-    // over the lanes of warp 1 (shares and pieces rounded to 16 bytes inside
-    // the workspace); the distance covers a CTA's lag behind the leading one
+    // L2 prefetch of step gs's whole chunks (records and, backward, sa_dq and
+    // the natural indices) by the pass's leading CTA (the one without an
+    // upstream slab: every other CTA reaches each step after it)
+    const bool lead_f = G.me == 0, lead_b = G.me == G.ce - 1;
     auto prefetch = [&](int gs) {
-      if (gs >= 2 * H || (tid >> 5) != 1) return;
+      if (gs >= 2 * H || tid >= 35 || tid < 32) return;
       const bool fwd = gs < H;
+      if (!(fwd ? lead_f : lead_b)) return;
       const long base = B.poff[G.plane(gs)];
       const long cnt = B.poff[G.plane(gs) + 1] - base;
-      const int lane = tid & 31;
-      auto share = [&](const void* chunk, long bytes) {
-        const long part = ((bytes + G.ce - 1) / G.ce + 15) & ~15L;
-        const long off = part * G.me, len = min(part, bytes - off);
-        if (len <= 0) return;
-        const long piece = ((len + 31) / 32 + 15) & ~15L;
-        const long o = (long)lane * piece;
-        if (o < len) slab::prefetch_span((const char*)chunk + off + o, min(piece, len - o));
-      };
-      share(B.sa_rec + kSaRec * base, 8L * kSaRec * cnt);
-      if (!fwd) {
-        share(B.sa_dq + base, 8L * cnt);
-        share(B.nat + base, 8L * cnt);
-      }
+      if (tid == 32) slab::prefetch_span(B.sa_rec + kSaRec * base, 8L * kSaRec * cnt);
+      if (tid == 33 && !fwd) slab::prefetch_span(B.sa_dq + base, 8L * cnt);
+      if (tid == 34 && !fwd) slab::prefetch_span(B.nat + base, 8L * cnt);
     };
     unsigned parity = 0;  // bit x: parity of the next phase of full[x] to wait for
     // one plane step; false (in every thread) when a wait of this CTA ran out
@@ -583,7 +573,7 @@ __global__ void __launch_bounds__(512, 1) k_sa_sweep_slab(const BlockView* __res
       }
       return true;
     };
-    constexpr int PF = 8;  // prefetch distance in steps
+    constexpr int PF = 4;  // prefetch distance in steps
     for (int gs = 0; gs < PF; ++gs) prefetch(gs);
     preload(0, pf[0], pb[0]);
     preload(1, pf[1], pb[1]);
