@@ -390,6 +390,15 @@ __device__ __forceinline__ void faces_body(const BlockView* __restrict__ blocks,
   for (int c = 0; c < 5; ++c) out[(long)c * B.plane] = f[c];
 }
 __global__ void k_inviscid_faces(const BlockView* __restrict__ blocks, CaseConsts cc) { faces_body<false>(blocks, cc); }
+// The same under register bounds for 6 or 8 resident CTAs of 128 threads per
+// SM (more warps to hide the FP64 latency, at the cost of a few spills); the
+// autotuner chooses.
+__global__ void __launch_bounds__(128, 6) k_inviscid_faces_o6(const BlockView* __restrict__ blocks, CaseConsts cc) {
+  faces_body<false>(blocks, cc);
+}
+__global__ void __launch_bounds__(128, 8) k_inviscid_faces_o8(const BlockView* __restrict__ blocks, CaseConsts cc) {
+  faces_body<false>(blocks, cc);
+}
 __global__ void k_inviscid_faces_mixed(const BlockView* __restrict__ blocks, CaseConsts cc) { faces_body<true>(blocks, cc); }
 
 __global__ void k_inviscid_combine(const BlockView* __restrict__ blocks, CaseConsts cc) {

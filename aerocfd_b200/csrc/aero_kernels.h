@@ -76,6 +76,8 @@ __global__ void k_inviscid_mixed_64(const BlockView* __restrict__ blocks, CaseCo
 __global__ void k_inviscid_mixed_128(const BlockView* __restrict__ blocks, CaseConsts cc);
 // face-based variant: face fluxes into FVH planes, then the node combine
 __global__ void k_inviscid_faces(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_inviscid_faces_o6(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_inviscid_faces_o8(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_inviscid_faces_mixed(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_inviscid_combine(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_faces_sw_weno5(const BlockView* __restrict__ blocks, CaseConsts cc);

@@ -236,7 +236,7 @@ struct State {
   bool rhsi_ghosts_zero = false;
   // launch shapes (aero_autotune); none of them changes the arithmetic
   struct Tune {
-    int inv_tile = 64;  // nodes per CTA of the inviscid flux; 0: face-based kernels
+    int inv_tile = 64;  // nodes per CTA of the inviscid flux; 0: face-based kernels (-6, -8: FP64 faces for 6, 8 CTAs/SM)
     int ew = 256;       // threads per CTA of the element-wise kernels
     int visc = 128;     // threads per CTA of k_viscous_a
     int mats = 128;     // threads per CTA of k_lusgs_mats
@@ -622,11 +622,13 @@ int launch_inviscid(const BlockView* views, int nblk, long maxN, long maxN1, lon
     PROF_ON(P_INVISCID, st, (faces<<<dim3(cdiv(maxF, 128), nblk, 3), 128, 0, st>>>(views, cc)));
     CKL();
     PROF_ON(P_INVISCID, st, (k_inviscid_combine<<<dim3(cdiv(maxN1, g.tune.ew), nblk), g.tune.ew, 0, st>>>(views, cc)));
-  } else if (tile == 0) {  // face-based: each face once, then the combine
+  } else if (tile <= 0) {  // face-based: each face once, then the combine
     // faces per direction <= updated box grown by one node in that direction
+    // (tile -6 / -8: the FP64 kernel under a register bound for 6 / 8 CTAs per SM)
     long maxF = maxN1 + maxFace;
-    PROF_ON(P_INVISCID, st, ((g.mixed ? k_inviscid_faces_mixed : k_inviscid_faces)<<<dim3(cdiv(maxF, 128), nblk, 3),
-                                                                                    128, 0, st>>>(views, cc)));
+    auto faces = g.mixed ? k_inviscid_faces_mixed
+                         : (tile == -6 ? k_inviscid_faces_o6 : tile == -8 ? k_inviscid_faces_o8 : k_inviscid_faces);
+    PROF_ON(P_INVISCID, st, (faces<<<dim3(cdiv(maxF, 128), nblk, 3), 128, 0, st>>>(views, cc)));
     CKL();
     PROF_ON(P_INVISCID, st, (k_inviscid_combine<<<dim3(cdiv(maxN1, g.tune.ew), nblk), g.tune.ew, 0, st>>>(views, cc)));
   } else {
@@ -1452,7 +1454,7 @@ int aero_autotune(int iters) {
   // exchange), since the exchanges are only eligible for some sizes
   int sweep_mode = 4 * g.tune.sweep_cl + g.tune.sweep_x;
   struct Knob { int* v; std::vector<int> cand; };
-  std::vector<Knob> knobs = {{&g.tune.inv_tile, {0, 32, 64, 128}}, {&g.tune.ew, {128, 256, 512}},
+  std::vector<Knob> knobs = {{&g.tune.inv_tile, {0, -6, -8, 32, 64, 128}}, {&g.tune.ew, {128, 256, 512}},
                              {&g.tune.visc, {64, 128, 256}}, {&g.tune.mats, {64, 128, 256}},
                              {&g.tune.nst_max, {2, 3, 4}},
                              {&sweep_mode, {0, 8, 16, 32, 9, 17, 33, 10, 18, 34}}};
@@ -1496,7 +1498,7 @@ int aero_set_tuning(int inv_tile, int ew, int visc, int mats, int nst_max) {
   int rc = need_init();
   if (rc) return rc;
   auto in = [](int v, std::initializer_list<int> ok) { return std::find(ok.begin(), ok.end(), v) != ok.end(); };
-  if (!in(inv_tile, {0, 32, 64, 128}) || !in(ew, {128, 256, 512}) || !in(visc, {64, 128, 256}) ||
+  if (!in(inv_tile, {-8, -6, 0, 32, 64, 128}) || !in(ew, {128, 256, 512}) || !in(visc, {64, 128, 256}) ||
       !in(mats, {64, 128, 256}) || !in(nst_max, {2, 3, 4}))
     return fail(AERO_ERR_ARG, "launch shape %d/%d/%d/%d/%d is not one the autotuner offers", inv_tile, ew, visc, mats,
                 nst_max);
