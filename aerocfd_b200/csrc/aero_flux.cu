@@ -786,7 +786,7 @@ __device__ __forceinline__ double cdiff(const double* f, long n, long st, int po
 // sub_viscous.f90:187-293: gradients, Sutherland viscosity, stresses, heat flux,
 // vorticity and the contravariant viscous fluxes on the physical nodes.  The
 // fluxes fv,gv,hv (components 2..5 each) go to the FVH scratch field.
-__global__ void k_viscous_a(const BlockView* __restrict__ blocks, CaseConsts cc_launch, int store_dudx_tao) {
+__device__ __forceinline__ void viscous_a_body(const BlockView* __restrict__ blocks, CaseConsts cc_launch, int store_dudx_tao) {
   const BlockView& B = blocks[blockIdx.y];
   if (B.retired()) return;
   const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
@@ -863,6 +863,17 @@ __global__ void k_viscous_a(const BlockView* __restrict__ blocks, CaseConsts cc_
     fvh[(4 * dd + 3) * P + n] = (x1 * bx + x2 * by + x3 * bz) * ij;
   }
 }
+// k_viscous_a_bound: the same under a register bound of 64 per thread (at
+// most 256 threads per CTA, 4 CTAs of 256 per SM; a few spills); the
+// autotuner chooses.
+__global__ void k_viscous_a(const BlockView* __restrict__ blocks, CaseConsts cc_launch, int store_dudx_tao) {
+  viscous_a_body(blocks, cc_launch, store_dudx_tao);
+}
+__global__ void __launch_bounds__(256, 4) k_viscous_a_bound(const BlockView* __restrict__ blocks, CaseConsts cc_launch,
+                                                             int store_dudx_tao) {
+  viscous_a_body(blocks, cc_launch, store_dudx_tao);
+}
+
 
 // Mixed-precision variant of k_viscous_a: the gradients are FP64 central
 // differences, the viscosity (Sutherland) stays FP64 since the local time step

@@ -85,6 +85,7 @@ __global__ void k_faces_wcns5(const BlockView* __restrict__ blocks, CaseConsts c
 __global__ void k_faces_sw_weno5_mixed(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_faces_wcns5_mixed(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_viscous_a(const BlockView* __restrict__ blocks, CaseConsts cc, int store_dudx_tao);
+__global__ void k_viscous_a_bound(const BlockView* __restrict__ blocks, CaseConsts cc, int store_dudx_tao);
 __global__ void k_viscous_a_mixed(const BlockView* __restrict__ blocks, CaseConsts cc, int store_dudx_tao);
 __global__ void k_viscous_b(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_find_dt(const BlockView* __restrict__ blocks, CaseConsts cc, double* cta_max);
@@ -103,6 +104,7 @@ __global__ void k_lusgs_mats_f32(const BlockView* __restrict__ blocks, CaseConst
 __global__ void k_sa_length(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_a(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_b(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_sa_b_bound(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_b_mixed(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_recs(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_sweep(const BlockView* __restrict__ blocks);

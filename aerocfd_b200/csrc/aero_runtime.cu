@@ -239,6 +239,7 @@ struct State {
     int inv_tile = 64;  // nodes per CTA of the inviscid flux; 0: face-based kernels (-6, -8: FP64 faces for 6, 8 CTAs/SM)
     int ew = 256;       // threads per CTA of the element-wise kernels
     int visc = 128;     // threads per CTA of k_viscous_a
+    int bound = 0;      // 1: the register-bounded FP64 k_viscous_a and k_sa_b
     int mats = 128;     // threads per CTA of k_lusgs_mats
     int nst_max = 4;    // most shared-memory stages of the staged sweep
     int sweep_cl = 0;   // CTAs per block of the global-memory sweep (0, 1: one CTA; 2..8: a cluster)
@@ -647,7 +648,8 @@ int launch_viscous_a(const BlockView* views, int nblk, long maxN0, const CaseCon
   if (g.mixed)
     PROF(P_VISC_A, (k_viscous_a_mixed<<<dim3(cdiv(maxN0, vt), nblk), vt, 0, g.stream>>>(views, cc, store)));
   else
-    PROF(P_VISC_A, (k_viscous_a<<<dim3(cdiv(maxN0, vt), nblk), vt, 0, g.stream>>>(views, cc, store)));
+    PROF(P_VISC_A, ((g.tune.bound ? k_viscous_a_bound : k_viscous_a)<<<dim3(cdiv(maxN0, vt), nblk), vt, 0, g.stream>>>(
+                       views, cc, store)));
   CKL();
   return AERO_OK;
 }
@@ -877,7 +879,8 @@ int launch_sa(const BlockView* views, int nblk, long maxN, long maxN1, int pmax,
     PROF_ON(P_SA_A, st, (k_sa_a<<<dim3(cdiv(maxN1, 256), nblk), 256, 0, st>>>(views, cc)));
     CKL();
     PROF_ON(P_SA_B, st,
-            ((g.mixed ? k_sa_b_mixed : k_sa_b)<<<dim3(cdiv(maxN1, 128), nblk), 128, 0, st>>>(views, cc)));
+            ((g.mixed ? k_sa_b_mixed : g.tune.bound ? k_sa_b_bound : k_sa_b)<<<dim3(cdiv(maxN1, 128), nblk), 128, 0,
+                                                                                   st>>>(views, cc)));
     CKL();
   }
   if (!(parts & 2)) return AERO_OK;
@@ -1399,9 +1402,9 @@ void set_tuning_text() {
   char buf[240];
   std::snprintf(buf, sizeof buf,
                 "inviscid_tile=%d elementwise_threads=%d viscous_threads=%d mats_threads=%d sweep_stages<=%d "
-                "sweep_cluster=%d sweep_exchange=%s sa_sweep_cluster=%d",
+                "sweep_cluster=%d sweep_exchange=%s sa_sweep_cluster=%d register_bound=%d",
                 g.tune.inv_tile, g.tune.ew, g.tune.visc, g.tune.mats, g.tune.nst_max, std::max(1, g.tune.sweep_cl),
-                exchange_name(g.tune.sweep_x), std::max(1, g.tune.sa_cl));
+                exchange_name(g.tune.sweep_x), std::max(1, g.tune.sa_cl), g.tune.bound);
   g.tuning = buf;
 }
 
@@ -1457,7 +1460,7 @@ int aero_autotune(int iters) {
   std::vector<Knob> knobs = {{&g.tune.inv_tile, {0, -6, -8, 32, 64, 128}}, {&g.tune.ew, {128, 256, 512}},
                              {&g.tune.visc, {64, 128, 256}}, {&g.tune.mats, {64, 128, 256}},
                              {&g.tune.nst_max, {2, 3, 4}},
-                             {&sweep_mode, {0, 8, 16, 32, 9, 17, 33, 10, 18, 34}}};
+                             {&sweep_mode, {0, 8, 16, 32, 9, 17, 33, 10, 18, 34}}, {&g.tune.bound, {0, 1}}};
   if (bulk_cluster16_fits()) knobs.back().cand.push_back(65);   // 16 CTAs, bulk exchange
   if (slab_cluster16_fits(5)) knobs.back().cand.push_back(66);  // 16 CTAs, slabs
   if (sa_on()) {
@@ -1551,6 +1554,16 @@ int aero_set_sweep_cluster(int ctas) {
     return fail(AERO_ERR_ARG, "a cluster of 16 sweep CTAs does not fit this device or these blocks "
                               "(16 CTAs take the bulk or the slab exchange only)");
   g.tune.sweep_cl = ctas == 1 ? 0 : ctas;
+  graph_release();
+  set_tuning_text();
+  return AERO_OK;
+}
+
+int aero_set_register_bound(int on) {
+  int rc = need_init();
+  if (rc) return rc;
+  if (on != 0 && on != 1) return fail(AERO_ERR_ARG, "register bound %d is not 0 or 1", on);
+  g.tune.bound = on;
   graph_release();
   set_tuning_text();
   return AERO_OK;

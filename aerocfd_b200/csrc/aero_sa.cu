@@ -66,7 +66,7 @@ __global__ void k_sa_a(const BlockView* __restrict__ blocks, CaseConsts cc_launc
 // Pass B over the updated box: sa_rhs = advection (sa_rhs1) + diffusion
 // (sa_rhs2) + production/destruction (sa_rhs3), in that order, and the source
 // linearisation diasd (sub_tur_sa.f90:152-208, :359-512, :561-625).
-__global__ void k_sa_b(const BlockView* __restrict__ blocks, CaseConsts cc_launch) {
+__device__ __forceinline__ void sa_b_body(const BlockView* __restrict__ blocks, CaseConsts cc_launch) {
   const BlockView& B = blocks[blockIdx.y];
   if (B.retired()) return;
   const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
@@ -161,6 +161,14 @@ __global__ void k_sa_b(const BlockView* __restrict__ blocks, CaseConsts cc_launc
             (p2(nut0) / p2(dist0)) + sdn;
   B.s(F_DIASD, n) = fmin(spn + sdn, 0.0);
 }
+// k_sa_b_bound: the same under a register bound for 10 resident CTAs of 128
+// threads per SM (more warps for the FP64 latency, a few spills); the
+// autotuner chooses.
+__global__ void k_sa_b(const BlockView* __restrict__ blocks, CaseConsts cc_launch) { sa_b_body(blocks, cc_launch); }
+__global__ void __launch_bounds__(128, 10) k_sa_b_bound(const BlockView* __restrict__ blocks, CaseConsts cc_launch) {
+  sa_b_body(blocks, cc_launch);
+}
+
 
 // k_sa_b for mixed precision (aero_set_precision(1)): the same three terms
 // with their arithmetic in FP32 -- the advection products of FP32 contravariant

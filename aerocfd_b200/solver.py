@@ -145,6 +145,11 @@ class GpuCase:
         code = {"l2": 0, "shared": 1, "slab": 2}[mode] if isinstance(mode, str) else (1 if mode else 0)
         _lib.check(self.L.aero_set_sweep_exchange(ctypes.c_int(code)), "aero_set_sweep_exchange")
 
+    def set_register_bound(self, on: bool) -> None:
+        """aero_set_register_bound: the register-bounded FP64 viscous part a
+        and SA right-hand-side kernels."""
+        _lib.check(self.L.aero_set_register_bound(ctypes.c_int(1 if on else 0)), "aero_set_register_bound")
+
     def set_sa_sweep_cluster(self, ctas: int) -> None:
         """aero_set_sa_sweep_cluster: CTAs per block of the SA sweep (1, 2, 4,
         8, 16), pipelined by k-slabs."""

@@ -112,6 +112,12 @@ module aerocfd_gpu
       integer(c_int), value :: mode
     end function
 
+    ! register-bounded FP64 viscous part a and SA right-hand-side kernels (0 / 1)
+    integer(c_int) function aero_set_register_bound(on) bind(C, name="aero_set_register_bound")
+      import :: c_int
+      integer(c_int), value :: on
+    end function
+
     ! CTAs per block of the SA sweep, pipelined by k-slabs (1, 2, 4, 8, 16)
     integer(c_int) function aero_set_sa_sweep_cluster(ctas) bind(C, name="aero_set_sa_sweep_cluster")
       import :: c_int

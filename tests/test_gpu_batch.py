@@ -104,11 +104,12 @@ def test_every_launch_shape_gives_the_same_bits(gpu, make):
               (-6, 256, 128, 128, 4), (-8, 128, 256, 64, 3)]
     for mixed in (False, True):
         ref = None
-        for shape in shapes:
+        for x, shape in enumerate(shapes):
             case = make()
             gc = gpu.GpuCase(case)
             try:
                 gc.set_tuning(*shape)
+                gc.set_register_bound(x % 2 == 1)  # the register-bounded viscous and SA kernels too
                 gc.set_precision(mixed)
                 gc.compute_geometry()
                 gc.init_flowfield()

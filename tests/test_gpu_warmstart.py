@@ -46,3 +46,37 @@ def test_warm_start_saves_iterations(solver):
         rel = np.abs(fw - fc)[[0, 1, 2, 6, 7]] / np.abs(fc)[[0, 1, 2, 6, 7]]
         print("member", i, "cold", fc[[0, 1, 2, 6, 7]], "rel diff", rel)
         assert rel.max() < 1e-3
+
+
+def test_warm_start_on_the_naca_sa_family(solver):
+    """The NACA 4-digit / SA family (config 5's parameter ranges, 4-block
+    O-grids of 4 x 65 x 33 x 3): 16 members run 1500 iterations as one
+    batch give the training fields, the network predicts 4 held-out
+    members, and the held-out batch runs 1500 iterations from the freestream
+    and from the prediction.  Every member runs without a failure; the
+    prediction starts every held-out member at under 0.8 of its cold
+    iteration-1 residual, and no member takes more iterations to fall to
+    1e-2 of it warm than cold, fewer in total."""
+    from aerocfd_b200 import grids, warmstart as W
+    fam = W.naca_family(20, seed=21, ni=65, nj=33)
+    train, test = fam[:16], fam[16:]
+    _, _, batch, st = W.run_family_batch(solver, train, 1500, chunk=50)
+    assert np.all(st == 0), st
+    cases = [c for c, _ in train]
+    X = np.concatenate([W.naca_features(*m) for m in train])
+    T = np.concatenate([W.naca_targets(grids.unbatch(batch, cases, i)) for i in range(len(train))])
+    net = W.Network(n_in=W.NACA_IN, n_out=W.NACA_OUT, width=256, depth=8, batch=8192, seed=3)
+    try:
+        loss = net.train(X, T, steps=2000, lr=1e-3)
+        assert loss[-20:].mean() < 0.1 * loss[:5].mean()
+        warm = {i: net.predict(W.naca_features(c, p)) for i, (c, p) in enumerate(test)}
+    finally:
+        net.close()
+    hc, _, _, stc = W.run_family_batch(solver, test, 1500, chunk=50)
+    hw, _, _, stw = W.run_family_batch(solver, test, 1500, chunk=50, warm=warm)
+    assert np.all(stc == 0) and np.all(stw == 0), (stc, stw)
+    ratio = hw[0] / hc[0]
+    ic, iw = W.first_below(hc, hc[0] * 1e-2, 50), W.first_below(hw, hc[0] * 1e-2, 50)
+    print("iteration-1 residual warm / cold", ratio, "iterations to 1e-2: cold", ic, "warm", iw)
+    assert np.all(ratio < 0.8)
+    assert np.all(ic > 0) and np.all(iw > 0) and np.all(iw <= ic) and iw.sum() < ic.sum()
