@@ -104,7 +104,6 @@ __global__ void k_lusgs_mats_f32(const BlockView* __restrict__ blocks, CaseConst
 __global__ void k_sa_length(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_a(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_b(const BlockView* __restrict__ blocks, CaseConsts cc);
-__global__ void k_sa_b_bound(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_b_mixed(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_recs(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_sa_sweep(const BlockView* __restrict__ blocks);

@@ -239,7 +239,7 @@ struct State {
     int inv_tile = 64;  // nodes per CTA of the inviscid flux; 0: face-based kernels (-6, -8: FP64 faces for 6, 8 CTAs/SM)
     int ew = 256;       // threads per CTA of the element-wise kernels
     int visc = 128;     // threads per CTA of k_viscous_a
-    int bound = 0;      // 1: the register-bounded FP64 k_viscous_a and k_sa_b
+    int bound = 0;      // 1: the register-bounded FP64 k_viscous_a
     int mats = 128;     // threads per CTA of k_lusgs_mats
     int nst_max = 4;    // most shared-memory stages of the staged sweep
     int sweep_cl = 0;   // CTAs per block of the global-memory sweep (0, 1: one CTA; 2..8: a cluster)
@@ -879,8 +879,7 @@ int launch_sa(const BlockView* views, int nblk, long maxN, long maxN1, int pmax,
     PROF_ON(P_SA_A, st, (k_sa_a<<<dim3(cdiv(maxN1, 256), nblk), 256, 0, st>>>(views, cc)));
     CKL();
     PROF_ON(P_SA_B, st,
-            ((g.mixed ? k_sa_b_mixed : g.tune.bound ? k_sa_b_bound : k_sa_b)<<<dim3(cdiv(maxN1, 128), nblk), 128, 0,
-                                                                                   st>>>(views, cc)));
+            ((g.mixed ? k_sa_b_mixed : k_sa_b)<<<dim3(cdiv(maxN1, 128), nblk), 128, 0, st>>>(views, cc)));
     CKL();
   }
   if (!(parts & 2)) return AERO_OK;
@@ -1461,8 +1460,11 @@ int aero_autotune(int iters) {
                              {&g.tune.visc, {64, 128, 256}}, {&g.tune.mats, {64, 128, 256}},
                              {&g.tune.nst_max, {2, 3, 4}},
                              {&sweep_mode, {0, 8, 16, 32, 9, 17, 33, 10, 18, 34}}, {&g.tune.bound, {0, 1}}};
-  if (bulk_cluster16_fits()) knobs.back().cand.push_back(65);   // 16 CTAs, bulk exchange
-  if (slab_cluster16_fits(5)) knobs.back().cand.push_back(66);  // 16 CTAs, slabs
+  for (Knob& k : knobs)
+    if (k.v == &sweep_mode) {
+      if (bulk_cluster16_fits()) k.cand.push_back(65);   // 16 CTAs, bulk exchange
+      if (slab_cluster16_fits(5)) k.cand.push_back(66);  // 16 CTAs, slabs
+    }
   if (sa_on()) {
     knobs.push_back({&g.tune.sa_cl, {0, 2, 4, 8}});
     if (slab_cluster16_fits(1)) knobs.back().cand.push_back(16);

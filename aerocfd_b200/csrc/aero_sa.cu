@@ -161,13 +161,7 @@ __device__ __forceinline__ void sa_b_body(const BlockView* __restrict__ blocks, 
             (p2(nut0) / p2(dist0)) + sdn;
   B.s(F_DIASD, n) = fmin(spn + sdn, 0.0);
 }
-// k_sa_b_bound: the same under a register bound for 10 resident CTAs of 128
-// threads per SM (more warps for the FP64 latency, a few spills); the
-// autotuner chooses.
 __global__ void k_sa_b(const BlockView* __restrict__ blocks, CaseConsts cc_launch) { sa_b_body(blocks, cc_launch); }
-__global__ void __launch_bounds__(128, 10) k_sa_b_bound(const BlockView* __restrict__ blocks, CaseConsts cc_launch) {
-  sa_b_body(blocks, cc_launch);
-}
 
 
 // k_sa_b for mixed precision (aero_set_precision(1)): the same three terms

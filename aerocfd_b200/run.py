@@ -42,7 +42,7 @@ def main(argv=None) -> int:
                     help="plane exchange of a cluster sweep (default: the autotuner's or L2)")
     ap.add_argument("--sa-sweep-cluster", type=int, default=0, help="CTAs per block of the SA sweep (0: autotune)")
     ap.add_argument("--register-bound", type=int, choices=[0, 1], default=None,
-                    help="register-bounded viscous part a and SA right-hand side (default: the autotuner's)")
+                    help="register-bounded viscous part a (default: the autotuner's)")
     ap.add_argument("--no-graphs", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes")
     ap.add_argument("--tuning", type=int, nargs=5, metavar=("INV_TILE", "EW", "VISC", "MATS", "NST"),

@@ -147,7 +147,7 @@ class GpuCase:
 
     def set_register_bound(self, on: bool) -> None:
         """aero_set_register_bound: the register-bounded FP64 viscous part a
-        and SA right-hand-side kernels."""
+        kernel."""
         _lib.check(self.L.aero_set_register_bound(ctypes.c_int(1 if on else 0)), "aero_set_register_bound")
 
     def set_sa_sweep_cluster(self, ctas: int) -> None:

@@ -112,7 +112,7 @@ module aerocfd_gpu
       integer(c_int), value :: mode
     end function
 
-    ! register-bounded FP64 viscous part a and SA right-hand-side kernels (0 / 1)
+    ! register-bounded FP64 viscous part a kernel (0 / 1)
     integer(c_int) function aero_set_register_bound(on) bind(C, name="aero_set_register_bound")
       import :: c_int
       integer(c_int), value :: on

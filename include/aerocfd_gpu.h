@@ -346,9 +346,9 @@ int aero_set_sweep_exchange(int mode);
  * after aero_finish_setup when the device can hold such a cluster).  The
  * arithmetic is the same for every choice. */
 int aero_set_sa_sweep_cluster(int ctas);
-/* 1: the FP64 viscous part a and SA right-hand-side kernels under register
- * bounds (more resident warps, a few spills); 0 (default): without.  The
- * arithmetic is the same either way; aero_autotune chooses it too. */
+/* 1: the FP64 viscous part a kernel under a register bound of 64 per thread
+ * (more resident warps, a few spills); 0 (default): without.  The arithmetic
+ * is the same either way; aero_autotune chooses it too. */
 int aero_set_register_bound(int on);
 /* Polls each bounded wait of the staged LU-SGS sweep (one CTA per block)
  * makes before it gives up, 0..1048576 (the default); each poll may suspend

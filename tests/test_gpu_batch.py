@@ -109,7 +109,7 @@ def test_every_launch_shape_gives_the_same_bits(gpu, make):
             gc = gpu.GpuCase(case)
             try:
                 gc.set_tuning(*shape)
-                gc.set_register_bound(x % 2 == 1)  # the register-bounded viscous and SA kernels too
+                gc.set_register_bound(x % 2 == 1)  # the register-bounded viscous kernel too
                 gc.set_precision(mixed)
                 gc.compute_geometry()
                 gc.init_flowfield()
