@@ -1045,7 +1045,7 @@ __device__ __forceinline__ double row_from_ring(const RowRecs& r, const double* 
 //    before any CTA leaves.  Without a failure every CTA has seen every byte
 //    sent to it before the last barrier, so no copy is in flight at exit.
 // The sweep raises ST_TIMEOUT; its values are then meaningless.
-template <typename R>
+template <typename R, int DEPTH>
 __device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ blocks, unsigned* status) {
   constexpr int W = RecFmt<R>::kWords;
   extern __shared__ __align__(16) double xring[];  // 2 halves x (G + 2) doubles
@@ -1077,8 +1077,10 @@ __device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ bl
     const int n = min(T, 5 * cnt - (int)r * T);
     return n <= 0 ? 0u : (unsigned)((n * 8 + 15) & ~15);
   };
-  RowRecs pre;
-  auto preload = [&](int gs) {
+  // this thread's row of the next DEPTH planes, loaded ahead (records and
+  // scalars are read-only during the sweep)
+  RowRecs pre0, pre1;
+  auto preload = [&](int gs, RowRecs& pre) {
     if (gs >= 2 * H) return;
     const bool fwd = gs < H;
     const long base = poff[plane_of(gs)];
@@ -1111,9 +1113,8 @@ __device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ bl
   auto failed_by = [&](int p) { return p >= 0 && *failed_at <= (unsigned)p; };
   auto fail_at = [&](int p) { atomicMin(&s_failed, (unsigned)p); };
   int armed0 = -1, armed1 = -1;  // thread 0: the last plane armed on ring half 0 / 1
-  prefetch(1);
-  preload(0);
-  for (int gs = 0; gs < 2 * H; ++gs) {
+  // one plane step with this thread's row preloaded in `pre`
+  auto step = [&](int gs, const RowRecs& pre) {
     const bool fwd = gs < H;
     const long base = poff[plane_of(gs)];
     const int cnt = count_of(gs);
@@ -1161,8 +1162,19 @@ __device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ bl
         bulk_to_cluster(map_rank(ring_local + off, threadIdx.x), ring_local + off, bytes,
                         map_rank(bar_local + boff, threadIdx.x));
     }
+  };
+  prefetch(1);
+  preload(0, pre0);
+  if (DEPTH == 2) preload(1, pre1);
+  for (int gs = 0; gs < 2 * H; gs += DEPTH) {
+    step(gs, pre0);
     prefetch(gs + 2);
-    preload(gs + 1);
+    preload(gs + DEPTH, pre0);
+    if (DEPTH == 2 && gs + 1 < 2 * H) {
+      step(gs + 1, pre1);
+      prefetch(gs + 3);
+      preload(gs + 3, pre1);
+    }
   }
   // the last plane's bytes
   if (H > 0 && !failed_by(2 * H - 1) &&
@@ -1200,11 +1212,20 @@ __device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ bl
   }
 }
 __global__ void __launch_bounds__(512, 1) k_lusgs_sweep_bulk(const BlockView* __restrict__ blocks, unsigned* status) {
-  lusgs_bulk_body<double>(blocks, status);
+  lusgs_bulk_body<double, 1>(blocks, status);
 }
 __global__ void __launch_bounds__(512, 1) k_lusgs_sweep_bulk_f32(const BlockView* __restrict__ blocks,
                                                                  unsigned* status) {
-  lusgs_bulk_body<float>(blocks, status);
+  lusgs_bulk_body<float, 1>(blocks, status);
+}
+// CTAs of at most 256 threads (a cluster's share of the largest plane's rows):
+// each thread's records loaded two planes ahead
+__global__ void __launch_bounds__(256, 1) k_lusgs_sweep_bulk2(const BlockView* __restrict__ blocks, unsigned* status) {
+  lusgs_bulk_body<double, 2>(blocks, status);
+}
+__global__ void __launch_bounds__(256, 1) k_lusgs_sweep_bulk2_f32(const BlockView* __restrict__ blocks,
+                                                                  unsigned* status) {
+  lusgs_bulk_body<float, 2>(blocks, status);
 }
 
 // ------------------------------------------------------------ slab sweeps

@@ -157,8 +157,11 @@ struct State {
   std::vector<cudaEvent_t> xfer_ev;  // host transfers: one per array of a batch, plus one
   // dynamic shared memory limits already raised on this device (cudaFuncSetAttribute
   // is per device), per sweep kernel [FP64 records, FP32 records]
-  size_t smem_staged[2] = {0, 0}, smem_bulk[2] = {0, 0};
-  bool np_cluster[2] = {false, false};  // bulk sweep: clusters of 16 CTAs allowed on this device
+  // bulk sweep (index: 0 / 1 FP64 / FP32 records, 2 / 3 the variants with
+  // loads two planes ahead): dynamic shared memory set so far, clusters of 16
+  // CTAs allowed on this device
+  size_t smem_staged[2] = {0, 0}, smem_bulk[4] = {0, 0, 0, 0};
+  bool np_cluster[4] = {false, false, false, false};
   // slab sweeps (mean flow FP64 / FP32 records, SA): dynamic shared memory
   // set so far, clusters of 16 allowed, and the launch shapes of the
   // registered blocks per (cluster size, rows per node)
@@ -788,14 +791,21 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
     const int cl = g.tune.sweep_cl;
     int threads = (int)std::max<long>(64, ((5L * pmax + cl - 1) / cl + 31) / 32 * 32);
     const size_t smem = (size_t)2 * ((size_t)cl * threads + 2) * sizeof(double);
-    auto kern = f ? k_lusgs_sweep_bulk_f32 : k_lusgs_sweep_bulk;
-    if (smem > 48 * 1024 && smem > g.smem_bulk[f]) {
+    // clusters of 16 CTAs (at most 256 threads each on planes that fit them)
+    // take the variant with loads two planes ahead; smaller clusters keep the
+    // leaner one, which leaves room for two CTAs per SM when a batch has more
+    // CTAs than SMs
+    const bool deep = cl >= 16 && threads <= 256;
+    const int k = f + (deep ? 2 : 0);
+    auto kern = deep ? (f ? k_lusgs_sweep_bulk2_f32 : k_lusgs_sweep_bulk2)
+                     : (f ? k_lusgs_sweep_bulk_f32 : k_lusgs_sweep_bulk);
+    if (smem > 48 * 1024 && smem > g.smem_bulk[k]) {
       CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      g.smem_bulk[f] = smem;
+      g.smem_bulk[k] = smem;
     }
-    if (cl > 8 && !g.np_cluster[f]) {  // 16 CTAs: a non-portable cluster size
+    if (cl > 8 && !g.np_cluster[k]) {  // 16 CTAs: a non-portable cluster size
       CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-      g.np_cluster[f] = true;
+      g.np_cluster[k] = true;
     }
     cudaLaunchConfig_t lc = {};
     lc.gridDim = dim3((unsigned)(nblk * cl));
@@ -1178,8 +1188,9 @@ const char* aero_last_error(void) { return g.err.c_str(); }
 int aero_init(int device) {
   if (g.inited) return AERO_OK;
   CK(cudaSetDevice(device));
-  for (int f = 0; f < 2; ++f) {
-    g.smem_staged[f] = g.smem_bulk[f] = 0;
+  for (int f = 0; f < 2; ++f) g.smem_staged[f] = 0;
+  for (int f = 0; f < 4; ++f) {
+    g.smem_bulk[f] = 0;
     g.np_cluster[f] = false;
   }
   CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
@@ -1327,12 +1338,14 @@ bool bulk_cluster16_fits() {
   const int threads = (int)std::max<long>(64, ((5L * g.pmax_all + cl - 1) / cl + 31) / 32 * 32);
   const size_t smem = (size_t)2 * ((size_t)cl * threads + 2) * sizeof(double);
   for (int f = 0; f < 2; ++f) {
-    auto kern = f ? k_lusgs_sweep_bulk_f32 : k_lusgs_sweep_bulk;
+    const int k = f + (threads <= 256 ? 2 : 0);
+    auto kern = threads <= 256 ? (f ? k_lusgs_sweep_bulk2_f32 : k_lusgs_sweep_bulk2)
+                               : (f ? k_lusgs_sweep_bulk_f32 : k_lusgs_sweep_bulk);
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) break;
-    g.np_cluster[f] = true;
-    if (smem > 48 * 1024 && smem > g.smem_bulk[f]) {
+    g.np_cluster[k] = true;
+    if (smem > 48 * 1024 && smem > g.smem_bulk[k]) {
       if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) break;
-      g.smem_bulk[f] = smem;
+      g.smem_bulk[k] = smem;
     }
     cudaLaunchConfig_t lc = {};
     lc.gridDim = dim3((unsigned)cl);
