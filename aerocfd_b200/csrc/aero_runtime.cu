@@ -1159,7 +1159,8 @@ int run_step() {
       return rc;
     }
     if (e != cudaSuccess) return fail(AERO_ERR_CUDA, "stream capture failed: %s", cudaGetErrorString(e));
-    e = cudaGraphInstantiate(&g.graph_exec, graph, 0);
+    // each kernel node keeps the priority of the stream it was captured from
+    e = cudaGraphInstantiate(&g.graph_exec, graph, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) {
       g.graph_exec = nullptr;
@@ -1193,10 +1194,16 @@ int aero_init(int device) {
     g.smem_bulk[f] = 0;
     g.np_cluster[f] = false;
   }
-  CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
-  CK(cudaStreamCreateWithFlags(&g.stream2, cudaStreamNonBlocking));
-  CK(cudaStreamCreateWithFlags(&g.stream3, cudaStreamNonBlocking));
-  CK(cudaStreamCreateWithFlags(&g.stream4, cudaStreamNonBlocking));
+  // The mean-flow chain (the library's stream, fed by the inviscid and the
+  // block-record streams) is the iteration's critical path; the SA stream,
+  // which has slack beside it, takes the lowest priority, so where both have
+  // CTAs waiting for an SM the block scheduler serves the mean flow first.
+  int prio_low = 0, prio_high = 0;
+  CK(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+  CK(cudaStreamCreateWithPriority(&g.stream, cudaStreamNonBlocking, prio_high));
+  CK(cudaStreamCreateWithPriority(&g.stream2, cudaStreamNonBlocking, prio_high));
+  CK(cudaStreamCreateWithPriority(&g.stream3, cudaStreamNonBlocking, prio_high));
+  CK(cudaStreamCreateWithPriority(&g.stream4, cudaStreamNonBlocking, prio_low));
   CK(cudaEventCreateWithFlags(&g.ev_join3, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&g.ev_dt, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&g.ev_fork, cudaEventDisableTiming));
