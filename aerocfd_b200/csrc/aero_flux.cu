@@ -399,6 +399,12 @@ __global__ void __launch_bounds__(128, 6) k_inviscid_faces_o6(const BlockView* _
 __global__ void __launch_bounds__(128, 8) k_inviscid_faces_o8(const BlockView* __restrict__ blocks, CaseConsts cc) {
   faces_body<false>(blocks, cc);
 }
+// The mixed-precision face kernel under a register bound for 10 resident CTAs
+// of 128 threads per SM (48 registers, a few spills).
+__global__ void __launch_bounds__(128, 10) k_inviscid_faces_mixed_o10(const BlockView* __restrict__ blocks,
+                                                                     CaseConsts cc) {
+  faces_body<true>(blocks, cc);
+}
 __global__ void k_inviscid_faces_mixed(const BlockView* __restrict__ blocks, CaseConsts cc) { faces_body<true>(blocks, cc); }
 
 __global__ void k_inviscid_combine(const BlockView* __restrict__ blocks, CaseConsts cc) {

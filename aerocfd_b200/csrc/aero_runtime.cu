@@ -628,9 +628,10 @@ int launch_inviscid(const BlockView* views, int nblk, long maxN, long maxN1, lon
     PROF_ON(P_INVISCID, st, (k_inviscid_combine<<<dim3(cdiv(maxN1, g.tune.ew), nblk), g.tune.ew, 0, st>>>(views, cc)));
   } else if (tile <= 0) {  // face-based: each face once, then the combine
     // faces per direction <= updated box grown by one node in that direction
-    // (tile -6 / -8: the FP64 kernel under a register bound for 6 / 8 CTAs per SM)
+    // (tile -6 / -8: the FP64 kernel under a register bound for 6 / 8 CTAs per
+    // SM; in mixed precision both take the mixed kernel bounded for 10)
     long maxF = maxN1 + maxFace;
-    auto faces = g.mixed ? k_inviscid_faces_mixed
+    auto faces = g.mixed ? (tile < 0 ? k_inviscid_faces_mixed_o10 : k_inviscid_faces_mixed)
                          : (tile == -6 ? k_inviscid_faces_o6 : tile == -8 ? k_inviscid_faces_o8 : k_inviscid_faces);
     PROF_ON(P_INVISCID, st, (faces<<<dim3(cdiv(maxF, 128), nblk, 3), 128, 0, st>>>(views, cc)));
     CKL();

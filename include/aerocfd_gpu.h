@@ -320,7 +320,8 @@ int aero_autotune(int iters);
 const char* aero_tuning(void);
 /* Sets the launch shapes directly (e.g. to apply a saved tuning): inviscid
  * tile 0 (face-based kernels; -6 / -8: the FP64 face kernel under a register
- * bound for 6 / 8 CTAs per SM), 32, 64 or 128; element-wise threads 128, 256,
+ * bound for 6 / 8 CTAs per SM, and in mixed precision the mixed face kernel
+ * bounded for 10), 32, 64 or 128; element-wise threads 128, 256,
  * 512; viscous and block-record threads 64, 128, 256; sweep stages 2..4. */
 int aero_set_tuning(int inv_tile, int ew, int visc, int mats, int nst_max);
 /* CTAs that share each block's LU-SGS sweep: 1 (one CTA per block, the
