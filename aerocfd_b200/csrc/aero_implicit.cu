@@ -1218,6 +1218,16 @@ __global__ void __launch_bounds__(512, 1) k_lusgs_sweep_bulk_f32(const BlockView
                                                                  unsigned* status) {
   lusgs_bulk_body<float, 1>(blocks, status);
 }
+// CTAs of at most 384 threads, two resident per SM (80 registers): for
+// batches whose sweep CTAs outnumber the SMs
+__global__ void __launch_bounds__(384, 2) k_lusgs_sweep_bulk_o2(const BlockView* __restrict__ blocks,
+                                                                unsigned* status) {
+  lusgs_bulk_body<double, 1>(blocks, status);
+}
+__global__ void __launch_bounds__(384, 2) k_lusgs_sweep_bulk_o2_f32(const BlockView* __restrict__ blocks,
+                                                                    unsigned* status) {
+  lusgs_bulk_body<float, 1>(blocks, status);
+}
 // CTAs of at most 256 threads (a cluster's share of the largest plane's rows):
 // each thread's records loaded two planes ahead
 __global__ void __launch_bounds__(256, 1) k_lusgs_sweep_bulk2(const BlockView* __restrict__ blocks, unsigned* status) {

@@ -122,6 +122,9 @@ __global__ void k_lusgs_sweep_cluster_f32(const BlockView* __restrict__ blocks);
 // cluster sweeps exchanging plane values by bulk copies between shared memories
 __global__ void k_lusgs_sweep_bulk(const BlockView* __restrict__ blocks, unsigned* status);
 __global__ void k_lusgs_sweep_bulk_f32(const BlockView* __restrict__ blocks, unsigned* status);
+// the same for CTAs of at most 384 threads, two resident per SM
+__global__ void k_lusgs_sweep_bulk_o2(const BlockView* __restrict__ blocks, unsigned* status);
+__global__ void k_lusgs_sweep_bulk_o2_f32(const BlockView* __restrict__ blocks, unsigned* status);
 // the same for CTAs of at most 256 threads, records loaded two planes ahead
 __global__ void k_lusgs_sweep_bulk2(const BlockView* __restrict__ blocks, unsigned* status);
 __global__ void k_lusgs_sweep_bulk2_f32(const BlockView* __restrict__ blocks, unsigned* status);

@@ -158,10 +158,10 @@ struct State {
   // dynamic shared memory limits already raised on this device (cudaFuncSetAttribute
   // is per device), per sweep kernel [FP64 records, FP32 records]
   // bulk sweep (index: 0 / 1 FP64 / FP32 records, 2 / 3 the variants with
-  // loads two planes ahead): dynamic shared memory set so far, clusters of 16
-  // CTAs allowed on this device
-  size_t smem_staged[2] = {0, 0}, smem_bulk[4] = {0, 0, 0, 0};
-  bool np_cluster[4] = {false, false, false, false};
+  // loads two planes ahead, 4 / 5 the ones with two CTAs per SM): dynamic
+  // shared memory set so far, clusters of 16 CTAs allowed on this device
+  size_t smem_staged[2] = {0, 0}, smem_bulk[6] = {0, 0, 0, 0, 0, 0};
+  bool np_cluster[6] = {false, false, false, false, false, false};
   // slab sweeps (mean flow FP64 / FP32 records, SA): dynamic shared memory
   // set so far, clusters of 16 allowed, and the launch shapes of the
   // registered blocks per (cluster size, rows per node)
@@ -797,9 +797,12 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
     // leaner one, which leaves room for two CTAs per SM when a batch has more
     // CTAs than SMs
     const bool deep = cl >= 16 && threads <= 256;
-    const int k = f + (deep ? 2 : 0);
-    auto kern = deep ? (f ? k_lusgs_sweep_bulk2_f32 : k_lusgs_sweep_bulk2)
-                     : (f ? k_lusgs_sweep_bulk_f32 : k_lusgs_sweep_bulk);
+    // exchange 3: two CTAs per SM (80 registers) where the rows fit 384 threads
+    const bool two = !deep && g.tune.sweep_x == 3 && threads <= 384;
+    const int k = f + (deep ? 2 : two ? 4 : 0);
+    auto kern = deep  ? (f ? k_lusgs_sweep_bulk2_f32 : k_lusgs_sweep_bulk2)
+                : two ? (f ? k_lusgs_sweep_bulk_o2_f32 : k_lusgs_sweep_bulk_o2)
+                      : (f ? k_lusgs_sweep_bulk_f32 : k_lusgs_sweep_bulk);
     if (smem > 48 * 1024 && smem > g.smem_bulk[k]) {
       CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       g.smem_bulk[k] = smem;
@@ -1191,7 +1194,7 @@ int aero_init(int device) {
   if (g.inited) return AERO_OK;
   CK(cudaSetDevice(device));
   for (int f = 0; f < 2; ++f) g.smem_staged[f] = 0;
-  for (int f = 0; f < 4; ++f) {
+  for (int f = 0; f < 6; ++f) {
     g.smem_bulk[f] = 0;
     g.np_cluster[f] = false;
   }
@@ -1416,7 +1419,7 @@ bool slab_cluster16_fits(int rows) {
   return true;
 }
 
-const char* exchange_name(int x) { return x == 2 ? "slab" : x == 1 ? "shared" : "l2"; }
+const char* exchange_name(int x) { return x == 3 ? "shared2" : x == 2 ? "slab" : x == 1 ? "shared" : "l2"; }
 
 void set_tuning_text() {
   char buf[240];
@@ -1480,7 +1483,8 @@ int aero_autotune(int iters) {
   std::vector<Knob> knobs = {{&g.tune.inv_tile, {0, -6, -8, 32, 64, 128}}, {&g.tune.ew, {128, 256, 512}},
                              {&g.tune.visc, {64, 128, 256}}, {&g.tune.mats, {64, 128, 256}},
                              {&g.tune.nst_max, {2, 3, 4}},
-                             {&sweep_mode, {0, 8, 16, 32, 9, 17, 33, 10, 18, 34}}, {&g.tune.bound, {0, 1}}};
+                             {&sweep_mode, {0, 8, 16, 32, 9, 17, 33, 10, 18, 34, 11, 19, 35}},
+                             {&g.tune.bound, {0, 1}}};
   for (Knob& k : knobs)
     if (k.v == &sweep_mode) {
       if (bulk_cluster16_fits()) k.cand.push_back(65);   // 16 CTAs, bulk exchange
@@ -1560,8 +1564,10 @@ int aero_inject_sweep_stall(int plane) {
 int aero_set_sweep_exchange(int mode) {
   int rc = need_init();
   if (rc) return rc;
-  if (mode < 0 || mode > 2)
-    return fail(AERO_ERR_ARG, "sweep exchange %d is not 0 (L2), 1 (shared memory) or 2 (pipelined k-slabs)", mode);
+  if (mode < 0 || mode > 3)
+    return fail(AERO_ERR_ARG,
+                "sweep exchange %d is not 0 (L2), 1 (shared memory), 2 (pipelined k-slabs) or 3 (shared memory, "
+                "two CTAs per SM)", mode);
   g.tune.sweep_x = mode;
   graph_release();
   set_tuning_text();

@@ -38,7 +38,7 @@ def main(argv=None) -> int:
     ap.add_argument("--inviscid", type=int, default=4, help="4 Roe + WENO3, 5 SW + WENO5, 8 WCNS5")
     ap.add_argument("--mixed", action="store_true")
     ap.add_argument("--sweep-cluster", type=int, default=0, help="CTAs per block of the LU-SGS sweep (0: autotune)")
-    ap.add_argument("--sweep-exchange", choices=["l2", "shared", "slab"], default=None,
+    ap.add_argument("--sweep-exchange", choices=["l2", "shared", "slab", "shared2"], default=None,
                     help="plane exchange of a cluster sweep (default: the autotuner's or L2)")
     ap.add_argument("--sa-sweep-cluster", type=int, default=0, help="CTAs per block of the SA sweep (0: autotune)")
     ap.add_argument("--register-bound", type=int, choices=[0, 1], default=None,

@@ -140,9 +140,10 @@ class GpuCase:
 
     def set_sweep_exchange(self, mode) -> None:
         """aero_set_sweep_exchange: how a cluster shares a sweep: "l2" (or
-        False), "shared" (or True: bulk copies between shared memories) or
-        "slab" (CTAs pipelined by k-slabs)."""
-        code = {"l2": 0, "shared": 1, "slab": 2}[mode] if isinstance(mode, str) else (1 if mode else 0)
+        False), "shared" (or True: bulk copies between shared memories),
+        "slab" (CTAs pipelined by k-slabs) or "shared2" (bulk copies, two CTAs
+        per SM)."""
+        code = {"l2": 0, "shared": 1, "slab": 2, "shared2": 3}[mode] if isinstance(mode, str) else (1 if mode else 0)
         _lib.check(self.L.aero_set_sweep_exchange(ctypes.c_int(code)), "aero_set_sweep_exchange")
 
     def set_register_bound(self, on: bool) -> None:

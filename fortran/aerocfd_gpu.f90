@@ -105,8 +105,8 @@ module aerocfd_gpu
     end function
 
     ! plane-value exchange of a cluster sweep: 0 through L2, 1 bulk copies
-    ! between shared memories, 2 pipelined k-slabs (no counterpart in the
-    ! reference)
+    ! between shared memories, 2 pipelined k-slabs, 3 as 1 with two CTAs per
+    ! SM (no counterpart in the reference)
     integer(c_int) function aero_set_sweep_exchange(mode) bind(C, name="aero_set_sweep_exchange")
       import :: c_int
       integer(c_int), value :: mode

@@ -338,8 +338,9 @@ int aero_set_sweep_cluster(int ctas);
  * thread: 5 x plane nodes <= 512 x CTAs); 2 every CTA one range of k
  * (a k-slab), the CTAs pipelined plane by plane, each passing only its edge
  * k-segment's values to the next CTA (used when each slab's part of a plane
- * has at most 102 nodes; else 1).  The arithmetic is the same for every
- * choice. */
+ * has at most 102 nodes; else 1); 3 as 1 with CTAs of at most 384 threads
+ * built for two resident per SM (for batches whose sweep CTAs outnumber the
+ * SMs; larger CTAs take 1).  The arithmetic is the same for every choice. */
 int aero_set_sweep_exchange(int mode);
 /* CTAs that share each block's SA sweep: 1 (default; one CTA per block) or a
  * cluster of 2, 4 or 8 CTAs pipelined by k-slabs as exchange 2 above (used

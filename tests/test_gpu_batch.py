@@ -147,7 +147,7 @@ def test_sweep_cluster_gives_the_same_bits(gpu, make):
         for ctas, exch, sa_ctas in ((1, "l2", 1), (2, "l2", 1), (4, "l2", 1), (8, "l2", 1), (2, "shared", 1),
                                     (4, "shared", 1), (8, "shared", 1), (16, "shared", 1), (2, "slab", 2),
                                     (4, "slab", 4), (8, "slab", 8), (16, "slab", 16), (8, "slab", 1),
-                                    (1, "l2", 4)):
+                                    (1, "l2", 4), (4, "shared2", 1), (8, "shared2", 2)):
             case = make()
             gc = gpu.GpuCase(case)
             try:

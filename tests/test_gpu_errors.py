@@ -56,7 +56,7 @@ def test_supported_extensions_are_accepted(lib):
 
 def test_launch_options_outside_their_sets(lib):
     assert lib.aero_set_sweep_cluster(ctypes.c_int(3)) == ERR_ARG
-    assert lib.aero_set_sweep_exchange(ctypes.c_int(3)) == ERR_ARG
+    assert lib.aero_set_sweep_exchange(ctypes.c_int(4)) == ERR_ARG
     assert lib.aero_set_sa_sweep_cluster(ctypes.c_int(3)) == ERR_ARG
     assert lib.aero_set_precision(ctypes.c_int(2)) == ERR_ARG
     assert lib.aero_set_tuning(ctypes.c_int(48), ctypes.c_int(256), ctypes.c_int(128), ctypes.c_int(128),
