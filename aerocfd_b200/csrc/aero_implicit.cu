@@ -1046,7 +1046,7 @@ __device__ __forceinline__ double row_from_ring(const RowRecs& r, const double* 
 //    sent to it before the last barrier, so no copy is in flight at exit.
 // The sweep raises ST_TIMEOUT; its values are then meaningless.
 template <typename R, int DEPTH>
-__device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ blocks, unsigned* status) {
+__device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ blocks, unsigned* status, int pf) {
   constexpr int W = RecFmt<R>::kWords;
   extern __shared__ __align__(16) double xring[];  // 2 halves x (G + 2) doubles
   __shared__ __align__(8) unsigned long long xbar[2];
@@ -1089,7 +1089,7 @@ __device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ bl
   };
   // L2 prefetch of plane gs's records and scalars (and, backward, dq*): each
   // CTA asks for its 1/ncta share of each chunk, so the whole chunk is in L2
-  // before preload() reads it a plane later.  Every chunk starts and ends on a
+  // before preload() reads it (pf - 1 planes later, pf >= 2, a kernel argument).  Every chunk starts and ends on a
   // 16-byte boundary (W * sizeof(R), kSca * 8 and 8 * 8 bytes per node are
   // multiples of 16), and so does every share.
   auto prefetch = [&](int gs) {
@@ -1163,16 +1163,17 @@ __device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ bl
                         map_rank(bar_local + boff, threadIdx.x));
     }
   };
-  prefetch(1);
+  // planes 1 .. pf-1 now, then plane gs+pf after each step gs (pf >= 2)
+  for (int x = 1; x < pf; ++x) prefetch(x);
   preload(0, pre0);
   if (DEPTH == 2) preload(1, pre1);
   for (int gs = 0; gs < 2 * H; gs += DEPTH) {
     step(gs, pre0);
-    prefetch(gs + 2);
+    prefetch(gs + pf);
     preload(gs + DEPTH, pre0);
     if (DEPTH == 2 && gs + 1 < 2 * H) {
       step(gs + 1, pre1);
-      prefetch(gs + 3);
+      prefetch(gs + 1 + pf);
       preload(gs + 3, pre1);
     }
   }
@@ -1211,31 +1212,33 @@ __device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ bl
     __syncthreads();
   }
 }
-__global__ void __launch_bounds__(512, 1) k_lusgs_sweep_bulk(const BlockView* __restrict__ blocks, unsigned* status) {
-  lusgs_bulk_body<double, 1>(blocks, status);
+__global__ void __launch_bounds__(512, 1) k_lusgs_sweep_bulk(const BlockView* __restrict__ blocks, unsigned* status,
+                                                             int pf) {
+  lusgs_bulk_body<double, 1>(blocks, status, pf);
 }
 __global__ void __launch_bounds__(512, 1) k_lusgs_sweep_bulk_f32(const BlockView* __restrict__ blocks,
-                                                                 unsigned* status) {
-  lusgs_bulk_body<float, 1>(blocks, status);
+                                                                 unsigned* status, int pf) {
+  lusgs_bulk_body<float, 1>(blocks, status, pf);
 }
 // CTAs of at most 384 threads, two resident per SM (80 registers): for
 // batches whose sweep CTAs outnumber the SMs
 __global__ void __launch_bounds__(384, 2) k_lusgs_sweep_bulk_o2(const BlockView* __restrict__ blocks,
-                                                                unsigned* status) {
-  lusgs_bulk_body<double, 1>(blocks, status);
+                                                                unsigned* status, int pf) {
+  lusgs_bulk_body<double, 1>(blocks, status, pf);
 }
 __global__ void __launch_bounds__(384, 2) k_lusgs_sweep_bulk_o2_f32(const BlockView* __restrict__ blocks,
-                                                                    unsigned* status) {
-  lusgs_bulk_body<float, 1>(blocks, status);
+                                                                    unsigned* status, int pf) {
+  lusgs_bulk_body<float, 1>(blocks, status, pf);
 }
 // CTAs of at most 256 threads (a cluster's share of the largest plane's rows):
 // each thread's records loaded two planes ahead
-__global__ void __launch_bounds__(256, 1) k_lusgs_sweep_bulk2(const BlockView* __restrict__ blocks, unsigned* status) {
-  lusgs_bulk_body<double, 2>(blocks, status);
+__global__ void __launch_bounds__(256, 1) k_lusgs_sweep_bulk2(const BlockView* __restrict__ blocks, unsigned* status,
+                                                              int pf) {
+  lusgs_bulk_body<double, 2>(blocks, status, pf);
 }
 __global__ void __launch_bounds__(256, 1) k_lusgs_sweep_bulk2_f32(const BlockView* __restrict__ blocks,
-                                                                  unsigned* status) {
-  lusgs_bulk_body<float, 2>(blocks, status);
+                                                                  unsigned* status, int pf) {
+  lusgs_bulk_body<float, 2>(blocks, status, pf);
 }
 
 // ------------------------------------------------------------ slab sweeps

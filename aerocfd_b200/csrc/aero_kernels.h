@@ -120,14 +120,14 @@ __global__ void k_lusgs_sweep_staged_f32(const BlockView* __restrict__ blocks, i
 __global__ void k_lusgs_sweep_global_f32(const BlockView* __restrict__ blocks, int nst, unsigned* status);
 __global__ void k_lusgs_sweep_cluster_f32(const BlockView* __restrict__ blocks);
 // cluster sweeps exchanging plane values by bulk copies between shared memories
-__global__ void k_lusgs_sweep_bulk(const BlockView* __restrict__ blocks, unsigned* status);
-__global__ void k_lusgs_sweep_bulk_f32(const BlockView* __restrict__ blocks, unsigned* status);
+__global__ void k_lusgs_sweep_bulk(const BlockView* __restrict__ blocks, unsigned* status, int pf);
+__global__ void k_lusgs_sweep_bulk_f32(const BlockView* __restrict__ blocks, unsigned* status, int pf);
 // the same for CTAs of at most 384 threads, two resident per SM
-__global__ void k_lusgs_sweep_bulk_o2(const BlockView* __restrict__ blocks, unsigned* status);
-__global__ void k_lusgs_sweep_bulk_o2_f32(const BlockView* __restrict__ blocks, unsigned* status);
+__global__ void k_lusgs_sweep_bulk_o2(const BlockView* __restrict__ blocks, unsigned* status, int pf);
+__global__ void k_lusgs_sweep_bulk_o2_f32(const BlockView* __restrict__ blocks, unsigned* status, int pf);
 // the same for CTAs of at most 256 threads, records loaded two planes ahead
-__global__ void k_lusgs_sweep_bulk2(const BlockView* __restrict__ blocks, unsigned* status);
-__global__ void k_lusgs_sweep_bulk2_f32(const BlockView* __restrict__ blocks, unsigned* status);
+__global__ void k_lusgs_sweep_bulk2(const BlockView* __restrict__ blocks, unsigned* status, int pf);
+__global__ void k_lusgs_sweep_bulk2_f32(const BlockView* __restrict__ blocks, unsigned* status, int pf);
 // cluster sweeps pipelined by k-slabs (D slots: rings of 5 x So values, edge
 // inboxes and staging areas of 5 x L values)
 __global__ void k_lusgs_sweep_slab(const BlockView* __restrict__ blocks, unsigned* status, int So, int L, int D);

@@ -249,6 +249,7 @@ struct State {
     int sweep_x = 0;    // cluster exchange: 0 through L2, 1 bulk copies between shared memories (when it fits),
                         // 2 pipelined k-slabs (when it fits; else 1)
     int sa_cl = 0;      // CTAs per block of the SA sweep (0, 1: one CTA; 2..16: a cluster pipelined by k-slabs)
+    int sweep_pf = 2;   // L2 prefetch distance of the bulk-exchange sweep, in planes (2..4)
   } tune;
   // CUDA graph of one time step (aero_use_graphs)
   bool graph_want = false;
@@ -824,7 +825,7 @@ int launch_implicit(const BlockView* views, int nblk, long maxExt, long maxN1, i
     lc.attrs = at;
     lc.numAttrs = 1;
     cudaError_t le = cudaSuccess;
-    PROF(P_LUSGS_SWEEP, (le = cudaLaunchKernelEx(&lc, kern, sv, g.d_status)));
+    PROF(P_LUSGS_SWEEP, (le = cudaLaunchKernelEx(&lc, kern, sv, g.d_status, g.tune.sweep_pf)));
     CK(le);
   } else if (g.tune.sweep_cl >= 2) {
     // one cluster of sweep_cl CTAs per block, one thread per row of every
@@ -1422,12 +1423,12 @@ bool slab_cluster16_fits(int rows) {
 const char* exchange_name(int x) { return x == 3 ? "shared2" : x == 2 ? "slab" : x == 1 ? "shared" : "l2"; }
 
 void set_tuning_text() {
-  char buf[240];
+  char buf[280];
   std::snprintf(buf, sizeof buf,
                 "inviscid_tile=%d elementwise_threads=%d viscous_threads=%d mats_threads=%d sweep_stages<=%d "
-                "sweep_cluster=%d sweep_exchange=%s sa_sweep_cluster=%d register_bound=%d",
+                "sweep_cluster=%d sweep_exchange=%s sa_sweep_cluster=%d register_bound=%d sweep_prefetch=%d",
                 g.tune.inv_tile, g.tune.ew, g.tune.visc, g.tune.mats, g.tune.nst_max, std::max(1, g.tune.sweep_cl),
-                exchange_name(g.tune.sweep_x), std::max(1, g.tune.sa_cl), g.tune.bound);
+                exchange_name(g.tune.sweep_x), std::max(1, g.tune.sa_cl), g.tune.bound, g.tune.sweep_pf);
   g.tuning = buf;
 }
 
@@ -1484,7 +1485,7 @@ int aero_autotune(int iters) {
                              {&g.tune.visc, {64, 128, 256}}, {&g.tune.mats, {64, 128, 256}},
                              {&g.tune.nst_max, {2, 3, 4}},
                              {&sweep_mode, {0, 8, 16, 32, 9, 17, 33, 10, 18, 34, 11, 19, 35}},
-                             {&g.tune.bound, {0, 1}}};
+                             {&g.tune.bound, {0, 1}}, {&g.tune.sweep_pf, {2, 3, 4}}};
   for (Knob& k : knobs)
     if (k.v == &sweep_mode) {
       if (bulk_cluster16_fits()) k.cand.push_back(65);   // 16 CTAs, bulk exchange
@@ -1583,6 +1584,16 @@ int aero_set_sweep_cluster(int ctas) {
     return fail(AERO_ERR_ARG, "a cluster of 16 sweep CTAs does not fit this device or these blocks "
                               "(16 CTAs take the bulk or the slab exchange only)");
   g.tune.sweep_cl = ctas == 1 ? 0 : ctas;
+  graph_release();
+  set_tuning_text();
+  return AERO_OK;
+}
+
+int aero_set_sweep_prefetch(int planes) {
+  int rc = need_init();
+  if (rc) return rc;
+  if (planes < 2 || planes > 4) return fail(AERO_ERR_ARG, "sweep prefetch distance %d is outside 2..4", planes);
+  g.tune.sweep_pf = planes;
   graph_release();
   set_tuning_text();
   return AERO_OK;

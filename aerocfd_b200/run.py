@@ -41,6 +41,8 @@ def main(argv=None) -> int:
     ap.add_argument("--sweep-exchange", choices=["l2", "shared", "slab", "shared2"], default=None,
                     help="plane exchange of a cluster sweep (default: the autotuner's or L2)")
     ap.add_argument("--sa-sweep-cluster", type=int, default=0, help="CTAs per block of the SA sweep (0: autotune)")
+    ap.add_argument("--sweep-prefetch", type=int, choices=[2, 3, 4], default=0,
+                    help="L2 prefetch distance of the bulk-exchange sweep (default: the autotuner's)")
     ap.add_argument("--register-bound", type=int, choices=[0, 1], default=None,
                     help="register-bounded viscous part a (default: the autotuner's)")
     ap.add_argument("--no-graphs", action="store_true")
@@ -68,6 +70,8 @@ def main(argv=None) -> int:
             gc.set_sa_sweep_cluster(args.sa_sweep_cluster)
         if args.register_bound is not None:
             gc.set_register_bound(args.register_bound == 1)
+        if args.sweep_prefetch:
+            gc.set_sweep_prefetch(args.sweep_prefetch)
         gc.use_graphs(not args.no_graphs)
         gc.step(args.warmup, history=False)
         ms = ctypes.c_double(0.0)

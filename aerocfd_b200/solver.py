@@ -146,6 +146,11 @@ class GpuCase:
         code = {"l2": 0, "shared": 1, "slab": 2, "shared2": 3}[mode] if isinstance(mode, str) else (1 if mode else 0)
         _lib.check(self.L.aero_set_sweep_exchange(ctypes.c_int(code)), "aero_set_sweep_exchange")
 
+    def set_sweep_prefetch(self, planes: int) -> None:
+        """aero_set_sweep_prefetch: L2 prefetch distance of the bulk-exchange
+        sweep (2..4 planes)."""
+        _lib.check(self.L.aero_set_sweep_prefetch(ctypes.c_int(planes)), "aero_set_sweep_prefetch")
+
     def set_register_bound(self, on: bool) -> None:
         """aero_set_register_bound: the register-bounded FP64 viscous part a
         kernel."""

@@ -112,6 +112,12 @@ module aerocfd_gpu
       integer(c_int), value :: mode
     end function
 
+    ! L2 prefetch distance of the bulk-exchange sweep in planes (2..4)
+    integer(c_int) function aero_set_sweep_prefetch(planes) bind(C, name="aero_set_sweep_prefetch")
+      import :: c_int
+      integer(c_int), value :: planes
+    end function
+
     ! register-bounded FP64 viscous part a kernel (0 / 1)
     integer(c_int) function aero_set_register_bound(on) bind(C, name="aero_set_register_bound")
       import :: c_int

@@ -352,6 +352,10 @@ int aero_set_sa_sweep_cluster(int ctas);
  * (more resident warps, a few spills); 0 (default): without.  The arithmetic
  * is the same either way; aero_autotune chooses it too. */
 int aero_set_register_bound(int on);
+/* Planes ahead (2, the default, 3 or 4) at which the bulk-exchange sweep's
+ * CTAs prefetch their shares of the plane records into L2.  Results are the
+ * same for every choice; aero_autotune chooses it too. */
+int aero_set_sweep_prefetch(int planes);
 /* Polls each bounded wait of the staged LU-SGS sweep (one CTA per block)
  * makes before it gives up, 0..1048576 (the default); each poll may suspend
  * the waiting thread for a short, system-dependent time.  A wait that gives

@@ -147,12 +147,15 @@ def test_sweep_cluster_gives_the_same_bits(gpu, make):
         for ctas, exch, sa_ctas in ((1, "l2", 1), (2, "l2", 1), (4, "l2", 1), (8, "l2", 1), (2, "shared", 1),
                                     (4, "shared", 1), (8, "shared", 1), (16, "shared", 1), (2, "slab", 2),
                                     (4, "slab", 4), (8, "slab", 8), (16, "slab", 16), (8, "slab", 1),
-                                    (1, "l2", 4), (4, "shared2", 1), (8, "shared2", 2)):
+                                    (1, "l2", 4), (4, "shared2", 1), (8, "shared2", 2), (8, "shared", 0)):
             case = make()
             gc = gpu.GpuCase(case)
             try:
                 try:
                     gc.set_sweep_cluster(ctas)
+                    if sa_ctas == 0:  # the bulk sweep prefetching four planes ahead
+                        gc.set_sweep_prefetch(4)
+                        sa_ctas = 1
                     gc.set_sa_sweep_cluster(sa_ctas)
                 except _lib.AeroError:
                     assert 16 in (ctas, sa_ctas)  # the device holds no 16-CTA cluster
