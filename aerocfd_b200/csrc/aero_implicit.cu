@@ -833,7 +833,6 @@ __device__ __forceinline__ double lusgs_row_l2(const R* rec, const double* sca, 
 struct RowRecs {
   double packed, m[15], rhs, diag, invj, rdiag, rinvj;
   int row, node;
-  bool bok;  // divisors in div2_rn's fast range
 };
 template <typename R>
 __device__ __forceinline__ void load_row_recs(const R* rec, const double* sca, int cnt, int t, RowRecs& r) {
@@ -851,7 +850,8 @@ __device__ __forceinline__ void load_row_recs(const R* rec, const double* sca, i
   r.invj = sn[6 * cnt];
   r.rdiag = sn[7 * cnt];
   r.rinvj = sn[8 * cnt];
-  r.bok = !nbr_slow_div(r.packed);
+  // (the divisor flag in `packed` is read where the row is computed, so that
+  // this load of the next plane's row does not wait for its data)
 }
 // lusgs_rows' arithmetic for one row from preloaded records; the previous
 // plane's dq and dq* are loaded from L2 (written by other SMs during the sweep).
@@ -873,9 +873,9 @@ __device__ __forceinline__ double row_from_recs(const RowRecs& r, const double* 
     }
     acc[d] = sd;
   }
-  if (FWD) return div2_rn(r.rhs + (acc[0] + acc[1] + acc[2]), r.diag, r.rdiag, r.invj, r.rinvj, r.bok);
-  return __ldcg(dsv + r.row * cnt + r.node) -
-         div2_rn(acc[0] + acc[1] + acc[2], r.invj, r.rinvj, r.diag, r.rdiag, r.bok);
+  const bool bok = !nbr_slow_div(r.packed);  // divisors in div2_rn's fast range
+  if (FWD) return div2_rn(r.rhs + (acc[0] + acc[1] + acc[2]), r.diag, r.rdiag, r.invj, r.rinvj, bok);
+  return __ldcg(dsv + r.row * cnt + r.node) - div2_rn(acc[0] + acc[1] + acc[2], r.invj, r.rinvj, r.diag, r.rdiag, bok);
 }
 
 // The global-memory sweeps of one block spread over a thread-block cluster
@@ -1008,9 +1008,9 @@ __device__ __forceinline__ double row_from_ring(const RowRecs& r, const double* 
     }
     acc[d] = sd;
   }
-  if (FWD) return div2_rn(r.rhs + (acc[0] + acc[1] + acc[2]), r.diag, r.rdiag, r.invj, r.rinvj, r.bok);
-  return __ldcg(dsv + r.row * cnt + r.node) -
-         div2_rn(acc[0] + acc[1] + acc[2], r.invj, r.rinvj, r.diag, r.rdiag, r.bok);
+  const bool bok = !nbr_slow_div(r.packed);  // divisors in div2_rn's fast range
+  if (FWD) return div2_rn(r.rhs + (acc[0] + acc[1] + acc[2]), r.diag, r.rdiag, r.invj, r.rinvj, bok);
+  return __ldcg(dsv + r.row * cnt + r.node) - div2_rn(acc[0] + acc[1] + acc[2], r.invj, r.rinvj, r.diag, r.rdiag, bok);
 }
 
 }  // namespace
@@ -1249,7 +1249,6 @@ namespace {
 struct SlabRow {
   double packed, m[15], rhs, diag, invj, rdiag, rinvj, dsv;
   int row, node;
-  bool bok;  // divisors in div2_rn's fast range
 };
 template <typename R>
 __device__ __forceinline__ void load_slab_row(const BlockView& B, bool fwd, long base, int cnt, int row, int node,
@@ -1273,7 +1272,8 @@ __device__ __forceinline__ void load_slab_row(const BlockView& B, bool fwd, long
   // dq* of the node, written by this CTA in the forward pass (read from L2;
   // complete once the forward pass has passed the node's plane)
   r.dsv = fwd ? 0.0 : __ldcg(B.dqs + 8 * base + row * cnt + node);
-  r.bok = !nbr_slow_div(r.packed);
+  // (the divisor flag in `packed` is read where the row is computed, so that
+  // this load ahead does not wait for its data)
 }
 // lusgs_rows' arithmetic for one row from preloaded records.  The previous
 // plane's values: row c of plane-local node w at own[c*So + w - o0] for the
@@ -1300,8 +1300,9 @@ __device__ __forceinline__ double row_from_slab(const SlabRow& r, const double* 
     }
     acc[d] = sd;
   }
-  if (FWD) return div2_rn(r.rhs + (acc[0] + acc[1] + acc[2]), r.diag, r.rdiag, r.invj, r.rinvj, r.bok);
-  return dsv - div2_rn(acc[0] + acc[1] + acc[2], r.invj, r.rinvj, r.diag, r.rdiag, r.bok);
+  const bool bok = !nbr_slow_div(r.packed);  // divisors in div2_rn's fast range
+  if (FWD) return div2_rn(r.rhs + (acc[0] + acc[1] + acc[2]), r.diag, r.rdiag, r.invj, r.rinvj, bok);
+  return dsv - div2_rn(acc[0] + acc[1] + acc[2], r.invj, r.rinvj, r.diag, r.rdiag, bok);
 }
 
 }  // namespace
