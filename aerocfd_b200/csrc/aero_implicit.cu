@@ -1163,20 +1163,17 @@ __device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ bl
                         map_rank(bar_local + boff, threadIdx.x));
     }
   };
-  // planes 1 .. pf-1 now, then plane gs+pf at the start of each step gs (pf
-  // >= 2): the prefetch goes to this SM's copy engine ahead of the wait, so
-  // that the plane's slice copies to the other CTAs, issued after the step's
-  // barrier, do not queue behind it
+  // planes 1 .. pf-1 now, then plane gs+pf after each step gs (pf >= 2)
   for (int x = 1; x < pf; ++x) prefetch(x);
   preload(0, pre0);
   if (DEPTH == 2) preload(1, pre1);
   for (int gs = 0; gs < 2 * H; gs += DEPTH) {
-    prefetch(gs + pf);
     step(gs, pre0);
+    prefetch(gs + pf);
     preload(gs + DEPTH, pre0);
     if (DEPTH == 2 && gs + 1 < 2 * H) {
-      prefetch(gs + 1 + pf);
       step(gs + 1, pre1);
+      prefetch(gs + 1 + pf);
       preload(gs + 3, pre1);
     }
   }
