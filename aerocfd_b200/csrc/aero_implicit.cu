@@ -838,20 +838,18 @@ template <typename R>
 __device__ __forceinline__ void load_row_recs(const R* rec, const double* sca, int cnt, int t, RowRecs& r) {
   r.row = row_of(t, cnt);
   r.node = t - r.row * cnt;
-  // the records are read once: through L2 only, so that they do not push the
-  // plane offsets and views this thread needs next out of L1
   const R* rn = rec + r.node;
-  r.packed = __ldcg(RecFmt<R>::packed_ptr(rec, cnt) + r.node);
+  r.packed = RecFmt<R>::packed(rec, cnt, r.node);
 #pragma unroll
   for (int d = 0; d < 3; ++d)
 #pragma unroll
-    for (int c = 0; c < 5; ++c) r.m[5 * d + c] = (double)__ldcg(rn + (25 * d + 5 * r.row + c) * cnt);
+    for (int c = 0; c < 5; ++c) r.m[5 * d + c] = (double)rn[(25 * d + 5 * r.row + c) * cnt];
   const double* sn = sca + r.node;
-  r.rhs = __ldcg(sn + r.row * cnt);
-  r.diag = __ldcg(sn + 5 * cnt);
-  r.invj = __ldcg(sn + 6 * cnt);
-  r.rdiag = __ldcg(sn + 7 * cnt);
-  r.rinvj = __ldcg(sn + 8 * cnt);
+  r.rhs = sn[r.row * cnt];
+  r.diag = sn[5 * cnt];
+  r.invj = sn[6 * cnt];
+  r.rdiag = sn[7 * cnt];
+  r.rinvj = sn[8 * cnt];
   // (the divisor flag in `packed` is read where the row is computed, so that
   // this load of the next plane's row does not wait for its data)
 }
@@ -1022,7 +1020,7 @@ __device__ __forceinline__ double row_from_ring(const RowRecs& r, const double* 
 // belongs to thread t of the cluster (5 * pmax <= cluster threads), so CTA r
 // computes the contiguous slice [r*T, (r+1)*T) of the plane's values.  Each CTA
 // writes its slice into a two-plane ring in its own shared memory (row-major
-// item order), and after a CTA barrier lane 0 of warp r copies the slice into
+// item order), and after a CTA barrier lane r of warp 0 copies the slice into
 // the same place in CTA r with cp.async.bulk, the bytes counted on the receiver's mbarrier
 // for that ring half; a CTA arms its mbarrier with the bytes it expects and its
 // threads wait (bounded) for the previous plane's bytes before reading the
@@ -1152,20 +1150,17 @@ __device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ bl
         B.dq[5 * (base + pre.node) + pre.row] = v;
     }
     // the slice is complete once every thread has written and fenced its value;
-    // lane 0 of warp r then copies it to CTA r, unless a wait of this CTA up to
+    // lane r of warp 0 then copies it to CTA r, unless a wait of this CTA up to
     // this plane ran out (every such failure is recorded before the barrier)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
-    // lane 0 of warp r copies the slice to CTA r (warps r, r + warps, ... when
-    // the CTA has fewer warps than the cluster has CTAs), so the copies are
-    // issued side by side
-    if ((threadIdx.x & 31) == 0 && !failed_by(gs)) {
+    if (threadIdx.x < ncta && threadIdx.x != me && !failed_by(gs)) {
       const unsigned bytes = slice_bytes(cnt, me);
       const unsigned off = (unsigned)(((gs & 1) * HS + (int)me * T) * sizeof(double));
       const unsigned boff = (unsigned)((gs & 1) * sizeof(unsigned long long));
-      for (unsigned r = threadIdx.x >> 5; r < ncta; r += blockDim.x >> 5)
-        if (r != me && bytes)
-          bulk_to_cluster(map_rank(ring_local + off, r), ring_local + off, bytes, map_rank(bar_local + boff, r));
+      if (bytes)
+        bulk_to_cluster(map_rank(ring_local + off, threadIdx.x), ring_local + off, bytes,
+                        map_rank(bar_local + boff, threadIdx.x));
     }
   };
   // planes 1 .. pf-1 now, then plane gs+pf after each step gs (pf >= 2)
@@ -1262,19 +1257,18 @@ __device__ __forceinline__ void load_slab_row(const BlockView& B, bool fwd, long
   const R* rec = recs<R>(B, fwd) + W * base;
   r.row = row;
   r.node = node;
-  // read once, through L2 only (see load_row_recs)
   const R* rn = rec + node;
-  r.packed = __ldcg(RecFmt<R>::packed_ptr(rec, cnt) + node);
+  r.packed = RecFmt<R>::packed(rec, cnt, node);
 #pragma unroll
   for (int d = 0; d < 3; ++d)
 #pragma unroll
-    for (int c = 0; c < 5; ++c) r.m[5 * d + c] = (double)__ldcg(rn + (25 * d + 5 * row + c) * cnt);
+    for (int c = 0; c < 5; ++c) r.m[5 * d + c] = (double)rn[(25 * d + 5 * row + c) * cnt];
   const double* sn = B.sca + kSca * base + node;
-  r.rhs = __ldcg(sn + row * cnt);
-  r.diag = __ldcg(sn + 5 * cnt);
-  r.invj = __ldcg(sn + 6 * cnt);
-  r.rdiag = __ldcg(sn + 7 * cnt);
-  r.rinvj = __ldcg(sn + 8 * cnt);
+  r.rhs = sn[row * cnt];
+  r.diag = sn[5 * cnt];
+  r.invj = sn[6 * cnt];
+  r.rdiag = sn[7 * cnt];
+  r.rinvj = sn[8 * cnt];
   // dq* of the node, written by this CTA in the forward pass (read from L2;
   // complete once the forward pass has passed the node's plane)
   r.dsv = fwd ? 0.0 : __ldcg(B.dqs + 8 * base + row * cnt + node);
