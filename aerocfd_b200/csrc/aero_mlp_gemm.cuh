@@ -6,13 +6,14 @@
 //
 // Per CTA (128 threads): one 128 x 128 FP32 accumulator in tensor memory (128
 // columns), A and B tiles of 128 x 64 BF16 staged in shared memory by the
-// threads in the canonical no-swizzle K-major layout (8-row x 16-byte core
-// matrices; LBO = 128 B between core matrices along K, SBO = 1024 B between
-// 8-row groups), two stages so that staging overlaps the MMAs, four kind::f16
-// MMAs of K = 16 per tile issued by one thread, completion through
-// tcgen05.commit on the stage's mbarrier, and the epilogue reading tensor
-// memory with tcgen05.ld (warp w reads lanes 32w..32w+31 = rows).
-// Every wait is bounded; the tensor memory is always released.
+// threads' asynchronous 16-byte copies (cp.async) in the canonical no-swizzle
+// K-major layout (8-row x 16-byte core matrices; LBO = 128 B between core
+// matrices along K, SBO = 1024 B between 8-row groups), four stages so that
+// the copies of the next three K-tiles are in flight while the tensor cores
+// work, four kind::f16 MMAs of K = 16 per tile issued by one thread,
+// completion through tcgen05.commit on the stage's mbarrier, and the epilogue
+// reading tensor memory with tcgen05.ld (warp w reads lanes 32w..32w+31 =
+// rows).  Every wait is bounded; the tensor memory is always released.
 #pragma once
 #include <cstdint>
 
@@ -40,9 +41,9 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
 }
 
 constexpr long kGemmSpin = 1L << 22;
-// Dynamic shared memory of k_gemm_bf16: two stages of A and B tiles (2 x 2 x
+// Dynamic shared memory of k_gemm_bf16: four stages of A and B tiles (4 x 2 x
 // 16 KB) plus slack to align the first tile to 1024 bytes.
-constexpr int kGemmStages = 2;
+constexpr int kGemmStages = 4;
 constexpr size_t kGemmSmem = (size_t)kGemmStages * (kBM + kBN) * kBK * sizeof(uint16_t) + 1024;
 
 __device__ __forceinline__ bool gemm_try_wait(uint32_t bar, unsigned parity) {
@@ -60,26 +61,30 @@ __device__ __forceinline__ bool gemm_wait(uint32_t bar, unsigned parity, long bu
   return false;
 }
 
-// Two-stage pipeline: the threads stage K-tile t into shared-memory stage
-// t % 2 while the tensor cores still run the MMAs of tile t - 1 from the other
-// stage; before restaging a stage they wait for the commit of the MMAs that
-// read it two tiles earlier (tcgen05.commit arrives on that stage's mbarrier
-// once every MMA issued before it is done).
+// Pipeline over the K-tiles t = 0 .. nt-1 of the CTA's K range, stage t % S
+// (S = kGemmStages): every thread copies its 16 chunks of tile t with
+// cp.async, one commit group per tile, S-1 tiles ahead.  For tile t the
+// threads wait for their own copies (cp.async.wait_group), make them visible
+// to the tensor cores (fence.proxy.async, then a CTA barrier), and one thread
+// issues the tile's MMAs and commits them on the stage's mbarrier; then the
+// stage of tile t-1 is refilled with tile t+S-1 once that tile's commit has
+// arrived (its MMAs have read the stage).
 __global__ void __launch_bounds__(128) k_gemm_bf16(const uint16_t* __restrict__ A, const uint16_t* __restrict__ B,
                                                   float* __restrict__ C, int M, int N, int K, int klen,
                                                   unsigned* status) {
+  constexpr int S = kGemmStages;
   extern __shared__ uint8_t gemm_smem[];
-  __shared__ __align__(8) unsigned long long bar[kGemmStages];
+  __shared__ __align__(8) unsigned long long bar[S];
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
   const int kbeg = blockIdx.z * klen, kend = min(K, kbeg + klen);
+  const int nt = (kend - kbeg) / kBK;  // K-tiles of this CTA (K and klen are multiples of kBK)
   float* Cs = C + (long)blockIdx.z * M * N;
   // stage s: A tile at base + s * 32 KB, B tile 16 KB after it
   const uint32_t raw = smem_addr(gemm_smem);
   const uint32_t base_s = (raw + 1023u) & ~1023u;
-  uint8_t* base = gemm_smem + (base_s - raw);
   const uint32_t stage_bytes = (kBM + kBN) * kBK * sizeof(uint16_t);
 
   if (warp == 0) {
@@ -89,8 +94,8 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(const uint16_t* __restrict__ 
   }
   if (tid == 0) {
     abort_flag = 0;
-    for (int s = 0; s < kGemmStages; ++s)
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar[s])) : "memory");
+    for (int x = 0; x < S; ++x)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar[x])) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -98,42 +103,45 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(const uint16_t* __restrict__ 
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_slot;
   const uint32_t idesc = idesc_bf16(kBM, kBN);
-  // per stage: parity of the next commit to wait for, and whether one is
-  // pending (scalars, so nothing goes to local memory)
-  unsigned ph0 = 0u, ph1 = 0u;
-  bool pend0 = false, pend1 = false;
-  int it = 0;
-  for (int k0 = kbeg; k0 < kend; k0 += kBK, ++it) {
-    const int s = it & 1;
-    uint16_t* sA = (uint16_t*)(base + s * stage_bytes);
-    uint16_t* sB = sA + kBM * kBK;
-    if (s ? pend1 : pend0) {  // the MMAs that read this stage two tiles ago
-      if (gemm_wait(smem_addr(&bar[s]), s ? ph1 : ph0, kGemmSpin)) {
-        if (s) { ph1 ^= 1u; pend1 = false; } else { ph0 ^= 1u; pend0 = false; }
-      } else {
-        abort_flag = 1;
-      }
-      __syncthreads();
-      if (abort_flag) break;
-    }
-    // stage A and B: 128 rows x 8 chunks of 8 BF16 each, 8 chunks per thread
+  // this thread's 16-byte chunks of tile t into stage x: chunk c = tid + 128 j
+  // (j < 8) of the A and of the B tile, row c / 8, K-chunk c % 8
+  auto copy_tile = [&](int t, int x) {
+    const int k0 = kbeg + t * kBK;
+    const uint32_t sA = base_s + (uint32_t)x * stage_bytes;
+    const uint32_t sB = sA + kBM * kBK * sizeof(uint16_t);
 #pragma unroll
-    for (int x = 0; x < 8; ++x) {
-      int c = tid + 128 * x;
-      int r = c >> 3, kc = c & 7;
-      int so = (r >> 3) * 512 + kc * 64 + (r & 7) * 8;  // in BF16 elements (1024 B, 128 B, 16 B)
-      *(uint4*)(sA + so) = *(const uint4*)(A + (long)(m0 + r) * K + k0 + kc * 8);
-      *(uint4*)(sB + so) = *(const uint4*)(B + (long)(n0 + r) * K + k0 + kc * 8);
+    for (int j = 0; j < 8; ++j) {
+      const int c = tid + 128 * j;
+      const int r = c >> 3, kc = c & 7;
+      const uint32_t so = (uint32_t)(((r >> 3) * 512 + kc * 64 + (r & 7) * 8) * sizeof(uint16_t));
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sA + so),
+                   "l"(A + (long)(m0 + r) * K + k0 + kc * 8)
+                   : "memory");
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sB + so),
+                   "l"(B + (long)(n0 + r) * K + k0 + kc * 8)
+                   : "memory");
     }
+  };
+  for (int t = 0; t < S - 1; ++t) {
+    if (t < nt) copy_tile(t, t);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
+  int last = -1;  // the last tile whose MMAs were committed
+  for (int t = 0; t < nt; ++t) {
+    const int x = t % S;
+    // tile t's copies are the oldest of the S-1 groups in flight
+    asm volatile("cp.async.wait_group %0;" ::"n"(S - 2) : "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t sA = base_s + (uint32_t)x * stage_bytes;
+      const uint32_t sB = sA + kBM * kBK * sizeof(uint16_t);
 #pragma unroll
       for (int kk = 0; kk < kBK / 16; ++kk) {
-        uint64_t da = umma_desc(smem_addr(sA) + kk * 256, 128, 1024);
-        uint64_t db = umma_desc(smem_addr(sB) + kk * 256, 128, 1024);
-        uint32_t acc = (k0 > kbeg || kk > 0) ? 1u : 0u;
+        uint64_t da = umma_desc(sA + kk * 256, 128, 1024);
+        uint64_t db = umma_desc(sB + kk * 256, 128, 1024);
+        uint32_t acc = (t > 0 || kk > 0) ? 1u : 0u;
         asm volatile(
             "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
             " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(tmem),
@@ -141,30 +149,34 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(const uint16_t* __restrict__ 
             : "memory");
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                       smem_addr(&bar[s]))
+                       smem_addr(&bar[x]))
                    : "memory");
     }
-    if (s) pend1 = true; else pend0 = true;
-  }
-  // every commit still pending: the last tile's covers all MMAs issued
-  if (!abort_flag) {
-    if (pend0) {
-      if (gemm_wait(smem_addr(&bar[0]), ph0, kGemmSpin)) pend0 = false; else abort_flag = 1;
+    last = t;
+    // refill the stage of tile t-1 with tile t+S-1 once tile t-1's MMAs are
+    // done (their commit is the (t-1)/S-th completion of that stage's barrier)
+    const int tn = t + S - 1;
+    if (tn < nt) {
+      const int xp = tn % S;
+      if (t >= 1 && !gemm_wait(smem_addr(&bar[xp]), (unsigned)(((t - 1) / S) & 1), kGemmSpin)) abort_flag = 1;
+      __syncthreads();
+      if (abort_flag) break;
+      copy_tile(tn, xp);
     }
-    if (pend1) {
-      if (gemm_wait(smem_addr(&bar[1]), ph1, kGemmSpin)) pend1 = false; else abort_flag = 1;
-    }
-    __syncthreads();
+    asm volatile("cp.async.commit_group;" ::: "memory");
   }
+  // no copy may still be landing in shared memory when the CTA goes on
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  // the last commit covers every MMA issued before it
+  if (!abort_flag && last >= 0 && !gemm_wait(smem_addr(&bar[last % S]), (unsigned)((last / S) & 1), kGemmSpin))
+    abort_flag = 1;
+  __syncthreads();
   if (abort_flag) {
-    // MMAs committed on a stage whose wait ran out may still read the staged
-    // tiles and write the accumulator: wait once more, with a longer bound,
-    // for each pending commit before the accumulator is freed.  If such a
-    // wait runs out too, the status bit below is the only guarantee left.
-    if (tid == 0) {
-      if (pend0) gemm_wait(smem_addr(&bar[0]), ph0, 16 * kGemmSpin);
-      if (pend1) gemm_wait(smem_addr(&bar[1]), ph1, 16 * kGemmSpin);
-    }
+    // MMAs committed before a wait ran out may still read the staged tiles
+    // and write the accumulator: wait once more, with a longer bound, for the
+    // last commit before the accumulator is freed.  If that wait runs out too,
+    // the status bit below is the only guarantee left.
+    if (tid == 0 && last >= 0) gemm_wait(smem_addr(&bar[last % S]), (unsigned)((last / S) & 1), 16 * kGemmSpin);
     __syncthreads();
   }
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
