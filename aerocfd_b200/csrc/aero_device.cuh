@@ -92,6 +92,9 @@ struct BlockView {
   unsigned* bstat;
   const int* live;
   __device__ __forceinline__ bool retired() const { return live && *live == 0; }
+  // 2-D mode (iflag_dimension = 2): the block is the single plane k = 1 (a
+  // 3-D block has at least three k-planes)
+  __host__ __device__ __forceinline__ bool planar() const { return b.ks == b.ke; }
   __device__ __forceinline__ void raise(unsigned bits) const {
 #if defined(__CUDA_ARCH__)
     if (bstat) atomicOr(bstat, bits);
@@ -107,6 +110,15 @@ struct BlockView {
   __device__ __forceinline__ double& s(int fid, long n) const { return f[fid][n]; }
 };
 
+
+// The updated box grown by one node on every side, where the implicit
+// schemes form their radii and diagonals (sub_timeadvancement_1stimplicit.f90:
+// 110-156); in 2-D only in i and j (:157-210), the block having one plane.
+__host__ __device__ __forceinline__ Box grown_box(const Box& b, const Box& b1) {
+  const int kx = b.ks == b.ke ? 0 : 1;
+  return Box{b1.is - 1, b1.ie + 1, b1.js - 1, b1.je + 1, b1.ks - kx, b1.ke + kx};
+}
+__host__ __device__ __forceinline__ Box grown_box(const BlockView& B) { return grown_box(B.b, B.b1); }
 // LU-SGS record stride: three 5x5 blocks (75 doubles) plus the packed
 // neighbour positions, 608 bytes (bulk-copy alignment: multiples of 16).
 constexpr int kRec = 76;

@@ -365,7 +365,7 @@ __device__ __forceinline__ void faces_body(const BlockView* __restrict__ blocks,
   const BlockView& B = blocks[blockIdx.y];
   if (B.retired()) return;
   const int d = blockIdx.z;
-  if (d >= (cc.dimension == IFLAG_3D ? 3 : 2)) return;
+  if (d >= (cc.dimension == IFLAG_3D && !B.planar() ? 3 : 2)) return;
   const Box& b1 = B.b1;
   Box e = b1;
   if (d == 0) e.is -= 1; else if (d == 1) e.js -= 1; else e.ks -= 1;
@@ -606,6 +606,7 @@ struct FaceAt {
   int pos, lo, hi;
 };
 __device__ __forceinline__ bool face_at(const BlockView& B, int d, FaceAt& F) {
+  if (d == 2 && B.planar()) return false;  // 2-D: no zeta faces (sub_inviscid1.f90:137)
   Box e = B.b1;
   if (d == 0) e.is -= 1; else if (d == 1) e.js -= 1; else e.ks -= 1;
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;

@@ -1,10 +1,11 @@
 // Wall forces and lift / drag of clcd_output (sub_output_forceintegration.f90:
-// 8-479, 3-D branch :182-457, force_compute :481-509) on the device: one
-// thread per wall quad of every wall subface, a fixed-order reduction of the
-// pressure and viscous force components, then cl and cd.  The per-quad
-// arithmetic keeps the reference's operation order, including its mix of
-// metric components in the wall-normal vector; only the order of the sums
-// over quads differs from the serial loop.
+// 8-479, 3-D branch :182-457, 2-D branch :48-180, force_compute :481-509) on
+// the device: one thread per wall quad (2-D: wall edge) of every wall
+// subface, a fixed-order reduction of the pressure and viscous force
+// components, then cl and cd.  The per-quad arithmetic keeps the reference's
+// operation order, including its mix of metric components in the wall-normal
+// vector and, in 2-D, its 0.25 viscosity average on face 3 (:128); only the
+// order of the sums over quads differs from the serial loop.
 #include <cmath>
 
 #include "aero_device.cuh"
@@ -52,6 +53,38 @@ __global__ void k_forces(const BlockView* __restrict__ blocks, const WallFace* _
     int t2 = W.lo2 + (int)(r / W.n1);
     const int w0 = W.w0, w1 = low ? w0 + 1 : w0 - 1;
     const int c1 = 3 * D + 1, c2 = 3 * D + 2, c3 = 3 * D + 3;
+    if (B.planar()) {
+      // 2-D edge (t1, t1+1): velocity and the unit normal from the two nodes
+      // one layer in, pressure and viscosity from the two wall nodes, s the
+      // edge's spacing along the wall, dn the mean spacing normal to it
+      int a[3], b[3];
+      a[T1] = t1; a[T2] = t2; a[D] = w1;
+      b[T1] = t1 + 1; b[T2] = t2; b[D] = w1;
+      const long ia = B.at(a[0], a[1], a[2]), ib = B.at(b[0], b[1], b[2]);
+      a[D] = w0; b[D] = w0;
+      const long wa = B.at(a[0], a[1], a[2]), wb = B.at(b[0], b[1], b[2]);
+      double uc = (B.v(F_PRI, 2, ia) + B.v(F_PRI, 2, ib)) * 0.5;
+      double vc = (B.v(F_PRI, 3, ia) + B.v(F_PRI, 3, ib)) * 0.5;
+      double wc = 0.0;
+      double pc = (B.v(F_PRI, 5, wa) + B.v(F_PRI, 5, wb)) * 0.5;
+      double t00 = 1.0 / sqrt(p2(B.v(F_DXIDX, c1, ia)) + p2(B.v(F_DXIDX, c2, ia)) + p2(B.v(F_DXIDX, c3, ia)));
+      double t10 = 1.0 / sqrt(p2(B.v(F_DXIDX, c1, ib)) + p2(B.v(F_DXIDX, c2, ib)) + p2(B.v(F_DXIDX, c3, ib)));
+      const double sgn = low ? -1.0 : 1.0;
+      double n3[3];
+#pragma unroll
+      for (int x = 0; x < 3; ++x)
+        n3[x] = sgn * ((B.v(F_DXIDX, c1 + x, ia) * t00 + B.v(F_DXIDX, c1 + x, ib) * t10) * 0.5);
+      double miuc = (B.v(F_AMU, 3, wa) + B.v(F_AMU, 3, wb)) * (W.face == 3 ? 0.25 : 0.5);
+      double area = spacing_at(B, T1, a[0], a[1], a[2]);
+      double dn = (spacing_at(B, D, a[0], a[1], a[2]) + spacing_at(B, D, b[0], b[1], b[2])) * 0.5;
+      double u3[3] = {uc, vc, wc};
+      double un = uc * n3[0] + vc * n3[1] + wc * n3[2];
+#pragma unroll
+      for (int x = 0; x < 3; ++x) {
+        f[x] = (pc - cc.p_0) * area * n3[x];
+        f[3 + x] = miuc * (u3[x] - un * n3[x]) / dn * area / cc.re;
+      }
+    } else {
     const int da[4] = {0, 1, 0, 1}, db[4] = {0, 0, 1, 1};  // corners 00, 10, 01, 11
     long ni[4], nw[4];
 #pragma unroll
@@ -94,6 +127,7 @@ __global__ void k_forces(const BlockView* __restrict__ blocks, const WallFace* _
     for (int x = 0; x < 3; ++x) {
       f[x] = (pc - cc.p_0) * area * n3[x];
       f[3 + x] = miuc * (u3[x] - un * n3[x]) / dn * area / cc.re;
+    }
     }
   }
   __shared__ double sm[6][32];

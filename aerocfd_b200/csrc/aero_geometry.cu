@@ -69,6 +69,13 @@ __global__ void k_metric_pass1(const BlockView* __restrict__ blocks) {
   long P = B.plane;
   double der[3][3];  // der[d][c] = d x_c / d xi_d
   for (int d = 0; d < 3; ++d) {
+    if (d == 2 && B.planar()) {  // 2-D (:270-273): d x / d zeta = (0, 0, 1) everywhere
+      for (int c = 0; c < 3; ++c) {
+        der[2][c] = c == 2 ? 1.0 : 0.0;
+        D[(6 + c) * P + n] = der[2][c];
+      }
+      continue;
+    }
     int lo, hi;
     bool on = deriv_region(B, d, i, j, k, lo, hi);
     for (int c = 0; c < 3; ++c) {
@@ -115,7 +122,8 @@ __device__ __forceinline__ void temp_products(const BlockView& B, int which, lon
 
 // Pass 2 (:587-865): derivatives of the temp products along their own
 // direction (same five-region rule), the metrics dxidx = difference / (1/J)
-// over the full box, and alpha, beta, gamma.
+// over the full box (2-D: from the in-plane derivatives, :543-557), and
+// alpha, beta, gamma.
 __global__ void k_metric_pass2(const BlockView* __restrict__ blocks) {
   const BlockView& B = blocks[blockIdx.y];
   long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -124,6 +132,23 @@ __global__ void k_metric_pass2(const BlockView* __restrict__ blocks) {
   long r = n / B.nx;
   int j = B.b.js + (int)(r % B.ny);
   int k = B.b.ks + (int)(r / B.ny);
+  double ij = B.s(F_INVJ, n);
+  double m[9];
+  if (B.planar()) {
+    // 2-D (:543-557): the in-plane metrics from dx/dxi and dx/deta (scratch
+    // planes 0-2 and 3-5) over the whole box
+    const double* D = B.f[F_FVH];
+    const long P = B.plane;
+    m[0] = D[4 * P + n] / ij;
+    m[1] = -D[3 * P + n] / ij;
+    m[2] = 0.0;
+    m[3] = -D[1 * P + n] / ij;
+    m[4] = D[0 * P + n] / ij;
+    m[5] = 0.0;
+    m[6] = 0.0;
+    m[7] = 0.0;
+    m[8] = 1.0;
+  } else {
   const long st[3] = {1, (long)B.nx, (long)B.nx * B.ny};
   const int pos[3] = {i, j, k};
   const int lof[3] = {B.b.is, B.b.js, B.b.ks}, hif[3] = {B.b.ie, B.b.je, B.b.ke};
@@ -142,8 +167,6 @@ __global__ void k_metric_pass2(const BlockView* __restrict__ blocks) {
     else for (int c = 0; c < 6; ++c) tm[c] = 0.0;
     for (int c = 0; c < 6; ++c) dd[d][c] = dcentral(tm[c], t0[c], tp[c], pos[d], lo, hi);
   }
-  double ij = B.s(F_INVJ, n);
-  double m[9];
   m[0] = (dd[2][0] - dd[1][0]) / ij;
   m[1] = (dd[2][1] - dd[1][1]) / ij;
   m[2] = (dd[2][2] - dd[1][2]) / ij;
@@ -153,6 +176,7 @@ __global__ void k_metric_pass2(const BlockView* __restrict__ blocks) {
   m[6] = (dd[1][3] - dd[0][3]) / ij;
   m[7] = (dd[1][4] - dd[0][4]) / ij;
   m[8] = (dd[1][5] - dd[0][5]) / ij;
+  }
   for (int c = 0; c < 9; ++c) B.v(F_DXIDX, c + 1, n) = m[c];
   double x1 = m[0], x2 = m[1], x3 = m[2], e1 = m[3], e2 = m[4], e3 = m[5], z1 = m[6], z2 = m[7], z3 = m[8];
   B.v(F_ALPHA, 1, n) = (x1 * x1 + x2 * x2 + x3 * x3) * ij;

@@ -16,14 +16,13 @@
 namespace aero {
 
 // sub_timeadvancement_1stimplicit.f90:108-156, first half: the spectral
-// radii ra, rb, rc on the updated box grown by one.  They need only the
+// radii ra, rb, rc on the updated box grown by one (2-D: in i and j only).  They need only the
 // primitives and the metrics, so they (and the off-diagonal blocks made from
 // them) can be formed while the fluxes and the time step are computed.
 __global__ void k_lusgs_radii(const BlockView* __restrict__ blocks) {
   const BlockView& B = blocks[blockIdx.y];
   if (B.retired()) return;
-  const Box& b1 = B.b1;
-  Box e{b1.is - 1, b1.ie + 1, b1.js - 1, b1.je + 1, b1.ks - 1, b1.ke + 1};
+  const Box e = grown_box(B);
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= e.size()) return;
   int i = e.is + (int)(t % e.nx());
@@ -54,7 +53,7 @@ __global__ void k_lusgs_prep(const BlockView* __restrict__ blocks, CaseConsts cc
   if (B.retired()) return;
   const CaseConsts& cc = B.ccb ? *B.ccb : cc_launch;
   const Box& b1 = B.b1;
-  Box e{b1.is - 1, b1.ie + 1, b1.js - 1, b1.je + 1, b1.ks - 1, b1.ke + 1};
+  const Box e = grown_box(B);
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= e.size()) return;
   int i = e.is + (int)(t % e.nx());
@@ -67,7 +66,10 @@ __global__ void k_lusgs_prep(const BlockView* __restrict__ blocks, CaseConsts cc
     for (int c = 1; c <= 5; ++c) B.v(F_RHS, c, n) = B.v(F_RHSI, c, n) + B.v(F_RHSV, c, n);
   }
   double phi = cc.cfl >= 1.0e3 ? 0.0 : 1.0;
-  B.s(F_DIAG, n) = phi * 1.0 / B.s(F_DT, n) + B.s(F_RA, n) + B.s(F_RB, n) + B.s(F_RC, n);
+  if (B.planar())  // 2-D (:157-210): no zeta radius
+    B.s(F_DIAG, n) = phi * 1.0 / B.s(F_DT, n) + B.s(F_RA, n) + B.s(F_RB, n);
+  else
+    B.s(F_DIAG, n) = phi * 1.0 / B.s(F_DT, n) + B.s(F_RA, n) + B.s(F_RB, n) + B.s(F_RC, n);
 }
 
 // calc_jm (sub_timeadvancement_jac.f90:17-62) at node n with the metric row

@@ -531,7 +531,11 @@ int resolve(const Box& b, const Box& b0, const Box& b1, const std::vector<Arg>& 
     t.d_view = g.d_blocks + m;
     return AERO_OK;
   }
-  // transient
+  // transient: a 2-D configuration works on one-plane boxes, a 3-D one on
+  // boxes of at least three planes (the kernels reach k-1 and k+1 there)
+  const int dim = g.configured ? g.cc.dimension : IFLAG_3D;
+  if (dim == IFLAG_2D ? (b.nz() != 1) : (b.nz() < 3))
+    return fail(AERO_ERR_ARG, "index box with %d k-planes in a %d-D configuration", b.nz(), dim);
   long plane = round32(b.size());
   size_t need = view_doubles(plane);
   if (need > g.t_doubles) {
@@ -595,6 +599,7 @@ int finish(const BlockTarget& t, const std::vector<Arg>& args) {
 
 CaseConsts consts_with(double gamma, double cv, double re) {
   CaseConsts c = g.cc;
+  if (!g.configured) c.dimension = IFLAG_3D;  // drop-in calls before aero_configure: 3-D
   c.gamma = gamma;
   c.cv = cv;
   c.re = re;
@@ -987,7 +992,8 @@ int launch_crank(const BlockView* views, int nblk, long maxN, long maxN1, const 
   PROF(P_CRANK, (k_fill<<<dim3(cdiv(maxN, 256), nblk), 256, 0, g.stream>>>(views, F_FVH, 5, 0.0)));
   CKL();
   const long nl[3] = {(long)lines->ny() * lines->nz(), (long)lines->nx() * lines->nz(), (long)lines->nx() * lines->ny()};
-  for (int d = 0; d < 3; ++d) {
+  // 2-D (sub_timeadvancement_2ndcrank.f90:335): no k lines
+  for (int d = 0; d < (cc.dimension == IFLAG_2D ? 2 : 3); ++d) {
     PROF(P_CRANK, (k_crank_sweep<<<dim3(cdiv(nl[d], 64), nblk), 64, 0, g.stream>>>(views, d, cc.gamma)));
     CKL();
   }
@@ -1678,7 +1684,8 @@ int aero_set_retirement(int on) {
 int aero_configure(const int* iflags, const double* params) {
   int rc = need_init();
   if (rc) return rc;
-  if (iflags[0] != IFLAG_3D) return fail(AERO_ERR_ARG, "iflag_dimension=%d: only 3-D is supported", iflags[0]);
+  if (iflags[0] != IFLAG_3D && iflags[0] != IFLAG_2D)
+    return fail(AERO_ERR_ARG, "iflag_dimension=%d is not 2 or 3", iflags[0]);
   if (iflags[1] != IFLAG_NSSOLVER && iflags[1] != IFLAG_EULERSOLVER)
     return fail(AERO_ERR_ARG, "iflag_solver=%d is not 0 (NS) or 1 (Euler)", iflags[1]);
   bool steady_lusgs = iflags[2] == IFLAG_STEADY && iflags[3] == IFLAG_1STIMPLICIT;
@@ -1718,13 +1725,19 @@ int aero_register_block(int m, const int* box18, int num_subface, const int* sub
   H.b1 = Box{box18[12], box18[13], box18[14], box18[15], box18[16], box18[17]};
   // Stencils reach two nodes along each direction and the updated box sits
   // inside the physical one; require at least 3 nodes per direction and
-  // consistent nested boxes.
+  // consistent nested boxes.  A 2-D block (iflag_dimension = 2) is the single
+  // plane k = 1 in all three boxes (sub_init_allocatememory.f90:66-68,
+  // :134-144).
   const Box &b = H.b, &b0 = H.b0, &b1 = H.b1;
-  if (b0.nx() < 3 || b0.ny() < 3 || b0.nz() < 3)
-    return fail(AERO_ERR_ARG, "block %d: need at least 3 nodes per direction in 3-D", m);
+  const bool plane = b0.nz() == 1;
+  if (b0.nx() < 3 || b0.ny() < 3 || (!plane && b0.nz() < 3))
+    return fail(AERO_ERR_ARG, "block %d: need at least 3 nodes per direction (one k-plane in 2-D)", m);
+  if (plane && (b.ks != b0.ks || b.ke != b0.ke || b1.ks != b0.ks || b1.ke != b0.ke))
+    return fail(AERO_ERR_ARG, "block %d: a 2-D block has the one plane k = %d in every index box", m, b0.ks);
+  const int kg = plane ? 0 : 1;
   if (b.is > b0.is || b.ie < b0.ie || b.js > b0.js || b.je < b0.je || b.ks > b0.ks || b.ke < b0.ke ||
       b1.is < b.is + 1 || b1.ie > b.ie - 1 || b1.js < b.js + 1 || b1.je > b.je - 1 ||
-      b1.ks < b.ks + 1 || b1.ke > b.ke - 1 || b1.is < b0.is - 0 || b1.ie > b0.ie)
+      b1.ks < b.ks + kg || b1.ke > b.ke - kg || b1.is < b0.is - 0 || b1.ie > b0.ie)
     return fail(AERO_ERR_ARG, "block %d: index boxes are not nested as is <= is0 <= is1", m);
   for (int s = 0; s < num_subface; ++s) {
     const int* r = subfaces + 11 * s;
@@ -1755,8 +1768,12 @@ int aero_finish_setup(void) {
   if (!g.configured) return fail(AERO_ERR_STATE, "aero_configure has not been called");
   int nb = (int)g.blocks.size();
   if (nb == 0) return fail(AERO_ERR_STATE, "no blocks registered");
-  for (int m = 0; m < nb; ++m)
+  for (int m = 0; m < nb; ++m) {
     if (!g.blocks[m].used) return fail(AERO_ERR_ARG, "block %d missing (blocks must be 1..n)", m + 1);
+    if ((g.blocks[m].b0.nz() == 1) != (g.cc.dimension == IFLAG_2D))
+      return fail(AERO_ERR_ARG, "block %d: %s block in a %d-D case", m + 1,
+                  g.blocks[m].b0.nz() == 1 ? "a one-plane" : "a 3-D", g.cc.dimension);
+  }
   // topology tables
   std::vector<TopoBlock> tb(nb);
   for (int m = 0; m < nb; ++m) {
@@ -1764,7 +1781,7 @@ int aero_finish_setup(void) {
     tb[m].subs = g.blocks[m].subs;
   }
   Topology topo;
-  std::string why = build_topology(tb, g.cc.bufferLength, g.cc.solver, topo);
+  std::string why = build_topology(tb, g.cc.bufferLength, g.cc.solver, g.cc.dimension, topo);
   if (!why.empty()) return fail(AERO_ERR_ARG, "%s", why.c_str());
   // arena
   size_t total = 0;
@@ -1780,8 +1797,7 @@ int aero_finish_setup(void) {
     g.max_box = std::max(g.max_box, H.b.size());
     g.max_b0 = std::max(g.max_b0, H.b0.size());
     max_b1 = std::max(max_b1, H.b1.size());
-    Box e{H.b1.is - 1, H.b1.ie + 1, H.b1.js - 1, H.b1.je + 1, H.b1.ks - 1, H.b1.ke + 1};
-    g.max_ext = std::max(g.max_ext, e.size());
+    g.max_ext = std::max(g.max_ext, grown_box(H.b, H.b1).size());
     g.totalnodes += (double)H.b0.size();
     g.max_b1_face = std::max({g.max_b1_face, (long)H.b1.ny() * H.b1.nz(), (long)H.b1.nx() * H.b1.nz(),
                               (long)H.b1.nx() * H.b1.ny()});
@@ -1899,6 +1915,7 @@ int aero_finish_setup(void) {
         int T1 = D == 0 ? 1 : 0, T2 = D == 2 ? 1 : 2;
         const int lo[3] = {r.is, r.js, r.ks}, hi[3] = {r.ie, r.je, r.ke};
         WallFace w{m, r.face, lo[T1], hi[T1] - lo[T1], lo[T2], hi[T2] - lo[T2], r.face % 2 ? lo[D] : hi[D], q};
+        if (g.cc.dimension == IFLAG_2D) w.n2 = 1;  // 2-D: one row of wall edges along T1
         if (w.n1 <= 0 || w.n2 <= 0) continue;  // a wall line has no quads
         walls.push_back(w);
         q += (long)w.n1 * w.n2;
@@ -2063,6 +2080,17 @@ int aero_inviscid_flux_1(double* rhsi, const double* q, const double* dxidx, con
   return finish(t, args);
 }
 
+// The faces of is0..ke0 grown by one node down along coord, and the node up
+// along coord each face also reads, lie inside the box is..ke (the drop-in
+// face routines below read nothing outside it; a one-plane 2-D box has no
+// faces along k).
+bool faces_inside(const Box& b, const Box& e, int coord) {
+  if (e.is < b.is || e.ie > b.ie || e.js < b.js || e.je > b.je || e.ks < b.ks || e.ke > b.ke) return false;
+  const int hi = coord == 1 ? e.ie : (coord == 2 ? e.je : e.ke);
+  const int bh = coord == 1 ? b.ie : (coord == 2 ? b.je : b.ke);
+  return hi <= bh - 1;
+}
+
 // thirdorder_weno (sub_inviscid_upwind.f90:1): the WENO3 state at every face
 // of the caller's box is0..ke0 grown by one node down along coord, right
 // (direction 1) or left (direction -1) of the face; df keeps the caller's
@@ -2081,6 +2109,8 @@ int aero_thirdorder_weno(double* df, const double* f, const int* is, const int* 
   if (t.resident) return fail(AERO_ERR_ARG, "thirdorder_weno works on unregistered arrays");
   Box e = r0;
   if (*coord == 1) e.is -= 1; else if (*coord == 2) e.js -= 1; else e.ks -= 1;
+  if (e.size() > 0 && !faces_inside(b, e, *coord))
+    return fail(AERO_ERR_ARG, "thirdorder_weno: faces along coord %d reach outside the array", *coord);
   // direction 1: right states, -1: left states, anything else: nothing (the
   // reference's if / else if)
   if (e.size() > 0 && (*direction == 1 || *direction == -1)) {
@@ -2108,6 +2138,8 @@ int aero_roe_3d(const double* ql, const double* qr, double* flux, const double* 
   if (t.resident) return fail(AERO_ERR_ARG, "roe_3d works on unregistered arrays");
   Box e = r0;
   if (*coord == 1) e.is -= 1; else if (*coord == 2) e.js -= 1; else e.ks -= 1;
+  if (e.size() > 0 && !faces_inside(b, e, *coord))
+    return fail(AERO_ERR_ARG, "roe_3d: faces along coord %d reach outside the array", *coord);
   if (e.size() > 0) {
     k_roe_states<<<cdiv(e.size(), 128), 128, 0, g.stream>>>(t.d_view, *coord, r0, *gamma);
     CKL();
@@ -2223,7 +2255,7 @@ int aero_implicit1st(double* q, const double* dt, const double* pri_v, double* r
   if ((rc = resolve(b, b0, b1, args, t))) return rc;
   CaseConsts cc = consts_with(*gamma, g.cc.cv, g.cc.re);
   cc.cfl = *cfl;
-  Box e{b1.is - 1, b1.ie + 1, b1.js - 1, b1.je + 1, b1.ks - 1, b1.ke + 1};
+  Box e = grown_box(b, b1);
   if (!t.resident && (rc = launch_index(t.d_view, 1, b1.size()))) return rc;
   if ((rc = launch_implicit(t.d_view, 1, e.size(), b1.size(), t.view.pmax, t.view.nplanes, cc, nullptr, true,
                             nullptr, &t.view)))

@@ -75,8 +75,19 @@ void bc_levels(Topology& out) {
 
 namespace {
 
+// 2-D mode (sub_bc_updatebuffer2d.f90, sub_bc_updatebuffercoordinate2d.f90,
+// sub_bc_updatebufferaverage2d.f90): a face is a line and ua(ll) runs along
+// it (j on faces 1/2, i on faces 3/4), nn = max(n11, n12) of the donor
+// subface (:218-222); ori 2 keeps the order, ori 3 reverses it (:284-293).
+// The maps below take (l, m) = (ll, 1) when `two` is set.
+
 // (l,m) extents of a donor subface as ua is shaped for its face.
-void donor_extent(const SubRow& d, int& l1, int& m1) {
+void donor_extent(bool two, const SubRow& d, int& l1, int& m1) {
+  if (two) {
+    l1 = std::max(d.ie - d.is + 1, d.je - d.js + 1);
+    m1 = 1;
+    return;
+  }
   int n1 = d.ie - d.is + 1, n2 = d.je - d.js + 1, n3 = d.ke - d.ks + 1;
   static const int L[6] = {3, 2, 1, 3, 2, 1};  // extent used for l on faces 1..6
   static const int M[6] = {2, 3, 3, 1, 1, 2};  // extent used for m
@@ -86,7 +97,13 @@ void donor_extent(const SubRow& d, int& l1, int& m1) {
 }
 
 // Donor face node feeding ua(l,m).
-void donor_face_node(const SubRow& d, int l, int m, int& i, int& j, int& k) {
+void donor_face_node(bool two, const SubRow& d, int l, int m, int& i, int& j, int& k) {
+  if (two) {
+    k = d.ks;
+    i = d.face <= 2 ? (d.face == 1 ? d.is : d.ie) : d.is + l - 1;
+    j = d.face <= 2 ? d.js + l - 1 : (d.face == 3 ? d.js : d.je);
+    return;
+  }
   switch (d.face) {
     case 1: i = d.is; j = d.js + m - 1; k = d.ks + l - 1; break;
     case 2: i = d.ie; j = d.js + l - 1; k = d.ks + m - 1; break;
@@ -98,12 +115,17 @@ void donor_face_node(const SubRow& d, int l, int m, int& i, int& j, int& k) {
 }
 
 // Reoriented array ua2(l2,m2) takes ua(l,m) with (l,m) from (l2,m2) by ori.
-void ori_extent(int ori, int l1, int m1, int& l2, int& m2) {
-  bool swap = (ori == 2 || ori == 4);
+void ori_extent(bool two, int ori, int l1, int m1, int& l2, int& m2) {
+  bool swap = !two && (ori == 2 || ori == 4);
   l2 = swap ? m1 : l1;
   m2 = swap ? l1 : m1;
 }
-void ori_source(int ori, int l1, int m1, int l2i, int m2i, int& l, int& m) {
+void ori_source(bool two, int ori, int l1, int m1, int l2i, int m2i, int& l, int& m) {
+  if (two) {
+    l = ori == 2 ? l2i : l1 - l2i + 1;
+    m = m2i;
+    return;
+  }
   if (ori == 1) { l = l2i; m = m1 - m2i + 1; }
   else if (ori == 2) { l = m2i; m = l2i; }
   else if (ori == 3) { l = l1 - l2i + 1; m = m2i; }
@@ -111,8 +133,18 @@ void ori_source(int ori, int l1, int m1, int l2i, int m2i, int& l, int& m) {
 }
 
 // Receiver face node written by ua2(a,b), and the outward unit step.
-void own_face_node(const SubRow& s, int a, int b, int& i, int& j, int& k, int& di, int& dj, int& dk) {
+void own_face_node(bool two, const SubRow& s, int a, int b, int& i, int& j, int& k, int& di, int& dj, int& dk) {
   di = dj = dk = 0;
+  if (two) {
+    k = s.ks;
+    switch (s.face) {
+      case 1: i = s.is; j = s.js + a - 1; di = -1; break;
+      case 2: i = s.ie; j = s.js + a - 1; di = 1; break;
+      case 3: i = s.is + a - 1; j = s.js; dj = -1; break;
+      default: i = s.is + a - 1; j = s.je; dj = 1; break;
+    }
+    return;
+  }
   switch (s.face) {
     case 1: i = s.is; j = s.js + b - 1; k = s.ks + a - 1; di = -1; break;
     case 2: i = s.ie; j = s.js + a - 1; k = s.ks + b - 1; di = 1; break;
@@ -139,15 +171,16 @@ bool planar(const SubRow& s) {
 }  // namespace
 
 std::string build_topology(const std::vector<TopoBlock>& blocks, int buffer_length, int solver,
-                           Topology& out) {
+                           int dimension, Topology& out) {
   char msg[256];
   int nb = (int)blocks.size();
   out = Topology{};
+  const bool two = dimension == IFLAG_2D;
   // ---------------------------------------------------------------- validate
   for (int m = 0; m < nb; ++m) {
     for (size_t s = 0; s < blocks[m].subs.size(); ++s) {
       const SubRow& r = blocks[m].subs[s];
-      if (r.face < 1 || r.face > 6 || !planar(r)) {
+      if (r.face < 1 || r.face > (two ? 4 : 6) || !planar(r)) {
         std::snprintf(msg, sizeof msg, "block %d subface %zu: bad face or non-planar range", m + 1, s + 1);
         return msg;
       }
@@ -167,7 +200,7 @@ std::string build_topology(const std::vector<TopoBlock>& blocks, int buffer_leng
       }
       if (r.blk_t > 0) {
         if (r.blk_t > nb || r.subface_t < 1 || r.subface_t > (int)blocks[r.blk_t - 1].subs.size() ||
-            r.ori < 1 || r.ori > 4) {
+            (two ? (r.ori != 2 && r.ori != 3) : (r.ori < 1 || r.ori > 4))) {
           std::snprintf(msg, sizeof msg, "block %d subface %zu: bad neighbour/orientation", m + 1, s + 1);
           return msg;
         }
@@ -186,8 +219,8 @@ std::string build_topology(const std::vector<TopoBlock>& blocks, int buffer_leng
       const TopoBlock& D = blocks[s.blk_t - 1];
       const SubRow& d = D.subs[s.subface_t - 1];
       int l1, m1, l2, m2;
-      donor_extent(d, l1, m1);
-      ori_extent(s.ori, l1, m1, l2, m2);
+      donor_extent(two, d, l1, m1);
+      ori_extent(two, s.ori, l1, m1, l2, m2);
       int own_n = (s.ie - s.is + 1) * (s.je - s.js + 1) * (s.ke - s.ks + 1);
       if (l2 * m2 != own_n) {
         std::snprintf(msg, sizeof msg, "block %d subface %d: neighbour face has %d nodes, own %d",
@@ -199,10 +232,10 @@ std::string build_topology(const std::vector<TopoBlock>& blocks, int buffer_leng
       for (int b2 = 1; b2 <= m2; ++b2)
         for (int a2 = 1; a2 <= l2; ++a2) {
           int l, mm;
-          ori_source(s.ori, l1, m1, a2, b2, l, mm);
+          ori_source(two, s.ori, l1, m1, a2, b2, l, mm);
           int si, sj, sk, oi, oj, ok, di, dj, dk;
-          donor_face_node(d, l, mm, si, sj, sk);
-          own_face_node(s, a2, b2, oi, oj, ok, di, dj, dk);
+          donor_face_node(two, d, l, mm, si, sj, sk);
+          own_face_node(two, s, a2, b2, oi, oj, ok, di, dj, dk);
           for (int layer = 1; layer <= buffer_length; ++layer) {
             int gi = oi + di * layer, gj = oj + dj * layer, gk = ok + dk * layer;
             int xi = si + sdi * layer, xj = sj + sdj * layer, xk = sk + sdk * layer;
@@ -239,18 +272,18 @@ std::string build_topology(const std::vector<TopoBlock>& blocks, int buffer_leng
       const TopoBlock& D = blocks[s.blk_t - 1];
       const SubRow& d = D.subs[s.subface_t - 1];
       int l1, m1, l2, m2;
-      donor_extent(d, l1, m1);
-      ori_extent(s.ori, l1, m1, l2, m2);
+      donor_extent(two, d, l1, m1);
+      ori_extent(two, s.ori, l1, m1, l2, m2);
       // buffer(own node) <- donor face node (average1); then average2 walks the
       // own subface box in k, j, i order.
       std::map<long, AvgSrc> buffer;
       for (int b2 = 1; b2 <= m2; ++b2)
         for (int a2 = 1; a2 <= l2; ++a2) {
           int l, mm;
-          ori_source(s.ori, l1, m1, a2, b2, l, mm);
+          ori_source(two, s.ori, l1, m1, a2, b2, l, mm);
           int si, sj, sk, oi, oj, ok, di, dj, dk;
-          donor_face_node(d, l, mm, si, sj, sk);
-          own_face_node(s, a2, b2, oi, oj, ok, di, dj, dk);
+          donor_face_node(two, d, l, mm, si, sj, sk);
+          own_face_node(two, s, a2, b2, oi, oj, ok, di, dj, dk);
           buffer[B.at(oi, oj, ok)] = AvgSrc{s.blk_t - 1, D.at(si, sj, sk)};
         }
       for (int k = s.ks; k <= s.ke; ++k)

@@ -32,10 +32,11 @@ struct Topology {
   std::vector<int> bc_level;       // per op: dependency level within its block (see bc_levels)
 };
 
-// Builds all tables; returns an empty string on success or the reason the
-// block/subface description is inconsistent.
+// Builds all tables (dimension: iflag_dimension, 2 or 3); returns an empty
+// string on success or the reason the block/subface description is
+// inconsistent.
 std::string build_topology(const std::vector<TopoBlock>& blocks, int buffer_length, int solver,
-                           Topology& out);
+                           int dimension, Topology& out);
 
 // Fills out.bc_level from out.bc_ops and out.bc_start: each op's dependency
 // level within its block (build_topology calls it).

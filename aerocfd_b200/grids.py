@@ -10,6 +10,12 @@ the path is quoted on:
 * ``naca_ogrid``    - NACA 4-digit O-grid split into ``nblk`` blocks around the
   airfoil, block interfaces on the i faces, wall at j=1, farfield at j=max.
 * ``bump_batch``    - many bump channels of uneven size (a Mach/geometry sweep).
+* ``bump_channel_2d`` - the bump channel in 2-D mode (iflag_dimension = 2) as
+  two blocks, the second turned by 180 degrees in the plane, so their shared
+  face runs in opposite directions (2-D orientation code 3).
+
+``naca_ogrid`` builds its 2-D form (one plane, no k faces, orientation code 2)
+when the configuration asks for iflag_dimension = 2.
 """
 from __future__ import annotations
 
@@ -18,7 +24,7 @@ from typing import List, Optional
 
 import numpy as np
 
-from .case import (BC_FARFIELD, BC_INFLOW, BC_OUTFLOW, BC_SYMM, BC_WALL, IFLAG_EULERSOLVER,
+from .case import (BC_FARFIELD, BC_INFLOW, BC_OUTFLOW, BC_SYMM, BC_WALL, IFLAG_2D, IFLAG_EULERSOLVER,
                    IFLAG_NSSOLVER, Block, Case, Config, Subface)
 
 
@@ -139,6 +145,9 @@ def naca_ogrid(nblk: int = 4, ni: int = 129, nj: int = 65, nk: int = 3, t: float
     connected face 2 -> face 1 with orientation code 2 (the reference's
     transposed (l,m) convention between an i+ and an i- face)."""
     cfg = cfg or Config(solver=IFLAG_NSSOLVER, ma=0.5, re=5000.0, aoa_deg=2.0, cfl=2.0)
+    two = cfg.dimension == IFLAG_2D
+    if two:
+        nk = 1                           # one plane, z = 0 (sub_init_allocatememory.f90:389-401)
     ntot = nblk * (ni - 1)               # intervals around the loop
     sx, sy = naca4_loop(ntot, t, m, p)
     # outer circle, clockwise from angle 0, at the same loop fraction
@@ -159,21 +168,69 @@ def naca_ogrid(nblk: int = 4, ni: int = 129, nj: int = 65, nk: int = 3, t: float
         Y2 = by[None, :] + (ey - by)[None, :] * dist[:, None]
         left = nblk if b == 0 else b          # neighbour on face 1 (i-)
         right = 1 if b == nblk - 1 else b + 2  # neighbour on face 2 (i+)
+        # in 2-D the shared i faces run the same way in j: orientation code 2
+        # (same order); in 3-D code 2 is the transposed (l,m) convention
         subs = [
             Subface(1, 1, 1, 1, 1, nj, 1, nk, left, 2, 2),
             Subface(2, 2, ni, ni, 1, nj, 1, nk, right, 1, 2),
             Subface(3, 3, 1, ni, 1, 1, 1, nk, BC_WALL),
             Subface(4, 4, 1, ni, nj, nj, 1, nk, BC_FARFIELD),
-            Subface(5, 5, 1, ni, 1, nj, 1, 1, BC_SYMM),
-            Subface(6, 6, 1, ni, 1, nj, nk, nk, BC_SYMM),
         ]
+        if not two:
+            subs += [Subface(5, 5, 1, ni, 1, nj, 1, 1, BC_SYMM),
+                     Subface(6, 6, 1, ni, 1, nj, nk, nk, BC_SYMM)]
         blk = Block(b + 1, ni, nj, nk, subs, cfg.buffer_length, cfg.dimension)
         X = np.broadcast_to(X2[None], (nk, nj, ni)).copy()
         Y = np.broadcast_to(Y2[None], (nk, nj, ni)).copy()
-        Z = np.broadcast_to(zs[:, None, None], (nk, nj, ni)).copy()
+        Z = np.zeros((nk, nj, ni)) if two else np.broadcast_to(zs[:, None, None], (nk, nj, ni)).copy()
         _set_coords(blk, X, Y, Z)
         blocks.append(blk)
     return Case(name, cfg, blocks)
+
+
+def bump_channel_2d(ni: int = 97, nj: int = 49, h: float = 0.10, length: float = 3.0,
+                    ratio: float = 1.05, cfg: Optional[Config] = None, name: str = "bump2d") -> Case:
+    """The bump channel of ``bump_channel`` in 2-D mode, as two blocks that
+    share the node line x = x_mid (ni points in total along x, the split at
+    node ni // 2 + 1).  Block 1 is the left part in (x, y) index order; block 2
+    is the right part turned by 180 degrees in the plane (its i runs from the
+    outlet back to the split, its j from the top down), so the grid stays
+    right-handed, its wall is face 4, its outflow face 1, and the shared
+    faces (face 2 of both blocks) run in opposite directions: orientation
+    code 3 (sub_bc_updatebuffer2d.f90:284-293)."""
+    cfg = cfg or Config(solver=IFLAG_EULERSOLVER, ma=0.5, re=1.0e6, cfl=5.0, dimension=IFLAG_2D)
+    if cfg.dimension != IFLAG_2D:
+        raise ValueError("bump_channel_2d needs a 2-D configuration")
+    x = np.linspace(0.0, length, ni)
+    R = (0.25 + h * h) / (2.0 * h)
+    ywall = np.where((x >= 1.0) & (x <= 2.0),
+                     np.sqrt(np.maximum(R * R - (x - 1.5) ** 2, 0.0)) - (R - h), 0.0)
+    n = nj - 1
+    eta = (ratio ** np.arange(nj) - 1.0) / (ratio ** n - 1.0)
+    Y2 = ywall[None, :] + (1.0 - ywall[None, :]) * eta[:, None]          # (nj, ni)
+    X2 = np.broadcast_to(x[None, :], (nj, ni))
+    mid = ni // 2                                                        # 0-based split node
+    n1, n2 = mid + 1, ni - mid
+    s1 = [
+        Subface(1, 1, 1, 1, 1, nj, 1, 1, BC_INFLOW),
+        Subface(2, 2, n1, n1, 1, nj, 1, 1, 2, 2, 3),
+        Subface(3, 3, 1, n1, 1, 1, 1, 1, BC_WALL),
+        Subface(4, 4, 1, n1, nj, nj, 1, 1, BC_SYMM),
+    ]
+    s2 = [
+        Subface(1, 1, 1, 1, 1, nj, 1, 1, BC_OUTFLOW),
+        Subface(2, 2, n2, n2, 1, nj, 1, 1, 1, 2, 3),
+        Subface(3, 3, 1, n2, 1, 1, 1, 1, BC_SYMM),
+        Subface(4, 4, 1, n2, nj, nj, 1, 1, BC_WALL),
+    ]
+    b1 = Block(1, n1, nj, 1, s1, cfg.buffer_length, cfg.dimension)
+    b2 = Block(2, n2, nj, 1, s2, cfg.buffer_length, cfg.dimension)
+    _set_coords(b1, X2[None, :, :n1].copy(), Y2[None, :, :n1].copy(), np.zeros((1, nj, n1)))
+    # block 2 node (i', j') = global node (ni - i', nj + 1 - j') (1-based)
+    X2r = X2[::-1, ::-1][:, :n2]
+    Y2r = Y2[::-1, ::-1][:, :n2]
+    _set_coords(b2, X2r[None].copy(), Y2r[None].copy(), np.zeros((1, nj, n2)))
+    return Case(name, cfg, [b1, b2])
 
 
 def bump_batch(ncase: int = 64, seed: int = 0, nk: int = 5):

@@ -432,7 +432,8 @@ void viscous_flux(V rhsv, V pri_v, V amu, V vor, V dudx, V tao, V dxidx, V inv_j
   Tmp fv(5, b), gv(5, b), hv(5, b), fvxi(5, b), gveta(5, b), hvzeta(5, b);
   bool three = g_flags.dimension == IFLAG_3D;
 
-  for (int k = b1.ks - 1; k <= b1.ke + 1; ++k)  // :82-92
+  const int kx = three ? 1 : 0;  // 2-D: the plane k = 1 only (:93-101)
+  for (int k = b1.ks - kx; k <= b1.ke + kx; ++k)  // :82-92
     for (int j = b1.js - 1; j <= b1.je + 1; ++j)
       for (int i = b1.is - 1; i <= b1.ie + 1; ++i) {
         u(i, j, k) = pri_v(2, i, j, k);
@@ -648,7 +649,7 @@ static double matrow(const double m[25], int n, V dq, int i, int j, int k) {
   return s;
 }
 
-// sub_timeadvancement_1stimplicit.f90:7-585 (3-D branch).
+// sub_timeadvancement_1stimplicit.f90:7-585 (3-D and 2-D branches).
 void implicit1st(V q, V dt, V pri_v, V rhs, V rhsi, V rhsv, V dxidx, V inv_j, const Box& b,
                  const Box& b0, const Box& b1, double gamma, double cfl) {
   (void)b0;
@@ -658,7 +659,11 @@ void implicit1st(V q, V dt, V pri_v, V rhs, V rhsi, V rhsv, V dxidx, V inv_j, co
       for (int i = b1.is; i <= b1.ie; ++i)
         for (int n = 1; n <= 5; ++n) rhs(n, i, j, k) = rhsi(n, i, j, k) + rhsv(n, i, j, k);
   double phi = cfl >= 1.0e3 ? 0.0 : 1.0;  // :98-102
-  for (int k = b1.ks - 1; k <= b1.ke + 1; ++k)  // :110-156
+  // 2-D (:157-210, :213-278, :388-453): the plane k = 1, no zeta radius in
+  // the diagonal and no zeta neighbour in the sweeps
+  const bool three = g_flags.dimension == IFLAG_3D;
+  const int kx = three ? 1 : 0;
+  for (int k = b1.ks - kx; k <= b1.ke + kx; ++k)  // :110-156
     for (int j = b1.js - 1; j <= b1.je + 1; ++j)
       for (int i = b1.is - 1; i <= b1.ie + 1; ++i) {
         double u = pri_v(2, i, j, k), v = pri_v(3, i, j, k), w = pri_v(4, i, j, k);
@@ -673,7 +678,10 @@ void implicit1st(V q, V dt, V pri_v, V rhs, V rhsi, V rhsv, V dxidx, V inv_j, co
           r3[dd] = std::fabs(cu) + std::fabs(c * temp);
         }
         ra(i, j, k) = r3[0]; rb(i, j, k) = r3[1]; rc(i, j, k) = r3[2];
-        diag(i, j, k) = phi * 1.0 / dt(i, j, k) + ra(i, j, k) + rb(i, j, k) + rc(i, j, k);
+        if (three)
+          diag(i, j, k) = phi * 1.0 / dt(i, j, k) + ra(i, j, k) + rb(i, j, k) + rc(i, j, k);
+        else
+          diag(i, j, k) = phi * 1.0 / dt(i, j, k) + ra(i, j, k) + rb(i, j, k);
       }
   double ma[25], mb[25], mc[25];
   for (int k = b1.ks; k <= b1.ke; ++k)  // forward sweep :279-368
@@ -681,10 +689,14 @@ void implicit1st(V q, V dt, V pri_v, V rhs, V rhsi, V rhsv, V dxidx, V inv_j, co
       for (int i = b1.is; i <= b1.ie; ++i) {
         lusgs_block(ma, q, dxidx, ra(i - 1, j, k), inv_j(i - 1, j, k), 1, i - 1, j, k, gamma, +1);
         lusgs_block(mb, q, dxidx, rb(i, j - 1, k), inv_j(i, j - 1, k), 4, i, j - 1, k, gamma, +1);
-        lusgs_block(mc, q, dxidx, rc(i, j, k - 1), inv_j(i, j, k - 1), 7, i, j, k - 1, gamma, +1);
+        if (three) lusgs_block(mc, q, dxidx, rc(i, j, k - 1), inv_j(i, j, k - 1), 7, i, j, k - 1, gamma, +1);
         for (int n = 0; n < 5; ++n) {
           double ta = matrow(ma, n, dqstar.view, i - 1, j, k);
           double tb = matrow(mb, n, dqstar.view, i, j - 1, k);
+          if (!three) {
+            dqstar(n + 1, i, j, k) = (rhs(n + 1, i, j, k) + (ta + tb)) / diag(i, j, k) / inv_j(i, j, k);
+            continue;
+          }
           double tc = matrow(mc, n, dqstar.view, i, j, k - 1);
           dqstar(n + 1, i, j, k) = (rhs(n + 1, i, j, k) + (ta + tb + tc)) / diag(i, j, k) / inv_j(i, j, k);
         }
@@ -694,10 +706,14 @@ void implicit1st(V q, V dt, V pri_v, V rhs, V rhsi, V rhsv, V dxidx, V inv_j, co
       for (int i = b1.ie; i >= b1.is; --i) {
         lusgs_block(ma, q, dxidx, ra(i + 1, j, k), inv_j(i + 1, j, k), 1, i + 1, j, k, gamma, -1);
         lusgs_block(mb, q, dxidx, rb(i, j + 1, k), inv_j(i, j + 1, k), 4, i, j + 1, k, gamma, -1);
-        lusgs_block(mc, q, dxidx, rc(i, j, k + 1), inv_j(i, j, k + 1), 7, i, j, k + 1, gamma, -1);
+        if (three) lusgs_block(mc, q, dxidx, rc(i, j, k + 1), inv_j(i, j, k + 1), 7, i, j, k + 1, gamma, -1);
         for (int n = 0; n < 5; ++n) {
           double ta = matrow(ma, n, dq.view, i + 1, j, k);
           double tb = matrow(mb, n, dq.view, i, j + 1, k);
+          if (!three) {
+            dq(n + 1, i, j, k) = dqstar(n + 1, i, j, k) - (ta + tb) / inv_j(i, j, k) / diag(i, j, k);
+            continue;
+          }
           double tc = matrow(mc, n, dq.view, i, j, k + 1);
           dq(n + 1, i, j, k) = dqstar(n + 1, i, j, k) - (ta + tb + tc) / inv_j(i, j, k) / diag(i, j, k);
         }
@@ -865,7 +881,10 @@ static void sa_lusgs(V nut, V dt, V sa_rhs, V pri_v, V dxidx, V diasd, double re
                      const Box& b, const Box& b1) {
   Tmp dnut(1, b), dnut1(1, b), diag(1, b), contrau(1, b), contrav(1, b), contraw(1, b);
   double phi = (cfl >= 1.0e3 && g_flags.time == IFLAG_STEADY) ? 0.0 : 1.0;
-  for (int k = b1.ks - 1; k <= b1.ke + 1; ++k)  // :719-753
+  // 2-D (:683-717, :785-806): the plane k = 1, sweeps without the zeta term
+  const bool three = g_flags.dimension == IFLAG_3D;
+  const int kx = three ? 1 : 0;
+  for (int k = b1.ks - kx; k <= b1.ke + kx; ++k)  // :719-753
     for (int j = b1.js - 1; j <= b1.je + 1; ++j)
       for (int i = b1.is - 1; i <= b1.ie + 1; ++i) {
         double u = pri_v(2, i, j, k), v = pri_v(3, i, j, k), w = pri_v(4, i, j, k);
@@ -887,6 +906,10 @@ static void sa_lusgs(V nut, V dt, V sa_rhs, V pri_v, V dxidx, V diasd, double re
       for (int i = b1.is; i <= b1.ie; ++i) {
         double ta = 0.5 * (contrau(i, j, k) + std::fabs(contrau(i, j, k))) * dnut1(i - 1, j, k);
         double tb = 0.5 * (contrav(i, j, k) + std::fabs(contrav(i, j, k))) * dnut1(i, j - 1, k);
+        if (!three) {
+          dnut1(i, j, k) = (sa_rhs(i, j, k) + (ta + tb)) / diag(i, j, k);
+          continue;
+        }
         double tc = 0.5 * (contraw(i, j, k) + std::fabs(contraw(i, j, k))) * dnut1(i, j, k - 1);
         dnut1(i, j, k) = (sa_rhs(i, j, k) + (ta + tb + tc)) / diag(i, j, k);
       }
@@ -895,6 +918,10 @@ static void sa_lusgs(V nut, V dt, V sa_rhs, V pri_v, V dxidx, V diasd, double re
       for (int i = b1.ie; i >= b1.is; --i) {
         double ta = 0.5 * (contrau(i, j, k) - std::fabs(contrau(i, j, k))) * dnut(i + 1, j, k);
         double tb = 0.5 * (contrav(i, j, k) - std::fabs(contrav(i, j, k))) * dnut(i, j + 1, k);
+        if (!three) {
+          dnut(i, j, k) = dnut1(i, j, k) - (ta + tb) / diag(i, j, k);
+          continue;
+        }
         double tc = 0.5 * (contraw(i, j, k) - std::fabs(contraw(i, j, k))) * dnut(i, j, k + 1);
         dnut(i, j, k) = dnut1(i, j, k) - (ta + tb + tc) / diag(i, j, k);
       }
@@ -1002,7 +1029,10 @@ void crank2nd(V q, V q0, V dt, V pri_v, V rhs, V rhsi, V rhsv, V dxidx, V inv_j,
                                        alph * Q0(q0, -1, c, i, j, k)) * inv_j(i, j, k));
   std::vector<double> dtsub_s(b.size(), 0.0), rou_s(b.size(), 0.0), dq_s(5 * (size_t)b.size(), 0.0);
   V dtsub{dtsub_s.data(), 1, b}, rou{rou_s.data(), 1, b}, dq{dq_s.data(), 5, b};
-  for (int k = b1.ks - 1; k <= b1.ke + 1; ++k)
+  // 2-D (sub_timeadvancement_2ndcrank.f90:84-99, :335): the plane k = 1, no k lines
+  const bool three = g_flags.dimension == IFLAG_3D;
+  const int kx = three ? 1 : 0;
+  for (int k = b1.ks - kx; k <= b1.ke + kx; ++k)
     for (int j = b1.js - 1; j <= b1.je + 1; ++j)
       for (int i = b1.is - 1; i <= b1.ie + 1; ++i) dtsub(i, j, k) = dt(i, j, k) / (1.0 + alph);
   double s[5], a[5];
@@ -1044,7 +1074,7 @@ void crank2nd(V q, V q0, V dt, V pri_v, V rhs, V rhsi, V rhsv, V dxidx, V inv_j,
       }
     }
   // k lines
-  for (int j = b1.js; j <= b1.je; ++j)
+  for (int j = b1.js; j <= b1.je && three; ++j)
     for (int i = b1.is; i <= b1.ie; ++i) {
       for (int k = b1.ks - 1; k <= b1.ke + 1; ++k) rou(i, j, k) = crank_rou(pri_v, dxidx, 7, i, j, k);
       for (int k = b1.ks + 1; k <= b1.ke; ++k) {

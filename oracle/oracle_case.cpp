@@ -250,9 +250,22 @@ void physical_bc() {
 }
 
 // ------------------------------------------------------------------ halo
+// 2-D mode (UpdateBuffer2d, UpdateBufferCoordinate2d, average2d1 in
+// sub_bc_updatebuffer2d.f90, sub_bc_updatebuffercoordinate2d.f90,
+// sub_bc_updatebufferaverage2d.f90): a face is a line, ua(ll) runs along it
+// (j on faces 1/2, i on faces 3/4) with nn = max(n11, n12) of the donor
+// subface (:218-222), ori 2 keeps the order and ori 3 reverses it (:284-293);
+// every map below takes (l, m) = (ll, 1) there.
+static bool two_d() { return g_flags.dimension == IFLAG_2D; }
+
 // Donor-face (l,m) indexing of a received subface (sub_bc_updatebuffer.f90:265-354).
 static void donor_lm(const Sub& d, int& l1, int& m1) {
   int n11 = d.ie - d.is + 1, n12 = d.je - d.js + 1, n13 = d.ke - d.ks + 1;
+  if (two_d()) {
+    l1 = std::max(n11, n12);
+    m1 = 1;
+    return;
+  }
   switch (d.face) {
     case 1: l1 = n13; m1 = n12; break;
     case 2: l1 = n12; m1 = n13; break;
@@ -263,6 +276,16 @@ static void donor_lm(const Sub& d, int& l1, int& m1) {
   }
 }
 static void donor_node(const Sub& d, int ll0, int mm0, int& i, int& j, int& k) {
+  if (two_d()) {
+    k = d.ks;
+    switch (d.face) {
+      case 1: i = d.is; j = d.js + ll0 - 1; break;
+      case 2: i = d.ie; j = d.js + ll0 - 1; break;
+      case 3: i = d.is + ll0 - 1; j = d.js; break;
+      default: i = d.is + ll0 - 1; j = d.je; break;
+    }
+    return;
+  }
   switch (d.face) {
     case 1: i = d.is; j = d.js + mm0 - 1; k = d.ks + ll0 - 1; break;
     case 2: i = d.ie; j = d.js + ll0 - 1; k = d.ks + mm0 - 1; break;
@@ -274,9 +297,19 @@ static void donor_node(const Sub& d, int ll0, int mm0, int& i, int& j, int& k) {
 }
 // Reorientation by ori (:358-395): element (ll,mm) of ua2 comes from ua(la,ma).
 static void ori_map(int ori, int l1, int m1, int& l2, int& m2) {
+  if (two_d()) { l2 = l1; m2 = m1; return; }
   if (ori == 2 || ori == 4) { l2 = m1; m2 = l1; } else { l2 = l1; m2 = m1; }
 }
 static void ori_src(int ori, int l1, int m1, int ll, int mm, int& la, int& ma) {
+  if (two_d()) {
+    if (ori != 2 && ori != 3) {
+      std::fprintf(stderr, "oracle: 2-D interface orientation %d (only 2 and 3 are defined)\n", ori);
+      std::abort();
+    }
+    la = ori == 2 ? ll : l1 - ll + 1;
+    ma = mm;
+    return;
+  }
   switch (ori) {
     case 1: la = ll; ma = m1 - mm + 1; break;
     case 2: la = mm; ma = ll; break;
@@ -287,6 +320,16 @@ static void ori_src(int ori, int l1, int m1, int ll, int mm, int& la, int& ma) {
 // Own-face node written by element (a,b) of ua2 (:398-540), plus the outward step.
 static void own_node(const Sub& s, int a, int bidx, int& i, int& j, int& k, int& di, int& dj, int& dk) {
   di = dj = dk = 0;
+  if (two_d()) {
+    k = s.ks;
+    switch (s.face) {
+      case 1: i = s.is; j = s.js + a - 1; di = -1; break;
+      case 2: i = s.ie; j = s.js + a - 1; di = 1; break;
+      case 3: i = s.is + a - 1; j = s.js; dj = -1; break;
+      default: i = s.is + a - 1; j = s.je; dj = 1; break;
+    }
+    return;
+  }
   switch (s.face) {
     case 1: i = s.is; j = s.js + bidx - 1; k = s.ks + a - 1; di = -1; break;
     case 2: i = s.ie; j = s.js + a - 1; k = s.ks + bidx - 1; di = 1; break;
@@ -484,6 +527,49 @@ void clcd_output(double sref, double out[14]) {
     V pri = B.v(F_PRI), m = B.v(F_DXIDX), amu = B.v(F_AMU);
     for (auto& s : B.bc) {
       if (s.blk_t != BC_WALL) continue;
+      if (two_d()) {
+        // sub_output_forceintegration.f90:48-180: the wall is a line; each
+        // edge (t, t+1) averages velocity and the unit normal over the two
+        // nodes one layer in, pressure and viscosity over the two wall nodes
+        // (face 3 averages the viscosity with 0.25, :128), s = the edge's
+        // spacing along the wall, dn = the mean spacing normal to it
+        const int k = s.ks;
+        const bool iface = s.face <= 2;
+        const bool low = s.face % 2 == 1;
+        const double sgn = low ? -1.0 : 1.0;
+        const int w = iface ? (low ? s.is : s.ie) : (low ? s.js : s.je);
+        const int w1 = low ? w + 1 : w - 1;
+        const int lo = iface ? s.js : s.is, hi = iface ? s.je : s.ie;
+        const int c1 = iface ? 1 : 4;
+        const double mfac = s.face == 3 ? 0.25 : 0.5;
+        for (int t = lo; t <= hi - 1; ++t) {
+          const int ia = iface ? w1 : t, ja = iface ? t : w1, ib = iface ? w1 : t + 1, jb = iface ? t + 1 : w1;
+          const int iwa = iface ? w : t, jwa = iface ? t : w, iwb = iface ? w : t + 1, jwb = iface ? t + 1 : w;
+          double uc = (pri(2, ia, ja, k) + pri(2, ib, jb, k)) * 0.5;
+          double vc = (pri(3, ia, ja, k) + pri(3, ib, jb, k)) * 0.5;
+          double wc = 0.0;
+          double pc = (pri(5, iwa, jwa, k) + pri(5, iwb, jwb, k)) * 0.5;
+          double t00 = 1.0 / std::sqrt(p2(m(c1, ia, ja, k)) + p2(m(c1 + 1, ia, ja, k)) + p2(m(c1 + 2, ia, ja, k)));
+          double t10 = 1.0 / std::sqrt(p2(m(c1, ib, jb, k)) + p2(m(c1 + 1, ib, jb, k)) + p2(m(c1 + 2, ib, jb, k)));
+          double n3[3];
+          for (int x = 0; x < 3; ++x) n3[x] = sgn * ((m(c1 + x, ia, ja, k) * t00 + m(c1 + x, ib, jb, k) * t10) * 0.5);
+          double miuc = (amu(3, iwa, jwa, k) + amu(3, iwb, jwb, k)) * mfac;
+          double area = iface ? spcv[1](1, w, t, k) : spcv[0](1, t, w, k);
+          double dn = iface ? 0.5 * (spcv[0](1, w, t, k) + spcv[0](1, w, t + 1, k))
+                            : (spcv[1](1, t, w, k) + spcv[1](1, t + 1, w, k)) * 0.5;
+          double u3[3] = {uc, vc, wc};
+          double un = uc * n3[0] + vc * n3[1] + wc * n3[2];
+          for (int x = 0; x < 3; ++x) {
+            double f_prs = (pc - pinf) * area * n3[x];
+            double f_vis = miuc * (u3[x] - un * n3[x]) / dn * area / c.re;
+            fp[x] = fp[x] + f_prs;
+            fv[x] = fv[x] + f_vis;
+            ap[x] += std::fabs(f_prs);
+            av[x] += std::fabs(f_vis);
+          }
+        }
+        continue;
+      }
       const int D = (s.face - 1) / 2;
       const bool low = s.face % 2 == 1;
       const int lo[3] = {s.is, s.js, s.ks}, hi[3] = {s.ie, s.je, s.ke};

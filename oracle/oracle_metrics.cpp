@@ -56,7 +56,7 @@ void region_derivative(V src, V dst, int nc, int dir, const Box& b, const Box& b
 
 }  // namespace
 
-// sub_init_gridtransformation.f90:27-874 (3-D branch).  Nodes with two or more
+// sub_init_gridtransformation.f90:27-874 (3-D and 2-D branches).  Nodes with two or more
 // indices in ghost layers (block corners/edges of the overlap) are never
 // written by the reference; inv_j, dxidx, alpha, beta, gamma keep whatever the
 // caller stored there (zero-filled arrays give 0 for inv_j and NaN = 0/0 for the
@@ -75,7 +75,18 @@ void gridtransformation(V dxidx, V inv_j, V alpha, V beta, V gamma, V x, V y, V 
       }
   region_derivative(xyz.view, dxdxi.view, 3, 0, b, b0);
   region_derivative(xyz.view, dxdeta.view, 3, 1, b, b0);
-  region_derivative(xyz.view, dxdzeta.view, 3, 2, b, b0);
+  const bool two = g_flags.dimension == IFLAG_2D;
+  if (two) {  // :270-273: the zeta direction is the unit z vector everywhere
+    for (int k = b.ks; k <= b.ke; ++k)
+      for (int j = b.js; j <= b.je; ++j)
+        for (int i = b.is; i <= b.ie; ++i) {
+          dxdzeta(1, i, j, k) = 0.0;
+          dxdzeta(2, i, j, k) = 0.0;
+          dxdzeta(3, i, j, k) = 1.0;
+        }
+  } else {
+    region_derivative(xyz.view, dxdzeta.view, 3, 2, b, b0);
+  }
 
   auto jac = [&](int i, int j, int k) {  // :366-371
     double dxdxi0 = dxdxi(1, i, j, k), dxdeta0 = dxdeta(1, i, j, k), dxdzeta0 = dxdzeta(1, i, j, k);
@@ -105,7 +116,23 @@ void gridtransformation(V dxidx, V inv_j, V alpha, V beta, V gamma, V x, V y, V 
       for (int k = b0.ke; k <= b.ke; ++k) jac(i, j, k);
     }
 
-  for (int k = b.ks; k <= b.ke; ++k)  // :559-584
+  if (two) {  // :543-557: in-plane metrics from the in-plane derivatives
+    for (int k = b.ks; k <= b.ke; ++k)
+      for (int j = b.js; j <= b.je; ++j)
+        for (int i = b.is; i <= b.ie; ++i) {
+          double ij = inv_j(i, j, k);
+          dxidx(1, i, j, k) = dxdeta(2, i, j, k) / ij;
+          dxidx(2, i, j, k) = -dxdeta(1, i, j, k) / ij;
+          dxidx(3, i, j, k) = 0.0;
+          dxidx(4, i, j, k) = -dxdxi(2, i, j, k) / ij;
+          dxidx(5, i, j, k) = dxdxi(1, i, j, k) / ij;
+          dxidx(6, i, j, k) = 0.0;
+          dxidx(7, i, j, k) = 0.0;
+          dxidx(8, i, j, k) = 0.0;
+          dxidx(9, i, j, k) = 1.0;
+        }
+  }
+  for (int k = b.ks; k <= b.ke && !two; ++k)  // :559-584
     for (int j = b.js; j <= b.je; ++j)
       for (int i = b.is; i <= b.ie; ++i) {
         double X = xyz(1, i, j, k), Y = xyz(2, i, j, k), Z = xyz(3, i, j, k);
@@ -128,11 +155,13 @@ void gridtransformation(V dxidx, V inv_j, V alpha, V beta, V gamma, V x, V y, V 
         tempzeta(5, i, j, k) = dxdxi(3, i, j, k) * X;
         tempzeta(6, i, j, k) = dxdxi(1, i, j, k) * Y;
       }
-  region_derivative(tempxi.view, tempxixi.view, 6, 0, b, b0);        // :587-655
-  region_derivative(tempeta.view, tempetaeta.view, 6, 1, b, b0);     // :658-726
-  region_derivative(tempzeta.view, tempzetazeta.view, 6, 2, b, b0);  // :729-797
+  if (!two) {
+    region_derivative(tempxi.view, tempxixi.view, 6, 0, b, b0);        // :587-655
+    region_derivative(tempeta.view, tempetaeta.view, 6, 1, b, b0);     // :658-726
+    region_derivative(tempzeta.view, tempzetazeta.view, 6, 2, b, b0);  // :729-797
+  }
 
-  for (int k = b.ks; k <= b.ke; ++k)  // :799-831
+  for (int k = b.ks; k <= b.ke && !two; ++k)  // :799-831
     for (int j = b.js; j <= b.je; ++j)
       for (int i = b.is; i <= b.ie; ++i) {
         double ij = inv_j(i, j, k);

@@ -32,7 +32,7 @@ def _configure(L, **over):
 
 
 @pytest.mark.parametrize("over, text", [
-    (dict(dimension=2), b"3-D"),
+    (dict(dimension=1), b"iflag_dimension"),
     (dict(solver=5), b"iflag_solver"),
     (dict(time=0, timeadvance=3), b"iflag_time"),
     (dict(time=1, timeadvance=2), b"iflag_time"),
@@ -50,7 +50,7 @@ def test_unsupported_flags_are_rejected(lib, over, text):
 
 def test_supported_extensions_are_accepted(lib):
     for over in (dict(inviscid=5, buffer=3), dict(inviscid=8, buffer=3), dict(turbulence=2, des=1),
-                 dict(turbulence=2, des=2), dict(time=1, timeadvance=3)):
+                 dict(turbulence=2, des=2), dict(time=1, timeadvance=3), dict(dimension=2)):
         assert _configure(lib, **over) == 0, over
 
 
