@@ -29,7 +29,7 @@ from typing import Iterator, List, Sequence, Tuple
 
 import numpy as np
 
-from .case import Block, Case, Config, Subface, IFLAG_3D, buffer_length_for
+from .case import Block, Case, Config, Subface, IFLAG_2D, IFLAG_3D, buffer_length_for
 
 _TOKEN = re.compile(r"'[^']*'|\"[^\"]*\"|[^\s,]+")
 
@@ -77,6 +77,14 @@ class _Reader:
             vals.extend(_tokens(self.lines[self.pos]))
             self.pos += 1
         return vals[:n]
+
+    def read_records(self, n: int, m: int) -> np.ndarray:
+        """n read statements of m values each: every read starts on a new
+        record and drops what is left of its last one."""
+        out = np.empty((n, m))
+        for r in range(n):
+            out[r] = [_num(t) for t in self.read(m)]
+        return out
 
     def read_array(self, n: int) -> np.ndarray:
         out = np.empty(n)
@@ -298,19 +306,25 @@ def save_case(case: Case, directory: str, control: Control = None) -> str:
 
 # ------------------------------------------------- flow field output / restart
 def write_flowfield(path: str, case: Case) -> None:
-    """flowfield_output (sub_output_flowfield.f90:15-90, 3-D): per block a
+    """flowfield_output (sub_output_flowfield.f90:15-90): per block a
     Tecplot point-format zone of x, y, z, d, u, v, w, p, nut over the physical
-    nodes, i fastest, from the case's host arrays (sync them from the device
-    first).  Values carry 17 significant digits, so the file restarts a run
-    exactly as the reference's list-directed output does."""
+    nodes, i fastest (2-D, :36-57: x, y, d, u, v, w, p, nut and no k
+    extent), from the case's host arrays (sync them from the device first).
+    Values carry 17 significant digits, so the file restarts a run exactly as
+    the reference's list-directed output does."""
+    two = case.cfg.dimension == IFLAG_2D
     with open(path, "w") as f:
         for b in case.blocks:
             s = b.sl(b.box0)
             pri = b.fields["pri_v"][s]
-            cols = [b.fields["x"][s], b.fields["y"][s], b.fields["z"][s]] + [pri[..., c] for c in range(5)] + \
-                   [b.fields["nut"][s]]
-            f.write(" variables = x,y,z,d,u,v,w,p,nut\n")
-            f.write(f" zone i= {b.ni} j= {b.nj} k= {b.nk} datapacking=point\n")
+            xyz = [b.fields["x"][s], b.fields["y"][s]] + ([] if two else [b.fields["z"][s]])
+            cols = xyz + [pri[..., c] for c in range(5)] + [b.fields["nut"][s]]
+            if two:
+                f.write(" variables = x,y,d,u,v,w,p,nut\n")
+                f.write(f" zone i= {b.ni} j= {b.nj} datapacking=point\n")
+            else:
+                f.write(" variables = x,y,z,d,u,v,w,p,nut\n")
+                f.write(f" zone i= {b.ni} j= {b.nj} k= {b.nk} datapacking=point\n")
             table = np.stack([c.ravel() for c in cols], axis=1)
             for row in table:
                 f.write(" ".join(f"{v:.17e}" for v in row) + "\n")
@@ -350,24 +364,37 @@ def read_surface(path: str) -> List[Tuple[Tuple[int, int, int], np.ndarray]]:
 
 
 def read_restart(path: str, case: Case) -> None:
-    """The restart branch of sub_init_flowfield.f90:117-268 (iflag_init = 1,
-    3-D): reads a flowfield file written by flowfield_output and sets, on the
+    """The restart branch of sub_init_flowfield.f90:117-268 (iflag_init = 1):
+    reads a flowfield file written by flowfield_output and sets, on the
     physical nodes of every block, q from (d, u, v, w, p), the primitive
     variables the reference derives there, rhs = rhsi = rhsv = 0, dt = the
     Control.in dt, amu(1) = 1 and, with SA, nut.  The derived primitives keep
     the reference's expressions, including q2 = d**2 + u**2 + v**2 and
-    c = sqrt(p)/ma; the iteration's start-up recomputes them from q."""
+    c = sqrt(p)/ma; the iteration's start-up recomputes them from q.
+
+    2-D (:163-210): each record holds seven values, x, y, d, u, v, p, nut (the
+    reference reads no w there; its w array is never set on that branch and
+    is taken as 0 here).  A 2-D file of flowfield_output has eight columns
+    (w before p), which this record layout reads as the reference does: the
+    first seven values of each line."""
     cfg = case.cfg
     gamma = 1.4
     ma = cfg.ma
     cv = 1.0 / gamma / (gamma - 1.0) / ma / ma
+    two = cfg.dimension == IFLAG_2D
     r = _Reader(path)
     for b in case.blocks:
         r.skip(2)
         n = b.ni * b.nj * b.nk
-        vals = r.read_array(9 * n).reshape(n, 9)
-        col = lambda c: vals[:, c].reshape(b.nk, b.nj, b.ni)
-        d, u, v, w, p, tur = col(3), col(4), col(5), col(6), col(7), col(8)
+        if two:
+            rows = r.read_records(n, 7)
+            col = lambda c: rows[:, c].reshape(b.nk, b.nj, b.ni)
+            d, u, v, p, tur = col(2), col(3), col(4), col(5), col(6)
+            w = np.zeros_like(d)
+        else:
+            vals = r.read_array(9 * n).reshape(n, 9)
+            col = lambda c: vals[:, c].reshape(b.nk, b.nj, b.ni)
+            d, u, v, w, p, tur = col(3), col(4), col(5), col(6), col(7), col(8)
         s = b.sl(b.box0)
         t = p / d * gamma * ma * ma
         q = b.fields["q"][s]

@@ -23,9 +23,13 @@
  *    its module state.
  *
  * One host thread drives the library; calls run in order on the library's
- * CUDA stream.  Only 3-D cases (iflag_dimension = 3) are supported, with the
- * steady 1st-order implicit (LU-SGS) or the unsteady 2nd-order Crank-Nicolson
- * time advance; other flags are rejected.
+ * CUDA stream.  3-D cases (iflag_dimension = 3) and 2-D cases
+ * (iflag_dimension = 2: every block the single plane k = 1, faces 1-4 only,
+ * interface orientation codes 2 and 3 as UpdateBuffer2d reads them) are
+ * supported, with the steady 1st-order implicit (LU-SGS) or the unsteady
+ * 2nd-order Crank-Nicolson time advance; other flags are rejected.  Transient
+ * calls take boxes of one k-plane in a 2-D configuration and of at least three
+ * in a 3-D one.
  */
 #ifndef AEROCFD_GPU_H
 #define AEROCFD_GPU_H
@@ -229,7 +233,8 @@ int aero_sa_model(double* nut, double* sa_rhs, const double* dt, const double* p
                   const int* ke, const int* is0, const int* ie0, const int* js0, const int* je0,
                   const int* ks0, const int* ke0, const int* is1, const int* ie1, const int* js1,
                   const int* je1, const int* ks1, const int* ke1);
-/* sub_init_gridtransformation.f90:27-29 (3-D): metrics, 1/J, alpha/beta/gamma.
+/* sub_init_gridtransformation.f90:27-29 (3-D and 2-D branches): metrics,
+ * 1/J, alpha/beta/gamma.
  * Ghost-corner nodes (two or more indices in overlap layers) are left as the
  * caller stored them, as in the reference. */
 int aero_gridtransformation(double* dxidx, double* inv_j, double* alpha, double* beta, double* gamma,
@@ -238,7 +243,7 @@ int aero_gridtransformation(double* dxidx, double* inv_j, double* alpha, double*
                             const int* ke, const int* is0, const int* ie0, const int* js0,
                             const int* je0, const int* ks0, const int* ke0, const int* m0);
 
-/* sub_timeadvancement_2ndcrank.f90:1-11 (crank2nd, 3-D): the dual-time
+/* sub_timeadvancement_2ndcrank.f90:1-11 (crank2nd; 2-D: no k lines): the dual-time
  * Crank-Nicolson sub-iteration update of q (alph = 1/2) with the factorised
  * point-implicit i, j, k line recurrences; q0 is q0(-1:0,5,is:ie,js:je,ks:ke).
  * mm and ssub are accepted for the reference's argument list. */
@@ -255,6 +260,10 @@ int aero_update_q0(double* q0, const double* q, const int* is, const int* ie, co
 
 /* ---- module-state routines (no arguments in the reference) ------------ */
 int aero_physical_bc(void);          /* sub_bc.f90:9                        */
+/* In a 2-D configuration these four are UpdateBuffer2d
+ * (sub_bc_updatebuffer2d.f90:10), average2d1 / average2d2
+ * (sub_bc_updatebufferaverage2d.f90:10, :317) and UpdateBufferCoordinate2d
+ * (sub_bc_updatebuffercoordinate2d.f90:10). */
 int aero_updatebuffer(void);         /* sub_bc_updatebuffer.f90:10          */
 int aero_average1(void);             /* sub_bc_updatebufferaverage.f90:10   */
 int aero_average2(void);             /* sub_bc_updatebufferaverage.f90:442  */
@@ -263,7 +272,8 @@ int aero_updatebuffercoordinate(void); /* sub_bc_updatebuffercoordinate.f90:10 *
  * nut, (unused) over the updated nodes / totalnodes; the reference prints
  * these and appends them to resi_history.dat. */
 int aero_residual(double* out7);
-/* sub_output_forceintegration.f90:8-479 (clcd_output, 3-D): pressure and
+/* sub_output_forceintegration.f90:8-479 (clcd_output, 3-D quads and 2-D
+ * wall edges): pressure and
  * viscous forces over every wall subface (blk_t = -20) of the registered
  * blocks from their current pri_v, dxidx, amu and x, y, z, then the lift and
  * drag coefficients.  out8 = fpx, fpy, fpz, fvx, fvy, fvz, cl, cd (what the

@@ -125,3 +125,53 @@ def test_surface_file_round_trip(tmp_path):
     assert [z for z, _ in back] == [(5, 1, 3), (0, 1, 3), (2, 4, 1)]
     assert np.array_equal(np.concatenate([r for _, r in back]), rows)
     assert io.surface_path(12, 3) == "result/surfcp_000012_0003.dat"
+
+
+def test_flowfield_and_restart_2d(tmp_path):
+    """2-D mode: flowfield_output writes x, y, d, u, v, w, p, nut and a zone
+    without a k extent (sub_output_flowfield.f90:36-57); the 2-D restart
+    (sub_init_flowfield.f90:163-210) reads seven values per record, x, y, d,
+    u, v, p, nut, with w = 0."""
+    from aerocfd_b200.case import IFLAG_2D
+    case = grids.bump_channel_2d(ni=9, nj=5)
+    rng = np.random.default_rng(0)
+    for b in case.blocks:
+        s = b.sl(b.box0)
+        b.fields["pri_v"][s] = 1.0 + rng.random(b.fields["pri_v"][s].shape)
+        b.fields["nut"][s] = rng.random(b.fields["nut"][s].shape)
+    path = tmp_path / "ff2d.dat"
+    io.write_flowfield(str(path), case)
+    lines = path.read_text().splitlines()
+    assert lines[0].split() == ["variables", "=", "x,y,d,u,v,w,p,nut"]
+    assert lines[1].split() == ["zone", "i=", str(case.blocks[0].ni), "j=", str(case.blocks[0].nj),
+                                "datapacking=point"]
+    assert len(lines[2].split()) == 8
+    # a restart file in the 2-D record layout (seven values per line)
+    rst = tmp_path / "restart2d.dat"
+    want = {}
+    with open(rst, "w") as f:
+        for b in case.blocks:
+            n = b.ni * b.nj
+            vals = 0.5 + rng.random((n, 7))
+            want[b.m] = vals
+            f.write(" variables = x,y,d,u,v,p,nut\n zone\n")
+            for row in vals:
+                f.write(" ".join(f"{v:.17e}" for v in row) + "\n")
+    cb = grids.bump_channel_2d(ni=9, nj=5)
+    cb.cfg.turbulence = 2
+    io.read_restart(str(rst), cb)
+    for b in cb.blocks:
+        s = b.sl(b.box0)
+        v = want[b.m]
+        col = lambda c: v[:, c].reshape(1, b.nj, b.ni)
+        d, u, vv, p = col(2), col(3), col(4), col(5)
+        q = b.fields["q"][s]
+        assert np.array_equal(q[..., 0], d)
+        assert np.array_equal(q[..., 1], d * u) and np.array_equal(q[..., 2], d * vv)
+        assert np.all(q[..., 3] == 0.0)
+        assert np.array_equal(b.fields["nut"][s], col(6))
+        gamma, ma = 1.4, cb.cfg.ma
+        cv = 1.0 / gamma / (gamma - 1.0) / ma / ma
+        t = p / d * gamma * ma * ma
+        assert np.array_equal(q[..., 4], d * t * cv + 0.5 * d * (u * u + vv * vv + 0.0 * 0.0))
+    assert cb.cfg.dimension == IFLAG_2D
