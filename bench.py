@@ -380,6 +380,47 @@ def plate_cf(case) -> np.ndarray:
     return np.array(out)
 
 
+def batched_split_gpu(solver, steps: int, warmup: int, rank: int, world: int, dist):
+    """At N > 1: the 64-case batch of ``batched_gpu`` split over the ranks by
+    whole cases (longest-processing-time on node counts,
+    aerocfd_b200/distribute.py), each rank's share one batch in mixed
+    precision with CUDA-graph replay and its own autotuned launch shapes; no
+    data moves between ranks.  The job's time is the slowest rank's device
+    time (max over ranks), so `value` is the whole list's node updates per
+    second: strong scaling over the fixed list."""
+    import torch
+    from aerocfd_b200 import _lib, distribute, grids
+    cases = grids.bump_batch(64, seed=0)
+    nodes = [c.nodes for c in cases]
+    parts = distribute.assign(nodes, world)
+    mine = [cases[i] for i in parts[rank]]
+    batch, params = grids.batch_case(mine)
+    gc = solver.GpuCase(batch, block_params=params)
+    ms = ctypes.c_double(0.0)
+    try:
+        gc.compute_geometry()
+        gc.init_flowfield()
+        gc.start()
+        gc.set_precision(True)
+        gc.autotune(3)
+        gc.use_graphs(True)
+        gc.step(warmup, history=False)
+        torch.cuda.synchronize()
+        dist.barrier()
+        _lib.check(gc.L.aero_step_timed(ctypes.c_int(steps), ctypes.c_int(1), ctypes.byref(ms)), "split timed")
+        status = gc.status()
+    finally:
+        gc.close()
+    t = max_over_ranks(ms.value / 1e3, dist)
+    bad = max_over_ranks(float(status != 0), dist)
+    total = sum(nodes)
+    return {"workload": BATCH_WORKLOAD, "cases": len(cases), "nodes": total, "steps": steps,
+            "value": total * steps / t / 1e6, "unit": "Mcell-iter/s", "ms_per_step": 1e3 * t / steps,
+            "scaling": "strong", "split": "whole cases per rank, longest-processing-time on node counts",
+            "rank_nodes": [sum(nodes[i] for i in p) for p in parts], "rank_cases": [len(p) for p in parts],
+            "precision": "mixed", "any_rank_status_nonzero": bool(bad)}
+
+
 def sa_plate_gpu(solver, its: int = 3000, chunk: int = 500):
     """The headline plate run from the freestream for `its` iterations in
     FP64 and in mixed precision (autotuned shapes, CUDA graphs): the residual
@@ -878,6 +919,9 @@ def main():
             nm["cpu_baseline"] = {"value": v, "unit": "Mcell-iter/s", "cores": thr, "kind": "port",
                                   "sample": f"{n} full iterations, {el:.1f} s, {thr} threads (one per block)"}
         line["naca"] = nm
+    if world > 1 and not args.no_batch:
+        line["batched_split"] = batched_split_gpu(solver, max(5, min(args.steps, 20)), args.warmup, rank, world,
+                                                  dist)
     if world == 1 and not args.no_batch:
         line["batched"] = batched_gpu(solver, max(5, min(args.steps, 20)), args.warmup)
     if world == 1 and not args.no_schemes:
