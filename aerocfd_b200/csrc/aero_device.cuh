@@ -245,6 +245,44 @@ enum StatusBits : unsigned {
 // its neighbours in the cluster)
 // Ring, inbox and staging slots (planes) of a slab sweep, at most.
 constexpr int kSlabSlots = 8;
+// Nanoseconds of the GPU's global timer.
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Bound of every wait of the cluster sweeps: a wait not satisfied within
+// kWaitNs of the global timer (or, as a second bound, within 2^30 polls)
+// gives up, and the sweep ends with ST_TIMEOUT.  A plane step takes
+// microseconds, so the bound only ends a wait that cannot finish.
+constexpr unsigned long long kWaitNs = 1000000000ull;
+// Polls `done` until it holds (true) or the bound passes (false); the timer is
+// read every 64 polls.
+template <class Done>
+__device__ __forceinline__ bool wait_bounded(Done done) {
+  if (done()) return true;
+  const unsigned long long t0 = global_ns();
+  for (unsigned n = 1; n < (1u << 30); ++n) {
+    if (done()) return true;
+    if ((n & 63u) == 0u && global_ns() - t0 > kWaitNs) return false;
+  }
+  return false;
+}
+// Sweep codes and wait kinds of the first wait that gave up, recorded in
+// status words 1..6 (aero_timeout_site): word 1 claims the record, then the
+// sweep, the block, the CTA's rank in its cluster, the step and the wait.
+enum TimeoutSweep { TS_BULK = 1, TS_SLAB = 2, TS_SA_SLAB = 3 };
+enum TimeoutWait { TW_PLANE = 1, TW_PROGRESS = 2, TW_LAST_PLANE = 3 };
+__device__ __forceinline__ void note_timeout(unsigned* status, int sweep, int block, int rank, int step,
+                                             int wait) {
+  if (!status || atomicCAS(status + 1, 0u, 1u) != 0u) return;
+  status[2] = (unsigned)sweep;
+  status[3] = (unsigned)block;
+  status[4] = (unsigned)rank;
+  status[5] = (unsigned)step;
+  status[6] = (unsigned)wait;
+}
+
 namespace slab {
 __device__ __forceinline__ unsigned rank() {
   unsigned r;
@@ -295,13 +333,10 @@ __device__ __forceinline__ bool bar_try(unsigned long long* bar, unsigned parity
       : "memory");
   return ok != 0;
 }
-// bounded wait for the phase of `bar` with this parity; false when it did not
-// complete within `limit` polls
-__device__ __forceinline__ bool bar_wait(unsigned long long* bar, unsigned parity, long limit) {
-  long spins = 0;
-  while (!bar_try(bar, parity))
-    if (++spins > limit) return false;
-  return true;
+// bounded wait for the phase of `bar` with this parity; false when it did
+// not complete within the wait bound (wait_bounded)
+__device__ __forceinline__ bool bar_wait(unsigned long long* bar, unsigned parity) {
+  return wait_bounded([&] { return bar_try(bar, parity); });
 }
 // bulk copy of `bytes` from this CTA's shared memory into another CTA's of the
 // cluster, counted in bytes on the receiver's mbarrier (no multicast); both
@@ -315,12 +350,9 @@ __device__ __forceinline__ void copy_to(unsigned dst, unsigned src, unsigned byt
 // this thread's shared-memory writes visible to the bulk copies it issues next
 __device__ __forceinline__ void fence_to_copies() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 // Bounded wait until a counter of this CTA (written by a neighbour with
-// store_relaxed) reaches v; false when it did not within `limit` polls.
-__device__ __forceinline__ bool wait_for(const int* counter, int v, long limit) {
-  long spins = 0;
-  while (load_relaxed(counter) < v)
-    if (++spins > limit) return false;
-  return true;
+// store_relaxed) reaches v; false when it did not within the wait bound.
+__device__ __forceinline__ bool wait_for(const int* counter, int v) {
+  return wait_bounded([&] { return load_relaxed(counter) >= v; });
 }
 // L2 prefetch of [p, p + bytes) widened to 16-byte boundaries; the caller
 // keeps the widened range inside one allocation

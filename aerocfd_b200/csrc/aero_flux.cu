@@ -164,32 +164,39 @@ __device__ __forceinline__ void roe_face(const BlockView& B, int coord, long n, 
 // Flux through face pos+1/2 along `coord` starting at node (i,j,k); pos is the
 // node's index along coord, lo/hi the full-box bounds along coord, st the
 // linear stride along coord.
-__device__ __forceinline__ void face_flux(const BlockView& B, int coord, long n, int pos, int lo,
-                                          int hi, long st, double gamma, double flux[5]) {
+// q(c, m) supplies q's component c at node index m (global memory, or a
+// shared-memory copy in the staged face kernel).
+template <class Q>
+__device__ __forceinline__ void face_flux_q(const BlockView& B, int coord, long n, int pos, int lo, int hi,
+                                            long st, double gamma, double flux[5], Q q) {
   double ulc[5], urc[5];
   bool rone = (pos == hi - 1);  // right state one-sided at ie-1 (:25-26)
   bool lone = (pos == lo);      // left state one-sided at is (:50-51)
 #pragma unroll
   for (int c = 1; c <= 5; ++c) {
-    double f0 = B.v(F_Q, c, n);
-    double fp = B.v(F_Q, c, n + st);
+    double f0 = q(c, n);
+    double fp = q(c, n + st);
     // the weight of the face's own difference serves both states (the
     // reference's s2 of each)
     const double a_mid = (rone && lone) ? 0.0 : weno_weight(fp - f0);
     if (rone) {
       urc[c - 1] = fp;
     } else {
-      double fpp = B.v(F_Q, c, n + 2 * st);
+      double fpp = q(c, n + 2 * st);
       urc[c - 1] = weno_mix(weno_weight(fp - fpp), 2.0 * a_mid, -fpp / 2.0 + 3.0 * fp / 2.0, fp / 2.0 + f0 / 2.0);
     }
     if (lone) {
       ulc[c - 1] = f0;
     } else {
-      double fm = B.v(F_Q, c, n - st);
+      double fm = q(c, n - st);
       ulc[c - 1] = weno_mix(weno_weight(f0 - fm), 2.0 * a_mid, -fm / 2.0 + 3.0 * f0 / 2.0, f0 / 2.0 + fp / 2.0);
     }
   }
   roe_face(B, coord, n, n + st, ulc, urc, gamma, flux);
+}
+__device__ __forceinline__ void face_flux(const BlockView& B, int coord, long n, int pos, int lo,
+                                          int hi, long st, double gamma, double flux[5]) {
+  face_flux_q(B, coord, n, pos, lo, hi, st, gamma, flux, [&](int c, long m) { return B.v(F_Q, c, m); });
 }
 
 // ------------------------------------------------ inviscid flux, mixed precision
@@ -406,6 +413,71 @@ __global__ void __launch_bounds__(128, 10) k_inviscid_faces_mixed_o10(const Bloc
   faces_body<true>(blocks, cc);
 }
 __global__ void k_inviscid_faces_mixed(const BlockView* __restrict__ blocks, CaseConsts cc) { faces_body<true>(blocks, cc); }
+
+// The FP64 face kernel with its WENO stencil values staged in shared memory
+// (inviscid tile -10).  A CTA's 128 faces are consecutive in the face box (i
+// fastest), so the nodes their stencils read (n - st .. n + 2 st) lie in one
+// index range of the block, from the first face's node - st to the last
+// face's node + 2 st, clamped to the block: about 150 nodes along i and 230
+// along j on the plate's blocks.  The CTA copies that range of the five q
+// components once, coalesced, and each face reads its four values per
+// component from there; the metrics come from global memory as before.
+// Where the range exceeds kStageSpan nodes (the k faces, whose stride is a
+// whole plane, and long j strides) the faces read global memory.  The
+// arithmetic is face_flux's, so the results are the same bits.
+constexpr int kStageSpan = 512;
+__global__ void __launch_bounds__(128, 8) k_inviscid_faces_staged(const BlockView* __restrict__ blocks,
+                                                                 CaseConsts cc) {
+  __shared__ double sq[5][kStageSpan];
+  const BlockView& B = blocks[blockIdx.y];
+  if (B.retired()) return;
+  const int d = blockIdx.z;
+  if (d >= (cc.dimension == IFLAG_3D && !B.planar() ? 3 : 2)) return;
+  const Box& b1 = B.b1;
+  Box e = b1;
+  if (d == 0) e.is -= 1; else if (d == 1) e.js -= 1; else e.ks -= 1;
+  const long nf = e.size();
+  const long t0 = (long)blockIdx.x * blockDim.x;
+  if (t0 >= nf) return;  // the whole CTA
+  auto node_of = [&](long t) {
+    int i = e.is + (int)(t % e.nx());
+    long r = t / e.nx();
+    int j = e.js + (int)(r % e.ny());
+    int k = e.ks + (int)(r / e.ny());
+    return B.at(i, j, k);
+  };
+  const long st = d == 0 ? 1 : (d == 1 ? (long)B.nx : (long)B.nx * B.ny);
+  const long first = max(node_of(t0) - st, 0L);
+  const long last = min(node_of(min(t0 + (long)blockDim.x, nf) - 1) + 2 * st, B.b.size() - 1);
+  const long span = last - first + 1;
+  const bool staged = span <= kStageSpan;  // the same for every thread of the CTA
+  if (staged) {
+    for (long x = threadIdx.x; x < 5 * span; x += blockDim.x) {
+      const int c = (int)(x / span);
+      const long o = x - c * span;
+      sq[c][o] = B.v(F_Q, c + 1, first + o);
+    }
+    __syncthreads();
+  }
+  const long t = t0 + threadIdx.x;
+  if (t >= nf) return;
+  int i = e.is + (int)(t % e.nx());
+  long r = t / e.nx();
+  int j = e.js + (int)(r % e.ny());
+  int k = e.ks + (int)(r / e.ny());
+  long n = B.at(i, j, k);
+  const int pos = d == 0 ? i : (d == 1 ? j : k);
+  const int lo = d == 0 ? B.b.is : (d == 1 ? B.b.js : B.b.ks);
+  const int hi = d == 0 ? B.b.ie : (d == 1 ? B.b.je : B.b.ke);
+  double f[5];
+  if (staged)
+    face_flux_q(B, d + 1, n, pos, lo, hi, st, cc.gamma, f, [&](int c, long m) { return sq[c - 1][m - first]; });
+  else
+    face_flux(B, d + 1, n, pos, lo, hi, st, cc.gamma, f);
+  double* out = B.f[F_FIH] + (long)(5 * d) * B.plane + n;
+#pragma unroll
+  for (int c = 0; c < 5; ++c) out[(long)c * B.plane] = f[c];
+}
 
 __global__ void k_inviscid_combine(const BlockView* __restrict__ blocks, CaseConsts cc) {
   const BlockView& B = blocks[blockIdx.y];

@@ -397,11 +397,11 @@ __device__ __forceinline__ double row_dot5(const R* m, int mst, const double* x,
   return s;
 }
 
-// Bounded mbarrier waits (well under a second).  The staged sweep takes its
-// budget as an argument (aero_set_poll_budget; this is the default and the
-// largest), except for the producer's final wait for its own copies in
-// flight, which always has the full budget so that no copy lands after the
-// CTA has left.
+// Poll budget of the staged sweep's mbarrier waits (well under a second).  It
+// takes its budget as an argument (aero_set_poll_budget; this is the default
+// and the largest), except for the producer's final wait for its own copies
+// in flight, which always has the full budget so that no copy lands after the
+// CTA has left.  The cluster sweeps bound their waits by time (wait_bounded).
 constexpr long kSpinLimit = 1L << 20;
 
 // Rows r0 .. r0+nr-1 (nr <= 3) of plane-local node `t` of one plane of the
@@ -978,10 +978,7 @@ __device__ __forceinline__ void bulk_to_cluster(unsigned dst, unsigned src, unsi
                : "memory");
 }
 __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
-  long spins = 0;
-  while (!mbar_try_wait(bar, parity))
-    if (++spins > kSpinLimit) return false;
-  return true;
+  return wait_bounded([&] { return mbar_try_wait(bar, parity); });
 }
 // "no wait has run out" in the bulk sweep's failure stamp
 constexpr unsigned kNoFailure = 0xffffffffu;
@@ -1135,8 +1132,10 @@ __device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ bl
     int cnt_prev = 0;
     if (gs > 0) {
       cnt_prev = count_of(gs - 1);
-      if (!failed_by(gs - 1) && !mbar_wait_bounded(&xbar[(gs - 1) & 1], (unsigned)(((gs - 1) >> 1) & 1)))
+      if (!failed_by(gs - 1) && !mbar_wait_bounded(&xbar[(gs - 1) & 1], (unsigned)(((gs - 1) >> 1) & 1))) {
         fail_at(gs);
+        note_timeout(status, TS_BULK, (int)(blockIdx.x / ncta), (int)me, gs, TW_PLANE);
+      }
     }
     if (gs == H) cluster_sync_all();  // the forward dq* stores, for dsv
     const double* prev = xring + ((gs - 1) & 1) * HS;
@@ -1181,8 +1180,10 @@ __device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ bl
   }
   // the last plane's bytes
   if (H > 0 && !failed_by(2 * H - 1) &&
-      !mbar_wait_bounded(&xbar[(2 * H - 1) & 1], (unsigned)(((2 * H - 1) >> 1) & 1)))
+      !mbar_wait_bounded(&xbar[(2 * H - 1) & 1], (unsigned)(((2 * H - 1) >> 1) & 1))) {
     fail_at(2 * H);
+    note_timeout(status, TS_BULK, (int)(blockIdx.x / ncta), (int)me, 2 * H, TW_LAST_PLANE);
+  }
   __syncthreads();
   // every CTA's outcome is final once all have reached the barrier; each
   // reads the others' and no CTA leaves before all have read
@@ -1204,8 +1205,7 @@ __device__ __forceinline__ void lusgs_bulk_body(const BlockView* __restrict__ bl
       for (int h = 0; h < 2; ++h) {
         const int a = h ? armed1 : armed0;
         if (a >= 0)
-          for (long s = 0; s < kSpinLimit && !mbar_try_wait(&xbar[h], (unsigned)((a >> 1) & 1)); ++s) {
-          }
+          wait_bounded([&] { return mbar_try_wait(&xbar[h], (unsigned)((a >> 1) & 1)); });
       }
       for (int s = 0; s < 2000; ++s) __nanosleep(1000);
       if (status) atomicOr(status, (unsigned)ST_TIMEOUT);
@@ -1411,12 +1411,16 @@ __device__ __forceinline__ void lusgs_slab_body(const BlockView* __restrict__ bl
       if (G.need_up(gs)) {
         // the upstream slab's edge values of step gs-1, copied into inbox slot xp
         if (tid == 0) slab::bar_expect(&full[xp], slot_bytes);
-        fail = !slab::bar_wait(&full[xp], (parity >> xp) & 1u, kSpinLimit);
+        fail = !slab::bar_wait(&full[xp], (parity >> xp) & 1u);
         parity ^= 1u << xp;
+        if (fail) note_timeout(status, TS_SLAB, (int)(blockIdx.x / ncta), G.me, gs, TW_PLANE);
       }
       // room downstream: it has completed step gs-D+1, which waited for the
       // previous copy into slot x (so that copy also finished reading stage x)
-      if (!fail && need_dn) fail = !slab::wait_for(&s_prog[fwd ? 1 : 0], gs - D + 1, kSpinLimit);
+      if (!fail && need_dn) {
+        fail = !slab::wait_for(&s_prog[fwd ? 1 : 0], gs - D + 1);
+        if (fail) note_timeout(status, TS_SLAB, (int)(blockIdx.x / ncta), G.me, gs, TW_PROGRESS);
+      }
       if (!fail && tid < 5 * n) {  // the launch gives every row of a slab's plane a thread
         const int hp = G.plane(gs > 0 ? gs - 1 : 0);
         const int p0 = G.seg(hp, G.c0), np = G.seg(hp, G.c1) - p0;

@@ -78,6 +78,7 @@ __global__ void k_inviscid_mixed_128(const BlockView* __restrict__ blocks, CaseC
 __global__ void k_inviscid_faces(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_inviscid_faces_o6(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_inviscid_faces_o8(const BlockView* __restrict__ blocks, CaseConsts cc);
+__global__ void k_inviscid_faces_staged(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_inviscid_faces_mixed_o10(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_inviscid_faces_mixed(const BlockView* __restrict__ blocks, CaseConsts cc);
 __global__ void k_inviscid_combine(const BlockView* __restrict__ blocks, CaseConsts cc);

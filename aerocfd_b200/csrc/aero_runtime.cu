@@ -239,7 +239,8 @@ struct State {
   bool rhsi_ghosts_zero = false;
   // launch shapes (aero_autotune); none of them changes the arithmetic
   struct Tune {
-    int inv_tile = 64;  // nodes per CTA of the inviscid flux; 0: face-based kernels (-6, -8: FP64 faces for 6, 8 CTAs/SM)
+    int inv_tile = 64;  // nodes per CTA of the inviscid flux; 0: face-based kernels (-6, -8: FP64 faces for 6, 8 CTAs/SM;
+                        // -10: FP64 faces with shared-memory stencils)
     int ew = 256;       // threads per CTA of the element-wise kernels
     int visc = 128;     // threads per CTA of k_viscous_a
     int bound = 0;      // 1: the register-bounded FP64 k_viscous_a
@@ -638,7 +639,10 @@ int launch_inviscid(const BlockView* views, int nblk, long maxN, long maxN1, lon
     // SM; in mixed precision both take the mixed kernel bounded for 10)
     long maxF = maxN1 + maxFace;
     auto faces = g.mixed ? (tile < 0 ? k_inviscid_faces_mixed_o10 : k_inviscid_faces_mixed)
-                         : (tile == -6 ? k_inviscid_faces_o6 : tile == -8 ? k_inviscid_faces_o8 : k_inviscid_faces);
+                         : (tile == -6    ? k_inviscid_faces_o6
+                            : tile == -8  ? k_inviscid_faces_o8
+                            : tile == -10 ? k_inviscid_faces_staged
+                                          : k_inviscid_faces);
     PROF_ON(P_INVISCID, st, (faces<<<dim3(cdiv(maxF, 128), nblk, 3), 128, 0, st>>>(views, cc)));
     CKL();
     PROF_ON(P_INVISCID, st, (k_inviscid_combine<<<dim3(cdiv(maxN1, g.tune.ew), nblk), g.tune.ew, 0, st>>>(views, cc)));
@@ -1223,8 +1227,10 @@ int aero_init(int device) {
   CK(cudaEventCreateWithFlags(&g.ev_join2, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&g.ev_prep, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&g.ev_resid, cudaEventDisableTiming));
-  CK(cudaMalloc(&g.d_status, sizeof(unsigned)));
-  CK(cudaMemset(g.d_status, 0, sizeof(unsigned)));
+  // word 0: the status word; words 1..6: the first cluster-sweep wait that
+  // gave up (note_timeout, aero_timeout_site)
+  CK(cudaMalloc(&g.d_status, 8 * sizeof(unsigned)));
+  CK(cudaMemset(g.d_status, 0, 8 * sizeof(unsigned)));
   CK(cudaMalloc(&g.d_out, 16 * sizeof(double)));
   CK(cudaMallocHost(&g.h_out, 16 * sizeof(double)));
   g.device = device;
@@ -1487,7 +1493,7 @@ int aero_autotune(int iters) {
   // exchange), since the exchanges are only eligible for some sizes
   int sweep_mode = 4 * g.tune.sweep_cl + g.tune.sweep_x;
   struct Knob { int* v; std::vector<int> cand; };
-  std::vector<Knob> knobs = {{&g.tune.inv_tile, {0, -6, -8, 32, 64, 128}}, {&g.tune.ew, {128, 256, 512}},
+  std::vector<Knob> knobs = {{&g.tune.inv_tile, {0, -6, -8, -10, 32, 64, 128}}, {&g.tune.ew, {128, 256, 512}},
                              {&g.tune.visc, {64, 128, 256}}, {&g.tune.mats, {64, 128, 256}},
                              {&g.tune.nst_max, {2, 3, 4}},
                              {&sweep_mode, {0, 8, 16, 32, 9, 17, 33, 10, 18, 34, 11, 19, 35}},
@@ -1535,7 +1541,7 @@ int aero_set_tuning(int inv_tile, int ew, int visc, int mats, int nst_max) {
   int rc = need_init();
   if (rc) return rc;
   auto in = [](int v, std::initializer_list<int> ok) { return std::find(ok.begin(), ok.end(), v) != ok.end(); };
-  if (!in(inv_tile, {-8, -6, 0, 32, 64, 128}) || !in(ew, {128, 256, 512}) || !in(visc, {64, 128, 256}) ||
+  if (!in(inv_tile, {-10, -8, -6, 0, 32, 64, 128}) || !in(ew, {128, 256, 512}) || !in(visc, {64, 128, 256}) ||
       !in(mats, {64, 128, 256}) || !in(nst_max, {2, 3, 4}))
     return fail(AERO_ERR_ARG, "launch shape %d/%d/%d/%d/%d is not one the autotuner offers", inv_tile, ew, visc, mats,
                 nst_max);
@@ -1643,6 +1649,17 @@ int aero_get_status(unsigned* status) {
   CK(cudaMemsetAsync(g.d_status, 0, sizeof(unsigned), g.stream));
   CK(cudaStreamSynchronize(g.stream));
   *status = h;
+  return AERO_OK;
+}
+
+int aero_timeout_site(int* out5) {
+  int rc = need_init();
+  if (rc) return rc;
+  unsigned h[7] = {0, 0, 0, 0, 0, 0, 0};
+  CK(cudaMemcpyAsync(h, g.d_status, 7 * sizeof(unsigned), cudaMemcpyDeviceToHost, g.stream));
+  CK(cudaMemsetAsync(g.d_status + 1, 0, 6 * sizeof(unsigned), g.stream));
+  CK(cudaStreamSynchronize(g.stream));
+  for (int x = 0; x < 5; ++x) out5[x] = h[1] ? (int)h[2 + x] : -1;
   return AERO_OK;
 }
 

@@ -516,10 +516,14 @@ __global__ void __launch_bounds__(512, 1) k_sa_sweep_slab(const BlockView* __res
       bool fail = false;
       if (G.need_up(gs)) {
         if (tid == 0) slab::bar_expect(&full[xp], slot_bytes);
-        fail = !slab::bar_wait(&full[xp], (parity >> xp) & 1u, 1L << 20);
+        fail = !slab::bar_wait(&full[xp], (parity >> xp) & 1u);
         parity ^= 1u << xp;
+        if (fail) note_timeout(status, TS_SA_SLAB, (int)(blockIdx.x / ncta), G.me, gs, TW_PLANE);
       }
-      if (!fail && need_dn) fail = !slab::wait_for(&s_prog[fwd ? 1 : 0], gs - D + 1, 1L << 20);
+      if (!fail && need_dn) {
+        fail = !slab::wait_for(&s_prog[fwd ? 1 : 0], gs - D + 1);
+        if (fail) note_timeout(status, TS_SA_SLAB, (int)(blockIdx.x / ncta), G.me, gs, TW_PROGRESS);
+      }
       if (!fail && tid < n) {  // the launch gives every node of a slab's plane a thread
         const int hp = G.plane(gs > 0 ? gs - 1 : 0);
         const int p0 = G.seg(hp, G.c0), np = G.seg(hp, G.c1) - p0;

@@ -290,6 +290,13 @@ module aerocfd_gpu
       integer(c_int) :: status
     end function
 
+    ! the first cluster-sweep wait that gave up: sweep, block, rank, step, wait
+    ! (all -1 when none did); clears the record
+    integer(c_int) function aero_timeout_site(out5) bind(C, name="aero_timeout_site")
+      import :: c_int
+      integer(c_int) :: out5(5)
+    end function
+
     ! per-block status words and retirement of failed blocks (batches)
     integer(c_int) function aero_get_block_status(out) bind(C, name="aero_get_block_status")
       import :: c_int

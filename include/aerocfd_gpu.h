@@ -88,6 +88,14 @@ int aero_finalize(void);
 const char* aero_last_error(void);
 /* OR of the device status bits raised since the last call; clears them. */
 int aero_get_status(unsigned* status);
+/* Where the first cluster-sweep wait that gave up (AERO_ST_TIMEOUT) was, since
+ * the last call: out5 = sweep (1: mean-flow bulk exchange, 2: mean-flow slab,
+ * 3: SA slab), block (0-based), the CTA's rank in its cluster, the step
+ * (plane step of the forward then backward pass) and the wait (1: a plane's
+ * values, 2: the downstream slab's progress, 3: the last plane's values);
+ * all -1 when none gave up.  Clears the record.  The cluster sweeps bound
+ * every wait by one second of the GPU's global timer. */
+int aero_timeout_site(int* out5);
 
 /* Per-block status and retirement (batches of independent cases, where a
  * case is one block; no counterpart in the reference, which stops the run).
@@ -330,8 +338,9 @@ int aero_autotune(int iters);
 const char* aero_tuning(void);
 /* Sets the launch shapes directly (e.g. to apply a saved tuning): inviscid
  * tile 0 (face-based kernels; -6 / -8: the FP64 face kernel under a register
- * bound for 6 / 8 CTAs per SM, and in mixed precision the mixed face kernel
- * bounded for 10), 32, 64 or 128; element-wise threads 128, 256,
+ * bound for 6 / 8 CTAs per SM, -10: the FP64 face kernel reading its WENO
+ * stencils from shared memory, and in mixed precision for any of the three
+ * the mixed face kernel bounded for 10), 32, 64 or 128; element-wise threads 128, 256,
  * 512; viscous and block-record threads 64, 128, 256; sweep stages 2..4. */
 int aero_set_tuning(int inv_tile, int ew, int visc, int mats, int nst_max);
 /* CTAs that share each block's LU-SGS sweep: 1 (one CTA per block, the

@@ -97,11 +97,12 @@ def test_graphs_and_autotune_change_no_result(gpu):
                                   lambda: grids.flat_plate(ni=17, nj=13, nk=7, dy_wall=1e-3)])
 def test_every_launch_shape_gives_the_same_bits(gpu, make):
     """All launch shapes the autotuner can pick, including the face-based
-    inviscid kernels (tile 0, and -6 / -8 under register bounds), in FP64 and
-    mixed precision: identical histories and states (the default shape is the
-    one checked against the oracle)."""
+    inviscid kernels (tile 0, -6 / -8 under register bounds, -10 with its
+    stencils staged in shared memory), in FP64 and mixed precision: identical
+    histories and states (the default shape is the one checked against the
+    oracle)."""
     shapes = [(64, 256, 128, 128, 4), (0, 128, 64, 64, 2), (32, 512, 256, 256, 3), (128, 256, 128, 128, 4),
-              (-6, 256, 128, 128, 4), (-8, 128, 256, 64, 3)]
+              (-6, 256, 128, 128, 4), (-8, 128, 256, 64, 3), (-10, 256, 128, 128, 4)]
     for mixed in (False, True):
         ref = None
         for x, shape in enumerate(shapes):
