@@ -271,7 +271,7 @@ __device__ __forceinline__ bool wait_bounded(Done done) {
 // Sweep codes and wait kinds of the first wait that gave up, recorded in
 // status words 1..6 (aero_timeout_site): word 1 claims the record, then the
 // sweep, the block, the CTA's rank in its cluster, the step and the wait.
-enum TimeoutSweep { TS_BULK = 1, TS_SLAB = 2, TS_SA_SLAB = 3 };
+enum TimeoutSweep { TS_BULK = 1, TS_SLAB = 2, TS_SA_SLAB = 3, TS_STAGED = 4 };
 enum TimeoutWait { TW_PLANE = 1, TW_PROGRESS = 2, TW_LAST_PLANE = 3 };
 __device__ __forceinline__ void note_timeout(unsigned* status, int sweep, int block, int rank, int step,
                                              int wait) {

@@ -585,6 +585,7 @@ __device__ __forceinline__ void lusgs_staged_body(const BlockView* __restrict__ 
     while (!mbar_try_wait(&full[ls], lph)) {
       if (++spins > spin_limit) {
         q.timeout = true;
+        note_timeout(status, TS_STAGED, (int)blockIdx.x, 0, gs, TW_PLANE);
         break;
       }
     }

@@ -90,7 +90,8 @@ const char* aero_last_error(void);
 int aero_get_status(unsigned* status);
 /* Where the first cluster-sweep wait that gave up (AERO_ST_TIMEOUT) was, since
  * the last call: out5 = sweep (1: mean-flow bulk exchange, 2: mean-flow slab,
- * 3: SA slab), block (0-based), the CTA's rank in its cluster, the step
+ * 3: SA slab, 4: the one-CTA staged sweep, whose waits have the poll budget
+ * of aero_set_poll_budget), block (0-based), the CTA's rank in its cluster, the step
  * (plane step of the forward then backward pass) and the wait (1: a plane's
  * values, 2: the downstream slab's progress, 3: the last plane's values);
  * all -1 when none gave up.  Clears the record.  The cluster sweeps bound

@@ -4,6 +4,7 @@ NaN planted in q between iterations, and a staged LU-SGS sweep whose producer
 never issues one plane's copies (aero_inject_sweep_stall), so that the
 consumers' bounded waits run out.  Each raises its status bit, the call itself
 returns normally, and the same context runs clean iterations afterwards."""
+import ctypes
 import time
 
 import numpy as np
@@ -86,8 +87,16 @@ def test_withheld_plane_times_out_and_recovers(gpu, graphs, plane):
     t0 = time.perf_counter()
     gc.step(1)
     waited = time.perf_counter() - t0
+    site = (ctypes.c_int * 5)()
+    assert gc.L.aero_timeout_site(site) == 0
     assert gc.status() & ST_TIMEOUT
     assert waited < 30.0
+    # the staged sweep (4), one of the case's blocks, its only CTA, the
+    # withheld plane's step, a plane's values (1)
+    assert site[0] == 4 and 0 <= site[1] < len(case.blocks) and site[2] == 0, list(site)
+    assert site[3] == plane and site[4] == 1, list(site)
+    gc.L.aero_timeout_site(site)
+    assert list(site) == [-1] * 5
     gc.inject_sweep_stall(-1)
     gc.set_poll_budget(1 << 20)
     clean_run_after(gpu, case, gc, snap)
