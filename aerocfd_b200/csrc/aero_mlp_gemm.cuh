@@ -6,9 +6,11 @@
 //
 // Per CTA (128 threads): one 128 x 128 FP32 accumulator in tensor memory (128
 // columns), A and B tiles of 128 x 64 BF16 staged in shared memory by the
-// threads' asynchronous 16-byte copies (cp.async) in the canonical no-swizzle
-// K-major layout (8-row x 16-byte core matrices; LBO = 128 B between core
-// matrices along K, SBO = 1024 B between 8-row groups), four stages so that
+// threads' asynchronous 16-byte copies (cp.async) in the 128-byte-swizzled
+// K-major layout (each tile row one 128-byte line, its 16-byte chunk c stored
+// at chunk c ^ (row % 8); SBO = 1024 B between 8-row groups, the K = 16 steps
+// 32 bytes apart inside the row), so a warp's copies fill four whole lines
+// (no bank conflicts) from four whole rows of global memory, four stages so that
 // the copies of the next three K-tiles are in flight while the tensor cores
 // work, four kind::f16 MMAs of K = 16 per tile issued by one thread,
 // completion through tcgen05.commit on the stage's mbarrier, and the epilogue
@@ -24,14 +26,18 @@ constexpr int kBM = 128, kBN = 128, kBK = 64;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// Shared-memory matrix descriptor (tcgen05): start >> 4 in [0,14), LBO >> 4 in
-// [16,30), SBO >> 4 in [32,46), version 1 in [46,48), no swizzle.
-__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+// Shared-memory matrix descriptor (tcgen05) of a tile in the 128-byte-swizzled
+// K-major layout (1024-byte aligned 8-row groups): start >> 4 in [0,14), the
+// leading offset in [16,30) (not used when the K step stays inside the
+// 128-byte row), SBO = 1024 B >> 4 in [32,46), version 1 in [46,48), layout
+// type SWIZZLE_128B (2) in [61,64).
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t addr) {
   uint64_t d = 0;
   d |= (uint64_t)((addr >> 4) & 0x3FFFu);
-  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
-  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)(1024 >> 4) << 32;
   d |= 1ull << 46;
+  d |= 2ull << 61;
   return d;
 }
 // Instruction descriptor, kind::f16: FP32 accumulator, BF16 A and B, both
@@ -104,7 +110,8 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(const uint16_t* __restrict__ 
   const uint32_t tmem = tmem_slot;
   const uint32_t idesc = idesc_bf16(kBM, kBN);
   // this thread's 16-byte chunks of tile t into stage x: chunk c = tid + 128 j
-  // (j < 8) of the A and of the B tile, row c / 8, K-chunk c % 8
+  // (j < 8) of the A and of the B tile, row c / 8, K-chunk c % 8, stored at
+  // row * 128 + ((K-chunk ^ row % 8) * 16)
   auto copy_tile = [&](int t, int x) {
     const int k0 = kbeg + t * kBK;
     const uint32_t sA = base_s + (uint32_t)x * stage_bytes;
@@ -113,7 +120,7 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(const uint16_t* __restrict__ 
     for (int j = 0; j < 8; ++j) {
       const int c = tid + 128 * j;
       const int r = c >> 3, kc = c & 7;
-      const uint32_t so = (uint32_t)(((r >> 3) * 512 + kc * 64 + (r & 7) * 8) * sizeof(uint16_t));
+      const uint32_t so = (uint32_t)(r * 128 + ((kc ^ (r & 7)) << 4));
       asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sA + so),
                    "l"(A + (long)(m0 + r) * K + k0 + kc * 8)
                    : "memory");
@@ -139,8 +146,8 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(const uint16_t* __restrict__ 
       const uint32_t sB = sA + kBM * kBK * sizeof(uint16_t);
 #pragma unroll
       for (int kk = 0; kk < kBK / 16; ++kk) {
-        uint64_t da = umma_desc(sA + kk * 256, 128, 1024);
-        uint64_t db = umma_desc(sB + kk * 256, 128, 1024);
+        uint64_t da = umma_desc_sw128(sA + kk * 32);
+        uint64_t db = umma_desc_sw128(sB + kk * 32);
         uint32_t acc = (t > 0 || kk > 0) ? 1u : 0u;
         asm volatile(
             "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
