@@ -182,7 +182,7 @@ int gemm(const uint16_t* A, const uint16_t* B, float* C, int M, int N, int K, in
     MCK(cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
     smem_dev = dev;
   }
-  k_gemm_bf16<<<grid, 128, kGemmSmem, st>>>(A, B, splits > 1 ? scratch : C, M, N, K, klen, status);
+  k_gemm_bf16<<<grid, kGemmThreads, kGemmSmem, st>>>(A, B, splits > 1 ? scratch : C, M, N, K, klen, status);
   MCK(cudaGetLastError());
   if (splits > 1) {
     long n = (long)M * N;

@@ -10,9 +10,11 @@
 // K-major layout (each tile row one 128-byte line, its 16-byte chunk c stored
 // at chunk c ^ (row % 8); SBO = 1024 B between 8-row groups, the K = 16 steps
 // 32 bytes apart inside the row), so a warp's copies fill four whole lines
-// (no bank conflicts) from four whole rows of global memory, four stages so that
-// the copies of the next three K-tiles are in flight while the tensor cores
-// work, four kind::f16 MMAs of K = 16 per tile issued by one thread,
+// (no bank conflicts) from four whole rows of global memory, three stages so
+// that the copies of the next two K-tiles are in flight while the tensor cores
+// work, and two CTAs per SM (97 KB of shared memory and 128 TMEM columns
+// each), so one CTA's copies, MMAs or epilogue overlap the other's; four
+// kind::f16 MMAs of K = 16 per tile issued by one thread,
 // completion through tcgen05.commit on the stage's mbarrier, and the epilogue
 // reading tensor memory with tcgen05.ld (warp w reads lanes 32w..32w+31 =
 // rows).  Every wait is bounded; the tensor memory is always released.
@@ -47,9 +49,11 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
 }
 
 constexpr long kGemmSpin = 1L << 22;
-// Dynamic shared memory of k_gemm_bf16: four stages of A and B tiles (4 x 2 x
-// 16 KB) plus slack to align the first tile to 1024 bytes.
-constexpr int kGemmStages = 4;
+// Dynamic shared memory of k_gemm_bf16: three stages of A and B tiles (3 x 2 x
+// 16 KB) plus slack to align the first tile to 1024 bytes; two CTAs of
+// kGemmThreads fit on an SM.
+constexpr int kGemmStages = 3;
+constexpr int kGemmThreads = 128;
 constexpr size_t kGemmSmem = (size_t)kGemmStages * (kBM + kBN) * kBK * sizeof(uint16_t) + 1024;
 
 __device__ __forceinline__ bool gemm_try_wait(uint32_t bar, unsigned parity) {
@@ -75,7 +79,7 @@ __device__ __forceinline__ bool gemm_wait(uint32_t bar, unsigned parity, long bu
 // issues the tile's MMAs and commits them on the stage's mbarrier; then the
 // stage of tile t-1 is refilled with tile t+S-1 once that tile's commit has
 // arrived (its MMAs have read the stage).
-__global__ void __launch_bounds__(128) k_gemm_bf16(const uint16_t* __restrict__ A, const uint16_t* __restrict__ B,
+__global__ void __launch_bounds__(kGemmThreads, 2) k_gemm_bf16(const uint16_t* __restrict__ A, const uint16_t* __restrict__ B,
                                                   float* __restrict__ C, int M, int N, int K, int klen,
                                                   unsigned* status) {
   constexpr int S = kGemmStages;
@@ -109,16 +113,16 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(const uint16_t* __restrict__ 
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_slot;
   const uint32_t idesc = idesc_bf16(kBM, kBN);
-  // this thread's 16-byte chunks of tile t into stage x: chunk c = tid + 128 j
-  // (j < 8) of the A and of the B tile, row c / 8, K-chunk c % 8, stored at
-  // row * 128 + ((K-chunk ^ row % 8) * 16)
+  // this thread's 16-byte chunks of tile t into stage x: chunk c = tid +
+  // kGemmThreads j of the A and of the B tile (1024 chunks each), row c / 8,
+  // K-chunk c % 8, stored at row * 128 + ((K-chunk ^ row % 8) * 16)
   auto copy_tile = [&](int t, int x) {
     const int k0 = kbeg + t * kBK;
     const uint32_t sA = base_s + (uint32_t)x * stage_bytes;
     const uint32_t sB = sA + kBM * kBK * sizeof(uint16_t);
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const int c = tid + 128 * j;
+    for (int j = 0; j < 1024 / kGemmThreads; ++j) {
+      const int c = tid + kGemmThreads * j;
       const int r = c >> 3, kc = c & 7;
       const uint32_t so = (uint32_t)(r * 128 + ((kc ^ (r & 7)) << 4));
       asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sA + so),
@@ -188,13 +192,17 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(const uint16_t* __restrict__ 
   }
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (!abort_flag) {
-    const int row = m0 + warp * 32 + lane;
+    // warp w reads accumulator lanes 32 (w % 4) .. +31 (its rows) and the
+    // (w / 4)-th share of the columns
+    const int quarter = warp & 3;
+    const int ncol = kBN / (kGemmThreads / 128), col0 = (warp >> 2) * ncol;
+    const int row = m0 + quarter * 32 + lane;
 #pragma unroll 1
-    for (int j = 0; j < kBN; j += 8) {
+    for (int j = col0; j < col0 + ncol; j += 8) {
       uint32_t v[8];
       asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
-                   : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)j));
+                   : "r"(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)j));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       float* out = Cs + (long)row * N + n0 + j;
       *(float4*)out = make_float4(__uint_as_float(v[0]), __uint_as_float(v[1]), __uint_as_float(v[2]),
