@@ -94,7 +94,8 @@ def test_graphs_and_autotune_change_no_result(gpu):
 
 
 @pytest.mark.parametrize("make", [lambda: grids.naca_ogrid(nblk=4, ni=33, nj=17, nk=3),
-                                  lambda: grids.flat_plate(ni=17, nj=13, nk=7, dy_wall=1e-3)])
+                                  lambda: grids.flat_plate(ni=17, nj=13, nk=7, dy_wall=1e-3),
+                                  lambda: naca_2d_sa()])
 def test_every_launch_shape_gives_the_same_bits(gpu, make):
     """All launch shapes the autotuner can pick, including the face-based
     inviscid kernels (tile 0, -6 / -8 under register bounds, -10 with its
@@ -128,9 +129,16 @@ def test_every_launch_shape_gives_the_same_bits(gpu, make):
                 assert np.array_equal(a, b), (mixed, shape)
 
 
+def naca_2d_sa():
+    from aerocfd_b200.case import IFLAG_2D, IFLAG_NSSOLVER, IFLAG_SA, Config
+    cfg = Config(solver=IFLAG_NSSOLVER, ma=0.5, re=5000.0, aoa_deg=2.0, cfl=2.0, dimension=IFLAG_2D,
+                 turbulence=IFLAG_SA)
+    return grids.naca_ogrid(nblk=4, ni=33, nj=17, first=1e-3, cfg=cfg)
+
+
 @pytest.mark.parametrize("make", [lambda: grids.naca_ogrid(nblk=4, ni=33, nj=17, nk=3),
                                   lambda: grids.flat_plate(ni=17, nj=13, nk=7, dy_wall=1e-3),
-                                  lambda: grids.bump_channel(129, 65, 9)])
+                                  lambda: grids.bump_channel(129, 65, 9), naca_2d_sa])
 def test_sweep_cluster_gives_the_same_bits(gpu, make):
     """The LU-SGS sweep on one CTA per block (staged in shared memory, or from
     global memory when the planes are too large: the 129 x 65 x 9 bump) and
@@ -140,7 +148,8 @@ def test_sweep_cluster_gives_the_same_bits(gpu, make):
     taken where the device holds one); the SA sweep (the plate) on one CTA or
     on clusters of k-slabs: identical histories and states, in FP64 and mixed
     precision.  Slab clusters larger than a block's k-extent leave CTAs idle
-    (the aerofoil: one k-offset), and slabs too wide for one CTA fall back to
+    (the aerofoil: one k-offset; the 2-D aerofoil: a single plane, so one
+    active CTA per slab cluster), and slabs too wide for one CTA fall back to
     the bulk or the L2 exchange (the bump on 2 and 4 CTAs)."""
     from aerocfd_b200 import _lib
     for mixed in (False, True):
