@@ -130,6 +130,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-converge", action="store_true", help="skip the time-to-1e-8 runs")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-case batch")
+    ap.add_argument("--batch-split", action="store_true",
+                    help="at N > 1, also split the 64-case batch over the ranks by whole cases")
     ap.add_argument("--no-warm-start", action="store_true", help="skip the learned warm start")
     ap.add_argument("--no-plate", action="store_true", help="skip the plate's 3000-iteration runs")
     ap.add_argument("--no-schemes", action="store_true", help="skip the WENO5 / WCNS5 workloads")
@@ -920,7 +922,7 @@ def main():
             nm["cpu_baseline"] = {"value": v, "unit": "Mcell-iter/s", "cores": thr, "kind": "port",
                                   "sample": f"{n} full iterations, {el:.1f} s, {thr} threads (one per block)"}
         line["naca"] = nm
-    if world > 1 and not args.no_batch:
+    if world > 1 and args.batch_split:
         line["batched_split"] = batched_split_gpu(solver, max(5, min(args.steps, 20)), args.warmup, rank, world,
                                                   dist)
     if world == 1 and not args.no_batch:
