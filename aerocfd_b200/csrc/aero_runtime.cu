@@ -2345,6 +2345,34 @@ int aero_getpri_all(void) {
   int rc = need_setup();
   return rc ? rc : do_getpri_all();
 }
+// The reference's 2-D names (sub_bc_updatebuffer2d.f90:10,
+// sub_bc_updatebufferaverage2d.f90:10, :317, sub_bc_updatebuffercoordinate2d.f90:10):
+// the same tables, which a 2-D configuration builds with the 2-D index maps;
+// in a 3-D configuration they are an error, as calling them there would be a
+// mistake in the caller.
+static int need_2d(const char* name) {
+  int rc = need_setup();
+  if (rc) return rc;
+  if (g.cc.dimension != IFLAG_2D) return fail(AERO_ERR_STATE, "%s: the case is not 2-D (iflag_dimension = %d)", name,
+                                               g.cc.dimension);
+  return AERO_OK;
+}
+int aero_updatebuffer2d(void) {
+  int rc = need_2d("UpdateBuffer2d");
+  return rc ? rc : do_halo();
+}
+int aero_average2d1(void) {
+  int rc = need_2d("average2d1");
+  return rc ? rc : do_average1();
+}
+int aero_average2d2(void) {
+  int rc = need_2d("average2d2");
+  return rc ? rc : do_average2();
+}
+int aero_updatebuffercoordinate2d(void) {
+  int rc = need_2d("UpdateBufferCoordinate2d");
+  return rc ? rc : aero_updatebuffercoordinate();
+}
 
 int aero_residual(double* out7) {
   int rc = need_setup();

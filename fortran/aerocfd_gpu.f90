@@ -266,6 +266,19 @@ module aerocfd_gpu
     integer(c_int) function aero_updatebuffercoordinate() bind(C, name="aero_updatebuffercoordinate")
       import :: c_int
     end function
+    ! the reference's 2-D names (2-D cases only)
+    integer(c_int) function aero_updatebuffer2d() bind(C, name="aero_updatebuffer2d")
+      import :: c_int
+    end function
+    integer(c_int) function aero_average2d1() bind(C, name="aero_average2d1")
+      import :: c_int
+    end function
+    integer(c_int) function aero_average2d2() bind(C, name="aero_average2d2")
+      import :: c_int
+    end function
+    integer(c_int) function aero_updatebuffercoordinate2d() bind(C, name="aero_updatebuffercoordinate2d")
+      import :: c_int
+    end function
     integer(c_int) function aero_init_walldist() bind(C, name="aero_init_walldist")
       import :: c_int
     end function

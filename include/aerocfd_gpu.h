@@ -277,6 +277,12 @@ int aero_updatebuffer(void);         /* sub_bc_updatebuffer.f90:10          */
 int aero_average1(void);             /* sub_bc_updatebufferaverage.f90:10   */
 int aero_average2(void);             /* sub_bc_updatebufferaverage.f90:442  */
 int aero_updatebuffercoordinate(void); /* sub_bc_updatebuffercoordinate.f90:10 */
+/* The same under the reference's 2-D names, for the iflag_dimension = 2 arms
+ * of main.f90:142-146, :310-318, :424-432; AERO_ERR_STATE in a 3-D case. */
+int aero_updatebuffer2d(void);       /* sub_bc_updatebuffer2d.f90:10        */
+int aero_average2d1(void);           /* sub_bc_updatebufferaverage2d.f90:10 */
+int aero_average2d2(void);           /* sub_bc_updatebufferaverage2d.f90:317 */
+int aero_updatebuffercoordinate2d(void); /* sub_bc_updatebuffercoordinate2d.f90:10 */
 /* sub_output_residual.f90:8: out7 = rms of rho,rho*u,rho*v,rho*w,rho*E,
  * nut, (unused) over the updated nodes / totalnodes; the reference prints
  * these and appends them to resi_history.dat. */

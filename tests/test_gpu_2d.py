@@ -161,3 +161,37 @@ def test_2d_crank_time_steps(gpu, oracle_mod):
         assert gc.status() == 0
     finally:
         gc.close()
+
+
+def test_2d_named_halo_entries(gpu, oracle_mod):
+    """aero_updatebuffer2d, aero_average2d1 and aero_average2d2 (the
+    reference's 2-D names) on random q and nut match the oracle's
+    UpdateBuffer2d / average2d1 / average2d2 bit for bit; in a 3-D case they
+    refuse with AERO_ERR_STATE."""
+    co, cg = naca2d_sa(), naca2d_sa()
+    rng = np.random.default_rng(7)
+    for bo, bg in zip(co.blocks, cg.blocks):
+        for name in ("q", "nut"):
+            bo.fields[name][...] = 1.0 + rng.random(bo.fields[name].shape)
+            bg.fields[name][...] = bo.fields[name]
+    oc = oracle_mod.OracleCase(co)
+    gc = gpu.GpuCase(cg)
+    try:
+        gc.sync_to_device(gpu.mask("q", "nut"))
+        for f in ("aero_updatebuffer2d", "aero_average2d1", "aero_average2d2"):
+            assert getattr(gc.L, f)() == 0, f
+        gc.sync_to_host(gpu.mask("q", "nut"))
+        oc.updatebuffer()
+        oc.average1()
+        oc.average2()
+        for bo, bg in zip(co.blocks, cg.blocks):
+            for name in ("q", "nut"):
+                assert np.array_equal(bg.fields[name], bo.fields[name]), (bo.m, name)
+    finally:
+        gc.close()
+    g3 = gpu.GpuCase(grids.naca_ogrid(nblk=4, ni=17, nj=9, nk=3))
+    try:
+        for f in ("aero_updatebuffer2d", "aero_average2d1", "aero_average2d2", "aero_updatebuffercoordinate2d"):
+            assert getattr(g3.L, f)() == 2, f   # AERO_ERR_STATE
+    finally:
+        g3.close()
