@@ -26,7 +26,8 @@ def lib():
     return _lib.load()
 
 
-@pytest.mark.parametrize("M,N,K,splits", [(128, 128, 64, 1), (256, 384, 192, 1), (128, 256, 1024, 4), (384, 128, 640, 3)])
+@pytest.mark.parametrize("M,N,K,splits", [(128, 128, 64, 1), (256, 384, 192, 1), (128, 256, 1024, 4), (384, 128, 640, 3),
+                                          (256, 1024, 320, 1), (128, 1152, 256, 2)])
 def test_tensor_core_gemm(lib, M, N, K, splits):
     rng = np.random.default_rng(M + N + K)
     a = bf16_bits(rng.standard_normal((M, K)))
