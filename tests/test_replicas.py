@@ -59,3 +59,14 @@ def test_reference_arm_runs_on_rank_zero_only(rank):
     else:
         line = json.loads(p.stdout.strip().splitlines()[-1])
         assert line["impl"] == "reference" and line["n_gpus"] == 2 and line["value"] > 0
+
+
+def test_batch_split_is_opt_in(monkeypatch):
+    """At N > 1 the default run times replicas only; the split of the 64-case
+    batch over the ranks runs only with --batch-split."""
+    sys.path.insert(0, ROOT)
+    import bench
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--gpus", "2"])
+    assert bench.parse().batch_split is False
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--gpus", "2", "--batch-split"])
+    assert bench.parse().batch_split is True
